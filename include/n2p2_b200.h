@@ -1,0 +1,202 @@
+/*
+ * n2p2_b200.h -- C ABI of the B200 short-range (2G) HDNNP energy/force path.
+ *
+ * The entry points replace the short-range evaluation path of nnp::Mode
+ * (reference: src/libnnp/Mode.h and Mode.cpp of n2p2).  A handle of type
+ * n2p2_mode carries what an nnp::Mode object carries after setup (settings,
+ * elements, symmetry functions, scaling, networks); a handle of type
+ * n2p2_batch carries one or many nnp::Structure objects resident on the GPU.
+ * Each function names the reference member function it stands for.
+ *
+ * Conventions
+ *  - Every function returns an n2p2_status; 0 is success.  The message of the
+ *    last failure on the calling thread is returned by n2p2_last_error().
+ *    The status codes map the reference's exception types (see below); the
+ *    C ABI itself never throws.
+ *  - All arrays are plain host pointers unless a function says otherwise.
+ *    Lengths are in elements.  Positions, forces and neighbour vectors are
+ *    [atom][3] row-major doubles.  Boxes are [structure][3][3] with row k the
+ *    k-th cell vector (Structure::box).
+ *  - Element indices follow the element map of the settings file, i.e. the
+ *    elements sorted by atomic number (ElementMap::registerElements).
+ *  - Physical units are those of input.data; if the settings file defines
+ *    mean_energy/conv_energy/conv_length the library normalises internally
+ *    exactly like Prediction::readStructureFromFile / predict.
+ */
+#ifndef N2P2_B200_H
+#define N2P2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int n2p2_status;
+
+#define N2P2_OK 0
+#define N2P2_ERR_RUNTIME 1          /* std::runtime_error (settings, files, state)  */
+#define N2P2_ERR_RANGE 2            /* std::range_error                               */
+#define N2P2_ERR_OUT_OF_RANGE 3     /* std::out_of_range (stop on extrapolation)      */
+#define N2P2_ERR_INVALID_ARGUMENT 4 /* std::invalid_argument (cutoff parameters)      */
+#define N2P2_ERR_CUDA 5             /* CUDA runtime failure                           */
+#define N2P2_ERR_NULL 6             /* null handle or pointer                         */
+
+/* Precision of the symmetry-function and network stages. */
+#define N2P2_PRECISION_FP64 0       /* plain FP64 throughout                          */
+#define N2P2_PRECISION_MIXED 1      /* FP32 descriptors, FP64 cutoff/scaling/sums     */
+
+/* Flags of n2p2_batch_evaluate. */
+#define N2P2_EVAL_FORCES 1          /* Mode::evaluateNNP(useForces = true)            */
+#define N2P2_EVAL_STORE_DGDR 2      /* keep dG/dr per neighbour (Atom::Neighbor::dGdr) */
+#define N2P2_EVAL_NO_GRAPH 4        /* launch kernels one by one (no CUDA graph)      */
+
+typedef struct n2p2_mode n2p2_mode;
+typedef struct n2p2_batch n2p2_batch;
+
+/* Message of the last failure on this thread ("" if none). */
+const char* n2p2_last_error(void);
+
+/* Library version string. */
+const char* n2p2_version(void);
+
+/* ---- model set-up: nnp::Mode ------------------------------------------------ */
+
+/* new nnp::Mode bound to CUDA device `device` (Mode::Mode, Mode.cpp:43-54). */
+n2p2_status n2p2_mode_create(n2p2_mode** mode, int device);
+n2p2_status n2p2_mode_destroy(n2p2_mode* mode);
+
+/* Mode::initialize (Mode.cpp:56-160): prints nothing, kept for call parity. */
+n2p2_status n2p2_mode_initialize(n2p2_mode* mode);
+
+/* Mode::loadSettingsFile (Mode.cpp:162-211). */
+n2p2_status n2p2_mode_load_settings_file(n2p2_mode* mode, const char* fileName);
+
+/* Mode::setupGeneric (Mode.cpp:213-237), 2G-HDNNP path: normalisation,
+ * element map, elements, cutoff, symmetry functions (sorted), derivative
+ * tables, groups, network topology. */
+n2p2_status n2p2_mode_setup_generic(n2p2_mode* mode);
+
+/* Mode::setupSymmetryFunctionScaling (Mode.cpp:781-909). */
+n2p2_status n2p2_mode_setup_symmetry_function_scaling(n2p2_mode* mode, const char* fileName);
+
+/* Mode::setupSymmetryFunctionScalingNone (Mode.cpp:761-779). */
+n2p2_status n2p2_mode_setup_symmetry_function_scaling_none(n2p2_mode* mode);
+
+/* Mode::setupNeuralNetworkWeights (Mode.cpp:1514-1547); `fileNameFormat` is
+ * a printf format taking the atomic number, e.g. "weights.%03zu.data". */
+n2p2_status n2p2_mode_setup_neural_network_weights(n2p2_mode* mode, const char* fileNameFormat);
+
+/* NeuralNetwork::setConnections (NeuralNetwork.cpp:147-169) for one element,
+ * values in weights-file order. */
+n2p2_status n2p2_mode_set_connections(n2p2_mode* mode, int element, const double* connections, int64_t count);
+
+/* Mode::setupSymmetryFunctionStatistics (Mode.cpp:1172-1210).  Any non-zero
+ * flag enables the extrapolation check of every evaluation; with
+ * stopOnExtrapolationWarnings a warning makes evaluation fail with
+ * N2P2_ERR_OUT_OF_RANGE, with writeExtrapolationWarnings one line per atom is
+ * written to stderr. */
+n2p2_status n2p2_mode_setup_symmetry_function_statistics(n2p2_mode* mode, int collectStatistics,
+                                                         int collectExtrapolationWarnings,
+                                                         int writeExtrapolationWarnings,
+                                                         int stopOnExtrapolationWarnings);
+
+/* Precision of later evaluations (N2P2_PRECISION_*). */
+n2p2_status n2p2_mode_set_precision(n2p2_mode* mode, int precision);
+
+/* Mode::getMaxCutoffRadius (Mode.h:513). */
+n2p2_status n2p2_mode_get_max_cutoff_radius(n2p2_mode* mode, double* radius);
+
+/* Number of elements; symbol and index of element e (ElementMap). */
+n2p2_status n2p2_mode_get_num_elements(n2p2_mode* mode, int* count);
+n2p2_status n2p2_mode_get_element_symbol(n2p2_mode* mode, int element, char* buffer, int capacity);
+n2p2_status n2p2_mode_get_element_index(n2p2_mode* mode, const char* symbol, int* element);
+
+/* Element::numSymmetryFunctions (Element.h:161). */
+n2p2_status n2p2_mode_get_num_symmetry_functions(n2p2_mode* mode, int element, int* count);
+
+/* Element::getSymmetryFunctionNumTable()[neighborElement] (Element.h:188):
+ * dG/dr rows stored for a neighbour of element `neighborElement` around a
+ * centre of element `element`. */
+n2p2_status n2p2_mode_get_num_derivative_rows(n2p2_mode* mode, int element, int neighborElement, int* rows);
+
+/* ---- structures on the GPU: nnp::Structure ---------------------------------- */
+
+n2p2_status n2p2_batch_create(n2p2_mode* mode, n2p2_batch** batch);
+n2p2_status n2p2_batch_destroy(n2p2_batch* batch);
+
+/* Define the structures of the batch (Structure::readFromLines,
+ * Structure.cpp:142-271, without the text parsing).  numAtoms[s] atoms per
+ * structure, elements[atom], boxes[s][3][3] in physical units and
+ * periodic[s] (0 = isolated cluster).  With remap != 0 periodic positions are
+ * folded into the cell on the device exactly like Structure::remap
+ * (Structure.cpp:1224-1248). */
+n2p2_status n2p2_batch_set_structures(n2p2_batch* batch, int64_t numStructures, const int64_t* numAtoms,
+                                      const int32_t* elements, const double* boxes, const int32_t* periodic,
+                                      int remap);
+
+/* Positions [atom][3] in physical units; `onDevice` says whether `positions`
+ * is a device pointer.  Asynchronous on the batch's stream. */
+n2p2_status n2p2_batch_set_positions(n2p2_batch* batch, const double* positions, int onDevice);
+
+/* Mode::evaluateNNP (Mode.cpp:2029-2077) on every structure: neighbour list,
+ * symmetry functions, networks, energies and (flag) forces.  Asynchronous
+ * except for the first call after n2p2_batch_set_structures. */
+n2p2_status n2p2_batch_evaluate(n2p2_batch* batch, int flags);
+
+/* Wait for the batch's stream; reports device-side input errors. */
+n2p2_status n2p2_batch_synchronize(n2p2_batch* batch);
+
+/* Structure::energy per structure after Prediction::predict's conversion
+ * (physical units, atomic energy offsets added). */
+n2p2_status n2p2_batch_get_energies(n2p2_batch* batch, double* energies);
+
+/* Atom::f of every atom in physical units, [atom][3]. */
+n2p2_status n2p2_batch_get_forces(n2p2_batch* batch, double* forces);
+
+/* End-to-end: copy positions from host memory, evaluate, copy energies and
+ * forces back, all on the batch's stream (forces may be NULL without the
+ * force flag).  Pinned host memory from n2p2_host_alloc gives the fastest copies. */
+n2p2_status n2p2_batch_evaluate_host(n2p2_batch* batch, const double* positions, double* energies,
+                                     double* forces, int flags);
+
+/* Sizes. */
+n2p2_status n2p2_batch_get_num_atoms(n2p2_batch* batch, int64_t* atoms);
+n2p2_status n2p2_batch_get_num_neighbor_entries(n2p2_batch* batch, int64_t* entries);
+
+/* Neighbour lists in internal units (Atom::neighbors): offsets[N+1],
+ * index[M] (atom index in the batch), image[M] (periodic image code,
+ * ((bc0+p0)(2p1+1) + (bc1+p1))(2p2+1) + (bc2+p2)), d[M], dr[M][3].
+ * Any pointer may be NULL. */
+n2p2_status n2p2_batch_get_neighbors(n2p2_batch* batch, int64_t* offsets, int32_t* index, int32_t* image,
+                                     double* d, double* dr);
+
+/* Atom::G, Atom::dEdG (concatenated per atom, numSymmetryFunctions values each)
+ * and Atom::energy (internal units). */
+n2p2_status n2p2_batch_get_symmetry_functions(n2p2_batch* batch, double* G);
+n2p2_status n2p2_batch_get_dEdG(n2p2_batch* batch, double* dEdG);
+n2p2_status n2p2_batch_get_atomic_energies(n2p2_batch* batch, double* energies);
+
+/* Atom::dGdr (self, [sum numSF][3]) and Atom::Neighbor::dGdr (per entry,
+ * numDerivativeRows of the pair, [rows][3]); needs N2P2_EVAL_STORE_DGDR. */
+n2p2_status n2p2_batch_get_dGdr(n2p2_batch* batch, double* selfDGdr, double* neighborDGdr);
+
+/* Positions after remap and normalisation (internal units), [atom][3]. */
+n2p2_status n2p2_batch_get_internal_positions(n2p2_batch* batch, double* positions);
+
+/* Extrapolation warnings of the last evaluation: total and per atom (may be NULL). */
+n2p2_status n2p2_batch_get_extrapolation_warnings(n2p2_batch* batch, int64_t* total, int32_t* perAtom);
+
+/* Kernel launches issued by one evaluation with the last flags. */
+n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches);
+
+/* Pinned (page-locked) host memory for fast transfers. */
+n2p2_status n2p2_host_alloc(void** ptr, size_t bytes);
+n2p2_status n2p2_host_free(void* ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* N2P2_B200_H */

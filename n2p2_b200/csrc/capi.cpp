@@ -1,0 +1,523 @@
+// extern "C" boundary; see include/n2p2_b200.h.  Exceptions of the C++ layer
+// are turned into status codes here and never cross the ABI.
+#include "../../include/n2p2_b200.h"
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "engine.hpp"
+#include "host_model.hpp"
+
+using namespace n2p2b200;
+
+struct n2p2_mode
+{
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    Model model;
+    DeviceModel dmodel;
+    bool uploaded = false;
+    int precision = PREC_FP64;
+    bool checkExtrapolation = false;
+    bool writeWarnings = false;
+    bool stopOnWarnings = false;
+};
+
+struct n2p2_batch
+{
+    n2p2_mode* mode = nullptr;
+    std::unique_ptr<Batch> batch;
+    int lastFlags = 0;
+    int64_t lastWarnings = 0;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+n2p2_status fail(int code, std::string const& msg)
+{
+    g_error = msg;
+    return code;
+}
+
+template <class F>
+n2p2_status guard(F&& f)
+{
+    try
+    {
+        f();
+        return N2P2_OK;
+    }
+    catch (std::out_of_range const& e)
+    {
+        return fail(N2P2_ERR_OUT_OF_RANGE, e.what());
+    }
+    catch (std::range_error const& e)
+    {
+        return fail(N2P2_ERR_RANGE, e.what());
+    }
+    catch (std::invalid_argument const& e)
+    {
+        return fail(N2P2_ERR_INVALID_ARGUMENT, e.what());
+    }
+    catch (std::runtime_error const& e)
+    {
+        std::string m = e.what();
+        return fail(m.rfind("CUDA error", 0) == 0 ? N2P2_ERR_CUDA : N2P2_ERR_RUNTIME, m);
+    }
+    catch (std::exception const& e)
+    {
+        return fail(N2P2_ERR_RUNTIME, e.what());
+    }
+}
+
+void setDevice(n2p2_mode* m) { cudaCheck(cudaSetDevice(m->device), "cudaSetDevice"); }
+
+void ensureUploaded(n2p2_mode* m)
+{
+    if (!m->uploaded)
+    {
+        setDevice(m);
+        m->dmodel.upload(m->model);
+        m->uploaded = true;
+    }
+}
+
+#define N2P2_REQUIRE(p)                                                      \
+    do                                                                       \
+    {                                                                        \
+        if (!(p)) return fail(N2P2_ERR_NULL, "null handle or pointer: " #p); \
+    } while (0)
+
+void afterEvaluate(n2p2_batch* b)
+{
+    n2p2_mode* m = b->mode;
+    if (!m->checkExtrapolation) return;
+    DevStatus st = b->batch->status();
+    b->lastWarnings = st.extrapolationWarnings;
+    if (st.extrapolationWarnings > 0)
+    {
+        if (m->writeWarnings)
+        {
+            std::vector<int> w(b->batch->numAtoms());
+            b->batch->copyAtomWarnings(w.data());
+            for (size_t a = 0; a < w.size(); ++a)
+                if (w[a] > 0)
+                    std::fprintf(stderr, "### NNP EXTRAPOLATION WARNING ### ATOM: %9zu SYMFUNCS OUT OF RANGE: %d\n", a,
+                                 w[a]);
+        }
+        if (m->stopOnWarnings)
+            throw std::out_of_range("### NNP EXTRAPOLATION WARNING ### ERROR: Symmetry function value out of range.\n");
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+const char* n2p2_last_error(void) { return g_error.c_str(); }
+
+const char* n2p2_version(void) { return "n2p2_b200 0.1 (sm_100a)"; }
+
+n2p2_status n2p2_mode_create(n2p2_mode** mode, int device)
+{
+    N2P2_REQUIRE(mode);
+    return guard([&] {
+        auto m = std::make_unique<n2p2_mode>();
+        m->device = device;
+        cudaCheck(cudaSetDevice(device), "cudaSetDevice");
+        cudaDeviceProp p{};
+        cudaCheck(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
+        m->sms = p.multiProcessorCount;
+        cudaCheck(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        *mode = m.release();
+    });
+}
+
+n2p2_status n2p2_mode_destroy(n2p2_mode* mode)
+{
+    if (!mode) return N2P2_OK;
+    return guard([&] {
+        cudaSetDevice(mode->device);
+        cudaStream_t s = mode->stream;
+        delete mode;
+        if (s) cudaStreamDestroy(s);
+    });
+}
+
+n2p2_status n2p2_mode_initialize(n2p2_mode* mode)
+{
+    N2P2_REQUIRE(mode);
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_mode_load_settings_file(n2p2_mode* mode, const char* fileName)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(fileName);
+    return guard([&] {
+        mode->model.loadSettingsFile(fileName);
+        mode->uploaded = false;
+    });
+}
+
+n2p2_status n2p2_mode_setup_generic(n2p2_mode* mode)
+{
+    N2P2_REQUIRE(mode);
+    return guard([&] {
+        mode->model.setupGeneric();
+        mode->uploaded = false;
+    });
+}
+
+n2p2_status n2p2_mode_setup_symmetry_function_scaling(n2p2_mode* mode, const char* fileName)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(fileName);
+    return guard([&] {
+        mode->model.setupSymmetryFunctionScaling(fileName);
+        mode->uploaded = false;
+    });
+}
+
+n2p2_status n2p2_mode_setup_symmetry_function_scaling_none(n2p2_mode* mode)
+{
+    N2P2_REQUIRE(mode);
+    return guard([&] {
+        mode->model.setupSymmetryFunctionScalingNone();
+        mode->uploaded = false;
+    });
+}
+
+n2p2_status n2p2_mode_setup_neural_network_weights(n2p2_mode* mode, const char* fileNameFormat)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(fileNameFormat);
+    return guard([&] {
+        mode->model.setupNeuralNetworkWeights(fileNameFormat);
+        mode->uploaded = false;
+    });
+}
+
+n2p2_status n2p2_mode_set_connections(n2p2_mode* mode, int element, const double* connections, int64_t count)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(connections);
+    return guard([&] {
+        if (element < 0 || element >= (int)mode->model.numElements())
+            throw std::runtime_error("ERROR: element index out of range.\n");
+        mode->model.setConnections(element, std::vector<double>(connections, connections + count));
+        mode->uploaded = false;
+    });
+}
+
+n2p2_status n2p2_mode_setup_symmetry_function_statistics(n2p2_mode* mode, int collectStatistics,
+                                                         int collectExtrapolationWarnings,
+                                                         int writeExtrapolationWarnings,
+                                                         int stopOnExtrapolationWarnings)
+{
+    N2P2_REQUIRE(mode);
+    mode->checkExtrapolation =
+        collectStatistics || collectExtrapolationWarnings || writeExtrapolationWarnings || stopOnExtrapolationWarnings;
+    mode->writeWarnings = writeExtrapolationWarnings != 0;
+    mode->stopOnWarnings = stopOnExtrapolationWarnings != 0;
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_mode_set_precision(n2p2_mode* mode, int precision)
+{
+    N2P2_REQUIRE(mode);
+    if (precision != N2P2_PRECISION_FP64 && precision != N2P2_PRECISION_MIXED)
+        return fail(N2P2_ERR_INVALID_ARGUMENT, "unknown precision");
+    mode->precision = precision;
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_mode_get_max_cutoff_radius(n2p2_mode* mode, double* radius)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(radius);
+    *radius = mode->model.maxCutoffRadius;
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_mode_get_num_elements(n2p2_mode* mode, int* count)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(count);
+    *count = (int)mode->model.numElements();
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_mode_get_element_symbol(n2p2_mode* mode, int element, char* buffer, int capacity)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(buffer);
+    return guard([&] {
+        std::string const& s = mode->model.elements.at(element).symbol;
+        if ((int)s.size() + 1 > capacity) throw std::runtime_error("buffer too small");
+        std::memcpy(buffer, s.c_str(), s.size() + 1);
+    });
+}
+
+n2p2_status n2p2_mode_get_element_index(n2p2_mode* mode, const char* symbol, int* element)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(symbol);
+    N2P2_REQUIRE(element);
+    return guard([&] { *element = mode->model.elementMap.index(symbol); });
+}
+
+n2p2_status n2p2_mode_get_num_symmetry_functions(n2p2_mode* mode, int element, int* count)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(count);
+    return guard([&] { *count = (int)mode->model.elements.at(element).sf.size(); });
+}
+
+n2p2_status n2p2_mode_get_num_derivative_rows(n2p2_mode* mode, int element, int neighborElement, int* rows)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(rows);
+    return guard([&] { *rows = (int)mode->model.elements.at(element).table.at(neighborElement).size(); });
+}
+
+n2p2_status n2p2_batch_create(n2p2_mode* mode, n2p2_batch** batch)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        ensureUploaded(mode);
+        auto b = std::make_unique<n2p2_batch>();
+        b->mode = mode;
+        b->batch = std::make_unique<Batch>(mode->model, mode->dmodel, mode->stream, mode->sms);
+        *batch = b.release();
+    });
+}
+
+n2p2_status n2p2_batch_destroy(n2p2_batch* batch)
+{
+    if (!batch) return N2P2_OK;
+    return guard([&] {
+        setDevice(batch->mode);
+        delete batch;
+    });
+}
+
+n2p2_status n2p2_batch_set_structures(n2p2_batch* batch, int64_t numStructures, const int64_t* numAtoms,
+                                      const int32_t* elements, const double* boxes, const int32_t* periodic,
+                                      int remap)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(numAtoms);
+    N2P2_REQUIRE(elements);
+    return guard([&] {
+        setDevice(batch->mode);
+        if (!batch->mode->uploaded)
+            throw std::runtime_error("ERROR: model changed after the batch was created; create a new batch.\n");
+        std::vector<StructureInput> s((size_t)numStructures);
+        for (int64_t k = 0; k < numStructures; ++k)
+        {
+            s[k].numAtoms = (int)numAtoms[k];
+            s[k].periodic = periodic ? periodic[k] : (boxes ? 1 : 0);
+            if (s[k].periodic)
+            {
+                if (!boxes) throw std::runtime_error("ERROR: periodic structure without box.\n");
+                std::memcpy(s[k].box, boxes + 9 * k, sizeof(double) * 9);
+            }
+        }
+        batch->batch->setStructures(s, elements, remap);
+    });
+}
+
+n2p2_status n2p2_batch_set_positions(n2p2_batch* batch, const double* positions, int onDevice)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(positions);
+    return guard([&] {
+        setDevice(batch->mode);
+        if (onDevice) batch->batch->setPositionsDevice(positions);
+        else batch->batch->setPositionsHost(positions);
+    });
+}
+
+n2p2_status n2p2_batch_evaluate(n2p2_batch* batch, int flags)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->lastFlags = flags;
+        batch->batch->evaluate(flags, batch->mode->precision, batch->mode->checkExtrapolation ? 1 : 0);
+        afterEvaluate(batch);
+    });
+}
+
+n2p2_status n2p2_batch_synchronize(n2p2_batch* batch)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->status();
+    });
+}
+
+n2p2_status n2p2_batch_get_energies(n2p2_batch* batch, double* energies)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(energies);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->energies(energies);
+    });
+}
+
+n2p2_status n2p2_batch_get_forces(n2p2_batch* batch, double* forces)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(forces);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->forces(forces);
+    });
+}
+
+n2p2_status n2p2_batch_evaluate_host(n2p2_batch* batch, const double* positions, double* energies, double* forces,
+                                     int flags)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(positions);
+    N2P2_REQUIRE(energies);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->lastFlags = flags;
+        batch->batch->setPositionsHost(positions);
+        batch->batch->evaluate(flags, batch->mode->precision, batch->mode->checkExtrapolation ? 1 : 0);
+        afterEvaluate(batch);
+        batch->batch->energies(energies);
+        if (forces && (flags & N2P2_EVAL_FORCES)) batch->batch->forces(forces);
+    });
+}
+
+n2p2_status n2p2_batch_get_num_atoms(n2p2_batch* batch, int64_t* atoms)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(atoms);
+    *atoms = batch->batch->numAtoms();
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_batch_get_num_neighbor_entries(n2p2_batch* batch, int64_t* entries)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(entries);
+    return guard([&] {
+        setDevice(batch->mode);
+        *entries = batch->batch->numNeighborEntries();
+    });
+}
+
+n2p2_status n2p2_batch_get_neighbors(n2p2_batch* batch, int64_t* offsets, int32_t* index, int32_t* image,
+                                     double* d, double* dr)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->synchronize();
+        batch->batch->copyNeighbors(offsets, index, image, d, dr);
+    });
+}
+
+n2p2_status n2p2_batch_get_symmetry_functions(n2p2_batch* batch, double* G)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(G);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->synchronize();
+        batch->batch->copyG(G);
+    });
+}
+
+n2p2_status n2p2_batch_get_dEdG(n2p2_batch* batch, double* dEdG)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(dEdG);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->synchronize();
+        batch->batch->copyDEdG(dEdG);
+    });
+}
+
+n2p2_status n2p2_batch_get_atomic_energies(n2p2_batch* batch, double* energies)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(energies);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->synchronize();
+        batch->batch->copyAtomicEnergies(energies);
+    });
+}
+
+n2p2_status n2p2_batch_get_dGdr(n2p2_batch* batch, double* selfDGdr, double* neighborDGdr)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->synchronize();
+        batch->batch->copyDGdr(selfDGdr, neighborDGdr);
+    });
+}
+
+n2p2_status n2p2_batch_get_internal_positions(n2p2_batch* batch, double* positions)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(positions);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->synchronize();
+        batch->batch->copyPositions(positions);
+    });
+}
+
+n2p2_status n2p2_batch_get_extrapolation_warnings(n2p2_batch* batch, int64_t* total, int32_t* perAtom)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        DevStatus st = batch->batch->status();
+        if (total) *total = st.extrapolationWarnings;
+        if (perAtom) batch->batch->copyAtomWarnings(perAtom);
+    });
+}
+
+n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(launches);
+    *launches = batch->batch->launchesPerEvaluate();
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_host_alloc(void** ptr, size_t bytes)
+{
+    N2P2_REQUIRE(ptr);
+    return guard([&] { cudaCheck(cudaHostAlloc(ptr, bytes, cudaHostAllocDefault), "cudaHostAlloc"); });
+}
+
+n2p2_status n2p2_host_free(void* ptr)
+{
+    if (!ptr) return N2P2_OK;
+    return guard([&] { cudaCheck(cudaFreeHost(ptr), "cudaFreeHost"); });
+}
+
+} // extern "C"

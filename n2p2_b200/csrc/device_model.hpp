@@ -1,0 +1,130 @@
+// Plain-old-data layout of the model and of a batch of structures as the
+// sm_100a kernels see them.  Shared by host (.cpp) and device (.cu) code.
+#pragma once
+
+#include <cstdint>
+
+namespace n2p2b200 {
+
+// Numbering follows the reference enums (CutoffFunction.h:44-72,
+// SymFnc.h:43-65, NeuralNetwork.h:32-56) so stored codes read the same.
+enum CutoffType { CT_HARD = 0, CT_COS, CT_TANHU, CT_TANH, CT_EXP, CT_POLY1, CT_POLY2, CT_POLY3, CT_POLY4 };
+enum ScalingType { ST_NONE = 0, ST_SCALE, ST_CENTER, ST_SCALECENTER, ST_SCALESIGMA };
+enum Activation {
+    AF_UNSET = 0, AF_IDENTITY, AF_TANH, AF_LOGISTIC, AF_SOFTPLUS, AF_RELU,
+    AF_GAUSSIAN, AF_COS, AF_REVLOGISTIC, AF_EXP, AF_HARMONIC
+};
+
+constexpr int kDevMaxElements = 8;
+constexpr int kDevMaxLayers = 6;
+constexpr int kMaxMembers = 32;     // members of one symmetry-function group
+constexpr int kMaxSFPerElement = 256;
+constexpr int kMaxNeurons = 128;    // widest layer of an atomic network
+
+// One member of a symmetry-function group (SymGrpExpRad / SymGrpExpAngn /
+// SymGrpExpAngw member arrays, e.g. SymGrpExpAngn.cpp:108-148).
+struct DevMember
+{
+    double eta, rs, lambda, zeta;
+    double factorNorm;     // angular: 2^(1-zeta)*scalingFactor; radial: scalingFactor
+    double factorDeriv;    // angular: 2*eta/zeta/lambda
+    double zetaLambda;     // zeta*lambda
+    double gNorm;          // angular: factorNorm/scalingFactor (final G prefactor)
+    int    sf;             // index of the symmetry function in its element
+    int    rowE1, rowE2;   // derivative row in the neighbour-element tables of e1 / e2
+    int    zetaInt;
+    int    useIntPow;
+    int    calcExp;        // recompute the Gaussian for this member
+};
+
+struct DevGroup
+{
+    int    type;           // 2, 3, 9
+    int    e1, e2;
+    int    cutoffType;
+    int    cutoffSlot;     // which precomputed f_c/df_c set this group uses
+    int    memberBegin, memberCount;
+    int    pad_;
+    double rc, rc2;
+};
+
+// Cutoff function parameters (CutoffFunction::setCutoffRadius/Parameter,
+// CutoffFunction.cpp:95-112).
+struct DevCutoff
+{
+    int    type;
+    int    pad_;
+    double rc, rcinv, rci, iw, alpha;
+    double tanhPre;        // CutoffFunction::TANH_PRE (CutoffFunction.cpp:28)
+};
+
+// Per symmetry function scaling (SymFnc::scale / unscale, SymFnc.cpp:169-223).
+struct DevScaling
+{
+    int    type;
+    int    pad_;
+    double Smin, Gmin, Gmax, Gmean, scalingFactor;
+};
+
+struct DevElement
+{
+    int numSF;
+    int sfBegin;                      // into the scaling array
+    int groupBegin, groupCount;
+    int rows[kDevMaxElements];        // derivative rows per neighbour element
+    int tableBegin[kDevMaxElements];  // into rowTable: SF index of each row
+    // atomic network
+    int numLayers;
+    int neurons[kDevMaxLayers];
+    int activation[kDevMaxLayers];
+    int wOffset[kDevMaxLayers];       // layer l (1..) weights W[l] (n_l x n_{l-1}) in `weights`
+    int bOffset[kDevMaxLayers];
+};
+
+struct DevModel
+{
+    int numElements;
+    int numCutoffSlots;
+    int maxSF;
+    int maxRows;
+    int normalizeNeurons;
+    int pad_;
+    double maxCutoff, maxCutoff2;
+    DevElement el[kDevMaxElements];
+    DevCutoff cutoff[4];
+    const DevGroup*   groups;
+    const DevMember*  members;
+    const DevScaling* scaling;
+    const int*        rowTable;
+    const double*     weights;
+    const float*      weightsF;       // FP32 copy for the mixed path
+};
+
+// Per structure geometry for the neighbour build.
+struct DevStructInfo
+{
+    double box[9];        // normalised units, row k = box vector k
+    double invbox[9];
+    double boxPhys[9];    // physical units (for the optional remap)
+    double invboxPhys[9];
+    int    pbc[3];        // Structure::calculatePbcCopies (Structure.cpp:485-516)
+    int    periodic;
+    int    nc[3];         // cell grid
+    int    stencil[3];    // cells searched on each side
+    int    atomBegin, numAtoms;
+    int    cellBegin;
+    int    pad_;
+};
+
+// Status words written by kernels and read by the host after a launch.
+struct DevStatus
+{
+    int overflowNeighbors;   // neighbour capacity exceeded
+    int maxNeighbors;
+    int64_t totalNeighbors;
+    int extrapolationWarnings;
+    int badInput;
+    int pad_[2];
+};
+
+} // namespace n2p2b200

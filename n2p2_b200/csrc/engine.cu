@@ -1,0 +1,785 @@
+// Device-side engine; see engine.hpp.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <set>
+#include <stdexcept>
+#include <string>
+
+namespace n2p2b200 {
+
+void cudaCheck(cudaError_t e, char const* what)
+{
+    if (e != cudaSuccess)
+        throw std::runtime_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+void setDynamicSmemOnce(const void* kernel, size_t bytes)
+{
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(kernel, dev);
+    if (done.count(key)) return;
+    cudaCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+              "cudaFuncSetAttribute");
+    done.insert(key);
+}
+
+namespace {
+
+template <typename T>
+T* devAlloc(size_t count, std::vector<void*>& owned)
+{
+    void* p = nullptr;
+    if (count == 0) count = 1;
+    cudaCheck(cudaMalloc(&p, sizeof(T) * count), "cudaMalloc");
+    owned.push_back(p);
+    return static_cast<T*>(p);
+}
+
+void freeAll(std::vector<void*>& owned)
+{
+    for (void* p : owned) cudaFree(p);
+    owned.clear();
+}
+
+// Structure::calculateInverseBox (Structure.cpp:518-544), same operation order.
+void inverseBox(double const* b, double* ib)
+{
+    auto B = [&](int k, int c) { return b[k * 3 + c]; };
+    double invdet = B(0, 0) * B(1, 1) * B(2, 2) + B(1, 0) * B(2, 1) * B(0, 2) + B(2, 0) * B(0, 1) * B(1, 2) -
+                    B(2, 0) * B(1, 1) * B(0, 2) - B(0, 0) * B(2, 1) * B(1, 2) - B(1, 0) * B(0, 1) * B(2, 2);
+    invdet = 1.0 / invdet;
+    ib[0] = B(1, 1) * B(2, 2) - B(2, 1) * B(1, 2);
+    ib[1] = B(2, 1) * B(0, 2) - B(0, 1) * B(2, 2);
+    ib[2] = B(0, 1) * B(1, 2) - B(1, 1) * B(0, 2);
+    ib[3] = B(2, 0) * B(1, 2) - B(1, 0) * B(2, 2);
+    ib[4] = B(0, 0) * B(2, 2) - B(2, 0) * B(0, 2);
+    ib[5] = B(1, 0) * B(0, 2) - B(0, 0) * B(1, 2);
+    ib[6] = B(1, 0) * B(2, 1) - B(2, 0) * B(1, 1);
+    ib[7] = B(2, 0) * B(0, 1) - B(0, 0) * B(2, 1);
+    ib[8] = B(0, 0) * B(1, 1) - B(1, 0) * B(0, 1);
+    for (int k = 0; k < 9; ++k) ib[k] *= invdet;
+}
+
+void cross(double const* a, double const* v, double* w)
+{
+    w[0] = a[1] * v[2] - a[2] * v[1];
+    w[1] = a[2] * v[0] - a[0] * v[2];
+    w[2] = a[0] * v[1] - a[1] * v[0];
+}
+
+void normalize3(double* v)
+{
+    double n = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    v[0] /= n;
+    v[1] /= n;
+    v[2] /= n;
+}
+
+double dot3(double const* a, double const* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+// Structure::calculatePbcCopies (Structure.cpp:485-516) plus the plane
+// spacings used for the cell grid.
+void pbcCopies(double const* box, double rc, int* pbc, double* proj)
+{
+    double axb[3], axc[3], bxc[3];
+    cross(box + 0, box + 3, axb);
+    normalize3(axb);
+    cross(box + 0, box + 6, axc);
+    normalize3(axc);
+    cross(box + 3, box + 6, bxc);
+    normalize3(bxc);
+    proj[0] = std::fabs(dot3(box + 0, bxc));
+    proj[1] = std::fabs(dot3(box + 3, axc));
+    proj[2] = std::fabs(dot3(box + 6, axb));
+    for (int a = 0; a < 3; ++a)
+    {
+        pbc[a] = 0;
+        while (pbc[a] * proj[a] <= rc) pbc[a]++;
+    }
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// DeviceModel
+// ---------------------------------------------------------------------------
+
+DeviceModel::~DeviceModel() { release(); }
+
+void DeviceModel::release()
+{
+    cudaFree(groups_);
+    cudaFree(members_);
+    cudaFree(scaling_);
+    cudaFree(rowTable_);
+    cudaFree(weights_);
+    cudaFree(weightsF_);
+    groups_ = nullptr;
+    members_ = nullptr;
+    scaling_ = nullptr;
+    rowTable_ = nullptr;
+    weights_ = nullptr;
+    weightsF_ = nullptr;
+}
+
+void DeviceModel::upload(Model const& m)
+{
+    if (!m.setupDone) throw std::runtime_error("ERROR: setupGeneric() has not been called.\n");
+    if (!m.scalingDone) throw std::runtime_error("ERROR: symmetry function scaling has not been set up.\n");
+    release();
+    DevModel v{};
+    v.numElements = (int)m.elements.size();
+    v.normalizeNeurons = m.normalizeNeurons ? 1 : 0;
+    v.maxCutoff = m.maxCutoffRadius;
+    v.maxCutoff2 = m.maxCutoffRadius * m.maxCutoffRadius;
+
+    std::vector<double> slotRc;
+    std::vector<DevGroup> groups;
+    std::vector<DevMember> members;
+    std::vector<DevScaling> scaling;
+    std::vector<int> rowTable;
+    std::vector<double> weights;
+    int maxSF = 0, maxRows = 0;
+    for (std::size_t e = 0; e < m.elements.size(); ++e)
+    {
+        ElementSetup const& el = m.elements[e];
+        DevElement& de = v.el[e];
+        de.numSF = (int)el.sf.size();
+        if (de.numSF > kMaxSFPerElement) throw std::runtime_error("ERROR: too many symmetry functions per element.\n");
+        maxSF = std::max(maxSF, de.numSF);
+        de.sfBegin = (int)scaling.size();
+        for (auto const& s : el.sf)
+        {
+            DevScaling sc{};
+            sc.type = s.scalingType;
+            sc.Smin = s.Smin;
+            sc.Gmin = s.Gmin;
+            sc.Gmax = s.Gmax;
+            sc.Gmean = s.Gmean;
+            sc.scalingFactor = s.scalingFactor;
+            scaling.push_back(sc);
+        }
+        for (std::size_t en = 0; en < m.elements.size(); ++en)
+        {
+            de.rows[en] = (int)el.table[en].size();
+            de.tableBegin[en] = (int)rowTable.size();
+            for (int idx : el.table[en]) rowTable.push_back(idx);
+            maxRows = std::max(maxRows, de.rows[en]);
+        }
+        de.groupBegin = (int)groups.size();
+        de.groupCount = (int)el.groups.size();
+        for (auto const& g : el.groups)
+        {
+            if ((int)g.members.size() > kMaxMembers) throw std::runtime_error("ERROR: symmetry function group too large.\n");
+            DevGroup dg{};
+            dg.type = g.type;
+            dg.e1 = g.e1;
+            dg.e2 = g.e2;
+            dg.cutoffType = g.cutoffType;
+            dg.rc = g.rc;
+            dg.rc2 = g.rc * g.rc;
+            auto it = std::find(slotRc.begin(), slotRc.end(), g.rc);
+            if (it == slotRc.end())
+            {
+                if (slotRc.size() >= 4) throw std::runtime_error("ERROR: more than 4 distinct cutoff radii.\n");
+                slotRc.push_back(g.rc);
+                it = slotRc.end() - 1;
+            }
+            dg.cutoffSlot = (int)(it - slotRc.begin());
+            dg.memberBegin = (int)members.size();
+            dg.memberCount = (int)g.members.size();
+            for (std::size_t q = 0; q < g.members.size(); ++q)
+            {
+                SymFunc const& s = el.sf[g.members[q]];
+                DevMember dm{};
+                dm.eta = s.eta;
+                dm.rs = s.rs;
+                dm.lambda = s.lambda;
+                dm.zeta = s.zeta;
+                dm.sf = s.index;
+                dm.zetaInt = s.zetaInt;
+                dm.useIntPow = s.useIntegerPow ? 1 : 0;
+                dm.calcExp = g.calculateExp[q] ? 1 : 0;
+                dm.rowE1 = s.indexPerElement[s.e1];
+                dm.rowE2 = (s.type == 2) ? dm.rowE1 : s.indexPerElement[s.e2];
+                if (s.type == 2)
+                {
+                    dm.factorNorm = s.scalingFactor;
+                    dm.gNorm = 1.0;
+                }
+                else
+                {
+                    dm.factorNorm = g.factorNorm[q];
+                    dm.factorDeriv = g.factorDeriv[q];
+                    dm.zetaLambda = s.zeta * s.lambda;
+                    dm.gNorm = g.factorNorm[q] / s.scalingFactor;
+                }
+                members.push_back(dm);
+            }
+            groups.push_back(dg);
+        }
+        // network
+        NetworkTopology const& t = el.topology;
+        if (!el.hasWeights) throw std::runtime_error("ERROR: weights of element " + el.symbol + " not set.\n");
+        if (t.numLayers > kDevMaxLayers) throw std::runtime_error("ERROR: too many network layers.\n");
+        de.numLayers = t.numLayers;
+        for (int l = 0; l < t.numLayers; ++l)
+        {
+            de.neurons[l] = t.neurons[l];
+            de.activation[l] = t.activations[l];
+            if (t.neurons[l] > kMaxNeurons && l > 0) throw std::runtime_error("ERROR: network layer too wide.\n");
+        }
+        for (int l = 1; l < t.numLayers; ++l)
+        {
+            de.wOffset[l] = (int)weights.size();
+            weights.insert(weights.end(), el.W[l - 1].begin(), el.W[l - 1].end());
+            de.bOffset[l] = (int)weights.size();
+            weights.insert(weights.end(), el.b[l - 1].begin(), el.b[l - 1].end());
+        }
+    }
+    v.maxSF = maxSF;
+    v.maxRows = maxRows;
+    v.numCutoffSlots = (int)slotRc.size();
+    const double E = std::exp(1.0);
+    for (std::size_t s = 0; s < slotRc.size(); ++s)
+    {
+        DevCutoff& c = v.cutoff[s];
+        c.type = m.cutoffType;
+        c.rc = slotRc[s];
+        c.rcinv = 1.0 / slotRc[s];
+        c.alpha = m.cutoffAlpha;
+        c.rci = c.rc * c.alpha;
+        c.iw = 1.0 / (c.rc - c.rci);
+        c.tanhPre = std::pow((E + 1 / E) / (E - 1 / E), 3);
+    }
+    std::vector<float> weightsF(weights.begin(), weights.end());
+    auto up = [](void** dst, void const* src, size_t bytes) {
+        cudaCheck(cudaMalloc(dst, bytes ? bytes : 16), "cudaMalloc(model)");
+        if (bytes) cudaCheck(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(model)");
+    };
+    up((void**)&groups_, groups.data(), groups.size() * sizeof(DevGroup));
+    up((void**)&members_, members.data(), members.size() * sizeof(DevMember));
+    up((void**)&scaling_, scaling.data(), scaling.size() * sizeof(DevScaling));
+    up((void**)&rowTable_, rowTable.data(), rowTable.size() * sizeof(int));
+    up((void**)&weights_, weights.data(), weights.size() * sizeof(double));
+    up((void**)&weightsF_, weightsF.data(), weightsF.size() * sizeof(float));
+    v.groups = groups_;
+    v.members = members_;
+    v.scaling = scaling_;
+    v.rowTable = rowTable_;
+    v.weights = weights_;
+    v.weightsF = weightsF_;
+    view = v;
+    this->maxSF = maxSF;
+}
+
+// ---------------------------------------------------------------------------
+// Batch
+// ---------------------------------------------------------------------------
+
+Batch::Batch(Model const& model, DeviceModel const& dmodel, cudaStream_t stream, int sms)
+    : model_(model), dmodel_(dmodel), stream_(stream), sms_(sms)
+{
+}
+
+Batch::~Batch() { releaseAll(); }
+
+void Batch::releaseGraph()
+{
+    if (graphExec_) cudaGraphExecDestroy(graphExec_);
+    graphExec_ = nullptr;
+    graphKey_ = -1;
+}
+
+void Batch::releaseAll()
+{
+    releaseGraph();
+    freeAll(ownedDGdr_);
+    freeAll(ownedNbr_);
+    freeAll(owned_);
+    dgdrAllocated_ = false;
+}
+
+void Batch::setStructures(std::vector<StructureInput> const& s, const int* elements, int remap)
+{
+    releaseAll();
+    structs_ = s;
+    S_ = (int)s.size();
+    N_ = 0;
+    structBegin_.assign(S_ + 1, 0);
+    for (int k = 0; k < S_; ++k)
+    {
+        if (s[k].numAtoms <= 0) throw std::runtime_error("ERROR: structure without atoms.\n");
+        structBegin_[k + 1] = structBegin_[k] + s[k].numAtoms;
+    }
+    N_ = structBegin_[S_];
+    int ne = (int)model_.numElements();
+    elemHost_.assign(elements, elements + N_);
+    numAtomsPerElement_.assign((size_t)S_ * ne, 0);
+    for (int k = 0; k < S_; ++k)
+        for (int a = structBegin_[k]; a < structBegin_[k + 1]; ++a)
+        {
+            if (elemHost_[a] < 0 || elemHost_[a] >= ne) throw std::runtime_error("ERROR: element index out of range.\n");
+            numAtomsPerElement_[(size_t)k * ne + elemHost_[a]]++;
+        }
+    remap_ = remap;
+
+    // geometry per structure
+    const double rc = model_.maxCutoffRadius;
+    const double conv = model_.normalize ? model_.convLength : 1.0;
+    std::vector<DevStructInfo> info(S_);
+    int cellTotal = 0;
+    int64_t capacity = 0;
+    for (int k = 0; k < S_; ++k)
+    {
+        DevStructInfo& d = info[k];
+        std::memset(&d, 0, sizeof(d));
+        d.atomBegin = structBegin_[k];
+        d.numAtoms = s[k].numAtoms;
+        d.periodic = s[k].periodic;
+        const int n = s[k].numAtoms;
+        if (s[k].periodic)
+        {
+            std::memcpy(d.boxPhys, s[k].box, sizeof(d.boxPhys));
+            inverseBox(d.boxPhys, d.invboxPhys);
+            for (int q = 0; q < 9; ++q)
+            {
+                d.box[q] = model_.normalize ? d.boxPhys[q] * conv : d.boxPhys[q];
+                d.invbox[q] = model_.normalize ? d.invboxPhys[q] / conv : d.invboxPhys[q];
+            }
+            double proj[3];
+            pbcCopies(d.box, rc, d.pbc, proj);
+            int64_t cells = 1;
+            for (int a = 0; a < 3; ++a)
+            {
+                double want = rc * 0.5 * (1.0 + 1e-6);
+                int nc = (int)std::floor(proj[a] / want);
+                nc = std::max(1, std::min(nc, 256));
+                double w = proj[a] / nc;
+                d.nc[a] = nc;
+                d.stencil[a] = (int)std::ceil(rc / w + 1e-9);
+                cells *= nc;
+            }
+            if (cells > 64 * (int64_t)n + 64)
+            {
+                // very sparse structure: coarser grid (search cost bounded by the atom count)
+                for (int a = 0; a < 3; ++a)
+                {
+                    int nc = std::max(1, (int)std::floor(proj[a] / (rc * (1.0 + 1e-6))));
+                    nc = std::min(nc, 64);
+                    d.nc[a] = nc;
+                    d.stencil[a] = (int)std::ceil(rc / (proj[a] / nc) + 1e-9);
+                }
+                cells = (int64_t)d.nc[0] * d.nc[1] * d.nc[2];
+            }
+            d.cellBegin = cellTotal;
+            cellTotal += (int)cells;
+            double vol = std::fabs(d.box[0] * (d.box[4] * d.box[8] - d.box[5] * d.box[7]) -
+                                   d.box[1] * (d.box[3] * d.box[8] - d.box[5] * d.box[6]) +
+                                   d.box[2] * (d.box[3] * d.box[7] - d.box[4] * d.box[6]));
+            double expected = n / vol * 4.18879020478639 * rc * rc * rc;
+            int64_t images = (int64_t)(2 * d.pbc[0] + 1) * (2 * d.pbc[1] + 1) * (2 * d.pbc[2] + 1);
+            int64_t perAtom = std::min<int64_t>(images * n, (int64_t)std::ceil(expected * 1.4 + 32));
+            capacity += perAtom * n;
+        }
+        else
+        {
+            d.nc[0] = d.nc[1] = d.nc[2] = 1;
+            d.cellBegin = cellTotal;
+            cellTotal += 1;
+            capacity += (int64_t)n * (n - 1);
+        }
+    }
+
+    allocateAtoms();
+    v_.numCells = cellTotal;
+    v_.cellCount = devAlloc<int>(cellTotal, owned_);
+    v_.cellStart = devAlloc<int>(cellTotal, owned_);
+    v_.cellStart64 = devAlloc<int64_t>(cellTotal + 1, owned_);
+    v_.scanTmp = devAlloc<int64_t>(std::max(scanTileCount(cellTotal), scanTileCount(N_)) + 8, owned_);
+    cudaCheck(cudaMemcpyAsync(infoDev_, info.data(), sizeof(DevStructInfo) * S_, cudaMemcpyHostToDevice, stream_),
+              "upload structure info");
+    std::vector<int> atomStruct(N_);
+    for (int k = 0; k < S_; ++k)
+        for (int a = structBegin_[k]; a < structBegin_[k + 1]; ++a) atomStruct[a] = k;
+    cudaCheck(cudaMemcpyAsync(atomStructDev_, atomStruct.data(), sizeof(int) * N_, cudaMemcpyHostToDevice, stream_),
+              "upload atom map");
+    cudaCheck(cudaMemcpyAsync(elemDev_, elemHost_.data(), sizeof(int) * N_, cudaMemcpyHostToDevice, stream_),
+              "upload elements");
+    cudaCheck(cudaMemcpyAsync(structBeginDev_, structBegin_.data(), sizeof(int) * (S_ + 1), cudaMemcpyHostToDevice,
+                              stream_),
+              "upload offsets");
+    cudaCheck(cudaStreamSynchronize(stream_), "setStructures");
+    allocateNeighbors(std::max<int64_t>(capacity, 1));
+    capacityVerified_ = false;
+}
+
+void Batch::allocateAtoms()
+{
+    const int N = N_;
+    const int stride = dmodel_.maxSF;
+    v_ = BatchView{};
+    v_.N = N;
+    v_.S = S_;
+    v_.gStride = stride;
+    infoDev_ = devAlloc<DevStructInfo>(S_, owned_);
+    atomStructDev_ = devAlloc<int>(N, owned_);
+    elemDev_ = devAlloc<int>(N, owned_);
+    structBeginDev_ = devAlloc<int>(S_ + 1, owned_);
+    rin_ = devAlloc<double>(3 * (size_t)N, owned_);
+    v_.info = infoDev_;
+    v_.atomStruct = atomStructDev_;
+    v_.elem = elemDev_;
+    v_.structAtomBegin = structBeginDev_;
+    v_.px = devAlloc<double>(N, owned_);
+    v_.py = devAlloc<double>(N, owned_);
+    v_.pz = devAlloc<double>(N, owned_);
+    v_.atomCell = devAlloc<int>(N, owned_);
+    v_.atomSlot = devAlloc<int>(N, owned_);
+    v_.cellAtoms = devAlloc<int>(N, owned_);
+    v_.nbrCount = devAlloc<int>(N, owned_);
+    v_.nbrOffset = devAlloc<int64_t>((size_t)N + 1, owned_);
+    v_.G = devAlloc<double>((size_t)N * stride, owned_);
+    v_.dEdG = devAlloc<double>((size_t)N * stride, owned_);
+    v_.Eatom = devAlloc<double>(N, owned_);
+    v_.Estruct = devAlloc<double>(S_, owned_);
+    v_.fSelf = devAlloc<double>(3 * (size_t)N, owned_);
+    v_.F = devAlloc<double>(3 * (size_t)N, owned_);
+    v_.atomWarnings = devAlloc<int>(N, owned_);
+    v_.status = devAlloc<DevStatus>(1, owned_);
+    cudaCheck(cudaMemsetAsync(v_.G, 0, sizeof(double) * (size_t)N * stride, stream_), "memset");
+    cudaCheck(cudaMemsetAsync(v_.dEdG, 0, sizeof(double) * (size_t)N * stride, stream_), "memset");
+}
+
+void Batch::allocateNeighbors(int64_t capacity)
+{
+    releaseGraph();
+    freeAll(ownedDGdr_);
+    dgdrAllocated_ = false;
+    freeAll(ownedNbr_);
+    const int slots = std::max(1, dmodel_.view.numCutoffSlots);
+    capacity_ = capacity;
+    v_.nbrCapacity = capacity;
+    v_.scrKey = devAlloc<int64_t>(capacity, ownedNbr_);
+    v_.scrD = devAlloc<double>(capacity, ownedNbr_);
+    v_.scrDx = devAlloc<double>(capacity, ownedNbr_);
+    v_.scrDy = devAlloc<double>(capacity, ownedNbr_);
+    v_.scrDz = devAlloc<double>(capacity, ownedNbr_);
+    v_.nbrJ = devAlloc<int>(capacity, ownedNbr_);
+    v_.nbrCode = devAlloc<int>(capacity, ownedNbr_);
+    v_.nbrD = devAlloc<double>(capacity, ownedNbr_);
+    v_.nbrDx = devAlloc<double>(capacity, ownedNbr_);
+    v_.nbrDy = devAlloc<double>(capacity, ownedNbr_);
+    v_.nbrDz = devAlloc<double>(capacity, ownedNbr_);
+    v_.rev = devAlloc<int64_t>(capacity, ownedNbr_);
+    v_.nbrFc = devAlloc<double>((size_t)slots * capacity, ownedNbr_);
+    v_.nbrDfc = devAlloc<double>((size_t)slots * capacity, ownedNbr_);
+    v_.hx = devAlloc<double>(capacity, ownedNbr_);
+    v_.hy = devAlloc<double>(capacity, ownedNbr_);
+    v_.hz = devAlloc<double>(capacity, ownedNbr_);
+    v_.dGdr = nullptr;
+    v_.dGdrSelf = nullptr;
+}
+
+void Batch::allocateDGdr()
+{
+    if (dgdrAllocated_) return;
+    releaseGraph();
+    const int rows = std::max(1, dmodel_.view.maxRows);
+    v_.dGdr = devAlloc<double>((size_t)rows * capacity_ * 3, ownedDGdr_);
+    v_.dGdrSelf = devAlloc<double>((size_t)N_ * v_.gStride * 3, ownedDGdr_);
+    cudaCheck(cudaMemsetAsync(v_.dGdrSelf, 0, sizeof(double) * (size_t)N_ * v_.gStride * 3, stream_), "memset");
+    dgdrAllocated_ = true;
+}
+
+void Batch::setPositionsHost(const double* r)
+{
+    cudaCheck(cudaMemcpyAsync(rin_, r, sizeof(double) * 3 * (size_t)N_, cudaMemcpyHostToDevice, stream_),
+              "positions H2D");
+}
+
+void Batch::setPositionsDevice(const double* r)
+{
+    cudaCheck(cudaMemcpyAsync(rin_, r, sizeof(double) * 3 * (size_t)N_, cudaMemcpyDeviceToDevice, stream_),
+              "positions D2D");
+}
+
+// The kernel sequence of one evaluation (Mode::evaluateNNP, Mode.cpp:2029-2077).
+void Batch::record(int flags, int precision, int checkExtrapolation)
+{
+    DevModel const& m = dmodel_.view;
+    const bool forces = (flags & EVAL_FORCES) != 0;
+    const bool stored = (flags & EVAL_STORE_DGDR) != 0;
+    int launches = 0;
+    cudaCheck(cudaMemsetAsync(v_.status, 0, sizeof(DevStatus), stream_), "status reset");
+    launchPreparePositions(v_, rin_, remap_, model_.normalize ? 1 : 0, model_.convLength, stream_);
+    launches += 1;
+    launchNeighborBuild(v_, model_.maxCutoffRadius * model_.maxCutoffRadius, stream_);
+    launches += 3 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1;
+    launchCutoffValues(m, v_, sms_, stream_);
+    launches += 1;
+    if (stored)
+    {
+        launchSFDerivatives(m, v_, sms_, stream_);
+        launches += 2;
+    }
+    else
+    {
+        launchSFValues(m, v_, precision, sms_, stream_);
+        launches += 2;
+    }
+    if (checkExtrapolation)
+    {
+        launchExtrapolationCheck(m, v_, sms_, stream_);
+        launches += 1;
+    }
+    launchNetworkFP64(m, v_, forces ? 1 : 0, sms_, stream_);
+    launches += 1;
+    launchEnergySum(v_, stream_);
+    launches += 1;
+    if (forces)
+    {
+        if (stored)
+        {
+            launchContractStored(m, v_, sms_, stream_);
+            launches += 1;
+        }
+        else
+        {
+            launchSFForces(m, v_, precision, sms_, stream_);
+            launches += 2;
+        }
+        launchGatherForces(v_, sms_, stream_);
+        launches += 1;
+    }
+    cudaCheck(cudaGetLastError(), "kernel launch");
+    launches_ = launches;
+}
+
+void Batch::evaluate(int flags, int precision, int checkExtrapolation)
+{
+    if (N_ == 0) throw std::runtime_error("ERROR: no structures set.\n");
+    if (flags & EVAL_STORE_DGDR)
+    {
+        if (precision != PREC_FP64) throw std::runtime_error("ERROR: stored dG/dr is FP64 only.\n");
+        allocateDGdr();
+    }
+    if (!capacityVerified_)
+    {
+        for (int attempt = 0; attempt < 3; ++attempt)
+        {
+            record(flags, precision, checkExtrapolation);
+            DevStatus st = status();
+            if (st.totalNeighbors <= capacity_) break;
+            allocateNeighbors((int64_t)(st.totalNeighbors * 1.05) + 1024);
+            if (flags & EVAL_STORE_DGDR) allocateDGdr();
+        }
+        DevStatus st = status();
+        if (st.totalNeighbors > capacity_) throw std::runtime_error("ERROR: neighbour capacity could not be established.\n");
+        capacityVerified_ = true;
+        return;
+    }
+    if (flags & EVAL_NO_GRAPH)
+    {
+        record(flags, precision, checkExtrapolation);
+        return;
+    }
+    const int key = (flags & (EVAL_FORCES | EVAL_STORE_DGDR)) | (precision << 4) | ((checkExtrapolation ? 1 : 0) << 5);
+    if (graphExec_ == nullptr || graphKey_ != key)
+    {
+        releaseGraph();
+        cudaGraph_t graph;
+        cudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed), "begin capture");
+        try
+        {
+            record(flags, precision, checkExtrapolation);
+        }
+        catch (...)
+        {
+            cudaStreamEndCapture(stream_, &graph);
+            throw;
+        }
+        cudaCheck(cudaStreamEndCapture(stream_, &graph), "end capture");
+        cudaCheck(cudaGraphInstantiate(&graphExec_, graph, 0), "graph instantiate");
+        cudaGraphDestroy(graph);
+        graphKey_ = key;
+    }
+    cudaCheck(cudaGraphLaunch(graphExec_, stream_), "graph launch");
+}
+
+void Batch::synchronize() { cudaCheck(cudaStreamSynchronize(stream_), "synchronize"); }
+
+DevStatus Batch::status()
+{
+    DevStatus st{};
+    cudaCheck(cudaMemcpyAsync(&st, v_.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream_), "status D2H");
+    synchronize();
+    if (st.badInput) throw std::runtime_error("ERROR: invalid input detected on the device (atoms outside the cell, "
+                                              "asymmetric neighbour pairs or more than 2048 neighbours).\n");
+    return st;
+}
+
+int64_t Batch::numNeighborEntries()
+{
+    int64_t total = 0;
+    cudaCheck(cudaMemcpyAsync(&total, v_.nbrOffset + N_, sizeof(int64_t), cudaMemcpyDeviceToHost, stream_), "D2H");
+    synchronize();
+    return total;
+}
+
+void Batch::energies(double* out)
+{
+    std::vector<double> e(S_);
+    cudaCheck(cudaMemcpyAsync(e.data(), v_.Estruct, sizeof(double) * S_, cudaMemcpyDeviceToHost, stream_), "E D2H");
+    synchronize();
+    const int ne = (int)model_.numElements();
+    for (int k = 0; k < S_; ++k)
+    {
+        double E = e[k];
+        // Structure::toPhysicalUnits (Structure.cpp:1279-1306) and
+        // Mode::addEnergyOffset (Mode.cpp:2079-2097)
+        if (model_.normalize) E = E / model_.convEnergy + structs_[k].numAtoms * model_.meanEnergy;
+        for (int q = 0; q < ne; ++q)
+            E += numAtomsPerElement_[(size_t)k * ne + q] * model_.elements[q].atomicEnergyOffset;
+        out[k] = E;
+    }
+}
+
+void Batch::forces(double* out)
+{
+    cudaCheck(cudaMemcpyAsync(out, v_.F, sizeof(double) * 3 * (size_t)N_, cudaMemcpyDeviceToHost, stream_), "F D2H");
+    synchronize();
+    if (model_.normalize)
+    {
+        // Atom::toPhysicalUnits: f /= convEnergy / convLength (Atom.cpp:123-130)
+        const double c = model_.convEnergy / model_.convLength;
+        for (size_t q = 0; q < 3 * (size_t)N_; ++q) out[q] /= c;
+    }
+}
+
+void Batch::copyNeighbors(int64_t* offsets, int* index, int* image, double* d, double* dr)
+{
+    std::vector<int64_t> off(N_ + 1);
+    cudaCheck(cudaMemcpy(off.data(), v_.nbrOffset, sizeof(int64_t) * (N_ + 1), cudaMemcpyDeviceToHost), "D2H");
+    const int64_t M = off[N_];
+    if (offsets) std::memcpy(offsets, off.data(), sizeof(int64_t) * (N_ + 1));
+    if (index) cudaCheck(cudaMemcpy(index, v_.nbrJ, sizeof(int) * M, cudaMemcpyDeviceToHost), "D2H");
+    if (image) cudaCheck(cudaMemcpy(image, v_.nbrCode, sizeof(int) * M, cudaMemcpyDeviceToHost), "D2H");
+    if (d) cudaCheck(cudaMemcpy(d, v_.nbrD, sizeof(double) * M, cudaMemcpyDeviceToHost), "D2H");
+    if (dr)
+    {
+        std::vector<double> x(M), y(M), z(M);
+        cudaCheck(cudaMemcpy(x.data(), v_.nbrDx, sizeof(double) * M, cudaMemcpyDeviceToHost), "D2H");
+        cudaCheck(cudaMemcpy(y.data(), v_.nbrDy, sizeof(double) * M, cudaMemcpyDeviceToHost), "D2H");
+        cudaCheck(cudaMemcpy(z.data(), v_.nbrDz, sizeof(double) * M, cudaMemcpyDeviceToHost), "D2H");
+        for (int64_t e = 0; e < M; ++e)
+        {
+            dr[3 * e + 0] = x[e];
+            dr[3 * e + 1] = y[e];
+            dr[3 * e + 2] = z[e];
+        }
+    }
+}
+
+namespace {
+void packPerAtom(std::vector<double> const& src, int stride, std::vector<int> const& elem, Model const& m, double* out)
+{
+    size_t k = 0;
+    for (size_t a = 0; a < elem.size(); ++a)
+    {
+        int ns = (int)m.elements[elem[a]].sf.size();
+        for (int s = 0; s < ns; ++s) out[k++] = src[a * stride + s];
+    }
+}
+} // namespace
+
+void Batch::copyG(double* out)
+{
+    std::vector<double> g((size_t)N_ * v_.gStride);
+    cudaCheck(cudaMemcpy(g.data(), v_.G, sizeof(double) * g.size(), cudaMemcpyDeviceToHost), "D2H");
+    packPerAtom(g, v_.gStride, elemHost_, model_, out);
+}
+
+void Batch::copyDEdG(double* out)
+{
+    std::vector<double> g((size_t)N_ * v_.gStride);
+    cudaCheck(cudaMemcpy(g.data(), v_.dEdG, sizeof(double) * g.size(), cudaMemcpyDeviceToHost), "D2H");
+    packPerAtom(g, v_.gStride, elemHost_, model_, out);
+}
+
+void Batch::copyAtomicEnergies(double* out)
+{
+    cudaCheck(cudaMemcpy(out, v_.Eatom, sizeof(double) * N_, cudaMemcpyDeviceToHost), "D2H");
+}
+
+void Batch::copyAtomWarnings(int* out)
+{
+    cudaCheck(cudaMemcpy(out, v_.atomWarnings, sizeof(int) * N_, cudaMemcpyDeviceToHost), "D2H");
+}
+
+void Batch::copyPositions(double* out)
+{
+    std::vector<double> x(N_), y(N_), z(N_);
+    cudaCheck(cudaMemcpy(x.data(), v_.px, sizeof(double) * N_, cudaMemcpyDeviceToHost), "D2H");
+    cudaCheck(cudaMemcpy(y.data(), v_.py, sizeof(double) * N_, cudaMemcpyDeviceToHost), "D2H");
+    cudaCheck(cudaMemcpy(z.data(), v_.pz, sizeof(double) * N_, cudaMemcpyDeviceToHost), "D2H");
+    for (int a = 0; a < N_; ++a)
+    {
+        out[3 * a + 0] = x[a];
+        out[3 * a + 1] = y[a];
+        out[3 * a + 2] = z[a];
+    }
+}
+
+void Batch::copyDGdr(double* self, double* nbr)
+{
+    if (!dgdrAllocated_) throw std::runtime_error("ERROR: dG/dr was not stored (evaluate with the store flag).\n");
+    std::vector<int64_t> off(N_ + 1);
+    cudaCheck(cudaMemcpy(off.data(), v_.nbrOffset, sizeof(int64_t) * (N_ + 1), cudaMemcpyDeviceToHost), "D2H");
+    const int64_t M = off[N_];
+    std::vector<int> J(M);
+    cudaCheck(cudaMemcpy(J.data(), v_.nbrJ, sizeof(int) * M, cudaMemcpyDeviceToHost), "D2H");
+    if (self)
+    {
+        std::vector<double> s((size_t)N_ * v_.gStride * 3);
+        cudaCheck(cudaMemcpy(s.data(), v_.dGdrSelf, sizeof(double) * s.size(), cudaMemcpyDeviceToHost), "D2H");
+        size_t k = 0;
+        for (int a = 0; a < N_; ++a)
+        {
+            int ns = (int)model_.elements[elemHost_[a]].sf.size();
+            for (int q = 0; q < ns * 3; ++q) self[k++] = s[(size_t)a * v_.gStride * 3 + q];
+        }
+    }
+    if (nbr)
+    {
+        const int rowsMax = std::max(1, dmodel_.view.maxRows);
+        std::vector<double> rowbuf((size_t)M * 3);
+        size_t k = 0;
+        // rows of entry e follow the centre element's table for the neighbour element
+        std::vector<int> rowsOf(M);
+        for (int a = 0; a < N_; ++a)
+            for (int64_t e = off[a]; e < off[a + 1]; ++e)
+                rowsOf[e] = (int)model_.elements[elemHost_[a]].table[elemHost_[J[e]]].size();
+        std::vector<std::vector<double>> rows(rowsMax);
+        for (int r = 0; r < rowsMax; ++r)
+        {
+            rows[r].resize((size_t)M * 3);
+            cudaCheck(cudaMemcpy(rows[r].data(), v_.dGdr + (size_t)r * capacity_ * 3, sizeof(double) * M * 3,
+                                 cudaMemcpyDeviceToHost),
+                      "D2H");
+        }
+        for (int64_t e = 0; e < M; ++e)
+            for (int r = 0; r < rowsOf[e]; ++r)
+                for (int c = 0; c < 3; ++c) nbr[k++] = rows[r][(size_t)e * 3 + c];
+    }
+}
+
+} // namespace n2p2b200

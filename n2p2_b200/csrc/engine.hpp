@@ -1,0 +1,127 @@
+// Device-side engine: the uploaded model, batches of structures and the
+// evaluation sequence of Mode::evaluateNNP (Mode.cpp:2029-2077) on one GPU.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "device_model.hpp"
+#include "host_model.hpp"
+#include "kernels.hpp"
+
+namespace n2p2b200 {
+
+enum Precision { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+// Evaluation flags (bit set).
+enum EvalFlags : int {
+    EVAL_FORCES = 1,          // forces (else energies only)
+    EVAL_STORE_DGDR = 2,      // keep dG/dr per neighbour row (API form)
+    EVAL_NO_GRAPH = 4,        // launch kernels directly instead of replaying a CUDA graph
+};
+
+void cudaCheck(cudaError_t e, char const* what);
+
+// Device copy of a set-up model.
+class DeviceModel
+{
+public:
+    ~DeviceModel();
+    void upload(Model const& m);
+    DevModel view;
+    int maxSF = 0;
+
+private:
+    void release();
+    DevGroup* groups_ = nullptr;
+    DevMember* members_ = nullptr;
+    DevScaling* scaling_ = nullptr;
+    int* rowTable_ = nullptr;
+    double* weights_ = nullptr;
+    float* weightsF_ = nullptr;
+};
+
+struct StructureInput
+{
+    int numAtoms = 0;
+    double box[9] = {0};      // physical units, rows = box vectors
+    int periodic = 0;
+};
+
+class Batch
+{
+public:
+    Batch(Model const& model, DeviceModel const& dmodel, cudaStream_t stream, int sms);
+    ~Batch();
+
+    // Structures and atoms.  Positions are physical units (as in input.data);
+    // `remap` folds periodic positions into the cell (Structure::remap),
+    // normalisation (if the model uses it) is applied on the device.
+    void setStructures(std::vector<StructureInput> const& s, const int* elements, int remap);
+    // Positions host -> device (pinned or pageable host memory), async on the stream.
+    void setPositionsHost(const double* r);
+    void setPositionsDevice(const double* r);
+    // Mode::evaluateNNP; asynchronous unless the neighbour capacity must be
+    // (re)established, which happens on the first call and after overflow.
+    void evaluate(int flags, int precision, int checkExtrapolation);
+    // Host-side results (synchronise first).
+    void energies(double* out);       // physical units, with atomic energy offsets
+    void forces(double* out);         // physical units, [N][3]
+    void synchronize();
+    DevStatus status();
+
+    int numAtoms() const { return N_; }
+    int numStructures() const { return S_; }
+    int64_t numNeighborEntries();
+    BatchView const& view() const { return v_; }
+    cudaStream_t stream() const { return stream_; }
+    int launchesPerEvaluate() const { return launches_; }
+
+    // Internal-unit results for inspection (neighbour lists, G, dEdG, dGdr).
+    void copyNeighbors(int64_t* offsets, int* index, int* image, double* d, double* dr);
+    void copyG(double* out);          // [N][numSF of the atom's element], concatenated
+    void copyDEdG(double* out);
+    void copyAtomicEnergies(double* out);
+    void copyDGdr(double* self, double* nbr);   // self [sum numSF][3], nbr [sum rows][3]
+    void copyPositions(double* out);  // internal units after remap/normalisation
+    void copyAtomWarnings(int* out);
+
+private:
+    void allocateAtoms();
+    void allocateNeighbors(int64_t capacity);
+    void allocateDGdr();
+    void record(int flags, int precision, int checkExtrapolation);
+    void releaseGraph();
+    void releaseAll();
+
+    Model const& model_;
+    DeviceModel const& dmodel_;
+    cudaStream_t stream_;
+    int sms_;
+    int N_ = 0, S_ = 0;
+    std::vector<StructureInput> structs_;
+    std::vector<int> elemHost_;
+    std::vector<int> structBegin_;
+    std::vector<int> numAtomsPerElement_;   // [S][numElements]
+    int remap_ = 1;
+    BatchView v_{};
+    double* rin_ = nullptr;                 // raw positions (physical)
+    DevStructInfo* infoDev_ = nullptr;
+    int* atomStructDev_ = nullptr;
+    int* elemDev_ = nullptr;
+    int* structBeginDev_ = nullptr;
+    int64_t capacity_ = 0;
+    bool capacityVerified_ = false;
+    bool dgdrAllocated_ = false;
+    cudaGraphExec_t graphExec_ = nullptr;
+    int graphKey_ = -1;
+    int launches_ = 0;
+    std::vector<void*> owned_;
+    std::vector<void*> ownedNbr_;
+    std::vector<void*> ownedDGdr_;
+};
+
+} // namespace n2p2b200

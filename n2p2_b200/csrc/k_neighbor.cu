@@ -1,0 +1,489 @@
+// Neighbour-list build on sm_100a: remap, cell binning, candidate search over
+// a periodic cell stencil, per-atom ordering and the reverse-entry index.
+//
+// Result contract (Structure::calculateNeighborList, Structure.cpp:287-398):
+// for every atom i the entries are all (j, image) with
+//     dr = r_i - r_j + bc0*box0 + bc1*box1 + bc2*box2,   dr.dr <= rc^2,
+// excluding (i, 0), ordered by j ascending then (bc0, bc1, bc2)
+// lexicographically, with d = sqrt(dr.dr).  Every floating-point step uses
+// explicit round-to-nearest intrinsics in the reference's evaluation order
+// (Vec3D.h:294-361), so d and dr are bit-identical to the reference.
+#include "kernels_common.cuh"
+#include "kernels.hpp"
+
+namespace n2p2b200 {
+
+namespace {
+
+__device__ __forceinline__ int floorDiv(int a, int b)
+{
+    int q = a / b;
+    if ((a % b != 0) && ((a < 0) != (b < 0))) --q;
+    return q;
+}
+
+__device__ __forceinline__ int imageCode(int bc0, int bc1, int bc2, int const* p)
+{
+    return ((bc0 + p[0]) * (2 * p[1] + 1) + (bc1 + p[1])) * (2 * p[2] + 1) + (bc2 + p[2]);
+}
+
+__device__ __forceinline__ void imageFromCode(int code, int const* p, int& bc0, int& bc1, int& bc2)
+{
+    int n2 = 2 * p[2] + 1, n1 = 2 * p[1] + 1;
+    bc2 = code % n2 - p[2];
+    code /= n2;
+    bc1 = code % n1 - p[1];
+    code /= n1;
+    bc0 = code - p[0];
+}
+
+// dr = r_i - r_j + bc0*b0 + bc1*b1 + bc2*b2, component c, no contraction.
+__device__ __forceinline__ double pairComponent(double ri, double rj, double const* box, int c, int bc0, int bc1,
+                                                int bc2)
+{
+    double v = __dsub_rn(ri, rj);
+    v = __dadd_rn(v, __dmul_rn(box[0 * 3 + c], (double)bc0));
+    v = __dadd_rn(v, __dmul_rn(box[1 * 3 + c], (double)bc1));
+    v = __dadd_rn(v, __dmul_rn(box[2 * 3 + c], (double)bc2));
+    return v;
+}
+
+__device__ __forceinline__ double norm2Exact(double x, double y, double z)
+{
+    return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+} // namespace
+
+// Structure::remap (Structure.cpp:1224-1248) in physical units, then
+// Atom::toNormalizedUnits' r *= convLength (Atom.cpp:78-85).
+__global__ void kPreparePositions(int N, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
+                                  const double* __restrict__ rin, double* __restrict__ px, double* __restrict__ py,
+                                  double* __restrict__ pz, int doRemap, int doNormalize, double convLength)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    {
+        DevStructInfo const& s = info[atomStruct[i]];
+        double r[3] = {rin[3 * i + 0], rin[3 * i + 1], rin[3 * i + 2]};
+        if (doRemap && s.periodic)
+        {
+            double f[3];
+            for (int c = 0; c < 3; ++c)
+            {
+                double t = __dmul_rn(s.invboxPhys[0 * 3 + c], r[0]);
+                t = __dadd_rn(t, __dmul_rn(s.invboxPhys[1 * 3 + c], r[1]));
+                t = __dadd_rn(t, __dmul_rn(s.invboxPhys[2 * 3 + c], r[2]));
+                f[c] = t;
+            }
+            for (int c = 0; c < 3; ++c)
+            {
+                if (f[c] > 1.0) f[c] = __dsub_rn(f[c], (double)(int)f[c]);
+                if (f[c] < 0.0) f[c] = __dadd_rn(f[c], __dsub_rn(1.0, (double)(int)f[c]));
+                if (f[c] == 1.0) f[c] = 0.0;
+            }
+            for (int c = 0; c < 3; ++c)
+            {
+                double t = __dmul_rn(s.boxPhys[0 * 3 + c], f[0]);
+                t = __dadd_rn(t, __dmul_rn(s.boxPhys[1 * 3 + c], f[1]));
+                t = __dadd_rn(t, __dmul_rn(s.boxPhys[2 * 3 + c], f[2]));
+                r[c] = t;
+            }
+        }
+        if (doNormalize)
+        {
+            for (int c = 0; c < 3; ++c) r[c] = __dmul_rn(r[c], convLength);
+        }
+        px[i] = r[0];
+        py[i] = r[1];
+        pz[i] = r[2];
+    }
+}
+
+// Cell of every atom: fractional coordinate f = r . invbox, cell = floor(f*nc).
+__global__ void kAssignCells(int N, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
+                             const double* __restrict__ px, const double* __restrict__ py,
+                             const double* __restrict__ pz, int* __restrict__ atomCell, int* __restrict__ atomSlot,
+                             int* __restrict__ cellCount)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    {
+        DevStructInfo const& s = info[atomStruct[i]];
+        int c3[3] = {0, 0, 0};
+        if (s.periodic)
+        {
+            double r[3] = {px[i], py[i], pz[i]};
+            for (int a = 0; a < 3; ++a)
+            {
+                double f = s.invbox[0 * 3 + a] * r[0] + s.invbox[1 * 3 + a] * r[1] + s.invbox[2 * 3 + a] * r[2];
+                f -= floor(f);  // positions outside the cell are folded for binning only
+                int c = (int)floor(f * s.nc[a]);
+                c3[a] = min(max(c, 0), s.nc[a] - 1);
+            }
+        }
+        int cell = s.cellBegin + (c3[0] * s.nc[1] + c3[1]) * s.nc[2] + c3[2];
+        atomCell[i] = cell;
+        atomSlot[i] = atomicAdd(&cellCount[cell], 1);
+    }
+}
+
+__global__ void kScatterCells(int N, const int* __restrict__ atomCell, const int* __restrict__ atomSlot,
+                              const int* __restrict__ cellStart, int* __restrict__ cellAtoms)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        cellAtoms[cellStart[atomCell[i]] + atomSlot[i]] = i;
+}
+
+// One warp per centre atom.  PASS 0 counts, PASS 1 writes the unordered
+// candidates into the atom's segment of the scratch arrays.
+template <int PASS>
+__global__ void __launch_bounds__(256) kNeighborSearch(
+    int N, double rc2, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
+    const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
+    const int* __restrict__ atomCell, const int* __restrict__ cellStart, const int* __restrict__ cellCountArr,
+    const int* __restrict__ cellAtoms, int* __restrict__ nbrCount, const int64_t* __restrict__ nbrOffset,
+    int64_t capacity, int64_t* __restrict__ scrKey, double* __restrict__ scrD, double* __restrict__ scrDx,
+    double* __restrict__ scrDy, double* __restrict__ scrDz, DevStatus* __restrict__ status)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warpsPerGrid)
+    {
+        DevStructInfo const& s = info[atomStruct[i]];
+        const double xi = px[i], yi = py[i], zi = pz[i];
+        const int local = atomCell[i] - s.cellBegin;
+        const int cz = local % s.nc[2];
+        const int cy = (local / s.nc[2]) % s.nc[1];
+        const int cx = local / (s.nc[2] * s.nc[1]);
+        const int K = (2 * s.pbc[0] + 1) * (2 * s.pbc[1] + 1) * (2 * s.pbc[2] + 1);
+        int count = 0;
+        int64_t base = 0, limit = 0;
+        if (PASS == 1)
+        {
+            base = nbrOffset[i];
+            limit = nbrOffset[i + 1];
+            if (limit > capacity) limit = capacity;   // overflow is flagged by the host check
+        }
+        for (int ox = -s.stencil[0]; ox <= s.stencil[0]; ++ox)
+        {
+            int qx = cx + ox, tx = floorDiv(qx, s.nc[0]), wx = qx - tx * s.nc[0], bc0 = -tx;
+            if (bc0 < -s.pbc[0] || bc0 > s.pbc[0]) continue;
+            for (int oy = -s.stencil[1]; oy <= s.stencil[1]; ++oy)
+            {
+                int qy = cy + oy, ty = floorDiv(qy, s.nc[1]), wy = qy - ty * s.nc[1], bc1 = -ty;
+                if (bc1 < -s.pbc[1] || bc1 > s.pbc[1]) continue;
+                for (int oz = -s.stencil[2]; oz <= s.stencil[2]; ++oz)
+                {
+                    int qz = cz + oz, tz = floorDiv(qz, s.nc[2]), wz = qz - tz * s.nc[2], bc2 = -tz;
+                    if (bc2 < -s.pbc[2] || bc2 > s.pbc[2]) continue;
+                    const int cell = s.cellBegin + (wx * s.nc[1] + wy) * s.nc[2] + wz;
+                    const int cnt = cellCountArr[cell];
+                    const int start = cellStart[cell];
+                    for (int t0 = 0; t0 < cnt; t0 += 32)
+                    {
+                        const int t = t0 + lane;
+                        bool hit = false;
+                        double dx = 0, dy = 0, dz = 0, d2 = 0;
+                        int j = -1;
+                        if (t < cnt)
+                        {
+                            j = cellAtoms[start + t];
+                            if (!(j == i && bc0 == 0 && bc1 == 0 && bc2 == 0))
+                            {
+                                dx = pairComponent(xi, px[j], s.box, 0, bc0, bc1, bc2);
+                                dy = pairComponent(yi, py[j], s.box, 1, bc0, bc1, bc2);
+                                dz = pairComponent(zi, pz[j], s.box, 2, bc0, bc1, bc2);
+                                d2 = norm2Exact(dx, dy, dz);
+                                hit = (d2 <= rc2);
+                            }
+                        }
+                        if (PASS == 0)
+                        {
+                            count += hit ? 1 : 0;
+                        }
+                        else
+                        {
+                            unsigned m = __ballot_sync(kFullMask, hit);
+                            int pos = __popc(m & ((1u << lane) - 1u));
+                            if (hit)
+                            {
+                                int64_t e = base + count + pos;
+                                if (e < limit)
+                                {
+                                    scrKey[e] = (int64_t)(j - s.atomBegin) * K + imageCode(bc0, bc1, bc2, s.pbc);
+                                    scrD[e] = __dsqrt_rn(d2);
+                                    scrDx[e] = dx;
+                                    scrDy[e] = dy;
+                                    scrDz[e] = dz;
+                                }
+                            }
+                            count += __popc(m);
+                        }
+                    }
+                }
+            }
+        }
+        if (PASS == 0)
+        {
+            count = warpSumInt(count);
+            if (lane == 0)
+            {
+                nbrCount[i] = count;
+                atomicMax(&status->maxNeighbors, count);
+            }
+        }
+    }
+}
+
+// Orders every atom's segment by key = (j - atomBegin) * K + imageCode, i.e.
+// j ascending, then images in the reference loop order.  Rank sort: keys are
+// unique within a segment, so an entry's rank is the number of smaller keys.
+__global__ void __launch_bounds__(256) kNeighborSort(
+    int N, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
+    const int64_t* __restrict__ nbrOffset, int64_t capacity, const int64_t* __restrict__ scrKey,
+    const double* __restrict__ scrD, const double* __restrict__ scrDx, const double* __restrict__ scrDy,
+    const double* __restrict__ scrDz, int* __restrict__ nbrJ, int* __restrict__ nbrCode, double* __restrict__ nbrD,
+    double* __restrict__ nbrDx, double* __restrict__ nbrDy, double* __restrict__ nbrDz)
+{
+    constexpr int kSmemKeys = 512;
+    __shared__ int64_t skeys[8][kSmemKeys];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warpsPerGrid)
+    {
+        const int64_t off = nbrOffset[i];
+        const int64_t end = nbrOffset[i + 1];
+        if (end > capacity) continue;
+        const int n = (int)(end - off);
+        DevStructInfo const& s = info[atomStruct[i]];
+        const int K = (2 * s.pbc[0] + 1) * (2 * s.pbc[1] + 1) * (2 * s.pbc[2] + 1);
+        const bool inSmem = n <= kSmemKeys;
+        if (inSmem)
+            for (int e = lane; e < n; e += 32) skeys[w][e] = scrKey[off + e];
+        __syncwarp();
+        const int64_t* keys = inSmem ? skeys[w] : scrKey + off;
+        for (int e = lane; e < n; e += 32)
+        {
+            const int64_t k = keys[e];
+            int rank = 0;
+            for (int q = 0; q < n; ++q) rank += (keys[q] < k) ? 1 : 0;
+            const int64_t dst = off + rank;
+            nbrJ[dst] = (int)(k / K) + s.atomBegin;
+            nbrCode[dst] = (int)(k % K);
+            nbrD[dst] = scrD[off + e];
+            nbrDx[dst] = scrDx[off + e];
+            nbrDy[dst] = scrDy[off + e];
+            nbrDz[dst] = scrDz[off + e];
+        }
+        __syncwarp();
+    }
+}
+
+// rev[e] for entry e = (i -> j, bc): the entry (j -> i, -bc) in j's list.
+// Pairs are exactly symmetric because the pair vector arithmetic is odd under
+// exchange of i and j with negated images.
+__global__ void kNeighborReverse(int N, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
+                                 const int64_t* __restrict__ nbrOffset, int64_t capacity,
+                                 const int* __restrict__ nbrJ, const int* __restrict__ nbrCode,
+                                 int64_t* __restrict__ rev, DevStatus* __restrict__ status)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warpsPerGrid)
+    {
+        if (nbrOffset[i + 1] > capacity) continue;   // overflow: the host re-runs with more room
+        DevStructInfo const& s = info[atomStruct[i]];
+        const int K = (2 * s.pbc[0] + 1) * (2 * s.pbc[1] + 1) * (2 * s.pbc[2] + 1);
+        for (int64_t e = nbrOffset[i] + lane; e < nbrOffset[i + 1]; e += 32)
+        {
+            const int j = nbrJ[e];
+            if (nbrOffset[j + 1] > capacity)
+            {
+                rev[e] = -1;
+                continue;
+            }
+            int bc0, bc1, bc2;
+            imageFromCode(nbrCode[e], s.pbc, bc0, bc1, bc2);
+            const int64_t want = (int64_t)(i - s.atomBegin) * K + imageCode(-bc0, -bc1, -bc2, s.pbc);
+            int64_t lo = nbrOffset[j], hi = nbrOffset[j + 1] - 1, found = -1;
+            while (lo <= hi)
+            {
+                int64_t mid = (lo + hi) >> 1;
+                int64_t k = (int64_t)(nbrJ[mid] - s.atomBegin) * K + nbrCode[mid];
+                if (k == want)
+                {
+                    found = mid;
+                    break;
+                }
+                if (k < want) lo = mid + 1;
+                else hi = mid - 1;
+            }
+            rev[e] = found;
+            if (found < 0) atomicAdd(&status->badInput, 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Device-wide exclusive scan (three phases) of int counts into int64 offsets.
+// ---------------------------------------------------------------------------
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(kScanThreads) kScanTiles(int n, const int* __restrict__ in,
+                                                           int64_t* __restrict__ out, int64_t* __restrict__ tileSums)
+{
+    __shared__ int64_t warpTot[kScanThreads / 32];
+    const int tile = blockIdx.x;
+    const int base = tile * kScanTile + threadIdx.x * kScanItems;
+    int64_t v[kScanItems];
+    int64_t run = 0;
+    for (int k = 0; k < kScanItems; ++k)
+    {
+        int idx = base + k;
+        int64_t x = idx < n ? (int64_t)in[idx] : 0;
+        v[k] = run;
+        run += x;
+    }
+    // inclusive scan of per-thread totals across the block
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t incl = run;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        int64_t y = __shfl_up_sync(kFullMask, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) warpTot[w] = incl;
+    __syncthreads();
+    if (w == 0)
+    {
+        int64_t t = lane < kScanThreads / 32 ? warpTot[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            int64_t y = __shfl_up_sync(kFullMask, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < kScanThreads / 32) warpTot[lane] = t;
+    }
+    __syncthreads();
+    int64_t prefix = (incl - run) + (w > 0 ? warpTot[w - 1] : 0);
+    for (int k = 0; k < kScanItems; ++k)
+    {
+        int idx = base + k;
+        if (idx < n) out[idx] = prefix + v[k];
+    }
+    if (threadIdx.x == kScanThreads - 1) tileSums[tile] = prefix + run;
+}
+
+// Single block: exclusive scan of the tile sums (in place); writes the grand
+// total to out[n] and, if given, to *total.
+__global__ void __launch_bounds__(1024) kScanTileSums(int numTiles, int64_t* __restrict__ tileSums, int n,
+                                                      int64_t* __restrict__ out, int64_t* __restrict__ total)
+{
+    __shared__ int64_t warpTot[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int per = (numTiles + blockDim.x - 1) / blockDim.x;
+    const int begin = threadIdx.x * per;
+    int64_t run = 0;
+    for (int k = 0; k < per; ++k)
+        if (begin + k < numTiles) run += tileSums[begin + k];
+    int64_t incl = run;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        int64_t y = __shfl_up_sync(kFullMask, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) warpTot[w] = incl;
+    __syncthreads();
+    if (w == 0)
+    {
+        int64_t t = warpTot[lane];
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            int64_t y = __shfl_up_sync(kFullMask, t, o);
+            if (lane >= o) t += y;
+        }
+        warpTot[lane] = t;
+    }
+    __syncthreads();
+    int64_t prefix = (incl - run) + (w > 0 ? warpTot[w - 1] : 0);
+    for (int k = 0; k < per; ++k)
+    {
+        if (begin + k < numTiles)
+        {
+            int64_t x = tileSums[begin + k];
+            tileSums[begin + k] = prefix;
+            prefix += x;
+        }
+    }
+    if (threadIdx.x == blockDim.x - 1)
+    {
+        out[n] = prefix;
+        if (total) *total = prefix;
+    }
+}
+
+__global__ void kScanAdd(int n, const int64_t* __restrict__ tileSums, int64_t* __restrict__ out)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x)
+        out[idx] += tileSums[idx / kScanTile];
+}
+
+void launchExclusiveScan(int n, const int* in, int64_t* out, int64_t* tileSums, int64_t* total, cudaStream_t st)
+{
+    int tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles < 1) tiles = 1;
+    kScanTiles<<<tiles, kScanThreads, 0, st>>>(n, in, out, tileSums);
+    kScanTileSums<<<1, 1024, 0, st>>>(tiles, tileSums, n, out, total);
+    kScanAdd<<<(n + 255) / 256 > 0 ? (n + 255) / 256 : 1, 256, 0, st>>>(n, tileSums, out);
+}
+
+int scanTileCount(int n) { return (n + kScanTile - 1) / kScanTile + 1; }
+
+// ---------------------------------------------------------------------------
+// Launch wrappers
+// ---------------------------------------------------------------------------
+
+__global__ void kCast64to32(int n, const int64_t* __restrict__ in, int* __restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (int)in[i];
+}
+
+void launchPreparePositions(BatchView const& b, const double* rin, int doRemap, int doNormalize, double convLength,
+                            cudaStream_t st)
+{
+    int blocks = (b.N + 255) / 256;
+    kPreparePositions<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(b.N, b.atomStruct, b.info, rin, b.px, b.py, b.pz,
+                                                               doRemap, doNormalize, convLength);
+}
+
+void launchNeighborBuild(BatchView const& b, double rc2, cudaStream_t st)
+{
+    const int N = b.N;
+    const int blocks = (N + 255) / 256 > 0 ? (N + 255) / 256 : 1;
+    cudaMemsetAsync(b.cellCount, 0, sizeof(int) * (size_t)b.numCells, st);
+    kAssignCells<<<blocks, 256, 0, st>>>(N, b.atomStruct, b.info, b.px, b.py, b.pz, b.atomCell, b.atomSlot,
+                                         b.cellCount);
+    launchExclusiveScan(b.numCells, b.cellCount, b.cellStart64, b.scanTmp, nullptr, st);
+    kCast64to32<<<(b.numCells + 255) / 256 > 0 ? (b.numCells + 255) / 256 : 1, 256, 0, st>>>(b.numCells,
+                                                                                          b.cellStart64, b.cellStart);
+    kScatterCells<<<blocks, 256, 0, st>>>(N, b.atomCell, b.atomSlot, b.cellStart, b.cellAtoms);
+    const int warpBlocks = (N + 7) / 8 > 0 ? (N + 7) / 8 : 1;
+    kNeighborSearch<0><<<warpBlocks, 256, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz, b.atomCell,
+                                                   b.cellStart, b.cellCount, b.cellAtoms, b.nbrCount, nullptr, 0,
+                                                   nullptr, nullptr, nullptr, nullptr, nullptr, b.status);
+    launchExclusiveScan(N, b.nbrCount, b.nbrOffset, b.scanTmp, &b.status->totalNeighbors, st);
+    kNeighborSearch<1><<<warpBlocks, 256, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz, b.atomCell,
+                                                   b.cellStart, b.cellCount, b.cellAtoms, nullptr, b.nbrOffset,
+                                                   b.nbrCapacity, b.scrKey, b.scrD, b.scrDx, b.scrDy, b.scrDz,
+                                                   b.status);
+    kNeighborSort<<<warpBlocks, 256, 0, st>>>(N, b.atomStruct, b.info, b.nbrOffset, b.nbrCapacity, b.scrKey, b.scrD,
+                                              b.scrDx, b.scrDy, b.scrDz, b.nbrJ, b.nbrCode, b.nbrD, b.nbrDx,
+                                              b.nbrDy, b.nbrDz);
+    kNeighborReverse<<<warpBlocks, 256, 0, st>>>(N, b.atomStruct, b.info, b.nbrOffset, b.nbrCapacity, b.nbrJ,
+                                                 b.nbrCode, b.rev, b.status);
+}
+
+} // namespace n2p2b200

@@ -1,0 +1,286 @@
+// Atomic neural networks (FP64 form), per-structure energy sums and the
+// deterministic force gather.
+//
+// Network: NeuralNetwork::propagate / propagateLayer (NeuralNetwork.cpp:386-394,
+// 761-896) for the activations of the reference, and dE/dG by reverse-mode
+// accumulation, which equals NeuralNetwork::calculateDEdG
+// (NeuralNetwork.cpp:396-442) including the normalize_nodes divisions.
+#include "kernels_common.cuh"
+#include "kernels.hpp"
+
+namespace n2p2b200 {
+
+namespace {
+
+constexpr double kExpLimit = 35.0;   // EXP_LIMIT, NeuralNetwork.cpp:25
+
+// Activation value and first derivative for one neuron.
+__device__ __forceinline__ void activate(int af, double x, double& y, double& dy)
+{
+    switch (af)
+    {
+    case AF_IDENTITY: y = x; dy = 1.0; return;
+    case AF_TANH:
+    {
+        double t = tanh(x);
+        y = t;
+        dy = 1.0 - t * t;
+        return;
+    }
+    case AF_LOGISTIC:
+        if (x > kExpLimit) { y = 1.0; dy = 0.0; }
+        else if (x < -kExpLimit) { y = 0.0; dy = 0.0; }
+        else
+        {
+            double t = 1.0 / (1.0 + exp(-x));
+            y = t;
+            dy = t * (1.0 - t);
+        }
+        return;
+    case AF_SOFTPLUS:
+        if (x > kExpLimit) { y = x; dy = 1.0; }
+        else if (x < -kExpLimit) { y = 0.0; dy = 0.0; }
+        else
+        {
+            double t = exp(x);
+            y = log(1.0 + t);
+            dy = 1.0 / (1.0 + 1.0 / t);
+        }
+        return;
+    case AF_RELU:
+        if (x > 0.0) { y = x; dy = 1.0; }
+        else { y = 0.0; dy = 0.0; }
+        return;
+    case AF_GAUSSIAN:
+    {
+        double t = exp(-0.5 * x * x);
+        y = t;
+        dy = -x * t;
+        return;
+    }
+    case AF_COS: y = cos(x); dy = -sin(x); return;
+    case AF_REVLOGISTIC:
+    {
+        double t = 1.0 / (1.0 + exp(-x));
+        y = 1.0 - t;
+        dy = t * (t - 1.0);
+        return;
+    }
+    case AF_EXP:
+    {
+        double t = exp(-x);
+        y = t;
+        dy = -t;
+        return;
+    }
+    case AF_HARMONIC: y = x * x; dy = 2.0 * x; return;
+    }
+    y = 0.0;
+    dy = 0.0;
+}
+
+constexpr int kNNWarps = 4;
+
+struct NNWarpSmem
+{
+    double act[2][kMaxNeurons < kMaxSFPerElement ? kMaxSFPerElement : kMaxNeurons];
+    double dfdx[kDevMaxLayers][kMaxNeurons];
+    double g[2][kMaxNeurons];
+};
+
+} // namespace
+
+// One warp per atom; lanes split the neurons of a layer.  Weights are read
+// through the read-only cache (all warps of an element share them).
+__global__ void __launch_bounds__(kNNWarps * 32) kNetworkFP64(DevModel model, BatchView b, int derivatives)
+{
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    NNWarpSmem* smAll = reinterpret_cast<NNWarpSmem*>(smemRaw);
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    NNWarpSmem& S = smAll[w];
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
+    {
+        const int ec = b.elem[i];
+        DevElement const& E = model.el[ec];
+        const int L = E.numLayers;
+        const double* Gi = b.G + (size_t)i * b.gStride;
+        __syncwarp();
+        for (int k = lane; k < E.neurons[0]; k += 32) S.act[0][k] = Gi[k];
+        __syncwarp();
+        int cur = 0;
+        for (int l = 1; l < L; ++l)
+        {
+            const int nin = E.neurons[l - 1], nout = E.neurons[l];
+            const double* W = model.weights + E.wOffset[l];
+            const double* bias = model.weights + E.bOffset[l];
+            for (int k = lane; k < nout; k += 32)
+            {
+                double x = 0.0;
+                const double* row = W + (size_t)k * nin;
+                for (int j = 0; j < nin; ++j) x += __ldg(&row[j]) * S.act[cur][j];
+                x += __ldg(&bias[k]);
+                if (model.normalizeNeurons) x /= nin;
+                double y, dy;
+                activate(E.activation[l], x, y, dy);
+                S.act[cur ^ 1][k] = y;
+                S.dfdx[l][k] = dy;
+            }
+            __syncwarp();
+            cur ^= 1;
+        }
+        if (lane == 0) b.Eatom[i] = S.act[cur][0];
+        if (!derivatives) continue;
+        // Reverse pass: g_L = f'_L; g_{l-1} = f'_{l-1} * (W_l^T g_l) / n_{l-1}?; dEdG = W_1^T g_1 / n_0?
+        __syncwarp();
+        int gc = 0;
+        if (lane == 0)
+        {
+            double g0 = S.dfdx[L - 1][0];
+            if (model.normalizeNeurons) g0 /= E.neurons[L - 2];
+            S.g[0][0] = g0;
+        }
+        __syncwarp();
+        for (int l = L - 1; l >= 2; --l)
+        {
+            const int nin = E.neurons[l - 1], nout = E.neurons[l];
+            const double* W = model.weights + E.wOffset[l];
+            for (int j = lane; j < nin; j += 32)
+            {
+                double s = 0.0;
+                for (int k = 0; k < nout; ++k) s += __ldg(&W[(size_t)k * nin + j]) * S.g[gc][k];
+                s *= S.dfdx[l - 1][j];
+                if (model.normalizeNeurons) s /= E.neurons[l - 2];
+                S.g[gc ^ 1][j] = s;
+            }
+            __syncwarp();
+            gc ^= 1;
+        }
+        {
+            const int nin = E.neurons[0], nout = E.neurons[1];
+            const double* W = model.weights + E.wOffset[1];
+            double* out = b.dEdG + (size_t)i * b.gStride;
+            for (int j = lane; j < nin; j += 32)
+            {
+                double s = 0.0;
+                for (int k = 0; k < nout; ++k) s += __ldg(&W[(size_t)k * nin + j]) * S.g[gc][k];
+                out[j] = s;
+            }
+        }
+    }
+}
+
+// E_s = sum of atomic energies of structure s (Mode::calculateEnergy,
+// Mode.cpp:1876-1901), one warp per structure, fixed summation order.
+__global__ void kEnergySum(BatchView b)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < b.S; s += warpsPerGrid)
+    {
+        const int a0 = b.structAtomBegin[s], a1 = b.structAtomBegin[s + 1];
+        double e = 0.0;
+        for (int a = a0 + lane; a < a1; a += 32) e += b.Eatom[a];
+        e = warpSum(e);
+        if (lane == 0) b.Estruct[s] = e;
+    }
+}
+
+// F_i = self force + sum over neighbours j != i of the force E_j puts on i
+// (Mode::calculateForces 2G part, Mode.cpp:1922-1984).  The entries of i's
+// list that point at the same j are visited in reverse image order, so that
+// the contributions arrive in the order of j's own list, as in the reference.
+__global__ void kGatherForces(BatchView b)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < b.N; i += gridDim.x * blockDim.x)
+    {
+        const int64_t off = b.nbrOffset[i];
+        const int64_t end = b.nbrOffset[i + 1];
+        double fx = b.fSelf[3 * (size_t)i + 0];
+        double fy = b.fSelf[3 * (size_t)i + 1];
+        double fz = b.fSelf[3 * (size_t)i + 2];
+        if (end <= b.nbrCapacity)
+        {
+            int64_t e = off;
+            while (e < end)
+            {
+                const int j = b.nbrJ[e];
+                int64_t runEnd = e + 1;
+                while (runEnd < end && b.nbrJ[runEnd] == j) ++runEnd;
+                if (j != i)
+                {
+                    for (int64_t q = runEnd - 1; q >= e; --q)
+                    {
+                        const int64_t r = b.rev[q];
+                        if (r < 0) continue;
+                        fx += b.hx[r];
+                        fy += b.hy[r];
+                        fz += b.hz[r];
+                    }
+                }
+                e = runEnd;
+            }
+        }
+        b.F[3 * (size_t)i + 0] = fx;
+        b.F[3 * (size_t)i + 1] = fy;
+        b.F[3 * (size_t)i + 2] = fz;
+    }
+}
+
+// Extrapolation check of Element::updateSymmetryFunctionStatistics
+// (Element.cpp:462-541): unscaled G outside [Gmin, Gmax] by more than
+// 1000 machine epsilon counts one warning.  One thread per atom.
+__global__ void kExtrapolationCheck(DevModel model, BatchView b)
+{
+    const double eps = 1000.0 * 2.220446049250313080847e-16;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < b.N; i += gridDim.x * blockDim.x)
+    {
+        DevElement const& E = model.el[b.elem[i]];
+        const double* g = b.G + (size_t)i * b.gStride;
+        int count = 0;
+        for (int s = 0; s < E.numSF; ++s)
+        {
+            DevScaling const& sc = model.scaling[E.sfBegin + s];
+            const double v = unscaleG(sc, g[s]);
+            if (v + eps < sc.Gmin || v - eps > sc.Gmax) count++;
+        }
+        b.atomWarnings[i] = count;
+        if (count) atomicAdd(&b.status->extrapolationWarnings, count);
+    }
+}
+
+void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
+{
+    int blocks = (b.N + 127) / 128;
+    if (blocks < 1) blocks = 1;
+    if (blocks > sms * 16) blocks = sms * 16;
+    kExtrapolationCheck<<<blocks, 128, 0, st>>>(m, b);
+}
+
+void launchNetworkFP64(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st)
+{
+    size_t smem = sizeof(NNWarpSmem) * kNNWarps;
+    setDynamicSmemOnce(reinterpret_cast<const void*>(kNetworkFP64), smem);
+    int blocks = (b.N + kNNWarps - 1) / kNNWarps;
+    if (blocks < 1) blocks = 1;
+    if (blocks > sms * 8) blocks = sms * 8;
+    kNetworkFP64<<<blocks, kNNWarps * 32, smem, st>>>(m, b, derivatives);
+}
+
+void launchEnergySum(BatchView const& b, cudaStream_t st)
+{
+    int blocks = (b.S + 7) / 8;
+    if (blocks < 1) blocks = 1;
+    kEnergySum<<<blocks, 256, 0, st>>>(b);
+}
+
+void launchGatherForces(BatchView const& b, int sms, cudaStream_t st)
+{
+    int blocks = (b.N + 127) / 128;
+    if (blocks < 1) blocks = 1;
+    if (blocks > sms * 16) blocks = sms * 16;
+    kGatherForces<<<blocks, 128, 0, st>>>(b);
+}
+
+} // namespace n2p2b200

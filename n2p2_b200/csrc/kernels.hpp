@@ -1,0 +1,92 @@
+// Device views of a batch and the kernel launch entry points.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_model.hpp"
+
+namespace n2p2b200 {
+
+// Raw device pointers of one batch of structures.  Atoms of all structures
+// are concatenated; neighbour lists are one CSR over all atoms.
+struct BatchView
+{
+    int N = 0;                 // atoms
+    int S = 0;                 // structures
+    int numCells = 0;
+    int gStride = 0;           // row stride of G / dEdG (>= max SF count)
+    const int* atomStruct = nullptr;
+    const int* elem = nullptr;
+    const int* structAtomBegin = nullptr;   // S+1
+    const DevStructInfo* info = nullptr;
+    double* px = nullptr;
+    double* py = nullptr;
+    double* pz = nullptr;
+    // cell list
+    int* atomCell = nullptr;
+    int* atomSlot = nullptr;
+    int* cellCount = nullptr;
+    int* cellStart = nullptr;
+    int64_t* cellStart64 = nullptr;
+    int* cellAtoms = nullptr;
+    int64_t* scanTmp = nullptr;
+    // neighbour CSR
+    int* nbrCount = nullptr;
+    int64_t* nbrOffset = nullptr;      // N+1
+    int64_t nbrCapacity = 0;
+    int64_t* scrKey = nullptr;
+    double* scrD = nullptr;
+    double* scrDx = nullptr;
+    double* scrDy = nullptr;
+    double* scrDz = nullptr;
+    int* nbrJ = nullptr;
+    int* nbrCode = nullptr;
+    double* nbrD = nullptr;
+    double* nbrDx = nullptr;
+    double* nbrDy = nullptr;
+    double* nbrDz = nullptr;
+    int64_t* rev = nullptr;
+    double* nbrFc = nullptr;           // [slot][entry]
+    double* nbrDfc = nullptr;
+    // symmetry functions and networks
+    double* G = nullptr;               // [atom][gStride]
+    double* dEdG = nullptr;
+    double* dGdr = nullptr;            // [row][entry][3] (stored form only)
+    double* dGdrSelf = nullptr;        // [atom][gStride][3] (stored form only)
+    double* Eatom = nullptr;
+    double* Estruct = nullptr;
+    double* hx = nullptr;              // force of E_i on neighbour entry (i -> j)
+    double* hy = nullptr;
+    double* hz = nullptr;
+    double* fSelf = nullptr;           // [atom][3]
+    double* F = nullptr;               // [atom][3]
+    int* atomWarnings = nullptr;
+    DevStatus* status = nullptr;
+};
+
+// Raise a kernel's dynamic shared-memory limit once per process.
+void setDynamicSmemOnce(const void* kernel, size_t bytes);
+
+// neighbour list
+void launchPreparePositions(BatchView const& b, const double* rin, int doRemap, int doNormalize, double convLength,
+                            cudaStream_t st);
+void launchNeighborBuild(BatchView const& b, double rc2, cudaStream_t st);
+void launchExclusiveScan(int n, const int* in, int64_t* out, int64_t* tileSums, int64_t* total, cudaStream_t st);
+int scanTileCount(int n);
+__global__ void kCast64to32(int n, const int64_t* __restrict__ in, int* __restrict__ out);
+
+// symmetry functions
+void launchCutoffValues(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
+void launchSFValues(DevModel const& m, BatchView const& b, int precision, int sms, cudaStream_t st);
+void launchSFForces(DevModel const& m, BatchView const& b, int precision, int sms, cudaStream_t st);
+void launchSFDerivatives(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
+void launchContractStored(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
+
+// networks, energies, forces
+void launchNetworkFP64(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st);
+void launchEnergySum(BatchView const& b, cudaStream_t st);
+void launchGatherForces(BatchView const& b, int sms, cudaStream_t st);
+void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
+
+} // namespace n2p2b200

@@ -1,0 +1,110 @@
+"""GPU parity of the FP64 path against the reference library (oracle/_ref).
+
+Tolerances: neighbour lists and remapped positions bit-exact; G within
+1e-12 (relative to the largest |G| of the structure); dE/dG, energies and
+forces within 1e-10 relative (forces relative to the largest force
+component of the structure), the plain-FP64 target of the path.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from n2p2_b200 import read_structures
+from n2p2_b200 import water
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+TOL_E = 1e-10
+TOL_F = 1e-10
+TOL_G = 1e-12
+
+
+def _compare_structure(b, a0, a1, snap, structure_index, energies, forces, check_g=True):
+    nb = H.split_neighbors(b.neighbors(), a0, a1)
+    # neighbour lists: same count, order, index and bit-identical d, dr
+    assert np.array_equal(nb["offset"], snap["nbr_offset"])
+    assert np.array_equal(nb["index"], snap["nbr_index"])
+    assert np.array_equal(nb["d"].view(np.int64), snap["nbr_d"].view(np.int64))
+    assert np.array_equal(nb["dr"].view(np.int64), snap["nbr_dr"].view(np.int64))
+    e_ref = snap["energy"]
+    assert abs(energies[structure_index] - e_ref) <= TOL_E * abs(e_ref)
+    f = forces[a0:a1]
+    assert H.max_rel(f, snap["forces"]) <= TOL_F
+
+
+@pytest.mark.parametrize("name", ["H2O_RPBE-D3", "Cu2S_PBE"])
+def test_reference_examples_golden(name):
+    """The reference's prediction regression examples (normalised units,
+    shifted G2, tanhU / poly2 cutoffs, tanh / softplus, scale+center /
+    sigma scaling, G3 and G9)."""
+    d = os.path.join(H.GOLDEN, "examples", name)
+    gold = json.load(open(os.path.join(d, "golden.json")))
+    s = read_structures(os.path.join(d, "input.data"))[0]
+    m = H.gpu_mode(d)
+    b = H.gpu_batch(m, [s])
+    e = b.energies()[0]
+    f = b.forces()
+    assert abs(e - gold["energy"]) <= TOL_E * abs(gold["energy"])
+    assert H.max_rel(f, np.array(gold["forces"])) <= TOL_F
+    # internal arrays against the reference library
+    snap = H.reference_snapshot(d, s)
+    pos = b.internalPositions()
+    assert np.array_equal(pos.view(np.int64), snap["positions"].view(np.int64))
+    _compare_structure(b, 0, s.numAtoms, snap, 0, b.energies(), f)
+    G = b.symmetryFunctions()
+    assert H.max_rel(G, snap["G"]) <= TOL_G
+    assert H.max_rel(b.dEdG(), snap["dEdG"]) <= TOL_E
+
+
+def test_water_box64_fp64():
+    s = water.water_box(64, seed=0)
+    m = H.gpu_mode(H.WATER40)
+    b = H.gpu_batch(m, [s])
+    snap = H.reference_snapshot(H.WATER40, s)
+    _compare_structure(b, 0, s.numAtoms, snap, 0, b.energies(), b.forces())
+    assert H.max_rel(b.symmetryFunctions(), snap["G"]) <= TOL_G
+    assert H.max_rel(b.atomicEnergies(), snap["atomic_energy"]) <= TOL_E
+    gold = json.load(open(os.path.join(H.GOLDEN, "water40_box64.json")))
+    assert abs(b.energies()[0] - gold["energy"]) <= TOL_E * abs(gold["energy"])
+
+
+def test_water_batch_uneven_fp64():
+    """Several boxes of uneven size in one batch (32..96 molecules)."""
+    boxes = water.water_batch(6, seed=7, n_min=32, n_max=96)
+    m = H.gpu_mode(H.WATER40)
+    b = H.gpu_batch(m, boxes)
+    E, F = b.energies(), b.forces()
+    a0 = 0
+    for k, s in enumerate(boxes):
+        snap = H.reference_snapshot(H.WATER40, s)
+        _compare_structure(b, a0, a0 + s.numAtoms, snap, k, E, F)
+        a0 += s.numAtoms
+
+
+def test_stored_dgdr_matches_reference():
+    """dG/dr stored per neighbour row (Atom::Neighbor::dGdr layout)."""
+    s = water.water_box(32, seed=1)
+    m = H.gpu_mode(H.WATER40)
+    b = H.gpu_batch(m, [s], store=True)
+    snap = H.reference_snapshot(H.WATER40, s)
+    selfd, nbr = b.dGdr(int(snap["row_offset"][-1]))
+    assert H.max_rel(selfd, snap["dGdr_self"]) <= 1e-11
+    assert H.max_rel(nbr, snap["dGdr_nbr"]) <= 1e-11
+    assert abs(b.energies()[0] - snap["energy"]) <= TOL_E * abs(snap["energy"])
+    assert H.max_rel(b.forces(), snap["forces"]) <= TOL_F
+
+
+def test_graph_replay_is_deterministic():
+    boxes = water.water_batch(4, seed=11, n_min=32, n_max=64)
+    m = H.gpu_mode(H.WATER40)
+    b = H.gpu_batch(m, boxes)
+    e1, f1 = b.energies(), b.forces()
+    for _ in range(3):
+        b.evaluate(forces=True)
+    b.synchronize()
+    e2, f2 = b.energies(), b.forces()
+    assert np.array_equal(e1.view(np.int64), e2.view(np.int64))
+    assert np.array_equal(f1.view(np.int64), f2.view(np.int64))
