@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Throughput of the 2G HDNNP energy + force path on B200.
+
+Workload (default): the batched benchmark configuration -- 2048 periodic water
+boxes of 32..512 molecules (log-uniform, seeded; ~1.06 M atoms), 40 symmetry
+functions per element (G2 + narrow G3, poly2 cutoff, rc = 12 bohr),
+40-25-25-1 softplus networks, plain FP64, all structures evaluated per step
+(neighbour lists, symmetry functions, networks, energies, forces) from one
+CUDA-graph launch.  Inputs are synthetic (seeded recipe), not a dataset.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One JSON line on rank 0.  `value` = atoms/s over all ranks (weak scaling:
+every rank evaluates its own batch of the same size, no collective on the
+data path; the time is the max over ranks).  `e2e` = the same metric through
+the C-ABI call with host buffers (positions H2D and energies + forces D2H
+inside the timed region).  `mixed` = the FP32-descriptor form on the same
+batch with its error against the FP64 reference.  `roofline` = the
+symmetry-function stage against the measured FP64 FMA throughput.
+`cpu_baseline` = the reference library on the host cores (bounded sample).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MODEL = os.path.join(ROOT, "tests", "golden", "models", "water40")
+METRIC = "atoms/s (E+F) on 1×B200: mixed/student vs plain FP64 at ≤1 meV/atom, 30 meV/Å"
+HA_TO_MEV = 27211.386
+HA_BOHR_TO_MEV_A = 27211.386 / 0.529177
+
+# Algorithmic FLOPs per unit of the reference's symmetry-function algorithm
+# with derivatives (add/mul/div/sqrt = 1, exp counted separately):
+# G2 23 per pair-member + 14 per pair (cutoff function), narrow G3 60 per
+# triplet + 57 per triplet-member, wide G9 45 per pair + 50 per pair-member.
+FLOPS_PER = {"radial_terms": 23, "radial_pairs": 14, "narrow_triplets": 60, "narrow_terms": 57,
+             "wide_pairs": 45, "wide_terms": 50}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--boxes", type=int, default=2048)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(boxes, seed):
+    from n2p2_b200 import water
+    return water.water_batch(boxes, seed=seed)
+
+
+class ClockSampler:
+    """nvidia-smi clocks during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            w = [x.strip() for x in line.split(",")]
+            if len(w) < 9:
+                continue
+            try:
+                sm.append(float(w[1]))
+                smax.append(float(w[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, w[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(texts, threads):
+    from oracle import ref
+    sec, energies = ref.time_batch(MODEL, texts, threads, fast=True)
+    return sec, energies
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_sample(structs, threads, target_atoms=None):
+    """A bounded sample of the workload for the CPU reference: whole
+    structures, round-robin over the batch, about 12 s of work on `threads`."""
+    if target_atoms is None:
+        target_atoms = int(1700 * 12 * max(1, threads) * 0.7)
+    out, n = [], 0
+    stride = max(1, len(structs) // 256)
+    for k in range(0, len(structs), stride):
+        out.append(structs[k])
+        n += structs[k].numAtoms
+        if n >= target_atoms:
+            break
+    return out, n
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    structs = workload(args.boxes, args.seed)
+    threads = host_threads()
+    sample, natoms = cpu_sample(structs, threads)
+    texts = [s.to_text() for s in sample]
+    for _ in range(args.warmup):
+        cpu_reference(texts[: max(1, len(texts) // 8)], threads)
+    secs = []
+    for _ in range(args.steps):
+        sec, _ = cpu_reference(texts, threads)
+        secs.append(sec)
+    t = float(np.mean(secs))
+    v = natoms / t
+    total_atoms = sum(s.numAtoms for s in structs)
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "atoms/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_atoms / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded water boxes)",
+            "config": {"workload": "2048 water boxes, 32-512 molecules log-uniform (%d atoms), water40 model, FP64"
+                       % total_atoms, "boxes": args.boxes, "atoms": total_atoms},
+            "cpu_baseline": {"value": v, "unit": "atoms/s", "cores": threads, "kind": "reference",
+                             "sample": "%d of %d structures (%d atoms) per step, structure-parallel, "
+                                       "reference libnnp (-O3 -march=x86-64-v3)" % (len(sample), len(structs), natoms)},
+            "e2e": {"value": v, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    from n2p2_b200 import Mode
+    from n2p2_b200 import _lib
+    rank, world, local = dist_env()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    structs = workload(args.boxes, args.seed + 7919 * rank)
+    natoms = sum(s.numAtoms for s in structs)
+    pos = np.ascontiguousarray(np.concatenate([s.positions for s in structs]))
+
+    mode = Mode(local)
+    mode.setupFromDirectory(MODEL)
+    mode.setPrecision("fp64")
+    batch = mode.batch(structs)
+    batch.setPositions(pos)
+    batch.evaluate(forces=True)     # establishes neighbour capacity (direct launches)
+    batch.synchronize()
+    stream = torch.cuda.ExternalStream(batch.stream(), device=torch.device("cuda", local))
+
+    def timed(steps, warmup):
+        for _ in range(warmup):
+            batch.evaluate(forces=True)
+        batch.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            batch.evaluate(forces=True)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = timed(args.steps, args.warmup)
+    clk = clocks.stop()
+    E64 = batch.energies()
+    F64 = batch.forces()
+    launches = batch.launchCount() * args.steps
+
+    # end to end through the C ABI with pinned host buffers
+    nbytes_pos = pos.nbytes
+    hp = ctypes_pinned(nbytes_pos)
+    he = ctypes_pinned(8 * len(structs))
+    hf = ctypes_pinned(nbytes_pos)
+    np.frombuffer(hp[1], dtype=np.float64)[:] = pos.ravel()
+    for _ in range(2):
+        batch.evaluateHost(np.frombuffer(hp[1], dtype=np.float64), np.frombuffer(he[1], dtype=np.float64),
+                           np.frombuffer(hf[1], dtype=np.float64))
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch.evaluateHost(np.frombuffer(hp[1], dtype=np.float64), np.frombuffer(he[1], dtype=np.float64),
+                           np.frombuffer(hf[1], dtype=np.float64))
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # stage profile and algorithmic work (rank-local, one direct evaluation)
+    stages = batch.profileStages(forces=True)
+    work = batch.countWork()
+    fp64_peak = fp32_peak = None
+    d64, d32 = ctypes_double(), ctypes_double()
+    if mode._lib.n2p2_device_fma_peak(local, d64.ref, d32.ref) == 0:
+        fp64_peak, fp32_peak = d64.value, d32.value
+
+    # mixed-precision form on the same batch
+    mixed = None
+    if not args.no_mixed:
+        mode.setPrecision("mixed")
+        batch.evaluate(forces=True)
+        batch.synchronize()
+        ms_mixed = timed(args.steps, args.warmup)
+        Em, Fm = batch.energies(), batch.forces()
+        mode.setPrecision("fp64")
+        atoms_per = np.array([s.numAtoms for s in structs])
+        de = np.abs(Em - E64) / atoms_per * HA_TO_MEV
+        df = np.abs(Fm - F64) * HA_BOHR_TO_MEV_A
+        mixed = {"value": world * natoms / (ms_mixed / 1000.0), "unit": "atoms/s", "ms_per_step": ms_mixed,
+                 "speedup_vs_fp64": ms / ms_mixed,
+                 "err_vs_fp64_gpu": {"energy_meV_per_atom_max": float(de.max()),
+                                     "force_meV_per_A_max": float(df.max()),
+                                     "force_meV_per_A_rms": float(np.sqrt((df ** 2).mean()))}}
+
+    sf_ms = sum(t for n, t in stages if n in ("sf_values", "sf_forces"))
+    sf_flops = sum(work[k] * f for k, f in FLOPS_PER.items())
+    roofline = None
+    if fp64_peak and sf_ms > 0:
+        achieved = sf_flops / (sf_ms * 1e-3) / 1e12
+        roofline = {"bound": "fp64", "kernel": "kSFValues + kSFForces (symmetry functions, values + derivatives)",
+                    "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                    "peak_source": "measured FP64 FMA throughput of this GPU (n2p2_device_fma_peak)",
+                    "algorithmic_flops_per_step": sf_flops, "traffic": None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            threads = host_threads()
+            sample, nsample = cpu_sample(structs, threads)
+            sec, e_ref = cpu_reference([s.to_text() for s in sample], threads)
+            idx = [structs.index(s) for s in sample]
+            rel = float(np.max(np.abs(E64[idx] - e_ref) / np.abs(e_ref)))
+            cpu = {"value": nsample / sec, "unit": "atoms/s", "cores": threads, "kind": "reference",
+                   "sample": "%d of %d structures (%d atoms), structure-parallel on %d host threads, reference "
+                             "libnnp (-O3 -march=x86-64-v3)" % (len(sample), len(structs), nsample, threads),
+                   "fp64_energy_max_rel_err_vs_gpu": rel}
+        except Exception as exc:  # the timed GPU numbers stand without it
+            cpu = {"value": None, "unit": "atoms/s", "cores": host_threads(), "kind": "reference",
+                   "sample": "failed: %s" % exc}
+
+    value = world * natoms / (ms / 1000.0)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water boxes)",
+                "config": {"workload": "2048 water boxes, 32-512 molecules log-uniform (%d atoms per GPU), "
+                                       "water40 model (40 SFs/element, 40-25-25-1 softplus), plain FP64, "
+                                       "one CUDA-graph launch per step" % natoms,
+                           "boxes": args.boxes, "atoms_per_gpu": natoms,
+                           "neighbor_entries_per_gpu": work["entries"],
+                           "l2": "inputs larger than L2 (neighbour data %.1f GB per step)" % (
+                               work["entries"] * 40 / 1e9),
+                           "parallelism": "dp%d (independent structures per GPU)" % world},
+                "e2e": {"value": world * natoms / (e2e_ms / 1000.0), "unit": "atoms/s", "ms_per_step": e2e_ms,
+                        "h2d_bytes_per_step": nbytes_pos, "d2h_bytes_per_step": nbytes_pos + 8 * len(structs)},
+                "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+                "mixed": mixed, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
+                "fp32_fma_peak_tflops": fp32_peak}
+        print(json.dumps(line), flush=True)
+    mode.close()
+    for h in (hp, he, hf):
+        mode._lib.n2p2_host_free(h[0])
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+class ctypes_double:
+    def __init__(self):
+        import ctypes
+        self._v = ctypes.c_double()
+        self.ref = ctypes.byref(self._v)
+
+    @property
+    def value(self):
+        return self._v.value
+
+
+def ctypes_pinned(nbytes):
+    import ctypes
+    from n2p2_b200 import _lib
+    lib = _lib.load()
+    p = ctypes.c_void_p()
+    _lib.check(lib.n2p2_host_alloc(ctypes.byref(p), nbytes))
+    buf = (ctypes.c_char * nbytes).from_address(p.value)
+    return p, buf
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

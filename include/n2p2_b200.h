@@ -191,6 +191,27 @@ n2p2_status n2p2_batch_get_extrapolation_warnings(n2p2_batch* batch, int64_t* to
 /* Kernel launches issued by one evaluation with the last flags. */
 n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches);
 
+/* ---- instrumentation (no counterpart in the reference) ------------------- */
+
+/* The CUDA stream (cudaStream_t) the batch's kernels run on, for event timing. */
+n2p2_status n2p2_batch_get_stream(n2p2_batch* batch, void** stream);
+
+/* One direct (non-graph) evaluation with CUDA events between the stages.
+ * Writes up to `capacity` stage names (32 bytes each, NUL-terminated) and
+ * their durations in milliseconds; *count receives the number of stages. */
+n2p2_status n2p2_batch_profile_stages(n2p2_batch* batch, int flags, int capacity, char* names, double* ms,
+                                      int* count);
+
+/* Algorithmic work of the batch's current neighbour lists, 10 counters:
+ * entries, radial pair-members, radial pairs, narrow triplets, narrow
+ * triplet-members, wide pairs, wide pair-members, G values, atoms,
+ * derivative rows. */
+n2p2_status n2p2_batch_count_work(n2p2_batch* batch, int64_t* counts);
+
+/* Measured fused-multiply-add throughput of the device (TFLOP/s), the
+ * compute roofline of the FP64 and FP32 symmetry-function kernels. */
+n2p2_status n2p2_device_fma_peak(int device, double* fp64Tflops, double* fp32Tflops);
+
 /* Pinned (page-locked) host memory for fast transfers. */
 n2p2_status n2p2_host_alloc(void** ptr, size_t bytes);
 n2p2_status n2p2_host_free(void* ptr);

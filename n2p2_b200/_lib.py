@@ -71,6 +71,10 @@ SIGNATURES = {
     "n2p2_batch_get_internal_positions": (_i, [_vp, _P(_d)]),
     "n2p2_batch_get_extrapolation_warnings": (_i, [_vp, _P(_i64), _P(ctypes.c_int32)]),
     "n2p2_batch_get_launch_count": (_i, [_vp, _P(_i)]),
+    "n2p2_batch_get_stream": (_i, [_vp, _P(_vp)]),
+    "n2p2_batch_profile_stages": (_i, [_vp, _i, _i, _cp, _P(_d), _P(_i)]),
+    "n2p2_batch_count_work": (_i, [_vp, _P(_i64)]),
+    "n2p2_device_fma_peak": (_i, [_i, _P(_d), _P(_d)]),
     "n2p2_host_alloc": (_i, [_P(_vp), ctypes.c_size_t]),
     "n2p2_host_free": (_i, [_vp]),
 }

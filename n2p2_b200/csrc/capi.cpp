@@ -508,6 +508,57 @@ n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches)
     return N2P2_OK;
 }
 
+n2p2_status n2p2_batch_get_stream(n2p2_batch* batch, void** stream)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(stream);
+    *stream = (void*)batch->batch->stream();
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_batch_profile_stages(n2p2_batch* batch, int flags, int capacity, char* names, double* ms,
+                                      int* count)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(count);
+    return guard([&] {
+        setDevice(batch->mode);
+        auto st = batch->batch->profileStages(flags, batch->mode->precision, batch->mode->checkExtrapolation ? 1 : 0);
+        *count = (int)st.size();
+        for (int k = 0; k < (int)st.size() && k < capacity; ++k)
+        {
+            if (names)
+            {
+                std::memset(names + 32 * k, 0, 32);
+                std::strncpy(names + 32 * k, st[k].first.c_str(), 31);
+            }
+            if (ms) ms[k] = st[k].second;
+        }
+    });
+}
+
+n2p2_status n2p2_batch_count_work(n2p2_batch* batch, int64_t* counts)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(counts);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->countWork(counts);
+    });
+}
+
+n2p2_status n2p2_device_fma_peak(int device, double* fp64Tflops, double* fp32Tflops)
+{
+    return guard([&] {
+        cudaCheck(cudaSetDevice(device), "cudaSetDevice");
+        cudaDeviceProp p{};
+        cudaCheck(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
+        if (fp64Tflops) *fp64Tflops = measureFmaPeak(1, p.multiProcessorCount);
+        if (fp32Tflops) *fp32Tflops = measureFmaPeak(0, p.multiProcessorCount);
+        cudaCheck(cudaGetLastError(), "fma probe");
+    });
+}
+
 n2p2_status n2p2_host_alloc(void** ptr, size_t bytes)
 {
     N2P2_REQUIRE(ptr);

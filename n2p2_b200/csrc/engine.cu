@@ -513,55 +513,104 @@ void Batch::setPositionsDevice(const double* r)
 }
 
 // The kernel sequence of one evaluation (Mode::evaluateNNP, Mode.cpp:2029-2077).
-void Batch::record(int flags, int precision, int checkExtrapolation)
+void Batch::record(int flags, int precision, int checkExtrapolation, std::vector<Mark>* marks)
 {
     DevModel const& m = dmodel_.view;
     const bool forces = (flags & EVAL_FORCES) != 0;
     const bool stored = (flags & EVAL_STORE_DGDR) != 0;
     int launches = 0;
+    auto mark = [&](char const* name) {
+        if (!marks) return;
+        Mark mk{name, nullptr};
+        cudaCheck(cudaEventCreate(&mk.event), "cudaEventCreate");
+        cudaCheck(cudaEventRecord(mk.event, stream_), "cudaEventRecord");
+        marks->push_back(mk);
+    };
+    mark("start");
     cudaCheck(cudaMemsetAsync(v_.status, 0, sizeof(DevStatus), stream_), "status reset");
     launchPreparePositions(v_, rin_, remap_, model_.normalize ? 1 : 0, model_.convLength, stream_);
     launches += 1;
+    mark("prepare_positions");
     launchNeighborBuild(v_, model_.maxCutoffRadius * model_.maxCutoffRadius, stream_);
     launches += 3 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1;
+    mark("neighbor_list");
     launchCutoffValues(m, v_, sms_, stream_);
     launches += 1;
+    mark("cutoff_values");
     if (stored)
     {
         launchSFDerivatives(m, v_, sms_, stream_);
         launches += 2;
+        mark("sf_derivatives");
     }
     else
     {
         launchSFValues(m, v_, precision, sms_, stream_);
         launches += 2;
+        mark("sf_values");
     }
     if (checkExtrapolation)
     {
         launchExtrapolationCheck(m, v_, sms_, stream_);
         launches += 1;
+        mark("extrapolation_check");
     }
     launchNetworkFP64(m, v_, forces ? 1 : 0, sms_, stream_);
     launches += 1;
+    mark("network");
     launchEnergySum(v_, stream_);
     launches += 1;
+    mark("energy_sum");
     if (forces)
     {
         if (stored)
         {
             launchContractStored(m, v_, sms_, stream_);
             launches += 1;
+            mark("contract_stored");
         }
         else
         {
             launchSFForces(m, v_, precision, sms_, stream_);
             launches += 2;
+            mark("sf_forces");
         }
         launchGatherForces(v_, sms_, stream_);
         launches += 1;
+        mark("gather_forces");
     }
     cudaCheck(cudaGetLastError(), "kernel launch");
     launches_ = launches;
+}
+
+std::vector<std::pair<std::string, double>> Batch::profileStages(int flags, int precision, int checkExtrapolation)
+{
+    if (!capacityVerified_) evaluate(flags, precision, checkExtrapolation);
+    std::vector<Mark> marks;
+    record(flags, precision, checkExtrapolation, &marks);
+    synchronize();
+    std::vector<std::pair<std::string, double>> out;
+    for (size_t k = 1; k < marks.size(); ++k)
+    {
+        float ms = 0.f;
+        cudaCheck(cudaEventElapsedTime(&ms, marks[k - 1].event, marks[k].event), "cudaEventElapsedTime");
+        out.emplace_back(marks[k].name, (double)ms);
+    }
+    for (auto& mk : marks) cudaEventDestroy(mk.event);
+    return out;
+}
+
+void Batch::countWork(int64_t* counts)
+{
+    unsigned long long* d = nullptr;
+    cudaCheck(cudaMalloc(&d, sizeof(unsigned long long) * 10), "cudaMalloc");
+    cudaCheck(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * 10, stream_), "memset");
+    launchCountWork(dmodel_.view, v_, d, sms_, stream_);
+    unsigned long long h[10];
+    cudaCheck(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, stream_), "D2H");
+    synchronize();
+    cudaFree(d);
+    for (int k = 0; k < 10; ++k) counts[k] = (int64_t)h[k];
 }
 
 void Batch::evaluate(int flags, int precision, int checkExtrapolation)

@@ -80,6 +80,13 @@ public:
     cudaStream_t stream() const { return stream_; }
     int launchesPerEvaluate() const { return launches_; }
 
+    // One direct evaluation with CUDA events between the stages; returns
+    // (stage name, milliseconds) in launch order.
+    std::vector<std::pair<std::string, double>> profileStages(int flags, int precision, int checkExtrapolation);
+    // Algorithmic work counters of the current neighbour lists (10 values,
+    // see kCountWork).
+    void countWork(int64_t* counts);
+
     // Internal-unit results for inspection (neighbour lists, G, dEdG, dGdr).
     void copyNeighbors(int64_t* offsets, int* index, int* image, double* d, double* dr);
     void copyG(double* out);          // [N][numSF of the atom's element], concatenated
@@ -93,7 +100,12 @@ private:
     void allocateAtoms();
     void allocateNeighbors(int64_t capacity);
     void allocateDGdr();
-    void record(int flags, int precision, int checkExtrapolation);
+    struct Mark
+    {
+        std::string name;
+        cudaEvent_t event;
+    };
+    void record(int flags, int precision, int checkExtrapolation, std::vector<Mark>* marks = nullptr);
     void releaseGraph();
     void releaseAll();
 

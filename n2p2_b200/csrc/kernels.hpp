@@ -89,4 +89,8 @@ void launchEnergySum(BatchView const& b, cudaStream_t st);
 void launchGatherForces(BatchView const& b, int sms, cudaStream_t st);
 void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 
+// instrumentation
+void launchCountWork(DevModel const& m, BatchView const& b, unsigned long long* counts, int sms, cudaStream_t st);
+double measureFmaPeak(int fp64, int sms);
+
 } // namespace n2p2b200

@@ -282,6 +282,28 @@ class Batch:
                                                                    per.ctypes.data_as(_P(ctypes.c_int32))))
         return t.value, per
 
+    def stream(self):
+        s = ctypes.c_void_p()
+        _lib.check(self._lib.n2p2_batch_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def profileStages(self, forces=True, storeDGdr=False):
+        flags = (_lib.EVAL_FORCES if forces else 0) | (_lib.EVAL_STORE_DGDR if storeDGdr else 0)
+        cap = 32
+        names = ctypes.create_string_buffer(32 * cap)
+        ms = np.zeros(cap)
+        n = ctypes.c_int()
+        _lib.check(self._lib.n2p2_batch_profile_stages(self._h, flags, cap, names, _dp(ms), ctypes.byref(n)))
+        raw = names.raw
+        return [(raw[32 * k:32 * k + 32].split(b"\0")[0].decode(), float(ms[k])) for k in range(n.value)]
+
+    def countWork(self):
+        c = np.zeros(10, dtype=np.int64)
+        _lib.check(self._lib.n2p2_batch_count_work(self._h, c.ctypes.data_as(_P(ctypes.c_int64))))
+        keys = ["entries", "radial_terms", "radial_pairs", "narrow_triplets", "narrow_terms", "wide_pairs",
+                "wide_terms", "g_values", "atoms", "derivative_rows"]
+        return dict(zip(keys, (int(x) for x in c)))
+
     def launchCount(self):
         n = ctypes.c_int()
         _lib.check(self._lib.n2p2_batch_get_launch_count(self._h, ctypes.byref(n)))

@@ -21,13 +21,14 @@ def box_edge(n_mol):
     return (n_mol / MOLECULE_DENSITY) ** (1.0 / 3.0)
 
 
-def _rotation(rng):
-    q = rng.normal(size=4)
-    q /= np.linalg.norm(q)
-    w, x, y, z = q
-    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
-                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
-                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+def _rotations(q):
+    """Rotation matrices [n,3,3] from unnormalised quaternions [n,4]."""
+    q = q / np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], axis=1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], axis=1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], axis=1)], axis=1)
 
 
 def water_box(n_mol, seed, jitter=0.5, sigma=0.0):
@@ -42,14 +43,14 @@ def water_box(n_mol, seed, jitter=0.5, sigma=0.0):
     half = math.radians(HOH_ANGLE) / 2.0
     h1 = OH_BOND * np.array([math.sin(half), 0.0, math.cos(half)])
     h2 = OH_BOND * np.array([-math.sin(half), 0.0, math.cos(half)])
-    pos = np.zeros((3 * n_mol, 3))
-    for k, s in enumerate(sites):
-        ix, iy, iz = s // (m * m), (s // m) % m, s % m
-        o = (np.array([ix, iy, iz]) + 0.5) * a + rng.uniform(-jitter, jitter, 3)
-        R = _rotation(rng)
-        pos[3 * k] = o
-        pos[3 * k + 1] = o + R @ h1
-        pos[3 * k + 2] = o + R @ h2
+    grid = np.stack([sites // (m * m), (sites // m) % m, sites % m], axis=1).astype(np.float64)
+    o = (grid + 0.5) * a + rng.uniform(-jitter, jitter, (n_mol, 3))
+    R = _rotations(rng.normal(size=(n_mol, 4)))
+    pos = np.empty((n_mol, 3, 3))
+    pos[:, 0] = o
+    pos[:, 1] = o + R @ h1
+    pos[:, 2] = o + R @ h2
+    pos = pos.reshape(-1, 3)
     if sigma > 0.0:
         pos += rng.normal(0.0, sigma, pos.shape)
     elements = ["O", "H", "H"] * n_mol

@@ -54,3 +54,52 @@ def max_rel(a, b):
     b = np.asarray(b, dtype=np.float64)
     scale = max(np.abs(b).max(), 1e-300)
     return float(np.abs(a - b).max() / scale)
+
+
+def scaling_table(model_dir):
+    """Per-SF (Smin, scalingFactor, Gmean/Gmin offset) to unscale G, in the
+    order of the scaling file (elements by atomic number, SFs sorted)."""
+    from oracle.port import PortModel
+    pm = PortModel(model_dir)
+    a = pm.arrays
+    return pm, a
+
+
+def unscaled(model_dir, structure, G):
+    """Raw G (SymFnc::unscale, SymFnc.cpp:197-223) of a concatenated G array."""
+    pm, a = scaling_table(model_dir)
+    out = np.empty_like(G)
+    k = 0
+    for sym in structure.elements:
+        e = pm.index[sym]
+        b0, b1 = a["sfBegin"][e], a["sfBegin"][e + 1]
+        for s in range(b0, b1):
+            t = a["scalingType"][s]
+            v = G[k]
+            if t == 0:
+                u = v
+            elif t == 1:
+                u = (v - a["Smin"][s]) / a["scalingFactor"][s] + a["Gmin"][s]
+            elif t == 2:
+                u = v + a["Gmean"][s]
+            else:
+                u = (v - a["Smin"][s]) / a["scalingFactor"][s] + a["Gmean"][s]
+            out[k] = u
+            k += 1
+    return out
+
+
+def reference_noise(model_dir, structure):
+    """Relative force and energy spread between the reference built with FMA
+    contraction (-O3, x86-64-v3) and without (-O2, -ffp-contract=off): the
+    floating-point noise floor of the reference on this input."""
+    if not oref.available(fast=True):
+        return 0.0, 0.0
+    a = reference_snapshot(model_dir, structure)
+    p = oref.RefPrediction(model_dir, fast=True)
+    try:
+        p.predict(structure.to_text())
+        b = p.arrays()
+    finally:
+        p.close()
+    return abs(a["energy"] - b["energy"]) / abs(a["energy"]), max_rel(b["forces"], a["forces"])

@@ -1,9 +1,15 @@
 """GPU parity of the FP64 path against the reference library (oracle/_ref).
 
-Tolerances: neighbour lists and remapped positions bit-exact; G within
-1e-12 (relative to the largest |G| of the structure); dE/dG, energies and
-forces within 1e-10 relative (forces relative to the largest force
-component of the structure), the plain-FP64 target of the path.
+Tolerances: neighbour lists and remapped positions bit-exact; unscaled G
+within 1e-12 (relative to the largest |G| of the structure); energies and
+forces within 1e-10 relative (forces relative to the largest force component
+of the structure), the plain-FP64 target of the path.
+
+The synthetic water model of the benchmark is ill-conditioned: its scaling
+statistics come from one box of rigid molecules, so a few symmetry functions
+have a min-max range of ~1e-8 and scaling factors up to 1e16.  There the
+reference disagrees with itself (FMA vs no-FMA build) by several 1e-10 in the
+forces, so water-model forces are held to max(1e-10, 2 x that spread).
 """
 import json
 import os
@@ -22,7 +28,7 @@ TOL_F = 1e-10
 TOL_G = 1e-12
 
 
-def _compare_structure(b, a0, a1, snap, structure_index, energies, forces, check_g=True):
+def _compare_structure(b, a0, a1, snap, structure_index, energies, forces, tol_f=TOL_F):
     nb = H.split_neighbors(b.neighbors(), a0, a1)
     # neighbour lists: same count, order, index and bit-identical d, dr
     assert np.array_equal(nb["offset"], snap["nbr_offset"])
@@ -32,7 +38,7 @@ def _compare_structure(b, a0, a1, snap, structure_index, energies, forces, check
     e_ref = snap["energy"]
     assert abs(energies[structure_index] - e_ref) <= TOL_E * abs(e_ref)
     f = forces[a0:a1]
-    assert H.max_rel(f, snap["forces"]) <= TOL_F
+    assert H.max_rel(f, snap["forces"]) <= tol_f
 
 
 @pytest.mark.parametrize("name", ["H2O_RPBE-D3", "Cu2S_PBE"])
@@ -55,8 +61,13 @@ def test_reference_examples_golden(name):
     assert np.array_equal(pos.view(np.int64), snap["positions"].view(np.int64))
     _compare_structure(b, 0, s.numAtoms, snap, 0, b.energies(), f)
     G = b.symmetryFunctions()
-    assert H.max_rel(G, snap["G"]) <= TOL_G
+    assert H.max_rel(H.unscaled(d, s, G), H.unscaled(d, s, snap["G"])) <= TOL_G
     assert H.max_rel(b.dEdG(), snap["dEdG"]) <= TOL_E
+
+
+def _water_tol_f(s):
+    _, noise_f = H.reference_noise(H.WATER40, s)
+    return max(TOL_F, 2.0 * noise_f)
 
 
 def test_water_box64_fp64():
@@ -64,8 +75,9 @@ def test_water_box64_fp64():
     m = H.gpu_mode(H.WATER40)
     b = H.gpu_batch(m, [s])
     snap = H.reference_snapshot(H.WATER40, s)
-    _compare_structure(b, 0, s.numAtoms, snap, 0, b.energies(), b.forces())
-    assert H.max_rel(b.symmetryFunctions(), snap["G"]) <= TOL_G
+    _compare_structure(b, 0, s.numAtoms, snap, 0, b.energies(), b.forces(), tol_f=_water_tol_f(s))
+    G = b.symmetryFunctions()
+    assert H.max_rel(H.unscaled(H.WATER40, s, G), H.unscaled(H.WATER40, s, snap["G"])) <= TOL_G
     assert H.max_rel(b.atomicEnergies(), snap["atomic_energy"]) <= TOL_E
     gold = json.load(open(os.path.join(H.GOLDEN, "water40_box64.json")))
     assert abs(b.energies()[0] - gold["energy"]) <= TOL_E * abs(gold["energy"])
@@ -80,7 +92,7 @@ def test_water_batch_uneven_fp64():
     a0 = 0
     for k, s in enumerate(boxes):
         snap = H.reference_snapshot(H.WATER40, s)
-        _compare_structure(b, a0, a0 + s.numAtoms, snap, k, E, F)
+        _compare_structure(b, a0, a0 + s.numAtoms, snap, k, E, F, tol_f=_water_tol_f(s))
         a0 += s.numAtoms
 
 
@@ -94,7 +106,7 @@ def test_stored_dgdr_matches_reference():
     assert H.max_rel(selfd, snap["dGdr_self"]) <= 1e-11
     assert H.max_rel(nbr, snap["dGdr_nbr"]) <= 1e-11
     assert abs(b.energies()[0] - snap["energy"]) <= TOL_E * abs(snap["energy"])
-    assert H.max_rel(b.forces(), snap["forces"]) <= TOL_F
+    assert H.max_rel(b.forces(), snap["forces"]) <= _water_tol_f(s)
 
 
 def test_graph_replay_is_deterministic():
@@ -108,3 +120,20 @@ def test_graph_replay_is_deterministic():
     e2, f2 = b.energies(), b.forces()
     assert np.array_equal(e1.view(np.int64), e2.view(np.int64))
     assert np.array_equal(f1.view(np.int64), f2.view(np.int64))
+
+
+def test_mixed_precision_error_budget():
+    """FP32 descriptors (FP64 cutoff, scaling, sums) stay within 1 meV/atom
+    and 30 meV/A of the FP64 reference."""
+    boxes = water.water_batch(4, seed=5, n_min=32, n_max=128)
+    m = H.gpu_mode(H.WATER40, precision="mixed")
+    b = H.gpu_batch(m, boxes)
+    E, F = b.energies(), b.forces()
+    a0 = 0
+    for k, s in enumerate(boxes):
+        snap = H.reference_snapshot(H.WATER40, s)
+        de = abs(E[k] - snap["energy"]) / s.numAtoms * H.HA_TO_MEV
+        df = np.abs(F[a0:a0 + s.numAtoms] - snap["forces"]).max() * H.HA_PER_BOHR_TO_MEV_PER_A
+        assert de <= 1.0, de
+        assert df <= 30.0, df
+        a0 += s.numAtoms
