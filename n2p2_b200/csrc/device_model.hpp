@@ -35,6 +35,8 @@ struct DevMember
     int    zetaInt;
     int    useIntPow;
     int    calcExp;        // recompute the Gaussian for this member
+    int    expBase;        // Gaussian exp(-eta r^2) = base^expPow; -1: evaluate directly
+    int    expPow;
 };
 
 struct DevGroup
@@ -44,9 +46,14 @@ struct DevGroup
     int    cutoffType;
     int    cutoffSlot;     // which precomputed f_c/df_c set this group uses
     int    memberBegin, memberCount;
-    int    pad_;
+    int    numBases;       // distinct exp(-eta r^2) bases of the group (<= kMaxBases)
+    int    fast;           // all members rs == 0 and planned on staged bases
     double rc, rc2;
+    double baseEta[4];
 };
+
+constexpr int kMaxBases = 4;        // exponential bases per group
+constexpr int kMaxStagedBases = 2;  // bases staged per neighbour for angular groups
 
 // Cutoff function parameters (CutoffFunction::setCutoffRadius/Parameter,
 // CutoffFunction.cpp:95-112).

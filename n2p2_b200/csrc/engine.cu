@@ -196,6 +196,44 @@ void DeviceModel::upload(Model const& m)
             dg.cutoffSlot = (int)(it - slotRc.begin());
             dg.memberBegin = (int)members.size();
             dg.memberCount = (int)g.members.size();
+            // Gaussian plan: exp(-eta r^2) of a member is an integer power
+            // (<= 16) of an earlier base when eta/eta_base is integral, which
+            // turns the per-triplet Gaussians into products of per-neighbour
+            // factors and one exponential of r_jk^2 per base.
+            std::vector<double> bases;
+            std::vector<int> planBase(g.members.size(), -1), planPow(g.members.size(), 1);
+            bool allRs0 = true;
+            for (std::size_t q = 0; q < g.members.size(); ++q)
+            {
+                SymFunc const& s = el.sf[g.members[q]];
+                if (s.rs != 0.0)
+                {
+                    allRs0 = false;
+                    continue;
+                }
+                for (std::size_t b = 0; b < bases.size(); ++b)
+                {
+                    double ratio = s.eta / bases[b];
+                    double k = std::round(ratio);
+                    if (k >= 1.0 && k <= 16.0 && std::fabs(ratio - k) <= 1e-9 * ratio)
+                    {
+                        planBase[q] = (int)b;
+                        planPow[q] = (int)k;
+                        break;
+                    }
+                }
+                if (planBase[q] < 0 && (int)bases.size() < kMaxBases)
+                {
+                    bases.push_back(s.eta);
+                    planBase[q] = (int)bases.size() - 1;
+                    planPow[q] = 1;
+                }
+            }
+            dg.numBases = (int)bases.size();
+            for (std::size_t b = 0; b < bases.size(); ++b) dg.baseEta[b] = bases[b];
+            bool planned = true;
+            for (int pb : planBase) planned = planned && pb >= 0;
+            dg.fast = (allRs0 && planned && (g.type == 2 || dg.numBases <= kMaxStagedBases)) ? 1 : 0;
             for (std::size_t q = 0; q < g.members.size(); ++q)
             {
                 SymFunc const& s = el.sf[g.members[q]];
@@ -208,6 +246,8 @@ void DeviceModel::upload(Model const& m)
                 dm.zetaInt = s.zetaInt;
                 dm.useIntPow = s.useIntegerPow ? 1 : 0;
                 dm.calcExp = g.calculateExp[q] ? 1 : 0;
+                dm.expBase = planBase[q];
+                dm.expPow = planPow[q];
                 dm.rowE1 = s.indexPerElement[s.e1];
                 dm.rowE2 = (s.type == 2) ? dm.rowE1 : s.indexPerElement[s.e2];
                 if (s.type == 2)
