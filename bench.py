@@ -175,15 +175,15 @@ def run_reference(args):
 def run_ours(args):
     import torch
     from n2p2_b200 import Mode
-    from n2p2_b200 import _lib
-    rank, world, local = dist_env()
+    from n2p2_b200 import ranks
+    rank, world, local = ranks.rank_env()
     dist = None
     if world > 1:
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
-    structs = workload(args.boxes, args.seed + 7919 * rank)
+    structs = workload(args.boxes, ranks.rank_seed(args.seed, rank))
     natoms = sum(s.numAtoms for s in structs)
     pos = np.ascontiguousarray(np.concatenate([s.positions for s in structs]))
 
@@ -212,11 +212,7 @@ def run_ours(args):
         e1.synchronize()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        if dist is not None:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return ranks.max_over_ranks(ms, device="cuda")
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -241,11 +237,7 @@ def run_ours(args):
     for _ in range(args.steps):
         batch.evaluateHost(np.frombuffer(hp[1], dtype=np.float64), np.frombuffer(he[1], dtype=np.float64),
                            np.frombuffer(hf[1], dtype=np.float64))
-    e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = ranks.max_over_ranks((time.perf_counter() - t0) * 1000.0 / args.steps, device="cuda")
 
     # stage profile and algorithmic work (rank-local, one direct evaluation)
     stages = batch.profileStages(forces=True)

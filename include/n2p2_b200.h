@@ -63,7 +63,9 @@ const char* n2p2_version(void);
 
 /* ---- model set-up: nnp::Mode ------------------------------------------------ */
 
-/* new nnp::Mode bound to CUDA device `device` (Mode::Mode, Mode.cpp:43-54). */
+/* new nnp::Mode bound to CUDA device `device` (Mode::Mode, Mode.cpp:43-54).
+ * The device is first used when a batch is created; the set-up functions
+ * work without a GPU. */
 n2p2_status n2p2_mode_create(n2p2_mode** mode, int device);
 n2p2_status n2p2_mode_destroy(n2p2_mode* mode);
 
@@ -115,6 +117,13 @@ n2p2_status n2p2_mode_get_element_index(n2p2_mode* mode, const char* symbol, int
 
 /* Element::numSymmetryFunctions (Element.h:161). */
 n2p2_status n2p2_mode_get_num_symmetry_functions(n2p2_mode* mode, int element, int* count);
+
+/* Element::getSymmetryFunction(index) (Element.h:176): parameters of the
+ * index-th symmetry function of `element` in the reference's sorted order:
+ * type, e1, e2 and params = {eta, rs, lambda, zeta, rc, scalingFactor}
+ * (internal length units). */
+n2p2_status n2p2_mode_get_symmetry_function(n2p2_mode* mode, int element, int index, int* type, int* e1, int* e2,
+                                            double* params);
 
 /* Element::getSymmetryFunctionNumTable()[neighborElement] (Element.h:188):
  * dG/dr rows stored for a neighbour of element `neighborElement` around a

@@ -52,6 +52,7 @@ SIGNATURES = {
     "n2p2_mode_get_element_index": (_i, [_vp, _cp, _P(_i)]),
     "n2p2_mode_get_num_symmetry_functions": (_i, [_vp, _i, _P(_i)]),
     "n2p2_mode_get_num_derivative_rows": (_i, [_vp, _i, _i, _P(_i)]),
+    "n2p2_mode_get_symmetry_function": (_i, [_vp, _i, _i, _P(_i), _P(_i), _P(_i), _P(_d)]),
     "n2p2_batch_create": (_i, [_vp, _P(_vp)]),
     "n2p2_batch_destroy": (_i, [_vp]),
     "n2p2_batch_set_structures": (_i, [_vp, _i64, _P(_i64), _P(ctypes.c_int32), _P(_d), _P(ctypes.c_int32), _i]),

@@ -79,13 +79,26 @@ n2p2_status guard(F&& f)
     }
 }
 
-void setDevice(n2p2_mode* m) { cudaCheck(cudaSetDevice(m->device), "cudaSetDevice"); }
+// The device is touched only when the first batch is created, so the
+// set-up half of the API (settings, symmetry functions, scaling, weights)
+// also works on a host without a GPU.
+void setDevice(n2p2_mode* m)
+{
+    cudaCheck(cudaSetDevice(m->device), "cudaSetDevice");
+    if (!m->stream)
+    {
+        cudaDeviceProp p{};
+        cudaCheck(cudaGetDeviceProperties(&p, m->device), "cudaGetDeviceProperties");
+        m->sms = p.multiProcessorCount;
+        cudaCheck(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    }
+}
 
 void ensureUploaded(n2p2_mode* m)
 {
+    setDevice(m);
     if (!m->uploaded)
     {
-        setDevice(m);
         m->dmodel.upload(m->model);
         m->uploaded = true;
     }
@@ -133,11 +146,6 @@ n2p2_status n2p2_mode_create(n2p2_mode** mode, int device)
     return guard([&] {
         auto m = std::make_unique<n2p2_mode>();
         m->device = device;
-        cudaCheck(cudaSetDevice(device), "cudaSetDevice");
-        cudaDeviceProp p{};
-        cudaCheck(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
-        m->sms = p.multiProcessorCount;
-        cudaCheck(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         *mode = m.release();
     });
 }
@@ -146,8 +154,8 @@ n2p2_status n2p2_mode_destroy(n2p2_mode* mode)
 {
     if (!mode) return N2P2_OK;
     return guard([&] {
-        cudaSetDevice(mode->device);
         cudaStream_t s = mode->stream;
+        if (s) cudaSetDevice(mode->device);
         delete mode;
         if (s) cudaStreamDestroy(s);
     });
@@ -281,6 +289,27 @@ n2p2_status n2p2_mode_get_num_symmetry_functions(n2p2_mode* mode, int element, i
     N2P2_REQUIRE(mode);
     N2P2_REQUIRE(count);
     return guard([&] { *count = (int)mode->model.elements.at(element).sf.size(); });
+}
+
+n2p2_status n2p2_mode_get_symmetry_function(n2p2_mode* mode, int element, int index, int* type, int* e1, int* e2,
+                                            double* params)
+{
+    N2P2_REQUIRE(mode);
+    return guard([&] {
+        SymFunc const& s = mode->model.elements.at(element).sf.at(index);
+        if (type) *type = s.type;
+        if (e1) *e1 = s.e1;
+        if (e2) *e2 = s.e2;
+        if (params)
+        {
+            params[0] = s.eta;
+            params[1] = s.rs;
+            params[2] = s.lambda;
+            params[3] = s.zeta;
+            params[4] = s.rc;
+            params[5] = s.scalingFactor;
+        }
+    });
 }
 
 n2p2_status n2p2_mode_get_num_derivative_rows(n2p2_mode* mode, int element, int neighborElement, int* rows)

@@ -108,6 +108,40 @@ void pbcCopies(double const* box, double rc, int* pbc, double* proj)
 
 } // namespace
 
+void inverseBoxOf(double const* box, double* invbox) { inverseBox(box, invbox); }
+
+void structureGeometry(DevStructInfo& d, double rc)
+{
+    // periodic copies and plane spacings of the (normalised) box
+    double proj[3];
+    pbcCopies(d.box, rc, d.pbc, proj);
+    const int n = d.numAtoms;
+    int64_t cells = 1;
+    for (int a = 0; a < 3; ++a)
+    {
+        // cell width >= rc/2 (plus a margin far above rounding), searched
+        // ceil(rc / width) cells to each side
+        double want = rc * 0.5 * (1.0 + 1e-6);
+        int nc = (int)std::floor(proj[a] / want);
+        nc = std::max(1, std::min(nc, 256));
+        double w = proj[a] / nc;
+        d.nc[a] = nc;
+        d.stencil[a] = (int)std::ceil(rc / w + 1e-9);
+        cells *= nc;
+    }
+    if (cells > 64 * (int64_t)n + 64)
+    {
+        // very sparse structure: coarser grid (search cost bounded by the atom count)
+        for (int a = 0; a < 3; ++a)
+        {
+            int nc = std::max(1, (int)std::floor(proj[a] / (rc * (1.0 + 1e-6))));
+            nc = std::min(nc, 64);
+            d.nc[a] = nc;
+            d.stencil[a] = (int)std::ceil(rc / (proj[a] / nc) + 1e-9);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // DeviceModel
 // ---------------------------------------------------------------------------
@@ -395,31 +429,8 @@ void Batch::setStructures(std::vector<StructureInput> const& s, const int* eleme
                 d.box[q] = model_.normalize ? d.boxPhys[q] * conv : d.boxPhys[q];
                 d.invbox[q] = model_.normalize ? d.invboxPhys[q] / conv : d.invboxPhys[q];
             }
-            double proj[3];
-            pbcCopies(d.box, rc, d.pbc, proj);
-            int64_t cells = 1;
-            for (int a = 0; a < 3; ++a)
-            {
-                double want = rc * 0.5 * (1.0 + 1e-6);
-                int nc = (int)std::floor(proj[a] / want);
-                nc = std::max(1, std::min(nc, 256));
-                double w = proj[a] / nc;
-                d.nc[a] = nc;
-                d.stencil[a] = (int)std::ceil(rc / w + 1e-9);
-                cells *= nc;
-            }
-            if (cells > 64 * (int64_t)n + 64)
-            {
-                // very sparse structure: coarser grid (search cost bounded by the atom count)
-                for (int a = 0; a < 3; ++a)
-                {
-                    int nc = std::max(1, (int)std::floor(proj[a] / (rc * (1.0 + 1e-6))));
-                    nc = std::min(nc, 64);
-                    d.nc[a] = nc;
-                    d.stencil[a] = (int)std::ceil(rc / (proj[a] / nc) + 1e-9);
-                }
-                cells = (int64_t)d.nc[0] * d.nc[1] * d.nc[2];
-            }
+            structureGeometry(d, rc);
+            const int64_t cells = (int64_t)d.nc[0] * d.nc[1] * d.nc[2];
             d.cellBegin = cellTotal;
             cellTotal += (int)cells;
             double vol = std::fabs(d.box[0] * (d.box[4] * d.box[8] - d.box[5] * d.box[7]) -

@@ -70,11 +70,14 @@ struct Members
     int zint[kMaxMembers], base[kMaxMembers], pw[kMaxMembers], flags[kMaxMembers];  // 1 intPow, 2 calcExp
 };
 
+constexpr int kQueue = 64;   // accepted (owner, partner) pairs waiting for a full warp
+
 template <typename T, int CAP>
 struct ValuesSmem
 {
     Stage<T, CAP> st;
     Members<T> mb;
+    int queue[kQueue];
 };
 
 template <typename T, int CAP>
@@ -83,7 +86,128 @@ struct ForcesSmem
     Stage<T, CAP> st;
     Members<T> mb;
     double h[3][CAP];
+    int queue[kQueue];
 };
+
+// Candidate pairs of one angular group, enumerated owner-major in phases:
+//   kind 0  circular: owner a in [0, nO), partner (a + 1 + t) mod nO, t < D
+//   kind 1  half-extra: owner a < nO / 2, partner a + nO / 2 (even nO, G pass)
+//   kind 2  rectangular: owner a in [0, nO), partner t in [0, D) of another block
+struct Phase
+{
+    int kind, O0, nO, P0, D, count;
+};
+
+// Lane-private decoding of candidate p = p0 + lane, advanced by 32 per step
+// without integer division in the loop.
+struct Cursor
+{
+    int a, t;
+    __device__ __forceinline__ void init(Phase const& ph, int lane)
+    {
+        if (ph.kind == 1 || ph.D <= 0)
+        {
+            a = lane;
+            t = 0;
+        }
+        else
+        {
+            a = lane / ph.D;
+            t = lane - a * ph.D;
+        }
+    }
+    __device__ __forceinline__ void advance(Phase const& ph)
+    {
+        if (ph.kind == 1)
+        {
+            a += 32;
+            return;
+        }
+        t += 32;
+        while (t >= ph.D)
+        {
+            t -= ph.D;
+            ++a;
+        }
+    }
+    __device__ __forceinline__ void slots(Phase const& ph, int& so, int& sp) const
+    {
+        so = ph.O0 + a;
+        if (ph.kind == 0)
+        {
+            int b = a + 1 + t;
+            if (b >= ph.nO) b -= ph.nO;
+            sp = ph.O0 + b;
+        }
+        else if (ph.kind == 1) sp = ph.O0 + a + ph.nO / 2;
+        else sp = ph.P0 + t;
+    }
+};
+
+// Test the next 32 candidates of a phase and append the accepted ones, in
+// candidate order, to the warp's queue (qn entries from q[0]).
+template <typename T, int CAP>
+__device__ __forceinline__ void enqueueCandidates(Stage<T, CAP> const& S, Phase const& ph, Cursor& cur, int p0,
+                                                  T rc, T rc2, bool narrow, int* queue, int& qn, int lane)
+{
+    const int p = p0 + lane;
+    bool ok = false;
+    int so = 0, sp = 0;
+    if (p < ph.count)
+    {
+        cur.slots(ph, so, sp);
+        ok = S.r[so] < rc && S.r[sp] < rc;
+        if (ok && narrow)
+        {
+            const T dx = S.x[sp] - S.x[so], dy = S.y[sp] - S.y[so], dz = S.z[sp] - S.z[so];
+            ok = (dx * dx + dy * dy + dz * dz) < rc2;
+        }
+    }
+    const unsigned m = __ballot_sync(kFullMask, ok);
+    if (ok) queue[qn + __popc(m & ((1u << lane) - 1u))] = (so << 16) | sp;
+    qn += __popc(m);
+    cur.advance(ph);
+    __syncwarp();
+}
+
+// Drop the first `used` queue entries, keep the rest in order.
+__device__ __forceinline__ void shiftQueue(int* queue, int& qn, int used, int lane)
+{
+    const int rest = qn - used;
+    int v = (lane < rest) ? queue[used + lane] : 0;
+    __syncwarp();
+    if (lane < rest) queue[lane] = v;
+    qn = rest;
+    __syncwarp();
+}
+
+// Phases of a group: G pass (each unordered pair once) or force pass
+// (ordered pairs, owner-major, both directions of a cross-element group).
+__device__ __forceinline__ int groupPhases(int A0, int nA, int B0, int nB, bool same, bool ordered, Phase* ph)
+{
+    int n = 0;
+    if (same)
+    {
+        if (nA < 2) return 0;
+        if (ordered)
+        {
+            ph[n++] = Phase{0, A0, nA, A0, nA - 1, nA * (nA - 1)};
+        }
+        else
+        {
+            const int hb = (nA - 1) / 2;
+            if (hb > 0) ph[n++] = Phase{0, A0, nA, A0, hb, nA * hb};
+            if ((nA & 1) == 0) ph[n++] = Phase{1, A0, nA, A0, 0, nA / 2};
+        }
+    }
+    else
+    {
+        if (nA == 0 || nB == 0) return 0;
+        ph[n++] = Phase{2, A0, nA, B0, nB, nA * nB};
+        if (ordered) ph[n++] = Phase{2, B0, nB, A0, nA, nA * nB};
+    }
+    return n;
+}
 
 // Neighbours of one atom into the stage, sorted by element (stable).
 template <typename T, int CAP>

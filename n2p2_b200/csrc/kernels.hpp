@@ -65,6 +65,16 @@ struct BatchView
     DevStatus* status = nullptr;
 };
 
+// Cell grid of one structure: periodic copies (Structure::calculatePbcCopies,
+// Structure.cpp:485-516), cells per axis and the search stencil, from
+// d.box, d.numAtoms and the cutoff radius.
+void structureGeometry(DevStructInfo& d, double rc);
+// Structure::calculateInverseBox (Structure.cpp:518-544).
+void inverseBoxOf(double const* box, double* invbox);
+
+// Throws std::runtime_error("CUDA error in ...") on failure.
+void cudaCheck(cudaError_t e, char const* what);
+
 // Raise a kernel's dynamic shared-memory limit once per process.
 void setDynamicSmemOnce(const void* kernel, size_t bytes);
 

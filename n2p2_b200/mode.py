@@ -113,6 +113,14 @@ class Mode:
         _lib.check(self._lib.n2p2_mode_get_num_symmetry_functions(self._h, int(e), ctypes.byref(n)))
         return n.value
 
+    def symmetryFunction(self, e, i):
+        """(type, e1, e2, eta, rs, lambda, zeta, rc, scalingFactor) of SF i of element e."""
+        t, a, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        p = np.zeros(6)
+        _lib.check(self._lib.n2p2_mode_get_symmetry_function(self._h, int(e), int(i), ctypes.byref(t), ctypes.byref(a),
+                                                             ctypes.byref(b), _dp(p)))
+        return (t.value, a.value, b.value, *p.tolist())
+
     def numDerivativeRows(self, e, en):
         n = ctypes.c_int()
         _lib.check(self._lib.n2p2_mode_get_num_derivative_rows(self._h, int(e), int(en), ctypes.byref(n)))

@@ -167,6 +167,12 @@ static void cutoff_fdf(int type, double alpha, double rc, double r, double* fc, 
     *dfc = df * iw;
 }
 
+/* Cutoff function value and derivative (exported for the known-answer test). */
+void oracle_cutoff(int type, double alpha, double rc, double r, double* fc, double* dfc)
+{
+    cutoff_fdf(type, alpha, rc, r, fc, dfc);
+}
+
 /* exponentiation by squaring (the algorithm of utility.cpp:292-316) */
 static double pow_by_squaring(double x, int n)
 {

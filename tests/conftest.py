@@ -18,3 +18,20 @@ def pytest_configure(config):
 @pytest.fixture(scope="session")
 def golden_dir():
     return GOLDEN
+
+
+@pytest.fixture(scope="session", autouse=True)
+def _oracle_built():
+    """Build the CPU oracles if they are missing (the C restatement always,
+    the reference library where the reference sources exist)."""
+    import subprocess
+    out = os.path.join(ROOT, "oracle", "_ref")
+    targets = []
+    if not os.path.exists(os.path.join(out, "libnnpport.so")):
+        targets.append("port")
+    if not os.path.exists(os.path.join(out, "libnnpref.so")) and os.path.isdir("/root/reference/src/libnnp"):
+        targets.append("ref")
+    if targets:
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", *targets], check=False,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    yield
