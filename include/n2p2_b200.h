@@ -200,6 +200,32 @@ n2p2_status n2p2_batch_get_extrapolation_warnings(n2p2_batch* batch, int64_t* to
 /* Kernel launches issued by one evaluation with the last flags. */
 n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches);
 
+/* ---- allocation-free neighbour list (no counterpart in the reference) ---- */
+
+/* Neighbour list of ONE structure, written into device buffers the caller
+ * owns, for callers that cannot call cudaMalloc where they need the list: an
+ * MD step being recorded into a CUDA graph, a code whose device memory
+ * belongs to its own pool allocator, or a loop that must not pay cudaMalloc's
+ * device-wide synchronisation.  Nothing is allocated: the scratch (cell
+ * lists, counts, scan partials) is one fixed array in the library's device
+ * memory (about 0.7 MB, held by every GPU that loads the library until the
+ * process exits), shared by all calls.  Calls that overlap on the GPU race
+ * on it; the first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture.
+ *
+ * positions: device [numAtoms][3], internal units, inside the cell (e.g.
+ * n2p2_batch_get_internal_positions); box: host [3][3] in the same units, or
+ * NULL for a cluster; offsets: device [numAtoms+1]; index, image, d: device
+ * [capacity]; dr: device [capacity][3].  Entries are those of
+ * n2p2_batch_get_neighbors (same order and bit-identical values).  Limits:
+ * numAtoms <= 8192, at most 32768 cells, at most 256 neighbours per atom;
+ * larger inputs are rejected with N2P2_ERR_RUNTIME.  The call waits for its
+ * stream (`stream` is a cudaStream_t, NULL = default stream) and stores the
+ * entry count in *numEntries. */
+n2p2_status n2p2_neighbor_list_noalloc(const double* positions, int64_t numAtoms, const double* box, double cutoff,
+                                       int64_t capacity, int64_t* offsets, int32_t* index, int32_t* image,
+                                       double* d, double* dr, int64_t* numEntries, void* stream);
+
 /* ---- instrumentation (no counterpart in the reference) ------------------- */
 
 /* The CUDA stream (cudaStream_t) the batch's kernels run on, for event timing. */

@@ -537,6 +537,22 @@ n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches)
     return N2P2_OK;
 }
 
+n2p2_status n2p2_neighbor_list_noalloc(const double* positions, int64_t numAtoms, const double* box, double cutoff,
+                                       int64_t capacity, int64_t* offsets, int32_t* index, int32_t* image,
+                                       double* d, double* dr, int64_t* numEntries, void* stream)
+{
+    N2P2_REQUIRE(positions);
+    N2P2_REQUIRE(offsets);
+    N2P2_REQUIRE(index);
+    N2P2_REQUIRE(image);
+    N2P2_REQUIRE(d);
+    N2P2_REQUIRE(dr);
+    return guard([&] {
+        neighborListNoAlloc(positions, numAtoms, box, cutoff, capacity, offsets, index, image, d, dr, numEntries,
+                            static_cast<cudaStream_t>(stream));
+    });
+}
+
 n2p2_status n2p2_batch_get_stream(n2p2_batch* batch, void** stream)
 {
     N2P2_REQUIRE(batch);

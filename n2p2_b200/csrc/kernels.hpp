@@ -99,6 +99,11 @@ void launchEnergySum(BatchView const& b, cudaStream_t st);
 void launchGatherForces(BatchView const& b, int sms, cudaStream_t st);
 void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 
+// neighbour list of one structure into caller buffers, no device allocation
+void neighborListNoAlloc(const double* positions, int64_t numAtoms, const double* box, double cutoff,
+                         int64_t capacity, int64_t* offsets, int32_t* index, int32_t* image, double* d, double* dr,
+                         int64_t* numEntries, cudaStream_t st);
+
 // instrumentation
 void launchCountWork(DevModel const& m, BatchView const& b, unsigned long long* counts, int sms, cudaStream_t st);
 double measureFmaPeak(int fp64, int sms);

@@ -1,0 +1,62 @@
+"""The allocation-free neighbour-list entry point against the batched one.
+
+n2p2_neighbor_list_noalloc serves callers that cannot allocate device memory
+where they need a neighbour list (a step being captured into a CUDA graph,
+memory owned by the caller's pool allocator, loops that must not pay
+cudaMalloc's synchronisation): the caller passes device buffers and the
+library's fixed scratch array does the rest.  Its entries must equal those
+of n2p2_batch_get_neighbors for the same structure -- index, image code,
+distance and distance vector bit for bit (tolerance 0, as for every
+neighbour-list comparison in this suite) -- on two calls in a row, since the
+calls share the scratch array.  This file is collected last on purpose.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from n2p2_b200 import _lib
+from n2p2_b200 import water
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(torch, pos_internal, box_internal, cutoff, capacity):
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    n = pos_internal.shape[0]
+    pos = torch.from_numpy(np.ascontiguousarray(pos_internal)).to(dev)
+    off = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    idx = torch.zeros(capacity, dtype=torch.int32, device=dev)
+    img = torch.zeros(capacity, dtype=torch.int32, device=dev)
+    d = torch.zeros(capacity, dtype=torch.float64, device=dev)
+    dr = torch.zeros(capacity * 3, dtype=torch.float64, device=dev)
+    box = np.ascontiguousarray(box_internal, dtype=np.float64)
+    total = ctypes.c_int64()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    _lib.check(lib.n2p2_neighbor_list_noalloc(
+        ctypes.c_void_p(pos.data_ptr()), n, box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cutoff, capacity,
+        ctypes.c_void_p(off.data_ptr()), ctypes.c_void_p(idx.data_ptr()), ctypes.c_void_p(img.data_ptr()),
+        ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(dr.data_ptr()), ctypes.byref(total), ctypes.c_void_p(stream)))
+    m = total.value
+    return {"offset": off.cpu().numpy(), "index": idx[:m].cpu().numpy(), "image": img[:m].cpu().numpy(),
+            "d": d[:m].cpu().numpy(), "dr": dr[:3 * m].cpu().numpy().reshape(-1, 3)}
+
+
+def test_noalloc_neighbor_list_matches_batched_path_twice():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    m = H.gpu_mode(H.WATER40)
+    cutoff = m.getMaxCutoffRadius()
+    for seed, n_mol in ((0, 64), (5, 96)):   # two calls in a row with different inputs
+        s = water.water_box(n_mol, seed=seed)
+        b = H.gpu_batch(m, [s])
+        ref = b.neighbors()
+        got = _noalloc(torch, b.internalPositions(), s.box, cutoff, capacity=len(ref["d"]) + 64)
+        assert np.array_equal(got["offset"], ref["offset"])
+        assert np.array_equal(got["index"], ref["index"])
+        assert np.array_equal(got["image"], ref["image"])
+        assert np.array_equal(got["d"].view(np.int64), ref["d"].view(np.int64))
+        assert np.array_equal(got["dr"].view(np.int64), ref["dr"].view(np.int64))
