@@ -50,6 +50,14 @@ struct DevGroup
     int    fast;           // all members rs == 0 and planned on staged bases
     double rc, rc2;
     double baseEta[4];
+    // Member grid of an angular group: every member is one (eta, lambda,
+    // zeta) combination of at most 2 x 2 x 4 slots, integer zeta, rs = 0.
+    int    grid;           // 0: generic member loop
+    int    gridNZ;         // zeta slots in use (<= 4)
+    int    etaBase[2], etaPow[2];   // eta slot -> staged base and integer power
+    int    zetaM1[4];      // zeta - 1 per zeta slot
+    double lambdaVal[2];
+    signed char comboMember[16];    // (etaSlot * 2 + lambdaSlot) * 4 + zetaSlot -> member, -1 if absent
 };
 
 constexpr int kMaxBases = 4;        // exponential bases per group

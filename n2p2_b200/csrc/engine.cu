@@ -268,6 +268,53 @@ void DeviceModel::upload(Model const& m)
             bool planned = true;
             for (int pb : planBase) planned = planned && pb >= 0;
             dg.fast = (allRs0 && planned && (g.type == 2 || dg.numBases <= kMaxStagedBases)) ? 1 : 0;
+            // Member grid (angular groups): slots of distinct eta, lambda and
+            // integer zeta; the kernels then evaluate each factor once per
+            // triplet and combine them with fixed-index arithmetic.
+            dg.grid = 0;
+            for (int c = 0; c < 16; ++c) dg.comboMember[c] = -1;
+            if (g.type != 2 && dg.fast && g.members.size() <= 16)
+            {
+                std::vector<double> etas, lams;
+                std::vector<int> zetas;
+                bool ok = true;
+                for (std::size_t q = 0; q < g.members.size() && ok; ++q)
+                {
+                    SymFunc const& s = el.sf[g.members[q]];
+                    if (!s.useIntegerPow || s.zetaInt < 1) ok = false;
+                    if (std::find(etas.begin(), etas.end(), s.eta) == etas.end()) etas.push_back(s.eta);
+                    if (std::find(lams.begin(), lams.end(), s.lambda) == lams.end()) lams.push_back(s.lambda);
+                    if (std::find(zetas.begin(), zetas.end(), s.zetaInt) == zetas.end()) zetas.push_back(s.zetaInt);
+                }
+                ok = ok && etas.size() <= 2 && lams.size() <= 2 && zetas.size() <= 4;
+                if (ok)
+                {
+                    for (std::size_t q = 0; q < g.members.size(); ++q)
+                    {
+                        SymFunc const& s = el.sf[g.members[q]];
+                        int es = (int)(std::find(etas.begin(), etas.end(), s.eta) - etas.begin());
+                        int ls = (int)(std::find(lams.begin(), lams.end(), s.lambda) - lams.begin());
+                        int zs = (int)(std::find(zetas.begin(), zetas.end(), s.zetaInt) - zetas.begin());
+                        int c = (es * 2 + ls) * 4 + zs;
+                        if (dg.comboMember[c] >= 0) ok = false;   // duplicate function
+                        dg.comboMember[c] = (signed char)q;
+                        dg.etaBase[es] = planBase[q];
+                        dg.etaPow[es] = planPow[q];
+                    }
+                    for (std::size_t k = 0; k < lams.size(); ++k) dg.lambdaVal[k] = lams[k];
+                    for (std::size_t k = lams.size(); k < 2; ++k) dg.lambdaVal[k] = 0.0;
+                    for (std::size_t k = 0; k < zetas.size(); ++k) dg.zetaM1[k] = zetas[k] - 1;
+                    for (std::size_t k = zetas.size(); k < 4; ++k) dg.zetaM1[k] = 0;
+                    for (std::size_t k = etas.size(); k < 2; ++k)
+                    {
+                        dg.etaBase[k] = 0;
+                        dg.etaPow[k] = 1;
+                    }
+                    dg.gridNZ = (int)zetas.size();
+                }
+                if (ok) dg.grid = 1;
+                else for (int c = 0; c < 16; ++c) dg.comboMember[c] = -1;
+            }
             for (std::size_t q = 0; q < g.members.size(); ++q)
             {
                 SymFunc const& s = el.sf[g.members[q]];

@@ -14,12 +14,12 @@
 //  * Gaussians: exp(-eta (rij^2 + rik^2 + rjk^2)) = E_b(rij) E_b(rik) exp(-eta_b rjk^2)
 //    raised to an integer power when eta = k eta_b (plan built on the host),
 //    so a triplet costs one exponential per base instead of one per eta.
-//  * Work split without atomics: lane l owns the block members l, l+32, ...
-//    For G each unordered pair is visited once (half circle within a block,
-//    or owner block x partner block); the force pass visits ordered pairs so
-//    every owner accumulates its own neighbour row and the self term in
-//    registers.  Candidate partners are compacted 32 at a time into a
-//    bitmask before the arithmetic, so lanes idle only at chunk ends.
+//  * Work split: each group's (owner, partner) pairs are enumerated
+//    owner-major (G: each unordered pair once; force pass: ordered pairs);
+//    the warp tests 32 candidates per step and appends the accepted ones to a
+//    shared-memory queue, which is consumed 32 triplets at a time, so lanes
+//    idle only in a group's last partial batch.  In the force pass the owner
+//    rows are combined by a segmented warp reduction (no atomics).
 //  * All sums run in a fixed order: results are bitwise reproducible.
 #include "kernels_common.cuh"
 #include "kernels.hpp"
@@ -68,6 +68,7 @@ struct Members
     T zl[kMaxMembers], fd[kMaxMembers], lambda[kMaxMembers], zeta[kMaxMembers], eta[kMaxMembers],
         rs[kMaxMembers];
     int zint[kMaxMembers], base[kMaxMembers], pw[kMaxMembers], flags[kMaxMembers];  // 1 intPow, 2 calcExp
+    T gcw[16], gzl[16], gfd[16];   // member grid: coefficients per (eta, lambda, zeta) combination, 0 if absent
 };
 
 constexpr int kQueue = 64;   // accepted (owner, partner) pairs waiting for a full warp
@@ -296,18 +297,154 @@ __device__ void stageMembers(Members<T>& mb, DevModel const& model, DevGroup con
         mb.pw[q] = M.expPow;
         mb.flags[q] = (M.useIntPow ? 1 : 0) | (M.calcExp ? 2 : 0);
     }
+    if (G.grid && lane < 16)
+    {
+        const int q = G.comboMember[lane];
+        if (q >= 0)
+        {
+            DevMember const& M = model.members[G.memberBegin + q];
+            mb.gcw[lane] = dEdG ? (T)(dEdG[M.sf] * M.factorNorm) : T(0);
+            mb.gzl[lane] = (T)M.zetaLambda;
+            mb.gfd[lane] = (T)M.factorDeriv;
+        }
+        else mb.gcw[lane] = mb.gzl[lane] = mb.gfd[lane] = T(0);
+    }
     __syncwarp();
 }
 
-__device__ __forceinline__ int halfRange(int j, int n)
+// Rare paths kept out of line so the hot loops stay small: real-valued zeta
+// and Gaussians with a shift r_s (which cannot use the factorised bases).
+template <typename T>
+__device__ __noinline__ T powReal(T b, T e)
 {
-    return (n - 1) / 2 + (((n & 1) == 0 && j < n / 2) ? 1 : 0);
+    return fpow<T>(b, e);
+}
+
+template <typename T>
+__device__ __noinline__ T gaussShifted(T eta, T rs, T r1, T r2, T r3, int narrow)
+{
+    const T u = r1 - rs, v = r2 - rs, w = r3 - rs;
+    return fexp<T>(-eta * (u * u + v * v + (narrow ? w * w : T(0))));
 }
 
 template <typename T>
 __device__ __forceinline__ T angularPow(T pl, Members<T> const& mb, int q)
 {
-    return (mb.flags[q] & 1) ? powInt<T>(pl, mb.zint[q] - 1) : fpow<T>(pl, mb.zeta[q] - T(1));
+    return (mb.flags[q] & 1) ? powInt<T>(pl, mb.zint[q] - 1) : powReal<T>(pl, mb.zeta[q] - T(1));
+}
+
+// Geometry of one triplet (owner j = slot so, partner k = slot sp).
+template <typename T>
+struct Triplet
+{
+    T x1, y1, z1, r1, ri1, fc1, dfcr1;
+    T x2, y2, z2, r2, ri2, fc2;
+    T dx3, dy3, dz3, rjk, rijk, rjk2;
+    T rinv, cost, fcjk, dfcjk;
+};
+
+template <typename T, int CAP>
+__device__ __forceinline__ void loadTriplet(Stage<T, CAP> const& S, DevCutoff const& cut, bool narrow, int so, int sp,
+                                            Triplet<T>& t)
+{
+    t.x1 = S.x[so];
+    t.y1 = S.y[so];
+    t.z1 = S.z[so];
+    t.r1 = S.r[so];
+    t.ri1 = S.rinv[so];
+    t.fc1 = S.fc[so];
+    t.dfcr1 = S.dfcr[so];
+    t.x2 = S.x[sp];
+    t.y2 = S.y[sp];
+    t.z2 = S.z[sp];
+    t.r2 = S.r[sp];
+    t.ri2 = S.rinv[sp];
+    t.fc2 = S.fc[sp];
+    t.dx3 = t.x2 - t.x1;
+    t.dy3 = t.y2 - t.y1;
+    t.dz3 = t.z2 - t.z1;
+    t.rinv = t.ri1 * t.ri2;
+    t.cost = (t.x1 * t.x2 + t.y1 * t.y2 + t.z1 * t.z2) * t.rinv;
+    t.rjk2 = t.dx3 * t.dx3 + t.dy3 * t.dy3 + t.dz3 * t.dz3;
+    t.rjk = T(0);
+    t.rijk = T(0);
+    t.fcjk = T(1);
+    t.dfcjk = T(0);
+    if (narrow)
+    {
+        t.rijk = frsqrt<T>(t.rjk2);
+        t.rjk = t.rjk2 * t.rijk;
+        double f, df;
+        cutoffFdf(cut, (double)t.rjk, f, df);   // FP64 near r_c in both forms
+        t.fcjk = (T)f;
+        t.dfcjk = (T)df;
+    }
+}
+
+// Gaussian bases of a triplet: E_b(rij) E_b(rik) exp(-eta_b rjk^2).
+template <typename T, int CAP>
+__device__ __forceinline__ void tripletBases(Stage<T, CAP> const& S, DevGroup const& G, bool narrow, int so, int sp,
+                                             T rjk2, T* bv)
+{
+#pragma unroll
+    for (int q = 0; q < kMaxStagedBases; ++q)
+        bv[q] = (q < G.numBases) ? S.E[q][so] * S.E[q][sp] * (narrow ? fexp<T>(-(T)G.baseEta[q] * rjk2) : T(1))
+                                 : T(0);
+}
+
+// Member grid, G pass: acc[(eta * 2 + lambda) * 4 + zeta] += E_eta * pl^zeta * pfc
+// (pl = 1 + lambda cos; terms with pl <= 0 vanish, SymGrpExpAngn.cpp:295).
+template <typename T, int NZ>
+__device__ __forceinline__ void gridValues(T const* bv, DevGroup const& G, T cost, T pfc, T* acc)
+{
+    T vS[2];
+#pragma unroll
+    for (int es = 0; es < 2; ++es) vS[es] = powInt<T>(G.etaBase[es] == 0 ? bv[0] : bv[1], G.etaPow[es]);
+#pragma unroll
+    for (int ls = 0; ls < 2; ++ls)
+    {
+        const T pl = T(1) + (T)G.lambdaVal[ls] * cost;
+        const T w = pl > T(0) ? pl * pfc : T(0);
+#pragma unroll
+        for (int zs = 0; zs < NZ; ++zs)
+        {
+            const T pz = powInt<T>(pl, G.zetaM1[zs]) * w;
+#pragma unroll
+            for (int es = 0; es < 2; ++es) acc[(es * 2 + ls) * 4 + zs] += vS[es] * pz;
+        }
+    }
+}
+
+// Member grid, force pass: the dE/dG-weighted member sums T1, T2 (= Uij =
+// Ujk, rs = 0) and T3 of one triplet.
+template <typename T, int NZ>
+__device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Members<T> const& mb, T cost, T& T1, T& T2,
+                                           T& T3)
+{
+    T vS[2];
+#pragma unroll
+    for (int es = 0; es < 2; ++es) vS[es] = powInt<T>(G.etaBase[es] == 0 ? bv[0] : bv[1], G.etaPow[es]);
+#pragma unroll
+    for (int ls = 0; ls < 2; ++ls)
+    {
+        const T pl = T(1) + (T)G.lambdaVal[ls] * cost;
+        const bool valid = pl > T(0);
+#pragma unroll
+        for (int zs = 0; zs < NZ; ++zs)
+        {
+            const T pz1 = valid ? powInt<T>(pl, G.zetaM1[zs]) : T(0);
+#pragma unroll
+            for (int es = 0; es < 2; ++es)
+            {
+                const int c = (es * 2 + ls) * 4 + zs;
+                const T a = mb.gcw[c] * vS[es] * pz1;
+                const T azl = a * mb.gzl[c];
+                T1 += azl;
+                T3 += a * pl;
+                T2 += azl * pl * mb.gfd[c];
+            }
+        }
+    }
 }
 
 } // namespace
@@ -352,7 +489,9 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
             if (G.type != 2 && G.fast) stageFactors<T, CAP>(S, G, lane);
             const T rc = (T)G.rc, rc2 = (T)G.rc2;
             const DevMember* mem = model.members + G.memberBegin;
-            for (int m0 = 0; m0 < G.memberCount; m0 += kChunkF)
+            const bool narrow = (G.type == 3);
+            const bool grid = (G.type != 2) && G.grid;
+            for (int m0 = 0; m0 < G.memberCount; m0 += (grid ? G.memberCount : kChunkF))
             {
                 const int mc = min(kChunkF, G.memberCount - m0);
                 T acc[kChunkF];
@@ -385,7 +524,7 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
                                         if (bq == t) e0 = eb[t];
                                     v = powInt<T>(e0, mb.pw[qq]);
                                 }
-                                else v = fexp<T>(-mb.eta[qq] * (r - mb.rs[qq]) * (r - mb.rs[qq]));
+                                else v = gaussShifted<T>(mb.eta[qq], mb.rs[qq], r, mb.rs[qq], mb.rs[qq], 0);
                                 acc[q] += v * fc;
                             }
                         }
@@ -393,106 +532,82 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
                 }
                 else
                 {
-                    const bool narrow = (G.type == 3);
                     const bool same = (G.e1 == G.e2);
                     const int A0 = S.blockBegin[G.e1], nA = S.blockBegin[G.e1 + 1] - A0;
                     const int B0 = S.blockBegin[G.e2], nB = S.blockBegin[G.e2 + 1] - B0;
-                    for (int a = lane; a < nA; a += 32)
+                    Phase ph[2];
+                    const int nph = groupPhases(A0, nA, B0, nB, same, false, ph);
+                    int qn = 0;
+                    for (int k = 0; k <= nph; ++k)
                     {
-                        const int sa = A0 + a;
-                        const T r1 = S.r[sa];
-                        if (!(r1 < rc)) continue;
-                        const T x1 = S.x[sa], y1 = S.y[sa], z1 = S.z[sa], ri1 = S.rinv[sa], fc1 = S.fc[sa];
-                        T e1b[kMaxStagedBases];
-#pragma unroll
-                        for (int q = 0; q < kMaxStagedBases; ++q) e1b[q] = G.fast ? S.E[q][sa] : T(0);
-                        const int cnt = same ? halfRange(a, nA) : nB;
-                        for (int t0 = 0; t0 < cnt; t0 += 32)
+                        const bool drain = (k == nph);
+                        Cursor cur;
+                        int cnt = 0;
+                        if (!drain)
                         {
-                            const int tm = min(32, cnt - t0);
-                            unsigned mask = 0;
-                            for (int bb = 0; bb < tm; ++bb)
+                            cur.init(ph[k], lane);
+                            cnt = ph[k].count;
+                        }
+                        int p0 = 0;
+                        while (true)
+                        {
+                            if (p0 < cnt)
                             {
-                                int p = same ? a + 1 + t0 + bb : t0 + bb;
-                                if (same && p >= nA) p -= nA;
-                                const int sb = (same ? A0 : B0) + p;
-                                bool ok = S.r[sb] < rc;
-                                if (ok && narrow)
-                                {
-                                    const T dx = S.x[sb] - x1, dy = S.y[sb] - y1, dz = S.z[sb] - z1;
-                                    ok = (dx * dx + dy * dy + dz * dz) < rc2;
-                                }
-                                mask |= (ok ? 1u : 0u) << bb;
+                                enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qn, lane);
+                                p0 += 32;
                             }
-                            while (mask)
+                            if (qn >= 32 || (drain && qn > 0))
                             {
-                                const int bb = __ffs(mask) - 1;
-                                mask &= mask - 1;
-                                int p = same ? a + 1 + t0 + bb : t0 + bb;
-                                if (same && p >= nA) p -= nA;
-                                const int sb = (same ? A0 : B0) + p;
-                                const T x2 = S.x[sb], y2 = S.y[sb], z2 = S.z[sb];
-                                const T cost = (x1 * x2 + y1 * y2 + z1 * z2) * (ri1 * S.rinv[sb]);
-                                T pfc = fc1 * S.fc[sb];
-                                T bv[kMaxStagedBases];
-                                T rjk = T(0), rjk2 = T(0);
-                                if (narrow)
+                                const int take = min(32, qn);
+                                if (lane < take)
                                 {
-                                    const T dx = x2 - x1, dy = y2 - y1, dz = z2 - z1;
-                                    rjk2 = dx * dx + dy * dy + dz * dz;
-                                    rjk = rjk2 * frsqrt<T>(rjk2);
-                                    double fjk, dfjk;
-                                    cutoffFdf(model.cutoff[G.cutoffSlot], (double)rjk, fjk, dfjk);
-                                    pfc *= (T)fjk;
-                                }
-                                if (G.fast)
-                                {
-#pragma unroll
-                                    for (int q = 0; q < kMaxStagedBases; ++q)
-                                        bv[q] = (q < G.numBases)
-                                                    ? e1b[q] * S.E[q][sb] *
-                                                          (narrow ? fexp<T>(-(T)G.baseEta[q] * rjk2) : T(1))
-                                                    : T(0);
-                                }
-                                const T r2 = S.r[sb];
-                                T vexp = T(0);
-#pragma unroll
-                                for (int q = 0; q < kChunkF; ++q)
-                                {
-                                    if (q < mc)
+                                    const int e = SM.queue[lane];
+                                    const int so = e >> 16, sp = e & 0xffff;
+                                    Triplet<T> t;
+                                    loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
+                                    const T pfc = t.fc1 * t.fc2 * t.fcjk;
+                                    T bv[kMaxStagedBases];
+                                    if (G.fast) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
+                                    T vexp = T(0);
+                                    if (grid)
                                     {
-                                        const int qq = m0 + q;
-                                        if ((mb.flags[qq] & 2) || q == 0)
+                                        if (G.gridNZ <= 2) gridValues<T, 2>(bv, G, t.cost, pfc, acc);
+                                        else gridValues<T, 4>(bv, G, t.cost, pfc, acc);
+                                    }
+                                    else
+#pragma unroll
+                                    for (int q = 0; q < kChunkF; ++q)
+                                    {
+                                        if (q < mc)
                                         {
-                                            if (G.fast)
-                                                vexp = powInt<T>(mb.base[qq] == 0 ? bv[0] : bv[kMaxStagedBases - 1],
-                                                                 mb.pw[qq]);
-                                            else
-                                            {
-                                                const T u = r1 - mb.rs[qq], v2 = r2 - mb.rs[qq], w3 = rjk - mb.rs[qq];
-                                                vexp = fexp<T>(-mb.eta[qq] *
-                                                               (u * u + v2 * v2 + (narrow ? w3 * w3 : T(0))));
-                                            }
+                                            const int qq = m0 + q;
+                                            if ((mb.flags[qq] & 2) || q == 0)
+                                                vexp = G.fast ? powInt<T>(mb.base[qq] == 0 ? bv[0] : bv[1], mb.pw[qq])
+                                                              : gaussShifted<T>(mb.eta[qq], mb.rs[qq], t.r1, t.r2,
+                                                                                t.rjk, narrow ? 1 : 0);
+                                            const T pl = T(1) + mb.lambda[qq] * t.cost;
+                                            if (pl > T(0)) acc[q] += vexp * angularPow<T>(pl, mb, qq) * pl * pfc;
                                         }
-                                        const T pl = T(1) + mb.lambda[qq] * cost;
-                                        if (pl > T(0)) acc[q] += vexp * angularPow<T>(pl, mb, qq) * pl * pfc;
                                     }
                                 }
+                                shiftQueue(SM.queue, qn, take, lane);
                             }
+                            else if (p0 >= cnt) break;
                         }
                     }
                 }
 #pragma unroll
                 for (int q = 0; q < kChunkF; ++q)
                 {
-                    if (q < mc)
+                    const int qq = grid ? (int)G.comboMember[q] : (q < mc ? m0 + q : -1);
+                    if (qq >= 0)
                     {
-                        double s = warpSum((double)acc[q]);
-                        if (lane == q)
+                        double sum = warpSum((double)acc[q]);
+                        if (lane == (q & 31))
                         {
-                            DevMember const& M = mem[m0 + q];
-                            if (G.type != 2) s *= M.gNorm;
-                            b.G[(size_t)i * b.gStride + M.sf] = scaleG(model.scaling[E.sfBegin + M.sf], s);
+                            DevMember const& M = mem[qq];
+                            if (G.type != 2) sum *= M.gNorm;
+                            b.G[(size_t)i * b.gStride + M.sf] = scaleG(model.scaling[E.sfBegin + M.sf], sum);
                         }
                     }
                 }
@@ -513,7 +628,9 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
 // T1 = sum a zeta lambda, T3 = sum a plambda,
 // Uij = sum a zeta lambda plambda factorDeriv (rij - rs)/rij  (Ujk alike).
 // The force E_i puts on j gains P1 dr_ij + P3 dr_jk; the self force on i
-// loses P1 dr_ij.
+// loses P1 dr_ij.  Triplets of a warp batch are owner-sorted; a segmented
+// warp reduction sums each owner's contributions before one lane adds them to
+// the owner's row (fixed order, no atomics).
 template <typename T, int CAP, int WARPS, int LOWER>
 __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchView b)
 {
@@ -572,7 +689,7 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                                 if (bq == t) e0 = eb[t];
                             v = powInt<T>(e0, mb.pw[q]);
                         }
-                        else v = fexp<T>(-mb.eta[q] * (r - mb.rs[q]) * (r - mb.rs[q]));
+                        else v = gaussShifted<T>(mb.eta[q], mb.rs[q], r, mb.rs[q], mb.rs[q], 0);
                         P += mb.cw[q] * (dfc - T(2) * mb.eta[q] * (r - mb.rs[q]) * fc) * v * ri;
                     }
                     const double Pd = (double)P;
@@ -584,100 +701,69 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                     sfy -= ddy;
                     sfz -= ddz;
                 }
+                __syncwarp();
                 continue;
             }
             if (G.fast) stageFactors<T, CAP>(S, G, lane);
             const bool narrow = (G.type == 3);
             const bool same = (G.e1 == G.e2);
-            for (int sweep = 0; sweep < (same ? 1 : 2); ++sweep)
+            const int A0 = S.blockBegin[G.e1], nA = S.blockBegin[G.e1 + 1] - A0;
+            const int B0 = S.blockBegin[G.e2], nB = S.blockBegin[G.e2 + 1] - B0;
+            Phase ph[2];
+            const int nph = groupPhases(A0, nA, B0, nB, same, true, ph);
+            int qn = 0;
+            for (int k = 0; k <= nph; ++k)
             {
-                const int eo = sweep == 0 ? G.e1 : G.e2;   // owners
-                const int ep = sweep == 0 ? G.e2 : G.e1;   // partners
-                const int O0 = S.blockBegin[eo], nO = S.blockBegin[eo + 1] - O0;
-                const int P0 = S.blockBegin[ep], nP = S.blockBegin[ep + 1] - P0;
-                for (int a = lane; a < nO; a += 32)
+                const bool drain = (k == nph);
+                Cursor cur;
+                int cnt = 0;
+                if (!drain)
                 {
-                    const int sa = O0 + a;
-                    const T r1 = S.r[sa];
-                    if (!(r1 < rc)) continue;
-                    const T x1 = S.x[sa], y1 = S.y[sa], z1 = S.z[sa], ri1 = S.rinv[sa], fc1 = S.fc[sa];
-                    const T dfcr1 = S.dfcr[sa];
-                    T e1b[kMaxStagedBases];
-#pragma unroll
-                    for (int q = 0; q < kMaxStagedBases; ++q) e1b[q] = G.fast ? S.E[q][sa] : T(0);
-                    T ax = T(0), ay = T(0), az = T(0), px = T(0), py = T(0), pz = T(0);
-                    const int cnt = same ? nO - 1 : nP;
-                    for (int t0 = 0; t0 < cnt; t0 += 32)
+                    cur.init(ph[k], lane);
+                    cnt = ph[k].count;
+                }
+                int p0 = 0;
+                while (true)
+                {
+                    if (p0 < cnt)
                     {
-                        const int tm = min(32, cnt - t0);
-                        unsigned mask = 0;
-                        for (int bb = 0; bb < tm; ++bb)
+                        enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qn, lane);
+                        p0 += 32;
+                    }
+                    if (qn >= 32 || (drain && qn > 0))
+                    {
+                        const int take = min(32, qn);
+                        int key = -1 - lane;    // inactive lanes never join a segment
+                        double cx = 0.0, cy = 0.0, cz = 0.0;
+                        if (lane < take)
                         {
-                            int p = same ? a + 1 + t0 + bb : t0 + bb;
-                            if (same && p >= nO) p -= nO;
-                            const int sb = P0 + p;
-                            bool ok = S.r[sb] < rc;
-                            if (ok && narrow)
+                            const int e = SM.queue[lane];
+                            const int so = e >> 16, sp = e & 0xffff;
+                            key = so;
+                            Triplet<T> t;
+                            loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
+                            const T pfc = t.fc1 * t.fc2 * t.fcjk;
+                            const T pr1 = t.fc2 * t.fcjk * t.dfcr1;
+                            const T pr3 = narrow ? t.fc1 * t.fc2 * t.dfcjk * t.rijk : T(0);
+                            T bv[kMaxStagedBases];
+                            if (G.fast) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
+                            T T1 = T(0), T3 = T(0), Uij = T(0), Ujk = T(0), vexp = T(0);
+                            if (G.grid)
                             {
-                                const T dx = S.x[sb] - x1, dy = S.y[sb] - y1, dz = S.z[sb] - z1;
-                                ok = (dx * dx + dy * dy + dz * dz) < rc2;
-                            }
-                            mask |= (ok ? 1u : 0u) << bb;
-                        }
-                        while (mask)
-                        {
-                            const int bb = __ffs(mask) - 1;
-                            mask &= mask - 1;
-                            int p = same ? a + 1 + t0 + bb : t0 + bb;
-                            if (same && p >= nO) p -= nO;
-                            const int sb = P0 + p;
-                            const T x2 = S.x[sb], y2 = S.y[sb], z2 = S.z[sb];
-                            const T ri2 = S.rinv[sb], fc2 = S.fc[sb];
-                            const T dx3 = x2 - x1, dy3 = y2 - y1, dz3 = z2 - z1;
-                            const T rinv = ri1 * ri2;
-                            const T cost = (x1 * x2 + y1 * y2 + z1 * z2) * rinv;
-                            T pfc, pr1, pr3 = T(0), rjk = T(0), rijk = T(0), rjk2 = T(0);
-                            if (narrow)
-                            {
-                                rjk2 = dx3 * dx3 + dy3 * dy3 + dz3 * dz3;
-                                rijk = frsqrt<T>(rjk2);
-                                rjk = rjk2 * rijk;
-                                double fjk, dfjk;
-                                cutoffFdf(model.cutoff[G.cutoffSlot], (double)rjk, fjk, dfjk);
-                                const T fcjk = (T)fjk, dfcjk = (T)dfjk;
-                                pfc = fc1 * fc2 * fcjk;
-                                pr1 = fc2 * fcjk * dfcr1;
-                                pr3 = fc1 * fc2 * dfcjk * rijk;
+                                T T2 = T(0);
+                                if (G.gridNZ <= 2) gridForces<T, 2>(bv, G, mb, t.cost, T1, T2, T3);
+                                else gridForces<T, 4>(bv, G, mb, t.cost, T1, T2, T3);
+                                Uij = T2;
+                                Ujk = T2;
                             }
                             else
-                            {
-                                pfc = fc1 * fc2;
-                                pr1 = fc2 * dfcr1;
-                            }
-                            T bv[kMaxStagedBases];
-                            if (G.fast)
-                            {
-#pragma unroll
-                                for (int q = 0; q < kMaxStagedBases; ++q)
-                                    bv[q] = (q < G.numBases)
-                                                ? e1b[q] * S.E[q][sb] * (narrow ? fexp<T>(-(T)G.baseEta[q] * rjk2) : T(1))
-                                                : T(0);
-                            }
-                            const T r2 = S.r[sb];
-                            T T1 = T(0), T3 = T(0), Uij = T(0), Ujk = T(0), vexp = T(0);
                             for (int q = 0; q < M; ++q)
                             {
                                 if ((mb.flags[q] & 2) || q == 0)
-                                {
-                                    if (G.fast)
-                                        vexp = powInt<T>(mb.base[q] == 0 ? bv[0] : bv[kMaxStagedBases - 1], mb.pw[q]);
-                                    else
-                                    {
-                                        const T u = r1 - mb.rs[q], v2 = r2 - mb.rs[q], w3 = rjk - mb.rs[q];
-                                        vexp = fexp<T>(-mb.eta[q] * (u * u + v2 * v2 + (narrow ? w3 * w3 : T(0))));
-                                    }
-                                }
-                                const T pl = T(1) + mb.lambda[q] * cost;
+                                    vexp = G.fast ? powInt<T>(mb.base[q] == 0 ? bv[0] : bv[1], mb.pw[q])
+                                                  : gaussShifted<T>(mb.eta[q], mb.rs[q], t.r1, t.r2, t.rjk,
+                                                                    narrow ? 1 : 0);
+                                const T pl = T(1) + mb.lambda[q] * t.cost;
                                 if (!(pl > T(0))) continue;
                                 const T a = mb.cw[q] * vexp * angularPow<T>(pl, mb, q);
                                 const T azl = a * mb.zl[q];
@@ -686,8 +772,8 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                                 T3 += a * pl;
                                 if (mb.rs[q] > T(0))
                                 {
-                                    Uij += azq * (r1 - mb.rs[q]) * ri1;
-                                    if (narrow) Ujk += azq * (rjk - mb.rs[q]) * rijk;
+                                    Uij += azq * (t.r1 - mb.rs[q]) * t.ri1;
+                                    if (narrow) Ujk += azq * (t.rjk - mb.rs[q]) * t.rijk;
                                 }
                                 else
                                 {
@@ -695,24 +781,41 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                                     Ujk += azq;
                                 }
                             }
-                            const T P1 = pfc * ((rinv - cost * ri1 * ri1) * T1 - Uij) + pr1 * T3;
-                            const T P3 = narrow ? (pfc * (rinv * T1 + Ujk) - pr3 * T3) : (pfc * rinv * T1);
-                            ax += P1 * x1 + P3 * dx3;
-                            ay += P1 * y1 + P3 * dy3;
-                            az += P1 * z1 + P3 * dz3;
-                            px += P1 * x1;
-                            py += P1 * y1;
-                            pz += P1 * z1;
+                            const T P1 = pfc * ((t.rinv - t.cost * t.ri1 * t.ri1) * T1 - Uij) + pr1 * T3;
+                            const T P3 = narrow ? (pfc * (t.rinv * T1 + Ujk) - pr3 * T3) : (pfc * t.rinv * T1);
+                            cx = (double)(P1 * t.x1 + P3 * t.dx3);
+                            cy = (double)(P1 * t.y1 + P3 * t.dy3);
+                            cz = (double)(P1 * t.z1 + P3 * t.dz3);
+                            sfx -= (double)(P1 * t.x1);
+                            sfy -= (double)(P1 * t.y1);
+                            sfz -= (double)(P1 * t.z1);
                         }
+                        // segmented suffix sums over lanes with equal owner key
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1)
+                        {
+                            const double ox = __shfl_down_sync(kFullMask, cx, o);
+                            const double oy = __shfl_down_sync(kFullMask, cy, o);
+                            const double oz = __shfl_down_sync(kFullMask, cz, o);
+                            const int ok = __shfl_down_sync(kFullMask, key, o);
+                            if (lane + o < 32 && ok == key)
+                            {
+                                cx += ox;
+                                cy += oy;
+                                cz += oz;
+                            }
+                        }
+                        const int prevKey = __shfl_up_sync(kFullMask, key, 1);
+                        if (lane < take && (lane == 0 || prevKey != key))
+                        {
+                            SM.h[0][key] += cx;
+                            SM.h[1][key] += cy;
+                            SM.h[2][key] += cz;
+                        }
+                        shiftQueue(SM.queue, qn, take, lane);
                     }
-                    SM.h[0][sa] += (double)ax;
-                    SM.h[1][sa] += (double)ay;
-                    SM.h[2][sa] += (double)az;
-                    sfx -= (double)px;
-                    sfy -= (double)py;
-                    sfz -= (double)pz;
+                    else if (p0 >= cnt) break;
                 }
-                __syncwarp();
             }
         }
         __syncwarp();
