@@ -103,7 +103,8 @@ struct DevModel
     int maxSF;
     int maxRows;
     int normalizeNeurons;
-    int pad_;
+    int allFast;          // 0, or the zeta slots (2, 4) when every group is planned (rs = 0 bases) and every
+                          // angular group is on the member grid
     double maxCutoff, maxCutoff2;
     DevElement el[kDevMaxElements];
     DevCutoff cutoff[4];

@@ -28,6 +28,10 @@ void setDynamicSmemOnce(const void* kernel, size_t bytes)
     if (done.count(key)) return;
     cudaCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
               "cudaFuncSetAttribute");
+    // Warp-per-atom kernels are limited by shared memory per SM: ask for the
+    // largest carveout so as many blocks as the registers allow stay resident.
+    cudaCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100),
+              "cudaFuncSetAttribute");
     done.insert(key);
 }
 
@@ -172,6 +176,7 @@ void DeviceModel::upload(Model const& m)
     DevModel v{};
     v.numElements = (int)m.elements.size();
     v.normalizeNeurons = m.normalizeNeurons ? 1 : 0;
+    v.allFast = 2;
     v.maxCutoff = m.maxCutoffRadius;
     v.maxCutoff2 = m.maxCutoffRadius * m.maxCutoffRadius;
 
@@ -281,7 +286,7 @@ void DeviceModel::upload(Model const& m)
                 for (std::size_t q = 0; q < g.members.size() && ok; ++q)
                 {
                     SymFunc const& s = el.sf[g.members[q]];
-                    if (!s.useIntegerPow || s.zetaInt < 1) ok = false;
+                    if (!s.useIntegerPow || s.zetaInt < 1 || s.zetaInt > 32) ok = false;   // zeta-1 in 5 bits
                     if (std::find(etas.begin(), etas.end(), s.eta) == etas.end()) etas.push_back(s.eta);
                     if (std::find(lams.begin(), lams.end(), s.lambda) == lams.end()) lams.push_back(s.lambda);
                     if (std::find(zetas.begin(), zetas.end(), s.zetaInt) == zetas.end()) zetas.push_back(s.zetaInt);
@@ -345,6 +350,8 @@ void DeviceModel::upload(Model const& m)
                 }
                 members.push_back(dm);
             }
+            if (!dg.fast || (dg.type != 2 && !dg.grid)) v.allFast = 0;
+            else if (dg.type != 2 && dg.gridNZ > 2 && v.allFast) v.allFast = 4;
             groups.push_back(dg);
         }
         // network

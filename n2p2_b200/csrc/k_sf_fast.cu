@@ -51,10 +51,11 @@ __device__ __forceinline__ double fpow<double>(double b, double e) { return pow(
 template <>
 __device__ __forceinline__ float fpow<float>(float b, float e) { return __powf(b, e); }
 
-template <typename T, int CAP>
+template <typename T, int CAP, bool DF>
 struct Stage
 {
-    T x[CAP], y[CAP], z[CAP], r[CAP], rinv[CAP], fc[CAP], dfcr[CAP];
+    T x[CAP], y[CAP], z[CAP], r[CAP], rinv[CAP], fc[CAP];
+    T dfcr[DF ? CAP : 1];                  // (df_c/dr)/r, force pass only
     T E[kMaxStagedBases][CAP];
     short perm[CAP];                       // staged slot -> position in the atom's list
     int blockBegin[kDevMaxElements + 1];
@@ -76,7 +77,7 @@ constexpr int kQueue = 64;   // accepted (owner, partner) pairs waiting for a fu
 template <typename T, int CAP>
 struct ValuesSmem
 {
-    Stage<T, CAP> st;
+    Stage<T, CAP, false> st;
     Members<T> mb;
     int queue[kQueue];
 };
@@ -84,7 +85,7 @@ struct ValuesSmem
 template <typename T, int CAP>
 struct ForcesSmem
 {
-    Stage<T, CAP> st;
+    Stage<T, CAP, true> st;
     Members<T> mb;
     double h[3][CAP];
     int queue[kQueue];
@@ -147,8 +148,8 @@ struct Cursor
 
 // Test the next 32 candidates of a phase and append the accepted ones, in
 // candidate order, to the warp's queue (qn entries from q[0]).
-template <typename T, int CAP>
-__device__ __forceinline__ void enqueueCandidates(Stage<T, CAP> const& S, Phase const& ph, Cursor& cur, int p0,
+template <typename T, int CAP, bool DF>
+__device__ __forceinline__ void enqueueCandidates(Stage<T, CAP, DF> const& S, Phase const& ph, Cursor& cur, int p0,
                                                   T rc, T rc2, bool narrow, int* queue, int& qn, int lane)
 {
     const int p = p0 + lane;
@@ -211,8 +212,8 @@ __device__ __forceinline__ int groupPhases(int A0, int nA, int B0, int nB, bool 
 }
 
 // Neighbours of one atom into the stage, sorted by element (stable).
-template <typename T, int CAP>
-__device__ void stageGeometry(Stage<T, CAP>& S, int64_t off, int n, int numElements, BatchView const& b, int lane)
+template <typename T, int CAP, bool DF>
+__device__ void stageGeometry(Stage<T, CAP, DF>& S, int64_t off, int n, int numElements, BatchView const& b, int lane)
 {
     __syncwarp();
     int base = 0;
@@ -244,8 +245,8 @@ __device__ void stageGeometry(Stage<T, CAP>& S, int64_t off, int n, int numEleme
 }
 
 // f_c and df_c/r of the cutoff slot (values computed in FP64 per entry).
-template <typename T, int CAP>
-__device__ void stageCutoff(Stage<T, CAP>& S, int64_t off, int n, int slot, BatchView const& b, int lane)
+template <typename T, int CAP, bool DF>
+__device__ void stageCutoff(Stage<T, CAP, DF>& S, int64_t off, int n, int slot, BatchView const& b, int lane)
 {
     __syncwarp();
     const double* fc = b.nbrFc + (size_t)slot * b.nbrCapacity + off;
@@ -254,15 +255,15 @@ __device__ void stageCutoff(Stage<T, CAP>& S, int64_t off, int n, int slot, Batc
     {
         const int m = S.perm[s];
         S.fc[s] = (T)fc[m];
-        S.dfcr[s] = (T)(dfc[m] / b.nbrD[off + m]);
+        if constexpr (DF) S.dfcr[s] = (T)(dfc[m] / b.nbrD[off + m]);
     }
     __syncwarp();
 }
 
 // Gaussian factors exp(-eta_b r^2) of the group's staged bases for the slots
 // of the group's element blocks.
-template <typename T, int CAP>
-__device__ void stageFactors(Stage<T, CAP>& S, DevGroup const& G, int lane)
+template <typename T, int CAP, bool DF>
+__device__ void stageFactors(Stage<T, CAP, DF>& S, DevGroup const& G, int lane)
 {
     __syncwarp();
     for (int pass = 0; pass < 2; ++pass)
@@ -343,8 +344,8 @@ struct Triplet
     T rinv, cost, fcjk, dfcjk;
 };
 
-template <typename T, int CAP>
-__device__ __forceinline__ void loadTriplet(Stage<T, CAP> const& S, DevCutoff const& cut, bool narrow, int so, int sp,
+template <typename T, int CAP, bool DF>
+__device__ __forceinline__ void loadTriplet(Stage<T, CAP, DF> const& S, DevCutoff const& cut, bool narrow, int so, int sp,
                                             Triplet<T>& t)
 {
     t.x1 = S.x[so];
@@ -353,7 +354,8 @@ __device__ __forceinline__ void loadTriplet(Stage<T, CAP> const& S, DevCutoff co
     t.r1 = S.r[so];
     t.ri1 = S.rinv[so];
     t.fc1 = S.fc[so];
-    t.dfcr1 = S.dfcr[so];
+    if constexpr (DF) t.dfcr1 = S.dfcr[so];
+    else t.dfcr1 = T(0);
     t.x2 = S.x[sp];
     t.y2 = S.y[sp];
     t.z2 = S.z[sp];
@@ -382,8 +384,8 @@ __device__ __forceinline__ void loadTriplet(Stage<T, CAP> const& S, DevCutoff co
 }
 
 // Gaussian bases of a triplet: E_b(rij) E_b(rik) exp(-eta_b rjk^2).
-template <typename T, int CAP>
-__device__ __forceinline__ void tripletBases(Stage<T, CAP> const& S, DevGroup const& G, bool narrow, int so, int sp,
+template <typename T, int CAP, bool DF>
+__device__ __forceinline__ void tripletBases(Stage<T, CAP, DF> const& S, DevGroup const& G, bool narrow, int so, int sp,
                                              T rjk2, T* bv)
 {
 #pragma unroll
@@ -392,25 +394,52 @@ __device__ __forceinline__ void tripletBases(Stage<T, CAP> const& S, DevGroup co
                                  : T(0);
 }
 
+// Binary powers of x shared by several exponents: x^e for 0 <= e < 32 with
+// the multiplication order of pow_int (utility.cpp:292-316) -- start from 1,
+// multiply in x^(2^k) for every set bit in increasing k -- without loops or
+// data-dependent branches.
+template <typename T>
+struct Powers
+{
+    T p1, p2, p4, p8, p16;
+    __device__ __forceinline__ explicit Powers(T x) : p1(x)
+    {
+        p2 = p1 * p1;
+        p4 = p2 * p2;
+        p8 = p4 * p4;
+        p16 = p8 * p8;
+    }
+    __device__ __forceinline__ T pow(int e) const
+    {
+        T r = (e & 1) ? p1 : T(1);
+        r = (e & 2) ? r * p2 : r;
+        r = (e & 4) ? r * p4 : r;
+        r = (e & 8) ? r * p8 : r;
+        r = (e & 16) ? r * p16 : r;
+        return r;
+    }
+};
+
 // Member grid, G pass: acc[(eta * 2 + lambda) * 4 + zeta] += E_eta * pl^zeta * pfc
 // (pl = 1 + lambda cos; terms with pl <= 0 vanish, SymGrpExpAngn.cpp:295).
-template <typename T, int NZ>
+template <typename T, int NZ, int STRIDE>
 __device__ __forceinline__ void gridValues(T const* bv, DevGroup const& G, T cost, T pfc, T* acc)
 {
     T vS[2];
 #pragma unroll
-    for (int es = 0; es < 2; ++es) vS[es] = powInt<T>(G.etaBase[es] == 0 ? bv[0] : bv[1], G.etaPow[es]);
+    for (int es = 0; es < 2; ++es) vS[es] = Powers<T>(G.etaBase[es] == 0 ? bv[0] : bv[1]).pow(G.etaPow[es]);
 #pragma unroll
     for (int ls = 0; ls < 2; ++ls)
     {
         const T pl = T(1) + (T)G.lambdaVal[ls] * cost;
         const T w = pl > T(0) ? pl * pfc : T(0);
+        const Powers<T> P(pl);
 #pragma unroll
         for (int zs = 0; zs < NZ; ++zs)
         {
-            const T pz = powInt<T>(pl, G.zetaM1[zs]) * w;
+            const T pz = P.pow(G.zetaM1[zs]) * w;
 #pragma unroll
-            for (int es = 0; es < 2; ++es) acc[(es * 2 + ls) * 4 + zs] += vS[es] * pz;
+            for (int es = 0; es < 2; ++es) acc[(es * 2 + ls) * STRIDE + zs] += vS[es] * pz;
         }
     }
 }
@@ -423,16 +452,17 @@ __device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Membe
 {
     T vS[2];
 #pragma unroll
-    for (int es = 0; es < 2; ++es) vS[es] = powInt<T>(G.etaBase[es] == 0 ? bv[0] : bv[1], G.etaPow[es]);
+    for (int es = 0; es < 2; ++es) vS[es] = Powers<T>(G.etaBase[es] == 0 ? bv[0] : bv[1]).pow(G.etaPow[es]);
 #pragma unroll
     for (int ls = 0; ls < 2; ++ls)
     {
         const T pl = T(1) + (T)G.lambdaVal[ls] * cost;
         const bool valid = pl > T(0);
+        const Powers<T> P(pl);
 #pragma unroll
         for (int zs = 0; zs < NZ; ++zs)
         {
-            const T pz1 = valid ? powInt<T>(pl, G.zetaM1[zs]) : T(0);
+            const T pz1 = valid ? P.pow(G.zetaM1[zs]) : T(0);
 #pragma unroll
             for (int es = 0; es < 2; ++es)
             {
@@ -447,19 +477,55 @@ __device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Membe
     }
 }
 
+// h[.][key] += c for every lane with key >= 0.  Lanes with equal keys are
+// combined first, in increasing lane order, by the lowest of them, so every
+// slot is written by one lane and the sums do not depend on timing.
+template <int CAP>
+__device__ __forceinline__ void addByKey(double (*h)[CAP], int key, double cx, double cy, double cz, int lane)
+{
+    const unsigned peers = __match_any_sync(kFullMask, key);
+    const bool leader = key >= 0 && lane == __ffs(peers) - 1;
+    unsigned rest = leader ? (peers & (peers - 1u)) : 0u;
+    const unsigned iters = __reduce_max_sync(kFullMask, (unsigned)__popc(rest));
+    for (unsigned r = 0; r < iters; ++r)
+    {
+        const int src = rest ? __ffs(rest) - 1 : lane;
+        const double sx = __shfl_sync(kFullMask, cx, src);
+        const double sy = __shfl_sync(kFullMask, cy, src);
+        const double sz = __shfl_sync(kFullMask, cz, src);
+        if (rest)
+        {
+            cx += sx;
+            cy += sy;
+            cz += sz;
+            rest &= rest - 1u;
+        }
+    }
+    if (leader)
+    {
+        h[0][key] += cx;
+        h[1][key] += cy;
+        h[2][key] += cz;
+    }
+    __syncwarp();
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
 // G values
 // ---------------------------------------------------------------------------
-template <typename T, int CAP, int WARPS, int LOWER>
-__global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchView b)
+template <typename T, int CAP, int WARPS, int LOWER, int FAST>
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(DevModel model, BatchView b)
 {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     ValuesSmem<T, CAP>& SM = reinterpret_cast<ValuesSmem<T, CAP>*>(smemRaw)[threadIdx.x >> 5];
-    Stage<T, CAP>& S = SM.st;
+    auto& S = SM.st;
     Members<T>& mb = SM.mb;
     const int lane = threadIdx.x & 31;
+    // Accumulators per sweep: the member grid of the model (FAST = its zeta
+    // slots) or a chunk of members.
+    constexpr int ACC = FAST ? 4 * FAST : kChunkF;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
     {
@@ -480,23 +546,24 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
         for (int g = 0; g < E.groupCount; ++g)
         {
             DevGroup const G = model.groups[E.groupBegin + g];
+            const bool fastG = FAST || G.fast;
             if (G.cutoffSlot != slot)
             {
                 stageCutoff<T, CAP>(S, off, n, G.cutoffSlot, b, lane);
                 slot = G.cutoffSlot;
             }
             stageMembers<T>(mb, model, G, nullptr, lane);
-            if (G.type != 2 && G.fast) stageFactors<T, CAP>(S, G, lane);
+            if (G.type != 2 && fastG) stageFactors<T, CAP>(S, G, lane);
             const T rc = (T)G.rc, rc2 = (T)G.rc2;
             const DevMember* mem = model.members + G.memberBegin;
             const bool narrow = (G.type == 3);
-            const bool grid = (G.type != 2) && G.grid;
-            for (int m0 = 0; m0 < G.memberCount; m0 += (grid ? G.memberCount : kChunkF))
+            const bool grid = (G.type != 2) && (FAST || G.grid);
+            for (int m0 = 0; m0 < G.memberCount; m0 += (grid ? G.memberCount : ACC))
             {
-                const int mc = min(kChunkF, G.memberCount - m0);
-                T acc[kChunkF];
+                const int mc = min(ACC, G.memberCount - m0);
+                T acc[ACC];
 #pragma unroll
-                for (int q = 0; q < kChunkF; ++q) acc[q] = T(0);
+                for (int q = 0; q < ACC; ++q) acc[q] = T(0);
                 if (G.type == 2)
                 {
                     for (int s = S.blockBegin[G.e1] + lane; s < S.blockBegin[G.e1 + 1]; s += 32)
@@ -507,22 +574,22 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
                         T eb[kMaxBases];
 #pragma unroll
                         for (int q = 0; q < kMaxBases; ++q)
-                            eb[q] = (G.fast && q < G.numBases) ? fexp<T>(-(T)G.baseEta[q] * r * r) : T(0);
+                            eb[q] = (fastG && q < G.numBases) ? fexp<T>(-(T)G.baseEta[q] * r * r) : T(0);
 #pragma unroll
-                        for (int q = 0; q < kChunkF; ++q)
+                        for (int q = 0; q < ACC; ++q)
                         {
                             if (q < mc)
                             {
                                 const int qq = m0 + q;
                                 T v;
-                                if (G.fast)
+                                if (fastG)
                                 {
                                     const int bq = mb.base[qq];
                                     T e0 = eb[0];
 #pragma unroll
                                     for (int t = 1; t < kMaxBases; ++t)
                                         if (bq == t) e0 = eb[t];
-                                    v = powInt<T>(e0, mb.pw[qq]);
+                                    v = Powers<T>(e0).pow(mb.pw[qq]);
                                 }
                                 else v = gaussShifted<T>(mb.eta[qq], mb.rs[qq], r, mb.rs[qq], mb.rs[qq], 0);
                                 acc[q] += v * fc;
@@ -567,22 +634,23 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
                                     loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
                                     const T pfc = t.fc1 * t.fc2 * t.fcjk;
                                     T bv[kMaxStagedBases];
-                                    if (G.fast) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
+                                    if (fastG) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
                                     T vexp = T(0);
                                     if (grid)
                                     {
-                                        if (G.gridNZ <= 2) gridValues<T, 2>(bv, G, t.cost, pfc, acc);
-                                        else gridValues<T, 4>(bv, G, t.cost, pfc, acc);
+                                        if constexpr (FAST > 0) gridValues<T, FAST, FAST>(bv, G, t.cost, pfc, acc);
+                                        else if (G.gridNZ <= 2) gridValues<T, 2, 4>(bv, G, t.cost, pfc, acc);
+                                        else gridValues<T, 4, 4>(bv, G, t.cost, pfc, acc);
                                     }
                                     else
 #pragma unroll
-                                    for (int q = 0; q < kChunkF; ++q)
+                                    for (int q = 0; q < ACC; ++q)
                                     {
                                         if (q < mc)
                                         {
                                             const int qq = m0 + q;
                                             if ((mb.flags[qq] & 2) || q == 0)
-                                                vexp = G.fast ? powInt<T>(mb.base[qq] == 0 ? bv[0] : bv[1], mb.pw[qq])
+                                                vexp = fastG ? Powers<T>(mb.base[qq] == 0 ? bv[0] : bv[1]).pow(mb.pw[qq])
                                                               : gaussShifted<T>(mb.eta[qq], mb.rs[qq], t.r1, t.r2,
                                                                                 t.rjk, narrow ? 1 : 0);
                                             const T pl = T(1) + mb.lambda[qq] * t.cost;
@@ -597,9 +665,10 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
                     }
                 }
 #pragma unroll
-                for (int q = 0; q < kChunkF; ++q)
+                for (int q = 0; q < ACC; ++q)
                 {
-                    const int qq = grid ? (int)G.comboMember[q] : (q < mc ? m0 + q : -1);
+                    const int c = FAST ? (q / (FAST ? FAST : 1)) * 4 + q % (FAST ? FAST : 1) : q;
+                    const int qq = grid ? (int)G.comboMember[c] : (q < mc ? m0 + q : -1);
                     if (qq >= 0)
                     {
                         double sum = warpSum((double)acc[q]);
@@ -620,23 +689,25 @@ __global__ void __launch_bounds__(WARPS * 32) kSFValuesF(DevModel model, BatchVi
 // Force pass (adjoint schedule)
 // ---------------------------------------------------------------------------
 // With a_s = dE/dG_s * factorNorm_s * fg_s, the reference's derivative
-// prefactors p1, p3 (SymGrpExpAngn.cpp:305-337) contract, for the ordered
-// pair (owner j, partner k), to
+// prefactors p1, p2, p3 (SymGrpExpAngn.cpp:305-337) contract, for the
+// unordered pair (j, k), to
 //   P1 = pfc ((1/(rij rik) - cos/rij^2) T1 - Uij) + pr1 T3
+//   P2 = pfc ((1/(rij rik) - cos/rik^2) T1 - Uik) + pr2 T3
 //   P3 = pfc (1/(rij rik) T1 + Ujk) - pr3 T3          (narrow)
 //   P3 = pfc /(rij rik) T1                            (wide)
 // T1 = sum a zeta lambda, T3 = sum a plambda,
-// Uij = sum a zeta lambda plambda factorDeriv (rij - rs)/rij  (Ujk alike).
-// The force E_i puts on j gains P1 dr_ij + P3 dr_jk; the self force on i
-// loses P1 dr_ij.  Triplets of a warp batch are owner-sorted; a segmented
-// warp reduction sums each owner's contributions before one lane adds them to
-// the owner's row (fixed order, no atomics).
-template <typename T, int CAP, int WARPS, int LOWER>
+// Uij = sum a zeta lambda plambda factorDeriv (rij - rs)/rij  (Uik, Ujk alike).
+// The force E_i puts on j gains P1 dr_ij + P3 dr_jk, on k P2 dr_ik - P3 dr_jk;
+// the self force on i loses P1 dr_ij + P2 dr_ik.  Each pair is evaluated once;
+// its two contributions are summed per slot inside the warp batch (owner runs
+// by a segmented scan, then both sides by key) and added by one lane per slot
+// in a fixed order, without atomics.
+template <typename T, int CAP, int WARPS, int LOWER, int FAST>
 __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchView b)
 {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     ForcesSmem<T, CAP>& SM = reinterpret_cast<ForcesSmem<T, CAP>*>(smemRaw)[threadIdx.x >> 5];
-    Stage<T, CAP>& S = SM.st;
+    auto& S = SM.st;
     Members<T>& mb = SM.mb;
     const int lane = threadIdx.x & 31;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
@@ -657,6 +728,7 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
         for (int g = 0; g < E.groupCount; ++g)
         {
             DevGroup const G = model.groups[E.groupBegin + g];
+            const bool fastG = FAST || G.fast;
             if (G.cutoffSlot != slot)
             {
                 stageCutoff<T, CAP>(S, off, n, G.cutoffSlot, b, lane);
@@ -675,19 +747,19 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                     T eb[kMaxBases];
 #pragma unroll
                     for (int q = 0; q < kMaxBases; ++q)
-                        eb[q] = (G.fast && q < G.numBases) ? fexp<T>(-(T)G.baseEta[q] * r * r) : T(0);
+                        eb[q] = (fastG && q < G.numBases) ? fexp<T>(-(T)G.baseEta[q] * r * r) : T(0);
                     T P = T(0);
                     for (int q = 0; q < M; ++q)
                     {
                         T v;
-                        if (G.fast)
+                        if (fastG)
                         {
                             const int bq = mb.base[q];
                             T e0 = eb[0];
 #pragma unroll
                             for (int t = 1; t < kMaxBases; ++t)
                                 if (bq == t) e0 = eb[t];
-                            v = powInt<T>(e0, mb.pw[q]);
+                            v = Powers<T>(e0).pow(mb.pw[q]);
                         }
                         else v = gaussShifted<T>(mb.eta[q], mb.rs[q], r, mb.rs[q], mb.rs[q], 0);
                         P += mb.cw[q] * (dfc - T(2) * mb.eta[q] * (r - mb.rs[q]) * fc) * v * ri;
@@ -704,13 +776,13 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                 __syncwarp();
                 continue;
             }
-            if (G.fast) stageFactors<T, CAP>(S, G, lane);
+            if (fastG) stageFactors<T, CAP>(S, G, lane);
             const bool narrow = (G.type == 3);
             const bool same = (G.e1 == G.e2);
             const int A0 = S.blockBegin[G.e1], nA = S.blockBegin[G.e1 + 1] - A0;
             const int B0 = S.blockBegin[G.e2], nB = S.blockBegin[G.e2 + 1] - B0;
             Phase ph[2];
-            const int nph = groupPhases(A0, nA, B0, nB, same, true, ph);
+            const int nph = groupPhases(A0, nA, B0, nB, same, false, ph);
             int qn = 0;
             for (int k = 0; k <= nph; ++k)
             {
@@ -733,34 +805,39 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                     if (qn >= 32 || (drain && qn > 0))
                     {
                         const int take = min(32, qn);
-                        int key = -1 - lane;    // inactive lanes never join a segment
-                        double cx = 0.0, cy = 0.0, cz = 0.0;
+                        int keyO = -1 - lane, keyP = -1 - lane;   // inactive lanes never join a segment
+                        double ox = 0.0, oy = 0.0, oz = 0.0, px = 0.0, py = 0.0, pz = 0.0;
                         if (lane < take)
                         {
                             const int e = SM.queue[lane];
                             const int so = e >> 16, sp = e & 0xffff;
-                            key = so;
+                            keyO = so;
+                            keyP = sp;
                             Triplet<T> t;
                             loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
+                            const T dfcr2 = S.dfcr[sp];
                             const T pfc = t.fc1 * t.fc2 * t.fcjk;
                             const T pr1 = t.fc2 * t.fcjk * t.dfcr1;
+                            const T pr2 = t.fc1 * t.fcjk * dfcr2;
                             const T pr3 = narrow ? t.fc1 * t.fc2 * t.dfcjk * t.rijk : T(0);
                             T bv[kMaxStagedBases];
-                            if (G.fast) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
-                            T T1 = T(0), T3 = T(0), Uij = T(0), Ujk = T(0), vexp = T(0);
-                            if (G.grid)
+                            if (fastG) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
+                            T T1 = T(0), T3 = T(0), Uij = T(0), Uik = T(0), Ujk = T(0), vexp = T(0);
+                            if (FAST || G.grid)
                             {
                                 T T2 = T(0);
-                                if (G.gridNZ <= 2) gridForces<T, 2>(bv, G, mb, t.cost, T1, T2, T3);
+                                if constexpr (FAST > 0) gridForces<T, FAST>(bv, G, mb, t.cost, T1, T2, T3);
+                                else if (G.gridNZ <= 2) gridForces<T, 2>(bv, G, mb, t.cost, T1, T2, T3);
                                 else gridForces<T, 4>(bv, G, mb, t.cost, T1, T2, T3);
                                 Uij = T2;
+                                Uik = T2;
                                 Ujk = T2;
                             }
                             else
                             for (int q = 0; q < M; ++q)
                             {
                                 if ((mb.flags[q] & 2) || q == 0)
-                                    vexp = G.fast ? powInt<T>(mb.base[q] == 0 ? bv[0] : bv[1], mb.pw[q])
+                                    vexp = fastG ? Powers<T>(mb.base[q] == 0 ? bv[0] : bv[1]).pow(mb.pw[q])
                                                   : gaussShifted<T>(mb.eta[q], mb.rs[q], t.r1, t.r2, t.rjk,
                                                                     narrow ? 1 : 0);
                                 const T pl = T(1) + mb.lambda[q] * t.cost;
@@ -773,45 +850,51 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                                 if (mb.rs[q] > T(0))
                                 {
                                     Uij += azq * (t.r1 - mb.rs[q]) * t.ri1;
+                                    Uik += azq * (t.r2 - mb.rs[q]) * t.ri2;
                                     if (narrow) Ujk += azq * (t.rjk - mb.rs[q]) * t.rijk;
                                 }
                                 else
                                 {
                                     Uij += azq;
+                                    Uik += azq;
                                     Ujk += azq;
                                 }
                             }
+                            // both ends of the unordered pair (j, k): P1 for j, P2 (= P1 with j, k
+                            // exchanged) for k; P3 is symmetric and enters with opposite signs.
                             const T P1 = pfc * ((t.rinv - t.cost * t.ri1 * t.ri1) * T1 - Uij) + pr1 * T3;
+                            const T P2 = pfc * ((t.rinv - t.cost * t.ri2 * t.ri2) * T1 - Uik) + pr2 * T3;
                             const T P3 = narrow ? (pfc * (t.rinv * T1 + Ujk) - pr3 * T3) : (pfc * t.rinv * T1);
-                            cx = (double)(P1 * t.x1 + P3 * t.dx3);
-                            cy = (double)(P1 * t.y1 + P3 * t.dy3);
-                            cz = (double)(P1 * t.z1 + P3 * t.dz3);
-                            sfx -= (double)(P1 * t.x1);
-                            sfy -= (double)(P1 * t.y1);
-                            sfz -= (double)(P1 * t.z1);
+                            ox = (double)(P1 * t.x1 + P3 * t.dx3);
+                            oy = (double)(P1 * t.y1 + P3 * t.dy3);
+                            oz = (double)(P1 * t.z1 + P3 * t.dz3);
+                            px = (double)(P2 * t.x2 - P3 * t.dx3);
+                            py = (double)(P2 * t.y2 - P3 * t.dy3);
+                            pz = (double)(P2 * t.z2 - P3 * t.dz3);
+                            sfx -= (double)(P1 * t.x1 + P2 * t.x2);
+                            sfy -= (double)(P1 * t.y1 + P2 * t.y2);
+                            sfz -= (double)(P1 * t.z1 + P2 * t.z2);
                         }
-                        // segmented suffix sums over lanes with equal owner key
+                        // owners: runs of equal keys (owner-major order) first collapse to
+                        // their head lane; then both sides add into h by key.
 #pragma unroll
                         for (int o = 1; o < 32; o <<= 1)
                         {
-                            const double ox = __shfl_down_sync(kFullMask, cx, o);
-                            const double oy = __shfl_down_sync(kFullMask, cy, o);
-                            const double oz = __shfl_down_sync(kFullMask, cz, o);
-                            const int ok = __shfl_down_sync(kFullMask, key, o);
-                            if (lane + o < 32 && ok == key)
+                            const double sx = __shfl_down_sync(kFullMask, ox, o);
+                            const double sy = __shfl_down_sync(kFullMask, oy, o);
+                            const double sz = __shfl_down_sync(kFullMask, oz, o);
+                            const int sk = __shfl_down_sync(kFullMask, keyO, o);
+                            if (lane + o < 32 && sk == keyO)
                             {
-                                cx += ox;
-                                cy += oy;
-                                cz += oz;
+                                ox += sx;
+                                oy += sy;
+                                oz += sz;
                             }
                         }
-                        const int prevKey = __shfl_up_sync(kFullMask, key, 1);
-                        if (lane < take && (lane == 0 || prevKey != key))
-                        {
-                            SM.h[0][key] += cx;
-                            SM.h[1][key] += cy;
-                            SM.h[2][key] += cz;
-                        }
+                        const int prevKey = __shfl_up_sync(kFullMask, keyO, 1);
+                        if (lane > 0 && prevKey == keyO) keyO = -1 - lane;
+                        addByKey<CAP>(SM.h, keyO, ox, oy, oz, lane);
+                        addByKey<CAP>(SM.h, keyP, px, py, pz, lane);
                         shiftQueue(SM.queue, qn, take, lane);
                     }
                     else if (p0 >= cnt) break;
@@ -859,8 +942,12 @@ void valuesT(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
 {
     const size_t s1 = sizeof(ValuesSmem<T, kStdCapF>) * kStdWarpsF;
     const size_t s2 = sizeof(ValuesSmem<T, kBigCapF>) * kBigWarpsF;
-    auto k1 = kSFValuesF<T, kStdCapF, kStdWarpsF, -1>;
-    auto k2 = kSFValuesF<T, kBigCapF, kBigWarpsF, kStdCapF>;
+    auto k1 = m.allFast == 2 ? kSFValuesF<T, kStdCapF, kStdWarpsF, -1, 2>
+            : m.allFast == 4 ? kSFValuesF<T, kStdCapF, kStdWarpsF, -1, 4>
+                             : kSFValuesF<T, kStdCapF, kStdWarpsF, -1, 0>;
+    auto k2 = m.allFast == 2 ? kSFValuesF<T, kBigCapF, kBigWarpsF, kStdCapF, 2>
+            : m.allFast == 4 ? kSFValuesF<T, kBigCapF, kBigWarpsF, kStdCapF, 4>
+                             : kSFValuesF<T, kBigCapF, kBigWarpsF, kStdCapF, 0>;
     setDynamicSmemOnce(reinterpret_cast<const void*>(k1), s1);
     setDynamicSmemOnce(reinterpret_cast<const void*>(k2), s2);
     k1<<<gridFor(b.N, kStdWarpsF, sms, 32), kStdWarpsF * 32, s1, st>>>(m, b);
@@ -872,8 +959,12 @@ void forcesT(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
 {
     const size_t s1 = sizeof(ForcesSmem<T, kStdCapF>) * kStdWarpsF;
     const size_t s2 = sizeof(ForcesSmem<T, kBigCapF>) * kBigWarpsF;
-    auto k1 = kSFForcesF<T, kStdCapF, kStdWarpsF, -1>;
-    auto k2 = kSFForcesF<T, kBigCapF, kBigWarpsF, kStdCapF>;
+    auto k1 = m.allFast == 2 ? kSFForcesF<T, kStdCapF, kStdWarpsF, -1, 2>
+            : m.allFast == 4 ? kSFForcesF<T, kStdCapF, kStdWarpsF, -1, 4>
+                             : kSFForcesF<T, kStdCapF, kStdWarpsF, -1, 0>;
+    auto k2 = m.allFast == 2 ? kSFForcesF<T, kBigCapF, kBigWarpsF, kStdCapF, 2>
+            : m.allFast == 4 ? kSFForcesF<T, kBigCapF, kBigWarpsF, kStdCapF, 4>
+                             : kSFForcesF<T, kBigCapF, kBigWarpsF, kStdCapF, 0>;
     setDynamicSmemOnce(reinterpret_cast<const void*>(k1), s1);
     setDynamicSmemOnce(reinterpret_cast<const void*>(k2), s2);
     k1<<<gridFor(b.N, kStdWarpsF, sms, 32), kStdWarpsF * 32, s1, st>>>(m, b);
