@@ -72,7 +72,7 @@ struct Members
     T gcw[16], gzl[16], gfd[16];   // member grid: coefficients per (eta, lambda, zeta) combination, 0 if absent
 };
 
-constexpr int kQueue = 64;   // accepted (owner, partner) pairs waiting for a full warp
+constexpr int kQueue = 128;  // ring of accepted (owner, partner) pairs waiting for a full warp (< 32 + 64)
 
 template <typename T, int CAP>
 struct ValuesSmem
@@ -91,13 +91,23 @@ struct ForcesSmem
     int queue[kQueue];
 };
 
-// Candidate pairs of one angular group, enumerated owner-major in phases:
+// Candidate pairs of one angular group, enumerated in phases:
 //   kind 0  circular: owner a in [0, nO), partner (a + 1 + t) mod nO, t < D
 //   kind 1  half-extra: owner a < nO / 2, partner a + nO / 2 (even nO, G pass)
 //   kind 2  rectangular: owner a in [0, nO), partner t in [0, D) of another block
+//   kind 3  tournament rounds over one block of nO slots (circle method on
+//           m = nO rounded up to even): round r < m - 1 pairs (m - 1, r) and
+//           ((r + i) mod (m - 1), (r - i) mod (m - 1)) for 0 < i < m / 2;
+//           slot m - 1 = nO (odd nO) is a bye
+//   kind 4  diagonal rounds over blocks nO <= D: round r < D pairs owner a
+//           with partner (a + r) mod D, a < nO
+// Kinds 0-2 are owner-major (G pass); in kinds 3 and 4 every round is a
+// matching -- no slot occurs twice in one round -- which the force pass uses to
+// add contributions without conflicts.  The cursor walks a major index a
+// (owner or round) and a minor index t < minor.
 struct Phase
 {
-    int kind, O0, nO, P0, D, count;
+    int kind, O0, nO, P0, D, count, minor;
 };
 
 // Lane-private decoding of candidate p = p0 + lane, advanced by 32 per step
@@ -107,15 +117,15 @@ struct Cursor
     int a, t;
     __device__ __forceinline__ void init(Phase const& ph, int lane)
     {
-        if (ph.kind == 1 || ph.D <= 0)
+        if (ph.kind == 1 || ph.minor <= 0)
         {
             a = lane;
             t = 0;
         }
         else
         {
-            a = lane / ph.D;
-            t = lane - a * ph.D;
+            a = lane / ph.minor;
+            t = lane - a * ph.minor;
         }
     }
     __device__ __forceinline__ void advance(Phase const& ph)
@@ -126,38 +136,74 @@ struct Cursor
             return;
         }
         t += 32;
-        while (t >= ph.D)
+        while (t >= ph.minor)
         {
-            t -= ph.D;
+            t -= ph.minor;
             ++a;
         }
     }
-    __device__ __forceinline__ void slots(Phase const& ph, int& so, int& sp) const
+    // Slots of the candidate; false for a bye.
+    __device__ __forceinline__ bool slots(Phase const& ph, int& so, int& sp) const
     {
+        if (ph.kind == 3)
+        {
+            const int m1 = ph.nO - 1 + (ph.nO & 1);
+            int u, v;
+            if (t == 0)
+            {
+                u = m1;
+                v = a;
+            }
+            else
+            {
+                u = a + t;
+                if (u >= m1) u -= m1;
+                v = a - t;
+                if (v < 0) v += m1;
+            }
+            so = ph.O0 + u;
+            sp = ph.O0 + v;
+            return u < ph.nO;
+        }
+        if (ph.kind == 4)
+        {
+            int q = t + a;
+            if (q >= ph.D) q -= ph.D;
+            so = ph.O0 + t;
+            sp = ph.P0 + q;
+            return true;
+        }
         so = ph.O0 + a;
         if (ph.kind == 0)
         {
-            int b = a + 1 + t;
-            if (b >= ph.nO) b -= ph.nO;
-            sp = ph.O0 + b;
+            int q = a + 1 + t;
+            if (q >= ph.nO) q -= ph.nO;
+            sp = ph.O0 + q;
         }
         else if (ph.kind == 1) sp = ph.O0 + a + ph.nO / 2;
         else sp = ph.P0 + t;
+        return true;
     }
+    // Round of the candidate (kinds 3, 4), 11 bits.
+    __device__ __forceinline__ int round(Phase const& ph) const { return ph.kind >= 3 ? (a & 0x7ff) : 0; }
 };
 
-// Test the next 32 candidates of a phase and append the accepted ones, in
-// candidate order, to the warp's queue (qn entries from q[0]).
+// Queue entries: round << 20 | owner slot << 10 | partner slot (slots < 1024).
+__device__ __forceinline__ int entryOwner(int e) { return (e >> 10) & 1023; }
+__device__ __forceinline__ int entryPartner(int e) { return e & 1023; }
+__device__ __forceinline__ int entryRound(int e) { return e >> 20; }
+
+// Test the next 64 candidates of a phase (two independent halves for
+// latency hiding) and append the accepted ones, in candidate order, to the
+// warp's ring queue (qn entries from q[qh]).
 template <typename T, int CAP, bool DF>
-__device__ __forceinline__ void enqueueCandidates(Stage<T, CAP, DF> const& S, Phase const& ph, Cursor& cur, int p0,
-                                                  T rc, T rc2, bool narrow, int* queue, int& qn, int lane)
+__device__ __forceinline__ bool testCandidate(Stage<T, CAP, DF> const& S, Phase const& ph, Cursor const& cur, int p,
+                                              T rc, T rc2, bool narrow, int& entry)
 {
-    const int p = p0 + lane;
-    bool ok = false;
     int so = 0, sp = 0;
-    if (p < ph.count)
+    bool ok = false;
+    if (p < ph.count && cur.slots(ph, so, sp))
     {
-        cur.slots(ph, so, sp);
         ok = S.r[so] < rc && S.r[sp] < rc;
         if (ok && narrow)
         {
@@ -165,21 +211,27 @@ __device__ __forceinline__ void enqueueCandidates(Stage<T, CAP, DF> const& S, Ph
             ok = (dx * dx + dy * dy + dz * dz) < rc2;
         }
     }
-    const unsigned m = __ballot_sync(kFullMask, ok);
-    if (ok) queue[qn + __popc(m & ((1u << lane) - 1u))] = (so << 16) | sp;
-    qn += __popc(m);
-    cur.advance(ph);
-    __syncwarp();
+    entry = (cur.round(ph) << 20) | (so << 10) | sp;
+    return ok;
 }
 
-// Drop the first `used` queue entries, keep the rest in order.
-__device__ __forceinline__ void shiftQueue(int* queue, int& qn, int used, int lane)
+template <typename T, int CAP, bool DF>
+__device__ __forceinline__ void enqueueCandidates(Stage<T, CAP, DF> const& S, Phase const& ph, Cursor& cur, int p0,
+                                                  T rc, T rc2, bool narrow, int* queue, int qh, int& qn, int lane)
 {
-    const int rest = qn - used;
-    int v = (lane < rest) ? queue[used + lane] : 0;
-    __syncwarp();
-    if (lane < rest) queue[lane] = v;
-    qn = rest;
+    Cursor c2 = cur;
+    c2.advance(ph);
+    int e1, e2;
+    const bool ok1 = testCandidate<T, CAP>(S, ph, cur, p0 + lane, rc, rc2, narrow, e1);
+    const bool ok2 = testCandidate<T, CAP>(S, ph, c2, p0 + 32 + lane, rc, rc2, narrow, e2);
+    const unsigned m1 = __ballot_sync(kFullMask, ok1);
+    const unsigned m2 = __ballot_sync(kFullMask, ok2);
+    const unsigned below = (1u << lane) - 1u;
+    if (ok1) queue[(qh + qn + __popc(m1 & below)) & (kQueue - 1)] = e1;
+    if (ok2) queue[(qh + qn + __popc(m1) + __popc(m2 & below)) & (kQueue - 1)] = e2;
+    qn += __popc(m1) + __popc(m2);
+    cur = c2;
+    cur.advance(ph);
     __syncwarp();
 }
 
@@ -193,22 +245,38 @@ __device__ __forceinline__ int groupPhases(int A0, int nA, int B0, int nB, bool 
         if (nA < 2) return 0;
         if (ordered)
         {
-            ph[n++] = Phase{0, A0, nA, A0, nA - 1, nA * (nA - 1)};
+            ph[n++] = Phase{0, A0, nA, A0, nA - 1, nA * (nA - 1), nA - 1};
         }
         else
         {
             const int hb = (nA - 1) / 2;
-            if (hb > 0) ph[n++] = Phase{0, A0, nA, A0, hb, nA * hb};
-            if ((nA & 1) == 0) ph[n++] = Phase{1, A0, nA, A0, 0, nA / 2};
+            if (hb > 0) ph[n++] = Phase{0, A0, nA, A0, hb, nA * hb, hb};
+            if ((nA & 1) == 0) ph[n++] = Phase{1, A0, nA, A0, 0, nA / 2, 0};
         }
     }
     else
     {
         if (nA == 0 || nB == 0) return 0;
-        ph[n++] = Phase{2, A0, nA, B0, nB, nA * nB};
-        if (ordered) ph[n++] = Phase{2, B0, nB, A0, nA, nA * nB};
+        ph[n++] = Phase{2, A0, nA, B0, nB, nA * nB, nB};
+        if (ordered) ph[n++] = Phase{2, B0, nB, A0, nA, nA * nB, nA};
     }
     return n;
+}
+
+// Force pass: the unordered pairs of a group as rounds of matchings.
+__device__ __forceinline__ int roundPhases(int A0, int nA, int B0, int nB, bool same, Phase* ph)
+{
+    if (same)
+    {
+        if (nA < 2) return 0;
+        const int m = nA + (nA & 1);
+        ph[0] = Phase{3, A0, nA, A0, 0, (m - 1) * (m / 2), m / 2};
+        return 1;
+    }
+    if (nA == 0 || nB == 0) return 0;
+    if (nA <= nB) ph[0] = Phase{4, A0, nA, B0, nB, nA * nB, nA};
+    else ph[0] = Phase{4, B0, nB, A0, nA, nA * nB, nB};
+    return 1;
 }
 
 // Neighbours of one atom into the stage, sorted by element (stable).
@@ -477,39 +545,6 @@ __device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Membe
     }
 }
 
-// h[.][key] += c for every lane with key >= 0.  Lanes with equal keys are
-// combined first, in increasing lane order, by the lowest of them, so every
-// slot is written by one lane and the sums do not depend on timing.
-template <int CAP>
-__device__ __forceinline__ void addByKey(double (*h)[CAP], int key, double cx, double cy, double cz, int lane)
-{
-    const unsigned peers = __match_any_sync(kFullMask, key);
-    const bool leader = key >= 0 && lane == __ffs(peers) - 1;
-    unsigned rest = leader ? (peers & (peers - 1u)) : 0u;
-    const unsigned iters = __reduce_max_sync(kFullMask, (unsigned)__popc(rest));
-    for (unsigned r = 0; r < iters; ++r)
-    {
-        const int src = rest ? __ffs(rest) - 1 : lane;
-        const double sx = __shfl_sync(kFullMask, cx, src);
-        const double sy = __shfl_sync(kFullMask, cy, src);
-        const double sz = __shfl_sync(kFullMask, cz, src);
-        if (rest)
-        {
-            cx += sx;
-            cy += sy;
-            cz += sz;
-            rest &= rest - 1u;
-        }
-    }
-    if (leader)
-    {
-        h[0][key] += cx;
-        h[1][key] += cy;
-        h[2][key] += cz;
-    }
-    __syncwarp();
-}
-
 } // namespace
 
 // ---------------------------------------------------------------------------
@@ -603,8 +638,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                     const int A0 = S.blockBegin[G.e1], nA = S.blockBegin[G.e1 + 1] - A0;
                     const int B0 = S.blockBegin[G.e2], nB = S.blockBegin[G.e2 + 1] - B0;
                     Phase ph[2];
-                    const int nph = groupPhases(A0, nA, B0, nB, same, false, ph);
-                    int qn = 0;
+                    const int nph = roundPhases(A0, nA, B0, nB, same, ph);
+                    int qn = 0, qh = 0;
                     for (int k = 0; k <= nph; ++k)
                     {
                         const bool drain = (k == nph);
@@ -618,18 +653,18 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                         int p0 = 0;
                         while (true)
                         {
-                            if (p0 < cnt)
+                            if (qn < 32 && p0 < cnt)   // queue stays below 32 + 64 entries
                             {
-                                enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qn, lane);
-                                p0 += 32;
+                                enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane);
+                                p0 += 64;
                             }
                             if (qn >= 32 || (drain && qn > 0))
                             {
                                 const int take = min(32, qn);
                                 if (lane < take)
                                 {
-                                    const int e = SM.queue[lane];
-                                    const int so = e >> 16, sp = e & 0xffff;
+                                    const int e = SM.queue[(qh + lane) & (kQueue - 1)];
+                                    const int so = entryOwner(e), sp = entryPartner(e);
                                     Triplet<T> t;
                                     loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
                                     const T pfc = t.fc1 * t.fc2 * t.fcjk;
@@ -658,7 +693,9 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                                         }
                                     }
                                 }
-                                shiftQueue(SM.queue, qn, take, lane);
+                                qh = (qh + take) & (kQueue - 1);
+                                qn -= take;
+                                __syncwarp();
                             }
                             else if (p0 >= cnt) break;
                         }
@@ -698,10 +735,10 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
 // T1 = sum a zeta lambda, T3 = sum a plambda,
 // Uij = sum a zeta lambda plambda factorDeriv (rij - rs)/rij  (Uik, Ujk alike).
 // The force E_i puts on j gains P1 dr_ij + P3 dr_jk, on k P2 dr_ik - P3 dr_jk;
-// the self force on i loses P1 dr_ij + P2 dr_ik.  Each pair is evaluated once;
-// its two contributions are summed per slot inside the warp batch (owner runs
-// by a segmented scan, then both sides by key) and added by one lane per slot
-// in a fixed order, without atomics.
+// the self force on i loses P1 dr_ij + P2 dr_ik.  Each pair is evaluated once.
+// Pairs are enumerated in rounds of matchings, so the lanes of one round add
+// their two contributions to distinct slots; rounds add one after another in
+// a fixed order (deterministic, no atomics).
 template <typename T, int CAP, int WARPS, int LOWER, int FAST>
 __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchView b)
 {
@@ -782,8 +819,8 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
             const int A0 = S.blockBegin[G.e1], nA = S.blockBegin[G.e1 + 1] - A0;
             const int B0 = S.blockBegin[G.e2], nB = S.blockBegin[G.e2 + 1] - B0;
             Phase ph[2];
-            const int nph = groupPhases(A0, nA, B0, nB, same, false, ph);
-            int qn = 0;
+            const int nph = roundPhases(A0, nA, B0, nB, same, ph);
+            int qn = 0, qh = 0;
             for (int k = 0; k <= nph; ++k)
             {
                 const bool drain = (k == nph);
@@ -797,20 +834,20 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                 int p0 = 0;
                 while (true)
                 {
-                    if (p0 < cnt)
+                    if (qn < 32 && p0 < cnt)   // queue stays below 32 + 64 entries
                     {
-                        enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qn, lane);
-                        p0 += 32;
+                        enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane);
+                        p0 += 64;
                     }
                     if (qn >= 32 || (drain && qn > 0))
                     {
                         const int take = min(32, qn);
-                        int keyO = -1 - lane, keyP = -1 - lane;   // inactive lanes never join a segment
+                        int keyO = 0, keyP = 0;
                         double ox = 0.0, oy = 0.0, oz = 0.0, px = 0.0, py = 0.0, pz = 0.0;
                         if (lane < take)
                         {
-                            const int e = SM.queue[lane];
-                            const int so = e >> 16, sp = e & 0xffff;
+                            const int e = SM.queue[(qh + lane) & (kQueue - 1)];
+                            const int so = entryOwner(e), sp = entryPartner(e);
                             keyO = so;
                             keyP = sp;
                             Triplet<T> t;
@@ -875,27 +912,29 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                             sfy -= (double)(P1 * t.y1 + P2 * t.y2);
                             sfz -= (double)(P1 * t.z1 + P2 * t.z2);
                         }
-                        // owners: runs of equal keys (owner-major order) first collapse to
-                        // their head lane; then both sides add into h by key.
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1)
+                        // One conflict-free add per round present in the batch: inside a
+                        // round no slot occurs twice.
+                        const int rnd = lane < take ? entryRound(SM.queue[(qh + lane) & (kQueue - 1)]) : -1;
+                        const int prevRnd = __shfl_up_sync(kFullMask, rnd, 1);
+                        const unsigned heads = __ballot_sync(kFullMask, lane < take && (lane == 0 || prevRnd != rnd));
+                        const int mySub = __popc(heads & ((2u << lane) - 1u)) - 1;
+                        const int nSub = __popc(heads);
+                        for (int r = 0; r < nSub; ++r)
                         {
-                            const double sx = __shfl_down_sync(kFullMask, ox, o);
-                            const double sy = __shfl_down_sync(kFullMask, oy, o);
-                            const double sz = __shfl_down_sync(kFullMask, oz, o);
-                            const int sk = __shfl_down_sync(kFullMask, keyO, o);
-                            if (lane + o < 32 && sk == keyO)
+                            if (lane < take && mySub == r)
                             {
-                                ox += sx;
-                                oy += sy;
-                                oz += sz;
+                                SM.h[0][keyO] += ox;
+                                SM.h[1][keyO] += oy;
+                                SM.h[2][keyO] += oz;
+                                SM.h[0][keyP] += px;
+                                SM.h[1][keyP] += py;
+                                SM.h[2][keyP] += pz;
                             }
+                            __syncwarp();
                         }
-                        const int prevKey = __shfl_up_sync(kFullMask, keyO, 1);
-                        if (lane > 0 && prevKey == keyO) keyO = -1 - lane;
-                        addByKey<CAP>(SM.h, keyO, ox, oy, oz, lane);
-                        addByKey<CAP>(SM.h, keyP, px, py, pz, lane);
-                        shiftQueue(SM.queue, qn, take, lane);
+                        qh = (qh + take) & (kQueue - 1);
+                        qn -= take;
+                        __syncwarp();
                     }
                     else if (p0 >= cnt) break;
                 }
