@@ -119,6 +119,9 @@ void structureGeometry(DevStructInfo& d, double rc)
     // periodic copies and plane spacings of the (normalised) box
     double proj[3];
     pbcCopies(d.box, rc, d.pbc, proj);
+    for (int a = 0; a < 3; ++a)
+        if (d.pbc[a] > 500)   // image offsets are packed in 10 bits by the search
+            throw std::range_error("ERROR: box too small for the cutoff radius (more than 500 periodic copies).\n");
     const int n = d.numAtoms;
     int64_t cells = 1;
     for (int a = 0; a < 3; ++a)
@@ -550,6 +553,7 @@ void Batch::allocateAtoms()
     v_.atomCell = devAlloc<int>(N, owned_);
     v_.atomSlot = devAlloc<int>(N, owned_);
     v_.cellAtoms = devAlloc<int>(N, owned_);
+    v_.cellPos = devAlloc<double4>(N, owned_);
     v_.nbrCount = devAlloc<int>(N, owned_);
     v_.nbrOffset = devAlloc<int64_t>((size_t)N + 1, owned_);
     v_.G = devAlloc<double>((size_t)N * stride, owned_);

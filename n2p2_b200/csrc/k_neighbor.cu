@@ -126,24 +126,48 @@ __global__ void kAssignCells(int N, const int* __restrict__ atomStruct, const De
     }
 }
 
+// Cell-ordered atom indices and positions (the position copy lets the search
+// read a cell's candidates with contiguous loads).
 __global__ void kScatterCells(int N, const int* __restrict__ atomCell, const int* __restrict__ atomSlot,
-                              const int* __restrict__ cellStart, int* __restrict__ cellAtoms)
+                              const int* __restrict__ cellStart, const double* __restrict__ px,
+                              const double* __restrict__ py, const double* __restrict__ pz,
+                              int* __restrict__ cellAtoms, double4* __restrict__ cellPos)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-        cellAtoms[cellStart[atomCell[i]] + atomSlot[i]] = i;
+    {
+        const int q = cellStart[atomCell[i]] + atomSlot[i];
+        cellAtoms[q] = i;
+        cellPos[q] = make_double4(px[i], py[i], pz[i], (double)i);
+    }
 }
 
 // One warp per centre atom.  PASS 0 counts, PASS 1 writes the unordered
-// candidates into the atom's segment of the scratch arrays.
+// candidates into the atom's segment of the scratch arrays.  The stencil cells
+// (with their periodic images) are tabulated in shared memory, kStencilChunk
+// at a time, with an exclusive scan of their atom counts; the warp then walks
+// the concatenated candidates 32 at a time (lane -> cell by binary search), so
+// every lane tests a candidate whatever the cell occupancy.
+constexpr int kStencilChunk = 128;
+constexpr int kSearchWarps = 8;
+
+struct StencilTable
+{
+    int start[kStencilChunk];
+    int pre[kStencilChunk + 1];
+    int code[kStencilChunk];      // (bc0 + 512) << 20 | (bc1 + 512) << 10 | (bc2 + 512)
+};
+
 template <int PASS>
-__global__ void __launch_bounds__(256) kNeighborSearch(
+__global__ void __launch_bounds__(kSearchWarps * 32) kNeighborSearch(
     int N, double rc2, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
     const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
     const int* __restrict__ atomCell, const int* __restrict__ cellStart, const int* __restrict__ cellCountArr,
-    const int* __restrict__ cellAtoms, int* __restrict__ nbrCount, const int64_t* __restrict__ nbrOffset,
+    const double4* __restrict__ cellPos, int* __restrict__ nbrCount, const int64_t* __restrict__ nbrOffset,
     int64_t capacity, int64_t* __restrict__ scrKey, double* __restrict__ scrD, double* __restrict__ scrDx,
     double* __restrict__ scrDy, double* __restrict__ scrDz, DevStatus* __restrict__ status)
 {
+    __shared__ StencilTable tables[kSearchWarps];
+    StencilTable& tab = tables[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warpsPerGrid)
@@ -155,6 +179,8 @@ __global__ void __launch_bounds__(256) kNeighborSearch(
         const int cy = (local / s.nc[2]) % s.nc[1];
         const int cx = local / (s.nc[2] * s.nc[1]);
         const int K = (2 * s.pbc[0] + 1) * (2 * s.pbc[1] + 1) * (2 * s.pbc[2] + 1);
+        const int nx = 2 * s.stencil[0] + 1, ny = 2 * s.stencil[1] + 1, nz = 2 * s.stencil[2] + 1;
+        const int numStencil = nx * ny * nz;
         int count = 0;
         int64_t base = 0, limit = 0;
         if (PASS == 1)
@@ -163,62 +189,99 @@ __global__ void __launch_bounds__(256) kNeighborSearch(
             limit = nbrOffset[i + 1];
             if (limit > capacity) limit = capacity;   // overflow is flagged by the host check
         }
-        for (int ox = -s.stencil[0]; ox <= s.stencil[0]; ++ox)
+        for (int c0 = 0; c0 < numStencil; c0 += kStencilChunk)
         {
-            int qx = cx + ox, tx = floorDiv(qx, s.nc[0]), wx = qx - tx * s.nc[0], bc0 = -tx;
-            if (bc0 < -s.pbc[0] || bc0 > s.pbc[0]) continue;
-            for (int oy = -s.stencil[1]; oy <= s.stencil[1]; ++oy)
+            __syncwarp();
+            int carry = 0;
+            for (int k0 = 0; k0 < kStencilChunk; k0 += 32)
             {
-                int qy = cy + oy, ty = floorDiv(qy, s.nc[1]), wy = qy - ty * s.nc[1], bc1 = -ty;
-                if (bc1 < -s.pbc[1] || bc1 > s.pbc[1]) continue;
-                for (int oz = -s.stencil[2]; oz <= s.stencil[2]; ++oz)
+                const int k = k0 + lane, o = c0 + k;
+                int cnt = 0, start = 0, code = 0;
+                if (o < numStencil)
                 {
-                    int qz = cz + oz, tz = floorDiv(qz, s.nc[2]), wz = qz - tz * s.nc[2], bc2 = -tz;
-                    if (bc2 < -s.pbc[2] || bc2 > s.pbc[2]) continue;
-                    const int cell = s.cellBegin + (wx * s.nc[1] + wy) * s.nc[2] + wz;
-                    const int cnt = cellCountArr[cell];
-                    const int start = cellStart[cell];
-                    for (int t0 = 0; t0 < cnt; t0 += 32)
+                    const int ox = o / (ny * nz) - s.stencil[0];
+                    const int oy = (o / nz) % ny - s.stencil[1];
+                    const int oz = o % nz - s.stencil[2];
+                    const int qx = cx + ox, tx = floorDiv(qx, s.nc[0]), wx = qx - tx * s.nc[0];
+                    const int qy = cy + oy, ty = floorDiv(qy, s.nc[1]), wy = qy - ty * s.nc[1];
+                    const int qz = cz + oz, tz = floorDiv(qz, s.nc[2]), wz = qz - tz * s.nc[2];
+                    const int bc0 = -tx, bc1 = -ty, bc2 = -tz;
+                    if (bc0 >= -s.pbc[0] && bc0 <= s.pbc[0] && bc1 >= -s.pbc[1] && bc1 <= s.pbc[1] &&
+                        bc2 >= -s.pbc[2] && bc2 <= s.pbc[2])
                     {
-                        const int t = t0 + lane;
-                        bool hit = false;
-                        double dx = 0, dy = 0, dz = 0, d2 = 0;
-                        int j = -1;
-                        if (t < cnt)
+                        const int cell = s.cellBegin + (wx * s.nc[1] + wy) * s.nc[2] + wz;
+                        cnt = cellCountArr[cell];
+                        start = cellStart[cell];
+                        code = ((bc0 + 512) << 20) | ((bc1 + 512) << 10) | (bc2 + 512);
+                    }
+                }
+                int incl = cnt;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1)
+                {
+                    const int y = __shfl_up_sync(kFullMask, incl, d);
+                    if (lane >= d) incl += y;
+                }
+                tab.start[k] = start;
+                tab.code[k] = code;
+                tab.pre[k] = carry + incl - cnt;
+                carry += __shfl_sync(kFullMask, incl, 31);
+            }
+            if (lane == 0) tab.pre[kStencilChunk] = carry;
+            __syncwarp();
+            const int total = carry;
+            for (int p0 = 0; p0 < total; p0 += 32)
+            {
+                const int p = p0 + lane;
+                bool hit = false;
+                double dx = 0, dy = 0, dz = 0, d2 = 0;
+                int j = -1, bc0 = 0, bc1 = 0, bc2 = 0;
+                if (p < total)
+                {
+                    int lo = 0, hi = kStencilChunk;   // pre[lo] <= p < pre[hi]
+#pragma unroll
+                    for (int it = 0; it < 7; ++it)
+                    {
+                        const int mid = (lo + hi) >> 1;
+                        if (tab.pre[mid] <= p) lo = mid;
+                        else hi = mid;
+                    }
+                    const int code = tab.code[lo];
+                    bc0 = (code >> 20) - 512;
+                    bc1 = ((code >> 10) & 1023) - 512;
+                    bc2 = (code & 1023) - 512;
+                    const double4 q = cellPos[tab.start[lo] + (p - tab.pre[lo])];
+                    j = (int)q.w;
+                    if (!(j == i && bc0 == 0 && bc1 == 0 && bc2 == 0))
+                    {
+                        dx = pairComponent(xi, q.x, s.box, 0, bc0, bc1, bc2);
+                        dy = pairComponent(yi, q.y, s.box, 1, bc0, bc1, bc2);
+                        dz = pairComponent(zi, q.z, s.box, 2, bc0, bc1, bc2);
+                        d2 = norm2Exact(dx, dy, dz);
+                        hit = (d2 <= rc2);
+                    }
+                }
+                if (PASS == 0)
+                {
+                    count += hit ? 1 : 0;
+                }
+                else
+                {
+                    const unsigned m = __ballot_sync(kFullMask, hit);
+                    const int pos = __popc(m & ((1u << lane) - 1u));
+                    if (hit)
+                    {
+                        const int64_t e = base + count + pos;
+                        if (e < limit)
                         {
-                            j = cellAtoms[start + t];
-                            if (!(j == i && bc0 == 0 && bc1 == 0 && bc2 == 0))
-                            {
-                                dx = pairComponent(xi, px[j], s.box, 0, bc0, bc1, bc2);
-                                dy = pairComponent(yi, py[j], s.box, 1, bc0, bc1, bc2);
-                                dz = pairComponent(zi, pz[j], s.box, 2, bc0, bc1, bc2);
-                                d2 = norm2Exact(dx, dy, dz);
-                                hit = (d2 <= rc2);
-                            }
-                        }
-                        if (PASS == 0)
-                        {
-                            count += hit ? 1 : 0;
-                        }
-                        else
-                        {
-                            unsigned m = __ballot_sync(kFullMask, hit);
-                            int pos = __popc(m & ((1u << lane) - 1u));
-                            if (hit)
-                            {
-                                int64_t e = base + count + pos;
-                                if (e < limit)
-                                {
-                                    scrKey[e] = (int64_t)(j - s.atomBegin) * K + imageCode(bc0, bc1, bc2, s.pbc);
-                                    scrD[e] = __dsqrt_rn(d2);
-                                    scrDx[e] = dx;
-                                    scrDy[e] = dy;
-                                    scrDz[e] = dz;
-                                }
-                            }
-                            count += __popc(m);
+                            scrKey[e] = (int64_t)(j - s.atomBegin) * K + imageCode(bc0, bc1, bc2, s.pbc);
+                            scrD[e] = __dsqrt_rn(d2);
+                            scrDx[e] = dx;
+                            scrDy[e] = dy;
+                            scrDz[e] = dz;
                         }
                     }
+                    count += __popc(m);
                 }
             }
         }
@@ -469,14 +532,17 @@ void launchNeighborBuild(BatchView const& b, double rc2, cudaStream_t st)
     launchExclusiveScan(b.numCells, b.cellCount, b.cellStart64, b.scanTmp, nullptr, st);
     kCast64to32<<<(b.numCells + 255) / 256 > 0 ? (b.numCells + 255) / 256 : 1, 256, 0, st>>>(b.numCells,
                                                                                           b.cellStart64, b.cellStart);
-    kScatterCells<<<blocks, 256, 0, st>>>(N, b.atomCell, b.atomSlot, b.cellStart, b.cellAtoms);
-    const int warpBlocks = (N + 7) / 8 > 0 ? (N + 7) / 8 : 1;
-    kNeighborSearch<0><<<warpBlocks, 256, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz, b.atomCell,
-                                                   b.cellStart, b.cellCount, b.cellAtoms, b.nbrCount, nullptr, 0,
+    kScatterCells<<<blocks, 256, 0, st>>>(N, b.atomCell, b.atomSlot, b.cellStart, b.px, b.py, b.pz, b.cellAtoms,
+                                          b.cellPos);
+    const int warpBlocks = (N + kSearchWarps - 1) / kSearchWarps > 0 ? (N + kSearchWarps - 1) / kSearchWarps : 1;
+    kNeighborSearch<0><<<warpBlocks, kSearchWarps * 32, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz,
+                                                   b.atomCell, b.cellStart, b.cellCount, b.cellPos, b.nbrCount,
+                                                   nullptr, 0,
                                                    nullptr, nullptr, nullptr, nullptr, nullptr, b.status);
     launchExclusiveScan(N, b.nbrCount, b.nbrOffset, b.scanTmp, &b.status->totalNeighbors, st);
-    kNeighborSearch<1><<<warpBlocks, 256, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz, b.atomCell,
-                                                   b.cellStart, b.cellCount, b.cellAtoms, nullptr, b.nbrOffset,
+    kNeighborSearch<1><<<warpBlocks, kSearchWarps * 32, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz,
+                                                   b.atomCell, b.cellStart, b.cellCount, b.cellPos, nullptr,
+                                                   b.nbrOffset,
                                                    b.nbrCapacity, b.scrKey, b.scrD, b.scrDx, b.scrDy, b.scrDz,
                                                    b.status);
     kNeighborSort<<<warpBlocks, 256, 0, st>>>(N, b.atomStruct, b.info, b.nbrOffset, b.nbrCapacity, b.scrKey, b.scrD,

@@ -30,6 +30,7 @@ struct BatchView
     int* cellStart = nullptr;
     int64_t* cellStart64 = nullptr;
     int* cellAtoms = nullptr;
+    double4* cellPos = nullptr;        // cell-ordered (x, y, z, atom index)
     int64_t* scanTmp = nullptr;
     // neighbour CSR
     int* nbrCount = nullptr;
