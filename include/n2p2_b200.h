@@ -54,6 +54,7 @@ typedef int n2p2_status;
 
 typedef struct n2p2_mode n2p2_mode;
 typedef struct n2p2_batch n2p2_batch;
+typedef struct n2p2_trainer n2p2_trainer;
 
 /* Message of the last failure on this thread ("" if none). */
 const char* n2p2_last_error(void);
@@ -225,6 +226,36 @@ n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches);
 n2p2_status n2p2_neighbor_list_noalloc(const double* positions, int64_t numAtoms, const double* box, double cutoff,
                                        int64_t capacity, int64_t* offsets, int32_t* index, int32_t* image,
                                        double* d, double* dr, int64_t* numEntries, void* stream);
+
+/* ---- training on energies and forces --------------------------------------
+ * The reference trains with nnp::Training (libnnptrain/Training.cpp) on the
+ * CPU; these entry points train a mode's networks on the GPU instead (used for
+ * the distilled student model): the loss
+ *   L = wE/S sum_s ((E_s - E_s^ref)/N_s)^2 + wF/(3N) sum_k |F_k - F_k^ref|^2
+ * in internal units, its exact gradient (through dE/dG for the force term)
+ * and Adam steps as in GradientDescent::update (GradientDescent.cpp:89-113).
+ * Supported networks: at most two hidden layers of <= 32 neurons, <= 128
+ * symmetry functions per element, activations l, t, s, p, no normalize_nodes
+ * (N2P2_ERR_INVALID_ARGUMENT otherwise).  The trainer updates the mode's
+ * device weights in place; evaluations of the mode's batches use them. */
+n2p2_status n2p2_trainer_create(n2p2_mode* mode, n2p2_trainer** trainer);
+n2p2_status n2p2_trainer_destroy(n2p2_trainer* trainer);
+/* Adam parameters (defaults 1e-3, 0.9, 0.999, 1e-8). */
+n2p2_status n2p2_trainer_set_adam(n2p2_trainer* trainer, double eta, double beta1, double beta2, double epsilon);
+/* Loss weights wE, wF (defaults 1, 10). */
+n2p2_status n2p2_trainer_set_loss_weights(n2p2_trainer* trainer, double energyWeight, double forceWeight);
+n2p2_status n2p2_trainer_get_num_parameters(n2p2_trainer* trainer, int64_t* count);
+/* All weights and biases, element by element in weight-file order
+ * (NeuralNetwork::setConnections, NeuralNetwork.cpp:147-169). */
+n2p2_status n2p2_trainer_get_parameters(n2p2_trainer* trainer, double* parameters);
+n2p2_status n2p2_trainer_set_parameters(n2p2_trainer* trainer, const double* parameters);
+/* Evaluates `batch` (a batch of the trainer's mode, positions set) with
+ * forces, computes the loss against energies[S] (physical units, with atomic
+ * energy offsets) and forces[N][3] (physical units) and, if `update`, takes
+ * one Adam step.  loss[3] = {total, energy term, force term} and the gradient
+ * (weight-file order) are written when the pointers are not NULL. */
+n2p2_status n2p2_trainer_step(n2p2_trainer* trainer, n2p2_batch* batch, const double* energies,
+                              const double* forces, int32_t update, double* loss, double* gradient);
 
 /* ---- instrumentation (no counterpart in the reference) ------------------- */
 

@@ -5,12 +5,12 @@ include/n2p2_b200.h; all evaluation runs in libn2p2b200.so (sm_100a).
 """
 from .structure import Structure, read_structures, write_structures  # noqa: F401
 
-__all__ = ["Structure", "read_structures", "write_structures", "Mode", "Prediction", "Batch"]
+__all__ = ["Structure", "read_structures", "write_structures", "Mode", "Prediction", "Batch", "Trainer"]
 
 
 def __getattr__(name):
     # The GPU classes load the shared library on first use.
-    if name in ("Mode", "Prediction", "Batch"):
+    if name in ("Mode", "Prediction", "Batch", "Trainer"):
         from . import mode
         return getattr(mode, name)
     raise AttributeError(name)

@@ -77,6 +77,14 @@ SIGNATURES = {
     "n2p2_batch_profile_stages": (_i, [_vp, _i, _i, _cp, _P(_d), _P(_i)]),
     "n2p2_batch_count_work": (_i, [_vp, _P(_i64)]),
     "n2p2_device_fma_peak": (_i, [_i, _P(_d), _P(_d)]),
+    "n2p2_trainer_create": (_i, [_vp, _P(_vp)]),
+    "n2p2_trainer_destroy": (_i, [_vp]),
+    "n2p2_trainer_set_adam": (_i, [_vp, _d, _d, _d, _d]),
+    "n2p2_trainer_set_loss_weights": (_i, [_vp, _d, _d]),
+    "n2p2_trainer_get_num_parameters": (_i, [_vp, _P(_i64)]),
+    "n2p2_trainer_get_parameters": (_i, [_vp, _P(_d)]),
+    "n2p2_trainer_set_parameters": (_i, [_vp, _P(_d)]),
+    "n2p2_trainer_step": (_i, [_vp, _vp, _P(_d), _P(_d), ctypes.c_int32, _P(_d), _P(_d)]),
     "n2p2_host_alloc": (_i, [_P(_vp), ctypes.c_size_t]),
     "n2p2_host_free": (_i, [_vp]),
 }

@@ -13,6 +13,7 @@
 
 #include "engine.hpp"
 #include "host_model.hpp"
+#include "trainer.hpp"
 
 using namespace n2p2b200;
 
@@ -28,6 +29,12 @@ struct n2p2_mode
     bool checkExtrapolation = false;
     bool writeWarnings = false;
     bool stopOnWarnings = false;
+};
+
+struct n2p2_trainer
+{
+    n2p2_mode* mode = nullptr;
+    std::unique_ptr<Trainer> trainer;
 };
 
 struct n2p2_batch
@@ -601,6 +608,93 @@ n2p2_status n2p2_device_fma_peak(int device, double* fp64Tflops, double* fp32Tfl
         if (fp64Tflops) *fp64Tflops = measureFmaPeak(1, p.multiProcessorCount);
         if (fp32Tflops) *fp32Tflops = measureFmaPeak(0, p.multiProcessorCount);
         cudaCheck(cudaGetLastError(), "fma probe");
+    });
+}
+
+n2p2_status n2p2_trainer_create(n2p2_mode* mode, n2p2_trainer** trainer)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(trainer);
+    return guard([&] {
+        ensureUploaded(mode);
+        auto t = std::make_unique<n2p2_trainer>();
+        t->mode = mode;
+        t->trainer = std::make_unique<Trainer>(mode->model, mode->dmodel, mode->sms);
+        *trainer = t.release();
+    });
+}
+
+n2p2_status n2p2_trainer_destroy(n2p2_trainer* trainer)
+{
+    if (!trainer) return N2P2_OK;
+    return guard([&] {
+        setDevice(trainer->mode);
+        delete trainer;
+    });
+}
+
+n2p2_status n2p2_trainer_set_adam(n2p2_trainer* trainer, double eta, double beta1, double beta2, double epsilon)
+{
+    N2P2_REQUIRE(trainer);
+    return guard([&] {
+        if (!(eta > 0.0) || !(beta1 >= 0.0 && beta1 < 1.0) || !(beta2 >= 0.0 && beta2 < 1.0) || !(epsilon > 0.0))
+            throw std::invalid_argument("ERROR: invalid Adam parameters.\n");
+        trainer->trainer->setAdam(eta, beta1, beta2, epsilon);
+    });
+}
+
+n2p2_status n2p2_trainer_set_loss_weights(n2p2_trainer* trainer, double energyWeight, double forceWeight)
+{
+    N2P2_REQUIRE(trainer);
+    return guard([&] {
+        if (!(energyWeight >= 0.0) || !(forceWeight >= 0.0))
+            throw std::invalid_argument("ERROR: loss weights must be non-negative.\n");
+        trainer->trainer->setLossWeights(energyWeight, forceWeight);
+    });
+}
+
+n2p2_status n2p2_trainer_get_num_parameters(n2p2_trainer* trainer, int64_t* count)
+{
+    N2P2_REQUIRE(trainer);
+    N2P2_REQUIRE(count);
+    return guard([&] { *count = trainer->trainer->numParameters(); });
+}
+
+n2p2_status n2p2_trainer_get_parameters(n2p2_trainer* trainer, double* parameters)
+{
+    N2P2_REQUIRE(trainer);
+    N2P2_REQUIRE(parameters);
+    return guard([&] {
+        setDevice(trainer->mode);
+        trainer->trainer->getParameters(parameters, trainer->mode->stream);
+    });
+}
+
+n2p2_status n2p2_trainer_set_parameters(n2p2_trainer* trainer, const double* parameters)
+{
+    N2P2_REQUIRE(trainer);
+    N2P2_REQUIRE(parameters);
+    return guard([&] {
+        setDevice(trainer->mode);
+        if (!trainer->mode->uploaded) throw std::runtime_error("ERROR: the mode was changed after the trainer was created.\n");
+        trainer->trainer->setParameters(parameters, trainer->mode->stream);
+        trainer->trainer->syncHostModel(trainer->mode->stream);
+    });
+}
+
+n2p2_status n2p2_trainer_step(n2p2_trainer* trainer, n2p2_batch* batch, const double* energies,
+                              const double* forces, int32_t update, double* loss, double* gradient)
+{
+    N2P2_REQUIRE(trainer);
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(energies);
+    N2P2_REQUIRE(forces);
+    return guard([&] {
+        setDevice(trainer->mode);
+        if (batch->mode != trainer->mode) throw std::invalid_argument("ERROR: batch belongs to another mode.\n");
+        if (!trainer->mode->uploaded) throw std::runtime_error("ERROR: the mode was changed after the trainer was created.\n");
+        trainer->trainer->step(*batch->batch, energies, forces, update != 0, loss, gradient);
+        if (update) trainer->trainer->syncHostModel(trainer->mode->stream);
     });
 }
 

@@ -35,21 +35,71 @@ void setDynamicSmemOnce(const void* kernel, size_t bytes)
     done.insert(key);
 }
 
+// Size classes: 256-byte steps up to 64 KiB, then quarter steps between
+// powers of two (at most 25 % slack).
+static size_t poolBucket(size_t bytes)
+{
+    if (bytes <= 65536) return (bytes + 255) & ~(size_t)255;
+    size_t p = 65536;
+    while (p * 2 < bytes) p *= 2;
+    const size_t q = p / 4;
+    return ((bytes + q - 1) / q) * q;
+}
+
+DevicePool::~DevicePool() { trim(); }
+
+void* DevicePool::get(size_t bytes)
+{
+    const size_t b = poolBucket(bytes);
+    auto it = free_.find(b);
+    if (it != free_.end() && !it->second.empty())
+    {
+        void* p = it->second.back();
+        it->second.pop_back();
+        return p;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        trim();
+        cudaCheck(cudaMalloc(&p, b), "cudaMalloc");
+    }
+    size_[p] = b;
+    return p;
+}
+
+void DevicePool::put(void* p)
+{
+    if (p) free_[size_.at(p)].push_back(p);
+}
+
+void DevicePool::trim()
+{
+    for (auto& kv : free_)
+        for (void* p : kv.second)
+        {
+            cudaFree(p);
+            size_.erase(p);
+        }
+    free_.clear();
+}
+
 namespace {
 
 template <typename T>
-T* devAlloc(size_t count, std::vector<void*>& owned)
+T* devAlloc(DevicePool& pool, size_t count, std::vector<void*>& owned)
 {
-    void* p = nullptr;
     if (count == 0) count = 1;
-    cudaCheck(cudaMalloc(&p, sizeof(T) * count), "cudaMalloc");
+    void* p = pool.get(sizeof(T) * count);
     owned.push_back(p);
     return static_cast<T*>(p);
 }
 
-void freeAll(std::vector<void*>& owned)
+void freeAll(DevicePool& pool, std::vector<void*>& owned)
 {
-    for (void* p : owned) cudaFree(p);
+    for (void* p : owned) pool.put(p);
     owned.clear();
 }
 
@@ -407,6 +457,7 @@ void DeviceModel::upload(Model const& m)
     v.scaling = scaling_;
     v.rowTable = rowTable_;
     v.weights = weights_;
+    numWeights = weights.size();
     v.weightsF = weightsF_;
     view = v;
     this->maxSF = maxSF;
@@ -421,7 +472,11 @@ Batch::Batch(Model const& model, DeviceModel const& dmodel, cudaStream_t stream,
 {
 }
 
-Batch::~Batch() { releaseAll(); }
+Batch::~Batch()
+{
+    releaseAll();
+    pool_.trim();
+}
 
 void Batch::releaseGraph()
 {
@@ -433,9 +488,9 @@ void Batch::releaseGraph()
 void Batch::releaseAll()
 {
     releaseGraph();
-    freeAll(ownedDGdr_);
-    freeAll(ownedNbr_);
-    freeAll(owned_);
+    freeAll(pool_, ownedDGdr_);
+    freeAll(pool_, ownedNbr_);
+    freeAll(pool_, owned_);
     dgdrAllocated_ = false;
 }
 
@@ -509,10 +564,10 @@ void Batch::setStructures(std::vector<StructureInput> const& s, const int* eleme
 
     allocateAtoms();
     v_.numCells = cellTotal;
-    v_.cellCount = devAlloc<int>(cellTotal, owned_);
-    v_.cellStart = devAlloc<int>(cellTotal, owned_);
-    v_.cellStart64 = devAlloc<int64_t>(cellTotal + 1, owned_);
-    v_.scanTmp = devAlloc<int64_t>(std::max(scanTileCount(cellTotal), scanTileCount(N_)) + 8, owned_);
+    v_.cellCount = devAlloc<int>(pool_, cellTotal, owned_);
+    v_.cellStart = devAlloc<int>(pool_, cellTotal, owned_);
+    v_.cellStart64 = devAlloc<int64_t>(pool_, cellTotal + 1, owned_);
+    v_.scanTmp = devAlloc<int64_t>(pool_, std::max(scanTileCount(cellTotal), scanTileCount(N_)) + 8, owned_);
     cudaCheck(cudaMemcpyAsync(infoDev_, info.data(), sizeof(DevStructInfo) * S_, cudaMemcpyHostToDevice, stream_),
               "upload structure info");
     std::vector<int> atomStruct(N_);
@@ -538,62 +593,68 @@ void Batch::allocateAtoms()
     v_.N = N;
     v_.S = S_;
     v_.gStride = stride;
-    infoDev_ = devAlloc<DevStructInfo>(S_, owned_);
-    atomStructDev_ = devAlloc<int>(N, owned_);
-    elemDev_ = devAlloc<int>(N, owned_);
-    structBeginDev_ = devAlloc<int>(S_ + 1, owned_);
-    rin_ = devAlloc<double>(3 * (size_t)N, owned_);
+    infoDev_ = devAlloc<DevStructInfo>(pool_, S_, owned_);
+    atomStructDev_ = devAlloc<int>(pool_, N, owned_);
+    elemDev_ = devAlloc<int>(pool_, N, owned_);
+    structBeginDev_ = devAlloc<int>(pool_, S_ + 1, owned_);
+    rin_ = devAlloc<double>(pool_, 3 * (size_t)N, owned_);
     v_.info = infoDev_;
     v_.atomStruct = atomStructDev_;
     v_.elem = elemDev_;
     v_.structAtomBegin = structBeginDev_;
-    v_.px = devAlloc<double>(N, owned_);
-    v_.py = devAlloc<double>(N, owned_);
-    v_.pz = devAlloc<double>(N, owned_);
-    v_.atomCell = devAlloc<int>(N, owned_);
-    v_.atomSlot = devAlloc<int>(N, owned_);
-    v_.cellAtoms = devAlloc<int>(N, owned_);
-    v_.cellPos = devAlloc<double4>(N, owned_);
-    v_.nbrCount = devAlloc<int>(N, owned_);
-    v_.nbrOffset = devAlloc<int64_t>((size_t)N + 1, owned_);
-    v_.G = devAlloc<double>((size_t)N * stride, owned_);
-    v_.dEdG = devAlloc<double>((size_t)N * stride, owned_);
-    v_.Eatom = devAlloc<double>(N, owned_);
-    v_.Estruct = devAlloc<double>(S_, owned_);
-    v_.fSelf = devAlloc<double>(3 * (size_t)N, owned_);
-    v_.F = devAlloc<double>(3 * (size_t)N, owned_);
-    v_.atomWarnings = devAlloc<int>(N, owned_);
-    v_.status = devAlloc<DevStatus>(1, owned_);
+    v_.px = devAlloc<double>(pool_, N, owned_);
+    v_.py = devAlloc<double>(pool_, N, owned_);
+    v_.pz = devAlloc<double>(pool_, N, owned_);
+    v_.atomCell = devAlloc<int>(pool_, N, owned_);
+    v_.atomSlot = devAlloc<int>(pool_, N, owned_);
+    v_.cellAtoms = devAlloc<int>(pool_, N, owned_);
+    v_.cellPos = devAlloc<double4>(pool_, N, owned_);
+    v_.nbrCount = devAlloc<int>(pool_, N, owned_);
+    v_.nbrOffset = devAlloc<int64_t>(pool_, (size_t)N + 1, owned_);
+    v_.G = devAlloc<double>(pool_, (size_t)N * stride, owned_);
+    v_.dEdG = devAlloc<double>(pool_, (size_t)N * stride, owned_);
+    v_.Eatom = devAlloc<double>(pool_, N, owned_);
+    v_.Estruct = devAlloc<double>(pool_, S_, owned_);
+    v_.fSelf = devAlloc<double>(pool_, 3 * (size_t)N, owned_);
+    v_.F = devAlloc<double>(pool_, 3 * (size_t)N, owned_);
+    v_.atomWarnings = devAlloc<int>(pool_, N, owned_);
+    v_.status = devAlloc<DevStatus>(pool_, 1, owned_);
+    // Pool blocks hold a previous user's data: clear what may be read before
+    // the first evaluation writes it.
     cudaCheck(cudaMemsetAsync(v_.G, 0, sizeof(double) * (size_t)N * stride, stream_), "memset");
     cudaCheck(cudaMemsetAsync(v_.dEdG, 0, sizeof(double) * (size_t)N * stride, stream_), "memset");
+    cudaCheck(cudaMemsetAsync(v_.status, 0, sizeof(DevStatus), stream_), "memset");
+    cudaCheck(cudaMemsetAsync(v_.atomWarnings, 0, sizeof(int) * (size_t)N, stream_), "memset");
+    cudaCheck(cudaMemsetAsync(v_.Estruct, 0, sizeof(double) * (size_t)S_, stream_), "memset");
+    cudaCheck(cudaMemsetAsync(v_.F, 0, sizeof(double) * 3 * (size_t)N, stream_), "memset");
 }
 
 void Batch::allocateNeighbors(int64_t capacity)
 {
     releaseGraph();
-    freeAll(ownedDGdr_);
+    freeAll(pool_, ownedDGdr_);
     dgdrAllocated_ = false;
-    freeAll(ownedNbr_);
+    freeAll(pool_, ownedNbr_);
     const int slots = std::max(1, dmodel_.view.numCutoffSlots);
     capacity_ = capacity;
     v_.nbrCapacity = capacity;
-    v_.scrKey = devAlloc<int64_t>(capacity, ownedNbr_);
-    v_.scrD = devAlloc<double>(capacity, ownedNbr_);
-    v_.scrDx = devAlloc<double>(capacity, ownedNbr_);
-    v_.scrDy = devAlloc<double>(capacity, ownedNbr_);
-    v_.scrDz = devAlloc<double>(capacity, ownedNbr_);
-    v_.nbrJ = devAlloc<int>(capacity, ownedNbr_);
-    v_.nbrCode = devAlloc<int>(capacity, ownedNbr_);
-    v_.nbrD = devAlloc<double>(capacity, ownedNbr_);
-    v_.nbrDx = devAlloc<double>(capacity, ownedNbr_);
-    v_.nbrDy = devAlloc<double>(capacity, ownedNbr_);
-    v_.nbrDz = devAlloc<double>(capacity, ownedNbr_);
-    v_.rev = devAlloc<int64_t>(capacity, ownedNbr_);
-    v_.nbrFc = devAlloc<double>((size_t)slots * capacity, ownedNbr_);
-    v_.nbrDfc = devAlloc<double>((size_t)slots * capacity, ownedNbr_);
-    v_.hx = devAlloc<double>(capacity, ownedNbr_);
-    v_.hy = devAlloc<double>(capacity, ownedNbr_);
-    v_.hz = devAlloc<double>(capacity, ownedNbr_);
+    v_.scrKey = devAlloc<int64_t>(pool_, capacity, ownedNbr_);
+    v_.scrD = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.scrDx = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.scrDy = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.scrDz = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.nbrJ = devAlloc<int>(pool_, capacity, ownedNbr_);
+    v_.nbrCode = devAlloc<int>(pool_, capacity, ownedNbr_);
+    v_.nbrD = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.nbrDx = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.nbrDy = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.nbrDz = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.rev = devAlloc<int64_t>(pool_, capacity, ownedNbr_);
+    v_.nbrFc = devAlloc<double>(pool_, (size_t)slots * capacity, ownedNbr_);
+    v_.nbrDfc = devAlloc<double>(pool_, (size_t)slots * capacity, ownedNbr_);
+    v_.hx = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.hy = devAlloc<double>(pool_, capacity, ownedNbr_);
+    v_.hz = devAlloc<double>(pool_, capacity, ownedNbr_);
     v_.dGdr = nullptr;
     v_.dGdrSelf = nullptr;
 }
@@ -603,8 +664,8 @@ void Batch::allocateDGdr()
     if (dgdrAllocated_) return;
     releaseGraph();
     const int rows = std::max(1, dmodel_.view.maxRows);
-    v_.dGdr = devAlloc<double>((size_t)rows * capacity_ * 3, ownedDGdr_);
-    v_.dGdrSelf = devAlloc<double>((size_t)N_ * v_.gStride * 3, ownedDGdr_);
+    v_.dGdr = devAlloc<double>(pool_, (size_t)rows * capacity_ * 3, ownedDGdr_);
+    v_.dGdrSelf = devAlloc<double>(pool_, (size_t)N_ * v_.gStride * 3, ownedDGdr_);
     cudaCheck(cudaMemsetAsync(v_.dGdrSelf, 0, sizeof(double) * (size_t)N_ * v_.gStride * 3, stream_), "memset");
     dgdrAllocated_ = true;
 }
@@ -809,6 +870,24 @@ void Batch::energies(double* out)
             E += numAtomsPerElement_[(size_t)k * ne + q] * model_.elements[q].atomicEnergyOffset;
         out[k] = E;
     }
+}
+
+void Batch::energiesToInternal(const double* phys, double* out) const
+{
+    const int ne = (int)model_.numElements();
+    for (int k = 0; k < S_; ++k)
+    {
+        double E = phys[k];
+        for (int q = 0; q < ne; ++q)
+            E -= numAtomsPerElement_[(size_t)k * ne + q] * model_.elements[q].atomicEnergyOffset;
+        if (model_.normalize) E = (E - structs_[k].numAtoms * model_.meanEnergy) * model_.convEnergy;
+        out[k] = E;
+    }
+}
+
+double Batch::forceToInternal() const
+{
+    return model_.normalize ? model_.convEnergy / model_.convLength : 1.0;
 }
 
 void Batch::forces(double* out)

@@ -3,7 +3,9 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -25,6 +27,23 @@ enum EvalFlags : int {
 
 void cudaCheck(cudaError_t e, char const* what);
 
+// Device memory cache of one batch: blocks given back by put() are handed out
+// again for requests of the same size class, so re-setting structures of
+// similar size allocates nothing.  Every user of a batch's memory works on
+// the batch's stream, so reuse is ordered after the previous users.
+class DevicePool
+{
+public:
+    ~DevicePool();
+    void* get(size_t bytes);
+    void put(void* p);
+    void trim();   // cudaFree every cached block
+
+private:
+    std::map<size_t, std::vector<void*>> free_;
+    std::unordered_map<void*, size_t> size_;
+};
+
 // Device copy of a set-up model.
 class DeviceModel
 {
@@ -33,6 +52,9 @@ public:
     void upload(Model const& m);
     DevModel view;
     int maxSF = 0;
+    size_t numWeights = 0;               // entries of the flat weight array
+    double* weightsDevice() const { return weights_; }
+    float* weightsFDevice() const { return weightsF_; }
 
 private:
     void release();
@@ -69,6 +91,11 @@ public:
     void evaluate(int flags, int precision, int checkExtrapolation);
     // Host-side results (synchronise first).
     void energies(double* out);       // physical units, with atomic energy offsets
+    // Inverse of the conversions of energies() / forces(): physical energies
+    // (with offsets) to internal network sums, and the factor that takes
+    // physical forces to internal ones.
+    void energiesToInternal(const double* phys, double* out) const;
+    double forceToInternal() const;
     void forces(double* out);         // physical units, [N][3]
     void synchronize();
     DevStatus status();
@@ -111,6 +138,11 @@ private:
 
     Model const& model_;
     DeviceModel const& dmodel_;
+public:
+    Model const& model() const { return model_; }
+    DeviceModel const& deviceModel() const { return dmodel_; }
+    std::vector<int> const& structBegin() const { return structBegin_; }
+private:
     cudaStream_t stream_;
     int sms_;
     int N_ = 0, S_ = 0;
@@ -131,6 +163,7 @@ private:
     cudaGraphExec_t graphExec_ = nullptr;
     int graphKey_ = -1;
     int launches_ = 0;
+    DevicePool pool_;
     std::vector<void*> owned_;
     std::vector<void*> ownedNbr_;
     std::vector<void*> ownedDGdr_;

@@ -318,6 +318,59 @@ class Batch:
         return n.value
 
 
+class Trainer:
+    """Device training of a mode's networks on energies and forces (the
+    distilled-student path; the reference's CPU counterpart is nnp::Training).
+    Parameters are exchanged in weight-file order, element by element."""
+
+    def __init__(self, mode, eta=1e-3, beta1=0.9, beta2=0.999, epsilon=1e-8, energyWeight=1.0, forceWeight=10.0):
+        self._mode = mode
+        self._lib = mode._lib
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.n2p2_trainer_create(mode._h, ctypes.byref(h)))
+        self._h = h
+        _lib.check(self._lib.n2p2_trainer_set_adam(self._h, eta, beta1, beta2, epsilon))
+        _lib.check(self._lib.n2p2_trainer_set_loss_weights(self._h, energyWeight, forceWeight))
+        n = ctypes.c_int64()
+        _lib.check(self._lib.n2p2_trainer_get_num_parameters(self._h, ctypes.byref(n)))
+        self.numParameters = n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.n2p2_trainer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def parameters(self):
+        out = np.zeros(self.numParameters)
+        _lib.check(self._lib.n2p2_trainer_get_parameters(self._h, _dp(out)))
+        return out
+
+    def setParameters(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        if w.size != self.numParameters:
+            raise ValueError("expected %d parameters" % self.numParameters)
+        _lib.check(self._lib.n2p2_trainer_set_parameters(self._h, _dp(w)))
+
+    def step(self, batch, energies, forces, update=True, gradient=False):
+        """Loss (total, energy term, force term) of `batch` against physical-unit
+        labels; an Adam step if `update`; the gradient too if `gradient`."""
+        e = np.ascontiguousarray(energies, dtype=np.float64)
+        f = np.ascontiguousarray(forces, dtype=np.float64)
+        if e.size != batch.numStructures or f.size != 3 * batch.numAtoms:
+            raise ValueError("labels do not match the batch")
+        loss = np.zeros(3)
+        g = np.zeros(self.numParameters) if gradient else None
+        _lib.check(self._lib.n2p2_trainer_step(self._h, batch._h, _dp(e), _dp(f), int(bool(update)), _dp(loss),
+                                               _dp(g) if g is not None else None))
+        return (loss, g) if gradient else loss
+
+
 class Prediction(Mode):
     """nnp::Prediction (Prediction.cpp:27-78): a Mode plus one Structure."""
 

@@ -1,0 +1,300 @@
+"""Distilled student HDNNP: a reduced descriptor (8 radial G2 + 6 angular G3
+per element) and a 14-16-16-1 softplus network, trained on the GPU by the
+library's own kernels (n2p2_trainer_*) on energies and forces that the full
+HDNNP (the teacher) computes, and evaluated with the teacher as fallback.
+
+The student is an ordinary n2p2 model directory (input.nn, scaling.data,
+weights.%03d.data), so the same engine evaluates it.  Evaluation follows the
+reference's extrapolation check (SymFnc scaling range, Mode.cpp:1172-1210):
+every structure in which any student symmetry function leaves its scaling
+range is re-evaluated by the teacher.  A small held-out sample of every
+evaluation batch is also run through the teacher and the student's error on
+it is recorded.
+
+    python -m n2p2_b200.student train --teacher tests/golden/models/water56 --out student_dir
+"""
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import water
+
+HA_TO_MEV = 27211.386245988
+BOHR_TO_A = 0.529177210903
+
+STUDENT_G2_ETAS = (0.001, 0.01, 0.06, 0.3)     # x {H, O} neighbours = 8 radial
+STUDENT_G3_ETA = 0.01                          # x {HH, HO, OO} x lambda +-1 = 6 angular
+STUDENT_G3_ZETA = 1.0
+STUDENT_NODES = (16, 16)
+
+
+def student_sf_lines(rc=water.RC, rc_angular=None):
+    rca = rc if rc_angular is None else rc_angular
+    out = []
+    for ec in ("H", "O"):
+        for e1 in ("H", "O"):
+            for eta in STUDENT_G2_ETAS:
+                out.append(f"symfunction_short {ec} 2 {e1} {eta:.6g} 0.0 {rc:.6g}")
+        for e1, e2 in (("H", "H"), ("H", "O"), ("O", "O")):
+            for lam in (-1.0, 1.0):
+                out.append(f"symfunction_short {ec} 3 {e1} {e2} {STUDENT_G3_ETA:.6g} {lam:.0f} "
+                           f"{STUDENT_G3_ZETA:.6g} {rca:.6g}")
+    return out
+
+
+def training_structures(num, seed, n_min=64, n_max=512, sigma_range=(0.05, 0.4)):
+    """Water boxes of 192-1536 atoms with Gaussian displacements sigma in the range."""
+    return water.water_batch(num, seed, n_min=n_min, n_max=n_max, sigma_range=sigma_range)
+
+
+def _positions(structs):
+    return np.ascontiguousarray(np.concatenate([s.positions for s in structs]))
+
+
+def label(mode, structs, chunk=512):
+    """Energies [S] and forces [N,3] (physical units) of `structs` by `mode`."""
+    E, F = [], []
+    b = None
+    for c0 in range(0, len(structs), chunk):
+        sub = structs[c0:c0 + chunk]
+        if b is None:
+            b = mode.batch(sub)
+        else:
+            b.setStructures(sub)
+        b.setPositions(_positions(sub))
+        b.evaluate(forces=True, graph=False)
+        E.append(b.energies())
+        F.append(b.forces())
+    return np.concatenate(E), np.concatenate(F)
+
+
+def write_student_model(directory, scaling_structs, seed=7, device=0, rc=water.RC, rc_angular=None):
+    """input.nn + N(0, 1/fan_in) weights + scaling.data of the student's
+    symmetry functions over `scaling_structs` (evaluated on the GPU)."""
+    from .mode import Mode
+    os.makedirs(directory, exist_ok=True)
+    lines = student_sf_lines(rc, rc_angular)
+    with open(os.path.join(directory, "input.nn"), "w") as f:
+        f.write(water.input_nn_text(lines, nodes=STUDENT_NODES, activations="p p l",
+                                    comment="distilled student: 8 G2 + 6 G3 per element, 14-16-16-1 softplus"))
+    rng = np.random.default_rng(seed)
+    nsf = len(lines) // 2
+    for Z in (1, 8):
+        water.write_weights(os.path.join(directory, "weights.%03d.data" % Z),
+                            water.random_weights((nsf,) + STUDENT_NODES + (1,), rng))
+    m = Mode(device)
+    m.initialize()
+    m.loadSettingsFile(os.path.join(directory, "input.nn"))
+    m.setupGeneric()
+    m.setupSymmetryFunctionScalingNone()
+    m.setupNeuralNetworkWeights(os.path.join(directory, "weights.%03zu.data"))
+    ne = m.numElements
+    nsf = np.array([m.numSymmetryFunctions(e) for e in range(ne)])
+    per_el = [[] for _ in range(ne)]
+    b = None
+    for c0 in range(0, len(scaling_structs), 512):
+        sub = scaling_structs[c0:c0 + 512]
+        if b is None:
+            b = m.batch(sub)
+        else:
+            b.setStructures(sub)
+        b.setPositions(_positions(sub))
+        b.evaluate(forces=False, graph=False)
+        G = b.symmetryFunctions()
+        off = np.concatenate([[0], np.cumsum(nsf[b.elements])])
+        for e in range(ne):
+            rows = np.nonzero(b.elements == e)[0]
+            per_el[e].append(G[off[rows][:, None] + np.arange(nsf[e])[None, :]])
+    stats = water.scaling_statistics([np.concatenate(x) for x in per_el])
+    water.write_scaling(os.path.join(directory, "scaling.data"), stats)
+    m.close()
+    return directory
+
+
+def write_trained_weights(directory, mode, parameters):
+    """Weight files of the mode's elements from a parameter vector in file order."""
+    pos = 0
+    for e in range(mode.numElements):
+        nsf = mode.numSymmetryFunctions(e)
+        sizes = (nsf,) + STUDENT_NODES + (1,)
+        n = sum(sizes[l] * sizes[l - 1] + sizes[l] for l in range(1, len(sizes)))
+        Z = {"H": 1, "O": 8}[mode.elementSymbol(e)]
+        water.write_weights(os.path.join(directory, "weights.%03d.data" % Z), parameters[pos:pos + n])
+        pos += n
+
+
+def load_mode(directory, device=0, extrapolation=False, precision="fp64"):
+    from .mode import Mode
+    m = Mode(device)
+    m.setupFromDirectory(directory)
+    if extrapolation:
+        m.setupSymmetryFunctionStatistics(False, True, False, False)
+    m.setPrecision(precision)
+    return m
+
+
+class StudentTraining:
+    """Mini-batch Adam training of the student on teacher labels."""
+
+    def __init__(self, student_mode, structs, energies, forces, batch_size=64, eta=1e-3, force_weight=10.0,
+                 seed=0):
+        from .mode import Trainer
+        self.mode = student_mode
+        self.structs = structs
+        self.E = np.asarray(energies)
+        self.atom_begin = np.concatenate([[0], np.cumsum([s.numAtoms for s in structs])])
+        self.F = np.asarray(forces).reshape(-1, 3)
+        self.batch_size = batch_size
+        self.rng = np.random.default_rng(seed)
+        self.trainer = Trainer(student_mode, eta=eta, forceWeight=force_weight)
+        self.batch = None
+        self.history = []
+
+    def _set(self, idx):
+        sub = [self.structs[k] for k in idx]
+        if self.batch is None:
+            self.batch = self.mode.batch(sub)
+        else:
+            self.batch.setStructures(sub)
+        self.batch.setPositions(_positions(sub))
+        e = self.E[idx]
+        f = np.concatenate([self.F[self.atom_begin[k]:self.atom_begin[k + 1]] for k in idx])
+        return e, f
+
+    def step(self, idx, update=True, gradient=False):
+        e, f = self._set(idx)
+        return self.trainer.step(self.batch, e, f, update=update, gradient=gradient)
+
+    def epoch(self):
+        order = self.rng.permutation(len(self.structs))
+        losses = []
+        for b0 in range(0, len(order) - self.batch_size + 1, self.batch_size):
+            losses.append(self.step(order[b0:b0 + self.batch_size])[0])
+        self.history.append(float(np.mean(losses)))
+        return self.history[-1]
+
+
+def errors(E, F, E_ref, F_ref, atoms_per_structure):
+    """Energy error per atom (meV/atom) and per-component force error (meV/A)."""
+    de = np.abs(np.asarray(E) - np.asarray(E_ref)) / np.asarray(atoms_per_structure) * HA_TO_MEV
+    df = np.abs(np.asarray(F) - np.asarray(F_ref)).ravel() * HA_TO_MEV / BOHR_TO_A
+    return {"energy_meV_per_atom_rms": float(np.sqrt(np.mean(de ** 2))), "energy_meV_per_atom_max": float(de.max()),
+            "force_meV_per_A_rms": float(np.sqrt(np.mean(df ** 2))), "force_meV_per_A_max": float(df.max())}
+
+
+class StudentEvaluator:
+    """Student evaluation of a batch with teacher fallback and a held-out monitor."""
+
+    def __init__(self, student_mode, teacher_mode, structs, monitor=2, seed=0):
+        self.student = student_mode
+        self.teacher = teacher_mode
+        self.structs = structs
+        self.batch = student_mode.batch(structs)
+        self.pos = _positions(structs)
+        self.batch.setPositions(self.pos)
+        self.atom_begin = np.concatenate([[0], np.cumsum([s.numAtoms for s in structs])])
+        self.monitor = monitor
+        self.rng = np.random.default_rng(seed)
+        self.fallback_batch = None
+        self.monitor_batch = None
+        self.monitor_log = []
+        self.fallbacks = 0
+        self.evaluations = 0
+
+    def evaluate(self):
+        """Energies [S] and forces [N,3]: student, or teacher where the
+        student's extrapolation check fired."""
+        b = self.batch
+        b.evaluate(forces=True)
+        E = b.energies()
+        F = b.forces()
+        _, per_atom = b.extrapolationWarnings()
+        flagged = np.add.reduceat(per_atom, self.atom_begin[:-1]) > 0
+        self.evaluations += len(self.structs)
+        idx = np.nonzero(flagged)[0]
+        if idx.size:
+            self.fallbacks += idx.size
+            sub = [self.structs[k] for k in idx]
+            if self.fallback_batch is None:
+                self.fallback_batch = self.teacher.batch(sub)
+            else:
+                self.fallback_batch.setStructures(sub)
+            self.fallback_batch.setPositions(_positions(sub))
+            self.fallback_batch.evaluate(forces=True, graph=False)
+            Et, Ft = self.fallback_batch.energies(), self.fallback_batch.forces()
+            E[idx] = Et
+            a = 0
+            for k in idx:
+                n = self.structs[k].numAtoms
+                F[self.atom_begin[k]:self.atom_begin[k + 1]] = Ft[a:a + n]
+                a += n
+        if self.monitor:
+            self._judge(E, F)
+        return E, F, flagged
+
+    def _judge(self, E, F):
+        idx = np.sort(self.rng.choice(len(self.structs), size=min(self.monitor, len(self.structs)), replace=False))
+        sub = [self.structs[k] for k in idx]
+        if self.monitor_batch is None:
+            self.monitor_batch = self.teacher.batch(sub)
+        else:
+            self.monitor_batch.setStructures(sub)
+        self.monitor_batch.setPositions(_positions(sub))
+        self.monitor_batch.evaluate(forces=True, graph=False)
+        Et, Ft = self.monitor_batch.energies(), self.monitor_batch.forces()
+        Fs = np.concatenate([F[self.atom_begin[k]:self.atom_begin[k + 1]] for k in idx])
+        self.monitor_log.append(errors(E[idx], Fs, Et, Ft, [s.numAtoms for s in sub]))
+
+    def fallback_rate(self):
+        return self.fallbacks / max(1, self.evaluations)
+
+
+def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=1e-3, seed=11, device=0, log=print):
+    """The full recipe: label, fit the scaling, train; writes the trained model
+    and returns a summary dict."""
+    t0 = time.perf_counter()
+    structs = training_structures(num_configs, seed)
+    log(f"{len(structs)} training structures, {sum(s.numAtoms for s in structs)} atoms "
+        f"({time.perf_counter() - t0:.1f} s)")
+    teacher = load_mode(teacher_dir, device)
+    E, F = label(teacher, structs)
+    log(f"teacher labels ({time.perf_counter() - t0:.1f} s)")
+    write_student_model(out_dir, structs[:2000], seed=seed, device=device)
+    student = load_mode(out_dir, device)
+    tr = StudentTraining(student, structs, E, F, batch_size=batch_size, eta=eta, seed=seed)
+    for ep in range(epochs):
+        t1 = time.perf_counter()
+        loss = tr.epoch()
+        log(f"epoch {ep + 1}: mean loss {loss:.6e} ({time.perf_counter() - t1:.1f} s)")
+    write_trained_weights(out_dir, student, tr.trainer.parameters())
+    summary = {"configs": num_configs, "atoms": int(sum(s.numAtoms for s in structs)), "epochs": epochs,
+               "batch_size": batch_size, "eta": eta, "force_weight": 10.0, "loss_history": tr.history,
+               "seconds": time.perf_counter() - t0}
+    with open(os.path.join(out_dir, "training.json"), "w") as f:
+        json.dump(summary, f, indent=1)
+    return summary
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--teacher", required=True)
+    t.add_argument("--out", required=True)
+    t.add_argument("--configs", type=int, default=20000)
+    t.add_argument("--epochs", type=int, default=8)
+    t.add_argument("--batch-size", type=int, default=64)
+    t.add_argument("--eta", type=float, default=1e-3)
+    t.add_argument("--seed", type=int, default=11)
+    a = ap.parse_args()
+    if a.cmd == "train":
+        s = train(a.teacher, a.out, a.configs, a.epochs, a.batch_size, a.eta, a.seed)
+        print(json.dumps({k: v for k, v in s.items() if k != "loss_history"}))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+"""Learned part: the GPU trainer's gradient against finite differences of the
+CPU oracle's loss, training progress, what the trained student gains, and the
+teacher fallback on extrapolation."""
+import os
+import time
+
+import numpy as np
+import pytest
+
+from n2p2_b200 import student, water
+
+from tests.helpers import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TEACHER = os.path.join(GOLDEN, "models", "water56")
+
+
+@pytest.fixture(scope="module")
+def teacher():
+    return student.load_mode(TEACHER)
+
+
+@pytest.fixture(scope="module")
+def student_dir(tmp_path_factory):
+    d = str(tmp_path_factory.mktemp("student"))
+    student.write_student_model(d, student.training_structures(24, seed=5, n_min=32, n_max=96), seed=3)
+    return d
+
+
+def _file_to_port_index(pm):
+    """Weight-file order -> index into the oracle's flat weight array."""
+    a = pm.arrays
+    ne = len(pm.symbols)
+    neurons = a["neurons"].reshape(ne, 8)
+    wb, bb = a["wBegin"].reshape(ne, 8), a["bBegin"].reshape(ne, 8)
+    out = []
+    for e in range(ne):
+        L = int(pm.numLayers[e])
+        for l in range(1, L):
+            nin, nout = int(neurons[e, l - 1]), int(neurons[e, l])
+            for j in range(nin):
+                for k in range(nout):
+                    out.append(int(wb[e, l]) + k * nin + j)
+            for k in range(nout):
+                out.append(int(bb[e, l]) + k)
+    return np.array(out)
+
+
+def _oracle_loss(pm, structs, E_ref, F_ref, wE=1.0, wF=10.0):
+    le, lf, n_all = 0.0, 0.0, 0
+    for s, st in enumerate(structs):
+        r = pm.evaluate(st)
+        n = st.numAtoms
+        le += ((r["energy"] - E_ref[s]) / n) ** 2
+        lf += float(np.sum((r["forces"] - F_ref[n_all:n_all + n]) ** 2))
+        n_all += n
+    return wE * le / len(structs) + wF * lf / (3 * n_all)
+
+
+def test_gradient_matches_oracle_finite_differences(student_dir):
+    from oracle.port import PortModel
+    structs = student.training_structures(3, seed=21, n_min=32, n_max=48)
+    m = student.load_mode(student_dir)
+    b = m.batch(structs)
+    b.setPositions(np.concatenate([s.positions for s in structs]))
+    b.evaluate(forces=True, graph=False)
+    rng = np.random.default_rng(2)
+    E_ref = b.energies() + rng.normal(0, 0.05, len(structs))
+    F_ref = b.forces() + rng.normal(0, 0.01, (b.numAtoms, 3))
+    from n2p2_b200 import Trainer
+    tr = Trainer(m)
+    loss, grad = tr.step(b, E_ref, F_ref, update=False, gradient=True)
+
+    pm = PortModel(student_dir)
+    w = pm.arrays["weights"]            # the oracle reads this buffer in place
+    idx = _file_to_port_index(pm)
+    assert idx.size == tr.numParameters
+    w0 = w.copy()
+    l0 = _oracle_loss(pm, structs, E_ref, F_ref)
+    assert abs(l0 - loss[0]) <= 1e-9 * abs(l0)
+    # parameters of every layer of both elements, weights and biases
+    picks = np.unique(np.concatenate([rng.choice(idx.size, 24, replace=False), [0, idx.size - 1]]))
+    scale = np.max(np.abs(grad))
+    for p in picks:
+        h = 1e-5 * max(1.0, abs(w0[idx[p]]))
+        w[idx[p]] = w0[idx[p]] + h
+        lp = _oracle_loss(pm, structs, E_ref, F_ref)
+        w[idx[p]] = w0[idx[p]] - h
+        lm = _oracle_loss(pm, structs, E_ref, F_ref)
+        w[idx[p]] = w0[idx[p]]
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - grad[p]) <= 2e-6 * scale + 1e-6 * abs(fd), (p, fd, grad[p])
+
+
+def test_parameters_round_trip(student_dir):
+    from n2p2_b200 import Trainer
+    m = student.load_mode(student_dir)
+    tr = Trainer(m)
+    w = tr.parameters()
+    assert w.size == 2 * (14 * 16 + 16 + 16 * 16 + 16 + 16 + 1)
+    w2 = w * 1.01
+    tr.setParameters(w2)
+    assert np.array_equal(tr.parameters(), w2)
+
+
+def test_training_gain_and_speed(teacher, student_dir):
+    train = student.training_structures(192, seed=31, n_min=32, n_max=128)
+    held = student.training_structures(32, seed=32, n_min=32, n_max=128)
+    E, F = student.label(teacher, train)
+    Eh, Fh = student.label(teacher, held)
+    m = student.load_mode(student_dir)
+    apa = [s.numAtoms for s in held]
+
+    def held_error():
+        Es, Fs = student.label(m, held)
+        return student.errors(Es, Fs, Eh, Fh, apa)
+
+    before = held_error()
+    tr = student.StudentTraining(m, train, E, F, batch_size=16, eta=2e-3, seed=1)
+    l_first = tr.epoch()
+    for _ in range(7):
+        tr.epoch()
+    assert tr.history[-1] < 0.5 * l_first
+    after = held_error()
+    # the trained network is much closer to the teacher than the untrained one
+    assert after["energy_meV_per_atom_rms"] < 0.3 * before["energy_meV_per_atom_rms"]
+    assert after["force_meV_per_A_rms"] < 0.5 * before["force_meV_per_A_rms"]
+
+    # and it is cheaper than the teacher on the same structures
+    big = water.water_batch(64, seed=41, n_min=128, n_max=512)
+    pos = np.concatenate([s.positions for s in big])
+
+    def timed(mode):
+        b = mode.batch(big)
+        b.setPositions(pos)
+        b.evaluate(forces=True)
+        b.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            b.evaluate(forces=True)
+        b.synchronize()
+        return (time.perf_counter() - t0) / 3
+    assert timed(m) < 0.7 * timed(teacher)
+
+
+def test_fallback_on_extrapolation(teacher, student_dir):
+    held = student.training_structures(6, seed=51, n_min=32, n_max=64)
+    # compress one box by 15 %: its symmetry functions leave the scaling range
+    s = held[2]
+    s.positions = s.positions * 0.85
+    s.box = s.box * 0.85
+    m = student.load_mode(student_dir, extrapolation=True)
+    ev = student.StudentEvaluator(m, teacher, held, monitor=2, seed=0)
+    E, F, flagged = ev.evaluate()
+    assert flagged[2]
+    Et, Ft = student.label(teacher, [held[2]])
+    assert E[2] == Et[0]
+    a0 = sum(x.numAtoms for x in held[:2])
+    assert np.array_equal(F[a0:a0 + held[2].numAtoms], Ft)
+    assert 0 < ev.fallback_rate() <= 1
+    assert len(ev.monitor_log) == 1 and ev.monitor_log[0]["energy_meV_per_atom_rms"] >= 0
