@@ -34,6 +34,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 MODEL = os.path.join(ROOT, "tests", "golden", "models", "water40")
+TEACHER = os.path.join(ROOT, "tests", "golden", "models", "water56")
+STUDENT = os.path.join(ROOT, "tests", "golden", "models", "student_water56")
 METRIC = "atoms/s (E+F) on 1×B200: mixed/student vs plain FP64 at ≤1 meV/atom, 30 meV/Å"
 HA_TO_MEV = 27211.386
 HA_BOHR_TO_MEV_A = 27211.386 / 0.529177
@@ -56,6 +58,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-student", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--student-boxes", type=int, default=2048)
     return ap.parse_args()
 
 
@@ -265,6 +270,18 @@ def run_ours(args):
                                      "force_meV_per_A_max": float(df.max()),
                                      "force_meV_per_A_rms": float(np.sqrt((df ** 2).mean()))}}
 
+    # the large single-system configuration (FP64 and mixed)
+    large = None
+    if rank == 0 and world == 1 and not args.no_large:
+        large = bench_large(args.steps, args.warmup, local)
+
+    # distilled student (with teacher fallback) against the plain FP64 teacher
+    stud = None
+    if rank == 0 and world == 1 and not args.no_student and os.path.isdir(STUDENT):
+        from n2p2_b200 import student as student_mod
+        stud = student_mod.benchmark(STUDENT, TEACHER, num=args.student_boxes, steps=args.steps,
+                                     warmup=args.warmup)
+
     sf_ms = sum(t for n, t in stages if n in ("sf_values", "sf_forces"))
     sf_flops = sum(work[k] * f for k, f in FLOPS_PER.items())
     roofline = None
@@ -290,6 +307,10 @@ def run_ours(args):
         except Exception as exc:  # the timed GPU numbers stand without it
             cpu = {"value": None, "unit": "atoms/s", "cores": host_threads(), "kind": "reference",
                    "sample": "failed: %s" % exc}
+        if stud is not None:
+            stud["err_vs_fp64_oracle"] = student_vs_oracle(stud["_predictions"])
+    if stud is not None:
+        stud.pop("_predictions", None)
 
     value = world * natoms / (ms / 1000.0)
     if rank == 0:
@@ -307,7 +328,7 @@ def run_ours(args):
                 "e2e": {"value": world * natoms / (e2e_ms / 1000.0), "unit": "atoms/s", "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": nbytes_pos, "d2h_bytes_per_step": nbytes_pos + 8 * len(structs)},
                 "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
-                "mixed": mixed, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
+                "mixed": mixed, "student": stud, "large_system": large, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
                 "fp32_fma_peak_tflops": fp32_peak}
         print(json.dumps(line), flush=True)
     mode.close()
@@ -315,6 +336,90 @@ def run_ours(args):
         mode._lib.n2p2_host_free(h[0])
     if dist is not None:
         dist.destroy_process_group()
+
+
+# Algorithmic HBM bytes of the symmetry-function passes: per neighbour entry
+# j, d, dx, dy, dz (36) + f_c, df_c (16) read by each pass, h_x,y,z (24)
+# written by the force pass; per atom G written (values) and dE/dG read
+# (forces), 8 bytes per function.
+SF_BYTES_PER_ENTRY = {"sf_values": 52, "sf_forces": 52 + 24}
+
+
+def bench_large(steps, warmup, device):
+    """36,864-molecule water box, water56 model, FP64 and mixed."""
+    import torch
+    from n2p2_b200 import Mode, water
+    s = water.water_box(36864, seed=2024, sigma=0.15)
+    out = {"workload": "36864-molecule water box (%d atoms, edge %.2f bohr, 1.0 g/cm^3, 0.15 bohr displacements), "
+                       "water56 model (G2 + G3 + wide G9, 56-64-64-1 softplus)" % (s.numAtoms, s.box[0, 0])}
+    mode = Mode(device)
+    mode.setupFromDirectory(TEACHER)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        mode.setPrecision(prec)
+        b = mode.batch([s])
+        b.setPositions(s.positions)
+        b.evaluate(forces=True)
+        b.synchronize()
+        stream = torch.cuda.ExternalStream(b.stream(), device=torch.device("cuda", device))
+        for _ in range(warmup):
+            b.evaluate(forces=True)
+        b.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            b.evaluate(forces=True)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        stages = dict(b.profileStages(forces=True))
+        work = b.countWork()
+        nsf = 56
+        gbs = {}
+        for k, per in SF_BYTES_PER_ENTRY.items():
+            if stages.get(k):
+                nbytes = work["entries"] * per + s.numAtoms * 8 * nsf
+                gbs[k] = nbytes / (stages[k] * 1e-3) / 1e9
+        res[prec] = {"value": s.numAtoms / (ms / 1000.0), "unit": "atoms/s", "ms_per_step": ms,
+                     "stages_ms": {k: round(v, 4) for k, v in stages.items()},
+                     "sf_hbm_GBps_algorithmic": gbs,
+                     "E": b.energies()[0], "F": b.forces()}
+        b.close()
+    de = abs(res["mixed"]["E"] - res["fp64"]["E"]) / s.numAtoms * HA_TO_MEV
+    df = np.abs(res["mixed"]["F"] - res["fp64"]["F"]) * HA_BOHR_TO_MEV_A
+    for prec in res:
+        res[prec].pop("E")
+        res[prec].pop("F")
+    res["mixed"]["speedup_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
+    res["mixed"]["err_vs_fp64_gpu"] = {"energy_meV_per_atom": float(de), "force_meV_per_A_max": float(df.max()),
+                                       "force_meV_per_A_rms": float(np.sqrt((df ** 2).mean()))}
+    out.update(res)
+    out["network"] = "FP64 CUDA-core kernel (warp per atom); no tensor-core GEMM in this build"
+    mode.close()
+    return out
+
+
+def student_vs_oracle(pred, count=4):
+    """Student (with fallback) against the FP64 CPU oracle of the teacher on
+    the first `count` held-out structures (the oracle restates the reference
+    on the host; it is the checker here, not a timed path)."""
+    from oracle.port import PortModel
+    from n2p2_b200 import student as student_mod
+    structs, Es, Fs = pred
+    pm = PortModel(TEACHER)
+    E_o, F_o, Fs_sel = [], [], []
+    a0 = 0
+    for k, s in enumerate(structs[:count]):
+        r = pm.evaluate(s)
+        E_o.append(r["energy"])
+        F_o.append(r["forces"])
+        Fs_sel.append(Fs[a0:a0 + s.numAtoms])
+        a0 += s.numAtoms
+    out = student_mod.errors(Es[:count], np.concatenate(Fs_sel), E_o, np.concatenate(F_o),
+                             [s.numAtoms for s in structs[:count]])
+    out["structures"] = count
+    return out
 
 
 class ctypes_double:

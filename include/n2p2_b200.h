@@ -242,6 +242,8 @@ n2p2_status n2p2_trainer_create(n2p2_mode* mode, n2p2_trainer** trainer);
 n2p2_status n2p2_trainer_destroy(n2p2_trainer* trainer);
 /* Adam parameters (defaults 1e-3, 0.9, 0.999, 1e-8). */
 n2p2_status n2p2_trainer_set_adam(n2p2_trainer* trainer, double eta, double beta1, double beta2, double epsilon);
+/* Step size of the following Adam updates (moments and bias correction kept). */
+n2p2_status n2p2_trainer_set_learning_rate(n2p2_trainer* trainer, double eta);
 /* Loss weights wE, wF (defaults 1, 10). */
 n2p2_status n2p2_trainer_set_loss_weights(n2p2_trainer* trainer, double energyWeight, double forceWeight);
 n2p2_status n2p2_trainer_get_num_parameters(n2p2_trainer* trainer, int64_t* count);

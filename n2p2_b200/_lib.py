@@ -80,6 +80,7 @@ SIGNATURES = {
     "n2p2_trainer_create": (_i, [_vp, _P(_vp)]),
     "n2p2_trainer_destroy": (_i, [_vp]),
     "n2p2_trainer_set_adam": (_i, [_vp, _d, _d, _d, _d]),
+    "n2p2_trainer_set_learning_rate": (_i, [_vp, _d]),
     "n2p2_trainer_set_loss_weights": (_i, [_vp, _d, _d]),
     "n2p2_trainer_get_num_parameters": (_i, [_vp, _P(_i64)]),
     "n2p2_trainer_get_parameters": (_i, [_vp, _P(_d)]),

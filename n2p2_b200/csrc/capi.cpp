@@ -643,6 +643,15 @@ n2p2_status n2p2_trainer_set_adam(n2p2_trainer* trainer, double eta, double beta
     });
 }
 
+n2p2_status n2p2_trainer_set_learning_rate(n2p2_trainer* trainer, double eta)
+{
+    N2P2_REQUIRE(trainer);
+    return guard([&] {
+        if (!(eta > 0.0)) throw std::invalid_argument("ERROR: the learning rate must be positive.\n");
+        trainer->trainer->setLearningRate(eta);
+    });
+}
+
 n2p2_status n2p2_trainer_set_loss_weights(n2p2_trainer* trainer, double energyWeight, double forceWeight)
 {
     N2P2_REQUIRE(trainer);

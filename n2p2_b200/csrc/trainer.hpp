@@ -18,6 +18,7 @@ public:
 
     int numParameters() const { return P_; }
     void setAdam(double eta, double beta1, double beta2, double eps);
+    void setLearningRate(double eta) { eta0_ = eta; }
     void setLossWeights(double wE, double wF)
     {
         wE_ = wE;

@@ -346,6 +346,9 @@ class Trainer:
         except Exception:
             pass
 
+    def setLearningRate(self, eta):
+        _lib.check(self._lib.n2p2_trainer_set_learning_rate(self._h, float(eta)))
+
     def parameters(self):
         out = np.zeros(self.numParameters)
         _lib.check(self._lib.n2p2_trainer_get_parameters(self._h, _dp(out)))

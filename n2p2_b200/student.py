@@ -46,6 +46,47 @@ def student_sf_lines(rc=water.RC, rc_angular=None):
     return out
 
 
+def teacher_sf_importance(teacher_mode, structs):
+    """Per element: mean |dE_i/dG_is| over the atoms times the spread (sigma)
+    of the scaled G_s -- how much each teacher symmetry function moves the
+    teacher's atomic energies on these structures."""
+    b = teacher_mode.batch(structs)
+    b.setPositions(_positions(structs))
+    b.evaluate(forces=True, graph=False)
+    G, D = b.symmetryFunctions(), b.dEdG()
+    ne = teacher_mode.numElements
+    nsf = np.array([teacher_mode.numSymmetryFunctions(e) for e in range(ne)])
+    off = np.concatenate([[0], np.cumsum(nsf[b.elements])])
+    out = []
+    for e in range(ne):
+        rows = np.nonzero(b.elements == e)[0]
+        ix = off[rows][:, None] + np.arange(nsf[e])[None, :]
+        out.append(np.mean(np.abs(D[ix]), axis=0) * np.std(G[ix], axis=0))
+    b.close()
+    return out
+
+
+def select_student_sfs(teacher_mode, importance, n_radial=8, n_angular=6):
+    """symfunction_short lines of the n_radial radial (type 2) and n_angular
+    narrow angular (type 3) teacher functions of highest importance, per
+    element."""
+    sym = [teacher_mode.elementSymbol(e) for e in range(teacher_mode.numElements)]
+    lines = []
+    for e in range(teacher_mode.numElements):
+        sfs = [teacher_mode.symmetryFunction(e, i) for i in range(teacher_mode.numSymmetryFunctions(e))]
+        for t, n in ((2, n_radial), (3, n_angular)):
+            cand = [i for i, f in enumerate(sfs) if f[0] == t]
+            cand.sort(key=lambda i: -importance[e][i])
+            for i in sorted(cand[:n]):
+                typ, e1, e2, eta, rs, lam, zeta, rc, _ = sfs[i]
+                if t == 2:
+                    lines.append(f"symfunction_short {sym[e]} 2 {sym[e1]} {eta:.10g} {rs:.10g} {rc:.10g}")
+                else:
+                    lines.append(f"symfunction_short {sym[e]} 3 {sym[e1]} {sym[e2]} {eta:.10g} {lam:.0f} "
+                                 f"{zeta:.10g} {rc:.10g}")
+    return lines
+
+
 def training_structures(num, seed, n_min=64, n_max=512, sigma_range=(0.05, 0.4)):
     """Water boxes of 192-1536 atoms with Gaussian displacements sigma in the range."""
     return water.water_batch(num, seed, n_min=n_min, n_max=n_max, sigma_range=sigma_range)
@@ -55,9 +96,11 @@ def _positions(structs):
     return np.ascontiguousarray(np.concatenate([s.positions for s in structs]))
 
 
-def label(mode, structs, chunk=512):
-    """Energies [S] and forces [N,3] (physical units) of `structs` by `mode`."""
-    E, F = [], []
+def label(mode, structs, chunk=512, warnings=False):
+    """Energies [S] and forces [N,3] (physical units) of `structs` by `mode`;
+    with `warnings`, also per structure whether the mode's extrapolation check
+    fired (the mode must collect extrapolation warnings)."""
+    E, F, W = [], [], []
     b = None
     for c0 in range(0, len(structs), chunk):
         sub = structs[c0:c0 + chunk]
@@ -69,15 +112,22 @@ def label(mode, structs, chunk=512):
         b.evaluate(forces=True, graph=False)
         E.append(b.energies())
         F.append(b.forces())
+        if warnings:
+            _, per_atom = b.extrapolationWarnings()
+            starts = np.concatenate([[0], np.cumsum([x.numAtoms for x in sub])[:-1]])
+            W.append(np.add.reduceat(per_atom, starts) > 0)
+    if warnings:
+        return np.concatenate(E), np.concatenate(F), np.concatenate(W)
     return np.concatenate(E), np.concatenate(F)
 
 
-def write_student_model(directory, scaling_structs, seed=7, device=0, rc=water.RC, rc_angular=None):
+def write_student_model(directory, scaling_structs, seed=7, device=0, rc=water.RC, rc_angular=None, sf_lines=None):
     """input.nn + N(0, 1/fan_in) weights + scaling.data of the student's
-    symmetry functions over `scaling_structs` (evaluated on the GPU)."""
+    symmetry functions (`sf_lines`, default student_sf_lines) over
+    `scaling_structs` (evaluated on the GPU)."""
     from .mode import Mode
     os.makedirs(directory, exist_ok=True)
-    lines = student_sf_lines(rc, rc_angular)
+    lines = student_sf_lines(rc, rc_angular) if sf_lines is None else list(sf_lines)
     with open(os.path.join(directory, "input.nn"), "w") as f:
         f.write(water.input_nn_text(lines, nodes=STUDENT_NODES, activations="p p l",
                                     comment="distilled student: 8 G2 + 6 G3 per element, 14-16-16-1 softplus"))
@@ -94,7 +144,10 @@ def write_student_model(directory, scaling_structs, seed=7, device=0, rc=water.R
     m.setupNeuralNetworkWeights(os.path.join(directory, "weights.%03zu.data"))
     ne = m.numElements
     nsf = np.array([m.numSymmetryFunctions(e) for e in range(ne)])
-    per_el = [[] for _ in range(ne)]
+    # running min, max, sum, sum of squares (the statistics of
+    # water.scaling_statistics without holding every G in memory)
+    acc = [dict(n=0, mn=np.full(nsf[e], np.inf), mx=np.full(nsf[e], -np.inf), s=np.zeros(nsf[e]),
+                s2=np.zeros(nsf[e])) for e in range(ne)]
     b = None
     for c0 in range(0, len(scaling_structs), 512):
         sub = scaling_structs[c0:c0 + 512]
@@ -108,8 +161,18 @@ def write_student_model(directory, scaling_structs, seed=7, device=0, rc=water.R
         off = np.concatenate([[0], np.cumsum(nsf[b.elements])])
         for e in range(ne):
             rows = np.nonzero(b.elements == e)[0]
-            per_el[e].append(G[off[rows][:, None] + np.arange(nsf[e])[None, :]])
-    stats = water.scaling_statistics([np.concatenate(x) for x in per_el])
+            Ge = G[off[rows][:, None] + np.arange(nsf[e])[None, :]]
+            a = acc[e]
+            a["n"] += Ge.shape[0]
+            a["mn"] = np.minimum(a["mn"], Ge.min(axis=0))
+            a["mx"] = np.maximum(a["mx"], Ge.max(axis=0))
+            a["s"] += Ge.sum(axis=0)
+            a["s2"] += (Ge * Ge).sum(axis=0)
+    stats = []
+    for a in acc:
+        mean = a["s"] / a["n"]
+        sigma = np.sqrt(np.maximum(a["s2"] - a["s"] * a["s"] / a["n"], 0.0) / (a["n"] - 1))
+        stats.append(np.stack([a["mn"], a["mx"], mean, sigma], axis=1))
     water.write_scaling(os.path.join(directory, "scaling.data"), stats)
     m.close()
     return directory
@@ -253,25 +316,116 @@ class StudentEvaluator:
         return self.fallbacks / max(1, self.evaluations)
 
 
-def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=1e-3, seed=11, device=0, log=print):
-    """The full recipe: label, fit the scaling, train; writes the trained model
-    and returns a summary dict."""
+def _subset_errors(Es, Fs, Et, Ft, apa, starts, idx):
+    if idx.size == 0:
+        return None
+    sel = np.concatenate([np.arange(starts[k], starts[k + 1]) for k in idx])
+    return errors(Es[idx], Fs[sel], Et[idx], Ft[sel], np.asarray(apa)[idx])
+
+
+def benchmark(student_dir, teacher_dir, num=2048, seed=97, steps=3, warmup=2, device=0, monitor=2):
+    """Held-out throughput and error of the student (with fallback and the
+    per-batch held-out monitor) against the plain FP64 teacher on `num` boxes
+    of the training recipe (own seed).  Both forms are timed the same way:
+    one evaluation plus the energies and forces read back, per step."""
+    structs = training_structures(num, seed)
+    natoms = sum(s.numAtoms for s in structs)
+    apa = [s.numAtoms for s in structs]
+    teacher = load_mode(teacher_dir, device, extrapolation=True)
+    tb = teacher.batch(structs)
+    tb.setPositions(_positions(structs))
+
+    def teacher_step():
+        tb.evaluate(forces=True)
+        return tb.energies(), tb.forces()
+
+    for _ in range(warmup):
+        Et, Ft = teacher_step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        Et, Ft = teacher_step()
+    t_teacher = (time.perf_counter() - t0) / steps
+    _, per_atom = tb.extrapolationWarnings()
+    starts = np.concatenate([[0], np.cumsum(apa)])
+    teacher_in_range = np.add.reduceat(per_atom, starts[:-1]) == 0
+
+    smode = load_mode(student_dir, device, extrapolation=True)
+    ev = StudentEvaluator(smode, teacher, structs, monitor=monitor, seed=seed)
+    for _ in range(warmup):
+        Es, Fs, flagged = ev.evaluate()
+    ev.fallbacks = ev.evaluations = 0
+    ev.monitor_log = []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        Es, Fs, flagged = ev.evaluate()
+    t_student = (time.perf_counter() - t0) / steps
+    mon = ev.monitor_log
+    out = {"workload": "%d held-out water boxes, 64-512 molecules, displacements 0.05-0.4 bohr (%d atoms)"
+                       % (num, natoms),
+           "value": natoms / t_student, "unit": "atoms/s", "ms_per_step": 1e3 * t_student,
+           "teacher_fp64": {"value": natoms / t_teacher, "unit": "atoms/s", "ms_per_step": 1e3 * t_teacher},
+           "speedup_vs_fp64": t_teacher / t_student,
+           "fallback_rate": ev.fallback_rate(),
+           "err_vs_teacher_fp64_gpu": errors(Es, Fs, Et, Ft, apa),
+           "err_vs_teacher_fp64_gpu_teacher_in_range": _subset_errors(Es, Fs, Et, Ft, apa, starts,
+                                                                      np.nonzero(teacher_in_range)[0]),
+           "teacher_in_range_fraction": float(teacher_in_range.mean()),
+           "held_out_monitor": {"structures_per_batch": monitor, "batches": len(mon),
+                                "energy_meV_per_atom_rms": float(np.mean([m["energy_meV_per_atom_rms"] for m in mon]))
+                                if mon else None,
+                                "force_meV_per_A_rms": float(np.mean([m["force_meV_per_A_rms"] for m in mon]))
+                                if mon else None}}
+    out["_predictions"] = (structs, Es, Fs)
+    return out
+
+
+def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=1e-3, seed=11, device=0, log=print,
+          select=True, decay=(0.5, 0.3)):
+    """The full recipe: label, choose the descriptor (the teacher's most
+    important functions when `select`), fit the scaling, train (step size
+    `eta`, times decay[1] after each further decay[0] fraction of the epochs);
+    writes the trained model and returns a summary dict."""
     t0 = time.perf_counter()
     structs = training_structures(num_configs, seed)
     log(f"{len(structs)} training structures, {sum(s.numAtoms for s in structs)} atoms "
         f"({time.perf_counter() - t0:.1f} s)")
     teacher = load_mode(teacher_dir, device)
     E, F = label(teacher, structs)
-    log(f"teacher labels ({time.perf_counter() - t0:.1f} s)")
-    write_student_model(out_dir, structs[:2000], seed=seed, device=device)
+    # Labels from far outside the teacher's scaling range (rare close
+    # contacts at the largest displacements) reach forces of many Ha/bohr and
+    # would dominate a squared-error fit; structures whose largest teacher
+    # force exceeds ten times the median of that maximum are not trained on
+    # (they remain the teacher's to answer).
+    starts = np.concatenate([[0], np.cumsum([s.numAtoms for s in structs])])
+    fmax = np.maximum.reduceat(np.abs(F).max(axis=1), starts[:-1])
+    outlier = fmax > 10.0 * np.median(fmax)
+    keep = np.nonzero(~outlier)[0]
+    all_structs = structs
+    F = np.concatenate([F[starts[k]:starts[k + 1]] for k in keep])
+    E = E[keep]
+    structs = [structs[k] for k in keep]
+    log(f"teacher labels ({time.perf_counter() - t0:.1f} s); {int(outlier.sum())} structures with outlying "
+        f"teacher forces left out")
+    lines = None
+    if select:
+        lines = select_student_sfs(teacher, teacher_sf_importance(teacher, structs[:256]))
+        log("descriptor: " + "; ".join(l.replace("symfunction_short ", "") for l in lines))
+    # scaling statistics (and hence the extrapolation range) over every training configuration
+    write_student_model(out_dir, all_structs, seed=seed, device=device, sf_lines=lines)
     student = load_mode(out_dir, device)
     tr = StudentTraining(student, structs, E, F, batch_size=batch_size, eta=eta, seed=seed)
+    first_decay = int(math.ceil(decay[0] * epochs))
     for ep in range(epochs):
         t1 = time.perf_counter()
+        lr = eta * decay[1] ** max(0, (ep - first_decay) // max(1, (epochs - first_decay) // 2) + 1) \
+            if ep >= first_decay else eta
+        tr.trainer.setLearningRate(lr)
         loss = tr.epoch()
-        log(f"epoch {ep + 1}: mean loss {loss:.6e} ({time.perf_counter() - t1:.1f} s)")
+        log(f"epoch {ep + 1}: lr {lr:.1e} mean loss {loss:.6e} ({time.perf_counter() - t1:.1f} s)")
     write_trained_weights(out_dir, student, tr.trainer.parameters())
-    summary = {"configs": num_configs, "atoms": int(sum(s.numAtoms for s in structs)), "epochs": epochs,
+    summary = {"configs": num_configs, "outlying_labels_left_out": int(outlier.sum()),
+               "atoms": int(sum(s.numAtoms for s in structs)), "epochs": epochs,
+               "descriptor": lines if lines is not None else student_sf_lines(),
                "batch_size": batch_size, "eta": eta, "force_weight": 10.0, "loss_history": tr.history,
                "seconds": time.perf_counter() - t0}
     with open(os.path.join(out_dir, "training.json"), "w") as f:
