@@ -199,6 +199,7 @@ def run_ours(args):
     batch.setPositions(pos)
     batch.evaluate(forces=True)     # establishes neighbour capacity (direct launches)
     batch.synchronize()
+    tune = batch.autotune(useCache=False)   # kernel shapes measured on this batch (outside the timed steps)
     stream = torch.cuda.ExternalStream(batch.stream(), device=torch.device("cuda", local))
 
     def timed(steps, warmup):
@@ -258,6 +259,7 @@ def run_ours(args):
         mode.setPrecision("mixed")
         batch.evaluate(forces=True)
         batch.synchronize()
+        tune_mixed = batch.autotune(useCache=False)
         ms_mixed = timed(args.steps, args.warmup)
         Em, Fm = batch.energies(), batch.forces()
         mode.setPrecision("fp64")
@@ -265,7 +267,7 @@ def run_ours(args):
         de = np.abs(Em - E64) / atoms_per * HA_TO_MEV
         df = np.abs(Fm - F64) * HA_BOHR_TO_MEV_A
         mixed = {"value": world * natoms / (ms_mixed / 1000.0), "unit": "atoms/s", "ms_per_step": ms_mixed,
-                 "speedup_vs_fp64": ms / ms_mixed,
+                 "speedup_vs_fp64": ms / ms_mixed, "autotune": _shape_names(tune_mixed),
                  "err_vs_fp64_gpu": {"energy_meV_per_atom_max": float(de.max()),
                                      "force_meV_per_A_max": float(df.max()),
                                      "force_meV_per_A_rms": float(np.sqrt((df ** 2).mean()))}}
@@ -327,7 +329,7 @@ def run_ours(args):
                            "parallelism": "dp%d (independent structures per GPU)" % world},
                 "e2e": {"value": world * natoms / (e2e_ms / 1000.0), "unit": "atoms/s", "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": nbytes_pos, "d2h_bytes_per_step": nbytes_pos + 8 * len(structs)},
-                "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+                "gpu_launches": launches, "autotune": _shape_names(tune), "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
                 "mixed": mixed, "student": stud, "large_system": large, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
                 "fp32_fma_peak_tflops": fp32_peak}
         print(json.dumps(line), flush=True)
@@ -420,6 +422,15 @@ def student_vs_oracle(pred, count=4):
                              [s.numAtoms for s in structs[:count]])
     out["structures"] = count
     return out
+
+
+def _shape_names(t):
+    from n2p2_b200.mode import Batch
+    name = lambda v: "%d x %d" % Batch.SHAPES[v]
+    return {"values": name(t["values"]), "forces": name(t["forces"]),
+            "values_ms": {name(v): round(x, 3) for v, x in enumerate(t["values_ms"])},
+            "forces_ms": {name(v): round(x, 3) for v, x in enumerate(t["forces_ms"])},
+            "shape": "first-tier stage capacity x warps per block"}
 
 
 class ctypes_double:

@@ -259,6 +259,23 @@ n2p2_status n2p2_trainer_set_parameters(n2p2_trainer* trainer, const double* par
 n2p2_status n2p2_trainer_step(n2p2_trainer* trainer, n2p2_batch* batch, const double* energies,
                               const double* forces, int32_t update, double* loss, double* gradient);
 
+/* ---- autotuning (no counterpart in the reference) -------------------------
+ * The symmetry-function passes run their first tier of atoms with one of
+ * three kernel shapes (stage capacity x warps per block: 0 = 128 x 4,
+ * 1 = 160 x 4, 2 = 192 x 2).  Before a batch's first graph capture in a
+ * precision the shapes are chosen per pass by timing all three on the batch
+ * (or taken from the cache file N2P2_B200_TUNE_CACHE, default
+ * ~/.cache/n2p2_b200/autotune.json).  Results do not depend on the shape. */
+/* Enable (default) or disable the automatic tuning for the mode's batches. */
+n2p2_status n2p2_mode_set_autotune(n2p2_mode* mode, int32_t enabled);
+/* Tune now for the mode's current precision (the batch must have been
+ * evaluated once); shapes[2] = {G pass, force pass}, ms[6] = the measured
+ * times per shape (zeros when taken from the cache), *fromCache. */
+n2p2_status n2p2_batch_autotune(n2p2_batch* batch, int32_t useCache, int32_t* shapes, double* ms,
+                                int32_t* fromCache);
+/* Fix the shapes for the mode's current precision (no tuning). */
+n2p2_status n2p2_batch_set_shapes(n2p2_batch* batch, int32_t valuesShape, int32_t forcesShape);
+
 /* ---- instrumentation (no counterpart in the reference) ------------------- */
 
 /* The CUDA stream (cudaStream_t) the batch's kernels run on, for event timing. */

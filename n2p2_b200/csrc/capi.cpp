@@ -27,6 +27,7 @@ struct n2p2_mode
     bool uploaded = false;
     int precision = PREC_FP64;
     bool checkExtrapolation = false;
+    bool autotune = true;
     bool writeWarnings = false;
     bool stopOnWarnings = false;
 };
@@ -391,6 +392,7 @@ n2p2_status n2p2_batch_evaluate(n2p2_batch* batch, int flags)
     return guard([&] {
         setDevice(batch->mode);
         batch->lastFlags = flags;
+        batch->batch->autotuneEnabled = batch->mode->autotune;
         batch->batch->evaluate(flags, batch->mode->precision, batch->mode->checkExtrapolation ? 1 : 0);
         afterEvaluate(batch);
     });
@@ -435,6 +437,7 @@ n2p2_status n2p2_batch_evaluate_host(n2p2_batch* batch, const double* positions,
         setDevice(batch->mode);
         batch->lastFlags = flags;
         batch->batch->setPositionsHost(positions);
+        batch->batch->autotuneEnabled = batch->mode->autotune;
         batch->batch->evaluate(flags, batch->mode->precision, batch->mode->checkExtrapolation ? 1 : 0);
         afterEvaluate(batch);
         batch->batch->energies(energies);
@@ -609,6 +612,41 @@ n2p2_status n2p2_device_fma_peak(int device, double* fp64Tflops, double* fp32Tfl
         if (fp32Tflops) *fp32Tflops = measureFmaPeak(0, p.multiProcessorCount);
         cudaCheck(cudaGetLastError(), "fma probe");
     });
+}
+
+n2p2_status n2p2_mode_set_autotune(n2p2_mode* mode, int32_t enabled)
+{
+    N2P2_REQUIRE(mode);
+    return guard([&] { mode->autotune = enabled != 0; });
+}
+
+n2p2_status n2p2_batch_autotune(n2p2_batch* batch, int32_t useCache, int32_t* shapes, double* ms,
+                                int32_t* fromCache)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        Batch::TuneResult r = batch->batch->autotune(batch->mode->precision, batch->mode->checkExtrapolation ? 1 : 0,
+                                                     useCache != 0);
+        if (shapes)
+        {
+            shapes[0] = r.values;
+            shapes[1] = r.forces;
+        }
+        if (ms)
+            for (int v = 0; v < kSFShapeCount; ++v)
+            {
+                ms[v] = r.valuesMs[v];
+                ms[kSFShapeCount + v] = r.forcesMs[v];
+            }
+        if (fromCache) *fromCache = r.fromCache ? 1 : 0;
+    });
+}
+
+n2p2_status n2p2_batch_set_shapes(n2p2_batch* batch, int32_t valuesShape, int32_t forcesShape)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] { batch->batch->setShapes(batch->mode->precision, valuesShape, forcesShape); });
 }
 
 n2p2_status n2p2_trainer_create(n2p2_mode* mode, n2p2_trainer** trainer)

@@ -3,11 +3,17 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <mutex>
 #include <set>
+#include <sstream>
 #include <stdexcept>
 #include <string>
+#include <sys/stat.h>
+#include <unistd.h>
 
 namespace n2p2b200 {
 
@@ -403,7 +409,7 @@ void DeviceModel::upload(Model const& m)
                 }
                 members.push_back(dm);
             }
-            if (!dg.fast || (dg.type != 2 && !dg.grid)) v.allFast = 0;
+            if (!dg.fast || (dg.type != 2 && (!dg.grid || dg.numBases > 1))) v.allFast = 0;   // one staged base
             else if (dg.type != 2 && dg.gridNZ > 2 && v.allFast) v.allFast = 4;
             groups.push_back(dg);
         }
@@ -458,6 +464,18 @@ void DeviceModel::upload(Model const& m)
     v.rowTable = rowTable_;
     v.weights = weights_;
     numWeights = weights.size();
+    // FNV-1a over the evaluation plan (what the kernels' speed depends on)
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t n) {
+        const unsigned char* c = static_cast<const unsigned char*>(p);
+        for (size_t k = 0; k < n; ++k) h = (h ^ c[k]) * 1099511628211ull;
+    };
+    mix(groups.data(), groups.size() * sizeof(DevGroup));
+    mix(members.data(), members.size() * sizeof(DevMember));
+    mix(&v.numElements, sizeof(int));
+    mix(&v.allFast, sizeof(int));
+    mix(v.cutoff, sizeof(v.cutoff));
+    fingerprint = h;
     v.weightsF = weightsF_;
     view = v;
     this->maxSF = maxSF;
@@ -583,6 +601,7 @@ void Batch::setStructures(std::vector<StructureInput> const& s, const int* eleme
     cudaCheck(cudaStreamSynchronize(stream_), "setStructures");
     allocateNeighbors(std::max<int64_t>(capacity, 1));
     capacityVerified_ = false;
+    tuned_[0] = tuned_[1] = false;   // new workload: shapes come from the cache or are measured again
 }
 
 void Batch::allocateAtoms()
@@ -715,7 +734,7 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
     }
     else
     {
-        launchSFValues(m, v_, precision, sms_, stream_);
+        launchSFValues(m, v_, precision, sms_, stream_, sfShape_[0][precision]);
         launches += 2;
         mark("sf_values");
     }
@@ -741,7 +760,7 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         }
         else
         {
-            launchSFForces(m, v_, precision, sms_, stream_);
+            launchSFForces(m, v_, precision, sms_, stream_, sfShape_[1][precision]);
             launches += 2;
             mark("sf_forces");
         }
@@ -783,6 +802,180 @@ void Batch::countWork(int64_t* counts)
     for (int k = 0; k < 10; ++k) counts[k] = (int64_t)h[k];
 }
 
+// ---------------------------------------------------------------------------
+// Autotuning of the symmetry-function shapes
+// ---------------------------------------------------------------------------
+
+namespace {
+
+std::string tuneCachePath()
+{
+    if (const char* p = std::getenv("N2P2_B200_TUNE_CACHE")) return p;
+    const char* home = std::getenv("HOME");
+    return std::string(home ? home : "/tmp") + "/.cache/n2p2_b200/autotune.json";
+}
+
+void makeParents(std::string const& path)
+{
+    for (size_t k = 1; k < path.size(); ++k)
+        if (path[k] == '/') mkdir(path.substr(0, k).c_str(), 0755);
+}
+
+// The cache is a JSON object written one entry per line:
+//   "key": {"values": v, "forces": f, "values_ms": [...], "forces_ms": [...]}
+std::vector<std::pair<std::string, std::string>> readTuneCache(std::string const& path)
+{
+    std::vector<std::pair<std::string, std::string>> out;
+    std::ifstream f(path);
+    std::string line;
+    while (std::getline(f, line))
+    {
+        size_t a = line.find('"');
+        if (a == std::string::npos) continue;
+        size_t b = line.find('"', a + 1);
+        size_t c = line.find('{', b == std::string::npos ? 0 : b);
+        if (b == std::string::npos || c == std::string::npos) continue;
+        size_t d = line.rfind('}');
+        if (d == std::string::npos || d < c) continue;
+        out.emplace_back(line.substr(a + 1, b - a - 1), line.substr(c, d - c + 1));
+    }
+    return out;
+}
+
+bool tuneField(std::string const& body, char const* name, int& v)
+{
+    std::string k = std::string("\"") + name + "\":";
+    size_t p = body.find(k);
+    if (p == std::string::npos) return false;
+    v = std::atoi(body.c_str() + p + k.size());
+    return true;
+}
+
+} // namespace
+
+std::string Batch::tuneKey(int precision)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp p{};
+    cudaGetDeviceProperties(&p, dev);
+    std::string gpu = p.name;
+    for (char& c : gpu)
+        if (c == '"' || c == ' ') c = '_';
+    const DevStatus st = status();
+    const double perAtom = N_ ? (double)st.totalNeighbors / N_ : 0.0;
+    int nb = 0;
+    while ((1 << (nb + 1)) <= N_) ++nb;
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%s|sm%d|plan%016llx|p%d|n2^%d|nbr%d", gpu.c_str(), p.multiProcessorCount,
+                  (unsigned long long)dmodel_.fingerprint, precision, nb, (int)std::lround(perAtom / 8.0) * 8);
+    return buf;
+}
+
+void Batch::setShapes(int precision, int values, int forces)
+{
+    if (precision < 0 || precision > 1 || values < 0 || values >= kSFShapeCount || forces < 0 ||
+        forces >= kSFShapeCount)
+        throw std::invalid_argument("ERROR: shape variant out of range.\n");
+    sfShape_[0][precision] = values;
+    sfShape_[1][precision] = forces;
+    tuned_[precision] = true;
+    releaseGraph();
+}
+
+Batch::TuneResult Batch::autotune(int precision, int checkExtrapolation, bool useCache)
+{
+    if (!capacityVerified_) throw std::runtime_error("ERROR: evaluate the batch once before autotuning.\n");
+    TuneResult r;
+    const std::string key = tuneKey(precision);
+    const std::string path = tuneCachePath();
+    if (useCache)
+    {
+        for (auto const& e : readTuneCache(path))
+        {
+            int v = -1, f = -1;
+            if (e.first == key && tuneField(e.second, "values", v) && tuneField(e.second, "forces", f) && v >= 0 &&
+                v < kSFShapeCount && f >= 0 && f < kSFShapeCount)
+            {
+                r.values = v;
+                r.forces = f;
+                r.fromCache = true;
+            }
+        }
+    }
+    if (!r.fromCache)
+    {
+        // fill every pass input (neighbour data, dE/dG) once, then time the passes alone
+        record(EVAL_FORCES, precision, checkExtrapolation);
+        DevModel const& m = dmodel_.view;
+        cudaEvent_t e0, e1;
+        cudaCheck(cudaEventCreate(&e0), "event");
+        cudaCheck(cudaEventCreate(&e1), "event");
+        for (int pass = 0; pass < 2; ++pass)
+            for (int v = 0; v < kSFShapeCount; ++v)
+            {
+                auto launch = [&] {
+                    if (pass == 0) launchSFValues(m, v_, precision, sms_, stream_, v);
+                    else launchSFForces(m, v_, precision, sms_, stream_, v);
+                };
+                launch();
+                double best = 1e300;
+                for (int rep = 0; rep < 2; ++rep)
+                {
+                    cudaCheck(cudaEventRecord(e0, stream_), "event");
+                    launch();
+                    cudaCheck(cudaEventRecord(e1, stream_), "event");
+                    cudaCheck(cudaEventSynchronize(e1), "event sync");
+                    float ms = 0.f;
+                    cudaCheck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+                    best = std::min(best, (double)ms);
+                }
+                (pass == 0 ? r.valuesMs : r.forcesMs)[v] = best;
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaCheck(cudaGetLastError(), "autotune");
+        r.values = (int)(std::min_element(r.valuesMs, r.valuesMs + kSFShapeCount) - r.valuesMs);
+        r.forces = (int)(std::min_element(r.forcesMs, r.forcesMs + kSFShapeCount) - r.forcesMs);
+        // the passes ran with every shape; results are identical whichever ran last
+        if (useCache)
+        {
+            auto entries = readTuneCache(path);
+            std::ostringstream body;
+            body << "{\"values\": " << r.values << ", \"forces\": " << r.forces << ", \"values_ms\": [";
+            for (int v = 0; v < kSFShapeCount; ++v) body << (v ? ", " : "") << r.valuesMs[v];
+            body << "], \"forces_ms\": [";
+            for (int v = 0; v < kSFShapeCount; ++v) body << (v ? ", " : "") << r.forcesMs[v];
+            body << "]}";
+            bool replaced = false;
+            for (auto& e : entries)
+                if (e.first == key)
+                {
+                    e.second = body.str();
+                    replaced = true;
+                }
+            if (!replaced) entries.emplace_back(key, body.str());
+            makeParents(path);
+            const std::string tmp = path + ".tmp." + std::to_string((long)getpid());
+            {
+                std::ofstream f(tmp);
+                f << "{\n";
+                for (size_t k = 0; k < entries.size(); ++k)
+                    f << "  \"" << entries[k].first << "\": " << entries[k].second
+                      << (k + 1 < entries.size() ? ",\n" : "\n");
+                f << "}\n";
+            }
+            std::rename(tmp.c_str(), path.c_str());   // atomic replace; a failed write leaves no cache
+        }
+    }
+    sfShape_[0][precision] = r.values;
+    sfShape_[1][precision] = r.forces;
+    tuned_[precision] = true;
+    lastTune_[precision] = r;
+    releaseGraph();
+    return r;
+}
+
 void Batch::evaluate(int flags, int precision, int checkExtrapolation)
 {
     if (N_ == 0) throw std::runtime_error("ERROR: no structures set.\n");
@@ -812,6 +1005,7 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
         return;
     }
     const int key = (flags & (EVAL_FORCES | EVAL_STORE_DGDR)) | (precision << 4) | ((checkExtrapolation ? 1 : 0) << 5);
+    if (autotuneEnabled && !tuned_[precision] && !(flags & EVAL_STORE_DGDR)) autotune(precision, checkExtrapolation, true);
     if (graphExec_ == nullptr || graphKey_ != key)
     {
         releaseGraph();

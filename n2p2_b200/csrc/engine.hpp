@@ -53,6 +53,7 @@ public:
     DevModel view;
     int maxSF = 0;
     size_t numWeights = 0;               // entries of the flat weight array
+    uint64_t fingerprint = 0;            // hash of the evaluation plan (groups, members, cutoffs)
     double* weightsDevice() const { return weights_; }
     float* weightsFDevice() const { return weightsF_; }
 
@@ -106,6 +107,24 @@ public:
     BatchView const& view() const { return v_; }
     cudaStream_t stream() const { return stream_; }
     int launchesPerEvaluate() const { return launches_; }
+
+    // Autotuning of the symmetry-function passes' first-tier shape (stage
+    // capacity x warps per block, kSFShapeCount variants): every shape of both
+    // passes is timed on this batch's own inputs and the fastest kept, or the
+    // choice is read from the on-disk cache (N2P2_B200_TUNE_CACHE, default
+    // ~/.cache/n2p2_b200/autotune.json) keyed by GPU, model plan, precision
+    // and workload class.  Runs by itself before the first graph capture of a
+    // precision unless disabled.
+    struct TuneResult
+    {
+        int values = 1, forces = 1;
+        double valuesMs[kSFShapeCount] = {0}, forcesMs[kSFShapeCount] = {0};
+        bool fromCache = false;
+    };
+    TuneResult autotune(int precision, int checkExtrapolation, bool useCache);
+    void setShapes(int precision, int values, int forces);
+    TuneResult lastTune(int precision) const { return lastTune_[precision]; }
+    bool autotuneEnabled = true;
 
     // One direct evaluation with CUDA events between the stages; returns
     // (stage name, milliseconds) in launch order.
@@ -163,6 +182,10 @@ private:
     cudaGraphExec_t graphExec_ = nullptr;
     int graphKey_ = -1;
     int launches_ = 0;
+    int sfShape_[2][2] = {{1, 1}, {1, 1}};   // [values, forces][precision]: first-tier shape variant
+    bool tuned_[2] = {false, false};
+    TuneResult lastTune_[2];
+    std::string tuneKey(int precision);
     DevicePool pool_;
     std::vector<void*> owned_;
     std::vector<void*> ownedNbr_;

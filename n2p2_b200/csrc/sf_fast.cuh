@@ -1,5 +1,6 @@
 // Symmetry-function kernels of the evaluation path (G values and the adjoint
-// force pass), one warp per centre atom.
+// force pass), one warp per centre atom; included by one translation unit per
+// precision (k_sf_fast_f64.cu, k_sf_fast_f32.cu).
 //
 // Formulas: SymGrpExpRad::calculate (SymGrpExpRad.cpp:144-239),
 // SymGrpExpAngn::calculate (SymGrpExpAngn.cpp:156-403),
@@ -9,18 +10,23 @@
 //  * The atom's neighbours are staged in shared memory sorted by element
 //    (stable), so the partners of a group form contiguous blocks and no
 //    element test is left in the triplet loops.  Per neighbour the stage holds
-//    dr, r, 1/r, f_c, df_c/r and, per group, the Gaussian factors
-//    exp(-eta_b r^2) of the group's bases.
+//    dr, r, 1/r, f_c, (df_c/r in the force pass) and, per group, the Gaussian
+//    factors exp(-eta_b r^2) of the group's bases.
 //  * Gaussians: exp(-eta (rij^2 + rik^2 + rjk^2)) = E_b(rij) E_b(rik) exp(-eta_b rjk^2)
 //    raised to an integer power when eta = k eta_b (plan built on the host),
 //    so a triplet costs one exponential per base instead of one per eta.
-//  * Work split: each group's (owner, partner) pairs are enumerated
-//    owner-major (G: each unordered pair once; force pass: ordered pairs);
-//    the warp tests 32 candidates per step and appends the accepted ones to a
-//    shared-memory queue, which is consumed 32 triplets at a time, so lanes
-//    idle only in a group's last partial batch.  In the force pass the owner
-//    rows are combined by a segmented warp reduction (no atomics).
+//  * Work split: each group's candidate (j, k) pairs are tested 64 at a time
+//    and the accepted ones appended to a ring queue in shared memory, which
+//    is consumed 32 triplets at a time, so lanes idle only in a group's last
+//    partial batch.  The G pass enumerates owner-major; the force pass
+//    evaluates each unordered pair once, enumerated in rounds of matchings,
+//    and adds a round's contributions to distinct slots (no atomics).
+//  * Tiers: an atom with n neighbours runs in the first kernel instance whose
+//    stage holds n (tier bounds are launch arguments); the last tier flags
+//    atoms beyond its stage.
 //  * All sums run in a fixed order: results are bitwise reproducible.
+#pragma once
+
 #include "kernels_common.cuh"
 #include "kernels.hpp"
 
@@ -51,42 +57,46 @@ __device__ __forceinline__ double fpow<double>(double b, double e) { return pow(
 template <>
 __device__ __forceinline__ float fpow<float>(float b, float e) { return __powf(b, e); }
 
-template <typename T, int CAP, bool DF>
+template <typename T, int CAP, bool DF, int NB>
 struct Stage
 {
     T x[CAP], y[CAP], z[CAP], r[CAP], rinv[CAP], fc[CAP];
     T dfcr[DF ? CAP : 1];                  // (df_c/dr)/r, force pass only
-    T E[kMaxStagedBases][CAP];
+    T E[NB][CAP];                          // Gaussian factors of the group's staged bases
     short perm[CAP];                       // staged slot -> position in the atom's list
     int blockBegin[kDevMaxElements + 1];
 };
 
 // Per-group member parameters (shared by all lanes).
-template <typename T>
+// COMPACT (model-specialised kernels): only what planned radial groups and
+// member grids read.
+template <typename T, bool COMPACT>
 struct Members
 {
-    T cw[kMaxMembers];       // force pass: dE/dG * factorNorm
-    T zl[kMaxMembers], fd[kMaxMembers], lambda[kMaxMembers], zeta[kMaxMembers], eta[kMaxMembers],
-        rs[kMaxMembers];
-    int zint[kMaxMembers], base[kMaxMembers], pw[kMaxMembers], flags[kMaxMembers];  // 1 intPow, 2 calcExp
+    static constexpr int kM = kMaxMembers, kC = COMPACT ? 1 : kMaxMembers;
+    T cw[kM];                // force pass: dE/dG * factorNorm
+    T eta[kM], rs[kM];
+    int base[kM], pw[kM];
+    T zl[kC], fd[kC], lambda[kC], zeta[kC];
+    int zint[kC], flags[kC];  // flags: 1 intPow, 2 calcExp
     T gcw[16], gzl[16], gfd[16];   // member grid: coefficients per (eta, lambda, zeta) combination, 0 if absent
 };
 
 constexpr int kQueue = 128;  // ring of accepted (owner, partner) pairs waiting for a full warp (< 32 + 64)
 
-template <typename T, int CAP>
+template <typename T, int CAP, int FAST>
 struct ValuesSmem
 {
-    Stage<T, CAP, false> st;
-    Members<T> mb;
+    Stage<T, CAP, false, FAST ? 1 : kMaxStagedBases> st;
+    Members<T, FAST != 0> mb;
     int queue[kQueue];
 };
 
-template <typename T, int CAP>
+template <typename T, int CAP, int FAST>
 struct ForcesSmem
 {
-    Stage<T, CAP, true> st;
-    Members<T> mb;
+    Stage<T, CAP, true, FAST ? 1 : kMaxStagedBases> st;
+    Members<T, FAST != 0> mb;
     double h[3][CAP];
     int queue[kQueue];
 };
@@ -196,8 +206,8 @@ __device__ __forceinline__ int entryRound(int e) { return e >> 20; }
 // Test the next 64 candidates of a phase (two independent halves for
 // latency hiding) and append the accepted ones, in candidate order, to the
 // warp's ring queue (qn entries from q[qh]).
-template <typename T, int CAP, bool DF>
-__device__ __forceinline__ bool testCandidate(Stage<T, CAP, DF> const& S, Phase const& ph, Cursor const& cur, int p,
+template <typename T, int CAP, bool DF, int NB>
+__device__ __forceinline__ bool testCandidate(Stage<T, CAP, DF, NB> const& S, Phase const& ph, Cursor const& cur, int p,
                                               T rc, T rc2, bool narrow, int& entry)
 {
     int so = 0, sp = 0;
@@ -215,8 +225,8 @@ __device__ __forceinline__ bool testCandidate(Stage<T, CAP, DF> const& S, Phase 
     return ok;
 }
 
-template <typename T, int CAP, bool DF>
-__device__ __forceinline__ void enqueueCandidates(Stage<T, CAP, DF> const& S, Phase const& ph, Cursor& cur, int p0,
+template <typename T, int CAP, bool DF, int NB>
+__device__ __forceinline__ void enqueueCandidates(Stage<T, CAP, DF, NB> const& S, Phase const& ph, Cursor& cur, int p0,
                                                   T rc, T rc2, bool narrow, int* queue, int qh, int& qn, int lane)
 {
     Cursor c2 = cur;
@@ -280,8 +290,8 @@ __device__ __forceinline__ int roundPhases(int A0, int nA, int B0, int nB, bool 
 }
 
 // Neighbours of one atom into the stage, sorted by element (stable).
-template <typename T, int CAP, bool DF>
-__device__ void stageGeometry(Stage<T, CAP, DF>& S, int64_t off, int n, int numElements, BatchView const& b, int lane)
+template <typename T, int CAP, bool DF, int NB>
+__device__ void stageGeometry(Stage<T, CAP, DF, NB>& S, int64_t off, int n, int numElements, BatchView const& b, int lane)
 {
     __syncwarp();
     int base = 0;
@@ -313,8 +323,8 @@ __device__ void stageGeometry(Stage<T, CAP, DF>& S, int64_t off, int n, int numE
 }
 
 // f_c and df_c/r of the cutoff slot (values computed in FP64 per entry).
-template <typename T, int CAP, bool DF>
-__device__ void stageCutoff(Stage<T, CAP, DF>& S, int64_t off, int n, int slot, BatchView const& b, int lane)
+template <typename T, int CAP, bool DF, int NB>
+__device__ void stageCutoff(Stage<T, CAP, DF, NB>& S, int64_t off, int n, int slot, BatchView const& b, int lane)
 {
     __syncwarp();
     const double* fc = b.nbrFc + (size_t)slot * b.nbrCapacity + off;
@@ -330,8 +340,8 @@ __device__ void stageCutoff(Stage<T, CAP, DF>& S, int64_t off, int n, int slot, 
 
 // Gaussian factors exp(-eta_b r^2) of the group's staged bases for the slots
 // of the group's element blocks.
-template <typename T, int CAP, bool DF>
-__device__ void stageFactors(Stage<T, CAP, DF>& S, DevGroup const& G, int lane)
+template <typename T, int CAP, bool DF, int NB>
+__device__ void stageFactors(Stage<T, CAP, DF, NB>& S, DevGroup const& G, int lane)
 {
     __syncwarp();
     for (int pass = 0; pass < 2; ++pass)
@@ -341,30 +351,33 @@ __device__ void stageFactors(Stage<T, CAP, DF>& S, DevGroup const& G, int lane)
         for (int s = S.blockBegin[e] + lane; s < S.blockBegin[e + 1]; s += 32)
         {
             const T r = S.r[s];
-            for (int q = 0; q < G.numBases && q < kMaxStagedBases; ++q) S.E[q][s] = fexp<T>(-(T)G.baseEta[q] * r * r);
+            for (int q = 0; q < G.numBases && q < NB; ++q) S.E[q][s] = fexp<T>(-(T)G.baseEta[q] * r * r);
         }
     }
     __syncwarp();
 }
 
-template <typename T>
-__device__ void stageMembers(Members<T>& mb, DevModel const& model, DevGroup const& G, const double* dEdG, int lane)
+template <typename T, bool COMPACT>
+__device__ void stageMembers(Members<T, COMPACT>& mb, DevModel const& model, DevGroup const& G, const double* dEdG, int lane)
 {
     __syncwarp();
     for (int q = lane; q < G.memberCount; q += 32)
     {
         DevMember const& M = model.members[G.memberBegin + q];
         mb.cw[q] = dEdG ? (T)(dEdG[M.sf] * M.factorNorm) : T(0);
-        mb.zl[q] = (T)M.zetaLambda;
-        mb.fd[q] = (T)M.factorDeriv;
-        mb.lambda[q] = (T)M.lambda;
-        mb.zeta[q] = (T)M.zeta;
         mb.eta[q] = (T)M.eta;
         mb.rs[q] = (T)M.rs;
-        mb.zint[q] = M.zetaInt;
         mb.base[q] = M.expBase;
         mb.pw[q] = M.expPow;
-        mb.flags[q] = (M.useIntPow ? 1 : 0) | (M.calcExp ? 2 : 0);
+        if constexpr (!COMPACT)
+        {
+            mb.zl[q] = (T)M.zetaLambda;
+            mb.fd[q] = (T)M.factorDeriv;
+            mb.lambda[q] = (T)M.lambda;
+            mb.zeta[q] = (T)M.zeta;
+            mb.zint[q] = M.zetaInt;
+            mb.flags[q] = (M.useIntPow ? 1 : 0) | (M.calcExp ? 2 : 0);
+        }
     }
     if (G.grid && lane < 16)
     {
@@ -396,8 +409,8 @@ __device__ __noinline__ T gaussShifted(T eta, T rs, T r1, T r2, T r3, int narrow
     return fexp<T>(-eta * (u * u + v * v + (narrow ? w * w : T(0))));
 }
 
-template <typename T>
-__device__ __forceinline__ T angularPow(T pl, Members<T> const& mb, int q)
+template <typename T, bool COMPACT>
+__device__ __forceinline__ T angularPow(T pl, Members<T, COMPACT> const& mb, int q)
 {
     return (mb.flags[q] & 1) ? powInt<T>(pl, mb.zint[q] - 1) : powReal<T>(pl, mb.zeta[q] - T(1));
 }
@@ -412,8 +425,8 @@ struct Triplet
     T rinv, cost, fcjk, dfcjk;
 };
 
-template <typename T, int CAP, bool DF>
-__device__ __forceinline__ void loadTriplet(Stage<T, CAP, DF> const& S, DevCutoff const& cut, bool narrow, int so, int sp,
+template <typename T, int CAP, bool DF, int NB>
+__device__ __forceinline__ void loadTriplet(Stage<T, CAP, DF, NB> const& S, DevCutoff const& cut, bool narrow, int so, int sp,
                                             Triplet<T>& t)
 {
     t.x1 = S.x[so];
@@ -451,15 +464,21 @@ __device__ __forceinline__ void loadTriplet(Stage<T, CAP, DF> const& S, DevCutof
     }
 }
 
-// Gaussian bases of a triplet: E_b(rij) E_b(rik) exp(-eta_b rjk^2).
-template <typename T, int CAP, bool DF>
-__device__ __forceinline__ void tripletBases(Stage<T, CAP, DF> const& S, DevGroup const& G, bool narrow, int so, int sp,
+// Gaussian bases of a triplet: E_b(rij) E_b(rik) exp(-eta_b rjk^2)
+// (bv has kMaxStagedBases entries; bases beyond the stage's NB are 0).
+template <typename T, int CAP, bool DF, int NB>
+__device__ __forceinline__ void tripletBases(Stage<T, CAP, DF, NB> const& S, DevGroup const& G, bool narrow, int so, int sp,
                                              T rjk2, T* bv)
 {
 #pragma unroll
     for (int q = 0; q < kMaxStagedBases; ++q)
-        bv[q] = (q < G.numBases) ? S.E[q][so] * S.E[q][sp] * (narrow ? fexp<T>(-(T)G.baseEta[q] * rjk2) : T(1))
-                                 : T(0);
+    {
+        if (q < NB)
+            bv[q] = (q < G.numBases) ? S.E[q][so] * S.E[q][sp] * (narrow ? fexp<T>(-(T)G.baseEta[q] * rjk2) : T(1))
+                                     : T(0);
+        else
+            bv[q] = T(0);
+    }
 }
 
 // Binary powers of x shared by several exponents: x^e for 0 <= e < 32 with
@@ -514,8 +533,8 @@ __device__ __forceinline__ void gridValues(T const* bv, DevGroup const& G, T cos
 
 // Member grid, force pass: the dE/dG-weighted member sums T1, T2 (= Uij =
 // Ujk, rs = 0) and T3 of one triplet.
-template <typename T, int NZ>
-__device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Members<T> const& mb, T cost, T& T1, T& T2,
+template <typename T, int NZ, bool COMPACT>
+__device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Members<T, COMPACT> const& mb, T cost, T& T1, T& T2,
                                            T& T3)
 {
     T vS[2];
@@ -550,13 +569,14 @@ __device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Membe
 // ---------------------------------------------------------------------------
 // G values
 // ---------------------------------------------------------------------------
-template <typename T, int CAP, int WARPS, int LOWER, int FAST>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(DevModel model, BatchView b)
+template <typename T, int CAP, int WARPS, int FAST>
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(DevModel model, BatchView b, int lower,
+                                                                     int flagOverflow)
 {
     extern __shared__ __align__(16) unsigned char smemRaw[];
-    ValuesSmem<T, CAP>& SM = reinterpret_cast<ValuesSmem<T, CAP>*>(smemRaw)[threadIdx.x >> 5];
+    ValuesSmem<T, CAP, FAST>& SM = reinterpret_cast<ValuesSmem<T, CAP, FAST>*>(smemRaw)[threadIdx.x >> 5];
     auto& S = SM.st;
-    Members<T>& mb = SM.mb;
+    auto& mb = SM.mb;
     const int lane = threadIdx.x & 31;
     // Accumulators per sweep: the member grid of the model (FAST = its zeta
     // slots) or a chunk of members.
@@ -568,12 +588,12 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
         const int64_t end = b.nbrOffset[i + 1];
         if (end > b.nbrCapacity) continue;
         const int n = (int)(end - off);
-        if (LOWER >= 0 && n > CAP)
+        if (flagOverflow && n > CAP)
         {
             if (lane == 0) atomicAdd(&b.status->badInput, 1);
             continue;
         }
-        if (!(n <= CAP && n > LOWER)) continue;
+        if (!(n <= CAP && n > lower)) continue;
         const int ec = b.elem[i];
         DevElement const& E = model.el[ec];
         stageGeometry<T, CAP>(S, off, n, model.numElements, b, lane);
@@ -677,19 +697,21 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                                         else if (G.gridNZ <= 2) gridValues<T, 2, 4>(bv, G, t.cost, pfc, acc);
                                         else gridValues<T, 4, 4>(bv, G, t.cost, pfc, acc);
                                     }
-                                    else
-#pragma unroll
-                                    for (int q = 0; q < ACC; ++q)
+                                    else if constexpr (FAST == 0)
                                     {
-                                        if (q < mc)
+#pragma unroll
+                                        for (int q = 0; q < ACC; ++q)
                                         {
-                                            const int qq = m0 + q;
-                                            if ((mb.flags[qq] & 2) || q == 0)
-                                                vexp = fastG ? Powers<T>(mb.base[qq] == 0 ? bv[0] : bv[1]).pow(mb.pw[qq])
-                                                              : gaussShifted<T>(mb.eta[qq], mb.rs[qq], t.r1, t.r2,
-                                                                                t.rjk, narrow ? 1 : 0);
-                                            const T pl = T(1) + mb.lambda[qq] * t.cost;
-                                            if (pl > T(0)) acc[q] += vexp * angularPow<T>(pl, mb, qq) * pl * pfc;
+                                            if (q < mc)
+                                            {
+                                                const int qq = m0 + q;
+                                                if ((mb.flags[qq] & 2) || q == 0)
+                                                    vexp = fastG ? Powers<T>(mb.base[qq] == 0 ? bv[0] : bv[1]).pow(mb.pw[qq])
+                                                                 : gaussShifted<T>(mb.eta[qq], mb.rs[qq], t.r1, t.r2,
+                                                                                   t.rjk, narrow ? 1 : 0);
+                                                const T pl = T(1) + mb.lambda[qq] * t.cost;
+                                                if (pl > T(0)) acc[q] += vexp * angularPow<T>(pl, mb, qq) * pl * pfc;
+                                            }
                                         }
                                     }
                                 }
@@ -739,13 +761,13 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
 // Pairs are enumerated in rounds of matchings, so the lanes of one round add
 // their two contributions to distinct slots; rounds add one after another in
 // a fixed order (deterministic, no atomics).
-template <typename T, int CAP, int WARPS, int LOWER, int FAST>
-__global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchView b)
+template <typename T, int CAP, int WARPS, int FAST>
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(DevModel model, BatchView b, int lower)
 {
     extern __shared__ __align__(16) unsigned char smemRaw[];
-    ForcesSmem<T, CAP>& SM = reinterpret_cast<ForcesSmem<T, CAP>*>(smemRaw)[threadIdx.x >> 5];
+    ForcesSmem<T, CAP, FAST>& SM = reinterpret_cast<ForcesSmem<T, CAP, FAST>*>(smemRaw)[threadIdx.x >> 5];
     auto& S = SM.st;
-    Members<T>& mb = SM.mb;
+    auto& mb = SM.mb;
     const int lane = threadIdx.x & 31;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
@@ -754,7 +776,7 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
         const int64_t end = b.nbrOffset[i + 1];
         if (end > b.nbrCapacity) continue;
         const int n = (int)(end - off);
-        if (!(n <= CAP && n > LOWER)) continue;
+        if (!(n <= CAP && n > lower)) continue;
         const int ec = b.elem[i];
         DevElement const& E = model.el[ec];
         const double* dEdG = b.dEdG + (size_t)i * b.gStride;
@@ -870,7 +892,8 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                                 Uik = T2;
                                 Ujk = T2;
                             }
-                            else
+                            else if constexpr (FAST == 0)
+                            {
                             for (int q = 0; q < M; ++q)
                             {
                                 if ((mb.flags[q] & 2) || q == 0)
@@ -896,6 +919,7 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
                                     Uik += azq;
                                     Ujk += azq;
                                 }
+                            }
                             }
                             // both ends of the unordered pair (j, k): P1 for j, P2 (= P1 with j, k
                             // exchanged) for k; P3 is symmetric and enters with opposite signs.
@@ -959,69 +983,6 @@ __global__ void __launch_bounds__(WARPS * 32) kSFForcesF(DevModel model, BatchVi
         }
         __syncwarp();
     }
-}
-
-// ---------------------------------------------------------------------------
-// Launch wrappers
-// ---------------------------------------------------------------------------
-namespace {
-
-constexpr int kStdCapF = 160, kStdWarpsF = 4;
-constexpr int kBigCapF = 1024, kBigWarpsF = 1;
-
-int gridFor(int N, int warpsPerBlock, int sms, int perSM)
-{
-    int need = (N + warpsPerBlock - 1) / warpsPerBlock;
-    int cap = sms * perSM;
-    return need < cap ? (need > 0 ? need : 1) : cap;
-}
-
-template <typename T>
-void valuesT(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
-{
-    const size_t s1 = sizeof(ValuesSmem<T, kStdCapF>) * kStdWarpsF;
-    const size_t s2 = sizeof(ValuesSmem<T, kBigCapF>) * kBigWarpsF;
-    auto k1 = m.allFast == 2 ? kSFValuesF<T, kStdCapF, kStdWarpsF, -1, 2>
-            : m.allFast == 4 ? kSFValuesF<T, kStdCapF, kStdWarpsF, -1, 4>
-                             : kSFValuesF<T, kStdCapF, kStdWarpsF, -1, 0>;
-    auto k2 = m.allFast == 2 ? kSFValuesF<T, kBigCapF, kBigWarpsF, kStdCapF, 2>
-            : m.allFast == 4 ? kSFValuesF<T, kBigCapF, kBigWarpsF, kStdCapF, 4>
-                             : kSFValuesF<T, kBigCapF, kBigWarpsF, kStdCapF, 0>;
-    setDynamicSmemOnce(reinterpret_cast<const void*>(k1), s1);
-    setDynamicSmemOnce(reinterpret_cast<const void*>(k2), s2);
-    k1<<<gridFor(b.N, kStdWarpsF, sms, 32), kStdWarpsF * 32, s1, st>>>(m, b);
-    k2<<<sms, kBigWarpsF * 32, s2, st>>>(m, b);
-}
-
-template <typename T>
-void forcesT(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
-{
-    const size_t s1 = sizeof(ForcesSmem<T, kStdCapF>) * kStdWarpsF;
-    const size_t s2 = sizeof(ForcesSmem<T, kBigCapF>) * kBigWarpsF;
-    auto k1 = m.allFast == 2 ? kSFForcesF<T, kStdCapF, kStdWarpsF, -1, 2>
-            : m.allFast == 4 ? kSFForcesF<T, kStdCapF, kStdWarpsF, -1, 4>
-                             : kSFForcesF<T, kStdCapF, kStdWarpsF, -1, 0>;
-    auto k2 = m.allFast == 2 ? kSFForcesF<T, kBigCapF, kBigWarpsF, kStdCapF, 2>
-            : m.allFast == 4 ? kSFForcesF<T, kBigCapF, kBigWarpsF, kStdCapF, 4>
-                             : kSFForcesF<T, kBigCapF, kBigWarpsF, kStdCapF, 0>;
-    setDynamicSmemOnce(reinterpret_cast<const void*>(k1), s1);
-    setDynamicSmemOnce(reinterpret_cast<const void*>(k2), s2);
-    k1<<<gridFor(b.N, kStdWarpsF, sms, 32), kStdWarpsF * 32, s1, st>>>(m, b);
-    k2<<<sms, kBigWarpsF * 32, s2, st>>>(m, b);
-}
-
-} // namespace
-
-void launchSFValues(DevModel const& m, BatchView const& b, int precision, int sms, cudaStream_t st)
-{
-    if (precision == 0) valuesT<double>(m, b, sms, st);
-    else valuesT<float>(m, b, sms, st);
-}
-
-void launchSFForces(DevModel const& m, BatchView const& b, int precision, int sms, cudaStream_t st)
-{
-    if (precision == 0) forcesT<double>(m, b, sms, st);
-    else forcesT<float>(m, b, sms, st);
 }
 
 } // namespace n2p2b200

@@ -77,6 +77,10 @@ class Mode:
         p = {"fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}.get(precision, precision)
         _lib.check(self._lib.n2p2_mode_set_precision(self._h, int(p)))
 
+    def setAutotune(self, enabled=True):
+        """Automatic choice of the symmetry-function kernel shapes (default on)."""
+        _lib.check(self._lib.n2p2_mode_set_autotune(self._h, int(bool(enabled))))
+
     def setupFromDirectory(self, d, fp=None):
         """Prediction::setup sequence on a model directory."""
         self.initialize()
@@ -289,6 +293,22 @@ class Batch:
         _lib.check(self._lib.n2p2_batch_get_extrapolation_warnings(self._h, ctypes.byref(t),
                                                                    per.ctypes.data_as(_P(ctypes.c_int32))))
         return t.value, per
+
+    SHAPES = ((128, 4), (160, 4), (192, 2))   # (stage capacity, warps per block) per shape index
+
+    def autotune(self, useCache=True):
+        """Times the three kernel shapes of both symmetry-function passes (the
+        batch must have been evaluated once) and keeps the fastest."""
+        sh = np.zeros(2, dtype=np.int32)
+        ms = np.zeros(6)
+        fc = ctypes.c_int32()
+        _lib.check(self._lib.n2p2_batch_autotune(self._h, int(bool(useCache)), sh.ctypes.data_as(_P(ctypes.c_int32)),
+                                                 _dp(ms), ctypes.byref(fc)))
+        return {"values": int(sh[0]), "forces": int(sh[1]), "values_ms": ms[:3].tolist(),
+                "forces_ms": ms[3:].tolist(), "from_cache": bool(fc.value)}
+
+    def setShapes(self, values, forces):
+        _lib.check(self._lib.n2p2_batch_set_shapes(self._h, int(values), int(forces)))
 
     def stream(self):
         s = ctypes.c_void_p()
