@@ -140,7 +140,8 @@ struct DevStatus
     int64_t totalNeighbors;
     int extrapolationWarnings;
     int badInput;
-    int pad_[2];
+    int tensorCoreTimeout;   // a tensor-core network tile gave up waiting for its MMAs
+    int pad_;
 };
 
 } // namespace n2p2b200

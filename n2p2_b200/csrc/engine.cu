@@ -476,6 +476,7 @@ void DeviceModel::upload(Model const& m)
     mix(&v.allFast, sizeof(int));
     mix(v.cutoff, sizeof(v.cutoff));
     fingerprint = h;
+    tcNetwork = networkTCSupported(m);
     v.weightsF = weightsF_;
     view = v;
     this->maxSF = maxSF;
@@ -581,6 +582,21 @@ void Batch::setStructures(std::vector<StructureInput> const& s, const int* eleme
     }
 
     allocateAtoms();
+    // atoms grouped by element (the tensor-core networks run per element)
+    {
+        std::vector<int> order;
+        order.reserve(N_);
+        v_.elemBegin[0] = 0;
+        for (int e = 0; e < ne; ++e)
+        {
+            for (int a = 0; a < N_; ++a)
+                if (elemHost_[a] == e) order.push_back(a);
+            v_.elemBegin[e + 1] = (int)order.size();
+        }
+        int* dev = devAlloc<int>(pool_, (size_t)N_, owned_);
+        cudaCheck(cudaMemcpy(dev, order.data(), sizeof(int) * (size_t)N_, cudaMemcpyHostToDevice), "upload element lists");
+        v_.elemAtoms = dev;
+    }
     v_.numCells = cellTotal;
     v_.cellCount = devAlloc<int>(pool_, cellTotal, owned_);
     v_.cellStart = devAlloc<int>(pool_, cellTotal, owned_);
@@ -744,7 +760,8 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         launches += 1;
         mark("extrapolation_check");
     }
-    launchNetworkFP64(m, v_, forces ? 1 : 0, sms_, stream_);
+    if (precision == PREC_MIXED && dmodel_.tcNetwork) launchNetworkTC(m, v_, forces ? 1 : 0, sms_, stream_);
+    else launchNetworkFP64(m, v_, forces ? 1 : 0, sms_, stream_);
     launches += 1;
     mark("network");
     launchEnergySum(v_, stream_);
@@ -1037,6 +1054,8 @@ DevStatus Batch::status()
     synchronize();
     if (st.badInput) throw std::runtime_error("ERROR: invalid input detected on the device (atoms outside the cell, "
                                               "asymmetric neighbour pairs or more than 2048 neighbours).\n");
+    if (st.tensorCoreTimeout) throw std::runtime_error("ERROR: a tensor-core network tile timed out waiting for its "
+                                                       "matrix products.\n");
     return st;
 }
 

@@ -27,6 +27,11 @@ enum EvalFlags : int {
 
 void cudaCheck(cudaError_t e, char const* what);
 
+// Whether the model's networks fit the tensor-core kernel of the mixed form
+// (two hidden layers of <= 64 neurons, <= 64 inputs, linear output, no
+// normalize_nodes).
+bool networkTCSupported(Model const& m);
+
 // Device memory cache of one batch: blocks given back by put() are handed out
 // again for requests of the same size class, so re-setting structures of
 // similar size allocates nothing.  Every user of a batch's memory works on
@@ -54,6 +59,7 @@ public:
     int maxSF = 0;
     size_t numWeights = 0;               // entries of the flat weight array
     uint64_t fingerprint = 0;            // hash of the evaluation plan (groups, members, cutoffs)
+    bool tcNetwork = false;              // mixed form runs the networks on the tensor cores
     double* weightsDevice() const { return weights_; }
     float* weightsFDevice() const { return weightsF_; }
 

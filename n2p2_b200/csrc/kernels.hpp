@@ -30,6 +30,8 @@ struct BatchView
     int* cellStart = nullptr;
     int64_t* cellStart64 = nullptr;
     int* cellAtoms = nullptr;
+    const int* elemAtoms = nullptr;    // atoms grouped by element (ascending within an element)
+    int elemBegin[kDevMaxElements + 1] = {0};
     double4* cellPos = nullptr;        // cell-ordered (x, y, z, atom index)
     int64_t* scanTmp = nullptr;
     // neighbour CSR
@@ -104,6 +106,9 @@ void launchContractStored(DevModel const& m, BatchView const& b, int sms, cudaSt
 
 // networks, energies, forces
 void launchNetworkFP64(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st);
+// Tensor-core (tcgen05, split bfloat16) networks of the mixed form; models
+// with two hidden layers of <= 64 neurons, <= 64 inputs, linear output.
+void launchNetworkTC(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st);
 void launchEnergySum(BatchView const& b, cudaStream_t st);
 void launchGatherForces(BatchView const& b, int sms, cudaStream_t st);
 void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
