@@ -481,31 +481,37 @@ __device__ __forceinline__ void tripletBases(Stage<T, CAP, DF, NB> const& S, Dev
     }
 }
 
-// Binary powers of x shared by several exponents: x^e for 0 <= e < 32 with
-// the multiplication order of pow_int (utility.cpp:292-316) -- start from 1,
-// multiply in x^(2^k) for every set bit in increasing k -- without loops or
-// data-dependent branches.
+// x^e for a warp-uniform 0 <= e < 32, in pow_int's multiplication order
+// (result = 1, times x^(2^k) for each set bit k in increasing k;
+// utility.cpp:292-316).  FP64: square-and-multiply over the set bits only
+// (uniform branches, no lane diverges); FP32: a branch-free ladder over all
+// five bits, cheaper where multiplies cost less than branches.
 template <typename T>
-struct Powers
+__device__ __forceinline__ T powUniform(T x, int e)
 {
-    T p1, p2, p4, p8, p16;
-    __device__ __forceinline__ explicit Powers(T x) : p1(x)
+    if constexpr (sizeof(T) == 8)
     {
-        p2 = p1 * p1;
-        p4 = p2 * p2;
-        p8 = p4 * p4;
-        p16 = p8 * p8;
+        T r = T(1);
+#pragma unroll 1
+        while (e)
+        {
+            if (e & 1) r *= x;
+            e >>= 1;
+            if (e) x *= x;
+        }
+        return r;
     }
-    __device__ __forceinline__ T pow(int e) const
+    else
     {
-        T r = (e & 1) ? p1 : T(1);
+        const T p2 = x * x, p4 = p2 * p2, p8 = p4 * p4, p16 = p8 * p8;
+        T r = (e & 1) ? x : T(1);
         r = (e & 2) ? r * p2 : r;
         r = (e & 4) ? r * p4 : r;
         r = (e & 8) ? r * p8 : r;
         r = (e & 16) ? r * p16 : r;
         return r;
     }
-};
+}
 
 // Member grid, G pass: acc[(eta * 2 + lambda) * 4 + zeta] += E_eta * pl^zeta * pfc
 // (pl = 1 + lambda cos; terms with pl <= 0 vanish, SymGrpExpAngn.cpp:295).
@@ -514,17 +520,16 @@ __device__ __forceinline__ void gridValues(T const* bv, DevGroup const& G, T cos
 {
     T vS[2];
 #pragma unroll
-    for (int es = 0; es < 2; ++es) vS[es] = Powers<T>(G.etaBase[es] == 0 ? bv[0] : bv[1]).pow(G.etaPow[es]);
+    for (int es = 0; es < 2; ++es) vS[es] = powUniform<T>(G.etaBase[es] == 0 ? bv[0] : bv[1], G.etaPow[es]);
 #pragma unroll
     for (int ls = 0; ls < 2; ++ls)
     {
         const T pl = T(1) + (T)G.lambdaVal[ls] * cost;
         const T w = pl > T(0) ? pl * pfc : T(0);
-        const Powers<T> P(pl);
 #pragma unroll
         for (int zs = 0; zs < NZ; ++zs)
         {
-            const T pz = P.pow(G.zetaM1[zs]) * w;
+            const T pz = powUniform<T>(pl, G.zetaM1[zs]) * w;
 #pragma unroll
             for (int es = 0; es < 2; ++es) acc[(es * 2 + ls) * STRIDE + zs] += vS[es] * pz;
         }
@@ -539,17 +544,16 @@ __device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Membe
 {
     T vS[2];
 #pragma unroll
-    for (int es = 0; es < 2; ++es) vS[es] = Powers<T>(G.etaBase[es] == 0 ? bv[0] : bv[1]).pow(G.etaPow[es]);
+    for (int es = 0; es < 2; ++es) vS[es] = powUniform<T>(G.etaBase[es] == 0 ? bv[0] : bv[1], G.etaPow[es]);
 #pragma unroll
     for (int ls = 0; ls < 2; ++ls)
     {
         const T pl = T(1) + (T)G.lambdaVal[ls] * cost;
         const bool valid = pl > T(0);
-        const Powers<T> P(pl);
 #pragma unroll
         for (int zs = 0; zs < NZ; ++zs)
         {
-            const T pz1 = valid ? P.pow(G.zetaM1[zs]) : T(0);
+            const T pz1 = valid ? powUniform<T>(pl, G.zetaM1[zs]) : T(0);
 #pragma unroll
             for (int es = 0; es < 2; ++es)
             {
@@ -644,7 +648,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
 #pragma unroll
                                     for (int t = 1; t < kMaxBases; ++t)
                                         if (bq == t) e0 = eb[t];
-                                    v = Powers<T>(e0).pow(mb.pw[qq]);
+                                    v = powUniform<T>(e0, mb.pw[qq]);
                                 }
                                 else v = gaussShifted<T>(mb.eta[qq], mb.rs[qq], r, mb.rs[qq], mb.rs[qq], 0);
                                 acc[q] += v * fc;
@@ -706,7 +710,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                                             {
                                                 const int qq = m0 + q;
                                                 if ((mb.flags[qq] & 2) || q == 0)
-                                                    vexp = fastG ? Powers<T>(mb.base[qq] == 0 ? bv[0] : bv[1]).pow(mb.pw[qq])
+                                                    vexp = fastG ? powUniform<T>(mb.base[qq] == 0 ? bv[0] : bv[1], mb.pw[qq])
                                                                  : gaussShifted<T>(mb.eta[qq], mb.rs[qq], t.r1, t.r2,
                                                                                    t.rjk, narrow ? 1 : 0);
                                                 const T pl = T(1) + mb.lambda[qq] * t.cost;
@@ -818,7 +822,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(Dev
 #pragma unroll
                             for (int t = 1; t < kMaxBases; ++t)
                                 if (bq == t) e0 = eb[t];
-                            v = Powers<T>(e0).pow(mb.pw[q]);
+                            v = powUniform<T>(e0, mb.pw[q]);
                         }
                         else v = gaussShifted<T>(mb.eta[q], mb.rs[q], r, mb.rs[q], mb.rs[q], 0);
                         P += mb.cw[q] * (dfc - T(2) * mb.eta[q] * (r - mb.rs[q]) * fc) * v * ri;
@@ -897,7 +901,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(Dev
                             for (int q = 0; q < M; ++q)
                             {
                                 if ((mb.flags[q] & 2) || q == 0)
-                                    vexp = fastG ? Powers<T>(mb.base[q] == 0 ? bv[0] : bv[1]).pow(mb.pw[q])
+                                    vexp = fastG ? powUniform<T>(mb.base[q] == 0 ? bv[0] : bv[1], mb.pw[q])
                                                   : gaussShifted<T>(mb.eta[q], mb.rs[q], t.r1, t.r2, t.rjk,
                                                                     narrow ? 1 : 0);
                                 const T pl = T(1) + mb.lambda[q] * t.cost;
