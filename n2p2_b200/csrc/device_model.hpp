@@ -142,6 +142,7 @@ struct DevStatus
     int badInput;
     int tensorCoreTimeout;   // a tensor-core network tile gave up waiting for its MMAs
     int pad_;
+    int64_t maskWords;       // candidate-acceptance words the evaluation needs (Batch::allocateMasks)
 };
 
 } // namespace n2p2b200

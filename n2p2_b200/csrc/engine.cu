@@ -507,6 +507,9 @@ void Batch::releaseGraph()
 void Batch::releaseAll()
 {
     releaseGraph();
+    freeAll(pool_, ownedMask_);
+    maskBuf_ = nullptr;
+    maskCap_ = 0;
     freeAll(pool_, ownedDGdr_);
     freeAll(pool_, ownedNbr_);
     freeAll(pool_, owned_);
@@ -653,6 +656,8 @@ void Batch::allocateAtoms()
     v_.fSelf = devAlloc<double>(pool_, 3 * (size_t)N, owned_);
     v_.F = devAlloc<double>(pool_, 3 * (size_t)N, owned_);
     v_.atomWarnings = devAlloc<int>(pool_, N, owned_);
+    v_.maskWords = devAlloc<int>(pool_, N, owned_);
+    v_.maskOffset = devAlloc<int64_t>(pool_, (size_t)N + 1, owned_);
     v_.status = devAlloc<DevStatus>(pool_, 1, owned_);
     // Pool blocks hold a previous user's data: clear what may be read before
     // the first evaluation writes it.
@@ -742,6 +747,17 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
     launchCutoffValues(m, v_, sms_, stream_);
     launches += 1;
     mark("cutoff_values");
+    // the G pass records its candidate acceptance for the force pass
+    v_.candMask = nullptr;
+    v_.maskCapacity = 0;
+    if (forces && !stored)
+    {
+        launchMaskOffsets(m, v_, sms_, stream_);
+        launches += 4;
+        mark("candidate_masks");
+        v_.candMask = maskBuf_;
+        v_.maskCapacity = maskBuf_ ? maskCap_ : 0;
+    }
     if (stored)
     {
         launchSFDerivatives(m, v_, sms_, stream_);
@@ -1013,6 +1029,14 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
         }
         DevStatus st = status();
         if (st.totalNeighbors > capacity_) throw std::runtime_error("ERROR: neighbour capacity could not be established.\n");
+        if ((flags & EVAL_FORCES) && st.maskWords > maskCap_)
+        {
+            // room for the candidate masks (atoms beyond it test their candidates again)
+            releaseGraph();
+            freeAll(pool_, ownedMask_);
+            maskCap_ = st.maskWords + st.maskWords / 4 + 4096;
+            maskBuf_ = devAlloc<uint32_t>(pool_, (size_t)maskCap_, ownedMask_);
+        }
         capacityVerified_ = true;
         return;
     }

@@ -196,6 +196,9 @@ private:
     std::vector<void*> owned_;
     std::vector<void*> ownedNbr_;
     std::vector<void*> ownedDGdr_;
+    std::vector<void*> ownedMask_;
+    uint32_t* maskBuf_ = nullptr;
+    int64_t maskCap_ = 0;
 };
 
 } // namespace n2p2b200

@@ -3,6 +3,58 @@
 
 namespace n2p2b200 {
 
+namespace {
+
+// Words of acceptance ballots the G pass records for atom i: two per 64
+// candidates of every angular group (the candidate counts of roundPhases,
+// from the numbers of neighbours of each element).
+__global__ void kMaskWords(DevModel model, BatchView b)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
+    {
+        const int64_t off = b.nbrOffset[i], end = b.nbrOffset[i + 1];
+        int cnt[kDevMaxElements];
+        for (int e = 0; e < kDevMaxElements; ++e) cnt[e] = 0;
+        if (end <= b.nbrCapacity)
+            for (int64_t q = off + lane; q < end; q += 32)
+            {
+                const int e = b.elem[b.nbrJ[q]];
+                for (int f = 0; f < kDevMaxElements; ++f) cnt[f] += (e == f) ? 1 : 0;
+            }
+        for (int f = 0; f < model.numElements; ++f) cnt[f] = warpSumInt(cnt[f]);
+        DevElement const& E = model.el[b.elem[i]];
+        int words = 0;
+        for (int g = 0; g < E.groupCount; ++g)
+        {
+            DevGroup const& G = model.groups[E.groupBegin + g];
+            if (G.type == 2) continue;
+            const int nA = cnt[G.e1], nB = cnt[G.e2];
+            int64_t count;
+            if (G.e1 == G.e2)
+            {
+                const int m = nA + (nA & 1);
+                count = nA < 2 ? 0 : (int64_t)(m - 1) * (m / 2);
+            }
+            else count = (int64_t)nA * nB;
+            words += 2 * (int)((count + 63) / 64);
+        }
+        if (lane == 0) b.maskWords[i] = words;
+    }
+}
+
+} // namespace
+
+void launchMaskOffsets(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
+{
+    int blocks = (b.N + 7) / 8;
+    if (blocks < 1) blocks = 1;
+    if (blocks > sms * 16) blocks = sms * 16;
+    kMaskWords<<<blocks, 256, 0, st>>>(m, b);
+    launchExclusiveScan(b.N, b.maskWords, b.maskOffset, b.scanTmp, &b.status->maskWords, st);
+}
+
 void launchSFValuesF64(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int variant)
 {
     valuesT<double>(m, b, sms, st, variant);

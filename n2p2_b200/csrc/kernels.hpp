@@ -31,6 +31,12 @@ struct BatchView
     int64_t* cellStart64 = nullptr;
     int* cellAtoms = nullptr;
     const int* elemAtoms = nullptr;    // atoms grouped by element (ascending within an element)
+    // Acceptance ballots of the G pass's candidate pairs (two words per
+    // 64-candidate step, groups in order), read back by the force pass.
+    uint32_t* candMask = nullptr;
+    int* maskWords = nullptr;          // per atom
+    int64_t* maskOffset = nullptr;     // N+1
+    int64_t maskCapacity = 0;
     int elemBegin[kDevMaxElements + 1] = {0};
     double4* cellPos = nullptr;        // cell-ordered (x, y, z, atom index)
     int64_t* scanTmp = nullptr;
@@ -106,6 +112,8 @@ void launchContractStored(DevModel const& m, BatchView const& b, int sms, cudaSt
 
 // networks, energies, forces
 void launchNetworkFP64(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st);
+// Per-atom acceptance-word counts of the angular groups and their offsets.
+void launchMaskOffsets(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 // Tensor-core (tcgen05, split bfloat16) networks of the mixed form; models
 // with two hidden layers of <= 64 neurons, <= 64 inputs, linear output.
 void launchNetworkTC(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st);

@@ -227,15 +227,38 @@ __device__ __forceinline__ bool testCandidate(Stage<T, CAP, DF, NB> const& S, Ph
 
 template <typename T, int CAP, bool DF, int NB>
 __device__ __forceinline__ void enqueueCandidates(Stage<T, CAP, DF, NB> const& S, Phase const& ph, Cursor& cur, int p0,
-                                                  T rc, T rc2, bool narrow, int* queue, int qh, int& qn, int lane)
+                                                  T rc, T rc2, bool narrow, int* queue, int qh, int& qn, int lane,
+                                                  uint32_t* maskOut, const uint32_t* maskIn, int& mwi)
 {
     Cursor c2 = cur;
     c2.advance(ph);
     int e1, e2;
-    const bool ok1 = testCandidate<T, CAP>(S, ph, cur, p0 + lane, rc, rc2, narrow, e1);
-    const bool ok2 = testCandidate<T, CAP>(S, ph, c2, p0 + 32 + lane, rc, rc2, narrow, e2);
-    const unsigned m1 = __ballot_sync(kFullMask, ok1);
-    const unsigned m2 = __ballot_sync(kFullMask, ok2);
+    unsigned m1, m2;
+    if (maskIn)
+    {
+        // acceptance recorded by the G pass for these 64 candidates
+        m1 = __ldg(maskIn + mwi);
+        m2 = __ldg(maskIn + mwi + 1);
+        int so, sp;
+        cur.slots(ph, so, sp);
+        e1 = (cur.round(ph) << 20) | (so << 10) | sp;
+        c2.slots(ph, so, sp);
+        e2 = (c2.round(ph) << 20) | (so << 10) | sp;
+    }
+    else
+    {
+        const bool ok1 = testCandidate<T, CAP>(S, ph, cur, p0 + lane, rc, rc2, narrow, e1);
+        const bool ok2 = testCandidate<T, CAP>(S, ph, c2, p0 + 32 + lane, rc, rc2, narrow, e2);
+        m1 = __ballot_sync(kFullMask, ok1);
+        m2 = __ballot_sync(kFullMask, ok2);
+        if (maskOut && lane == 0)
+        {
+            maskOut[mwi] = m1;
+            maskOut[mwi + 1] = m2;
+        }
+    }
+    mwi += 2;
+    const bool ok1 = (m1 >> lane) & 1u, ok2 = (m2 >> lane) & 1u;
     const unsigned below = (1u << lane) - 1u;
     if (ok1) queue[(qh + qn + __popc(m1 & below)) & (kQueue - 1)] = e1;
     if (ok2) queue[(qh + qn + __popc(m1) + __popc(m2 & below)) & (kQueue - 1)] = e2;
@@ -600,6 +623,9 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
         if (!(n <= CAP && n > lower)) continue;
         const int ec = b.elem[i];
         DevElement const& E = model.el[ec];
+        uint32_t* maskOut =
+            (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
+        int mwi = 0;
         stageGeometry<T, CAP>(S, off, n, model.numElements, b, lane);
         int slot = -1;
         for (int g = 0; g < E.groupCount; ++g)
@@ -617,8 +643,10 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
             const DevMember* mem = model.members + G.memberBegin;
             const bool narrow = (G.type == 3);
             const bool grid = (G.type != 2) && (FAST || G.grid);
+            const int mwiGroup = mwi;
             for (int m0 = 0; m0 < G.memberCount; m0 += (grid ? G.memberCount : ACC))
             {
+                mwi = mwiGroup;   // every member chunk enumerates the same candidates; the first records them
                 const int mc = min(ACC, G.memberCount - m0);
                 T acc[ACC];
 #pragma unroll
@@ -679,7 +707,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                         {
                             if (qn < 32 && p0 < cnt)   // queue stays below 32 + 64 entries
                             {
-                                enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane);
+                                enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane,
+                                                          m0 == 0 ? maskOut : nullptr, nullptr, mwi);
                                 p0 += 64;
                             }
                             if (qn >= 32 || (drain && qn > 0))
@@ -784,6 +813,9 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(Dev
         const int ec = b.elem[i];
         DevElement const& E = model.el[ec];
         const double* dEdG = b.dEdG + (size_t)i * b.gStride;
+        const uint32_t* maskIn =
+            (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
+        int mwi = 0;
         stageGeometry<T, CAP>(S, off, n, model.numElements, b, lane);
         for (int s = lane; s < n; s += 32) SM.h[0][s] = SM.h[1][s] = SM.h[2][s] = 0.0;
         double sfx = 0.0, sfy = 0.0, sfz = 0.0;
@@ -862,7 +894,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(Dev
                 {
                     if (qn < 32 && p0 < cnt)   // queue stays below 32 + 64 entries
                     {
-                        enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane);
+                        enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane,
+                                                  nullptr, maskIn, mwi);
                         p0 += 64;
                     }
                     if (qn >= 32 || (drain && qn > 0))
