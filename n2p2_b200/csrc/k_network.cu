@@ -188,43 +188,38 @@ __global__ void kEnergySum(BatchView b)
 }
 
 // F_i = self force + sum over neighbours j != i of the force E_j puts on i
-// (Mode::calculateForces 2G part, Mode.cpp:1922-1984).  The entries of i's
-// list that point at the same j are visited in reverse image order, so that
-// the contributions arrive in the order of j's own list, as in the reference.
+// (Mode::calculateForces 2G part, Mode.cpp:1922-1984): the force E_j puts on
+// i is stored on the reverse entry (j -> i) of each entry (i -> j).  One warp
+// per atom: lanes stride over the atom's entries (coalesced index loads) and
+// the partial sums are combined by a fixed shuffle tree, so the result is the
+// same on every run.
 __global__ void kGatherForces(BatchView b)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < b.N; i += gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
     {
         const int64_t off = b.nbrOffset[i];
         const int64_t end = b.nbrOffset[i + 1];
-        double fx = b.fSelf[3 * (size_t)i + 0];
-        double fy = b.fSelf[3 * (size_t)i + 1];
-        double fz = b.fSelf[3 * (size_t)i + 2];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
         if (end <= b.nbrCapacity)
-        {
-            int64_t e = off;
-            while (e < end)
+            for (int64_t e = off + lane; e < end; e += 32)
             {
-                const int j = b.nbrJ[e];
-                int64_t runEnd = e + 1;
-                while (runEnd < end && b.nbrJ[runEnd] == j) ++runEnd;
-                if (j != i)
-                {
-                    for (int64_t q = runEnd - 1; q >= e; --q)
-                    {
-                        const int64_t r = b.rev[q];
-                        if (r < 0) continue;
-                        fx += b.hx[r];
-                        fy += b.hy[r];
-                        fz += b.hz[r];
-                    }
-                }
-                e = runEnd;
+                const int64_t r = b.rev[e];
+                if (r < 0 || b.nbrJ[e] == i) continue;
+                fx += b.hx[r];
+                fy += b.hy[r];
+                fz += b.hz[r];
             }
+        fx = warpSum(fx);
+        fy = warpSum(fy);
+        fz = warpSum(fz);
+        if (lane == 0)
+        {
+            b.F[3 * (size_t)i + 0] = b.fSelf[3 * (size_t)i + 0] + fx;
+            b.F[3 * (size_t)i + 1] = b.fSelf[3 * (size_t)i + 1] + fy;
+            b.F[3 * (size_t)i + 2] = b.fSelf[3 * (size_t)i + 2] + fz;
         }
-        b.F[3 * (size_t)i + 0] = fx;
-        b.F[3 * (size_t)i + 1] = fy;
-        b.F[3 * (size_t)i + 2] = fz;
     }
 }
 
@@ -277,10 +272,10 @@ void launchEnergySum(BatchView const& b, cudaStream_t st)
 
 void launchGatherForces(BatchView const& b, int sms, cudaStream_t st)
 {
-    int blocks = (b.N + 127) / 128;
+    int blocks = (b.N + 7) / 8;
     if (blocks < 1) blocks = 1;
-    if (blocks > sms * 16) blocks = sms * 16;
-    kGatherForces<<<blocks, 128, 0, st>>>(b);
+    if (blocks > sms * 32) blocks = sms * 32;
+    kGatherForces<<<blocks, 256, 0, st>>>(b);
 }
 
 } // namespace n2p2b200
