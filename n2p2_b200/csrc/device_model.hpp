@@ -113,7 +113,7 @@ struct DevModel
     const DevScaling* scaling;
     const int*        rowTable;
     const double*     weights;
-    const float*      weightsF;       // FP32 copy for the mixed path
+    const double*     weightsT;       // weights with every matrix transposed ([n_{l-1}][n_l]), same offsets
 };
 
 // Per structure geometry for the neighbour build.

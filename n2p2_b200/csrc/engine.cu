@@ -218,13 +218,15 @@ void DeviceModel::release()
     cudaFree(scaling_);
     cudaFree(rowTable_);
     cudaFree(weights_);
-    cudaFree(weightsF_);
+    cudaFree(weightsT_);
+    cudaFree(transIndex_);
     groups_ = nullptr;
     members_ = nullptr;
     scaling_ = nullptr;
     rowTable_ = nullptr;
     weights_ = nullptr;
-    weightsF_ = nullptr;
+    weightsT_ = nullptr;
+    transIndex_ = nullptr;
 }
 
 void DeviceModel::upload(Model const& m)
@@ -447,7 +449,27 @@ void DeviceModel::upload(Model const& m)
         c.iw = 1.0 / (c.rc - c.rci);
         c.tanhPre = std::pow((E + 1 / E) / (E - 1 / E), 3);
     }
-    std::vector<float> weightsF(weights.begin(), weights.end());
+    // transposed copy of every weight matrix (same offsets; biases copied):
+    // element (k, j) of W_l [n_l x n_{l-1}] at j n_l + k, for reads that are
+    // contiguous over output neurons
+    std::vector<double> weightsT(weights);
+    transIndexHost.resize(weights.size());
+    for (size_t q = 0; q < weights.size(); ++q) transIndexHost[q] = (int)q;
+    for (std::size_t e = 0; e < m.elements.size(); ++e)
+    {
+        DevElement const& de = v.el[e];
+        for (int l = 1; l < de.numLayers; ++l)
+        {
+            const int nin = de.neurons[l - 1], nout = de.neurons[l];
+            for (int k = 0; k < nout; ++k)
+                for (int j = 0; j < nin; ++j)
+                {
+                    const int src = de.wOffset[l] + k * nin + j, dst = de.wOffset[l] + j * nout + k;
+                    weightsT[dst] = weights[src];
+                    transIndexHost[src] = dst;
+                }
+        }
+    }
     auto up = [](void** dst, void const* src, size_t bytes) {
         cudaCheck(cudaMalloc(dst, bytes ? bytes : 16), "cudaMalloc(model)");
         if (bytes) cudaCheck(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(model)");
@@ -457,7 +479,8 @@ void DeviceModel::upload(Model const& m)
     up((void**)&scaling_, scaling.data(), scaling.size() * sizeof(DevScaling));
     up((void**)&rowTable_, rowTable.data(), rowTable.size() * sizeof(int));
     up((void**)&weights_, weights.data(), weights.size() * sizeof(double));
-    up((void**)&weightsF_, weightsF.data(), weightsF.size() * sizeof(float));
+    up((void**)&weightsT_, weightsT.data(), weightsT.size() * sizeof(double));
+    up((void**)&transIndex_, transIndexHost.data(), transIndexHost.size() * sizeof(int));
     v.groups = groups_;
     v.members = members_;
     v.scaling = scaling_;
@@ -477,7 +500,7 @@ void DeviceModel::upload(Model const& m)
     mix(v.cutoff, sizeof(v.cutoff));
     fingerprint = h;
     tcNetwork = networkTCSupported(m);
-    v.weightsF = weightsF_;
+    v.weightsT = weightsT_;
     view = v;
     this->maxSF = maxSF;
 }

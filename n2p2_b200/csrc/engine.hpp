@@ -61,7 +61,9 @@ public:
     uint64_t fingerprint = 0;            // hash of the evaluation plan (groups, members, cutoffs)
     bool tcNetwork = false;              // mixed form runs the networks on the tensor cores
     double* weightsDevice() const { return weights_; }
-    float* weightsFDevice() const { return weightsF_; }
+    double* weightsTDevice() const { return weightsT_; }
+    int* transIndexDevice() const { return transIndex_; }
+    std::vector<int> transIndexHost;     // weight index -> index in the transposed copy
 
 private:
     void release();
@@ -70,7 +72,8 @@ private:
     DevScaling* scaling_ = nullptr;
     int* rowTable_ = nullptr;
     double* weights_ = nullptr;
-    float* weightsF_ = nullptr;
+    double* weightsT_ = nullptr;
+    int* transIndex_ = nullptr;
 };
 
 struct StructureInput

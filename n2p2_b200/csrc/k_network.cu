@@ -113,13 +113,12 @@ __global__ void __launch_bounds__(kNNWarps * 32) kNetworkFP64(DevModel model, Ba
         for (int l = 1; l < L; ++l)
         {
             const int nin = E.neurons[l - 1], nout = E.neurons[l];
-            const double* W = model.weights + E.wOffset[l];
+            const double* WT = model.weightsT + E.wOffset[l];   // lanes read consecutive output neurons
             const double* bias = model.weights + E.bOffset[l];
             for (int k = lane; k < nout; k += 32)
             {
                 double x = 0.0;
-                const double* row = W + (size_t)k * nin;
-                for (int j = 0; j < nin; ++j) x += __ldg(&row[j]) * S.act[cur][j];
+                for (int j = 0; j < nin; ++j) x += __ldg(&WT[(size_t)j * nout + k]) * S.act[cur][j];
                 x += __ldg(&bias[k]);
                 if (model.normalizeNeurons) x /= nin;
                 double y, dy;

@@ -290,10 +290,11 @@ __global__ void kReduceGrad(const double* __restrict__ gradPart, int warps, int 
 }
 
 // Adam (GradientDescent::update, DT_ADAM): m, v moments, step
-// eta0 sqrt(1 - beta2^t) / (1 - beta1^t); FP32 copy of the weights refreshed.
+// eta0 sqrt(1 - beta2^t) / (1 - beta1^t); the transposed weight copy is
+// refreshed as well.
 __global__ void kAdam(int P, const double* __restrict__ grad, double* __restrict__ m, double* __restrict__ v,
-                      double* __restrict__ w, float* __restrict__ wF, double beta1, double beta2, double eta,
-                      double eps)
+                      double* __restrict__ w, double* __restrict__ wT, const int* __restrict__ tidx, double beta1,
+                      double beta2, double eta, double eps)
 {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x)
     {
@@ -304,7 +305,7 @@ __global__ void kAdam(int P, const double* __restrict__ grad, double* __restrict
         v[p] = vp;
         const double wp = w[p] - eta * mp / (sqrt(vp) + eps);
         w[p] = wp;
-        wF[p] = (float)wp;
+        wT[tidx[p]] = wp;
     }
 }
 
@@ -436,8 +437,8 @@ void Trainer::step(Batch& batch, const double* energiesPhys, const double* force
     if (update)
     {
         const double eta = eta0_ * std::sqrt(1.0 - beta2t_) / (1.0 - beta1t_);
-        kAdam<<<(P_ + tb - 1) / tb, tb, 0, st>>>(P_, grad_, m_, v_, dmodel_.weightsDevice(), dmodel_.weightsFDevice(),
-                                                 beta1_, beta2_, eta, eps_);
+        kAdam<<<(P_ + tb - 1) / tb, tb, 0, st>>>(P_, grad_, m_, v_, dmodel_.weightsDevice(), dmodel_.weightsTDevice(),
+                                                 dmodel_.transIndexDevice(), beta1_, beta2_, eta, eps_);
         cudaCheck(cudaGetLastError(), "adam launch");
         beta1t_ *= beta1_;
         beta2t_ *= beta2_;
@@ -466,13 +467,12 @@ void Trainer::getParameters(double* fileOrder, cudaStream_t st) const
 
 void Trainer::setParameters(const double* fileOrder, cudaStream_t st)
 {
-    std::vector<double> w(P_);
-    std::vector<float> wf(P_);
+    std::vector<double> w(P_), wt(P_);
     for (int q = 0; q < P_; ++q) w[fileToDevice_[q]] = fileOrder[q];
-    for (int q = 0; q < P_; ++q) wf[q] = (float)w[q];
+    for (int q = 0; q < P_; ++q) wt[dmodel_.transIndexHost[q]] = w[q];
     cudaCheck(cudaMemcpyAsync(dmodel_.weightsDevice(), w.data(), sizeof(double) * P_, cudaMemcpyHostToDevice, st),
               "H2D");
-    cudaCheck(cudaMemcpyAsync(dmodel_.weightsFDevice(), wf.data(), sizeof(float) * P_, cudaMemcpyHostToDevice, st),
+    cudaCheck(cudaMemcpyAsync(dmodel_.weightsTDevice(), wt.data(), sizeof(double) * P_, cudaMemcpyHostToDevice, st),
               "H2D");
     cudaCheck(cudaStreamSynchronize(st), "sync");
 }
