@@ -103,6 +103,7 @@ struct DevModel
     int maxSF;
     int maxRows;
     int normalizeNeurons;
+    int sortByDistance;   // an angular group has a cutoff below the largest: stage blocks sorted by r
     int allFast;          // 0, or the zeta slots (2, 4) when every group is planned (rs = 0 bases) and every
                           // angular group is on the member grid
     double maxCutoff, maxCutoff2;

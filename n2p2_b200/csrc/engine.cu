@@ -57,13 +57,14 @@ DevicePool::~DevicePool() { trim(); }
 void* DevicePool::get(size_t bytes)
 {
     const size_t b = poolBucket(bytes);
-    auto it = free_.find(b);
-    if (it != free_.end() && !it->second.empty())
-    {
-        void* p = it->second.back();
-        it->second.pop_back();
-        return p;
-    }
+    // the smallest cached block of at least the size class, up to twice it
+    for (auto it = free_.lower_bound(b); it != free_.end() && it->first <= 2 * b; ++it)
+        if (!it->second.empty())
+        {
+            void* p = it->second.back();
+            it->second.pop_back();
+            return p;
+        }
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, b);
     if (e != cudaSuccess)
@@ -412,6 +413,7 @@ void DeviceModel::upload(Model const& m)
                 members.push_back(dm);
             }
             if (!dg.fast || (dg.type != 2 && (!dg.grid || dg.numBases > 1))) v.allFast = 0;   // one staged base
+            if (dg.type != 2 && dg.rc < m.maxCutoffRadius) v.sortByDistance = 1;
             else if (dg.type != 2 && dg.gridNZ > 2 && v.allFast) v.allFast = 4;
             groups.push_back(dg);
         }
@@ -497,6 +499,7 @@ void DeviceModel::upload(Model const& m)
     mix(members.data(), members.size() * sizeof(DevMember));
     mix(&v.numElements, sizeof(int));
     mix(&v.allFast, sizeof(int));
+    mix(&v.sortByDistance, sizeof(int));
     mix(v.cutoff, sizeof(v.cutoff));
     fingerprint = h;
     tcNetwork = networkTCSupported(m);

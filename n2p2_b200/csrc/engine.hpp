@@ -33,8 +33,8 @@ void cudaCheck(cudaError_t e, char const* what);
 bool networkTCSupported(Model const& m);
 
 // Device memory cache of one batch: blocks given back by put() are handed out
-// again for requests of the same size class, so re-setting structures of
-// similar size allocates nothing.  Every user of a batch's memory works on
+// again for requests of up to their size (at most twice the request's size
+// class), so re-setting structures of similar size allocates nothing.  Every user of a batch's memory works on
 // the batch's stream, so reuse is ordered after the previous users.
 class DevicePool
 {

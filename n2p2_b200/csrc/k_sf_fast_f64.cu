@@ -7,7 +7,8 @@ namespace {
 
 // Words of acceptance ballots the G pass records for atom i: two per 64
 // candidates of every angular group (the candidate counts of roundPhases,
-// from the numbers of neighbours of each element).
+// from the numbers of neighbours of each element inside the group's cutoff
+// when the stage is sorted by distance, else of all neighbours).
 __global__ void kMaskWords(DevModel model, BatchView b)
 {
     const int lane = threadIdx.x & 31;
@@ -15,22 +16,27 @@ __global__ void kMaskWords(DevModel model, BatchView b)
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
     {
         const int64_t off = b.nbrOffset[i], end = b.nbrOffset[i + 1];
-        int cnt[kDevMaxElements];
-        for (int e = 0; e < kDevMaxElements; ++e) cnt[e] = 0;
+        int cnt[4][kDevMaxElements];
+        for (int c = 0; c < 4; ++c)
+            for (int e = 0; e < kDevMaxElements; ++e) cnt[c][e] = 0;
         if (end <= b.nbrCapacity)
             for (int64_t q = off + lane; q < end; q += 32)
             {
                 const int e = b.elem[b.nbrJ[q]];
-                for (int f = 0; f < kDevMaxElements; ++f) cnt[f] += (e == f) ? 1 : 0;
+                const double d = b.nbrD[q];
+                for (int c = 0; c < 4; ++c)
+                    if (c < model.numCutoffSlots && (!model.sortByDistance || d < model.cutoff[c].rc))
+                        for (int f = 0; f < kDevMaxElements; ++f) cnt[c][f] += (e == f) ? 1 : 0;
             }
-        for (int f = 0; f < model.numElements; ++f) cnt[f] = warpSumInt(cnt[f]);
+        for (int c = 0; c < model.numCutoffSlots; ++c)
+            for (int f = 0; f < model.numElements; ++f) cnt[c][f] = warpSumInt(cnt[c][f]);
         DevElement const& E = model.el[b.elem[i]];
         int words = 0;
         for (int g = 0; g < E.groupCount; ++g)
         {
             DevGroup const& G = model.groups[E.groupBegin + g];
             if (G.type == 2) continue;
-            const int nA = cnt[G.e1], nB = cnt[G.e2];
+            const int nA = cnt[G.cutoffSlot][G.e1], nB = cnt[G.cutoffSlot][G.e2];
             int64_t count;
             if (G.e1 == G.e2)
             {

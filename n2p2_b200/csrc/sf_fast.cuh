@@ -65,6 +65,7 @@ struct Stage
     T E[NB][CAP];                          // Gaussian factors of the group's staged bases
     short perm[CAP];                       // staged slot -> position in the atom's list
     int blockBegin[kDevMaxElements + 1];
+    int nBelow[4][kDevMaxElements];        // per cutoff slot and element: block entries with r < r_c
 };
 
 // Per-group member parameters (shared by all lanes).
@@ -312,10 +313,15 @@ __device__ __forceinline__ int roundPhases(int A0, int nA, int B0, int nB, bool 
     return 1;
 }
 
-// Neighbours of one atom into the stage, sorted by element (stable).
+// Neighbours of one atom into the stage, sorted by element (stable) and, when
+// the model has angular groups with a smaller cutoff than the list's, by
+// distance within each element block, so that the neighbours inside a
+// group's cutoff are a prefix of the block (nBelow).
 template <typename T, int CAP, bool DF, int NB>
-__device__ void stageGeometry(Stage<T, CAP, DF, NB>& S, int64_t off, int n, int numElements, BatchView const& b, int lane)
+__device__ void stageGeometry(Stage<T, CAP, DF, NB>& S, int64_t off, int n, DevModel const& model, BatchView const& b,
+                              int lane)
 {
+    const int numElements = model.numElements;
     __syncwarp();
     int base = 0;
     for (int e = 0; e < numElements; ++e)
@@ -331,6 +337,45 @@ __device__ void stageGeometry(Stage<T, CAP, DF, NB>& S, int64_t off, int n, int 
         }
     }
     if (lane == 0) S.blockBegin[numElements] = base;
+    __syncwarp();
+    if (model.sortByDistance)
+    {
+        // FP64 distances and a scratch permutation in arrays filled below
+        double* rd = sizeof(T) == 8 ? reinterpret_cast<double*>(S.r) : reinterpret_cast<double*>(S.x);
+        short* tmp = sizeof(T) == 8 ? reinterpret_cast<short*>(S.x) : reinterpret_cast<short*>(S.z);
+        for (int s = lane; s < n; s += 32) rd[s] = b.nbrD[off + S.perm[s]];
+        __syncwarp();
+        for (int s = lane; s < n; s += 32)
+        {
+            int e = 0;
+            while (s >= S.blockBegin[e + 1]) ++e;
+            const int b0 = S.blockBegin[e], b1 = S.blockBegin[e + 1];
+            const double rs = rd[s];
+            int rank = b0;
+            for (int t = b0; t < b1; ++t)
+            {
+                const double rt = rd[t];
+                rank += (rt < rs || (rt == rs && t < s)) ? 1 : 0;
+            }
+            tmp[rank] = S.perm[s];
+        }
+        __syncwarp();
+        for (int c = 0; c < model.numCutoffSlots; ++c)
+            for (int e = 0; e < numElements; ++e)
+            {
+                int cnt = 0;
+                for (int s = S.blockBegin[e] + lane; s < S.blockBegin[e + 1]; s += 32)
+                    cnt += rd[s] < model.cutoff[c].rc ? 1 : 0;
+                cnt = warpSumInt(cnt);
+                if (lane == 0) S.nBelow[c][e] = cnt;
+            }
+        __syncwarp();
+        for (int s = lane; s < n; s += 32) S.perm[s] = tmp[s];
+    }
+    else if (lane < kDevMaxElements)
+    {
+        for (int c = 0; c < 4; ++c) S.nBelow[c][lane] = lane < numElements ? S.blockBegin[lane + 1] - S.blockBegin[lane] : 0;
+    }
     __syncwarp();
     for (int s = lane; s < n; s += 32)
     {
@@ -626,7 +671,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
         uint32_t* maskOut =
             (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
         int mwi = 0;
-        stageGeometry<T, CAP>(S, off, n, model.numElements, b, lane);
+        stageGeometry<T, CAP>(S, off, n, model, b, lane);
         int slot = -1;
         for (int g = 0; g < E.groupCount; ++g)
         {
@@ -687,8 +732,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                 else
                 {
                     const bool same = (G.e1 == G.e2);
-                    const int A0 = S.blockBegin[G.e1], nA = S.blockBegin[G.e1 + 1] - A0;
-                    const int B0 = S.blockBegin[G.e2], nB = S.blockBegin[G.e2 + 1] - B0;
+                    const int A0 = S.blockBegin[G.e1], nA = S.nBelow[G.cutoffSlot][G.e1];
+                    const int B0 = S.blockBegin[G.e2], nB = S.nBelow[G.cutoffSlot][G.e2];
                     Phase ph[2];
                     const int nph = roundPhases(A0, nA, B0, nB, same, ph);
                     int qn = 0, qh = 0;
@@ -816,7 +861,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(Dev
         const uint32_t* maskIn =
             (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
         int mwi = 0;
-        stageGeometry<T, CAP>(S, off, n, model.numElements, b, lane);
+        stageGeometry<T, CAP>(S, off, n, model, b, lane);
         for (int s = lane; s < n; s += 32) SM.h[0][s] = SM.h[1][s] = SM.h[2][s] = 0.0;
         double sfx = 0.0, sfy = 0.0, sfz = 0.0;
         int slot = -1;
@@ -874,8 +919,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(Dev
             if (fastG) stageFactors<T, CAP>(S, G, lane);
             const bool narrow = (G.type == 3);
             const bool same = (G.e1 == G.e2);
-            const int A0 = S.blockBegin[G.e1], nA = S.blockBegin[G.e1 + 1] - A0;
-            const int B0 = S.blockBegin[G.e2], nB = S.blockBegin[G.e2 + 1] - B0;
+            const int A0 = S.blockBegin[G.e1], nA = S.nBelow[G.cutoffSlot][G.e1];
+            const int B0 = S.blockBegin[G.e2], nB = S.nBelow[G.cutoffSlot][G.e2];
             Phase ph[2];
             const int nph = roundPhases(A0, nA, B0, nB, same, ph);
             int qn = 0, qh = 0;

@@ -66,10 +66,10 @@ def teacher_sf_importance(teacher_mode, structs):
     return out
 
 
-def select_student_sfs(teacher_mode, importance, n_radial=8, n_angular=6):
+def select_student_sfs(teacher_mode, importance, n_radial=8, n_angular=6, rc_angular=None):
     """symfunction_short lines of the n_radial radial (type 2) and n_angular
     narrow angular (type 3) teacher functions of highest importance, per
-    element."""
+    element (angular ones with cutoff rc_angular when given)."""
     sym = [teacher_mode.elementSymbol(e) for e in range(teacher_mode.numElements)]
     lines = []
     for e in range(teacher_mode.numElements):
@@ -82,8 +82,9 @@ def select_student_sfs(teacher_mode, importance, n_radial=8, n_angular=6):
                 if t == 2:
                     lines.append(f"symfunction_short {sym[e]} 2 {sym[e1]} {eta:.10g} {rs:.10g} {rc:.10g}")
                 else:
+                    rca = rc if rc_angular is None else rc_angular
                     lines.append(f"symfunction_short {sym[e]} 3 {sym[e1]} {sym[e2]} {eta:.10g} {lam:.0f} "
-                                 f"{zeta:.10g} {rc:.10g}")
+                                 f"{zeta:.10g} {rca:.10g}")
     return lines
 
 
@@ -380,7 +381,7 @@ def benchmark(student_dir, teacher_dir, num=2048, seed=97, steps=3, warmup=2, de
 
 
 def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=1e-3, seed=11, device=0, log=print,
-          select=True, decay=(0.5, 0.3)):
+          select=True, decay=(0.5, 0.3), rc_angular=None):
     """The full recipe: label, choose the descriptor (the teacher's most
     important functions when `select`), fit the scaling, train (step size
     `eta`, times decay[1] after each further decay[0] fraction of the epochs);
@@ -408,7 +409,7 @@ def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=
         f"teacher forces left out")
     lines = None
     if select:
-        lines = select_student_sfs(teacher, teacher_sf_importance(teacher, structs[:256]))
+        lines = select_student_sfs(teacher, teacher_sf_importance(teacher, structs[:256]), rc_angular=rc_angular)
         log("descriptor: " + "; ".join(l.replace("symfunction_short ", "") for l in lines))
     # scaling statistics (and hence the extrapolation range) over every training configuration
     write_student_model(out_dir, all_structs, seed=seed, device=device, sf_lines=lines)
@@ -425,7 +426,8 @@ def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=
     write_trained_weights(out_dir, student, tr.trainer.parameters())
     summary = {"configs": num_configs, "outlying_labels_left_out": int(outlier.sum()),
                "atoms": int(sum(s.numAtoms for s in structs)), "epochs": epochs,
-               "descriptor": lines if lines is not None else student_sf_lines(),
+               "descriptor": lines if lines is not None else student_sf_lines(rc_angular=rc_angular),
+               "rc_angular": rc_angular,
                "batch_size": batch_size, "eta": eta, "force_weight": 10.0, "loss_history": tr.history,
                "seconds": time.perf_counter() - t0}
     with open(os.path.join(out_dir, "training.json"), "w") as f:
@@ -444,9 +446,10 @@ def main():
     t.add_argument("--batch-size", type=int, default=64)
     t.add_argument("--eta", type=float, default=1e-3)
     t.add_argument("--seed", type=int, default=11)
+    t.add_argument("--rc-angular", type=float, default=None, help="cutoff of the angular functions (bohr)")
     a = ap.parse_args()
     if a.cmd == "train":
-        s = train(a.teacher, a.out, a.configs, a.epochs, a.batch_size, a.eta, a.seed)
+        s = train(a.teacher, a.out, a.configs, a.epochs, a.batch_size, a.eta, a.seed, rc_angular=a.rc_angular)
         print(json.dumps({k: v for k, v in s.items() if k != "loss_history"}))
 
 
