@@ -398,8 +398,8 @@ def bench_large(steps, warmup, device):
                                        "force_meV_per_A_rms": float(np.sqrt((df ** 2).mean()))}
     out.update(res)
     out["network"] = ("FP64 form: CUDA-core kernel (warp per atom); mixed form: tcgen05 tensor-core products with "
-                      "split-bfloat16 operands and FP32 accumulators (tensor-pipe utilisation from ncu in "
-                      "profiles/ncu_network_tc_water256_mixed.md)")
+                      "split-bfloat16 operands and FP32 accumulators (tensor-pipe utilisation is an ncu counter, "
+                      "not measured here)")
     mode.close()
     return out
 
