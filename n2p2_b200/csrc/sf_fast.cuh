@@ -102,20 +102,16 @@ struct ForcesSmem
     int queue[kQueue];
 };
 
-// Candidate pairs of one angular group, enumerated in phases:
-//   kind 0  circular: owner a in [0, nO), partner (a + 1 + t) mod nO, t < D
-//   kind 1  half-extra: owner a < nO / 2, partner a + nO / 2 (even nO, G pass)
-//   kind 2  rectangular: owner a in [0, nO), partner t in [0, D) of another block
-//   kind 3  tournament rounds over one block of nO slots (circle method on
+// Candidate pairs of one angular group, each unordered pair once, enumerated
+// in rounds of matchings (no slot occurs twice in one round, which lets the
+// force pass add a round's contributions without conflicts):
+//   kind 3  tournament over one block of nO slots (circle method on
 //           m = nO rounded up to even): round r < m - 1 pairs (m - 1, r) and
 //           ((r + i) mod (m - 1), (r - i) mod (m - 1)) for 0 < i < m / 2;
 //           slot m - 1 = nO (odd nO) is a bye
-//   kind 4  diagonal rounds over blocks nO <= D: round r < D pairs owner a
+//   kind 4  diagonals between blocks nO <= D: round r < D pairs owner a
 //           with partner (a + r) mod D, a < nO
-// Kinds 0-2 are owner-major (G pass); in kinds 3 and 4 every round is a
-// matching -- no slot occurs twice in one round -- which the force pass uses to
-// add contributions without conflicts.  The cursor walks a major index a
-// (owner or round) and a minor index t < minor.
+// The cursor walks the round a and the index t < minor within the round.
 struct Phase
 {
     int kind, O0, nO, P0, D, count, minor;
@@ -128,24 +124,11 @@ struct Cursor
     int a, t;
     __device__ __forceinline__ void init(Phase const& ph, int lane)
     {
-        if (ph.kind == 1 || ph.minor <= 0)
-        {
-            a = lane;
-            t = 0;
-        }
-        else
-        {
-            a = lane / ph.minor;
-            t = lane - a * ph.minor;
-        }
+        a = lane / ph.minor;
+        t = lane - a * ph.minor;
     }
     __device__ __forceinline__ void advance(Phase const& ph)
     {
-        if (ph.kind == 1)
-        {
-            a += 32;
-            return;
-        }
         t += 32;
         while (t >= ph.minor)
         {
@@ -176,27 +159,14 @@ struct Cursor
             sp = ph.O0 + v;
             return u < ph.nO;
         }
-        if (ph.kind == 4)
-        {
-            int q = t + a;
-            if (q >= ph.D) q -= ph.D;
-            so = ph.O0 + t;
-            sp = ph.P0 + q;
-            return true;
-        }
-        so = ph.O0 + a;
-        if (ph.kind == 0)
-        {
-            int q = a + 1 + t;
-            if (q >= ph.nO) q -= ph.nO;
-            sp = ph.O0 + q;
-        }
-        else if (ph.kind == 1) sp = ph.O0 + a + ph.nO / 2;
-        else sp = ph.P0 + t;
+        int q = t + a;
+        if (q >= ph.D) q -= ph.D;
+        so = ph.O0 + t;
+        sp = ph.P0 + q;
         return true;
     }
-    // Round of the candidate (kinds 3, 4), 11 bits.
-    __device__ __forceinline__ int round(Phase const& ph) const { return ph.kind >= 3 ? (a & 0x7ff) : 0; }
+    // Round of the candidate, 11 bits.
+    __device__ __forceinline__ int round(Phase const&) const { return a & 0x7ff; }
 };
 
 // Queue entries: round << 20 | owner slot << 10 | partner slot (slots < 1024).
@@ -269,35 +239,7 @@ __device__ __forceinline__ void enqueueCandidates(Stage<T, CAP, DF, NB> const& S
     __syncwarp();
 }
 
-// Phases of a group: G pass (each unordered pair once) or force pass
-// (ordered pairs, owner-major, both directions of a cross-element group).
-__device__ __forceinline__ int groupPhases(int A0, int nA, int B0, int nB, bool same, bool ordered, Phase* ph)
-{
-    int n = 0;
-    if (same)
-    {
-        if (nA < 2) return 0;
-        if (ordered)
-        {
-            ph[n++] = Phase{0, A0, nA, A0, nA - 1, nA * (nA - 1), nA - 1};
-        }
-        else
-        {
-            const int hb = (nA - 1) / 2;
-            if (hb > 0) ph[n++] = Phase{0, A0, nA, A0, hb, nA * hb, hb};
-            if ((nA & 1) == 0) ph[n++] = Phase{1, A0, nA, A0, 0, nA / 2, 0};
-        }
-    }
-    else
-    {
-        if (nA == 0 || nB == 0) return 0;
-        ph[n++] = Phase{2, A0, nA, B0, nB, nA * nB, nB};
-        if (ordered) ph[n++] = Phase{2, B0, nB, A0, nA, nA * nB, nA};
-    }
-    return n;
-}
-
-// Force pass: the unordered pairs of a group as rounds of matchings.
+// The unordered pairs of a group as rounds of matchings (both passes).
 __device__ __forceinline__ int roundPhases(int A0, int nA, int B0, int nB, bool same, Phase* ph)
 {
     if (same)
