@@ -183,10 +183,14 @@ __device__ __forceinline__ bool testCandidate(Stage<T, CAP, DF, NB> const& S, Ph
 {
     int so = 0, sp = 0;
     bool ok = false;
+    // Both slots are inside the group's cutoff by construction: with the
+    // stage sorted by distance the enumerated neighbours are the prefix with
+    // r < r_c, otherwise every group's cutoff is the list's and an entry at
+    // r = r_c exactly has f_c = df_c = 0, i.e. contributes exact zeros.
     if (p < ph.count && cur.slots(ph, so, sp))
     {
-        ok = S.r[so] < rc && S.r[sp] < rc;
-        if (ok && narrow)
+        ok = true;
+        if (narrow)
         {
             const T dx = S.x[sp] - S.x[so], dy = S.y[sp] - S.y[so], dz = S.z[sp] - S.z[so];
             ok = (dx * dx + dy * dy + dz * dz) < rc2;
