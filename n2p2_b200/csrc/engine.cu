@@ -711,6 +711,7 @@ void Batch::allocateNeighbors(int64_t capacity)
     v_.scrDz = devAlloc<double>(pool_, capacity, ownedNbr_);
     v_.nbrJ = devAlloc<int>(pool_, capacity, ownedNbr_);
     v_.nbrCode = devAlloc<int>(pool_, capacity, ownedNbr_);
+    v_.nbrElem = devAlloc<uint8_t>(pool_, capacity, ownedNbr_);
     v_.nbrD = devAlloc<double>(pool_, capacity, ownedNbr_);
     v_.nbrDx = devAlloc<double>(pool_, capacity, ownedNbr_);
     v_.nbrDy = devAlloc<double>(pool_, capacity, ownedNbr_);

@@ -304,7 +304,8 @@ __global__ void __launch_bounds__(256) kNeighborSort(
     int N, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
     const int64_t* __restrict__ nbrOffset, int64_t capacity, const int64_t* __restrict__ scrKey,
     const double* __restrict__ scrD, const double* __restrict__ scrDx, const double* __restrict__ scrDy,
-    const double* __restrict__ scrDz, int* __restrict__ nbrJ, int* __restrict__ nbrCode, double* __restrict__ nbrD,
+    const double* __restrict__ scrDz, const int* __restrict__ elem, int* __restrict__ nbrJ,
+    int* __restrict__ nbrCode, uint8_t* __restrict__ nbrElem, double* __restrict__ nbrD,
     double* __restrict__ nbrDx, double* __restrict__ nbrDy, double* __restrict__ nbrDz)
 {
     constexpr int kSmemKeys = 512;
@@ -331,8 +332,10 @@ __global__ void __launch_bounds__(256) kNeighborSort(
             int rank = 0;
             for (int q = 0; q < n; ++q) rank += (keys[q] < k) ? 1 : 0;
             const int64_t dst = off + rank;
-            nbrJ[dst] = (int)(k / K) + s.atomBegin;
+            const int j = (int)(k / K) + s.atomBegin;
+            nbrJ[dst] = j;
             nbrCode[dst] = (int)(k % K);
+            nbrElem[dst] = (uint8_t)elem[j];
             nbrD[dst] = scrD[off + e];
             nbrDx[dst] = scrDx[off + e];
             nbrDy[dst] = scrDy[off + e];
@@ -546,8 +549,8 @@ void launchNeighborBuild(BatchView const& b, double rc2, cudaStream_t st)
                                                    b.nbrCapacity, b.scrKey, b.scrD, b.scrDx, b.scrDy, b.scrDz,
                                                    b.status);
     kNeighborSort<<<warpBlocks, 256, 0, st>>>(N, b.atomStruct, b.info, b.nbrOffset, b.nbrCapacity, b.scrKey, b.scrD,
-                                              b.scrDx, b.scrDy, b.scrDz, b.nbrJ, b.nbrCode, b.nbrD, b.nbrDx,
-                                              b.nbrDy, b.nbrDz);
+                                              b.scrDx, b.scrDy, b.scrDz, b.elem, b.nbrJ, b.nbrCode, b.nbrElem,
+                                              b.nbrD, b.nbrDx, b.nbrDy, b.nbrDz);
     kNeighborReverse<<<warpBlocks, 256, 0, st>>>(N, b.atomStruct, b.info, b.nbrOffset, b.nbrCapacity, b.nbrJ,
                                                  b.nbrCode, b.rev, b.status);
 }

@@ -22,7 +22,7 @@ __global__ void kMaskWords(DevModel model, BatchView b)
         if (end <= b.nbrCapacity)
             for (int64_t q = off + lane; q < end; q += 32)
             {
-                const int e = b.elem[b.nbrJ[q]];
+                const int e = b.nbrElem[q];
                 const double d = b.nbrD[q];
                 for (int c = 0; c < 4; ++c)
                     if (c < model.numCutoffSlots && (!model.sortByDistance || d < model.cutoff[c].rc))

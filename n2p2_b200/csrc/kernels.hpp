@@ -51,6 +51,7 @@ struct BatchView
     double* scrDz = nullptr;
     int* nbrJ = nullptr;
     int* nbrCode = nullptr;
+    uint8_t* nbrElem = nullptr;        // element of each entry's neighbour
     double* nbrD = nullptr;
     double* nbrDx = nullptr;
     double* nbrDy = nullptr;

@@ -269,16 +269,26 @@ __device__ void stageGeometry(Stage<T, CAP, DF, NB>& S, int64_t off, int n, DevM
 {
     const int numElements = model.numElements;
     __syncwarp();
+    // neighbour elements of this lane's entries, all loads issued together
+    constexpr int kChunks = (CAP + 31) / 32;
+    int elemOf[kChunks];
+#pragma unroll
+    for (int c = 0; c < kChunks; ++c)
+    {
+        const int m = c * 32 + lane;
+        elemOf[c] = m < n ? (int)b.nbrElem[off + m] : -1;
+    }
     int base = 0;
     for (int e = 0; e < numElements; ++e)
     {
         if (lane == 0) S.blockBegin[e] = base;
-        for (int m0 = 0; m0 < n; m0 += 32)
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c)
         {
-            const int m = m0 + lane;
-            const bool mine = (m < n) && (b.elem[b.nbrJ[off + m]] == e);
+            if (c * 32 >= n) break;
+            const bool mine = elemOf[c] == e;
             const unsigned bal = __ballot_sync(kFullMask, mine);
-            if (mine) S.perm[base + __popc(bal & ((1u << lane) - 1u))] = (short)m;
+            if (mine) S.perm[base + __popc(bal & ((1u << lane) - 1u))] = (short)(c * 32 + lane);
             base += __popc(bal);
         }
     }
