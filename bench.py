@@ -40,6 +40,12 @@ METRIC = "atoms/s (E+F) on 1×B200: mixed/student vs plain FP64 at ≤1 meV/atom
 HA_TO_MEV = 27211.386
 HA_BOHR_TO_MEV_A = 27211.386 / 0.529177
 
+# DRAM bytes (read + write) of the two symmetry-function passes per neighbour
+# entry, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
+# of the 256-box case: G pass 608.8 + 41.0 MB, force pass 762.5 + 309.3 MB
+# over 13,792,482 entries; scaled to a batch by its entry count.
+SF_DRAM_BYTES_PER_ENTRY = (608.8 + 41.0 + 762.5 + 309.3) * 1e6 / 13792482
+
 # Algorithmic FLOPs per unit of the reference's symmetry-function algorithm
 # with derivatives (add/mul/div/sqrt = 1, exp counted separately):
 # G2 23 per pair-member + 14 per pair (cutoff function), narrow G3 60 per
@@ -292,7 +298,10 @@ def run_ours(args):
         roofline = {"bound": "fp64", "kernel": "kSFValues + kSFForces (symmetry functions, values + derivatives)",
                     "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                     "peak_source": "measured FP64 FMA throughput of this GPU (n2p2_device_fma_peak)",
-                    "algorithmic_flops_per_step": sf_flops, "traffic": None}
+                    "algorithmic_flops_per_step": sf_flops,
+                    "traffic": SF_DRAM_BYTES_PER_ENTRY * work["entries"],
+                    "traffic_source": "ncu DRAM bytes of a 256-box capture, scaled by neighbour entries",
+                    "traffic_GBps": SF_DRAM_BYTES_PER_ENTRY * work["entries"] / (sf_ms * 1e-3) / 1e9}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
