@@ -36,6 +36,8 @@ sys.path.insert(0, ROOT)
 MODEL = os.path.join(ROOT, "tests", "golden", "models", "water40")
 TEACHER = os.path.join(ROOT, "tests", "golden", "models", "water56")
 STUDENT = os.path.join(ROOT, "tests", "golden", "models", "student_water56")
+# the same recipe with the descriptor chosen by force span (angular cutoff 12 bohr): slower, closer to the teacher
+STUDENT_SPAN = os.path.join(ROOT, "tests", "golden", "models", "student_water56_span")
 METRIC = "atoms/s (E+F) on 1×B200: mixed/student vs plain FP64 at ≤1 meV/atom, 30 meV/Å"
 HA_TO_MEV = 27211.386
 HA_BOHR_TO_MEV_A = 27211.386 / 0.529177
@@ -289,6 +291,14 @@ def run_ours(args):
         from n2p2_b200 import student as student_mod
         stud = student_mod.benchmark(STUDENT, TEACHER, num=args.student_boxes, steps=args.steps,
                                      warmup=args.warmup)
+        stud["descriptor"] = "teacher functions of largest energy sensitivity, angular cutoff 8 bohr"
+        if os.path.isdir(STUDENT_SPAN):
+            span = student_mod.benchmark(STUDENT_SPAN, TEACHER, num=args.student_boxes, steps=args.steps,
+                                         warmup=args.warmup)
+            stud["span_descriptor"] = {k: span[k] for k in (
+                "value", "unit", "ms_per_step", "speedup_vs_fp64", "fallback_rate", "err_vs_teacher_fp64_gpu",
+                "err_vs_teacher_fp64_gpu_teacher_in_range", "held_out_monitor", "_predictions")}
+            stud["span_descriptor"]["descriptor"] = "chosen by force span from a candidate grid, angular cutoff 12 bohr"
 
     sf_ms = sum(t for n, t in stages if n in ("sf_values", "sf_forces"))
     sf_flops = sum(work[k] * f for k, f in FLOPS_PER.items())
@@ -320,8 +330,13 @@ def run_ours(args):
                    "sample": "failed: %s" % exc}
         if stud is not None:
             stud["err_vs_fp64_oracle"] = student_vs_oracle(stud["_predictions"])
+            if "span_descriptor" in stud:
+                stud["span_descriptor"]["err_vs_fp64_oracle"] = \
+                    student_vs_oracle(stud["span_descriptor"]["_predictions"])
     if stud is not None:
         stud.pop("_predictions", None)
+        if "span_descriptor" in stud:
+            stud["span_descriptor"].pop("_predictions", None)
 
     value = world * natoms / (ms / 1000.0)
     if rank == 0:

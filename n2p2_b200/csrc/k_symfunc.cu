@@ -1,7 +1,7 @@
 // Symmetry-function kernels of the API form (G2 radial, G3 narrow angular,
 // G9 wide angular) on sm_100a, one warp per centre atom with the atom's
 // neighbour list staged in shared memory.  (The evaluation path's G and force
-// kernels are in k_sf_fast.cu.)
+// kernels are in sf_fast.cuh, instantiated by k_sf_fast_f64.cu / k_sf_fast_f32.cu.)
 //
 //   kSFDerivatives G and dG/dr stored per neighbour row (the Atom::Neighbor::dGdr
 //                  layout of Element::setupSymmetryFunctionMemory,

@@ -17,6 +17,7 @@ import argparse
 import json
 import math
 import os
+import shutil
 import time
 
 import numpy as np
@@ -86,6 +87,192 @@ def select_student_sfs(teacher_mode, importance, n_radial=8, n_angular=6, rc_ang
                     lines.append(f"symfunction_short {sym[e]} 3 {sym[e1]} {sym[e2]} {eta:.10g} {lam:.0f} "
                                  f"{zeta:.10g} {rca:.10g}")
     return lines
+
+
+def _sf_line(sym, e, f, rc_angular=None):
+    typ, e1, e2, eta, rs, lam, zeta, rc, _ = f
+    if typ == 2:
+        return f"symfunction_short {sym[e]} 2 {sym[e1]} {eta:.10g} {rs:.10g} {rc:.10g}"
+    rca = rc if rc_angular is None else rc_angular
+    return f"symfunction_short {sym[e]} 3 {sym[e1]} {sym[e2]} {eta:.10g} {lam:.0f} {zeta:.10g} {rca:.10g}"
+
+
+def candidate_sf_lines(teacher_mode, rc_angular=None, angular_etas=(0.001, 0.003, 0.01, 0.03),
+                       angular_zetas=(1.0, 2.0, 4.0, 16.0), extra_radial_etas=(1.0, 3.0)):
+    """Descriptor candidates per element: the teacher's radial functions,
+    radial functions of the extra widths (per neighbour element, teacher's
+    radial cutoff), and narrow angular functions (type 3) over the grid of
+    eta x zeta x lambda +-1 for every neighbour-element pair, with cutoff
+    rc_angular (the teacher's largest cutoff when None)."""
+    ne = teacher_mode.numElements
+    sym = [teacher_mode.elementSymbol(e) for e in range(ne)]
+    rca = teacher_mode.getMaxCutoffRadius() if rc_angular is None else rc_angular
+    lines = []
+    for e in range(ne):
+        sfs = [teacher_mode.symmetryFunction(e, i) for i in range(teacher_mode.numSymmetryFunctions(e))]
+        radial = [f for f in sfs if f[0] == 2]
+        lines += [_sf_line(sym, e, f) for f in radial]
+        rcr = max(f[7] for f in radial) if radial else rca
+        for e1 in range(ne):
+            for eta in extra_radial_etas:
+                if not any(f[1] == e1 and f[3] == eta and f[4] == 0.0 for f in radial):
+                    lines.append(f"symfunction_short {sym[e]} 2 {sym[e1]} {eta:.10g} 0 {rcr:.10g}")
+        for e1 in range(ne):
+            for e2 in range(e1, ne):
+                for eta in angular_etas:
+                    for zeta in angular_zetas:
+                        for lam in (-1, 1):
+                            lines.append(f"symfunction_short {sym[e]} 3 {sym[e1]} {sym[e2]} {eta:.10g} {lam} "
+                                         f"{zeta:.10g} {rca:.10g}")
+    return lines
+
+
+def _derivative_tables(mode):
+    """rows[e][en]: symmetry-function indices of element e that depend on a
+    neighbour of element en, in the order of the per-neighbour dG/dr rows
+    (Element::symmetryFunctionTable order: ascending index)."""
+    ne = mode.numElements
+    out = [[[] for _ in range(ne)] for _ in range(ne)]
+    for e in range(ne):
+        for i in range(mode.numSymmetryFunctions(e)):
+            typ, e1, e2 = mode.symmetryFunction(e, i)[:3]
+            for en in range(ne):
+                if (en == e1) if typ == 2 else en in (e1, e2):
+                    out[e][en].append(i)
+    return out
+
+
+def _contribution_vectors(mode, batch, dEdG=None):
+    """Per atom in turn (a generator): the dG_is/dr_k vectors of its
+    symmetry functions over k = the atom itself, then its neighbour entries in
+    list order ([1 + n] x 3 x numSF) -- or, with per-atom dE/dG given, their
+    contraction sum_s dE_i/dG_is dG_is/dr_k ([1 + n] x 3), atom i's
+    contribution to the forces.  The batch was evaluated with stored dG/dr."""
+    nb = batch.neighbors()
+    off, idx = nb["offset"], nb["index"]
+    el = batch.elements
+    ne = mode.numElements
+    rows = np.array([[mode.numDerivativeRows(e, en) for en in range(ne)] for e in range(ne)])
+    row_count = rows[el[np.repeat(np.arange(batch.numAtoms), np.diff(off))], el[idx]]
+    row_off = np.concatenate([[0], np.cumsum(row_count)])
+    selfd, nbr = batch.dGdr(int(row_off[-1]))
+    nsf = np.array([mode.numSymmetryFunctions(e) for e in range(ne)])
+    sf_off = np.concatenate([[0], np.cumsum(nsf[el])])
+    tab = _derivative_tables(mode)
+    for i in range(batch.numAtoms):
+        e = el[i]
+        p0, p1 = off[i], off[i + 1]
+        V = np.zeros((1 + p1 - p0, 3, nsf[e]))
+        V[0] = selfd[sf_off[i]:sf_off[i + 1]].T
+        for q, p in enumerate(range(p0, p1)):
+            t = tab[e][el[idx[p]]]
+            V[1 + q][:, t] = nbr[row_off[p]:row_off[p] + len(t)].T
+        yield V if dEdG is None else V @ dEdG[sf_off[i]:sf_off[i + 1]]
+
+
+def force_span_statistics(teacher_mode, candidate_mode, structs):
+    """Per element: (M [atoms, C, C], B [atoms, C], c [atoms]) with, for each
+    atom i, V_i the dG/dr vectors of the C candidate functions (columns) and
+    f_i the teacher's force contributions of atom i (both over the atom and its
+    neighbours): M_i = V_i^T V_i, B_i = V_i^T f_i, c_i = |f_i|^2.  Both modes
+    must have the same largest cutoff (identical neighbour lists)."""
+    pos = _positions(structs)
+    bt = teacher_mode.batch(structs)
+    bt.setPositions(pos)
+    bt.evaluate(forces=True, storeDGdr=True, graph=False)
+    f = [g.ravel() for g in _contribution_vectors(teacher_mode, bt, bt.dEdG())]
+    nt = bt.neighbors()
+    bc = candidate_mode.batch(structs)
+    bc.setPositions(pos)
+    bc.evaluate(forces=True, storeDGdr=True, graph=False)
+    nc = bc.neighbors()
+    if not (np.array_equal(nt["offset"], nc["offset"]) and np.array_equal(nt["index"], nc["index"])):
+        raise ValueError("teacher and candidate descriptors need the same neighbour lists (same largest cutoff)")
+    el = bt.elements
+    acc = [([], [], []) for _ in range(teacher_mode.numElements)]
+    for i, V in enumerate(_contribution_vectors(candidate_mode, bc)):
+        V = V.reshape(-1, V.shape[-1])
+        M, B, c = acc[el[i]]
+        M.append(V.T @ V)
+        B.append(V.T @ f[i])
+        c.append(f[i] @ f[i])
+    out = [tuple(np.array(x) for x in a) for a in acc]
+    bt.close()
+    bc.close()
+    return out
+
+
+def span_residual(M, B, c, subset, ridge=1e-10):
+    """sum_i min_a |f_i - V_i[:, subset] a|^2 from the Gram statistics (a
+    ridge of `ridge` x the mean diagonal keeps near-collinear sets solvable)."""
+    S = list(subset)
+    if not S:
+        return float(c.sum())
+    Mss = M[:, S][:, :, S]
+    k = len(S)
+    Mss = Mss + (ridge * np.trace(Mss, axis1=1, axis2=2) / k)[:, None, None] * np.eye(k)[None]
+    b = B[:, S]
+    x = np.linalg.solve(Mss, b[..., None])[..., 0]
+    return float((c - (b * x).sum(axis=1)).sum())
+
+
+def greedy_span_selection(M, B, c, types, budget):
+    """Forward selection of candidate columns minimising span_residual, taking
+    at most budget[t] candidates of type types[j] == t; returns the chosen
+    indices in order and the relative residual after each choice."""
+    left = dict(budget)
+    chosen, trace = [], []
+    total = float(c.sum())
+    while any(left.get(t, 0) > 0 for t in set(types)):
+        best = None
+        for j, t in enumerate(types):
+            if j in chosen or left.get(t, 0) <= 0:
+                continue
+            r = span_residual(M, B, c, chosen + [j])
+            if best is None or r < best[0]:
+                best = (r, j)
+        if best is None:
+            break
+        chosen.append(best[1])
+        left[types[best[1]]] -= 1
+        trace.append(best[0] / total)
+    return chosen, trace
+
+
+def select_by_force_span(teacher_mode, structs, candidate_dir, n_radial=8, n_angular=6, rc_angular=None,
+                         device=0, log=None):
+    """symfunction_short lines of the student's descriptor chosen from
+    candidate_sf_lines: per element, the n_radial radial and n_angular angular
+    candidates whose dG/dr vectors best span the teacher's per-atom force
+    contributions on `structs` (greedy forward selection).
+
+    For atom i the teacher's contribution to the forces is
+    f_i = (sum_s dE_i/dG_is dG_is/dr_k)_k over k = i and its neighbours; a
+    student on descriptor set S produces sum_{s in S} a_s dG'_is/dr_k with
+    a_s its own dE_i/dG'_is.  The least-squares residual of f_i against the
+    span of those vectors, summed over atoms, is the part of the teacher's
+    forces that no network on S reproduces even with free per-atom
+    coefficients; the selection minimises it.  Returns (lines, report)."""
+    sym = [teacher_mode.elementSymbol(e) for e in range(teacher_mode.numElements)]
+    cand = candidate_sf_lines(teacher_mode, rc_angular)
+    write_student_model(candidate_dir, structs, device=device, sf_lines=cand)
+    cm = load_mode(candidate_dir, device)
+    stats = force_span_statistics(teacher_mode, cm, structs)
+    lines, report = [], {}
+    for e, (M, B, c) in enumerate(stats):
+        sfs = [cm.symmetryFunction(e, i) for i in range(cm.numSymmetryFunctions(e))]
+        types = [f[0] for f in sfs]
+        chosen, trace = greedy_span_selection(M, B, c, types, {2: n_radial, 3: n_angular})
+        every = span_residual(M, B, c, range(len(sfs))) / float(c.sum())
+        lines += [_sf_line(sym, e, sfs[j]) for j in sorted(chosen)]
+        report[sym[e]] = {"candidates": len(sfs), "atoms": int(c.size), "residual_all_candidates": every,
+                          "residual_after_each_choice": trace,
+                          "force_contribution_sq_sum": float(c.sum())}
+        if log:
+            log(f"{sym[e]}: relative span residual {trace[-1]:.4f} with {len(chosen)} of {len(sfs)} "
+                f"candidates ({every:.5f} with all)")
+    cm.close()
+    return lines, report
 
 
 def training_structures(num, seed, n_min=64, n_max=512, sigma_range=(0.05, 0.4)):
@@ -381,9 +568,10 @@ def benchmark(student_dir, teacher_dir, num=2048, seed=97, steps=3, warmup=2, de
 
 
 def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=1e-3, seed=11, device=0, log=print,
-          select=True, decay=(0.5, 0.3), rc_angular=None):
-    """The full recipe: label, choose the descriptor (the teacher's most
-    important functions when `select`), fit the scaling, train (step size
+          select="span", decay=(0.5, 0.3), rc_angular=None):
+    """The full recipe: label, choose the descriptor (`select`: "span" --
+    select_by_force_span, "importance" -- the teacher's functions of largest
+    teacher_sf_importance, None -- student_sf_lines), fit the scaling, train (step size
     `eta`, times decay[1] after each further decay[0] fraction of the epochs);
     writes the trained model and returns a summary dict."""
     t0 = time.perf_counter()
@@ -407,9 +595,15 @@ def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=
     structs = [structs[k] for k in keep]
     log(f"teacher labels ({time.perf_counter() - t0:.1f} s); {int(outlier.sum())} structures with outlying "
         f"teacher forces left out")
-    lines = None
-    if select:
+    lines, span = None, None
+    if select == "span":
+        sample = [s for s in structs if s.numAtoms <= 300][:12]
+        cdir = os.path.join(out_dir, "_candidates")
+        lines, span = select_by_force_span(teacher, sample, cdir, rc_angular=rc_angular, device=device, log=log)
+        shutil.rmtree(cdir)
+    elif select == "importance":
         lines = select_student_sfs(teacher, teacher_sf_importance(teacher, structs[:256]), rc_angular=rc_angular)
+    if lines is not None:
         log("descriptor: " + "; ".join(l.replace("symfunction_short ", "") for l in lines))
     # scaling statistics (and hence the extrapolation range) over every training configuration
     write_student_model(out_dir, all_structs, seed=seed, device=device, sf_lines=lines)
@@ -427,7 +621,7 @@ def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=
     summary = {"configs": num_configs, "outlying_labels_left_out": int(outlier.sum()),
                "atoms": int(sum(s.numAtoms for s in structs)), "epochs": epochs,
                "descriptor": lines if lines is not None else student_sf_lines(rc_angular=rc_angular),
-               "rc_angular": rc_angular,
+               "rc_angular": rc_angular, "selection": select, "force_span": span,
                "batch_size": batch_size, "eta": eta, "force_weight": 10.0, "loss_history": tr.history,
                "seconds": time.perf_counter() - t0}
     with open(os.path.join(out_dir, "training.json"), "w") as f:
@@ -447,9 +641,13 @@ def main():
     t.add_argument("--eta", type=float, default=1e-3)
     t.add_argument("--seed", type=int, default=11)
     t.add_argument("--rc-angular", type=float, default=None, help="cutoff of the angular functions (bohr)")
+    t.add_argument("--select", choices=("span", "importance", "fixed"), default="span",
+                   help="descriptor choice: force-span selection from a candidate grid, the teacher's most "
+                        "important functions, or the fixed student_sf_lines set")
     a = ap.parse_args()
     if a.cmd == "train":
-        s = train(a.teacher, a.out, a.configs, a.epochs, a.batch_size, a.eta, a.seed, rc_angular=a.rc_angular)
+        s = train(a.teacher, a.out, a.configs, a.epochs, a.batch_size, a.eta, a.seed, rc_angular=a.rc_angular,
+                  select=None if a.select == "fixed" else a.select)
         print(json.dumps({k: v for k, v in s.items() if k != "loss_history"}))
 
 

@@ -160,3 +160,47 @@ def test_fallback_on_extrapolation(teacher, student_dir):
     assert np.array_equal(F[a0:a0 + held[2].numAtoms], Ft)
     assert 0 < ev.fallback_rate() <= 1
     assert len(ev.monitor_log) == 1 and ev.monitor_log[0]["energy_meV_per_atom_rms"] >= 0
+
+
+def test_force_contributions_sum_to_forces(teacher):
+    """The per-atom force contributions the descriptor selection spans
+    (dE_i/dG_is dG_is/dr_k over each atom and its neighbours) add up to the
+    teacher's forces."""
+    structs = student.training_structures(2, seed=9, n_min=32, n_max=48)
+    b = teacher.batch(structs)
+    b.setPositions(np.concatenate([s.positions for s in structs]))
+    b.evaluate(forces=True, storeDGdr=True, graph=False)
+    nb = b.neighbors()
+    off = nb["offset"]
+    F = np.zeros((b.numAtoms, 3))
+    for i, g in enumerate(student._contribution_vectors(teacher, b, b.dEdG())):
+        F[i] += g[0]
+        np.add.at(F, nb["index"][off[i]:off[i + 1]], g[1:])
+    ref = b.forces()
+    assert np.abs(-F - ref).max() <= 1e-10 * np.abs(ref).max()
+    b.close()
+
+
+def test_force_span_selection(teacher, tmp_path):
+    """Descriptor selection from the candidate grid: the per-element budget
+    of radial and angular functions, a residual that falls with each choice,
+    and a chosen set that spans the teacher's force contributions better than
+    the fixed default set does."""
+    sample = student.training_structures(3, seed=12, n_min=32, n_max=48)
+    lines, rep = student.select_by_force_span(teacher, sample, str(tmp_path / "cand"))
+    for sym in ("H", "O"):
+        mine = [l.split() for l in lines if l.split()[1] == sym]
+        assert sum(p[2] == "2" for p in mine) == 8 and sum(p[2] == "3" for p in mine) == 6
+        tr = rep[sym]["residual_after_each_choice"]
+        assert len(tr) == 14 and all(a >= b - 1e-12 for a, b in zip(tr, tr[1:]))
+        assert rep[sym]["residual_all_candidates"] <= tr[-1] < 1.0
+    # the fixed set's residual on the same sample, through a candidate model of its own functions
+    fixed = str(tmp_path / "fixed")
+    student.write_student_model(fixed, sample, sf_lines=student.student_sf_lines())
+    fm = student.load_mode(fixed)
+    stats = student.force_span_statistics(teacher, fm, sample)
+    for e, sym in enumerate(("H", "O")):
+        M, B, c = stats[e]
+        fixed_res = student.span_residual(M, B, c, range(M.shape[1])) / float(c.sum())
+        assert rep[sym]["residual_after_each_choice"][-1] < fixed_res
+    fm.close()
