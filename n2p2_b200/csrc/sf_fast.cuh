@@ -449,9 +449,9 @@ struct Triplet
     T rinv, cost, fcjk, dfcjk;
 };
 
+// Slot geometry of a triplet (everything but the j-k cutoff).
 template <typename T, int CAP, bool DF, int NB>
-__device__ __forceinline__ void loadTriplet(Stage<T, CAP, DF, NB> const& S, DevCutoff const& cut, bool narrow, int so, int sp,
-                                            Triplet<T>& t)
+__device__ __forceinline__ void tripletGeometry(Stage<T, CAP, DF, NB> const& S, int so, int sp, Triplet<T>& t)
 {
     t.x1 = S.x[so];
     t.y1 = S.y[so];
@@ -477,14 +477,54 @@ __device__ __forceinline__ void loadTriplet(Stage<T, CAP, DF, NB> const& S, DevC
     t.rijk = T(0);
     t.fcjk = T(1);
     t.dfcjk = T(0);
+}
+
+// r_jk and its cutoff (narrow groups).
+template <typename T>
+__device__ __forceinline__ void tripletJK(DevCutoff const& cut, Triplet<T>& t)
+{
+    t.rijk = frsqrt<T>(t.rjk2);
+    t.rjk = t.rjk2 * t.rijk;
+    double f, df;
+    cutoffFdf(cut, (double)t.rjk, f, df);   // FP64 near r_c in both forms
+    t.fcjk = (T)f;
+    t.dfcjk = (T)df;
+}
+
+template <typename T, int CAP, bool DF, int NB>
+__device__ __forceinline__ void loadTriplet(Stage<T, CAP, DF, NB> const& S, DevCutoff const& cut, bool narrow, int so, int sp,
+                                            Triplet<T>& t)
+{
+    tripletGeometry<T, CAP>(S, so, sp, t);
+    if (narrow) tripletJK<T>(cut, t);
+}
+
+// ILP triplets per lane at once (model-specialised kernels): entries
+// lane + 32 u, u < ILP, of the queue window [qh, qh + take); a lane past
+// the window repeats the window's first entry (in bounds, finite) and its
+// ok[u] is false.  Each step is written for all u together so independent
+// chains could interleave; the kernels run ILP = 1: two triplets per lane
+// measured 1.5x slower on B200 (the extra live registers cut residency
+// from 16 to 12 warps per SM and spilled in the force pass).
+template <typename T, int CAP, bool DF, int NB, int ILP>
+__device__ __forceinline__ void loadTriplets(Stage<T, CAP, DF, NB> const& S, DevCutoff const& cut, bool narrow,
+                                             const int* queue, int qh, int take, int lane, Triplet<T> (&t)[ILP],
+                                             int (&so)[ILP], int (&sp)[ILP], bool (&ok)[ILP])
+{
+#pragma unroll
+    for (int u = 0; u < ILP; ++u)
+    {
+        const int idx = lane + 32 * u;
+        ok[u] = idx < take;
+        const int e = queue[(qh + (ok[u] ? idx : 0)) & (kQueue - 1)];
+        so[u] = entryOwner(e);
+        sp[u] = entryPartner(e);
+        tripletGeometry<T, CAP>(S, so[u], sp[u], t[u]);
+    }
     if (narrow)
     {
-        t.rijk = frsqrt<T>(t.rjk2);
-        t.rjk = t.rjk2 * t.rijk;
-        double f, df;
-        cutoffFdf(cut, (double)t.rjk, f, df);   // FP64 near r_c in both forms
-        t.fcjk = (T)f;
-        t.dfcjk = (T)df;
+#pragma unroll
+        for (int u = 0; u < ILP; ++u) tripletJK<T>(cut, t[u]);
     }
 }
 
@@ -592,15 +632,141 @@ __device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Membe
     }
 }
 
+// powUniform of U bases with one exponent (the same multiplications per
+// base, in the same order).
+template <typename T, int U>
+__device__ __forceinline__ void powUniformN(T (&x)[U], int e, T (&r)[U])
+{
+    if constexpr (sizeof(T) == 8)
+    {
+#pragma unroll
+        for (int u = 0; u < U; ++u) r[u] = T(1);
+#pragma unroll 1
+        while (e)
+        {
+            if (e & 1)
+            {
+#pragma unroll
+                for (int u = 0; u < U; ++u) r[u] *= x[u];
+            }
+            e >>= 1;
+            if (e)
+            {
+#pragma unroll
+                for (int u = 0; u < U; ++u) x[u] *= x[u];
+            }
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int u = 0; u < U; ++u) r[u] = powUniform<T>(x[u], e);
+    }
+}
+
+// gridValues of U triplets (pfc = 0 for a triplet that is not to count:
+// it then adds zeros).
+template <typename T, int NZ, int STRIDE, int U>
+__device__ __forceinline__ void gridValuesN(T const (&bv)[U][kMaxStagedBases], DevGroup const& G, T const (&cost)[U],
+                                            T const (&pfc)[U], T* acc)
+{
+    T vS[2][U];
+#pragma unroll
+    for (int es = 0; es < 2; ++es)
+    {
+        T x[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) x[u] = G.etaBase[es] == 0 ? bv[u][0] : bv[u][1];
+        powUniformN<T, U>(x, G.etaPow[es], vS[es]);
+    }
+#pragma unroll
+    for (int ls = 0; ls < 2; ++ls)
+    {
+        T pl[U], w[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            pl[u] = T(1) + (T)G.lambdaVal[ls] * cost[u];
+            w[u] = pl[u] > T(0) ? pl[u] * pfc[u] : T(0);
+        }
+#pragma unroll
+        for (int zs = 0; zs < NZ; ++zs)
+        {
+            T x[U], pz[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) x[u] = pl[u];
+            powUniformN<T, U>(x, G.zetaM1[zs], pz);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                const T p = pz[u] * w[u];
+#pragma unroll
+                for (int es = 0; es < 2; ++es) acc[(es * 2 + ls) * STRIDE + zs] += vS[es][u] * p;
+            }
+        }
+    }
+}
+
+// gridForces of U triplets.
+template <typename T, int NZ, bool COMPACT, int U>
+__device__ __forceinline__ void gridForcesN(T const (&bv)[U][kMaxStagedBases], DevGroup const& G,
+                                            Members<T, COMPACT> const& mb, T const (&cost)[U], T (&T1)[U], T (&T2)[U],
+                                            T (&T3)[U])
+{
+    T vS[2][U];
+#pragma unroll
+    for (int es = 0; es < 2; ++es)
+    {
+        T x[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) x[u] = G.etaBase[es] == 0 ? bv[u][0] : bv[u][1];
+        powUniformN<T, U>(x, G.etaPow[es], vS[es]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) T1[u] = T2[u] = T3[u] = T(0);
+#pragma unroll
+    for (int ls = 0; ls < 2; ++ls)
+    {
+        T pl[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) pl[u] = T(1) + (T)G.lambdaVal[ls] * cost[u];
+#pragma unroll
+        for (int zs = 0; zs < NZ; ++zs)
+        {
+            T x[U], pz[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) x[u] = pl[u];
+            powUniformN<T, U>(x, G.zetaM1[zs], pz);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                const T pz1 = pl[u] > T(0) ? pz[u] : T(0);
+#pragma unroll
+                for (int es = 0; es < 2; ++es)
+                {
+                    const int c = (es * 2 + ls) * 4 + zs;
+                    const T a = mb.gcw[c] * vS[es][u] * pz1;
+                    const T azl = a * mb.gzl[c];
+                    T1[u] += azl;
+                    T3[u] += a * pl[u];
+                    T2[u] += azl * pl[u] * mb.gfd[c];
+                }
+            }
+        }
+    }
+}
+
 } // namespace
 
 // ---------------------------------------------------------------------------
 // G values
 // ---------------------------------------------------------------------------
 template <typename T, int CAP, int WARPS, int FAST>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(DevModel model, BatchView b, int lower,
-                                                                     int flagOverflow)
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
+    kSFValuesF(DevModel model, BatchView b, int lower, int flagOverflow)
 {
+    constexpr int ILP = 1;            // triplets per lane and step (see loadTriplets)
+    constexpr int kStep = 32 * ILP;   // triplets per warp step
     extern __shared__ __align__(16) unsigned char smemRaw[];
     ValuesSmem<T, CAP, FAST>& SM = reinterpret_cast<ValuesSmem<T, CAP, FAST>*>(smemRaw)[threadIdx.x >> 5];
     auto& S = SM.st;
@@ -706,16 +872,33 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                         int p0 = 0;
                         while (true)
                         {
-                            if (qn < 32 && p0 < cnt)   // queue stays below 32 + 64 entries
+                            if (qn < kStep && p0 < cnt)   // queue stays below kStep + 64 entries
                             {
                                 enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane,
                                                           m0 == 0 ? maskOut : nullptr, nullptr, mwi);
                                 p0 += 64;
                             }
-                            if (qn >= 32 || (drain && qn > 0))
+                            if (qn >= kStep || (drain && qn > 0))
                             {
-                                const int take = min(32, qn);
-                                if (lane < take)
+                                const int take = min(kStep, qn);
+                                if constexpr (FAST > 0)
+                                {
+                                    Triplet<T> t[ILP];
+                                    int so[ILP], sp[ILP];
+                                    bool ok[ILP];
+                                    loadTriplets<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh, take, lane,
+                                                         t, so, sp, ok);
+                                    T bv[ILP][kMaxStagedBases], cost[ILP], pfc[ILP];
+#pragma unroll
+                                    for (int u = 0; u < ILP; ++u)
+                                    {
+                                        tripletBases<T, CAP>(S, G, narrow, so[u], sp[u], t[u].rjk2, bv[u]);
+                                        cost[u] = t[u].cost;
+                                        pfc[u] = ok[u] ? t[u].fc1 * t[u].fc2 * t[u].fcjk : T(0);
+                                    }
+                                    gridValuesN<T, FAST, FAST, ILP>(bv, G, cost, pfc, acc);
+                                }
+                                else if (lane < take)
                                 {
                                     const int e = SM.queue[(qh + lane) & (kQueue - 1)];
                                     const int so = entryOwner(e), sp = entryPartner(e);
@@ -727,11 +910,10 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
                                     T vexp = T(0);
                                     if (grid)
                                     {
-                                        if constexpr (FAST > 0) gridValues<T, FAST, FAST>(bv, G, t.cost, pfc, acc);
-                                        else if (G.gridNZ <= 2) gridValues<T, 2, 4>(bv, G, t.cost, pfc, acc);
+                                        if (G.gridNZ <= 2) gridValues<T, 2, 4>(bv, G, t.cost, pfc, acc);
                                         else gridValues<T, 4, 4>(bv, G, t.cost, pfc, acc);
                                     }
-                                    else if constexpr (FAST == 0)
+                                    else
                                     {
 #pragma unroll
                                         for (int q = 0; q < ACC; ++q)
@@ -795,9 +977,89 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFValuesF(Dev
 // Pairs are enumerated in rounds of matchings, so the lanes of one round add
 // their two contributions to distinct slots; rounds add one after another in
 // a fixed order (deterministic, no atomics).
-template <typename T, int CAP, int WARPS, int FAST>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(DevModel model, BatchView b, int lower)
+
+// One warp step of the force pass over the queue window [qh, qh + take),
+// ILP triplets per lane (model-specialised kernels): lane l evaluates
+// entries l + 32 u.  The self-force sums and the scatter into h keep the
+// one-triplet-per-lane order (entry l before l + 32, and the window's
+// halves scattered one after the other).
+template <typename T, int CAP, int FAST, int ILP>
+__device__ __forceinline__ void forcesStepN(Stage<T, CAP, true, 1> const& S, Members<T, true> const& mb, DevGroup const& G,
+                                            DevCutoff const& cut, bool narrow, const int* queue, int qh, int take,
+                                            int lane, double (&h)[3][CAP], double& sfx, double& sfy, double& sfz)
 {
+    Triplet<T> t[ILP];
+    int so[ILP], sp[ILP];
+    bool ok[ILP];
+    loadTriplets<T, CAP>(S, cut, narrow, queue, qh, take, lane, t, so, sp, ok);
+    T bv[ILP][kMaxStagedBases], cost[ILP];
+#pragma unroll
+    for (int u = 0; u < ILP; ++u)
+    {
+        tripletBases<T, CAP>(S, G, narrow, so[u], sp[u], t[u].rjk2, bv[u]);
+        cost[u] = t[u].cost;
+    }
+    T T1[ILP], T2[ILP], T3[ILP];
+    gridForcesN<T, FAST, true, ILP>(bv, G, mb, cost, T1, T2, T3);
+    double o[ILP][3], q[ILP][3];
+#pragma unroll
+    for (int u = 0; u < ILP; ++u)
+    {
+        Triplet<T> const& x = t[u];
+        const T dfcr2 = S.dfcr[sp[u]];
+        const T pfc = x.fc1 * x.fc2 * x.fcjk;
+        const T pr1 = x.fc2 * x.fcjk * x.dfcr1;
+        const T pr2 = x.fc1 * x.fcjk * dfcr2;
+        const T pr3 = narrow ? x.fc1 * x.fc2 * x.dfcjk * x.rijk : T(0);
+        const T P1 = pfc * ((x.rinv - x.cost * x.ri1 * x.ri1) * T1[u] - T2[u]) + pr1 * T3[u];
+        const T P2 = pfc * ((x.rinv - x.cost * x.ri2 * x.ri2) * T1[u] - T2[u]) + pr2 * T3[u];
+        const T P3 = narrow ? (pfc * (x.rinv * T1[u] + T2[u]) - pr3 * T3[u]) : (pfc * x.rinv * T1[u]);
+        o[u][0] = (double)(P1 * x.x1 + P3 * x.dx3);
+        o[u][1] = (double)(P1 * x.y1 + P3 * x.dy3);
+        o[u][2] = (double)(P1 * x.z1 + P3 * x.dz3);
+        q[u][0] = (double)(P2 * x.x2 - P3 * x.dx3);
+        q[u][1] = (double)(P2 * x.y2 - P3 * x.dy3);
+        q[u][2] = (double)(P2 * x.z2 - P3 * x.dz3);
+        if (ok[u])
+        {
+            sfx -= (double)(P1 * x.x1 + P2 * x.x2);
+            sfy -= (double)(P1 * x.y1 + P2 * x.y2);
+            sfz -= (double)(P1 * x.z1 + P2 * x.z2);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < ILP; ++u)
+    {
+        // one conflict-free add per round present in this half of the window
+        const int idx = lane + 32 * u;
+        const bool mine = idx < take;
+        const int rnd = mine ? entryRound(queue[(qh + idx) & (kQueue - 1)]) : -1;
+        const int prevRnd = __shfl_up_sync(kFullMask, rnd, 1);
+        const unsigned heads = __ballot_sync(kFullMask, mine && (lane == 0 || prevRnd != rnd));
+        const int mySub = __popc(heads & ((2u << lane) - 1u)) - 1;
+        const int nSub = __popc(heads);
+        for (int r = 0; r < nSub; ++r)
+        {
+            if (mine && mySub == r)
+            {
+                h[0][so[u]] += o[u][0];
+                h[1][so[u]] += o[u][1];
+                h[2][so[u]] += o[u][2];
+                h[0][sp[u]] += q[u][0];
+                h[1][sp[u]] += q[u][1];
+                h[2][sp[u]] += q[u][2];
+            }
+            __syncwarp();
+        }
+    }
+}
+
+template <typename T, int CAP, int WARPS, int FAST>
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
+    kSFForcesF(DevModel model, BatchView b, int lower)
+{
+    constexpr int ILP = 1;            // triplets per lane and step (see loadTriplets)
+    constexpr int kStep = 32 * ILP;   // triplets per warp step
     extern __shared__ __align__(16) unsigned char smemRaw[];
     ForcesSmem<T, CAP, FAST>& SM = reinterpret_cast<ForcesSmem<T, CAP, FAST>*>(smemRaw)[threadIdx.x >> 5];
     auto& S = SM.st;
@@ -893,11 +1155,25 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(Dev
                 int p0 = 0;
                 while (true)
                 {
-                    if (qn < 32 && p0 < cnt)   // queue stays below 32 + 64 entries
+                    if (qn < kStep && p0 < cnt)   // queue stays below kStep + 64 entries
                     {
                         enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane,
                                                   nullptr, maskIn, mwi);
                         p0 += 64;
+                    }
+                    if constexpr (FAST > 0)
+                    {
+                        if (qn >= kStep || (drain && qn > 0))
+                        {
+                            const int take = min(kStep, qn);
+                            forcesStepN<T, CAP, FAST, ILP>(S, mb, G, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh,
+                                                          take, lane, SM.h, sfx, sfy, sfz);
+                            qh = (qh + take) & (kQueue - 1);
+                            qn -= take;
+                            __syncwarp();
+                        }
+                        else if (p0 >= cnt) break;
+                        continue;
                     }
                     if (qn >= 32 || (drain && qn > 0))
                     {
@@ -920,17 +1196,16 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1) kSFForcesF(Dev
                             T bv[kMaxStagedBases];
                             if (fastG) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
                             T T1 = T(0), T3 = T(0), Uij = T(0), Uik = T(0), Ujk = T(0), vexp = T(0);
-                            if (FAST || G.grid)
+                            if (G.grid)
                             {
                                 T T2 = T(0);
-                                if constexpr (FAST > 0) gridForces<T, FAST>(bv, G, mb, t.cost, T1, T2, T3);
-                                else if (G.gridNZ <= 2) gridForces<T, 2>(bv, G, mb, t.cost, T1, T2, T3);
+                                if (G.gridNZ <= 2) gridForces<T, 2>(bv, G, mb, t.cost, T1, T2, T3);
                                 else gridForces<T, 4>(bv, G, mb, t.cost, T1, T2, T3);
                                 Uij = T2;
                                 Uik = T2;
                                 Ujk = T2;
                             }
-                            else if constexpr (FAST == 0)
+                            else
                             {
                             for (int q = 0; q < M; ++q)
                             {
