@@ -298,7 +298,8 @@ def run_ours(args):
             stud["span_descriptor"] = {k: span[k] for k in (
                 "value", "unit", "ms_per_step", "speedup_vs_fp64", "fallback_rate", "err_vs_teacher_fp64_gpu",
                 "err_vs_teacher_fp64_gpu_teacher_in_range", "held_out_monitor", "_predictions")}
-            stud["span_descriptor"]["descriptor"] = "chosen by force span from a candidate grid, angular cutoff 12 bohr"
+            stud["span_descriptor"]["descriptor"] = ("chosen by force span from a candidate grid within the groups the "
+                                                     "specialised kernels run, angular cutoff 12 bohr")
 
     sf_ms = sum(t for n, t in stages if n in ("sf_values", "sf_forces"))
     sf_flops = sum(work[k] * f for k, f in FLOPS_PER.items())

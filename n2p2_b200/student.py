@@ -216,17 +216,18 @@ def span_residual(M, B, c, subset, ridge=1e-10):
     return float((c - (b * x).sum(axis=1)).sum())
 
 
-def greedy_span_selection(M, B, c, types, budget):
+def greedy_span_selection(M, B, c, types, budget, admissible=None):
     """Forward selection of candidate columns minimising span_residual, taking
-    at most budget[t] candidates of type types[j] == t; returns the chosen
-    indices in order and the relative residual after each choice."""
+    at most budget[t] candidates of type types[j] == t (and, with
+    `admissible`, only j for which admissible(chosen, j) holds); returns the
+    chosen indices in order and the relative residual after each choice."""
     left = dict(budget)
     chosen, trace = [], []
     total = float(c.sum())
     while any(left.get(t, 0) > 0 for t in set(types)):
         best = None
         for j, t in enumerate(types):
-            if j in chosen or left.get(t, 0) <= 0:
+            if j in chosen or left.get(t, 0) <= 0 or (admissible is not None and not admissible(chosen, j)):
                 continue
             r = span_residual(M, B, c, chosen + [j])
             if best is None or r < best[0]:
@@ -239,8 +240,52 @@ def greedy_span_selection(M, B, c, types, budget):
     return chosen, trace
 
 
+GAUSSIAN_PLAN_MAX_POWER = 16   # exp(-eta r^2) as an integer power <= 16 of a group's base Gaussian
+GAUSSIAN_PLAN_MAX_BASES = 4    # base Gaussians of a radial group in the specialised kernels
+
+
+def gaussian_bases(etas):
+    """Base widths of the engine's Gaussian plan for one group's widths (in
+    ascending order, each width an integer multiple <= 16 of an earlier base
+    within 1e-9, else a new base)."""
+    bases = []
+    for eta in sorted(set(etas)):
+        for b in bases:
+            k = round(eta / b)
+            if 1 <= k <= GAUSSIAN_PLAN_MAX_POWER and abs(eta / b - k) <= 1e-9 * eta / b:
+                break
+        else:
+            bases.append(eta)
+    return bases
+
+
+def specialised_kernel_admissible(sfs):
+    """admissible(chosen, j) for greedy_span_selection: adding candidate j
+    keeps every group of the chosen set runnable by the model-specialised
+    symmetry-function kernels -- radial groups (per neighbour element and
+    cutoff) with at most GAUSSIAN_PLAN_MAX_BASES base Gaussians; angular
+    groups (per element pair and cutoff) with one base Gaussian, at most two
+    widths, two lambdas and four integer zetas <= 32.  A descriptor outside
+    this runs on the generic kernels, several times slower per triplet.
+    sfs: Mode.symmetryFunction tuples of the candidates."""
+    def key(f):
+        return (f[0], f[1], f[2] if f[0] != 2 else -1, f[7])
+
+    def admissible(chosen, j):
+        grp = [sfs[i] for i in chosen if key(sfs[i]) == key(sfs[j])] + [sfs[j]]
+        etas = [f[3] for f in grp]
+        if any(f[4] != 0.0 for f in grp):
+            return False
+        if sfs[j][0] == 2:
+            return len(gaussian_bases(etas)) <= GAUSSIAN_PLAN_MAX_BASES
+        zetas = {f[6] for f in grp}
+        return (len(gaussian_bases(etas)) == 1 and len(set(etas)) <= 2 and len({f[5] for f in grp}) <= 2
+                and len(zetas) <= 4 and all(float(z).is_integer() and 1 <= z <= 32 for z in zetas))
+    return admissible
+
+
 def select_by_force_span(teacher_mode, structs, candidate_dir, n_radial=8, n_angular=6, rc_angular=None,
-                         device=0, log=None):
+                         device=0, log=None, specialised=True):
     """symfunction_short lines of the student's descriptor chosen from
     candidate_sf_lines: per element, the n_radial radial and n_angular angular
     candidates whose dG/dr vectors best span the teacher's per-atom force
@@ -252,7 +297,9 @@ def select_by_force_span(teacher_mode, structs, candidate_dir, n_radial=8, n_ang
     a_s its own dE_i/dG'_is.  The least-squares residual of f_i against the
     span of those vectors, summed over atoms, is the part of the teacher's
     forces that no network on S reproduces even with free per-atom
-    coefficients; the selection minimises it.  Returns (lines, report)."""
+    coefficients; the selection minimises it.  With `specialised`, only
+    sets the model-specialised kernels run are considered
+    (specialised_kernel_admissible).  Returns (lines, report)."""
     sym = [teacher_mode.elementSymbol(e) for e in range(teacher_mode.numElements)]
     cand = candidate_sf_lines(teacher_mode, rc_angular)
     write_student_model(candidate_dir, structs, device=device, sf_lines=cand)
@@ -262,7 +309,8 @@ def select_by_force_span(teacher_mode, structs, candidate_dir, n_radial=8, n_ang
     for e, (M, B, c) in enumerate(stats):
         sfs = [cm.symmetryFunction(e, i) for i in range(cm.numSymmetryFunctions(e))]
         types = [f[0] for f in sfs]
-        chosen, trace = greedy_span_selection(M, B, c, types, {2: n_radial, 3: n_angular})
+        chosen, trace = greedy_span_selection(M, B, c, types, {2: n_radial, 3: n_angular},
+                                              specialised_kernel_admissible(sfs) if specialised else None)
         every = span_residual(M, B, c, range(len(sfs))) / float(c.sum())
         lines += [_sf_line(sym, e, sfs[j]) for j in sorted(chosen)]
         report[sym[e]] = {"candidates": len(sfs), "atoms": int(c.size), "residual_all_candidates": every,

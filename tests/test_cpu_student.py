@@ -80,3 +80,24 @@ def test_candidate_grid_is_a_valid_descriptor(tmp_path):
         assert all(f[7] == 8.0 for f in sfs if f[0] == 3)
     m.close()
     t.close()
+
+
+def test_gaussian_plan_and_specialised_admissibility():
+    """The selection's copy of the engine's Gaussian plan, and the group rules
+    of the model-specialised kernels it keeps the chosen set within."""
+    assert student.gaussian_bases([0.001, 0.01, 0.03, 0.06, 0.15, 0.3, 0.6, 1.5]) == [0.001, 0.03, 0.6, 1.5]
+    assert student.gaussian_bases([0.03, 0.01]) == [0.01]
+    assert student.gaussian_bases([0.001, 0.03]) == [0.001, 0.03]        # ratio 30 > 16
+    # (type, e1, e2, eta, rs, lambda, zeta, rc, scaling)
+    ang = lambda eta, lam, zeta, e1=0, e2=1, rc=12.0: (3, e1, e2, eta, 0.0, lam, zeta, rc, 1.0)
+    rad = lambda eta, e1=0: (2, e1, e1, eta, 0.0, 0.0, 0.0, 12.0, 1.0)
+    sfs = [ang(0.01, 1, 1), ang(0.03, -1, 4), ang(0.001, 1, 1), ang(0.003, 1, 2), ang(0.001, 1, 1, e1=1),
+           rad(0.001), rad(0.03), rad(0.6), rad(1.5), rad(1.0), rad(3.0)]
+    ok = student.specialised_kernel_admissible(sfs)
+    assert ok([0], 1)              # widths 0.01, 0.03 share a base
+    assert not ok([0, 1], 2)       # a third width
+    assert not ok([0], 3)          # 0.01 and 0.003: two bases
+    assert ok([0, 1], 4)           # another element pair is another group
+    assert ok([5, 6, 7], 8)        # four radial bases
+    assert not ok([5, 6, 7, 8], 9)  # a fifth
+    assert ok([5, 6, 7, 8], 10)    # 3.0 = 2 x 1.5: shares the last base
