@@ -55,6 +55,7 @@ typedef int n2p2_status;
 typedef struct n2p2_mode n2p2_mode;
 typedef struct n2p2_batch n2p2_batch;
 typedef struct n2p2_trainer n2p2_trainer;
+typedef struct n2p2_lammps n2p2_lammps;
 
 /* Message of the last failure on this thread ("" if none). */
 const char* n2p2_last_error(void);
@@ -226,6 +227,69 @@ n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches);
 n2p2_status n2p2_neighbor_list_noalloc(const double* positions, int64_t numAtoms, const double* box, double cutoff,
                                        int64_t capacity, int64_t* offsets, int32_t* index, int32_t* image,
                                        double* d, double* dr, int64_t* numEntries, void* stream);
+
+/* ---- LAMMPS interface ------------------------------------------------------
+ * nnp::InterfaceLammps (src/libnnpif/LAMMPS/InterfaceLammps.h:31-333), the
+ * object `pair_style hdnnp` (src/interface/LAMMPS/src/ML-HDNNP/pair_hdnnp.cpp)
+ * drives every MD step: local atoms and their full neighbour lists (local and
+ * ghost neighbours, LAMMPS indices) in, energy and forces on local AND ghost
+ * atoms out (LAMMPS folds the ghost forces back to their owners).  2G models.
+ * Units: LAMMPS units in and out, converted with cflength/cfenergy as the
+ * reference does.  The neighbours' forces are gathered on the device per
+ * target atom in a fixed order (no atomics).  Extra over the reference:
+ * n2p2_lammps_set_precision and n2p2_lammps_transfer_neighbor_list. */
+n2p2_status n2p2_lammps_create(n2p2_lammps** lammps, int device);
+n2p2_status n2p2_lammps_destroy(n2p2_lammps* lammps);
+/* InterfaceLammps::initialize (InterfaceLammps.cpp:51-255): reads
+ * directory/input.nn, scaling.data and weights.%03zu.data; emap "1:H,2:O"
+ * maps LAMMPS types to elements (empty: type t is element t-1, requires
+ * lammpsNtypes == number of elements; unmapped types are ignored); errors
+ * of the reference (cutoff smaller than the largest symmetry-function cutoff,
+ * inconsistent or invalid map) as N2P2_ERR_RUNTIME.  Extrapolation warnings
+ * are counted when showew, showewsum > 0 or maxew >= 0; resetew, showewsum,
+ * maxew and myRank are the pair style's business (kept for the signature). */
+n2p2_status n2p2_lammps_initialize(n2p2_lammps* lammps, const char* directory, const char* emap, int32_t showew,
+                                   int32_t resetew, int32_t showewsum, int32_t maxew, double cflength,
+                                   double cfenergy, double lammpsCutoff, int32_t lammpsNtypes, int32_t myRank);
+/* N2P2_PRECISION_FP64 (default) or N2P2_PRECISION_MIXED. */
+n2p2_status n2p2_lammps_set_precision(n2p2_lammps* lammps, int precision);
+/* InterfaceLammps::getMaxCutoffRadius (InterfaceLammps.cpp:528-532), LAMMPS units. */
+n2p2_status n2p2_lammps_get_max_cutoff_radius(n2p2_lammps* lammps, double* radius);
+/* InterfaceLammps::setLocalAtoms (InterfaceLammps.cpp:267-304): atomType[i]
+ * = LAMMPS type (1-based) of local atom i; clears the neighbour lists. */
+n2p2_status n2p2_lammps_set_local_atoms(n2p2_lammps* lammps, int32_t numAtomsLocal, const int32_t* atomType);
+/* InterfaceLammps::addNeighbor (InterfaceLammps.cpp:410-441): neighbour j
+ * (LAMMPS index, local or ghost) of local atom i, with j's tag and type,
+ * dx = x_i - x_j (LAMMPS units) and d2 = |dx|^2.  Tags are not used by 2G
+ * models.  Neighbours beyond the largest symmetry-function cutoff are dropped
+ * (they contribute nothing in the reference either). */
+n2p2_status n2p2_lammps_add_neighbor(n2p2_lammps* lammps, int32_t i, int32_t j, int64_t tag, int32_t type,
+                                     double dx, double dy, double dz, double d2);
+/* PairHDNNP::transferNeighborList (pair_hdnnp.cpp:274-290) in one call,
+ * with LAMMPS's own arrays: list->inum, ilist, numneigh, firstneigh
+ * (special-bond bits masked as NEIGHMASK does), atom->x, atom->type; every
+ * pair with d2 <= maxCutoffRadius^2 (the pair style's cutoff) is added. */
+n2p2_status n2p2_lammps_transfer_neighbor_list(n2p2_lammps* lammps, int32_t inum, const int32_t* ilist,
+                                               const int32_t* numneigh, const int32_t* const* firstneigh,
+                                               const double* const* x, const int32_t* type,
+                                               double maxCutoffRadius);
+/* InterfaceLammps::process (InterfaceLammps.cpp:463-500): symmetry
+ * functions, networks, energy and the force pass on the device. */
+n2p2_status n2p2_lammps_process(n2p2_lammps* lammps);
+/* InterfaceLammps::getEnergy / getAtomicEnergy (InterfaceLammps.cpp:550-570),
+ * LAMMPS units; `index` counts the local atoms of mapped types. */
+n2p2_status n2p2_lammps_get_energy(n2p2_lammps* lammps, double* energy);
+n2p2_status n2p2_lammps_get_atomic_energy(n2p2_lammps* lammps, int32_t index, double* energy);
+/* InterfaceLammps::getForces (InterfaceLammps.cpp:679-740): ADDS the forces
+ * (LAMMPS units) on every local and ghost atom named by the lists to
+ * atomF[k][0..2] (LAMMPS's atom->f rows). */
+n2p2_status n2p2_lammps_get_forces(n2p2_lammps* lammps, double* const* atomF);
+/* Mode::getNumExtrapolationWarnings: out-of-range (atom, symmetry function)
+ * occurrences summed over process() calls since the last
+ * clearExtrapolationWarnings (InterfaceLammps.cpp:1049-1058; the pair style
+ * clears after every step). */
+n2p2_status n2p2_lammps_get_num_extrapolation_warnings(n2p2_lammps* lammps, int64_t* count);
+n2p2_status n2p2_lammps_clear_extrapolation_warnings(n2p2_lammps* lammps);
 
 /* ---- training on energies and forces --------------------------------------
  * The reference trains with nnp::Training (libnnptrain/Training.cpp) on the

@@ -5,7 +5,8 @@ include/n2p2_b200.h; all evaluation runs in libn2p2b200.so (sm_100a).
 """
 from .structure import Structure, read_structures, write_structures  # noqa: F401
 
-__all__ = ["Structure", "read_structures", "write_structures", "Mode", "Prediction", "Batch", "Trainer"]
+__all__ = ["Structure", "read_structures", "write_structures", "Mode", "Prediction", "Batch", "Trainer",
+           "InterfaceLammps"]
 
 
 def __getattr__(name):
@@ -13,4 +14,7 @@ def __getattr__(name):
     if name in ("Mode", "Prediction", "Batch", "Trainer"):
         from . import mode
         return getattr(mode, name)
+    if name == "InterfaceLammps":
+        from . import lammps
+        return lammps.InterfaceLammps
     raise AttributeError(name)

@@ -89,6 +89,21 @@ SIGNATURES = {
     "n2p2_trainer_get_parameters": (_i, [_vp, _P(_d)]),
     "n2p2_trainer_set_parameters": (_i, [_vp, _P(_d)]),
     "n2p2_trainer_step": (_i, [_vp, _vp, _P(_d), _P(_d), ctypes.c_int32, _P(_d), _P(_d)]),
+    "n2p2_lammps_create": (_i, [_P(_vp), _i]),
+    "n2p2_lammps_destroy": (_i, [_vp]),
+    "n2p2_lammps_initialize": (_i, [_vp, _cp, _cp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                    _d, _d, _d, ctypes.c_int32, ctypes.c_int32]),
+    "n2p2_lammps_set_precision": (_i, [_vp, _i]),
+    "n2p2_lammps_get_max_cutoff_radius": (_i, [_vp, _P(_d)]),
+    "n2p2_lammps_set_local_atoms": (_i, [_vp, ctypes.c_int32, _vp]),
+    "n2p2_lammps_add_neighbor": (_i, [_vp, ctypes.c_int32, ctypes.c_int32, _i64, ctypes.c_int32, _d, _d, _d, _d]),
+    "n2p2_lammps_transfer_neighbor_list": (_i, [_vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp, _d]),
+    "n2p2_lammps_process": (_i, [_vp]),
+    "n2p2_lammps_get_energy": (_i, [_vp, _P(_d)]),
+    "n2p2_lammps_get_atomic_energy": (_i, [_vp, ctypes.c_int32, _P(_d)]),
+    "n2p2_lammps_get_forces": (_i, [_vp, _vp]),
+    "n2p2_lammps_get_num_extrapolation_warnings": (_i, [_vp, _P(_i64)]),
+    "n2p2_lammps_clear_extrapolation_warnings": (_i, [_vp]),
     "n2p2_host_alloc": (_i, [_P(_vp), ctypes.c_size_t]),
     "n2p2_host_free": (_i, [_vp]),
 }

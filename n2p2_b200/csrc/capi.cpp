@@ -13,6 +13,7 @@
 
 #include "engine.hpp"
 #include "host_model.hpp"
+#include "lammps.hpp"
 #include "trainer.hpp"
 
 using namespace n2p2b200;
@@ -36,6 +37,14 @@ struct n2p2_trainer
 {
     n2p2_mode* mode = nullptr;
     std::unique_ptr<Trainer> trainer;
+};
+
+struct n2p2_lammps
+{
+    n2p2_mode mode;                  // the model, its device copy and the stream
+    std::unique_ptr<Batch> batch;    // created by the first process()
+    LammpsInterface iface;
+    int64_t warnings = 0;
 };
 
 struct n2p2_batch
@@ -755,6 +764,158 @@ n2p2_status n2p2_host_free(void* ptr)
 {
     if (!ptr) return N2P2_OK;
     return guard([&] { cudaCheck(cudaFreeHost(ptr), "cudaFreeHost"); });
+}
+
+n2p2_status n2p2_lammps_create(n2p2_lammps** lammps, int device)
+{
+    N2P2_REQUIRE(lammps);
+    return guard([&] {
+        auto l = std::make_unique<n2p2_lammps>();
+        l->mode.device = device;
+        *lammps = l.release();
+    });
+}
+
+n2p2_status n2p2_lammps_destroy(n2p2_lammps* lammps)
+{
+    if (!lammps) return N2P2_OK;
+    return guard([&] {
+        cudaStream_t s = lammps->mode.stream;
+        if (s) cudaSetDevice(lammps->mode.device);
+        lammps->batch.reset();
+        delete lammps;
+        if (s) cudaStreamDestroy(s);
+    });
+}
+
+n2p2_status n2p2_lammps_initialize(n2p2_lammps* lammps, const char* directory, const char* emap, int32_t showew,
+                                   int32_t resetew, int32_t showewsum, int32_t maxew, double cflength,
+                                   double cfenergy, double lammpsCutoff, int32_t lammpsNtypes, int32_t myRank)
+{
+    N2P2_REQUIRE(lammps);
+    N2P2_REQUIRE(directory);
+    (void)resetew;
+    return guard([&] {
+        if (lammps->iface.isInitialized() || lammps->mode.model.setupDone)
+            throw std::runtime_error("ERROR: the LAMMPS interface is already initialized.\n");
+        std::string dir(directory);
+        if (dir.empty() || dir.back() != '/') dir += '/';
+        n2p2_mode& m = lammps->mode;
+        m.model.loadSettingsFile(dir + "input.nn");
+        m.model.setupGeneric();
+        m.model.setupSymmetryFunctionScaling(dir + "scaling.data");
+        m.checkExtrapolation = showew || showewsum > 0 || maxew >= 0;
+        m.model.setupNeuralNetworkWeights(dir + "weights.%03zu.data");
+        m.uploaded = false;
+        lammps->iface.initialize(m.model, emap ? emap : "", cflength, cfenergy, lammpsCutoff, lammpsNtypes, myRank);
+    });
+}
+
+n2p2_status n2p2_lammps_set_precision(n2p2_lammps* lammps, int precision)
+{
+    N2P2_REQUIRE(lammps);
+    return n2p2_mode_set_precision(&lammps->mode, precision);
+}
+
+n2p2_status n2p2_lammps_get_max_cutoff_radius(n2p2_lammps* lammps, double* radius)
+{
+    N2P2_REQUIRE(lammps);
+    N2P2_REQUIRE(radius);
+    return guard([&] {
+        if (!lammps->iface.isInitialized()) throw std::runtime_error("ERROR: the LAMMPS interface is not initialized.\n");
+        *radius = lammps->iface.maxCutoffRadius();
+    });
+}
+
+n2p2_status n2p2_lammps_set_local_atoms(n2p2_lammps* lammps, int32_t numAtomsLocal, const int32_t* atomType)
+{
+    N2P2_REQUIRE(lammps);
+    if (numAtomsLocal > 0) N2P2_REQUIRE(atomType);
+    return guard([&] { lammps->iface.setLocalAtoms(numAtomsLocal, atomType); });
+}
+
+n2p2_status n2p2_lammps_add_neighbor(n2p2_lammps* lammps, int32_t i, int32_t j, int64_t tag, int32_t type,
+                                     double dx, double dy, double dz, double d2)
+{
+    N2P2_REQUIRE(lammps);
+    (void)tag;
+    return guard([&] { lammps->iface.addNeighbor(i, j, type, dx, dy, dz, d2); });
+}
+
+n2p2_status n2p2_lammps_transfer_neighbor_list(n2p2_lammps* lammps, int32_t inum, const int32_t* ilist,
+                                               const int32_t* numneigh, const int32_t* const* firstneigh,
+                                               const double* const* x, const int32_t* type, double maxCutoffRadius)
+{
+    N2P2_REQUIRE(lammps);
+    if (inum > 0)
+    {
+        N2P2_REQUIRE(ilist);
+        N2P2_REQUIRE(numneigh);
+        N2P2_REQUIRE(firstneigh);
+        N2P2_REQUIRE(x);
+        N2P2_REQUIRE(type);
+    }
+    return guard(
+        [&] { lammps->iface.transferNeighborList(inum, ilist, numneigh, firstneigh, x, type, maxCutoffRadius); });
+}
+
+n2p2_status n2p2_lammps_process(n2p2_lammps* lammps)
+{
+    N2P2_REQUIRE(lammps);
+    return guard([&] {
+        n2p2_mode& m = lammps->mode;
+        ensureUploaded(&m);
+        if (!lammps->batch) lammps->batch = std::make_unique<Batch>(m.model, m.dmodel, m.stream, m.sms);
+        lammps->batch->autotuneEnabled = m.autotune;
+        lammps->iface.process(*lammps->batch, m.precision, m.checkExtrapolation);
+        if (m.checkExtrapolation && lammps->iface.numCenters() > 0)
+            lammps->warnings += lammps->batch->status().extrapolationWarnings;
+    });
+}
+
+n2p2_status n2p2_lammps_get_energy(n2p2_lammps* lammps, double* energy)
+{
+    N2P2_REQUIRE(lammps);
+    N2P2_REQUIRE(energy);
+    *energy = lammps->iface.energy();
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_lammps_get_atomic_energy(n2p2_lammps* lammps, int32_t index, double* energy)
+{
+    N2P2_REQUIRE(lammps);
+    N2P2_REQUIRE(energy);
+    return guard([&] {
+        if (!lammps->batch) throw std::runtime_error("ERROR: process() has not run.\n");
+        setDevice(&lammps->mode);
+        *energy = lammps->iface.atomicEnergy(*lammps->batch, index);
+    });
+}
+
+n2p2_status n2p2_lammps_get_forces(n2p2_lammps* lammps, double* const* atomF)
+{
+    N2P2_REQUIRE(lammps);
+    N2P2_REQUIRE(atomF);
+    return guard([&] {
+        if (!lammps->batch) throw std::runtime_error("ERROR: process() has not run.\n");
+        setDevice(&lammps->mode);
+        lammps->iface.addForces(*lammps->batch, atomF);
+    });
+}
+
+n2p2_status n2p2_lammps_get_num_extrapolation_warnings(n2p2_lammps* lammps, int64_t* count)
+{
+    N2P2_REQUIRE(lammps);
+    N2P2_REQUIRE(count);
+    *count = lammps->warnings;
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_lammps_clear_extrapolation_warnings(n2p2_lammps* lammps)
+{
+    N2P2_REQUIRE(lammps);
+    lammps->warnings = 0;
+    return N2P2_OK;
 }
 
 } // extern "C"

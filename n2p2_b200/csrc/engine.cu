@@ -545,6 +545,8 @@ void Batch::releaseAll()
 void Batch::setStructures(std::vector<StructureInput> const& s, const int* elements, int remap)
 {
     releaseAll();
+    external_ = false;
+    numTargets_ = 0;
     structs_ = s;
     S_ = (int)s.size();
     N_ = 0;
@@ -611,21 +613,7 @@ void Batch::setStructures(std::vector<StructureInput> const& s, const int* eleme
     }
 
     allocateAtoms();
-    // atoms grouped by element (the tensor-core networks run per element)
-    {
-        std::vector<int> order;
-        order.reserve(N_);
-        v_.elemBegin[0] = 0;
-        for (int e = 0; e < ne; ++e)
-        {
-            for (int a = 0; a < N_; ++a)
-                if (elemHost_[a] == e) order.push_back(a);
-            v_.elemBegin[e + 1] = (int)order.size();
-        }
-        int* dev = devAlloc<int>(pool_, (size_t)N_, owned_);
-        cudaCheck(cudaMemcpy(dev, order.data(), sizeof(int) * (size_t)N_, cudaMemcpyHostToDevice), "upload element lists");
-        v_.elemAtoms = dev;
-    }
+    uploadElementLists();
     v_.numCells = cellTotal;
     v_.cellCount = devAlloc<int>(pool_, cellTotal, owned_);
     v_.cellStart = devAlloc<int>(pool_, cellTotal, owned_);
@@ -647,6 +635,144 @@ void Batch::setStructures(std::vector<StructureInput> const& s, const int* eleme
     allocateNeighbors(std::max<int64_t>(capacity, 1));
     capacityVerified_ = false;
     tuned_[0] = tuned_[1] = false;   // new workload: shapes come from the cache or are measured again
+}
+
+// Atoms grouped by element (the tensor-core networks run per element).
+void Batch::uploadElementLists()
+{
+    const int ne = (int)model_.numElements();
+    std::vector<int> order;
+    order.reserve(N_);
+    v_.elemBegin[0] = 0;
+    for (int e = 0; e < ne; ++e)
+    {
+        for (int a = 0; a < N_; ++a)
+            if (elemHost_[a] == e) order.push_back(a);
+        v_.elemBegin[e + 1] = (int)order.size();
+    }
+    int* dev = devAlloc<int>(pool_, (size_t)std::max(N_, 1), owned_);
+    if (N_ > 0)
+        cudaCheck(cudaMemcpy(dev, order.data(), sizeof(int) * (size_t)N_, cudaMemcpyHostToDevice),
+                  "upload element lists");
+    v_.elemAtoms = dev;
+}
+
+void Batch::setExternalNeighbors(int numCenters, const int* elements, int64_t numEntries, const int64_t* offsets,
+                                 int numTargets, const int* target, const int* targetElement, const double* dr,
+                                 const double* d, const int* centerTarget)
+{
+    if (numCenters <= 0) throw std::runtime_error("ERROR: no local atoms.\n");
+    if (numEntries < 0 || offsets[0] != 0 || offsets[numCenters] != numEntries)
+        throw std::invalid_argument("ERROR: neighbour offsets do not match the entry count.\n");
+    const int ne = (int)model_.numElements();
+    // Everything but the candidate-mask buffer is released: a caller that
+    // sets new lists every step (an MD code) keeps masks of the last size.
+    releaseGraph();
+    freeAll(pool_, ownedDGdr_);
+    freeAll(pool_, ownedNbr_);
+    freeAll(pool_, owned_);
+    dgdrAllocated_ = false;
+    external_ = true;
+    S_ = 1;
+    N_ = numCenters;
+    structs_.assign(1, StructureInput{});
+    structs_[0].numAtoms = N_;
+    structBegin_ = {0, N_};
+    elemHost_.assign(elements, elements + N_);
+    numAtomsPerElement_.assign((size_t)ne, 0);
+    for (int a = 0; a < N_; ++a)
+    {
+        if (elemHost_[a] < 0 || elemHost_[a] >= ne) throw std::runtime_error("ERROR: element index out of range.\n");
+        numAtomsPerElement_[elemHost_[a]]++;
+    }
+    numTargets_ = numTargets;
+    std::vector<int> targetCenter(std::max(numTargets, 1), -1);
+    for (int a = 0; a < N_; ++a)
+    {
+        const int k = centerTarget[a];
+        if (k < 0 || k >= numTargets || targetCenter[k] >= 0)
+            throw std::invalid_argument("ERROR: local atom indices must be distinct and below the atom count.\n");
+        targetCenter[k] = a;
+    }
+    const double rcmax = model_.maxCutoffRadius;
+    std::vector<int64_t> tCount((size_t)numTargets + 1, 0);
+    for (int a = 0; a < N_; ++a)
+    {
+        if (offsets[a + 1] < offsets[a] || offsets[a + 1] - offsets[a] > 1024)
+            throw std::runtime_error("ERROR: more than 1024 neighbours of one atom.\n");
+        for (int64_t e = offsets[a]; e < offsets[a + 1]; ++e)
+        {
+            if (target[e] < 0 || target[e] >= numTargets)
+                throw std::invalid_argument("ERROR: neighbour index out of range.\n");
+            if (targetElement[e] < 0 || targetElement[e] >= ne)
+                throw std::runtime_error("ERROR: element index out of range.\n");
+            if (!(d[e] <= rcmax)) throw std::invalid_argument("ERROR: neighbour beyond the largest cutoff.\n");
+            tCount[(size_t)target[e] + 1]++;
+        }
+    }
+    // transposed lists: for each target the entries naming it, in entry order
+    for (int k = 0; k < numTargets; ++k) tCount[(size_t)k + 1] += tCount[k];
+    std::vector<int64_t> tEntry((size_t)std::max<int64_t>(numEntries, 1));
+    {
+        std::vector<int64_t> fill(tCount.begin(), tCount.end() - 1);
+        for (int64_t e = 0; e < numEntries; ++e) tEntry[(size_t)fill[target[e]]++] = e;
+    }
+    allocateAtoms();
+    uploadElementLists();
+    v_.numCells = 0;
+    v_.scanTmp = devAlloc<int64_t>(pool_, scanTileCount(N_) + 8, owned_);   // the candidate-mask offsets' scan
+    std::vector<DevStructInfo> info(1);
+    std::memset(info.data(), 0, sizeof(DevStructInfo));
+    info[0].numAtoms = N_;
+    cudaCheck(cudaMemcpyAsync(infoDev_, info.data(), sizeof(DevStructInfo), cudaMemcpyHostToDevice, stream_),
+              "upload structure info");
+    cudaCheck(cudaMemsetAsync(atomStructDev_, 0, sizeof(int) * N_, stream_), "memset");
+    cudaCheck(cudaMemcpyAsync(elemDev_, elemHost_.data(), sizeof(int) * N_, cudaMemcpyHostToDevice, stream_),
+              "upload elements");
+    cudaCheck(cudaMemcpyAsync(structBeginDev_, structBegin_.data(), sizeof(int) * 2, cudaMemcpyHostToDevice, stream_),
+              "upload offsets");
+    allocateNeighbors(std::max<int64_t>(numEntries, 1));
+    const size_t E = (size_t)numEntries;
+    std::vector<uint8_t> el(std::max<size_t>(E, 1));
+    std::vector<double> dx(std::max<size_t>(E, 1)), dy(dx.size()), dz(dx.size());
+    for (size_t e = 0; e < E; ++e)
+    {
+        el[e] = (uint8_t)targetElement[e];
+        dx[e] = dr[3 * e + 0];
+        dy[e] = dr[3 * e + 1];
+        dz[e] = dr[3 * e + 2];
+    }
+    auto up = [&](void* dst, const void* src, size_t bytes, char const* what) {
+        if (bytes) cudaCheck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), what);
+    };
+    up(v_.nbrOffset, offsets, sizeof(int64_t) * ((size_t)N_ + 1), "upload offsets");
+    up(v_.nbrJ, target, sizeof(int) * E, "upload neighbours");
+    up(v_.nbrElem, el.data(), E, "upload neighbour elements");
+    up(v_.nbrD, d, sizeof(double) * E, "upload distances");
+    up(v_.nbrDx, dx.data(), sizeof(double) * E, "upload dr");
+    up(v_.nbrDy, dy.data(), sizeof(double) * E, "upload dr");
+    up(v_.nbrDz, dz.data(), sizeof(double) * E, "upload dr");
+    tOffset_ = devAlloc<int64_t>(pool_, (size_t)numTargets + 1, ownedNbr_);
+    tEntry_ = devAlloc<int64_t>(pool_, tEntry.size(), ownedNbr_);
+    targetCenter_ = devAlloc<int>(pool_, targetCenter.size(), ownedNbr_);
+    entriesDev_ = devAlloc<int64_t>(pool_, 1, ownedNbr_);
+    up(entriesDev_, &numEntries, sizeof(int64_t), "upload entry count");
+    Ftarget_ = devAlloc<double>(pool_, 3 * (size_t)std::max(numTargets, 1), ownedNbr_);
+    up(tOffset_, tCount.data(), sizeof(int64_t) * ((size_t)numTargets + 1), "upload transposed offsets");
+    up(tEntry_, tEntry.data(), sizeof(int64_t) * E, "upload transposed entries");
+    up(targetCenter_, targetCenter.data(), sizeof(int) * targetCenter.size(), "upload centre map");
+    cudaCheck(cudaMemsetAsync(Ftarget_, 0, sizeof(double) * 3 * (size_t)std::max(numTargets, 1), stream_), "memset");
+    cudaCheck(cudaStreamSynchronize(stream_), "setExternalNeighbors");   // host staging vectors go out of scope
+    capacityVerified_ = false;
+    tuned_[0] = tuned_[1] = false;
+}
+
+void Batch::targetForces(double* out)
+{
+    if (!external_) throw std::runtime_error("ERROR: target forces need external neighbour lists.\n");
+    cudaCheck(cudaMemcpyAsync(out, Ftarget_, sizeof(double) * 3 * (size_t)numTargets_, cudaMemcpyDeviceToHost, stream_),
+              "F D2H");
+    synchronize();
 }
 
 void Batch::allocateAtoms()
@@ -739,12 +865,14 @@ void Batch::allocateDGdr()
 
 void Batch::setPositionsHost(const double* r)
 {
+    if (external_) throw std::runtime_error("ERROR: external neighbour lists carry no positions.\n");
     cudaCheck(cudaMemcpyAsync(rin_, r, sizeof(double) * 3 * (size_t)N_, cudaMemcpyHostToDevice, stream_),
               "positions H2D");
 }
 
 void Batch::setPositionsDevice(const double* r)
 {
+    if (external_) throw std::runtime_error("ERROR: external neighbour lists carry no positions.\n");
     cudaCheck(cudaMemcpyAsync(rin_, r, sizeof(double) * 3 * (size_t)N_, cudaMemcpyDeviceToDevice, stream_),
               "positions D2D");
 }
@@ -765,12 +893,19 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
     };
     mark("start");
     cudaCheck(cudaMemsetAsync(v_.status, 0, sizeof(DevStatus), stream_), "status reset");
-    launchPreparePositions(v_, rin_, remap_, model_.normalize ? 1 : 0, model_.convLength, stream_);
-    launches += 1;
-    mark("prepare_positions");
-    launchNeighborBuild(v_, model_.maxCutoffRadius * model_.maxCutoffRadius, stream_);
-    launches += 3 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1;
-    mark("neighbor_list");
+    if (external_)   // the entry count the neighbour build would report (read by the cutoff stage)
+        cudaCheck(cudaMemcpyAsync(&v_.status->totalNeighbors, entriesDev_, sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                                  stream_),
+                  "entry count");
+    else
+    {
+        launchPreparePositions(v_, rin_, remap_, model_.normalize ? 1 : 0, model_.convLength, stream_);
+        launches += 1;
+        mark("prepare_positions");
+        launchNeighborBuild(v_, model_.maxCutoffRadius * model_.maxCutoffRadius, stream_);
+        launches += 3 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1;
+        mark("neighbor_list");
+    }
     launchCutoffValues(m, v_, sms_, stream_);
     launches += 1;
     mark("cutoff_values");
@@ -824,7 +959,8 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
             launches += 2;
             mark("sf_forces");
         }
-        launchGatherForces(v_, sms_, stream_);
+        if (external_) launchGatherTargets(v_, numTargets_, tOffset_, tEntry_, targetCenter_, Ftarget_, sms_, stream_);
+        else launchGatherForces(v_, sms_, stream_);
         launches += 1;
         mark("gather_forces");
     }
@@ -851,6 +987,7 @@ std::vector<std::pair<std::string, double>> Batch::profileStages(int flags, int 
 
 void Batch::countWork(int64_t* counts)
 {
+    if (external_) throw std::runtime_error("ERROR: work counters need structures, not external neighbour lists.\n");
     unsigned long long* d = nullptr;
     cudaCheck(cudaMalloc(&d, sizeof(unsigned long long) * 10), "cudaMalloc");
     cudaCheck(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * 10, stream_), "memset");
@@ -1041,6 +1178,7 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
     if (N_ == 0) throw std::runtime_error("ERROR: no structures set.\n");
     if (flags & EVAL_STORE_DGDR)
     {
+        if (external_) throw std::runtime_error("ERROR: stored dG/dr is not available with external neighbour lists.\n");
         if (precision != PREC_FP64) throw std::runtime_error("ERROR: stored dG/dr is FP64 only.\n");
         allocateDGdr();
     }

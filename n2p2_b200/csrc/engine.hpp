@@ -93,6 +93,22 @@ public:
     // `remap` folds periodic positions into the cell (Structure::remap),
     // normalisation (if the model uses it) is applied on the device.
     void setStructures(std::vector<StructureInput> const& s, const int* elements, int remap);
+    // External neighbour lists instead of structures (the LAMMPS interface,
+    // InterfaceLammps::setLocalAtoms / addNeighbor, InterfaceLammps.cpp:267-441):
+    // `numCenters` atoms of one system with their elements; centre i's entries
+    // are [offsets[i], offsets[i+1]) with, per entry, the neighbour's index
+    // among `numTargets` atoms (the caller's numbering, ghosts included), its
+    // element, r_i - r_j ([E][3]) and |r_i - r_j|, internal units, every
+    // |r_i - r_j| <= the model's largest cutoff.  centerTarget[i] is centre
+    // i's own index among the targets.  evaluate() then skips the position
+    // and neighbour stages and gathers the forces of all targets
+    // (targetForces).  Stored dG/dr is not available in this form.
+    void setExternalNeighbors(int numCenters, const int* elements, int64_t numEntries, const int64_t* offsets,
+                              int numTargets, const int* target, const int* targetElement, const double* dr,
+                              const double* d, const int* centerTarget);
+    bool external() const { return external_; }
+    int numTargets() const { return numTargets_; }
+    void targetForces(double* out);   // [numTargets][3], internal units (synchronises)
     // Positions host -> device (pinned or pageable host memory), async on the stream.
     void setPositionsHost(const double* r);
     void setPositionsDevice(const double* r);
@@ -202,6 +218,15 @@ private:
     std::vector<void*> ownedMask_;
     uint32_t* maskBuf_ = nullptr;
     int64_t maskCap_ = 0;
+    void uploadElementLists();
+    // external neighbour lists
+    bool external_ = false;
+    int numTargets_ = 0;
+    int64_t* tOffset_ = nullptr;   // [numTargets + 1] entries naming each target ...
+    int64_t* tEntry_ = nullptr;    // ... in entry order
+    int* targetCenter_ = nullptr;  // [numTargets] centre index or -1
+    double* Ftarget_ = nullptr;    // [numTargets][3]
+    int64_t* entriesDev_ = nullptr;   // the entry count, copied into the status by every evaluation
 };
 
 } // namespace n2p2b200

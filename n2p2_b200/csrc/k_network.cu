@@ -222,6 +222,57 @@ __global__ void kGatherForces(BatchView b)
     }
 }
 
+// Forces on the atoms named by external neighbour lists (the LAMMPS
+// interface's local and ghost atoms, InterfaceLammps::getForces,
+// InterfaceLammps.cpp:679-740): F_k = sum, in entry order, of the force h
+// that each entry's centre puts on k (the entries naming k, listed by the
+// transposed lists tOffset/tEntry), plus the self force when k is a centre
+// (targetCenter[k] >= 0).  One warp per target, lanes strided over its
+// entries, fixed shuffle tree: the same result on every run, no atomics.
+__global__ void kGatherTargets(BatchView b, int numTargets, const int64_t* __restrict__ tOffset,
+                               const int64_t* __restrict__ tEntry, const int* __restrict__ targetCenter,
+                               double* __restrict__ F)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < numTargets; k += warpsPerGrid)
+    {
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int64_t t = tOffset[k] + lane; t < tOffset[k + 1]; t += 32)
+        {
+            const int64_t e = tEntry[t];
+            fx += b.hx[e];
+            fy += b.hy[e];
+            fz += b.hz[e];
+        }
+        fx = warpSum(fx);
+        fy = warpSum(fy);
+        fz = warpSum(fz);
+        if (lane == 0)
+        {
+            const int c = targetCenter[k];
+            if (c >= 0)
+            {
+                fx += b.fSelf[3 * (size_t)c + 0];
+                fy += b.fSelf[3 * (size_t)c + 1];
+                fz += b.fSelf[3 * (size_t)c + 2];
+            }
+            F[3 * (size_t)k + 0] = fx;
+            F[3 * (size_t)k + 1] = fy;
+            F[3 * (size_t)k + 2] = fz;
+        }
+    }
+}
+
+void launchGatherTargets(BatchView const& b, int numTargets, const int64_t* tOffset, const int64_t* tEntry,
+                         const int* targetCenter, double* F, int sms, cudaStream_t st)
+{
+    int blocks = (numTargets + 7) / 8;
+    if (blocks < 1) blocks = 1;
+    if (blocks > sms * 32) blocks = sms * 32;
+    kGatherTargets<<<blocks, 256, 0, st>>>(b, numTargets, tOffset, tEntry, targetCenter, F);
+}
+
 // Extrapolation check of Element::updateSymmetryFunctionStatistics
 // (Element.cpp:462-541): unscaled G outside [Gmin, Gmax] by more than
 // 1000 machine epsilon counts one warning.  One thread per atom.

@@ -120,6 +120,8 @@ void launchMaskOffsets(DevModel const& m, BatchView const& b, int sms, cudaStrea
 void launchNetworkTC(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st);
 void launchEnergySum(BatchView const& b, cudaStream_t st);
 void launchGatherForces(BatchView const& b, int sms, cudaStream_t st);
+void launchGatherTargets(BatchView const& b, int numTargets, const int64_t* tOffset, const int64_t* tEntry,
+                         const int* targetCenter, double* F, int sms, cudaStream_t st);
 void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 
 // neighbour list of one structure into caller buffers, no device allocation

@@ -103,3 +103,70 @@ def reference_noise(model_dir, structure):
     finally:
         p.close()
     return abs(a["energy"] - b["energy"]) / abs(a["energy"]), max_rel(b["forces"], a["forces"])
+
+
+BOHR_TO_A = 0.529177210903
+HA_TO_EV = 27.211386245988
+
+
+def lammps_domain(s, list_cut, type_of, length=1.0):
+    """One LAMMPS rank holding a whole orthorhombic periodic box: local atoms
+    wrapped into the cell, ghost images of them within `list_cut` (bohr)
+    outside it, and full neighbour lists of the local atoms (every local or
+    ghost atom j != i within list_cut, ascending j).  Coordinates are returned
+    in bohr x `length`.  Returns dict(x [nall,3], type [nall] (LAMMPS types
+    from type_of[element symbol]), owner [nall], nlocal, numneigh [nlocal],
+    firstneigh (flat, int32), ilist)."""
+    import itertools
+    box = np.asarray(s.box, dtype=np.float64)
+    assert np.allclose(box, np.diag(np.diag(box))), "orthorhombic boxes only"
+    L = np.diag(box)
+    assert np.all(L > list_cut), "one image layer must cover the list cutoff"
+    n = s.numAtoms
+    frac = s.positions / L
+    frac -= np.floor(frac)
+    local = frac * L
+    xs, owners = [local], [np.arange(n)]
+    for sh in itertools.product((-1, 0, 1), repeat=3):
+        if sh == (0, 0, 0):
+            continue
+        f = frac + np.array(sh, dtype=np.float64)
+        keep = np.all((f >= -list_cut / L) & (f < 1.0 + list_cut / L), axis=1)
+        xs.append(f[keep] * L)
+        owners.append(np.nonzero(keep)[0])
+    x = np.concatenate(xs)
+    owner = np.concatenate(owners)
+    types = np.array([type_of[e] for e in s.elements], dtype=np.int32)[owner]
+    numneigh, firstneigh = [], []
+    for i in range(n):
+        d = x - x[i]
+        d2 = np.einsum("ij,ij->i", d, d)
+        js = np.nonzero(d2 <= list_cut * list_cut)[0]
+        js = js[js != i]
+        numneigh.append(js.size)
+        firstneigh.append(js.astype(np.int32))
+    return {"x": x * length, "type": types, "owner": owner, "nlocal": n,
+            "numneigh": np.array(numneigh, dtype=np.int32), "firstneigh": np.concatenate(firstneigh),
+            "ilist": np.arange(n, dtype=np.int32)}
+
+
+def pair_style_entries(dom, pair_cut):
+    """The entries PairHDNNP::transferNeighborList hands to addNeighbor:
+    per local atom, neighbours with d2 <= pair_cut^2 (d2 summed in the pair
+    style's order), as CSR (offset, j, type, dr [E,3], d2)."""
+    x, off, js, dr, d2s = dom["x"], [0], [], [], []
+    start = 0
+    for i in range(dom["nlocal"]):
+        nb = dom["firstneigh"][start:start + dom["numneigh"][i]]
+        start += dom["numneigh"][i]
+        for j in nb:
+            dx, dy, dz = x[i, 0] - x[j, 0], x[i, 1] - x[j, 1], x[i, 2] - x[j, 2]
+            d2 = dx * dx + dy * dy + dz * dz
+            if d2 <= pair_cut * pair_cut:
+                js.append(j)
+                dr.append((dx, dy, dz))
+                d2s.append(d2)
+        off.append(len(js))
+    js = np.array(js, dtype=np.int32)
+    return {"offset": np.array(off, dtype=np.int64), "j": js, "type": dom["type"][js],
+            "dr": np.array(dr, dtype=np.float64).reshape(-1, 3), "d2": np.array(d2s, dtype=np.float64)}
