@@ -41,6 +41,8 @@ STUDENT_SPAN = os.path.join(ROOT, "tests", "golden", "models", "student_water56_
 METRIC = "atoms/s (E+F) on 1×B200: mixed/student vs plain FP64 at ≤1 meV/atom, 30 meV/Å"
 HA_TO_MEV = 27211.386
 HA_BOHR_TO_MEV_A = 27211.386 / 0.529177
+BOHR_TO_A = 0.529177210903
+HA_TO_EV = 27.211386245988
 
 # DRAM bytes (read + write) of the two symmetry-function passes per neighbour
 # entry, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
@@ -68,6 +70,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-student", action="store_true")
     ap.add_argument("--no-large", action="store_true")
+    ap.add_argument("--no-lammps", action="store_true")
     ap.add_argument("--student-boxes", type=int, default=2048)
     return ap.parse_args()
 
@@ -285,6 +288,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_large:
         large = bench_large(args.steps, args.warmup, local)
 
+    # MD steps through the LAMMPS interface (local + ghost atoms, host arrays)
+    lammps = None
+    if rank == 0 and world == 1 and not args.no_lammps:
+        lammps = bench_lammps(args.steps, args.warmup, local, cpu=not args.no_cpu)
+
     # distilled student (with teacher fallback) against the plain FP64 teacher
     stud = None
     if rank == 0 and world == 1 and not args.no_student and os.path.isdir(STUDENT):
@@ -355,7 +363,7 @@ def run_ours(args):
                 "e2e": {"value": world * natoms / (e2e_ms / 1000.0), "unit": "atoms/s", "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": nbytes_pos, "d2h_bytes_per_step": nbytes_pos + 8 * len(structs)},
                 "gpu_launches": launches, "autotune": _shape_names(tune), "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
-                "mixed": mixed, "student": stud, "large_system": large, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
+                "mixed": mixed, "student": stud, "large_system": large, "lammps_interface": lammps, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
                 "fp32_fma_peak_tflops": fp32_peak}
         print(json.dumps(line), flush=True)
     mode.close()
@@ -426,6 +434,118 @@ def bench_large(steps, warmup, device):
                       "split-bfloat16 operands and FP32 accumulators (tensor-pipe utilisation is an ncu counter, "
                       "not measured here)")
     mode.close()
+    return out
+
+
+def lammps_rank(s, list_cut_bohr, type_of):
+    """One LAMMPS rank holding a whole cubic periodic box (Angstrom units):
+    local atoms wrapped into the cell, ghost images within the list cutoff
+    (pair cutoff + skin) outside it, full neighbour lists of the local atoms
+    (ascending j, self excluded).  Returns x [nall,3], type [nall], nlocal,
+    numneigh, firstneigh (flat), ilist."""
+    import itertools
+    from scipy.spatial import cKDTree
+    L = np.diag(np.asarray(s.box, dtype=np.float64))
+    n = s.numAtoms
+    frac = s.positions / L
+    frac -= np.floor(frac)
+    xs, owners = [frac * L], [np.arange(n)]
+    for sh in itertools.product((-1, 0, 1), repeat=3):
+        if sh != (0, 0, 0):
+            f = frac + np.array(sh, dtype=np.float64)
+            keep = np.all((f >= -list_cut_bohr / L) & (f < 1.0 + list_cut_bohr / L), axis=1)
+            xs.append(f[keep] * L)
+            owners.append(np.nonzero(keep)[0])
+    x = np.concatenate(xs)
+    owner = np.concatenate(owners)
+    m = cKDTree(x[:n]).sparse_distance_matrix(cKDTree(x), list_cut_bohr, output_type="coo_matrix")
+    keep = m.row != m.col
+    r, c = m.row[keep], m.col[keep]
+    o = np.lexsort((c, r))
+    r, c = r[o], c[o]
+    types = np.array([type_of[e] for e in s.elements], dtype=np.int32)[owner]
+    return {"x": x * BOHR_TO_A, "type": types, "nlocal": n,
+            "numneigh": np.bincount(r, minlength=n).astype(np.int32), "firstneigh": c.astype(np.int32),
+            "ilist": np.arange(n, dtype=np.int32)}
+
+
+def bench_lammps(steps, warmup, device, cpu=True):
+    """MD steps through the LAMMPS interface (n2p2_lammps_*), as pair_style
+    hdnnp drives it on one rank: 12,288-molecule water box (36,864 local
+    atoms) in Angstrom/eV with its ghost atoms and full neighbour lists
+    (6.5 A pair cutoff + 1 A skin), water56 model.  Each step: setLocalAtoms,
+    neighbour transfer, process, energy, forces on local and ghost atoms; host
+    arrays in and out, wall clock (the interface is synchronous)."""
+    from n2p2_b200 import water
+    from n2p2_b200.lammps import InterfaceLammps
+    pair_cut, skin = 6.5, 1.0
+    cfl, cfe = 1.0 / BOHR_TO_A, 1.0 / HA_TO_EV
+    s = water.water_box(12288, seed=77, sigma=0.1)
+    dom = lammps_rank(s, (pair_cut + skin) / BOHR_TO_A, {"H": 1, "O": 2})
+    n, nall = dom["nlocal"], len(dom["x"])
+    out = {"workload": "LAMMPS-style rank: 12288-molecule water box (%d local + %d ghost atoms, %d list entries), "
+                       "water56, Angstrom/eV, pair cutoff 6.5 A + 1 A skin" % (n, nall - n, len(dom["firstneigh"])),
+           "unit": "atoms/s"}
+    F = np.zeros((nall, 3))
+    for prec in ("fp64", "mixed"):
+        lmp = InterfaceLammps(device).initialize(TEACHER, "1:H,2:O", False, False, 0, -1, cfl, cfe, pair_cut, 2, 0)
+        lmp.setPrecision(prec)
+        t_tr = t_pr = t_f = 0.0
+        for k in range(warmup + steps):
+            t0 = time.perf_counter()
+            lmp.setLocalAtoms(n, dom["type"][:n])
+            lmp.transferNeighborList(dom["ilist"], dom["numneigh"], dom["firstneigh"], dom["x"], dom["type"], pair_cut)
+            t1 = time.perf_counter()
+            lmp.process()
+            lmp.getEnergy()
+            t2 = time.perf_counter()
+            F[:] = 0.0
+            lmp.getForces(F)
+            t3 = time.perf_counter()
+            if k >= warmup:
+                t_tr += t1 - t0
+                t_pr += t2 - t1
+                t_f += t3 - t2
+        ms = 1e3 * (t_tr + t_pr + t_f) / steps
+        out[prec] = {"value": n / (ms / 1e3), "ms_per_step": ms,
+                     "host_ms": {"transfer_neighbor_list": 1e3 * t_tr / steps,
+                                 "process_and_energy": 1e3 * t_pr / steps, "get_forces": 1e3 * t_f / steps}}
+        lmp.close()
+    if cpu:
+        # the reference's own InterfaceLammps (timed build, one host thread) on
+        # a 1,536-atom rank of the same recipe
+        try:
+            from oracle import lammps_ref
+            small = water.water_box(512, seed=78, sigma=0.1)
+            d2 = lammps_rank(small, (pair_cut + skin) / BOHR_TO_A, {"H": 1, "O": 2})
+            ref = lammps_ref.RefInterfaceLammps(TEACHER, "1:H,2:O", cfl, cfe, pair_cut, 2, fast=True)
+            x = d2["x"]
+            offs, js, drs, d2s = [0], [], [], []
+            start = 0
+            for i in range(d2["nlocal"]):
+                nb = d2["firstneigh"][start:start + d2["numneigh"][i]]
+                start += d2["numneigh"][i]
+                dr = x[i] - x[nb]
+                q = dr[:, 0] * dr[:, 0] + dr[:, 1] * dr[:, 1] + dr[:, 2] * dr[:, 2]
+                sel = q <= pair_cut * pair_cut
+                js.append(nb[sel])
+                drs.append(dr[sel])
+                d2s.append(q[sel])
+                offs.append(offs[-1] + int(sel.sum()))
+            js = np.concatenate(js)
+            args = (d2["type"][:d2["nlocal"]], np.array(offs), js, d2["type"][js], np.concatenate(drs),
+                    np.concatenate(d2s), len(x))
+            ref.evaluate(*args, num_centres=0)
+            t0 = time.perf_counter()
+            ref.evaluate(*args, num_centres=0)
+            sec = time.perf_counter() - t0
+            ref.close()
+            out["cpu_reference"] = {"value": d2["nlocal"] / sec, "unit": "atoms/s", "cores": 1, "kind": "reference",
+                                    "sample": "reference InterfaceLammps (libnnp -O3, x86-64-v3), setLocalAtoms + "
+                                              "addNeighbor + process + getForces on a %d-atom rank, one thread"
+                                              % d2["nlocal"]}
+        except Exception as exc:   # the GPU numbers stand without it
+            out["cpu_reference"] = {"value": None, "sample": "failed: %s" % exc}
     return out
 
 

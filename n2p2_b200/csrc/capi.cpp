@@ -855,8 +855,10 @@ n2p2_status n2p2_lammps_transfer_neighbor_list(n2p2_lammps* lammps, int32_t inum
         N2P2_REQUIRE(x);
         N2P2_REQUIRE(type);
     }
-    return guard(
-        [&] { lammps->iface.transferNeighborList(inum, ilist, numneigh, firstneigh, x, type, maxCutoffRadius); });
+    return guard([&] {
+        setDevice(&lammps->mode);   // the staging is page-locked host memory
+        lammps->iface.transferNeighborList(inum, ilist, numneigh, firstneigh, x, type, maxCutoffRadius);
+    });
 }
 
 n2p2_status n2p2_lammps_process(n2p2_lammps* lammps)

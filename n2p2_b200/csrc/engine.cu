@@ -657,14 +657,22 @@ void Batch::uploadElementLists()
     v_.elemAtoms = dev;
 }
 
-void Batch::setExternalNeighbors(int numCenters, const int* elements, int64_t numEntries, const int64_t* offsets,
-                                 int numTargets, const int* target, const int* targetElement, const double* dr,
-                                 const double* d, const int* centerTarget)
+// Shared part of both external forms: one system of `numCenters` atoms,
+// its element lists and the buffers of the transposed lists.
+void Batch::beginExternal(int numCenters, const int* elements, int numTargets, const int* centerTarget,
+                          int64_t capacity)
 {
     if (numCenters <= 0) throw std::runtime_error("ERROR: no local atoms.\n");
-    if (numEntries < 0 || offsets[0] != 0 || offsets[numCenters] != numEntries)
-        throw std::invalid_argument("ERROR: neighbour offsets do not match the entry count.\n");
     const int ne = (int)model_.numElements();
+    std::vector<char> seen((size_t)std::max(numTargets, 1), 0);
+    for (int a = 0; a < numCenters; ++a)
+    {
+        const int k = centerTarget[a];
+        if (k < 0 || k >= numTargets || seen[k])
+            throw std::invalid_argument("ERROR: local atom indices must be distinct and below the atom count.\n");
+        seen[k] = 1;
+        if (elements[a] < 0 || elements[a] >= ne) throw std::runtime_error("ERROR: element index out of range.\n");
+    }
     // Everything but the candidate-mask buffer is released: a caller that
     // sets new lists every step (an MD code) keeps masks of the last size.
     releaseGraph();
@@ -680,47 +688,12 @@ void Batch::setExternalNeighbors(int numCenters, const int* elements, int64_t nu
     structBegin_ = {0, N_};
     elemHost_.assign(elements, elements + N_);
     numAtomsPerElement_.assign((size_t)ne, 0);
-    for (int a = 0; a < N_; ++a)
-    {
-        if (elemHost_[a] < 0 || elemHost_[a] >= ne) throw std::runtime_error("ERROR: element index out of range.\n");
-        numAtomsPerElement_[elemHost_[a]]++;
-    }
+    for (int a = 0; a < N_; ++a) numAtomsPerElement_[elemHost_[a]]++;
     numTargets_ = numTargets;
-    std::vector<int> targetCenter(std::max(numTargets, 1), -1);
-    for (int a = 0; a < N_; ++a)
-    {
-        const int k = centerTarget[a];
-        if (k < 0 || k >= numTargets || targetCenter[k] >= 0)
-            throw std::invalid_argument("ERROR: local atom indices must be distinct and below the atom count.\n");
-        targetCenter[k] = a;
-    }
-    const double rcmax = model_.maxCutoffRadius;
-    std::vector<int64_t> tCount((size_t)numTargets + 1, 0);
-    for (int a = 0; a < N_; ++a)
-    {
-        if (offsets[a + 1] < offsets[a] || offsets[a + 1] - offsets[a] > 1024)
-            throw std::runtime_error("ERROR: more than 1024 neighbours of one atom.\n");
-        for (int64_t e = offsets[a]; e < offsets[a + 1]; ++e)
-        {
-            if (target[e] < 0 || target[e] >= numTargets)
-                throw std::invalid_argument("ERROR: neighbour index out of range.\n");
-            if (targetElement[e] < 0 || targetElement[e] >= ne)
-                throw std::runtime_error("ERROR: element index out of range.\n");
-            if (!(d[e] <= rcmax)) throw std::invalid_argument("ERROR: neighbour beyond the largest cutoff.\n");
-            tCount[(size_t)target[e] + 1]++;
-        }
-    }
-    // transposed lists: for each target the entries naming it, in entry order
-    for (int k = 0; k < numTargets; ++k) tCount[(size_t)k + 1] += tCount[k];
-    std::vector<int64_t> tEntry((size_t)std::max<int64_t>(numEntries, 1));
-    {
-        std::vector<int64_t> fill(tCount.begin(), tCount.end() - 1);
-        for (int64_t e = 0; e < numEntries; ++e) tEntry[(size_t)fill[target[e]]++] = e;
-    }
     allocateAtoms();
     uploadElementLists();
     v_.numCells = 0;
-    v_.scanTmp = devAlloc<int64_t>(pool_, scanTileCount(N_) + 8, owned_);   // the candidate-mask offsets' scan
+    v_.scanTmp = devAlloc<int64_t>(pool_, scanTileCount(N_) + 8, owned_);   // entry offsets, candidate masks
     std::vector<DevStructInfo> info(1);
     std::memset(info.data(), 0, sizeof(DevStructInfo));
     info[0].numAtoms = N_;
@@ -731,7 +704,48 @@ void Batch::setExternalNeighbors(int numCenters, const int* elements, int64_t nu
               "upload elements");
     cudaCheck(cudaMemcpyAsync(structBeginDev_, structBegin_.data(), sizeof(int) * 2, cudaMemcpyHostToDevice, stream_),
               "upload offsets");
-    allocateNeighbors(std::max<int64_t>(numEntries, 1));
+    allocateNeighbors(std::max<int64_t>(capacity, 1));
+    const size_t T = (size_t)std::max(numTargets, 1);
+    tCount_ = devAlloc<int>(pool_, T, ownedNbr_);
+    tFill_ = devAlloc<int>(pool_, T, ownedNbr_);
+    tOffset_ = devAlloc<int64_t>(pool_, T + 1, ownedNbr_);
+    tEntryTmp_ = devAlloc<int64_t>(pool_, (size_t)capacity_, ownedNbr_);
+    tEntry_ = devAlloc<int64_t>(pool_, (size_t)capacity_, ownedNbr_);
+    targetCenter_ = devAlloc<int>(pool_, T, ownedNbr_);
+    centerIndex_ = devAlloc<int>(pool_, (size_t)N_, ownedNbr_);
+    tScanTmp_ = devAlloc<int64_t>(pool_, scanTileCount((int)T) + 8, ownedNbr_);
+    Ftarget_ = devAlloc<double>(pool_, 3 * T, ownedNbr_);
+    entriesDev_ = devAlloc<int64_t>(pool_, 1, ownedNbr_);
+    cudaCheck(cudaMemcpyAsync(centerIndex_, centerTarget, sizeof(int) * (size_t)N_, cudaMemcpyHostToDevice, stream_),
+              "upload centre indices");
+    cudaCheck(cudaMemsetAsync(Ftarget_, 0, sizeof(double) * 3 * T, stream_), "memset");
+    capacityVerified_ = false;
+    tuned_[0] = tuned_[1] = false;
+}
+
+void Batch::setExternalNeighbors(int numCenters, const int* elements, int64_t numEntries, const int64_t* offsets,
+                                 int numTargets, const int* target, const int* targetElement, const double* dr,
+                                 const double* d, const int* centerTarget)
+{
+    if (numEntries < 0 || offsets[0] != 0 || offsets[numCenters] != numEntries)
+        throw std::invalid_argument("ERROR: neighbour offsets do not match the entry count.\n");
+    const int ne = (int)model_.numElements();
+    const double rcmax = model_.maxCutoffRadius;
+    for (int a = 0; a < numCenters; ++a)
+    {
+        if (offsets[a + 1] < offsets[a] || offsets[a + 1] - offsets[a] > 1024)
+            throw std::runtime_error("ERROR: more than 1024 neighbours of one atom.\n");
+        for (int64_t e = offsets[a]; e < offsets[a + 1]; ++e)
+        {
+            if (target[e] < 0 || target[e] >= numTargets)
+                throw std::invalid_argument("ERROR: neighbour index out of range.\n");
+            if (targetElement[e] < 0 || targetElement[e] >= ne)
+                throw std::runtime_error("ERROR: element index out of range.\n");
+            if (!(d[e] <= rcmax)) throw std::invalid_argument("ERROR: neighbour beyond the largest cutoff.\n");
+        }
+    }
+    beginExternal(numCenters, elements, numTargets, centerTarget, std::max<int64_t>(numEntries, 1));
+    extRaw_ = false;
     const size_t E = (size_t)numEntries;
     std::vector<uint8_t> el(std::max<size_t>(E, 1));
     std::vector<double> dx(std::max<size_t>(E, 1)), dy(dx.size()), dz(dx.size());
@@ -752,19 +766,48 @@ void Batch::setExternalNeighbors(int numCenters, const int* elements, int64_t nu
     up(v_.nbrDx, dx.data(), sizeof(double) * E, "upload dr");
     up(v_.nbrDy, dy.data(), sizeof(double) * E, "upload dr");
     up(v_.nbrDz, dz.data(), sizeof(double) * E, "upload dr");
-    tOffset_ = devAlloc<int64_t>(pool_, (size_t)numTargets + 1, ownedNbr_);
-    tEntry_ = devAlloc<int64_t>(pool_, tEntry.size(), ownedNbr_);
-    targetCenter_ = devAlloc<int>(pool_, targetCenter.size(), ownedNbr_);
-    entriesDev_ = devAlloc<int64_t>(pool_, 1, ownedNbr_);
     up(entriesDev_, &numEntries, sizeof(int64_t), "upload entry count");
-    Ftarget_ = devAlloc<double>(pool_, 3 * (size_t)std::max(numTargets, 1), ownedNbr_);
-    up(tOffset_, tCount.data(), sizeof(int64_t) * ((size_t)numTargets + 1), "upload transposed offsets");
-    up(tEntry_, tEntry.data(), sizeof(int64_t) * E, "upload transposed entries");
-    up(targetCenter_, targetCenter.data(), sizeof(int) * targetCenter.size(), "upload centre map");
-    cudaCheck(cudaMemsetAsync(Ftarget_, 0, sizeof(double) * 3 * (size_t)std::max(numTargets, 1), stream_), "memset");
     cudaCheck(cudaStreamSynchronize(stream_), "setExternalNeighbors");   // host staging vectors go out of scope
-    capacityVerified_ = false;
-    tuned_[0] = tuned_[1] = false;
+}
+
+void Batch::setExternalLists(ExternalLists const& l)
+{
+    if (l.numCenters <= 0) throw std::runtime_error("ERROR: no local atoms.\n");
+    if (l.candOffset[0] != 0 || l.candOffset[l.numCenters] != l.numCand)
+        throw std::invalid_argument("ERROR: candidate offsets do not match the candidate count.\n");
+    for (int c = 0; c < l.numCenters; ++c)
+        if (l.candOffset[c + 1] < l.candOffset[c]) throw std::invalid_argument("ERROR: decreasing candidate offsets.\n");
+    if (l.numTypes < 0 || l.numAll <= 0) throw std::invalid_argument("ERROR: no atoms or types.\n");
+    // entries are a subset of the candidates: the candidate count bounds them
+    beginExternal(l.numCenters, l.centerElement, l.numAll, l.centerIndex, std::max<int64_t>(l.numCand, 1));
+    extRaw_ = true;
+    double* x = devAlloc<double>(pool_, 3 * (size_t)l.numAll, ownedNbr_);
+    int* type = devAlloc<int>(pool_, (size_t)l.numAll, ownedNbr_);
+    int* typeElement = devAlloc<int>(pool_, (size_t)l.numTypes + 1, ownedNbr_);
+    int64_t* candOffset = devAlloc<int64_t>(pool_, (size_t)l.numCenters + 1, ownedNbr_);
+    int* cand = devAlloc<int>(pool_, (size_t)std::max<int64_t>(l.numCand, 1), ownedNbr_);
+    auto up = [&](void* dst, const void* src, size_t bytes, char const* what) {
+        if (bytes) cudaCheck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), what);
+    };
+    up(x, l.x, sizeof(double) * 3 * (size_t)l.numAll, "upload positions");
+    up(type, l.type, sizeof(int) * (size_t)l.numAll, "upload types");
+    up(typeElement, l.typeElement, sizeof(int) * ((size_t)l.numTypes + 1), "upload type map");
+    up(candOffset, l.candOffset, sizeof(int64_t) * ((size_t)l.numCenters + 1), "upload candidate offsets");
+    up(cand, l.cand, sizeof(int) * (size_t)l.numCand, "upload candidates");
+    raw_ = ExtRawView{};
+    raw_.x = x;
+    raw_.type = type;
+    raw_.typeElement = typeElement;
+    raw_.numTypes = l.numTypes;
+    raw_.numAll = l.numAll;
+    raw_.centerIndex = centerIndex_;
+    raw_.candOffset = candOffset;
+    raw_.cand = cand;
+    raw_.cflength = l.cflength;
+    raw_.convLength = l.convLength;
+    raw_.normalize = l.normalize ? 1 : 0;
+    raw_.pairCut2 = l.pairCut2;
+    raw_.rcmax = model_.maxCutoffRadius;
 }
 
 void Batch::targetForces(double* out)
@@ -893,10 +936,22 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
     };
     mark("start");
     cudaCheck(cudaMemsetAsync(v_.status, 0, sizeof(DevStatus), stream_), "status reset");
-    if (external_)   // the entry count the neighbour build would report (read by the cutoff stage)
-        cudaCheck(cudaMemcpyAsync(&v_.status->totalNeighbors, entriesDev_, sizeof(int64_t), cudaMemcpyDeviceToDevice,
-                                  stream_),
-                  "entry count");
+    if (external_)
+    {
+        if (extRaw_)
+        {
+            launchExternalEntries(raw_, v_, v_.scanTmp, sms_, stream_);
+            launches += 5;
+        }
+        else   // the entry count the neighbour build would report (read by the cutoff stage)
+            cudaCheck(cudaMemcpyAsync(&v_.status->totalNeighbors, entriesDev_, sizeof(int64_t),
+                                      cudaMemcpyDeviceToDevice, stream_),
+                      "entry count");
+        launchExternalTranspose(v_, numTargets_, centerIndex_, tCount_, tFill_, tOffset_, tEntryTmp_, tEntry_,
+                                targetCenter_, tScanTmp_, sms_, stream_);
+        launches += 7;
+        mark("neighbor_list");
+    }
     else
     {
         launchPreparePositions(v_, rin_, remap_, model_.normalize ? 1 : 0, model_.convLength, stream_);

@@ -106,6 +106,29 @@ public:
     void setExternalNeighbors(int numCenters, const int* elements, int64_t numEntries, const int64_t* offsets,
                               int numTargets, const int* target, const int* targetElement, const double* dr,
                               const double* d, const int* centerTarget);
+    // The same from an MD code's own full neighbour lists (positions and
+    // types of all its atoms, candidates per centre): the entries are built
+    // on the device (k_external.cu).  The host arrays are read by
+    // asynchronous copies: keep them unchanged until the next call that
+    // synchronises (evaluate's results, targetForces).
+    struct ExternalLists
+    {
+        int numCenters = 0;
+        const int* centerElement = nullptr;   // [numCenters]
+        const int* centerIndex = nullptr;     // [numCenters] index among all atoms
+        const int64_t* candOffset = nullptr;  // [numCenters + 1]
+        const int* cand = nullptr;            // [numCand] indices among all atoms
+        int64_t numCand = 0;
+        int numAll = 0;
+        const double* x = nullptr;            // [numAll][3], the MD code's units
+        const int* type = nullptr;            // [numAll], 1-based
+        const int* typeElement = nullptr;     // [numTypes + 1], -1 = ignored
+        int numTypes = 0;
+        double cflength = 1.0, convLength = 1.0;
+        bool normalize = false;
+        double pairCut2 = 0.0;
+    };
+    void setExternalLists(ExternalLists const& lists);
     bool external() const { return external_; }
     int numTargets() const { return numTargets_; }
     void targetForces(double* out);   // [numTargets][3], internal units (synchronises)
@@ -220,13 +243,21 @@ private:
     int64_t maskCap_ = 0;
     void uploadElementLists();
     // external neighbour lists
+    void beginExternal(int numCenters, const int* elements, int numTargets, const int* centerTarget, int64_t capacity);
     bool external_ = false;
+    bool extRaw_ = false;           // entries built on the device from raw lists (raw_)
+    ExtRawView raw_{};
     int numTargets_ = 0;
-    int64_t* tOffset_ = nullptr;   // [numTargets + 1] entries naming each target ...
-    int64_t* tEntry_ = nullptr;    // ... in entry order
-    int* targetCenter_ = nullptr;  // [numTargets] centre index or -1
-    double* Ftarget_ = nullptr;    // [numTargets][3]
-    int64_t* entriesDev_ = nullptr;   // the entry count, copied into the status by every evaluation
+    int* tCount_ = nullptr;         // [numTargets] entries naming each target
+    int* tFill_ = nullptr;
+    int64_t* tOffset_ = nullptr;    // [numTargets + 1]
+    int64_t* tEntryTmp_ = nullptr;  // [capacity]
+    int64_t* tEntry_ = nullptr;     // [capacity] per target, in entry order
+    int* targetCenter_ = nullptr;   // [numTargets] centre index or -1
+    int* centerIndex_ = nullptr;    // [N] each centre's index among the targets
+    int64_t* tScanTmp_ = nullptr;
+    double* Ftarget_ = nullptr;     // [numTargets][3]
+    int64_t* entriesDev_ = nullptr; // host-built entries: their count, copied into the status by every evaluation
 };
 
 } // namespace n2p2b200

@@ -122,6 +122,34 @@ void launchEnergySum(BatchView const& b, cudaStream_t st);
 void launchGatherForces(BatchView const& b, int sms, cudaStream_t st);
 void launchGatherTargets(BatchView const& b, int numTargets, const int64_t* tOffset, const int64_t* tEntry,
                          const int* targetCenter, double* F, int sms, cudaStream_t st);
+
+// An MD code's own neighbour lists on the device (k_external.cu): positions
+// and types of all its atoms (local and ghost, its units), per centre the
+// candidate neighbours (its indices), the type -> element map (-1: ignored)
+// and the unit handling of InterfaceLammps::addNeighbor.
+struct ExtRawView
+{
+    const double* x = nullptr;          // [numAll][3]
+    const int* type = nullptr;          // [numAll], 1-based types
+    const int* typeElement = nullptr;   // [numTypes + 1]
+    int numTypes = 0;
+    int numAll = 0;
+    const int* centerIndex = nullptr;   // [N] the centre's own index among all atoms
+    const int64_t* candOffset = nullptr;   // [N + 1]
+    const int* cand = nullptr;
+    double cflength = 1.0, convLength = 1.0;
+    int normalize = 0;
+    double pairCut2 = 0.0;              // the pair style's cutoff squared (its units)
+    double rcmax = 0.0;                 // the model's largest cutoff (internal units)
+};
+// Entries of every centre (count, scan into nbrOffset and the status's
+// entry count, fill).
+void launchExternalEntries(ExtRawView const& r, BatchView const& b, int64_t* scanTmp, int sms, cudaStream_t st);
+// Transposed lists of the entries (per target, entry order) and the
+// target -> centre map.
+void launchExternalTranspose(BatchView const& b, int numTargets, const int* centerIndex, int* tCount, int* tFill,
+                             int64_t* tOffset, int64_t* tEntryTmp, int64_t* tEntry, int* targetCenter,
+                             int64_t* scanTmp, int sms, cudaStream_t st);
 void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 
 // neighbour list of one structure into caller buffers, no device allocation

@@ -89,7 +89,13 @@ void LammpsInterface::initialize(Model const& model, std::string const& emap, do
         }
     }
     ignoreType_.assign((size_t)std::max(lammpsNtypes, 0) + 1, true);
-    for (int t = 1; t <= lammpsNtypes; ++t) ignoreType_[t] = typeToElement_.find(t) == typeToElement_.end();
+    typeElement_.assign((size_t)std::max(lammpsNtypes, 0) + 1, -1);
+    for (int t = 1; t <= lammpsNtypes; ++t)
+    {
+        auto it = typeToElement_.find(t);
+        ignoreType_[t] = it == typeToElement_.end();
+        if (!ignoreType_[t]) typeElement_[t] = it->second;
+    }
     indexMap_.clear();
     center_.clear();
     dirty_ = true;
@@ -117,11 +123,13 @@ void LammpsInterface::setLocalAtoms(int numAtomsLocal, const int* atomType)
         center_.push_back(i);
         centerElement_.push_back(typeToElement_.at(t));
     }
-    const size_t n = center_.size();
-    nbrJ_.assign(n, {});
-    nbrElem_.assign(n, {});
-    nbrDr_.assign(n, {});
-    nbrD_.assign(n, {});
+    lists_ = LISTS_NONE;
+    eCenter_.clear();
+    eJ_.clear();
+    eElem_.clear();
+    eDr_.clear();
+    eD_.clear();
+    eOrdered_ = true;
     dirty_ = true;
     haveAtomic_ = false;
 }
@@ -131,6 +139,10 @@ void LammpsInterface::addNeighbor(int i, int j, int type, double dx, double dy, 
     if (i < 0 || i >= (int)indexMap_.size()) throw std::out_of_range("ERROR: local atom index out of range.\n");
     if (j < 0) throw std::out_of_range("ERROR: negative neighbour index.\n");
     if (type < 1 || type >= (int)ignoreType_.size()) throw std::out_of_range("ERROR: LAMMPS atom type out of range.\n");
+    if (lists_ == LISTS_TRANSFERRED)
+        throw std::runtime_error("ERROR: this step's lists were transferred in one call; addNeighbor does not "
+                                 "extend them.\n");
+    lists_ = LISTS_ADDED;
     if (ignoreType_[type] || indexMap_[i] < 0) return;
     // unit conversion in the order of InterfaceLammps::addNeighbor
     double rx = dx * cflength_, ry = dy * cflength_, rz = dz * cflength_;
@@ -146,33 +158,93 @@ void LammpsInterface::addNeighbor(int i, int j, int type, double dx, double dy, 
     // beyond the largest cutoff contributes nothing
     if (!(d <= rcmax_)) return;
     const int c = indexMap_[i];
-    nbrJ_[c].push_back(j);
-    nbrElem_[c].push_back(typeToElement_.at(type));
-    nbrDr_[c].push_back(rx);
-    nbrDr_[c].push_back(ry);
-    nbrDr_[c].push_back(rz);
-    nbrD_[c].push_back(d);
+    if (!eCenter_.empty() && c < eCenter_.back()) eOrdered_ = false;
+    eCenter_.push_back(c);
+    eJ_.push_back(j);
+    eElem_.push_back(typeElement_[type]);
+    eDr_.push_back(rx);
+    eDr_.push_back(ry);
+    eDr_.push_back(rz);
+    eD_.push_back(d);
     dirty_ = true;
 }
+
+void* LammpsInterface::Pinned::ensure(size_t n)
+{
+    if (n > bytes)
+    {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        const size_t want = n + n / 4 + 4096;
+        cudaCheck(cudaHostAlloc(&p, want, cudaHostAllocPortable), "cudaHostAlloc");
+        bytes = want;
+    }
+    return p;
+}
+
+LammpsInterface::Pinned::~Pinned()
+{
+    if (p) cudaFreeHost(p);
+}
+
+LammpsInterface::~LammpsInterface() = default;
 
 void LammpsInterface::transferNeighborList(int inum, const int* ilist, const int* numneigh,
                                            const int* const* firstneigh, const double* const* x, const int* type,
                                            double pairCutoff)
 {
-    const double rc2 = pairCutoff * pairCutoff;
+    if (!initialized_) throw std::runtime_error("ERROR: the LAMMPS interface is not initialized.\n");
+    if (lists_ != LISTS_NONE)
+        throw std::runtime_error("ERROR: this step already has neighbours (set the local atoms again first).\n");
+    const int nLocal = (int)indexMap_.size();
+    std::vector<char> listed((size_t)nLocal, 0);
     for (int ii = 0; ii < inum; ++ii)
     {
         const int i = ilist[ii];
-        for (int jj = 0; jj < numneigh[i]; ++jj)
-        {
-            const int j = firstneigh[i][jj] & kNeighMask;
-            const double dx = x[i][0] - x[j][0];
-            const double dy = x[i][1] - x[j][1];
-            const double dz = x[i][2] - x[j][2];
-            const double d2 = dx * dx + dy * dy + dz * dz;
-            if (d2 <= rc2) addNeighbor(i, j, type[j], dx, dy, dz, d2);
-        }
+        if (i < 0 || i >= nLocal) throw std::out_of_range("ERROR: local atom index out of range.\n");
+        listed[i] = 1;
     }
+    // candidates of every centre, in centre order, special-bond bits masked
+    const int n = (int)center_.size();
+    int64_t total = 0;
+    for (int c = 0; c < n; ++c)
+        if (listed[center_[c]]) total += numneigh[center_[c]];
+    auto* off = static_cast<int64_t*>(candOffBuf_.ensure(sizeof(int64_t) * ((size_t)n + 1)));
+    auto* cand = static_cast<int*>(candBuf_.ensure(sizeof(int) * (size_t)std::max<int64_t>(total, 1)));
+    int maxIndex = 0;
+    int64_t at = 0;
+    off[0] = 0;
+    for (int c = 0; c < n; ++c)
+    {
+        const int i = center_[c];
+        maxIndex = std::max(maxIndex, i);
+        if (listed[i])
+        {
+            const int* nb = firstneigh[i];
+            for (int q = 0; q < numneigh[i]; ++q)
+            {
+                const int j = nb[q] & kNeighMask;
+                cand[at++] = j;
+                maxIndex = std::max(maxIndex, j);
+            }
+        }
+        off[c + 1] = at;
+    }
+    numCand_ = at;
+    numAll_ = maxIndex + 1;
+    auto* xs = static_cast<double*>(xBuf_.ensure(sizeof(double) * 3 * (size_t)numAll_));
+    auto* ts = static_cast<int*>(typeBuf_.ensure(sizeof(int) * (size_t)numAll_));
+    for (int k = 0; k < numAll_; ++k)
+    {
+        xs[3 * (size_t)k + 0] = x[k][0];
+        xs[3 * (size_t)k + 1] = x[k][1];
+        xs[3 * (size_t)k + 2] = x[k][2];
+        ts[k] = type[k];
+    }
+    pairCut2_ = pairCutoff * pairCutoff;
+    lists_ = LISTS_TRANSFERRED;
+    dirty_ = true;
 }
 
 void LammpsInterface::process(Batch& batch, int precision, bool checkExtrapolation)
@@ -187,27 +259,52 @@ void LammpsInterface::process(Batch& batch, int precision, bool checkExtrapolati
     if (dirty_)
     {
         const int n = (int)center_.size();
-        std::vector<int64_t> offsets((size_t)n + 1, 0);
-        for (int c = 0; c < n; ++c) offsets[c + 1] = offsets[c] + (int64_t)nbrJ_[c].size();
-        const size_t E = (size_t)offsets[n];
-        std::vector<int> target(std::max<size_t>(E, 1)), elem(std::max<size_t>(E, 1));
-        std::vector<double> dr(3 * std::max<size_t>(E, 1)), d(std::max<size_t>(E, 1));
-        int numTargets = 0;
-        for (int c = 0; c < n; ++c)
+        if (lists_ == LISTS_TRANSFERRED)
         {
-            numTargets = std::max(numTargets, center_[c] + 1);
-            size_t e0 = (size_t)offsets[c];
-            for (size_t q = 0; q < nbrJ_[c].size(); ++q)
-            {
-                target[e0 + q] = nbrJ_[c][q];
-                elem[e0 + q] = nbrElem_[c][q];
-                d[e0 + q] = nbrD_[c][q];
-                for (int k = 0; k < 3; ++k) dr[3 * (e0 + q) + k] = nbrDr_[c][3 * q + k];
-                numTargets = std::max(numTargets, nbrJ_[c][q] + 1);
-            }
+            Batch::ExternalLists l;
+            l.numCenters = n;
+            l.centerElement = centerElement_.data();
+            l.centerIndex = center_.data();
+            l.candOffset = static_cast<const int64_t*>(candOffBuf_.p);
+            l.cand = static_cast<const int*>(candBuf_.p);
+            l.numCand = numCand_;
+            l.numAll = numAll_;
+            l.x = static_cast<const double*>(xBuf_.p);
+            l.type = static_cast<const int*>(typeBuf_.p);
+            l.typeElement = typeElement_.data();
+            l.numTypes = (int)typeElement_.size() - 1;
+            l.cflength = cflength_;
+            l.convLength = convLength_;
+            l.normalize = normalize_;
+            l.pairCut2 = pairCut2_;
+            batch.setExternalLists(l);
         }
-        batch.setExternalNeighbors(n, centerElement_.data(), (int64_t)E, offsets.data(), numTargets, target.data(),
-                                   elem.data(), dr.data(), d.data(), center_.data());
+        else
+        {
+            // addNeighbor entries (or none): centre-major CSR, call order within a centre
+            const size_t E = eCenter_.size();
+            std::vector<int64_t> offsets((size_t)n + 1, 0);
+            for (size_t e = 0; e < E; ++e) offsets[(size_t)eCenter_[e] + 1]++;
+            for (int c = 0; c < n; ++c) offsets[c + 1] += offsets[c];
+            std::vector<int> target(std::max<size_t>(E, 1)), elem(std::max<size_t>(E, 1));
+            std::vector<double> dr(3 * std::max<size_t>(E, 1)), d(std::max<size_t>(E, 1));
+            std::vector<int64_t> fill(offsets.begin(), offsets.end() - 1);
+            int numTargets = 0;
+            for (int c = 0; c < n; ++c) numTargets = std::max(numTargets, center_[c] + 1);
+            for (size_t e = 0; e < E; ++e)
+            {
+                const size_t at = eOrdered_ ? e : (size_t)fill[eCenter_[e]]++;
+                target[at] = eJ_[e];
+                elem[at] = eElem_[e];
+                d[at] = eD_[e];
+                dr[3 * at + 0] = eDr_[3 * e + 0];
+                dr[3 * at + 1] = eDr_[3 * e + 1];
+                dr[3 * at + 2] = eDr_[3 * e + 2];
+                numTargets = std::max(numTargets, eJ_[e] + 1);
+            }
+            batch.setExternalNeighbors(n, centerElement_.data(), (int64_t)E, offsets.data(), numTargets,
+                                       target.data(), elem.data(), dr.data(), d.data(), center_.data());
+        }
         dirty_ = false;
     }
     batch.evaluate(EVAL_FORCES, precision, checkExtrapolation ? 1 : 0);

@@ -36,6 +36,9 @@ public:
     void addNeighbor(int i, int j, int type, double dx, double dy, double dz, double d2);
     // PairHDNNP::transferNeighborList (pair_hdnnp.cpp:274-290) in one call:
     // every neighbour within the pair style's cutoff of every listed atom.
+    // The raw lists (candidates, positions and types of the atoms they
+    // name) are staged in pinned memory and filtered on the device; one step
+    // uses either this or addNeighbor.
     void transferNeighborList(int inum, const int* ilist, const int* numneigh, const int* const* firstneigh,
                               const double* const* x, const int* type, double pairCutoff);
 
@@ -51,7 +54,20 @@ public:
     void addForces(Batch& batch, double* const* atomF);
     int numCenters() const { return (int)center_.size(); }
 
+    LammpsInterface() = default;
+    LammpsInterface(LammpsInterface const&) = delete;
+    LammpsInterface& operator=(LammpsInterface const&) = delete;
+    ~LammpsInterface();
+
 private:
+    // page-locked host staging (grown on demand)
+    struct Pinned
+    {
+        void* p = nullptr;
+        size_t bytes = 0;
+        void* ensure(size_t n);
+        ~Pinned();
+    };
     bool initialized_ = false;
     double cflength_ = 1.0, cfenergy_ = 1.0;
     double convLength_ = 1.0, convEnergy_ = 1.0, meanEnergy_ = 0.0;
@@ -61,12 +77,21 @@ private:
     std::map<int, int> typeToElement_;
     std::vector<bool> ignoreType_;   // [type], 1-based
     std::vector<double> offsets_;    // atomic energy offset per element
+    std::vector<int> typeElement_;   // [type] element or -1 (ignored), type 0 unused
     // local atoms and their lists (staged)
     std::vector<int> indexMap_;      // LAMMPS local index -> centre, -1 if ignored
     std::vector<int> center_;        // centre -> LAMMPS local index
     std::vector<int> centerElement_;
-    std::vector<std::vector<int>> nbrJ_, nbrElem_;
-    std::vector<std::vector<double>> nbrDr_, nbrD_;
+    enum { LISTS_NONE, LISTS_ADDED, LISTS_TRANSFERRED } lists_ = LISTS_NONE;
+    // addNeighbor: entries in call order
+    std::vector<int> eCenter_, eJ_, eElem_;
+    std::vector<double> eDr_, eD_;
+    bool eOrdered_ = true;           // centres of the entries never decrease
+    // transferNeighborList: candidates per centre and the atoms they name
+    Pinned candBuf_, candOffBuf_, xBuf_, typeBuf_;
+    int64_t numCand_ = 0;
+    int numAll_ = 0;
+    double pairCut2_ = 0.0;
     bool dirty_ = true;
     double energy_ = 0.0;            // physical units of the model, offsets included
     std::vector<double> atomicEnergy_;

@@ -24,11 +24,15 @@ from ._lib import check
 _P = ctypes.POINTER
 
 
+def _pointers(base, offsets):
+    """A C array of pointers base + offsets[k] (bytes), built without a Python loop."""
+    addr = (np.uint64(base) + np.asarray(offsets, dtype=np.uint64)) if len(offsets) else np.zeros(1, np.uint64)
+    return (ctypes.c_void_p * len(addr)).from_buffer_copy(np.ascontiguousarray(addr, dtype=np.uint64).tobytes())
+
+
 def _rows(a):
     """LAMMPS-style row pointers (double**) into a C-contiguous [n][3] array."""
-    base = a.ctypes.data
-    step = a.strides[0]
-    return (ctypes.c_void_p * max(len(a), 1))(*[base + k * step for k in range(len(a))])
+    return _pointers(a.ctypes.data, np.arange(len(a), dtype=np.uint64) * np.uint64(a.strides[0]))
 
 
 class InterfaceLammps:
@@ -87,8 +91,8 @@ class InterfaceLammps:
         else:
             flat = np.ascontiguousarray(np.concatenate([np.asarray(a, dtype=np.int32) for a in firstneigh])
                                         if len(firstneigh) else np.zeros(0, dtype=np.int32))
-        starts = np.concatenate([[0], np.cumsum(nn)[:-1]]) if nn.size else np.zeros(0, dtype=np.int64)
-        fn = (ctypes.c_void_p * max(nn.size, 1))(*[flat.ctypes.data + 4 * int(s) for s in starts])
+        starts = np.concatenate([[0], np.cumsum(nn, dtype=np.int64)[:-1]]) if nn.size else np.zeros(0, np.int64)
+        fn = _pointers(flat.ctypes.data, starts.astype(np.uint64) * np.uint64(4))
         xa = np.ascontiguousarray(x, dtype=np.float64)
         xr = _rows(xa)
         ty = np.ascontiguousarray(atomType, dtype=np.int32)

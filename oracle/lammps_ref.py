@@ -11,21 +11,21 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = None
+_LIBS = {}
 
 
-def lib_path():
-    return os.path.join(_HERE, "_ref", "libnnplammps.so")
+def lib_path(fast=False):
+    """The parity build, or with `fast` the timed-baseline build (-O3, FMA)."""
+    return os.path.join(_HERE, "_ref", "libnnplammps_fast.so" if fast else "libnnplammps.so")
 
 
-def available():
-    return os.path.exists(lib_path())
+def available(fast=False):
+    return os.path.exists(lib_path(fast))
 
 
-def _lib():
-    global _LIB
-    if _LIB is None:
-        lib = ctypes.CDLL(lib_path())
+def _lib(fast=False):
+    if fast not in _LIBS:
+        lib = ctypes.CDLL(lib_path(fast))
         vp, i64, dbl, ip = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int
         lib.nnplmp_last_error.restype = ctypes.c_char_p
         lib.nnplmp_create.restype = vp
@@ -41,15 +41,16 @@ def _lib():
         lib.nnplmp_get_forces.argtypes = [vp, vp, i64]
         lib.nnplmp_num_ew.restype = i64
         lib.nnplmp_num_ew.argtypes = [vp]
-        _LIB = lib
-    return _LIB
+        _LIBS[fast] = lib
+    return _LIBS[fast]
 
 
 class RefInterfaceLammps:
     """One reference InterfaceLammps (initialize with the given units/map)."""
 
-    def __init__(self, model_dir, emap, cflength, cfenergy, lammps_cutoff, ntypes, showew=False):
-        lib = _lib()
+    def __init__(self, model_dir, emap, cflength, cfenergy, lammps_cutoff, ntypes, showew=False, fast=False):
+        self._fast = fast
+        lib = _lib(fast)
         d = model_dir if model_dir.endswith("/") else model_dir + "/"
         self._h = lib.nnplmp_create(d.encode(), emap.encode(), int(showew), cflength, cfenergy, lammps_cutoff,
                                     ntypes)
@@ -58,7 +59,7 @@ class RefInterfaceLammps:
 
     def close(self):
         if self._h:
-            _lib().nnplmp_destroy(self._h)
+            _lib(self._fast).nnplmp_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -69,13 +70,13 @@ class RefInterfaceLammps:
 
     def _check(self, rc):
         if rc:
-            raise RuntimeError(_lib().nnplmp_last_error().decode())
+            raise RuntimeError(_lib(self._fast).nnplmp_last_error().decode())
 
     def evaluate(self, local_types, offset, j, jtype, dr, d2, nall, num_centres=None):
         """setLocalAtoms + addNeighbor for every entry + process; returns
         (energy, atomic energies of the first num_centres mapped local atoms
         (default: all local atoms), forces [nall][3] added to zeros)."""
-        lib = _lib()
+        lib = _lib(self._fast)
         t = np.ascontiguousarray(local_types, dtype=np.int32)
         off = np.ascontiguousarray(offset, dtype=np.int64)
         jj = np.ascontiguousarray(j, dtype=np.int32)
@@ -94,4 +95,4 @@ class RefInterfaceLammps:
         return E, Ea, F
 
     def num_extrapolation_warnings(self):
-        return int(_lib().nnplmp_num_ew(self._h))
+        return int(_lib(self._fast).nnplmp_num_ew(self._h))
