@@ -71,6 +71,7 @@ def parse():
     ap.add_argument("--no-student", action="store_true")
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-lammps", action="store_true")
+    ap.add_argument("--no-scaling", action="store_true")
     ap.add_argument("--student-boxes", type=int, default=2048)
     return ap.parse_args()
 
@@ -293,6 +294,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_lammps:
         lammps = bench_lammps(args.steps, args.warmup, local, cpu=not args.no_cpu)
 
+    # nnp-scaling (input.data read + symmetry-function statistics) on the batched workload
+    scal = None
+    if rank == 0 and world == 1 and not args.no_scaling:
+        scal = bench_scaling(structs, local, cpu=not args.no_cpu)
+
     # distilled student (with teacher fallback) against the plain FP64 teacher
     stud = None
     if rank == 0 and world == 1 and not args.no_student and os.path.isdir(STUDENT):
@@ -363,7 +369,7 @@ def run_ours(args):
                 "e2e": {"value": world * natoms / (e2e_ms / 1000.0), "unit": "atoms/s", "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": nbytes_pos, "d2h_bytes_per_step": nbytes_pos + 8 * len(structs)},
                 "gpu_launches": launches, "autotune": _shape_names(tune), "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
-                "mixed": mixed, "student": stud, "large_system": large, "lammps_interface": lammps, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
+                "mixed": mixed, "student": stud, "large_system": large, "lammps_interface": lammps, "nnp_scaling": scal, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
                 "fp32_fma_peak_tflops": fp32_peak}
         print(json.dumps(line), flush=True)
     mode.close()
@@ -434,6 +440,47 @@ def bench_large(steps, warmup, device):
                       "split-bfloat16 operands and FP32 accumulators (tensor-pipe utilisation is an ncu counter, "
                       "not measured here)")
     mode.close()
+    return out
+
+
+def bench_scaling(structs, device, cpu=True):
+    """nnp-scaling on the GPU for the batched workload: the input.data file
+    read by the library's reader, then the symmetry-function statistics
+    written as scaling.data (n2p2_b200.scaling), wall clock per phase; beside
+    it the reference's per-structure nnp-scaling work (neighbour list +
+    symmetry functions without derivatives) on the host threads."""
+    import shutil
+    from n2p2_b200 import read_structures, scaling, write_structures
+    natoms = sum(s.numAtoms for s in structs)
+    out = {"workload": "%d water boxes (%d atoms), water40 descriptors, input.data -> scaling.data"
+                       % (len(structs), natoms), "unit": "atoms/s"}
+    with tempfile.TemporaryDirectory() as d:
+        shutil.copy(os.path.join(MODEL, "input.nn"), d)
+        path = os.path.join(d, "input.data")
+        write_structures(path, structs)
+        t0 = time.perf_counter()
+        ss = read_structures(path)
+        t_read = time.perf_counter() - t0
+        scaling.nnp_scaling(d, structures=ss[:64], device=device)   # CUDA context and kernels warm
+        t0 = time.perf_counter()
+        scaling.nnp_scaling(d, structures=ss, device=device)
+        t_stats = time.perf_counter() - t0
+        out["read_input_data"] = {"value": natoms / t_read, "seconds": t_read,
+                                  "file_bytes": os.path.getsize(path)}
+        out["statistics"] = {"value": natoms / t_stats, "seconds": t_stats}
+        out["value"] = natoms / (t_read + t_stats)
+    if cpu:
+        try:
+            from oracle import ref
+            threads = host_threads()
+            sample, nsample = cpu_sample(structs, threads)
+            sec = ref.time_sf_batch(MODEL, [x.to_text() for x in sample], threads, fast=True)
+            out["cpu_reference"] = {"value": nsample / sec, "unit": "atoms/s", "cores": threads, "kind": "reference",
+                                    "sample": "%d structures (%d atoms): neighbour list + calculateSymmetryFunction"
+                                              "Groups (no derivatives), reference libnnp -O3, structure-parallel"
+                                              % (len(sample), nsample)}
+        except Exception as exc:   # the GPU numbers stand without it
+            out["cpu_reference"] = {"value": None, "sample": "failed: %s" % exc}
     return out
 
 

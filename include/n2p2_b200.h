@@ -51,11 +51,13 @@ typedef int n2p2_status;
 #define N2P2_EVAL_FORCES 1          /* Mode::evaluateNNP(useForces = true)            */
 #define N2P2_EVAL_STORE_DGDR 2      /* keep dG/dr per neighbour (Atom::Neighbor::dGdr) */
 #define N2P2_EVAL_NO_GRAPH 4        /* launch kernels one by one (no CUDA graph)      */
+#define N2P2_EVAL_SYMMETRY_FUNCTIONS_ONLY 8  /* Mode::calculateSymmetryFunctionGroups alone */
 
 typedef struct n2p2_mode n2p2_mode;
 typedef struct n2p2_batch n2p2_batch;
 typedef struct n2p2_trainer n2p2_trainer;
 typedef struct n2p2_lammps n2p2_lammps;
+typedef struct n2p2_structures n2p2_structures;
 
 /* Message of the last failure on this thread ("" if none). */
 const char* n2p2_last_error(void);
@@ -189,6 +191,15 @@ n2p2_status n2p2_batch_get_symmetry_functions(n2p2_batch* batch, double* G);
 n2p2_status n2p2_batch_get_dEdG(n2p2_batch* batch, double* dEdG);
 n2p2_status n2p2_batch_get_atomic_energies(n2p2_batch* batch, double* energies);
 
+/* Symmetry-function statistics of the last evaluation, as nnp-scaling
+ * collects them (SymFncStatistics::addValue, SymFncStatistics.cpp:80-89, over
+ * the unscaled G of every atom; Dataset::collectSymmetryFunctionStatistics):
+ * counts[e] = atoms of element e; stats = per element e, four arrays of
+ * numSymmetryFunctions(e) values: minimum, maximum, sum, sum of squares.
+ * Sums are taken in atom order in chunks of 1024 atoms, the chunks added in
+ * order (the same result on every run). */
+n2p2_status n2p2_batch_get_symmetry_function_statistics(n2p2_batch* batch, int64_t* counts, double* stats);
+
 /* Atom::dGdr (self, [sum numSF][3]) and Atom::Neighbor::dGdr (per entry,
  * numDerivativeRows of the pair, [rows][3]); needs N2P2_EVAL_STORE_DGDR. */
 n2p2_status n2p2_batch_get_dGdr(n2p2_batch* batch, double* selfDGdr, double* neighborDGdr);
@@ -227,6 +238,28 @@ n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches);
 n2p2_status n2p2_neighbor_list_noalloc(const double* positions, int64_t numAtoms, const double* box, double cutoff,
                                        int64_t capacity, int64_t* offsets, int32_t* index, int32_t* image,
                                        double* d, double* dr, int64_t* numEntries, void* stream);
+
+/* ---- structure files --------------------------------------------------------
+ * input.data read in one pass: Structure::readFromLines (Structure.cpp:142-271)
+ * on every begin..end block, numbers through strtod (bit-identical to the
+ * reference's), the reference's error messages (N2P2_ERR_RUNTIME; a short
+ * atom line N2P2_ERR_OUT_OF_RANGE).  A trailing block without "end" is not
+ * read.  limit < 0 reads every structure. */
+n2p2_status n2p2_structures_read_file(const char* fileName, int64_t limit, n2p2_structures** structures);
+n2p2_status n2p2_structures_read_text(const char* text, int64_t length, int64_t limit,
+                                      n2p2_structures** structures);
+n2p2_status n2p2_structures_destroy(n2p2_structures* structures);
+n2p2_status n2p2_structures_get_count(n2p2_structures* structures, int64_t* numStructures, int64_t* numAtoms);
+/* Per structure: atoms, box [3][3] (rows = lattice vectors; zeros without
+ * one), periodic flag, reference energy and total charge (any pointer may be NULL). */
+n2p2_status n2p2_structures_get_structure_arrays(n2p2_structures* structures, int64_t* numAtoms, double* boxes,
+                                                 int32_t* periodic, double* energies, double* charges);
+/* Per atom, all structures concatenated: position [3], element symbol
+ * (4 bytes, NUL-padded), charge, reference force [3] (any pointer may be NULL). */
+n2p2_status n2p2_structures_get_atom_arrays(n2p2_structures* structures, double* positions, char* elements,
+                                            double* charges, double* forces);
+n2p2_status n2p2_structures_get_comment(n2p2_structures* structures, int64_t index, char* buffer,
+                                        int32_t capacity);
 
 /* ---- LAMMPS interface ------------------------------------------------------
  * nnp::InterfaceLammps (src/libnnpif/LAMMPS/InterfaceLammps.h:31-333), the

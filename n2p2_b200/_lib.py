@@ -23,6 +23,7 @@ PRECISION_MIXED = 1
 EVAL_FORCES = 1
 EVAL_STORE_DGDR = 2
 EVAL_NO_GRAPH = 4
+EVAL_SF_ONLY = 8
 
 # Every function the header declares, with (restype, argtypes).
 _vp = ctypes.c_void_p
@@ -104,6 +105,14 @@ SIGNATURES = {
     "n2p2_lammps_get_forces": (_i, [_vp, _vp]),
     "n2p2_lammps_get_num_extrapolation_warnings": (_i, [_vp, _P(_i64)]),
     "n2p2_lammps_clear_extrapolation_warnings": (_i, [_vp]),
+    "n2p2_batch_get_symmetry_function_statistics": (_i, [_vp, _P(_i64), _P(_d)]),
+    "n2p2_structures_read_file": (_i, [_cp, _i64, _P(_vp)]),
+    "n2p2_structures_read_text": (_i, [_cp, _i64, _i64, _P(_vp)]),
+    "n2p2_structures_destroy": (_i, [_vp]),
+    "n2p2_structures_get_count": (_i, [_vp, _P(_i64), _P(_i64)]),
+    "n2p2_structures_get_structure_arrays": (_i, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "n2p2_structures_get_atom_arrays": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "n2p2_structures_get_comment": (_i, [_vp, _i64, _vp, ctypes.c_int32]),
     "n2p2_host_alloc": (_i, [_P(_vp), ctypes.c_size_t]),
     "n2p2_host_free": (_i, [_vp]),
 }

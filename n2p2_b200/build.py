@@ -65,7 +65,7 @@ def build(verbose=False, jobs=8):
     for p in procs:
         _wait(p)
     if cmds or not os.path.exists(LIB):
-        link = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        link = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lpthread"]
         if verbose:
             print(" ".join(link), flush=True)
         r = subprocess.run(link, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)

@@ -2,6 +2,7 @@
 // are turned into status codes here and never cross the ABI.
 #include "../../include/n2p2_b200.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -14,6 +15,7 @@
 #include "engine.hpp"
 #include "host_model.hpp"
 #include "lammps.hpp"
+#include "structure_io.hpp"
 #include "trainer.hpp"
 
 using namespace n2p2b200;
@@ -45,6 +47,11 @@ struct n2p2_lammps
     std::unique_ptr<Batch> batch;    // created by the first process()
     LammpsInterface iface;
     int64_t warnings = 0;
+};
+
+struct n2p2_structures
+{
+    StructureSet set;
 };
 
 struct n2p2_batch
@@ -483,6 +490,28 @@ n2p2_status n2p2_batch_get_neighbors(n2p2_batch* batch, int64_t* offsets, int32_
     });
 }
 
+n2p2_status n2p2_batch_get_symmetry_function_statistics(n2p2_batch* batch, int64_t* counts, double* stats)
+{
+    N2P2_REQUIRE(batch);
+    N2P2_REQUIRE(counts);
+    N2P2_REQUIRE(stats);
+    return guard([&] {
+        setDevice(batch->mode);
+        Batch& b = *batch->batch;
+        const int ne = (int)batch->mode->model.numElements();
+        const int maxSF = std::max(b.maxSF(), 1);
+        std::vector<double> raw((size_t)ne * 4 * maxSF);
+        b.sfStatistics(counts, raw.data());
+        size_t at = 0;
+        for (int e = 0; e < ne; ++e)
+        {
+            const int nsf = (int)batch->mode->model.elements[e].sf.size();
+            for (int q = 0; q < 4; ++q)
+                for (int f = 0; f < nsf; ++f) stats[at++] = raw[((size_t)e * 4 + q) * maxSF + f];
+        }
+    });
+}
+
 n2p2_status n2p2_batch_get_symmetry_functions(n2p2_batch* batch, double* G)
 {
     N2P2_REQUIRE(batch);
@@ -918,6 +947,92 @@ n2p2_status n2p2_lammps_clear_extrapolation_warnings(n2p2_lammps* lammps)
     N2P2_REQUIRE(lammps);
     lammps->warnings = 0;
     return N2P2_OK;
+}
+
+n2p2_status n2p2_structures_read_file(const char* fileName, int64_t limit, n2p2_structures** structures)
+{
+    N2P2_REQUIRE(fileName);
+    N2P2_REQUIRE(structures);
+    return guard([&] {
+        auto s = std::make_unique<n2p2_structures>();
+        readStructuresFile(fileName, limit, s->set);
+        *structures = s.release();
+    });
+}
+
+n2p2_status n2p2_structures_read_text(const char* text, int64_t length, int64_t limit,
+                                      n2p2_structures** structures)
+{
+    N2P2_REQUIRE(text);
+    N2P2_REQUIRE(structures);
+    return guard([&] {
+        auto s = std::make_unique<n2p2_structures>();
+        const std::string copy(text, (size_t)length);   // NUL-terminated for strtod
+        readStructures(copy.c_str(), copy.size(), limit, s->set);
+        *structures = s.release();
+    });
+}
+
+n2p2_status n2p2_structures_destroy(n2p2_structures* structures)
+{
+    delete structures;
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_structures_get_count(n2p2_structures* structures, int64_t* numStructures, int64_t* numAtoms)
+{
+    N2P2_REQUIRE(structures);
+    if (numStructures) *numStructures = structures->set.numStructures();
+    if (numAtoms) *numAtoms = structures->set.numAtoms();
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_structures_get_structure_arrays(n2p2_structures* structures, int64_t* numAtoms, double* boxes,
+                                                 int32_t* periodic, double* energies, double* charges)
+{
+    N2P2_REQUIRE(structures);
+    StructureSet const& t = structures->set;
+    const size_t S = (size_t)t.numStructures();
+    for (size_t k = 0; k < S; ++k)
+        if (numAtoms) numAtoms[k] = t.atomBegin[k + 1] - t.atomBegin[k];
+    if (boxes && S) std::memcpy(boxes, t.boxes.data(), sizeof(double) * 9 * S);
+    if (periodic && S) std::memcpy(periodic, t.periodic.data(), sizeof(int32_t) * S);
+    if (energies && S) std::memcpy(energies, t.energies.data(), sizeof(double) * S);
+    if (charges && S) std::memcpy(charges, t.charges.data(), sizeof(double) * S);
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_structures_get_atom_arrays(n2p2_structures* structures, double* positions, char* elements,
+                                            double* charges, double* forces)
+{
+    N2P2_REQUIRE(structures);
+    return guard([&] {
+        StructureSet const& t = structures->set;
+        const size_t N = (size_t)t.numAtoms();
+        if (positions && N) std::memcpy(positions, t.positions.data(), sizeof(double) * 3 * N);
+        if (forces && N) std::memcpy(forces, t.forces.data(), sizeof(double) * 3 * N);
+        if (charges && N) std::memcpy(charges, t.atomCharges.data(), sizeof(double) * N);
+        if (elements)
+            for (size_t a = 0; a < N; ++a)
+            {
+                std::string const& e = t.elements[a];
+                if (e.size() > 3) throw std::runtime_error("ERROR: element symbol longer than 3 characters.\n");
+                std::memset(elements + 4 * a, 0, 4);
+                std::memcpy(elements + 4 * a, e.data(), e.size());
+            }
+    });
+}
+
+n2p2_status n2p2_structures_get_comment(n2p2_structures* structures, int64_t index, char* buffer,
+                                        int32_t capacity)
+{
+    N2P2_REQUIRE(structures);
+    N2P2_REQUIRE(buffer);
+    return guard([&] {
+        std::string const& c = structures->set.comments.at((size_t)index);
+        if ((int64_t)c.size() + 1 > capacity) throw std::runtime_error("buffer too small");
+        std::memcpy(buffer, c.c_str(), c.size() + 1);
+    });
 }
 
 } // extern "C"

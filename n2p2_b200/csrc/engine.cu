@@ -235,6 +235,8 @@ void DeviceModel::upload(Model const& m)
     if (!m.setupDone) throw std::runtime_error("ERROR: setupGeneric() has not been called.\n");
     if (!m.scalingDone) throw std::runtime_error("ERROR: symmetry function scaling has not been set up.\n");
     release();
+    networksSet = true;
+    missingWeights.clear();
     DevModel v{};
     v.numElements = (int)m.elements.size();
     v.normalizeNeurons = m.normalizeNeurons ? 1 : 0;
@@ -419,7 +421,11 @@ void DeviceModel::upload(Model const& m)
         }
         // network
         NetworkTopology const& t = el.topology;
-        if (!el.hasWeights) throw std::runtime_error("ERROR: weights of element " + el.symbol + " not set.\n");
+        if (!el.hasWeights)   // symmetry functions alone still run (nnp-scaling); networks refuse to
+        {
+            networksSet = false;
+            missingWeights = el.symbol;
+        }
         if (t.numLayers > kDevMaxLayers) throw std::runtime_error("ERROR: too many network layers.\n");
         de.numLayers = t.numLayers;
         for (int l = 0; l < t.numLayers; ++l)
@@ -431,9 +437,11 @@ void DeviceModel::upload(Model const& m)
         for (int l = 1; l < t.numLayers; ++l)
         {
             de.wOffset[l] = (int)weights.size();
-            weights.insert(weights.end(), el.W[l - 1].begin(), el.W[l - 1].end());
+            if (el.hasWeights) weights.insert(weights.end(), el.W[l - 1].begin(), el.W[l - 1].end());
+            else weights.insert(weights.end(), (size_t)t.neurons[l] * t.neurons[l - 1], 0.0);
             de.bOffset[l] = (int)weights.size();
-            weights.insert(weights.end(), el.b[l - 1].begin(), el.b[l - 1].end());
+            if (el.hasWeights) weights.insert(weights.end(), el.b[l - 1].begin(), el.b[l - 1].end());
+            else weights.insert(weights.end(), (size_t)t.neurons[l], 0.0);
         }
     }
     v.maxSF = maxSF;
@@ -924,7 +932,8 @@ void Batch::setPositionsDevice(const double* r)
 void Batch::record(int flags, int precision, int checkExtrapolation, std::vector<Mark>* marks)
 {
     DevModel const& m = dmodel_.view;
-    const bool forces = (flags & EVAL_FORCES) != 0;
+    const bool sfOnly = (flags & EVAL_SF_ONLY) != 0;
+    const bool forces = (flags & EVAL_FORCES) != 0 && !sfOnly;
     const bool stored = (flags & EVAL_STORE_DGDR) != 0;
     int launches = 0;
     auto mark = [&](char const* name) {
@@ -992,6 +1001,12 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         launchExtrapolationCheck(m, v_, sms_, stream_);
         launches += 1;
         mark("extrapolation_check");
+    }
+    if (sfOnly)   // Mode::calculateSymmetryFunctionGroups alone (nnp-scaling)
+    {
+        cudaCheck(cudaGetLastError(), "kernel launch");
+        launches_ = launches;
+        return;
     }
     if (precision == PREC_MIXED && dmodel_.tcNetwork) launchNetworkTC(m, v_, forces ? 1 : 0, sms_, stream_);
     else launchNetworkFP64(m, v_, forces ? 1 : 0, sms_, stream_);
@@ -1231,6 +1246,8 @@ Batch::TuneResult Batch::autotune(int precision, int checkExtrapolation, bool us
 void Batch::evaluate(int flags, int precision, int checkExtrapolation)
 {
     if (N_ == 0) throw std::runtime_error("ERROR: no structures set.\n");
+    if (!dmodel_.networksSet && !(flags & EVAL_SF_ONLY))
+        throw std::runtime_error("ERROR: weights of element " + dmodel_.missingWeights + " not set.\n");
     if (flags & EVAL_STORE_DGDR)
     {
         if (external_) throw std::runtime_error("ERROR: stored dG/dr is not available with external neighbour lists.\n");
@@ -1265,7 +1282,8 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
         record(flags, precision, checkExtrapolation);
         return;
     }
-    const int key = (flags & (EVAL_FORCES | EVAL_STORE_DGDR)) | (precision << 4) | ((checkExtrapolation ? 1 : 0) << 5);
+    const int key = (flags & (EVAL_FORCES | EVAL_STORE_DGDR | EVAL_SF_ONLY)) | (precision << 4) |
+                    ((checkExtrapolation ? 1 : 0) << 5);
     if (autotuneEnabled && !tuned_[precision] && !(flags & EVAL_STORE_DGDR)) autotune(precision, checkExtrapolation, true);
     if (graphExec_ == nullptr || graphKey_ != key)
     {
@@ -1412,6 +1430,29 @@ void Batch::copyDEdG(double* out)
 void Batch::copyAtomicEnergies(double* out)
 {
     cudaCheck(cudaMemcpy(out, v_.Eatom, sizeof(double) * N_, cudaMemcpyDeviceToHost), "D2H");
+}
+
+void Batch::sfStatistics(int64_t* counts, double* stats)
+{
+    const int ne = (int)model_.numElements();
+    const int maxSF = std::max(dmodel_.maxSF, 1);
+    int largest = 0;
+    for (int e = 0; e < ne; ++e)
+    {
+        counts[e] = v_.elemBegin[e + 1] - v_.elemBegin[e];
+        largest = std::max(largest, (int)counts[e]);
+    }
+    const int maxChunks = std::max(1, (largest + 1023) / 1024);
+    std::vector<void*> tmp;
+    double* partial = devAlloc<double>(pool_, (size_t)ne * maxChunks * 4 * maxSF, tmp);
+    double* result = devAlloc<double>(pool_, (size_t)ne * 4 * maxSF, tmp);
+    cudaCheck(cudaMemsetAsync(result, 0, sizeof(double) * (size_t)ne * 4 * maxSF, stream_), "memset");
+    launchSFStatistics(dmodel_.view, v_, ne, maxChunks, maxSF, partial, result, stream_);
+    cudaCheck(cudaGetLastError(), "statistics launch");
+    cudaCheck(cudaMemcpyAsync(stats, result, sizeof(double) * (size_t)ne * 4 * maxSF, cudaMemcpyDeviceToHost, stream_),
+              "statistics D2H");
+    synchronize();
+    freeAll(pool_, tmp);
 }
 
 void Batch::copyAtomWarnings(int* out)

@@ -23,6 +23,7 @@ enum EvalFlags : int {
     EVAL_FORCES = 1,          // forces (else energies only)
     EVAL_STORE_DGDR = 2,      // keep dG/dr per neighbour row (API form)
     EVAL_NO_GRAPH = 4,        // launch kernels directly instead of replaying a CUDA graph
+    EVAL_SF_ONLY = 8,         // symmetry functions (and the extrapolation check) only
 };
 
 void cudaCheck(cudaError_t e, char const* what);
@@ -60,6 +61,8 @@ public:
     size_t numWeights = 0;               // entries of the flat weight array
     uint64_t fingerprint = 0;            // hash of the evaluation plan (groups, members, cutoffs)
     bool tcNetwork = false;              // mixed form runs the networks on the tensor cores
+    bool networksSet = true;             // every element has weights (else symmetry functions only)
+    std::string missingWeights;
     double* weightsDevice() const { return weights_; }
     double* weightsTDevice() const { return weightsT_; }
     int* transIndexDevice() const { return transIndex_; }
@@ -189,6 +192,12 @@ public:
     void copyDGdr(double* self, double* nbr);   // self [sum numSF][3], nbr [sum rows][3]
     void copyPositions(double* out);  // internal units after remap/normalisation
     void copyAtomWarnings(int* out);
+    // Symmetry-function statistics of the last evaluation (SymFncStatistics,
+    // as nnp-scaling collects them): per element its atom count and, per
+    // function, min, max, sum and sum of squares of the unscaled G, in atom
+    // order.  counts [numElements], stats [numElements][4][maxSF].
+    void sfStatistics(int64_t* counts, double* stats);
+    int maxSF() const { return dmodel_.maxSF; }
 
 private:
     void allocateAtoms();

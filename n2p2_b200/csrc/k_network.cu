@@ -6,6 +6,8 @@
 // accumulation, which equals NeuralNetwork::calculateDEdG
 // (NeuralNetwork.cpp:396-442) including the normalize_nodes divisions.
 #include "kernels_common.cuh"
+
+#include <math_constants.h>
 #include "kernels.hpp"
 
 namespace n2p2b200 {
@@ -293,6 +295,73 @@ __global__ void kExtrapolationCheck(DevModel model, BatchView b)
         b.atomWarnings[i] = count;
         if (count) atomicAdd(&b.status->extrapolationWarnings, count);
     }
+}
+
+// Symmetry-function statistics of the batch (SymFncStatistics::addValue,
+// SymFncStatistics.cpp:80-89, as nnp-scaling collects them): per element and
+// function the minimum, maximum, sum and sum of squares of the unscaled G.
+// Block (chunk, element) = up to kStatChunk of the element's atoms in atom
+// order, thread = function; kSFStatisticsReduce adds the chunks in order, so
+// the sums do not depend on timing.
+constexpr int kStatChunk = 1024;
+
+__global__ void kSFStatistics(DevModel model, BatchView b, int maxChunks, int maxSF, double* __restrict__ partial)
+{
+    const int e = blockIdx.y, chunk = blockIdx.x;
+    const int a0 = b.elemBegin[e] + chunk * kStatChunk;
+    const int a1 = min(a0 + kStatChunk, b.elemBegin[e + 1]);
+    if (a0 >= a1) return;
+    DevElement const& E = model.el[e];
+    double* out = partial + ((size_t)e * maxChunks + chunk) * 4 * maxSF;
+    for (int s = threadIdx.x; s < E.numSF; s += blockDim.x)
+    {
+        DevScaling const& sc = model.scaling[E.sfBegin + s];
+        double mn = CUDART_INF, mx = -CUDART_INF, sum = 0.0, sum2 = 0.0;
+        for (int k = a0; k < a1; ++k)
+        {
+            const double v = unscaleG(sc, b.G[(size_t)b.elemAtoms[k] * b.gStride + s]);
+            sum = __dadd_rn(sum, v);
+            sum2 = __dadd_rn(sum2, __dmul_rn(v, v));
+            mn = fmin(mn, v);
+            mx = fmax(mx, v);
+        }
+        out[s] = mn;
+        out[maxSF + s] = mx;
+        out[2 * maxSF + s] = sum;
+        out[3 * maxSF + s] = sum2;
+    }
+}
+
+__global__ void kSFStatisticsReduce(DevModel model, BatchView b, int maxChunks, int maxSF,
+                                    const double* __restrict__ partial, double* __restrict__ result)
+{
+    const int e = blockIdx.x;
+    DevElement const& E = model.el[e];
+    const int chunks = (b.elemBegin[e + 1] - b.elemBegin[e] + kStatChunk - 1) / kStatChunk;
+    for (int s = threadIdx.x; s < E.numSF; s += blockDim.x)
+    {
+        double mn = CUDART_INF, mx = -CUDART_INF, sum = 0.0, sum2 = 0.0;
+        for (int c = 0; c < chunks; ++c)
+        {
+            const double* p = partial + ((size_t)e * maxChunks + c) * 4 * maxSF;
+            mn = fmin(mn, p[s]);
+            mx = fmax(mx, p[maxSF + s]);
+            sum = __dadd_rn(sum, p[2 * maxSF + s]);
+            sum2 = __dadd_rn(sum2, p[3 * maxSF + s]);
+        }
+        double* r = result + (size_t)e * 4 * maxSF;
+        r[s] = mn;
+        r[maxSF + s] = mx;
+        r[2 * maxSF + s] = sum;
+        r[3 * maxSF + s] = sum2;
+    }
+}
+
+void launchSFStatistics(DevModel const& m, BatchView const& b, int numElements, int maxChunks, int maxSF,
+                        double* partial, double* result, cudaStream_t st)
+{
+    kSFStatistics<<<dim3(maxChunks, numElements), 128, 0, st>>>(m, b, maxChunks, maxSF, partial);
+    kSFStatisticsReduce<<<numElements, 128, 0, st>>>(m, b, maxChunks, maxSF, partial, result);
 }
 
 void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)

@@ -120,6 +120,11 @@ void launchMaskOffsets(DevModel const& m, BatchView const& b, int sms, cudaStrea
 void launchNetworkTC(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st);
 void launchEnergySum(BatchView const& b, cudaStream_t st);
 void launchGatherForces(BatchView const& b, int sms, cudaStream_t st);
+// Per element and function: min, max, sum, sum of squares of the unscaled G
+// (result [numElements][4][maxSF]; partial [numElements][maxChunks][4][maxSF],
+// maxChunks = ceil(largest element count / 1024)).
+void launchSFStatistics(DevModel const& m, BatchView const& b, int numElements, int maxChunks, int maxSF,
+                        double* partial, double* result, cudaStream_t st);
 void launchGatherTargets(BatchView const& b, int numTargets, const int64_t* tOffset, const int64_t* tEntry,
                          const int* targetCenter, double* F, int sms, cudaStream_t st);
 

@@ -215,10 +215,28 @@ class Batch:
         # the copy is asynchronous; keep the buffer alive until the next sync
         _lib.check(self._lib.n2p2_batch_synchronize(self._h))
 
-    def evaluate(self, forces=True, storeDGdr=False, graph=True):
+    def evaluate(self, forces=True, storeDGdr=False, graph=True, symmetryFunctionsOnly=False):
         flags = (_lib.EVAL_FORCES if forces else 0) | (_lib.EVAL_STORE_DGDR if storeDGdr else 0) | \
-            (0 if graph else _lib.EVAL_NO_GRAPH)
+            (0 if graph else _lib.EVAL_NO_GRAPH) | (_lib.EVAL_SF_ONLY if symmetryFunctionsOnly else 0)
         _lib.check(self._lib.n2p2_batch_evaluate(self._h, flags))
+
+    def symmetryFunctionStatistics(self):
+        """Per element: dict(count, min, max, sum, sum2) of the unscaled G of
+        the last evaluation (n2p2_batch_get_symmetry_function_statistics)."""
+        m = self._mode
+        ne = m.numElements
+        nsf = [m.numSymmetryFunctions(e) for e in range(ne)]
+        counts = np.zeros(ne, dtype=np.int64)
+        stats = np.zeros(4 * sum(nsf))
+        _lib.check(self._lib.n2p2_batch_get_symmetry_function_statistics(
+            self._h, counts.ctypes.data_as(_P(ctypes.c_int64)), _dp(stats)))
+        out, at = [], 0
+        for e in range(ne):
+            block = stats[at:at + 4 * nsf[e]].reshape(4, nsf[e])
+            at += 4 * nsf[e]
+            out.append({"count": int(counts[e]), "min": block[0].copy(), "max": block[1].copy(),
+                        "sum": block[2].copy(), "sum2": block[3].copy()})
+        return out
 
     def synchronize(self):
         _lib.check(self._lib.n2p2_batch_synchronize(self._h))

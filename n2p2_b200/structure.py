@@ -1,10 +1,10 @@
 """Structures in the n2p2 `input.data` format (host-side I/O).
 
-Parsing follows Structure::readFromLines (reference src/libnnp/Structure.cpp:142-271):
+Reading follows Structure::readFromLines (reference src/libnnp/Structure.cpp:142-271):
 keywords begin / comment / lattice / atom / energy / charge / end, numbers
-converted with correct rounding (Python float == C atof on glibc), so
-positions are bit-identical to what the reference reads.  Remapping into the
-cell and unit normalisation happen on the GPU (see Batch).
+converted with correct rounding (strtod in the library), so positions are
+bit-identical to what the reference reads.  Remapping into the cell and unit
+normalisation happen on the GPU (see Batch).
 """
 import numpy as np
 
@@ -56,62 +56,51 @@ class Structure:
         return "\n".join(out) + "\n"
 
 
-def parse_lines(lines):
-    """Structure::readFromLines on one begin..end block."""
-    box_rows, pos, el, q, fref = [], [], [], [], []
-    comment, energy, charge = "", 0.0, 0.0
-    first = lines[0].split()
-    if not first or first[0] != "begin":
-        raise RuntimeError('ERROR: Unexpected line content, expected "begin" keyword.\n')
-    for line in lines:
-        w = line.split()
-        if not w:
-            continue
-        k = w[0]
-        if k == "begin":
-            for word in w[1:]:
-                if word not in ("set=train", "set=test"):
-                    raise RuntimeError('ERROR: Unknown keyword in structure specification, check "begin" arguments.\n')
-        elif k == "comment":
-            p = line.find("comment")
-            comment = line[:p] + line[p + len("comment") + 1:]
-        elif k == "lattice":
-            if len(box_rows) > 2:
-                raise RuntimeError("ERROR: Too many box vectors.\n")
-            box_rows.append([float(w[1]), float(w[2]), float(w[3])])
-        elif k == "atom":
-            pos.append([float(w[1]), float(w[2]), float(w[3])])
-            el.append(w[4])
-            q.append(float(w[5]))
-            fref.append([float(w[7]), float(w[8]), float(w[9])])
-        elif k == "energy":
-            energy = float(w[1])
-        elif k == "charge":
-            charge = float(w[1])
-        elif k == "end":
-            if len(box_rows) not in (0, 3):
-                raise RuntimeError("ERROR: Strange number of box vectors.\n")
-            break
-        else:
-            raise RuntimeError('ERROR: Unexpected file content, unknown keyword "%s".\n' % k)
-    box = np.array(box_rows) if len(box_rows) == 3 else None
-    return Structure(np.array(pos), el, box, comment, energy, charge, np.array(fref).reshape(-1, 3), np.array(q))
-
-
 def read_structures(path_or_text, is_text=False, limit=None):
-    """All structures of an input.data file (or text)."""
-    text = path_or_text if is_text else open(path_or_text).read()
-    out, block = [], []
-    for line in text.splitlines():
-        if not line.strip():
-            continue
-        block.append(line)
-        if line.split()[0] == "end":
-            out.append(parse_lines(block))
-            block = []
-            if limit is not None and len(out) >= limit:
-                break
-    return out
+    """All structures of an input.data file (or text): Structure::readFromLines
+    on every begin..end block, read by the library in one pass
+    (n2p2_structures_*; numbers bit-identical to the reference's)."""
+    import ctypes
+    import os
+
+    from . import _lib
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    lim = -1 if limit is None else int(limit)
+    if is_text:
+        data = path_or_text.encode()
+        _lib.check(lib.n2p2_structures_read_text(data, len(data), lim, ctypes.byref(h)))
+    else:
+        _lib.check(lib.n2p2_structures_read_file(os.fsencode(path_or_text), lim, ctypes.byref(h)))
+    try:
+        S, N = ctypes.c_int64(), ctypes.c_int64()
+        _lib.check(lib.n2p2_structures_get_count(h, ctypes.byref(S), ctypes.byref(N)))
+        S, N = S.value, N.value
+        na = np.zeros(S, dtype=np.int64)
+        boxes = np.zeros((S, 3, 3))
+        per = np.zeros(S, dtype=np.int32)
+        E = np.zeros(S)
+        Q = np.zeros(S)
+        _lib.check(lib.n2p2_structures_get_structure_arrays(h, na.ctypes.data, boxes.ctypes.data, per.ctypes.data,
+                                                            E.ctypes.data, Q.ctypes.data))
+        pos = np.zeros((N, 3))
+        sym = np.zeros(N, dtype="S4")
+        q = np.zeros(N)
+        f = np.zeros((N, 3))
+        _lib.check(lib.n2p2_structures_get_atom_arrays(h, pos.ctypes.data, sym.ctypes.data, q.ctypes.data,
+                                                       f.ctypes.data))
+        symbols = sym.astype(str)
+        buf = ctypes.create_string_buffer(1 << 16)
+        out, a0 = [], 0
+        for k in range(S):
+            a1 = a0 + int(na[k])
+            _lib.check(lib.n2p2_structures_get_comment(h, k, buf, len(buf)))
+            out.append(Structure(pos[a0:a1], symbols[a0:a1].tolist(), boxes[k] if per[k] else None,
+                                 buf.value.decode(), E[k], Q[k], f[a0:a1], q[a0:a1]))
+            a0 = a1
+        return out
+    finally:
+        lib.n2p2_structures_destroy(h)
 
 
 def write_structures(path, structures):

@@ -55,6 +55,8 @@ def _lib(fast=False):
         f = getattr(lib, "nnpref_" + n)
         f.restype = i64
         f.argtypes = [vp, ctypes.POINTER(i64), i64]
+    lib.nnpref_time_sf_batch.restype = dbl
+    lib.nnpref_time_sf_batch.argtypes = [ctypes.c_char_p, i64, ctypes.POINTER(ctypes.c_char_p), i64]
     lib.nnpref_time_batch.restype = dbl
     lib.nnpref_time_batch.argtypes = [ctypes.c_char_p, i64, ctypes.POINTER(ctypes.c_char_p), i64,
                                       ctypes.POINTER(dbl)]
@@ -145,3 +147,16 @@ def time_batch(model_dir, texts, threads, fast=True):
     if sec < 0:
         raise RuntimeError("reference timing failed: " + lib.nnpref_last_error().decode())
     return sec, energies
+
+
+def time_sf_batch(model_dir, texts, threads, fast=True):
+    """Wall seconds of the per-structure work of nnp-scaling (neighbour list +
+    calculateSymmetryFunctionGroups without derivatives) over `texts` on
+    `threads` host threads."""
+    lib = _lib(fast)
+    arr = (ctypes.c_char_p * len(texts))(*[t.encode() for t in texts])
+    sec = lib.nnpref_time_sf_batch(model_dir.encode(), len(texts), arr, threads)
+    if sec < 0:
+        raise RuntimeError("reference timing failed: " + lib.nnpref_last_error().decode())
+    return sec
+

@@ -79,6 +79,13 @@ public:
     size_t numRows(size_t ec, size_t en) const { return elements.at(ec).getSymmetryFunctionNumTable().at(en); }
     size_t nElem() const { return numElements; }
     double maxRc() const { return maxCutoffRadius; }
+    // the per-structure work of nnp-scaling (nnp-scaling.cpp: neighbour list,
+    // Mode::calculateSymmetryFunctionGroups without derivatives)
+    void symmetryFunctionsOnly(Structure& s)
+    {
+        s.calculateNeighborList(maxCutoffRadius, false);
+        calculateSymmetryFunctionGroups(s, false);
+    }
 };
 
 struct Snapshot
@@ -243,8 +250,26 @@ NNPREF_GETTER(atomic_energy, atomicEnergy, double)
 // NN objects hold per-neuron state and are not shared between threads).
 // Parsing and setup happen before the clock starts.  Returns wall seconds of
 // the evaluation phase; energies (physical units) are written to `energies`.
+static double timeBatch(const char* dir, int64_t numStructures, const char* const* texts, int64_t numThreads,
+                        double* energies, bool sfOnly);
+
 double nnpref_time_batch(const char* dir, int64_t numStructures, const char* const* texts,
                          int64_t numThreads, double* energies)
+{
+    return timeBatch(dir, numStructures, texts, numThreads, energies, false);
+}
+
+// The same for the symmetry functions alone (what nnp-scaling computes per
+// structure); no energies.
+double nnpref_time_sf_batch(const char* dir, int64_t numStructures, const char* const* texts, int64_t numThreads)
+{
+    return timeBatch(dir, numStructures, texts, numThreads, nullptr, true);
+}
+
+} // extern "C"
+
+static double timeBatch(const char* dir, int64_t numStructures, const char* const* texts, int64_t numThreads,
+                        double* energies, bool sfOnly)
 {
     try
     {
@@ -272,7 +297,8 @@ double nnpref_time_batch(const char* dir, int64_t numStructures, const char* con
                 for (size_t k = 0; k < perThread[t].size(); ++k)
                 {
                     Structure& st = perThread[t][k];
-                    hs[t]->mode.evaluateNNP(st, true);
+                    if (sfOnly) hs[t]->mode.symmetryFunctionsOnly(st);
+                    else hs[t]->mode.evaluateNNP(st, true);
                 }
             });
         }
@@ -283,7 +309,7 @@ double nnpref_time_batch(const char* dir, int64_t numStructures, const char* con
             for (size_t k = 0; k < perThread[t].size(); ++k)
             {
                 Structure& st = perThread[t][k];
-                hs[t]->mode.finish(st);
+                if (!sfOnly) hs[t]->mode.finish(st);
                 if (energies) energies[ids[t][k]] = st.energy;
             }
             delete hs[t];
@@ -297,4 +323,4 @@ double nnpref_time_batch(const char* dir, int64_t numStructures, const char* con
     }
 }
 
-} // extern "C"
+

@@ -170,3 +170,43 @@ def pair_style_entries(dom, pair_cut):
     js = np.array(js, dtype=np.int32)
     return {"offset": np.array(off, dtype=np.int64), "j": js, "type": dom["type"][js],
             "dr": np.array(dr, dtype=np.float64).reshape(-1, 3), "d2": np.array(d2s, dtype=np.float64)}
+
+
+def python_read_structures(text):
+    """An independent restatement of Structure::readFromLines (reference
+    Structure.cpp:142-271) in Python, the checker of the library's reader:
+    list of dicts (positions, elements, box, comment, energy, charge,
+    forces, charges)."""
+    out, block = [], []
+    for line in text.splitlines():
+        if not line.strip():
+            continue
+        block.append(line)
+        if line.split()[0] != "end":
+            continue
+        box, pos, el, q, f = [], [], [], [], []
+        comment, energy, charge = "", 0.0, 0.0
+        if block[0].split()[0] != "begin":
+            raise RuntimeError('ERROR: Unexpected line content, expected "begin" keyword.\n')
+        for ln in block:
+            w = ln.split()
+            k = w[0]
+            if k == "comment":
+                p = ln.find("comment")
+                comment = ln[:p] + ln[p + 8:]
+            elif k == "lattice":
+                box.append([float(w[1]), float(w[2]), float(w[3])])
+            elif k == "atom":
+                pos.append([float(w[1]), float(w[2]), float(w[3])])
+                el.append(w[4])
+                q.append(float(w[5]))
+                f.append([float(w[7]), float(w[8]), float(w[9])])
+            elif k == "energy":
+                energy = float(w[1])
+            elif k == "charge":
+                charge = float(w[1])
+        out.append({"positions": np.array(pos).reshape(-1, 3), "elements": el,
+                    "box": np.array(box) if len(box) == 3 else None, "comment": comment, "energy": energy,
+                    "charge": charge, "forces": np.array(f).reshape(-1, 3), "charges": np.array(q)})
+        block = []
+    return out
