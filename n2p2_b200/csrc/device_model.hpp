@@ -18,7 +18,7 @@ enum Activation {
 constexpr int kDevMaxElements = 8;
 constexpr int kDevMaxLayers = 6;
 constexpr int kMaxMembers = 32;     // members of one symmetry-function group
-constexpr int kMaxSFPerElement = 256;
+constexpr int kMaxSFPerElement = 512;
 constexpr int kMaxNeurons = 128;    // widest layer of an atomic network
 
 // One member of a symmetry-function group (SymGrpExpRad / SymGrpExpAngn /
@@ -60,6 +60,29 @@ struct DevGroup
     signed char comboMember[16];    // (etaSlot * 2 + lambdaSlot) * 4 + zetaSlot -> member, -1 if absent
 };
 
+// One compact symmetry function (SymFncCompRad, SymFncCompAngw): compact
+// radial function on (rl, rc) (CompactFunction: center, 1/width), and for the
+// angular type a compact function of the angle on (aLeft, aRight) radians.
+struct DevCompactMember
+{
+    int    sf;             // index of the symmetry function in its element
+    int    core;           // CompactCore
+    int    asym;           // asymmetric polynomial ((2 - x) x argument)
+    int    pad_;
+    double rl, rc, rCenter, rScale;
+    double aLeft, aRight, aCenter, aScale;
+};
+
+// Compact members sharing (type, e1[, e2]) (SymGrpCompRad / SymGrpCompAngw).
+struct DevCompactGroup
+{
+    int    type;           // 20 radial, 22 angular wide
+    int    e1, e2;
+    int    memberBegin, memberCount;
+    int    pad_;
+    double rmin, rmax;     // smallest lower and largest upper radial boundary of the members
+};
+
 constexpr int kMaxBases = 4;        // exponential bases per group
 constexpr int kMaxStagedBases = 2;  // bases staged per neighbour for angular groups
 
@@ -86,6 +109,7 @@ struct DevElement
     int numSF;
     int sfBegin;                      // into the scaling array
     int groupBegin, groupCount;
+    int compactBegin, compactCount;   // compact groups
     int rows[kDevMaxElements];        // derivative rows per neighbour element
     int tableBegin[kDevMaxElements];  // into rowTable: SF index of each row
     // atomic network
@@ -115,6 +139,10 @@ struct DevModel
     const int*        rowTable;
     const double*     weights;
     const double*     weightsT;       // weights with every matrix transposed ([n_{l-1}][n_l]), same offsets
+    int numCompactGroups;
+    int pad2_;
+    const DevCompactGroup*  compactGroups;
+    const DevCompactMember* compactMembers;
 };
 
 // Per structure geometry for the neighbour build.

@@ -221,6 +221,10 @@ void DeviceModel::release()
     cudaFree(weights_);
     cudaFree(weightsT_);
     cudaFree(transIndex_);
+    cudaFree(compactGroups_);
+    cudaFree(compactMembers_);
+    compactGroups_ = nullptr;
+    compactMembers_ = nullptr;
     groups_ = nullptr;
     members_ = nullptr;
     scaling_ = nullptr;
@@ -247,6 +251,8 @@ void DeviceModel::upload(Model const& m)
     std::vector<double> slotRc;
     std::vector<DevGroup> groups;
     std::vector<DevMember> members;
+    std::vector<DevCompactGroup> compactGroups;
+    std::vector<DevCompactMember> compactMembers;
     std::vector<DevScaling> scaling;
     std::vector<int> rowTable;
     std::vector<double> weights;
@@ -419,6 +425,46 @@ void DeviceModel::upload(Model const& m)
             else if (dg.type != 2 && dg.gridNZ > 2 && v.allFast) v.allFast = 4;
             groups.push_back(dg);
         }
+        // compact groups (SymGrpCompRad / SymGrpCompAngw members)
+        de.compactBegin = (int)compactGroups.size();
+        de.compactCount = (int)el.compactGroups.size();
+        for (auto const& g : el.compactGroups)
+        {
+            DevCompactGroup cg{};
+            cg.type = g.type;
+            cg.e1 = g.e1;
+            cg.e2 = g.e2;
+            cg.memberBegin = (int)compactMembers.size();
+            cg.memberCount = (int)g.members.size();
+            cg.rmin = 1e300;
+            cg.rmax = -1e300;
+            for (int q : g.members)
+            {
+                SymFunc const& s = el.sf[q];
+                DevCompactMember cm{};
+                cm.sf = s.index;
+                cm.core = s.core;
+                cm.asym = s.asymmetric ? 1 : 0;
+                // CompactFunction::setLeftRight (CompactFunction.cpp:62-76)
+                cm.rl = s.rl;
+                cm.rc = s.rc;
+                cm.rCenter = (s.rc + s.rl) / 2.0;
+                cm.rScale = 1.0 / ((s.rc - s.rl) / 2.0);
+                if (s.type != 20)
+                {
+                    // SymFncBaseCompAng::setParameters: the angles in radians
+                    const double pi = 3.14159265358979323846;
+                    cm.aLeft = s.angleLeft * pi / 180.0;
+                    cm.aRight = s.angleRight * pi / 180.0;
+                    cm.aCenter = (cm.aRight + cm.aLeft) / 2.0;
+                    cm.aScale = 1.0 / ((cm.aRight - cm.aLeft) / 2.0);
+                }
+                cg.rmin = std::min(cg.rmin, s.rl);
+                cg.rmax = std::max(cg.rmax, s.rc);
+                compactMembers.push_back(cm);
+            }
+            compactGroups.push_back(cg);
+        }
         // network
         NetworkTopology const& t = el.topology;
         if (!el.hasWeights)   // symmetry functions alone still run (nnp-scaling); networks refuse to
@@ -491,6 +537,11 @@ void DeviceModel::upload(Model const& m)
     up((void**)&weights_, weights.data(), weights.size() * sizeof(double));
     up((void**)&weightsT_, weightsT.data(), weightsT.size() * sizeof(double));
     up((void**)&transIndex_, transIndexHost.data(), transIndexHost.size() * sizeof(int));
+    up((void**)&compactGroups_, compactGroups.data(), compactGroups.size() * sizeof(DevCompactGroup));
+    up((void**)&compactMembers_, compactMembers.data(), compactMembers.size() * sizeof(DevCompactMember));
+    v.numCompactGroups = (int)compactGroups.size();
+    v.compactGroups = compactGroups_;
+    v.compactMembers = compactMembers_;
     v.groups = groups_;
     v.members = members_;
     v.scaling = scaling_;
@@ -505,6 +556,8 @@ void DeviceModel::upload(Model const& m)
     };
     mix(groups.data(), groups.size() * sizeof(DevGroup));
     mix(members.data(), members.size() * sizeof(DevMember));
+    mix(compactGroups.data(), compactGroups.size() * sizeof(DevCompactGroup));
+    mix(compactMembers.data(), compactMembers.size() * sizeof(DevCompactMember));
     mix(&v.numElements, sizeof(int));
     mix(&v.allFast, sizeof(int));
     mix(&v.sortByDistance, sizeof(int));
@@ -994,6 +1047,11 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
     {
         launchSFValues(m, v_, precision, sms_, stream_, sfShape_[0][precision]);
         launches += 2;
+        if (m.numCompactGroups > 0)
+        {
+            launchCompactValues(m, v_, sms_, stream_);
+            launches += 1;
+        }
         mark("sf_values");
     }
     if (checkExtrapolation)
@@ -1027,6 +1085,11 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         {
             launchSFForces(m, v_, precision, sms_, stream_, sfShape_[1][precision]);
             launches += 2;
+            if (m.numCompactGroups > 0)
+            {
+                launchCompactForces(m, v_, sms_, stream_);
+                launches += 1;
+            }
             mark("sf_forces");
         }
         if (external_) launchGatherTargets(v_, numTargets_, tOffset_, tEntry_, targetCenter_, Ftarget_, sms_, stream_);
@@ -1058,6 +1121,8 @@ std::vector<std::pair<std::string, double>> Batch::profileStages(int flags, int 
 void Batch::countWork(int64_t* counts)
 {
     if (external_) throw std::runtime_error("ERROR: work counters need structures, not external neighbour lists.\n");
+    if (dmodel_.view.numCompactGroups > 0)
+        throw std::runtime_error("ERROR: work counters cover the Gaussian symmetry functions only.\n");
     unsigned long long* d = nullptr;
     cudaCheck(cudaMalloc(&d, sizeof(unsigned long long) * 10), "cudaMalloc");
     cudaCheck(cudaMemsetAsync(d, 0, sizeof(unsigned long long) * 10, stream_), "memset");
@@ -1251,6 +1316,8 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
     if (flags & EVAL_STORE_DGDR)
     {
         if (external_) throw std::runtime_error("ERROR: stored dG/dr is not available with external neighbour lists.\n");
+        if (dmodel_.view.numCompactGroups > 0)
+            throw std::runtime_error("ERROR: stored dG/dr is not available for compact symmetry functions.\n");
         if (precision != PREC_FP64) throw std::runtime_error("ERROR: stored dG/dr is FP64 only.\n");
         allocateDGdr();
     }

@@ -77,6 +77,8 @@ private:
     double* weights_ = nullptr;
     double* weightsT_ = nullptr;
     int* transIndex_ = nullptr;
+    DevCompactGroup* compactGroups_ = nullptr;
+    DevCompactMember* compactMembers_ = nullptr;
 };
 
 struct StructureInput

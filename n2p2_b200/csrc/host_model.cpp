@@ -51,6 +51,21 @@ bool sfLess(SymFunc const& a, SymFunc const& b)
 {
     if (a.ec != b.ec) return a.ec < b.ec;
     if (a.type != b.type) return a.type < b.type;
+    if (a.compact())
+    {
+        // SymFncCompRad / SymFncCompAngw::operator< (SymFncCompRad.cpp:50-66, SymFncCompAngw.cpp:52-74)
+        if (a.subtype != b.subtype) return a.subtype < b.subtype;
+        if (a.e1 != b.e1) return a.e1 < b.e1;
+        if (!a.radial() && a.e2 != b.e2) return a.e2 < b.e2;
+        if (a.rc != b.rc) return a.rc < b.rc;
+        if (a.rl != b.rl) return a.rl < b.rl;
+        if (!a.radial())
+        {
+            if (a.angleLeft != b.angleLeft) return a.angleLeft < b.angleLeft;
+            if (a.angleRight != b.angleRight) return a.angleRight < b.angleRight;
+        }
+        return false;
+    }
     if (a.cutoffType != b.cutoffType) return a.cutoffType < b.cutoffType;
     if (a.cutoffAlpha != b.cutoffAlpha) return a.cutoffAlpha < b.cutoffAlpha;
     if (a.rc != b.rc) return a.rc < b.rc;
@@ -385,10 +400,61 @@ void Model::setupSymmetryFunctions()
             s.zetaInt = (int)std::round(s.zeta);
             s.useIntegerPow = std::fabs(s.zeta - s.zetaInt) <= std::numeric_limits<double>::min();
         }
+        else if (s.type == 20 || s.type == 22)
+        {
+            // SymFncCompRad::setParameters (SymFncCompRad.cpp:69-99),
+            // SymFncBaseCompAng::setParameters (SymFncBaseCompAng.cpp:48-113)
+            const bool rad = s.type == 20;
+            s.e1 = elementMap.index(a.at(2));
+            s.e2 = rad ? s.e1 : elementMap.index(a.at(3));
+            const std::size_t o = rad ? 3 : 4;
+            s.rl = std::atof(a.at(o).c_str());
+            s.rc = std::atof(a.at(o + 1).c_str());
+            if (!rad)
+            {
+                s.angleLeft = std::atof(a.at(6).c_str());
+                s.angleRight = std::atof(a.at(7).c_str());
+            }
+            s.subtype = a.at(rad ? 5 : 8);
+            if (!rad && s.e1 > s.e2) std::swap(s.e1, s.e2);
+            if (s.rl > s.rc) throw std::runtime_error("ERROR: Lower radial boundary >= upper radial boundary.\n");
+            // SymFncBaseComp::setCompactFunction (SymFncBaseComp.cpp:39-92)
+            std::string const& t = s.subtype;
+            if (t.size() < 1 || t.size() > 3)
+                throw std::runtime_error("ERROR: Invalid compact function type specification: \"" + t + "\".\n");
+            if (t.front() == 'p')
+            {
+                if (t.size() < 2) throw std::runtime_error("ERROR: Invalid polynom type: \"" + t + "\".\n");
+                if (t[1] == '1') s.core = CORE_POLY1;
+                else if (t[1] == '2') s.core = CORE_POLY2;
+                else if (t[1] == '3') s.core = CORE_POLY3;
+                else if (t[1] == '4') s.core = CORE_POLY4;
+                else throw std::runtime_error("ERROR: Invalid polynom type: \"" + t + "\".\n");
+                if (t.size() == 3)
+                {
+                    if (t[2] == 'a') s.asymmetric = true;
+                    else throw std::runtime_error("ERROR: Invalid polynom specifier: \"" + t + "\".\n");
+                }
+            }
+            else if (t.front() == 'e') s.core = CORE_EXP;
+            else throw std::runtime_error("ERROR: Unknown compact SF type: \"" + t + "\".\n");
+            if (!rad)
+            {
+                if (s.angleLeft >= s.angleRight)
+                    throw std::runtime_error("ERROR: Left angle boundary right of or equal to right angle boundary.\n");
+                const double center = (s.angleLeft + s.angleRight) / 2.0;
+                if ((s.angleLeft < 0.0 && center != 0.0) || (s.angleRight > 180.0 && center != 180.0))
+                    throw std::runtime_error("ERROR: Angle boundary out of [0,180] and center of angular function "
+                                             "/= 0 or /= 180.\n");
+                if (s.angleRight - s.angleLeft > 360.0)
+                    throw std::runtime_error("ERROR: Periodic symmetry function cannot spread over domain > 360 "
+                                             "degrees\n");
+            }
+        }
         else
         {
             throw std::runtime_error(fmt("ERROR: Symmetry function type %d is not supported by the GPU "
-                                         "short-range path (supported: 2, 3, 9).\n",
+                                         "short-range path (supported: 2, 3, 9, 20, 22).\n",
                                          s.type));
         }
         elements.at(s.ec).sf.push_back(s);
@@ -404,6 +470,7 @@ void Model::setupSymmetryFunctions()
                 s.eta /= convLength * convLength;
                 s.rc *= convLength;
                 s.rs *= convLength;
+                s.rl *= convLength;   // compact: SymFncCompRad / SymFncBaseCompAng::changeLengthUnit
             }
         }
         // Element::sortSymmetryFunctions (Element.cpp:154-166)
@@ -449,8 +516,29 @@ void Model::setupSymmetryFunctionGroups()
     for (auto& el : elements)
     {
         el.groups.clear();
+        el.compactGroups.clear();
         for (auto const& s : el.sf)
         {
+            if (s.compact())
+            {
+                // SymGrpCompRad / SymGrpCompAngw::operator== (SymGrpCompRad.cpp:39-46,
+                // SymGrpCompAngw.cpp:36-44): element pair only, any radii and angles
+                SymGroup* cg = nullptr;
+                for (auto& cand : el.compactGroups)
+                    if (cand.type == s.type && cand.e1 == s.e1 && (s.radial() || cand.e2 == s.e2)) cg = &cand;
+                if (!cg)
+                {
+                    el.compactGroups.emplace_back();
+                    cg = &el.compactGroups.back();
+                    cg->type = s.type;
+                    cg->ec = s.ec;
+                    cg->e1 = s.e1;
+                    cg->e2 = s.e2;
+                }
+                cg->rc = std::max(cg->rc, s.rc);
+                cg->members.push_back(s.index);
+                continue;
+            }
             SymGroup* g = nullptr;
             for (auto& cand : el.groups)
             {

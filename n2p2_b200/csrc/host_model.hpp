@@ -48,10 +48,15 @@ struct ElementMap
     static std::size_t atomicNumber(std::string const& symbol);
 };
 
-// One Gaussian-type symmetry function (types 2, 3 and 9).
+// Core functions of the compact symmetry functions (CoreFunction::Type,
+// CoreFunction.h:40-52, numbered as the cutoff cores).
+enum CompactCore { CORE_EXP = CT_EXP, CORE_POLY1 = CT_POLY1, CORE_POLY2, CORE_POLY3, CORE_POLY4 };
+
+// One symmetry function: Gaussian types 2, 3, 9 or compact types 20, 22.
 struct SymFunc
 {
-    int    type = 0;          // 2 radial, 3 angular narrow, 9 angular wide
+    int    type = 0;          // 2 radial, 3 angular narrow, 9 angular wide, 20 compact radial,
+                              // 22 compact angular wide
     int    ec = 0, e1 = 0, e2 = 0;
     double eta = 0.0, rs = 0.0, zeta = 0.0, lambda = 0.0, rc = 0.0;
     int    cutoffType = CT_HARD;
@@ -66,7 +71,16 @@ struct SymFunc
     double Smin = 0.0, Smax = 0.0, Gmin = 0.0, Gmax = 0.0, Gmean = 0.0, Gsigma = 0.0;
     double scalingFactor = 1.0;
 
-    bool relevant(int e) const { return type == 2 ? e == e1 : (e == e1 || e == e2); }
+    // compact functions (SymFncBaseComp / SymFncBaseCompAng::setParameters)
+    double rl = 0.0;                      // lower radial boundary
+    std::string subtype;                  // "p1".."p4", optionally + "a" (asymmetric), or "e..."
+    int    core = CORE_POLY2;
+    bool   asymmetric = false;
+    double angleLeft = 0.0, angleRight = 0.0;   // degrees
+
+    bool compact() const { return type >= 20; }
+    bool radial() const { return type == 2 || type == 20; }
+    bool relevant(int e) const { return radial() ? e == e1 : (e == e1 || e == e2); }
     double scale(double value) const;
     double unscale(double value) const;
 };
@@ -98,7 +112,8 @@ struct ElementSetup
     std::size_t atomicNumber = 0;
     double atomicEnergyOffset = 0.0;
     std::vector<SymFunc> sf;                       // sorted
-    std::vector<SymGroup> groups;
+    std::vector<SymGroup> groups;                  // Gaussian types
+    std::vector<SymGroup> compactGroups;           // compact types: (type, e1[, e2]) (SymGrpCompRad/Angw::operator==)
     std::vector<std::vector<int>> table;           // table[e] = SF indices with a derivative row for neighbour element e
     NetworkTopology topology;
     // weights[l] is layer l+1: W (neurons[l+1] x neurons[l], row major) then b

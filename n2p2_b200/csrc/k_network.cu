@@ -85,7 +85,7 @@ constexpr int kNNWarps = 4;
 
 struct NNWarpSmem
 {
-    double act[2][kMaxNeurons < kMaxSFPerElement ? kMaxSFPerElement : kMaxNeurons];
+    double act[2][kMaxNeurons];   // hidden layers; a wider input layer is read from G directly
     double dfdx[kDevMaxLayers][kMaxNeurons];
     double g[2][kMaxNeurons];
 };
@@ -109,7 +109,9 @@ __global__ void __launch_bounds__(kNNWarps * 32) kNetworkFP64(DevModel model, Ba
         const int L = E.numLayers;
         const double* Gi = b.G + (size_t)i * b.gStride;
         __syncwarp();
-        for (int k = lane; k < E.neurons[0]; k += 32) S.act[0][k] = Gi[k];
+        const bool staged = E.neurons[0] <= kMaxNeurons;
+        if (staged)
+            for (int k = lane; k < E.neurons[0]; k += 32) S.act[0][k] = Gi[k];
         __syncwarp();
         int cur = 0;
         for (int l = 1; l < L; ++l)
@@ -117,10 +119,11 @@ __global__ void __launch_bounds__(kNNWarps * 32) kNetworkFP64(DevModel model, Ba
             const int nin = E.neurons[l - 1], nout = E.neurons[l];
             const double* WT = model.weightsT + E.wOffset[l];   // lanes read consecutive output neurons
             const double* bias = model.weights + E.bOffset[l];
+            const double* in = (l == 1 && !staged) ? Gi : S.act[cur];
             for (int k = lane; k < nout; k += 32)
             {
                 double x = 0.0;
-                for (int j = 0; j < nin; ++j) x += __ldg(&WT[(size_t)j * nout + k]) * S.act[cur][j];
+                for (int j = 0; j < nin; ++j) x += __ldg(&WT[(size_t)j * nout + k]) * in[j];
                 x += __ldg(&bias[k]);
                 if (model.normalizeNeurons) x /= nin;
                 double y, dy;

@@ -59,6 +59,44 @@ __device__ __forceinline__ T powInt(T x, int n)
 // Cutoff function value and derivative, CutoffFunction::fdf
 // (CutoffFunction.h:210-220) with the per-type bodies of CutoffFunction.cpp
 // and CoreFunction.h:239-318.  Always evaluated in FP64.
+// Core functions of x in [0, 1) (CoreFunction::fdf*, CoreFunction.h:189-319):
+// exp (type 4) and the polynomials poly1..poly4 (types 5-8).
+__device__ __forceinline__ void coreFdf(int type, double x, double& fx, double& dfx)
+{
+    const double kE = 2.718281828459045235360287471352662498;
+    if (type == 4)
+    {
+        double t = 1.0 / (x * x - 1.0);
+        double e = exp(t);
+        fx = kE * e;
+        dfx = -2.0 * kE * x * t * t * e;
+    }
+    else if (type == 5)
+    {
+        fx = (2.0 * x - 3.0) * x * x + 1.0;
+        dfx = x * (6.0 * x - 6.0);
+    }
+    else if (type == 6)
+    {
+        double x2 = x * x;
+        fx = ((15.0 - 6.0 * x) * x - 10.0) * x * x2 + 1.0;
+        dfx = x2 * ((60.0 - 30.0 * x) * x - 30.0);
+    }
+    else if (type == 7)
+    {
+        double x2 = x * x;
+        fx = (x * (x * (20.0 * x - 70.0) + 84.0) - 35.0) * x2 * x2 + 1.0;
+        dfx = x2 * x * (x * (x * (140.0 * x - 420.0) + 420.0) - 140.0);
+    }
+    else
+    {
+        double x4 = x * x;
+        x4 *= x4;
+        fx = (x * (x * ((315.0 - 70.0 * x) * x - 540.0) + 420.0) - 126.0) * x * x4 + 1.0;
+        dfx = x4 * (x * (x * ((2520.0 - 630.0 * x) * x - 3780.0) + 2520.0) - 630.0);
+    }
+}
+
 __device__ __forceinline__ void cutoffFdf(DevCutoff const& c, double r, double& fc, double& dfc)
 {
     if (r >= c.rc)
@@ -68,7 +106,6 @@ __device__ __forceinline__ void cutoffFdf(DevCutoff const& c, double r, double& 
         return;
     }
     const double kPi = 3.141592653589793238462643383279502884;
-    const double kE = 2.718281828459045235360287471352662498;
     switch (c.type)
     {
     case 0:  // hard
@@ -109,37 +146,7 @@ __device__ __forceinline__ void cutoffFdf(DevCutoff const& c, double r, double& 
         }
         double x = (r - c.rci) * c.iw;
         double fx, dfx;
-        if (c.type == 4)
-        {
-            double t = 1.0 / (x * x - 1.0);
-            double e = exp(t);
-            fx = kE * e;
-            dfx = -2.0 * kE * x * t * t * e;
-        }
-        else if (c.type == 5)
-        {
-            fx = (2.0 * x - 3.0) * x * x + 1.0;
-            dfx = x * (6.0 * x - 6.0);
-        }
-        else if (c.type == 6)
-        {
-            double x2 = x * x;
-            fx = ((15.0 - 6.0 * x) * x - 10.0) * x * x2 + 1.0;
-            dfx = x2 * ((60.0 - 30.0 * x) * x - 30.0);
-        }
-        else if (c.type == 7)
-        {
-            double x2 = x * x;
-            fx = (x * (x * (20.0 * x - 70.0) + 84.0) - 35.0) * x2 * x2 + 1.0;
-            dfx = x2 * x * (x * (x * (140.0 * x - 420.0) + 420.0) - 140.0);
-        }
-        else
-        {
-            double x4 = x * x;
-            x4 *= x4;
-            fx = (x * (x * ((315.0 - 70.0 * x) * x - 540.0) + 420.0) - 126.0) * x * x4 + 1.0;
-            dfx = x4 * (x * (x * ((2520.0 - 630.0 * x) * x - 3780.0) + 2520.0) - 630.0);
-        }
+        coreFdf(c.type, x, fx, dfx);
         fc = fx;
         dfc = dfx * c.iw;
         return;

@@ -11,6 +11,7 @@ import pytest
 from n2p2_b200 import _lib, read_structures, water
 from n2p2_b200.mode import Mode
 from oracle import port
+from oracle import ref as oref
 from tests import helpers as H
 
 MODELS = [os.path.join(H.GOLDEN, "examples", "H2O_RPBE-D3"), os.path.join(H.GOLDEN, "examples", "Cu2S_PBE"),
@@ -68,7 +69,7 @@ def test_unsupported_generation_and_types_are_rejected():
     m2 = Mode(0)
     m2.loadSettingsFile(_settings("number_of_elements 1\nelements H\ncutoff_type 2\n"
                                   "global_hidden_layers_short 1\nglobal_nodes_short 2\n"
-                                  "global_activation_short t l\nsymfunction_short H 20 H 0.0 5.0 p2\n"))
+                                  "global_activation_short t l\nsymfunction_short H 21 H H 0.0 5.0 0.0 180.0 p2\n"))
     with pytest.raises(_lib.N2P2Error) as e:
         m2.setupGeneric()
     assert "not supported" in str(e.value)
@@ -115,3 +116,26 @@ def test_water_generator_recipe():
     assert all(np.array_equal(x.positions, y.positions) for x, y in zip(b1, b2))
     n = np.array([x.numAtoms // 3 for x in water.water_batch(400, seed=9)])
     assert n.min() >= 32 and n.max() <= 512
+
+
+@pytest.mark.skipif(not oref.available(), reason="reference library not built")
+@pytest.mark.parametrize("name", ["Anisole_SCAN", "DMABN_SCAN", "Ethylbenzene_SCAN"])
+def test_compact_models_set_up_like_the_reference(name):
+    """Compact symmetry functions (types 20, 22): per element the number of
+    functions, the derivative rows per neighbour element and the largest
+    cutoff equal the reference library's set-up of the same files."""
+    d = os.path.join(H.GOLDEN, "examples", name)
+    m = Mode(0)
+    m.setupFromDirectory(d)
+    r = oref.RefPrediction(d)
+    try:
+        ne = m.numElements
+        assert ne == r.num_elements
+        for e in range(ne):
+            assert m.numSymmetryFunctions(e) == r.num_sf(e)
+            for f in range(ne):
+                assert m.numDerivativeRows(e, f) == r.num_rows(e, f)
+        assert m.getMaxCutoffRadius() == r.max_cutoff
+    finally:
+        r.close()
+        m.close()
