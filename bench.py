@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-lammps", action="store_true")
     ap.add_argument("--no-scaling", action="store_true")
+    ap.add_argument("--no-compact", action="store_true")
     ap.add_argument("--student-boxes", type=int, default=2048)
     return ap.parse_args()
 
@@ -294,6 +295,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_lammps:
         lammps = bench_lammps(args.steps, args.warmup, local, cpu=not args.no_cpu)
 
+    # compact symmetry functions (the reference's SCAN example model)
+    compact = None
+    if rank == 0 and world == 1 and not args.no_compact:
+        compact = bench_compact(args.steps, args.warmup, local, cpu=not args.no_cpu)
+
     # nnp-scaling (input.data read + symmetry-function statistics) on the batched workload
     scal = None
     if rank == 0 and world == 1 and not args.no_scaling:
@@ -369,7 +375,7 @@ def run_ours(args):
                 "e2e": {"value": world * natoms / (e2e_ms / 1000.0), "unit": "atoms/s", "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": nbytes_pos, "d2h_bytes_per_step": nbytes_pos + 8 * len(structs)},
                 "gpu_launches": launches, "autotune": _shape_names(tune), "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
-                "mixed": mixed, "student": stud, "large_system": large, "lammps_interface": lammps, "nnp_scaling": scal, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
+                "mixed": mixed, "student": stud, "large_system": large, "lammps_interface": lammps, "nnp_scaling": scal, "compact_functions": compact, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
                 "fp32_fma_peak_tflops": fp32_peak}
         print(json.dumps(line), flush=True)
     mode.close()
@@ -479,6 +485,59 @@ def bench_scaling(structs, device, cpu=True):
                                     "sample": "%d structures (%d atoms): neighbour list + calculateSymmetryFunction"
                                               "Groups (no derivatives), reference libnnp -O3, structure-parallel"
                                               % (len(sample), nsample)}
+        except Exception as exc:   # the GPU numbers stand without it
+            out["cpu_reference"] = {"value": None, "sample": "failed: %s" % exc}
+    return out
+
+
+def bench_compact(steps, warmup, device, cpu=True):
+    """Compact symmetry functions (types 20, 22): the reference's Anisole SCAN
+    model (331-354 functions per element, compact radial + wide angular) on 64
+    copies of its 256-atom periodic box with seeded 0.02 displacements, FP64
+    energies and forces, CUDA events on the batch stream; beside it the
+    reference library on a bounded sample, all host threads."""
+    import torch
+    from n2p2_b200 import Mode, Structure, read_structures
+    d = os.path.join(ROOT, "tests", "golden", "examples", "Anisole_SCAN")
+    s0 = read_structures(os.path.join(d, "input.data"))[0]
+    rng = np.random.default_rng(5)
+    structs = [Structure(s0.positions + rng.normal(scale=0.02, size=s0.positions.shape), s0.elements, box=s0.box)
+               for _ in range(64)]
+    natoms = sum(x.numAtoms for x in structs)
+    mode = Mode(device)
+    mode.setupFromDirectory(d)
+    b = mode.batch(structs)
+    b.setPositions(np.concatenate([x.positions for x in structs]))
+    b.evaluate(forces=True)
+    b.synchronize()
+    stream = torch.cuda.ExternalStream(b.stream(), device=torch.device("cuda", device))
+    for _ in range(warmup):
+        b.evaluate(forces=True)
+    b.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        b.evaluate(forces=True)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    stages = dict(b.profileStages(forces=True))
+    out = {"workload": "Anisole_SCAN model (reference example; compact types 20 + 22), 64 x 256-atom periodic boxes "
+                       "(%d atoms)" % natoms, "value": natoms / (ms / 1e3), "unit": "atoms/s", "ms_per_step": ms,
+           "stages_ms": {k: round(v, 3) for k, v in stages.items()}}
+    b.close()
+    mode.close()
+    if cpu:
+        try:
+            from oracle import ref
+            threads = host_threads()
+            sample = structs[:max(1, min(len(structs), threads))]
+            sec, _ = ref.time_batch(d, [x.to_text() for x in sample], threads, fast=True)
+            n = sum(x.numAtoms for x in sample)
+            out["cpu_reference"] = {"value": n / sec, "unit": "atoms/s", "cores": threads, "kind": "reference",
+                                    "sample": "%d boxes (%d atoms), reference libnnp -O3 evaluateNNP, "
+                                              "structure-parallel" % (len(sample), n)}
         except Exception as exc:   # the GPU numbers stand without it
             out["cpu_reference"] = {"value": None, "sample": "failed: %s" % exc}
     return out
