@@ -491,19 +491,12 @@ def bench_scaling(structs, device, cpu=True):
     return out
 
 
-def bench_compact(steps, warmup, device, cpu=True):
-    """Compact symmetry functions (types 20, 22): the reference's Anisole SCAN
-    model (331-354 functions per element, compact radial + wide angular) on 64
-    copies of its 256-atom periodic box with seeded 0.02 displacements, FP64
-    energies and forces, CUDA events on the batch stream; beside it the
-    reference library on a bounded sample, all host threads."""
+def _compact_run(d, structs, steps, warmup, device, cpu, cpu_sample=None):
+    """FP64 energies and forces of `structs` under the model in `d`, CUDA
+    events on the batch stream; beside it the reference library on a bounded
+    sample, all host threads."""
     import torch
-    from n2p2_b200 import Mode, Structure, read_structures
-    d = os.path.join(ROOT, "tests", "golden", "examples", "Anisole_SCAN")
-    s0 = read_structures(os.path.join(d, "input.data"))[0]
-    rng = np.random.default_rng(5)
-    structs = [Structure(s0.positions + rng.normal(scale=0.02, size=s0.positions.shape), s0.elements, box=s0.box)
-               for _ in range(64)]
+    from n2p2_b200 import Mode
     natoms = sum(x.numAtoms for x in structs)
     mode = Mode(device)
     mode.setupFromDirectory(d)
@@ -524,8 +517,7 @@ def bench_compact(steps, warmup, device, cpu=True):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
     stages = dict(b.profileStages(forces=True))
-    out = {"workload": "Anisole_SCAN model (reference example; compact types 20 + 22), 64 x 256-atom periodic boxes "
-                       "(%d atoms)" % natoms, "value": natoms / (ms / 1e3), "unit": "atoms/s", "ms_per_step": ms,
+    out = {"value": natoms / (ms / 1e3), "unit": "atoms/s", "ms_per_step": ms,
            "stages_ms": {k: round(v, 3) for k, v in stages.items()}}
     b.close()
     mode.close()
@@ -533,14 +525,54 @@ def bench_compact(steps, warmup, device, cpu=True):
         try:
             from oracle import ref
             threads = host_threads()
-            sample = structs[:max(1, min(len(structs), threads))]
+            sample = structs[:max(1, min(len(structs), cpu_sample or threads))]
             sec, _ = ref.time_batch(d, [x.to_text() for x in sample], threads, fast=True)
             n = sum(x.numAtoms for x in sample)
             out["cpu_reference"] = {"value": n / sec, "unit": "atoms/s", "cores": threads, "kind": "reference",
-                                    "sample": "%d boxes (%d atoms), reference libnnp -O3 evaluateNNP, "
+                                    "sample": "%d structures (%d atoms), reference libnnp -O3 evaluateNNP, "
                                               "structure-parallel" % (len(sample), n)}
         except Exception as exc:   # the GPU numbers stand without it
             out["cpu_reference"] = {"value": None, "sample": "failed: %s" % exc}
+    return natoms, out
+
+
+def _perturbed(s0, count, seed, sigma):
+    from n2p2_b200 import Structure
+    rng = np.random.default_rng(seed)
+    return [Structure(s0.positions + rng.normal(scale=sigma, size=s0.positions.shape), s0.elements, box=s0.box)
+            for _ in range(count)]
+
+
+def bench_compact(steps, warmup, device, cpu=True):
+    """Compact symmetry functions, FP64 energies and forces.  Headline: the
+    reference's Anisole SCAN model (331-354 functions per element, compact
+    radial 20 + wide angular 22) on 64 copies of its 256-atom periodic box
+    with seeded 0.02 displacements.  Beside it the other compact types: the
+    SCAN functions made narrow (type 21) on 16 copies of the Ethylbenzene
+    288-atom box, and the reference's QM9 settings (weighted types 23-25,
+    five elements) on 4096 molecules (its 19 fixture molecules, seeded 0.02
+    displacements)."""
+    from n2p2_b200 import read_structures
+    golden = os.path.join(ROOT, "tests", "golden")
+    d = os.path.join(golden, "examples", "Anisole_SCAN")
+    natoms, out = _compact_run(d, _perturbed(read_structures(os.path.join(d, "input.data"))[0], 64, 5, 0.02),
+                               steps, warmup, device, cpu)
+    out = {"workload": "Anisole_SCAN model (reference example; compact types 20 + 22), 64 x 256-atom periodic boxes "
+                       "(%d atoms)" % natoms, **out}
+    d = os.path.join(golden, "models", "scan_narrow")
+    natoms, o = _compact_run(d, _perturbed(read_structures(os.path.join(d, "input.data"))[0], 16, 6, 0.02),
+                             steps, warmup, device, cpu)
+    out["narrow"] = {"workload": "SCAN functions made narrow (types 20 + 21), 16 x 288-atom Ethylbenzene boxes "
+                                 "(%d atoms)" % natoms, **o}
+    d = os.path.join(golden, "models", "qm9_weighted")
+    mols = read_structures(os.path.join(d, "input.data"))
+    rng = np.random.default_rng(7)
+    picks = [mols[k] for k in rng.integers(0, len(mols), size=4096)]
+    from n2p2_b200 import Structure
+    structs = [Structure(m.positions + rng.normal(scale=0.02, size=m.positions.shape), m.elements) for m in picks]
+    natoms, o = _compact_run(d, structs, steps, warmup, device, cpu, cpu_sample=512)
+    out["weighted"] = {"workload": "QM9 settings (reference training example; weighted types 23 + 24 + 25, five "
+                                   "elements), 4096 molecules (%d atoms)" % natoms, **o}
     return out
 
 

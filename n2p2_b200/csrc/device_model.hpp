@@ -68,19 +68,22 @@ struct DevCompactMember
     int    sf;             // index of the symmetry function in its element
     int    core;           // CompactCore
     int    asym;           // asymmetric polynomial ((2 - x) x argument)
-    int    pad_;
+    int    calcComp;       // narrow angular: recompute the r_jk radial part (else carry the last one)
     double rl, rc, rCenter, rScale;
     double aLeft, aRight, aCenter, aScale;
 };
 
-// Compact members sharing (type, e1[, e2]) (SymGrpCompRad / SymGrpCompAngw).
+// Compact members sharing (type, e1[, e2]) (SymGrpCompRad / SymGrpCompAngn / SymGrpCompAngw), or
+// all members of one weighted type (SymGrpCompRadWeighted / SymGrpCompAng{n,w}Weighted).
 struct DevCompactGroup
 {
-    int    type;           // 20 radial, 22 angular wide
+    int    type;           // 20 radial, 21 angular narrow, 22 angular wide, 23 radial weighted,
+                           // 24 angular narrow weighted, 25 angular wide weighted
     int    e1, e2;
     int    memberBegin, memberCount;
     int    pad_;
-    double rmin, rmax;     // smallest lower and largest upper radial boundary of the members
+    double rmin, rmax;     // group radial window (SymGrpComp*::addMember: rmin stays 0, rmax the
+                           // largest upper boundary)
 };
 
 constexpr int kMaxBases = 4;        // exponential bases per group
@@ -140,7 +143,8 @@ struct DevModel
     const double*     weights;
     const double*     weightsT;       // weights with every matrix transposed ([n_{l-1}][n_l]), same offsets
     int numCompactGroups;
-    int pad2_;
+    int compactTypes;     // bit (type - 20) set for every compact type present
+    double atomicNumber[kDevMaxElements];   // neighbour weights of the weighted compact functions
     const DevCompactGroup*  compactGroups;
     const DevCompactMember* compactMembers;
 };

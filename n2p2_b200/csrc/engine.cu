@@ -436,21 +436,24 @@ void DeviceModel::upload(Model const& m)
             cg.e2 = g.e2;
             cg.memberBegin = (int)compactMembers.size();
             cg.memberCount = (int)g.members.size();
-            cg.rmin = 1e300;
-            cg.rmax = -1e300;
-            for (int q : g.members)
+            // SymGrpBaseComp starts rmin and rmax at 0; addMember keeps rmin at 0 (min with 0 or
+            // reset to 0) and raises rmax to the largest rc (SymGrpCompAngn.cpp:84-86)
+            cg.rmin = 0.0;
+            cg.rmax = 0.0;
+            for (std::size_t mi = 0; mi < g.members.size(); ++mi)
             {
-                SymFunc const& s = el.sf[q];
+                SymFunc const& s = el.sf[g.members[mi]];
                 DevCompactMember cm{};
                 cm.sf = s.index;
                 cm.core = s.core;
                 cm.asym = s.asymmetric ? 1 : 0;
+                cm.calcComp = g.calculateComp.at(mi);
                 // CompactFunction::setLeftRight (CompactFunction.cpp:62-76)
                 cm.rl = s.rl;
                 cm.rc = s.rc;
                 cm.rCenter = (s.rc + s.rl) / 2.0;
                 cm.rScale = 1.0 / ((s.rc - s.rl) / 2.0);
-                if (s.type != 20)
+                if (!s.radial())
                 {
                     // SymFncBaseCompAng::setParameters: the angles in radians
                     const double pi = 3.14159265358979323846;
@@ -459,7 +462,6 @@ void DeviceModel::upload(Model const& m)
                     cm.aCenter = (cm.aRight + cm.aLeft) / 2.0;
                     cm.aScale = 1.0 / ((cm.aRight - cm.aLeft) / 2.0);
                 }
-                cg.rmin = std::min(cg.rmin, s.rl);
                 cg.rmax = std::max(cg.rmax, s.rc);
                 compactMembers.push_back(cm);
             }
@@ -540,6 +542,10 @@ void DeviceModel::upload(Model const& m)
     up((void**)&compactGroups_, compactGroups.data(), compactGroups.size() * sizeof(DevCompactGroup));
     up((void**)&compactMembers_, compactMembers.data(), compactMembers.size() * sizeof(DevCompactMember));
     v.numCompactGroups = (int)compactGroups.size();
+    v.compactTypes = 0;
+    for (auto const& cg : compactGroups) v.compactTypes |= 1 << (cg.type - 20);
+    // ElementMap::atomicNumber of every element (the weights of the weighted compact functions)
+    for (std::size_t e = 0; e < m.elements.size(); ++e) v.atomicNumber[e] = (double)m.elements[e].atomicNumber;
     v.compactGroups = compactGroups_;
     v.compactMembers = compactMembers_;
     v.groups = groups_;

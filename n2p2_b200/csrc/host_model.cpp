@@ -53,10 +53,16 @@ bool sfLess(SymFunc const& a, SymFunc const& b)
     if (a.type != b.type) return a.type < b.type;
     if (a.compact())
     {
-        // SymFncCompRad / SymFncCompAngw::operator< (SymFncCompRad.cpp:50-66, SymFncCompAngw.cpp:52-74)
+        // SymFncCompRad / SymFncCompAngn / SymFncCompAngw::operator< (SymFncCompRad.cpp:50-66,
+        // SymFncCompAngn.cpp:51-74, SymFncCompAngw.cpp:52-74); the weighted types have no
+        // neighbour elements (SymFncCompRadWeighted.cpp:49-64, SymFncCompAngnWeighted.cpp:51-70,
+        // SymFncCompAngwWeighted.cpp:51-70)
         if (a.subtype != b.subtype) return a.subtype < b.subtype;
-        if (a.e1 != b.e1) return a.e1 < b.e1;
-        if (!a.radial() && a.e2 != b.e2) return a.e2 < b.e2;
+        if (!a.weighted())
+        {
+            if (a.e1 != b.e1) return a.e1 < b.e1;
+            if (!a.radial() && a.e2 != b.e2) return a.e2 < b.e2;
+        }
         if (a.rc != b.rc) return a.rc < b.rc;
         if (a.rl != b.rl) return a.rl < b.rl;
         if (!a.radial())
@@ -400,22 +406,25 @@ void Model::setupSymmetryFunctions()
             s.zetaInt = (int)std::round(s.zeta);
             s.useIntegerPow = std::fabs(s.zeta - s.zetaInt) <= std::numeric_limits<double>::min();
         }
-        else if (s.type == 20 || s.type == 22)
+        else if (s.type >= 20 && s.type <= 25)
         {
             // SymFncCompRad::setParameters (SymFncCompRad.cpp:69-99),
-            // SymFncBaseCompAng::setParameters (SymFncBaseCompAng.cpp:48-113)
-            const bool rad = s.type == 20;
-            s.e1 = elementMap.index(a.at(2));
-            s.e2 = rad ? s.e1 : elementMap.index(a.at(3));
-            const std::size_t o = rad ? 3 : 4;
+            // SymFncBaseCompAng::setParameters (SymFncBaseCompAng.cpp:48-113),
+            // SymFncCompRadWeighted::setParameters (SymFncCompRadWeighted.cpp:66-95),
+            // SymFncBaseCompAngWeighted::setParameters (SymFncBaseCompAngWeighted.cpp:43-100)
+            const bool rad = s.radial();
+            const std::size_t ne = s.weighted() ? 0 : (rad ? 1 : 2);   // neighbour element fields
+            if (ne > 0) s.e1 = elementMap.index(a.at(2));
+            s.e2 = ne == 2 ? elementMap.index(a.at(3)) : s.e1;
+            const std::size_t o = 2 + ne;
             s.rl = std::atof(a.at(o).c_str());
             s.rc = std::atof(a.at(o + 1).c_str());
             if (!rad)
             {
-                s.angleLeft = std::atof(a.at(6).c_str());
-                s.angleRight = std::atof(a.at(7).c_str());
+                s.angleLeft = std::atof(a.at(o + 2).c_str());
+                s.angleRight = std::atof(a.at(o + 3).c_str());
             }
-            s.subtype = a.at(rad ? 5 : 8);
+            s.subtype = a.at(o + (rad ? 2 : 4));
             if (!rad && s.e1 > s.e2) std::swap(s.e1, s.e2);
             if (s.rl > s.rc) throw std::runtime_error("ERROR: Lower radial boundary >= upper radial boundary.\n");
             // SymFncBaseComp::setCompactFunction (SymFncBaseComp.cpp:39-92)
@@ -454,7 +463,7 @@ void Model::setupSymmetryFunctions()
         else
         {
             throw std::runtime_error(fmt("ERROR: Symmetry function type %d is not supported by the GPU "
-                                         "short-range path (supported: 2, 3, 9, 20, 22).\n",
+                                         "short-range path (supported: 2, 3, 9, 20-25).\n",
                                          s.type));
         }
         elements.at(s.ec).sf.push_back(s);
@@ -521,11 +530,15 @@ void Model::setupSymmetryFunctionGroups()
         {
             if (s.compact())
             {
-                // SymGrpCompRad / SymGrpCompAngw::operator== (SymGrpCompRad.cpp:39-46,
-                // SymGrpCompAngw.cpp:36-44): element pair only, any radii and angles
+                // SymGrpCompRad / SymGrpCompAngn / SymGrpCompAngw::operator== (SymGrpCompRad.cpp:39-46,
+                // SymGrpCompAngn.cpp:36-44, SymGrpCompAngw.cpp:36-44): element pair only, any radii and
+                // angles; the weighted groups take every member of their type
+                // (SymGrpCompRadWeighted.cpp:37-42, SymGrpCompAngwWeighted.cpp:36-41)
                 SymGroup* cg = nullptr;
                 for (auto& cand : el.compactGroups)
-                    if (cand.type == s.type && cand.e1 == s.e1 && (s.radial() || cand.e2 == s.e2)) cg = &cand;
+                    if (cand.type == s.type &&
+                        (s.weighted() || (cand.e1 == s.e1 && (s.radial() || cand.e2 == s.e2))))
+                        cg = &cand;
                 if (!cg)
                 {
                     el.compactGroups.emplace_back();
@@ -535,8 +548,13 @@ void Model::setupSymmetryFunctionGroups()
                     cg->e1 = s.e1;
                     cg->e2 = s.e2;
                 }
+                // calculateComp: the first member and every member whose radial boundaries differ
+                // from its predecessor's (SymGrpCompAngn.cpp:110-126, SymGrpCompAngnWeighted.cpp:98-114)
+                const bool comp = cg->members.empty() || el.sf[cg->members.back()].rc != s.rc ||
+                                  el.sf[cg->members.back()].rl != s.rl;
                 cg->rc = std::max(cg->rc, s.rc);
                 cg->members.push_back(s.index);
+                cg->calculateComp.push_back(comp ? 1 : 0);
                 continue;
             }
             SymGroup* g = nullptr;

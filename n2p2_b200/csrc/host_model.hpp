@@ -55,8 +55,9 @@ enum CompactCore { CORE_EXP = CT_EXP, CORE_POLY1 = CT_POLY1, CORE_POLY2, CORE_PO
 // One symmetry function: Gaussian types 2, 3, 9 or compact types 20, 22.
 struct SymFunc
 {
-    int    type = 0;          // 2 radial, 3 angular narrow, 9 angular wide, 20 compact radial,
-                              // 22 compact angular wide
+    int    type = 0;          // 2 radial, 3 angular narrow, 9 angular wide; compact: 20 radial,
+                              // 21 angular narrow, 22 angular wide, 23 radial weighted,
+                              // 24 angular narrow weighted, 25 angular wide weighted
     int    ec = 0, e1 = 0, e2 = 0;
     double eta = 0.0, rs = 0.0, zeta = 0.0, lambda = 0.0, rc = 0.0;
     int    cutoffType = CT_HARD;
@@ -79,8 +80,11 @@ struct SymFunc
     double angleLeft = 0.0, angleRight = 0.0;   // degrees
 
     bool compact() const { return type >= 20; }
-    bool radial() const { return type == 2 || type == 20; }
-    bool relevant(int e) const { return radial() ? e == e1 : (e == e1 || e == e2); }
+    bool radial() const { return type == 2 || type == 20 || type == 23; }
+    // element-weighted compact functions (SymFncCompRadWeighted, SymFncBaseCompAngWeighted):
+    // every neighbour counts, weighted by its atomic number
+    bool weighted() const { return type >= 23; }
+    bool relevant(int e) const { return weighted() || (radial() ? e == e1 : (e == e1 || e == e2)); }
     double scale(double value) const;
     double unscale(double value) const;
 };
@@ -95,6 +99,8 @@ struct SymGroup
     double cutoffAlpha = 0.0;
     std::vector<int> members;            // SF indices of the element, member order
     std::vector<char> calculateExp;      // recompute the Gaussian for this member
+    std::vector<char> calculateComp;     // compact narrow angular: recompute the r_jk radial part
+                                         // (SymGrpCompAngn::sortMembers, SymGrpCompAngn.cpp:110-126)
     std::vector<double> factorNorm;      // 2^(1-zeta) * scalingFactor (angular)
     std::vector<double> factorDeriv;     // 2 eta / zeta / lambda (angular)
 };
@@ -113,7 +119,8 @@ struct ElementSetup
     double atomicEnergyOffset = 0.0;
     std::vector<SymFunc> sf;                       // sorted
     std::vector<SymGroup> groups;                  // Gaussian types
-    std::vector<SymGroup> compactGroups;           // compact types: (type, e1[, e2]) (SymGrpCompRad/Angw::operator==)
+    std::vector<SymGroup> compactGroups;           // compact types: (type, e1[, e2]), weighted types: (type)
+                                                   // (SymGrpComp*::operator==)
     std::vector<std::vector<int>> table;           // table[e] = SF indices with a derivative row for neighbour element e
     NetworkTopology topology;
     // weights[l] is layer l+1: W (neurons[l+1] x neurons[l], row major) then b

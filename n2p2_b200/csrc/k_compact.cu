@@ -1,16 +1,24 @@
-// Compact symmetry functions on sm_100a: radial type 20 (SymGrpCompRad,
-// SymGrpCompRad.cpp:130-245) and angular wide type 22 (SymGrpCompAngw,
-// SymGrpCompAngw.cpp:134-366), values and the force pass.
+// Compact symmetry functions on sm_100a, values and the force pass, for all
+// six compact types:
+//   20 radial                   SymGrpCompRad.cpp:130-245
+//   21 angular narrow           SymGrpCompAngn.cpp:146-410
+//   22 angular wide             SymGrpCompAngw.cpp:134-366
+//   23 radial weighted          SymGrpCompRadWeighted.cpp:122-205
+//   24 angular narrow weighted  SymGrpCompAngnWeighted.cpp:135-393
+//   25 angular wide weighted    SymGrpCompAngwWeighted.cpp:120-351
+// The weighted types take every neighbour, weighted by its atomic number
+// (the product of both for an angle); the narrow types also need the j-k
+// distance inside the radial window and multiply by its radial function.
 //
 // One warp per atom, neighbour data read from the entry arrays.  The G pass
 // sums every member over the neighbours (radial) or the unordered pairs
 // (j < k, angular) lane by lane and combines the lanes by a fixed shuffle
 // tree.  The force pass gives every lane its own neighbours: for entry j it
 // adds the force E_i puts on j over all partners k (each pair is evaluated
-// from both ends, with the roles of j and k exchanged) and its half of the
-// self force; it runs after the Gaussian force pass and adds to that pass's
-// per-entry forces h and self forces.  No atomics; the same result on every
-// run.
+// from both ends, with j in the role of the first neighbour) and its half of
+// the self force; it runs after the Gaussian force pass and adds to that
+// pass's per-entry forces h and self forces.  No atomics; the same result on
+// every run.
 #include "kernels.hpp"
 #include "kernels_common.cuh"
 
@@ -40,9 +48,19 @@ __device__ __forceinline__ void compactFdf(int core, int asym, double center, do
     df = dfx * copysign(scale, u);
 }
 
-__device__ __forceinline__ bool pairElements(DevCompactGroup const& G, int ej, int ek)
+__device__ __forceinline__ void radialFdf(DevCompactMember const& M, double r, double& f, double& df)
 {
-    return (G.e1 == ej && G.e2 == ek) || (G.e2 == ej && G.e1 == ek);
+    compactFdf(M.core, M.asym, M.rCenter, M.rScale, r, f, df);
+}
+
+// Radial part of a neighbour for a member: 0 outside (rl, rc)
+// (SymGrpCompAngn.cpp:175-197).
+__device__ __forceinline__ double windowRadial(DevCompactMember const& M, double r, double& df)
+{
+    double f = 0.0;
+    df = 0.0;
+    if (r > M.rl && r < M.rc) radialFdf(M, r, f, df);
+    return f;
 }
 
 // Angle of the pair (j, k) seen from the centre; false when cos is +-1 (the
@@ -51,7 +69,21 @@ struct PairGeom
 {
     double cost, acost, dacost, rinvij, rinvik, rinvijik, phiijik0, phiikij0;
     double dr30, dr31, dr32;
+    double rjk, rinvjk;   // narrow types only
 };
+
+// The j-k distance test of the narrow groups (SymGrpCompAngn.cpp:218-226):
+// false when it is outside the group's window.
+__device__ __forceinline__ bool pairDistance(DevCompactGroup const& G, double x1, double y1, double z1, double x2,
+                                             double y2, double z2, PairGeom& p)
+{
+    const double a = x2 - x1, b = y2 - y1, c = z2 - z1;
+    const double r2 = a * a + b * b + c * c;
+    if (r2 >= G.rmax * G.rmax || r2 <= G.rmin * G.rmin) return false;
+    p.rjk = sqrt(r2);
+    p.rinvjk = 1.0 / p.rjk;
+    return true;
+}
 
 __device__ __forceinline__ bool pairGeometry(double rij, double rik, double x1, double y1, double z1, double x2,
                                              double y2, double z2, bool derivatives, PairGeom& p)
@@ -71,7 +103,151 @@ __device__ __forceinline__ bool pairGeometry(double rij, double rik, double x1, 
     return true;
 }
 
-__global__ void __launch_bounds__(128) kCompactValues(DevModel model, BatchView b)
+// Member break conditions of the angular groups (SymGrpCompAngn.cpp:263-272,
+// SymGrpCompAngw.cpp:230-236): radFirst is the first neighbour's radial part
+// (0 outside its window), rSecond the second neighbour's distance.
+__device__ __forceinline__ bool memberSkipped(DevCompactMember const& M, bool narrow, double radFirst, double rSecond,
+                                              PairGeom const& p)
+{
+    return radFirst == 0.0 || rSecond <= M.rl || rSecond >= M.rc ||
+           (narrow && (p.rjk <= M.rl || p.rjk >= M.rc)) || p.acost <= M.aLeft || p.acost >= M.aRight;
+}
+
+// The narrow groups compute the j-k radial part only for the first member of
+// a run of equal radial boundaries, or after a skipped member, and otherwise
+// carry the last value forward (calculateComp, SymGrpCompAngn.cpp:253-296).
+struct JkCarry
+{
+    double rad = 0.0, drad = 0.0;
+    bool skip = false;
+};
+
+__device__ __forceinline__ void carryStep(DevCompactMember const& M, double rjk, JkCarry& c)
+{
+    if (M.calcComp || c.skip)
+    {
+        radialFdf(M, rjk, c.rad, c.drad);
+        c.skip = false;
+    }
+}
+
+// The carry entering member m0 of a pair, replayed from the last member
+// before it that recomputes (member 0 always does).
+__device__ __forceinline__ JkCarry carryBefore(const DevCompactMember* mem, int m0, double rFirst, double rSecond,
+                                               PairGeom const& p)
+{
+    JkCarry c;
+    if (m0 == 0 || mem[m0].calcComp) return c;
+    int s = m0 - 1;
+    while (s > 0 && !mem[s].calcComp) --s;
+    for (int l = s; l < m0; ++l)
+    {
+        DevCompactMember const& M = mem[l];
+        double df;
+        if (memberSkipped(M, true, windowRadial(M, rFirst, df), rSecond, p))
+        {
+            c.skip = true;
+            continue;
+        }
+        carryStep(M, p.rjk, c);
+    }
+    return c;
+}
+
+// G pass of one chunk of radial members (types 20, 23) over the lane's
+// neighbours.
+template <bool WEIGHTED>
+__device__ __forceinline__ void radialChunk(DevModel const& model, BatchView const& b, DevCompactGroup const& G,
+                                            const DevCompactMember* mem, int mc, int64_t off, int n, int lane,
+                                            double (&acc)[kCompactChunk])
+{
+    for (int s = lane; s < n; s += 32)
+    {
+        const int64_t e = off + s;
+        const int el = b.nbrElem[e];
+        const double d = b.nbrD[e];
+        if (!(WEIGHTED || el == G.e1) || !(d < G.rmax && d > G.rmin)) continue;
+#pragma unroll
+        for (int q = 0; q < kCompactChunk; ++q)
+        {
+            DevCompactMember const& M = mem[q];
+            if (q < mc && d > M.rl && d < M.rc)
+            {
+                double f, df;
+                radialFdf(M, d, f, df);
+                acc[q] += WEIGHTED ? model.atomicNumber[el] * f : f;
+            }
+        }
+    }
+}
+
+// G pass of one chunk of angular members (types 21, 22, 24, 25) over the
+// lane's unordered neighbour pairs (j < k).
+template <bool NARROW, bool WEIGHTED>
+__device__ __forceinline__ void angularChunk(DevModel const& model, BatchView const& b, DevCompactGroup const& G,
+                                             const DevCompactMember* mem, int m0, int mc, int64_t off, int n,
+                                             int lane, double (&acc)[kCompactChunk])
+{
+    const DevCompactMember* cm = mem + m0;
+    for (int sj = lane; sj < n - 1; sj += 32)
+    {
+        const int64_t ej = off + sj;
+        const int elj = b.nbrElem[ej];
+        const double rij = b.nbrD[ej];
+        if (!((WEIGHTED || G.e1 == elj || G.e2 == elj) && rij < G.rmax && rij > G.rmin)) continue;
+        const double x1 = b.nbrDx[ej], y1 = b.nbrDy[ej], z1 = b.nbrDz[ej];
+        double radij[kCompactChunk];
+#pragma unroll
+        for (int q = 0; q < kCompactChunk; ++q)
+        {
+            double df;
+            radij[q] = q < mc ? windowRadial(cm[q], rij, df) : 0.0;
+        }
+        for (int sk = sj + 1; sk < n; ++sk)
+        {
+            const int64_t ek = off + sk;
+            const int elk = b.nbrElem[ek];
+            if (!(WEIGHTED || (G.e1 == elj && G.e2 == elk) || (G.e2 == elj && G.e1 == elk))) continue;
+            const double rik = b.nbrD[ek];
+            if (!(rik < G.rmax && rik > G.rmin)) continue;
+            const double x2 = b.nbrDx[ek], y2 = b.nbrDy[ek], z2 = b.nbrDz[ek];
+            PairGeom p;
+            if (NARROW && !pairDistance(G, x1, y1, z1, x2, y2, z2, p)) continue;
+            if (!pairGeometry(rij, rik, x1, y1, z1, x2, y2, z2, false, p)) continue;
+            double z = 1.0;
+            if (WEIGHTED) z = model.atomicNumber[elj] * model.atomicNumber[elk];
+            JkCarry carry;
+            if (NARROW) carry = carryBefore(mem, m0, rij, rik, p);
+#pragma unroll
+            for (int q = 0; q < kCompactChunk; ++q)
+            {
+                if (q < mc)
+                {
+                    DevCompactMember const& M = cm[q];
+                    if (memberSkipped(M, NARROW, radij[q], rik, p))
+                    {
+                        carry.skip = true;
+                    }
+                    else
+                    {
+                        double radik, dradik, ang, dang;
+                        radialFdf(M, rik, radik, dradik);
+                        if (NARROW) carryStep(M, p.rjk, carry);
+                        compactFdf(M.core, 0, M.aCenter, M.aScale, p.acost, ang, dang);
+                        if (WEIGHTED) ang *= z;
+                        const double rad = NARROW ? radij[q] * radik * carry.rad : radij[q] * radik;
+                        acc[q] += rad * ang;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// One launch per compact type present: every warp walks its atoms' groups of
+// type TYPE only, so each type's kernel holds only its own state.
+template <int TYPE>
+__global__ void __launch_bounds__(128, 2) kCompactValues(DevModel model, BatchView b)
 {
     const int lane = threadIdx.x & 31;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
@@ -86,6 +262,7 @@ __global__ void __launch_bounds__(128) kCompactValues(DevModel model, BatchView 
         for (int g = 0; g < E.compactCount; ++g)
         {
             DevCompactGroup const G = model.compactGroups[E.compactBegin + g];
+            if (G.type != TYPE) continue;
             const DevCompactMember* mem = model.compactMembers + G.memberBegin;
             for (int m0 = 0; m0 < G.memberCount; m0 += kCompactChunk)
             {
@@ -93,76 +270,10 @@ __global__ void __launch_bounds__(128) kCompactValues(DevModel model, BatchView 
                 double acc[kCompactChunk];
 #pragma unroll
                 for (int q = 0; q < kCompactChunk; ++q) acc[q] = 0.0;
-                if (G.type == 20)
-                {
-                    for (int s = lane; s < n; s += 32)
-                    {
-                        const int64_t e = off + s;
-                        if (b.nbrElem[e] != G.e1) continue;
-                        const double d = b.nbrD[e];
-#pragma unroll
-                        for (int q = 0; q < kCompactChunk; ++q)
-                        {
-                            if (q >= mc) break;
-                            DevCompactMember const& M = mem[m0 + q];
-                            if (d > M.rl && d < M.rc)
-                            {
-                                double f, df;
-                                compactFdf(M.core, M.asym, M.rCenter, M.rScale, d, f, df);
-                                acc[q] += f;
-                            }
-                        }
-                    }
-                }
+                if (TYPE == 20 || TYPE == 23)
+                    radialChunk<TYPE == 23>(model, b, G, mem + m0, mc, off, n, lane, acc);
                 else
-                {
-                    for (int sj = lane; sj < n - 1; sj += 32)
-                    {
-                        const int64_t ej = off + sj;
-                        const int elj = b.nbrElem[ej];
-                        const double rij = b.nbrD[ej];
-                        if (!((G.e1 == elj || G.e2 == elj) && rij < G.rmax && rij > G.rmin)) continue;
-                        const double x1 = b.nbrDx[ej], y1 = b.nbrDy[ej], z1 = b.nbrDz[ej];
-                        double radij[kCompactChunk];
-#pragma unroll
-                        for (int q = 0; q < kCompactChunk; ++q)
-                        {
-                            radij[q] = 0.0;
-                            if (q < mc)
-                            {
-                                DevCompactMember const& M = mem[m0 + q];
-                                if (rij > M.rl && rij < M.rc)
-                                {
-                                    double df;
-                                    compactFdf(M.core, M.asym, M.rCenter, M.rScale, rij, radij[q], df);
-                                }
-                            }
-                        }
-                        for (int sk = sj + 1; sk < n; ++sk)
-                        {
-                            const int64_t ek = off + sk;
-                            if (!pairElements(G, elj, b.nbrElem[ek])) continue;
-                            const double rik = b.nbrD[ek];
-                            if (!(rik < G.rmax && rik > G.rmin)) continue;
-                            PairGeom p;
-                            if (!pairGeometry(rij, rik, x1, y1, z1, b.nbrDx[ek], b.nbrDy[ek], b.nbrDz[ek], false, p))
-                                continue;
-#pragma unroll
-                            for (int q = 0; q < kCompactChunk; ++q)
-                            {
-                                if (q >= mc) break;
-                                DevCompactMember const& M = mem[m0 + q];
-                                if (radij[q] == 0.0 || rik <= M.rl || rik >= M.rc || p.acost <= M.aLeft ||
-                                    p.acost >= M.aRight)
-                                    continue;
-                                double radik, dradik, ang, dang;
-                                compactFdf(M.core, M.asym, M.rCenter, M.rScale, rik, radik, dradik);
-                                compactFdf(M.core, 0, M.aCenter, M.aScale, p.acost, ang, dang);
-                                acc[q] += radij[q] * radik * ang;
-                            }
-                        }
-                    }
-                }
+                    angularChunk<TYPE == 21 || TYPE == 24, TYPE >= 24>(model, b, G, mem, m0, mc, off, n, lane, acc);
 #pragma unroll
                 for (int q = 0; q < kCompactChunk; ++q)
                 {
@@ -178,7 +289,126 @@ __global__ void __launch_bounds__(128) kCompactValues(DevModel model, BatchView 
     }
 }
 
-__global__ void __launch_bounds__(128) kCompactForces(DevModel model, BatchView b)
+struct ForceAcc
+{
+    double hx = 0.0, hy = 0.0, hz = 0.0;   // force E_i puts on the lane's neighbour j
+    double sx = 0.0, sy = 0.0, sz = 0.0;   // the lane's share of the self force
+};
+
+// Force pass of a radial group (types 20, 23) for neighbour j: p1 =
+// scalingFactor drad / rij (SymGrpCompRad.cpp:176), times the atomic number
+// for the weighted type (SymGrpCompRadWeighted.cpp:163).
+template <bool WEIGHTED>
+__device__ __forceinline__ void radialForces(DevModel const& model, DevElement const& E, DevCompactGroup const& G,
+                                             const DevCompactMember* mem, const double* dEdG, int elj, double rij,
+                                             double x1, double y1, double z1, ForceAcc& a)
+{
+    if (!(WEIGHTED || elj == G.e1) || !(rij < G.rmax && rij > G.rmin)) return;
+    for (int q = 0; q < G.memberCount; ++q)
+    {
+        DevCompactMember const& M = mem[q];
+        if (!(rij > M.rl && rij < M.rc)) continue;
+        double f, df;
+        radialFdf(M, rij, f, df);
+        const double sfac = model.scaling[E.sfBegin + M.sf].scalingFactor;
+        const double c = dEdG[M.sf] * (df * ((WEIGHTED ? model.atomicNumber[elj] * sfac : sfac) / rij));
+        a.hx += c * x1;
+        a.hy += c * y1;
+        a.hz += c * z1;
+        a.sx -= c * x1;
+        a.sy -= c * y1;
+        a.sz -= c * z1;
+    }
+}
+
+// Force pass of an angular group (types 21, 22, 24, 25) for neighbour j over
+// all partners k, with j in the role of the first neighbour
+// (SymGrpCompAngn.cpp:298-338, SymGrpCompAngw.cpp:265-299).
+template <bool NARROW, bool WEIGHTED>
+__device__ __forceinline__ void angularForces(DevModel const& model, BatchView const& b, DevElement const& E,
+                                              DevCompactGroup const& G, const DevCompactMember* mem,
+                                              const double* dEdG, int64_t off, int n, int sj, int elj, double rij,
+                                              double x1, double y1, double z1, ForceAcc& a)
+{
+    if (!((WEIGHTED || G.e1 == elj || G.e2 == elj) && rij < G.rmax && rij > G.rmin)) return;
+    for (int sk = 0; sk < n; ++sk)
+    {
+        if (sk == sj) continue;
+        const int64_t ek = off + sk;
+        const int elk = b.nbrElem[ek];
+        if (!(WEIGHTED || (G.e1 == elj && G.e2 == elk) || (G.e2 == elj && G.e1 == elk))) continue;
+        const double rik = b.nbrD[ek];
+        if (!(rik < G.rmax && rik > G.rmin)) continue;
+        const double x2 = b.nbrDx[ek], y2 = b.nbrDy[ek], z2 = b.nbrDz[ek];
+        PairGeom p;
+        if (NARROW && !pairDistance(G, x1, y1, z1, x2, y2, z2, p)) continue;
+        if (!pairGeometry(rij, rik, x1, y1, z1, x2, y2, z2, true, p)) continue;
+        double z = 1.0;
+        if (WEIGHTED) z = model.atomicNumber[elj] * model.atomicNumber[elk];
+        // the reference visits the pair with the lower neighbour index first: its break test
+        // reads that neighbour's radial value
+        const bool ownFirst = sj < sk;
+        JkCarry carry;
+        for (int q = 0; q < G.memberCount; ++q)
+        {
+            DevCompactMember const& M = mem[q];
+            // windows first; then the first neighbour's radial value must not vanish
+            if (!(rij > M.rl && rij < M.rc) || !(rik > M.rl && rik < M.rc) ||
+                (NARROW && (p.rjk <= M.rl || p.rjk >= M.rc)) || p.acost <= M.aLeft || p.acost >= M.aRight)
+            {
+                carry.skip = true;
+                continue;
+            }
+            double radij, dradij, radik, dradik;
+            radialFdf(M, rij, radij, dradij);
+            radialFdf(M, rik, radik, dradik);
+            if ((ownFirst ? radij : radik) == 0.0)
+            {
+                carry.skip = true;
+                continue;
+            }
+            if (NARROW) carryStep(M, p.rjk, carry);
+            double ang, dang;
+            compactFdf(M.core, 0, M.aCenter, M.aScale, p.acost, ang, dang);
+            if (WEIGHTED) ang *= z;
+            const double sfac = model.scaling[E.sfBegin + M.sf].scalingFactor;
+            double rad = NARROW ? radij * radik * carry.rad : radij * radik;
+            dang *= p.dacost;
+            const double phiijik = p.phiijik0 * dang;
+            const double psiijik = p.rinvijik * dang;
+            const double chiij = NARROW ? p.rinvij * dradij * radik * carry.rad : p.rinvij * radik * dradij;
+            const double chijk = NARROW ? -p.rinvjk * radij * radik * carry.drad : 0.0;
+            double p1, p3;
+            if (dang != 0.0 && rad != 0.0)
+            {
+                rad *= sfac * z;
+                ang *= sfac;
+                p1 = rad * phiijik + ang * chiij;
+                p3 = NARROW ? rad * psiijik + ang * chijk : rad * psiijik;
+            }
+            else if (ang != 0.0)
+            {
+                ang *= sfac;
+                p1 = ang * chiij;
+                p3 = NARROW ? ang * chijk : 0.0;
+            }
+            else continue;
+            // j: -dE/dr_j = dE/dG (p1 dr_ij + p3 dr_jk); the centre's share: -dE/dG p1 dr_ij
+            const double w = dEdG[M.sf];
+            a.hx += w * (p1 * x1 + p3 * p.dr30);
+            a.hy += w * (p1 * y1 + p3 * p.dr31);
+            a.hz += w * (p1 * z1 + p3 * p.dr32);
+            a.sx -= w * p1 * x1;
+            a.sy -= w * p1 * y1;
+            a.sz -= w * p1 * z1;
+        }
+    }
+}
+
+// One launch per compact type present, in type order after the Gaussian
+// force pass; each adds its share to the per-entry and self forces.
+template <int TYPE>
+__global__ void __launch_bounds__(128, 2) kCompactForces(DevModel model, BatchView b)
 {
     const int lane = threadIdx.x & 31;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
@@ -191,102 +421,36 @@ __global__ void __launch_bounds__(128) kCompactForces(DevModel model, BatchView 
         if (end > b.nbrCapacity) continue;
         const int n = (int)(end - off);
         const double* dEdG = b.dEdG + (size_t)i * b.gStride;
-        double sx = 0.0, sy = 0.0, sz = 0.0;
+        ForceAcc a;
         for (int sj = lane; sj < n; sj += 32)
         {
             const int64_t ej = off + sj;
             const int elj = b.nbrElem[ej];
             const double rij = b.nbrD[ej];
             const double x1 = b.nbrDx[ej], y1 = b.nbrDy[ej], z1 = b.nbrDz[ej];
-            double hx = 0.0, hy = 0.0, hz = 0.0;   // force E_i puts on j
+            a.hx = a.hy = a.hz = 0.0;
             for (int g = 0; g < E.compactCount; ++g)
             {
                 DevCompactGroup const G = model.compactGroups[E.compactBegin + g];
+                if (G.type != TYPE) continue;
                 const DevCompactMember* mem = model.compactMembers + G.memberBegin;
-                if (G.type == 20)
-                {
-                    if (elj != G.e1) continue;
-                    for (int q = 0; q < G.memberCount; ++q)
-                    {
-                        DevCompactMember const& M = mem[q];
-                        if (!(rij > M.rl && rij < M.rc)) continue;
-                        double f, df;
-                        compactFdf(M.core, M.asym, M.rCenter, M.rScale, rij, f, df);
-                        // p1 = scalingFactor drad / rij (SymFncCompRad.cpp:183-190)
-                        const double c = dEdG[M.sf] * (model.scaling[E.sfBegin + M.sf].scalingFactor * df / rij);
-                        hx += c * x1;
-                        hy += c * y1;
-                        hz += c * z1;
-                        sx -= c * x1;
-                        sy -= c * y1;
-                        sz -= c * z1;
-                    }
-                    continue;
-                }
-                if (!((G.e1 == elj || G.e2 == elj) && rij < G.rmax && rij > G.rmin)) continue;
-                for (int sk = 0; sk < n; ++sk)
-                {
-                    if (sk == sj) continue;
-                    const int64_t ek = off + sk;
-                    if (!pairElements(G, elj, b.nbrElem[ek])) continue;
-                    const double rik = b.nbrD[ek];
-                    if (!(rik < G.rmax && rik > G.rmin)) continue;
-                    PairGeom p;
-                    if (!pairGeometry(rij, rik, x1, y1, z1, b.nbrDx[ek], b.nbrDy[ek], b.nbrDz[ek], true, p)) continue;
-                    for (int q = 0; q < G.memberCount; ++q)
-                    {
-                        DevCompactMember const& M = mem[q];
-                        if (!(rij > M.rl && rij < M.rc)) continue;   // radij == 0
-                        if (rik <= M.rl || rik >= M.rc || p.acost <= M.aLeft || p.acost >= M.aRight) continue;
-                        double radij, dradij, radik, dradik, ang, dang;
-                        compactFdf(M.core, M.asym, M.rCenter, M.rScale, rij, radij, dradij);
-                        if (radij == 0.0) continue;
-                        compactFdf(M.core, M.asym, M.rCenter, M.rScale, rik, radik, dradik);
-                        compactFdf(M.core, 0, M.aCenter, M.aScale, p.acost, ang, dang);
-                        // SymGrpCompAngw.cpp:265-299, with j in the role of the first neighbour
-                        const double sf = model.scaling[E.sfBegin + M.sf].scalingFactor;
-                        double rad = radij * radik;
-                        dang *= p.dacost;
-                        const double phiijik = p.phiijik0 * dang;
-                        const double psiijik = p.rinvijik * dang;
-                        const double chiij = p.rinvij * radik * dradij;
-                        double p1, p3;
-                        if (dang != 0.0 && rad != 0.0)
-                        {
-                            rad *= sf;
-                            ang *= sf;
-                            p1 = rad * phiijik + ang * chiij;
-                            p3 = rad * psiijik;
-                        }
-                        else if (ang != 0.0)
-                        {
-                            ang *= sf;
-                            p1 = ang * chiij;
-                            p3 = 0.0;
-                        }
-                        else continue;
-                        // j: -dE/dr_j = dE/dG (p1 dr_ij + p3 dr_jk); the centre's share: -dE/dG p1 dr_ij
-                        const double a = dEdG[M.sf];
-                        hx += a * (p1 * x1 + p3 * p.dr30);
-                        hy += a * (p1 * y1 + p3 * p.dr31);
-                        hz += a * (p1 * z1 + p3 * p.dr32);
-                        sx -= a * p1 * x1;
-                        sy -= a * p1 * y1;
-                        sz -= a * p1 * z1;
-                    }
-                }
+                if (TYPE == 20 || TYPE == 23)
+                    radialForces<TYPE == 23>(model, E, G, mem, dEdG, elj, rij, x1, y1, z1, a);
+                else
+                    angularForces<TYPE == 21 || TYPE == 24, TYPE >= 24>(model, b, E, G, mem, dEdG, off, n, sj, elj,
+                                                                        rij, x1, y1, z1, a);
             }
-            if (hx != 0.0 || hy != 0.0 || hz != 0.0)
+            if (a.hx != 0.0 || a.hy != 0.0 || a.hz != 0.0)
             {
-                b.hx[ej] += hx;
-                b.hy[ej] += hy;
-                b.hz[ej] += hz;
+                b.hx[ej] += a.hx;
+                b.hy[ej] += a.hy;
+                b.hz[ej] += a.hz;
             }
         }
-        sx = warpSum(sx);
-        sy = warpSum(sy);
-        sz = warpSum(sz);
-        if (lane == 0)
+        const double sx = warpSum(a.sx);
+        const double sy = warpSum(a.sy);
+        const double sz = warpSum(a.sz);
+        if (lane == 0 && (sx != 0.0 || sy != 0.0 || sz != 0.0))
         {
             b.fSelf[3 * (size_t)i + 0] += sx;
             b.fSelf[3 * (size_t)i + 1] += sy;
@@ -297,20 +461,38 @@ __global__ void __launch_bounds__(128) kCompactForces(DevModel model, BatchView 
 
 } // namespace
 
-void launchCompactValues(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
+namespace {
+
+int compactBlocks(BatchView const& b, int sms)
 {
     int blocks = (b.N + 3) / 4;
     if (blocks < 1) blocks = 1;
     if (blocks > sms * 16) blocks = sms * 16;
-    kCompactValues<<<blocks, 128, 0, st>>>(m, b);
+    return blocks;
+}
+
+} // namespace
+
+void launchCompactValues(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
+{
+    const int blocks = compactBlocks(b, sms);
+    if (m.compactTypes & (1 << 0)) kCompactValues<20><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 1)) kCompactValues<21><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 2)) kCompactValues<22><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 3)) kCompactValues<23><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 4)) kCompactValues<24><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 5)) kCompactValues<25><<<blocks, 128, 0, st>>>(m, b);
 }
 
 void launchCompactForces(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
 {
-    int blocks = (b.N + 3) / 4;
-    if (blocks < 1) blocks = 1;
-    if (blocks > sms * 16) blocks = sms * 16;
-    kCompactForces<<<blocks, 128, 0, st>>>(m, b);
+    const int blocks = compactBlocks(b, sms);
+    if (m.compactTypes & (1 << 0)) kCompactForces<20><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 1)) kCompactForces<21><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 2)) kCompactForces<22><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 3)) kCompactForces<23><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 4)) kCompactForces<24><<<blocks, 128, 0, st>>>(m, b);
+    if (m.compactTypes & (1 << 5)) kCompactForces<25><<<blocks, 128, 0, st>>>(m, b);
 }
 
 } // namespace n2p2b200

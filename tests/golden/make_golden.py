@@ -38,6 +38,22 @@ It writes
                           labels those configurations, and with the single box
                           alone they extrapolate to forces of 1e4 Ha/bohr.
   water40_box64.json      reference energy and forces of the 64-molecule box.
+  models/qm9_weighted/    the reference's QM9 training settings
+                          (examples/nnp-train/QM9/input.nn: weighted compact
+                          types 23, 24, 25 on five elements) with its first 16
+                          molecules and three more holding fluorine, seeded
+                          random weights and scaling
+                          statistics from the reference library over them
+                          (functions constant over the sample get a unit
+                          range and sigma).
+  models/scan_narrow/     the Ethylbenzene_SCAN functions with every wide
+                          angular function (22) turned narrow (21), plus two
+                          "p1" members per group whose radial window equals
+                          that of the first "p2" member (the reference then
+                          carries the j-k radial part across the subtype
+                          boundary); the example frame plus three copies with
+                          0.02 displacements, seeded weights, reference
+                          scaling.
 
 The reference library is oracle/_ref/libnnpref.so (built by oracle/Makefile).
 """
@@ -112,14 +128,129 @@ def write_model(dirname, sf_lines, nodes, seed, stats_structures):
     water.write_scaling(os.path.join(dirname, "scaling.data"), stats)
 
 
+SCALING_KEYS = ("scale_symmetry_functions", "center_symmetry_functions", "scale_symmetry_functions_sigma",
+                "scale_min_short", "scale_max_short")
+
+
+def _sf_counts(input_nn):
+    """Symmetry functions per element symbol of a settings text."""
+    counts = {}
+    for line in input_nn.splitlines():
+        w = line.split("#")[0].split()
+        if w and w[0] == "symfunction_short":
+            counts[w[1]] = counts.get(w[1], 0) + 1
+    return counts
+
+
+def _settings_value(input_nn, key):
+    for line in input_nn.splitlines():
+        w = line.split("#")[0].split()
+        if w and w[0] == key:
+            return w[1:]
+    raise KeyError(key)
+
+
+def write_derived_model(dirname, input_nn, structures, seed):
+    """A model directory from a settings text: seeded random weights
+    (N(0, 1/fan_in), zero biases), scaling.data from the reference library's
+    unscaled G over `structures` (the nnp-scaling statistics), input.data with
+    the structures."""
+    os.makedirs(dirname, exist_ok=True)
+    with open(os.path.join(dirname, "input.nn"), "w") as f:
+        f.write(input_nn)
+    with open(os.path.join(dirname, "input.data"), "w") as f:
+        for st in structures:
+            f.write(st.to_text())
+    symbols = _settings_value(input_nn, "elements")
+    nodes = [int(x) for x in _settings_value(input_nn, "global_nodes_short")]
+    counts = _sf_counts(input_nn)
+    z = {sym: atomic_number(sym) for sym in symbols}
+    order = sorted(symbols, key=lambda e: z[e])
+    rng = np.random.default_rng(seed)
+    for sym in order:
+        water.write_weights(os.path.join(dirname, "weights.%03d.data" % z[sym]),
+                            water.random_weights([counts[sym], *nodes, 1], rng))
+    with tempfile.TemporaryDirectory() as tmp:
+        plain = "\n".join(l for l in input_nn.splitlines()
+                          if not (l.split() and l.split()[0] in SCALING_KEYS)) + "\n"
+        with open(os.path.join(tmp, "input.nn"), "w") as f:
+            f.write(plain)
+        for sym in order:
+            shutil.copy(os.path.join(dirname, "weights.%03d.data" % z[sym]), tmp)
+        water.write_scaling(os.path.join(tmp, "scaling.data"), [np.zeros((counts[e], 4)) for e in order])
+        p = ref.RefPrediction(tmp)
+        G = {e: [] for e in order}
+        for st in structures:
+            p.predict(st.to_text(), use_forces=False)
+            g = p.arrays()["G"]
+            k = 0
+            for sym in st.elements:
+                G[sym].append(g[k:k + counts[sym]])
+                k += counts[sym]
+        p.close()
+    with np.errstate(invalid="ignore", divide="ignore"):   # QM9 holds a single F atom: no sigma
+        stats = water.scaling_statistics([np.array(G[e]) for e in order])
+    for st in stats:   # functions constant over the sample get a unit range and sigma (finite scaling)
+        flat = ~(st[:, 1] > st[:, 0])
+        st[flat, 1] = st[flat, 0] + 1.0
+        bad = ~(np.isfinite(st[:, 3]) & (st[:, 3] > 0.0))
+        st[bad, 3] = 1.0
+    water.write_scaling(os.path.join(dirname, "scaling.data"), stats)
+
+
+def atomic_number(symbol):
+    return {"H": 1, "C": 6, "N": 7, "O": 8, "F": 9, "S": 16, "Cu": 29}[symbol]
+
+
+def compact_models(refdir):
+    """The weighted (QM9) and narrow (from Ethylbenzene_SCAN) compact models."""
+    from n2p2_b200 import read_structures
+    qdir = os.path.join(refdir, "examples/nnp-train/QM9")
+    text = open(os.path.join(qdir, "input.nn")).read()
+    allm = read_structures(os.path.join(qdir, "input.data"))
+    mols = allm[:16]
+    for sym in _settings_value(text, "elements"):   # every element present (F is rare)
+        if not any(sym in m.elements for m in mols):
+            mols += [m for m in allm[16:] if sym in m.elements][:3]
+    write_derived_model(os.path.join(HERE, "models", "qm9_weighted"), text, mols, 2024)
+
+    edir = os.path.join(HERE, "examples", "Ethylbenzene_SCAN")
+    lines = []
+    extra = []
+    for line in open(os.path.join(edir, "input.nn")).read().splitlines():
+        w = line.split()
+        if w and w[0] == "symfunction_short" and w[2] == "22":
+            w[2] = "21"
+            line = " ".join(w)
+            key = (w[1], w[3], w[4])
+            if key not in [k for k, _ in extra]:
+                for al, ar in (("-90.00", "90.00"), ("0.00", "180.00")):
+                    extra.append((key, "symfunction_short %s 21 %s %s -1.50E+01 1.50E+01 %s %s p1"
+                                  % (key[0], key[1], key[2], al, ar)))
+        lines.append(line)
+    text = "\n".join(lines + [x for _, x in extra]) + "\n"
+    frame = read_structures(os.path.join(edir, "input.data"))[0]
+    frames = [frame]
+    for k in range(3):
+        c = read_structures(os.path.join(edir, "input.data"))[0]
+        c.positions = c.positions + np.random.default_rng(40 + k).normal(0.0, 0.02, c.positions.shape)
+        frames.append(c)
+    write_derived_model(os.path.join(HERE, "models", "scan_narrow"), text, frames, 2025)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--examples-only", action="store_true", help="copy the reference examples and their goldens only")
+    ap.add_argument("--compact-only", action="store_true", help="write the derived compact-function models only")
     args = ap.parse_args()
     refdir = args.reference
     if not ref.available():
         sys.exit("oracle/_ref/libnnpref.so missing: run `make -C oracle`")
+
+    if args.compact_only:
+        compact_models(refdir)
+        return
 
     src = open(os.path.join(refdir, "test/cpp/ExamplePrediction.h")).read()
     for name in EXAMPLES:
@@ -136,6 +267,7 @@ def main():
 
     if args.examples_only:
         return
+    compact_models(refdir)
 
     csrc = open(os.path.join(refdir, "test/cpp/test_CutoffFunction.cpp")).read()
     with open(os.path.join(HERE, "cutoff_functions.json"), "w") as fh:

@@ -89,6 +89,50 @@ def unscaled(model_dir, structure, G):
     return out
 
 
+ATOMIC_NUMBERS = {"H": 1, "He": 2, "Li": 3, "C": 6, "N": 7, "O": 8, "F": 9, "S": 16, "Cu": 29}
+
+
+def unscaled_from_files(model_dir, structure, G):
+    """Raw G of a concatenated scaled G array, from the model's own
+    input.nn scaling keywords (Mode::setupSymmetryFunctionScaling,
+    Mode.cpp:794-830) and scaling.data rows (elements by atomic number, SFs
+    in sorted order), undone as SymFnc::unscale (SymFnc.cpp:197-223)."""
+    keys, elements = {}, []
+    for line in open(os.path.join(model_dir, "input.nn")):
+        w = line.split("#")[0].split()
+        if w:
+            keys[w[0]] = w[1:]
+            if w[0] == "elements":
+                elements = w[1:]
+    smin = float(keys["scale_min_short"][0]) if "scale_min_short" in keys else 0.0
+    smax = float(keys["scale_max_short"][0]) if "scale_max_short" in keys else 1.0
+    sc, ce, sg = ("scale_symmetry_functions" in keys, "center_symmetry_functions" in keys,
+                  "scale_symmetry_functions_sigma" in keys)
+    rows = np.loadtxt(os.path.join(model_dir, "scaling.data"), ndmin=2)
+    order = sorted(elements, key=lambda e: ATOMIC_NUMBERS[e])
+    table = {sym: rows[rows[:, 0] == k + 1] for k, sym in enumerate(order)}
+    out = np.empty_like(G)
+    k = 0
+    for sym in structure.elements:
+        t = table[sym]
+        v = G[k:k + len(t)]
+        gmin, gmax, gmean, gsig = t[:, 2], t[:, 3], t[:, 4], t[:, 5]
+        if sc and ce:
+            u = (v - smin) / ((smax - smin) / (gmax - gmin)) + gmean
+        elif sc:
+            u = (v - smin) / ((smax - smin) / (gmax - gmin)) + gmin
+        elif ce:
+            u = v + gmean
+        elif sg:
+            u = (v - smin) / ((smax - smin) / gsig) + gmean
+        else:
+            u = v
+        out[k:k + len(t)] = u
+        k += len(t)
+    assert k == G.size
+    return out
+
+
 def reference_noise(model_dir, structure):
     """Relative force and energy spread between the reference built with FMA
     contraction (-O3, x86-64-v3) and without (-O2, -ffp-contract=off): the

@@ -69,7 +69,7 @@ def test_unsupported_generation_and_types_are_rejected():
     m2 = Mode(0)
     m2.loadSettingsFile(_settings("number_of_elements 1\nelements H\ncutoff_type 2\n"
                                   "global_hidden_layers_short 1\nglobal_nodes_short 2\n"
-                                  "global_activation_short t l\nsymfunction_short H 21 H H 0.0 5.0 0.0 180.0 p2\n"))
+                                  "global_activation_short t l\nsymfunction_short H 12 0.5 0.0 5.0\n"))
     with pytest.raises(_lib.N2P2Error) as e:
         m2.setupGeneric()
     assert "not supported" in str(e.value)
@@ -119,12 +119,14 @@ def test_water_generator_recipe():
 
 
 @pytest.mark.skipif(not oref.available(), reason="reference library not built")
-@pytest.mark.parametrize("name", ["Anisole_SCAN", "DMABN_SCAN", "Ethylbenzene_SCAN"])
+@pytest.mark.parametrize("name", ["examples/Anisole_SCAN", "examples/DMABN_SCAN", "examples/Ethylbenzene_SCAN",
+                                  "models/qm9_weighted", "models/scan_narrow"])
 def test_compact_models_set_up_like_the_reference(name):
-    """Compact symmetry functions (types 20, 22): per element the number of
-    functions, the derivative rows per neighbour element and the largest
-    cutoff equal the reference library's set-up of the same files."""
-    d = os.path.join(H.GOLDEN, "examples", name)
+    """Compact symmetry functions (types 20-25): per element the number of
+    functions, the derivative rows per neighbour element (every element for
+    the weighted types) and the largest cutoff equal the reference library's
+    set-up of the same files."""
+    d = os.path.join(H.GOLDEN, name)
     m = Mode(0)
     m.setupFromDirectory(d)
     r = oref.RefPrediction(d)
