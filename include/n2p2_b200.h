@@ -56,6 +56,7 @@ typedef int n2p2_status;
 typedef struct n2p2_mode n2p2_mode;
 typedef struct n2p2_batch n2p2_batch;
 typedef struct n2p2_trainer n2p2_trainer;
+typedef struct n2p2_training n2p2_training;
 typedef struct n2p2_lammps n2p2_lammps;
 typedef struct n2p2_structures n2p2_structures;
 
@@ -355,6 +356,56 @@ n2p2_status n2p2_trainer_set_parameters(n2p2_trainer* trainer, const double* par
  * (weight-file order) are written when the pointers are not NULL. */
 n2p2_status n2p2_trainer_step(n2p2_trainer* trainer, n2p2_batch* batch, const double* energies,
                               const double* forces, int32_t update, double* loss, double* gradient);
+
+/* ---- training updates (libnnptrain Training::update, KalmanFilter,
+ * GradientDescent) -----------------------------------------------------------
+ * Replaces the update loop of the reference's nnp-train
+ * (src/libnnptrain/Training.cpp:2256-3169) for the 2G networks with the
+ * combined update strategy and one update candidate per update (observation
+ * size 1), and its updaters (KalmanFilter.cpp:126-238,
+ * GradientDescent.cpp:81-118).  The training set is the batch's structures:
+ * their symmetry functions and dG/dr are computed at creation and stay on the
+ * device; the networks' weights are the mode's device weights, which the
+ * updates change in place (every later evaluation of the mode's batches uses
+ * them). */
+#define N2P2_TRAINING_ENERGY 0
+#define N2P2_TRAINING_FORCE 1
+n2p2_status n2p2_training_create(n2p2_batch* set, n2p2_training** training);
+n2p2_status n2p2_training_destroy(n2p2_training* training);
+/* energies[S] (physical units, with offsets) and forces[N][3]: the references
+ * of the set's structures (Structure::energyRef, Atom::fRef). */
+n2p2_status n2p2_training_set_references(n2p2_training* training, const double* energies, const double* forces);
+/* force_weight (Training.cpp:2910-2923): scales force errors and Jacobians. */
+n2p2_status n2p2_training_set_force_weight(n2p2_training* training, double weight);
+/* KalmanFilter::setParametersStandard / setParametersFadingMemory (P = I / epsilon). */
+n2p2_status n2p2_training_set_kalman_standard(n2p2_training* training, double epsilon, double q0, double qtau,
+                                              double qmin, double eta0, double etatau, double etamax);
+n2p2_status n2p2_training_set_kalman_fading_memory(n2p2_training* training, double epsilon, double q0, double qtau,
+                                                   double qmin, double lambda, double nu);
+/* GradientDescent::setParametersFixed / setParametersAdam. */
+n2p2_status n2p2_training_set_gradient_fixed(n2p2_training* training, double eta);
+n2p2_status n2p2_training_set_gradient_adam(n2p2_training* training, double eta, double beta1, double beta2,
+                                            double epsilon);
+/* `count` updates in order.  property N2P2_TRAINING_ENERGY: the energy of
+ * structure[k]; N2P2_TRAINING_FORCE: component component[k] (0..2) of atom
+ * atom[k] (index inside the structure) of structure[k]; atom and component
+ * may be NULL for energy updates.  errors[k] (optional): reference minus
+ * prediction before update k, internal units. */
+n2p2_status n2p2_training_update(n2p2_training* training, int32_t property, int32_t count, const int32_t* structure,
+                                 const int32_t* atom, const int32_t* component, double* errors);
+/* The error (reference minus prediction, internal units) and Jacobian
+ * (weight-file order; the force weight applied to force observations) of one
+ * observation at the current weights, without an update: the quantities
+ * Training::update hands to its updater. */
+n2p2_status n2p2_training_observe(n2p2_training* training, int32_t property, int32_t structure, int32_t atom,
+                                  int32_t component, double* error, double* jacobian);
+/* KalmanFilter::status: {numUpdates, mean |P_ii|, mean |P_ij| (i != j),
+ * mean |K|, q, eta (standard) or lambda (fading memory), gamma}. */
+n2p2_status n2p2_training_get_kalman_status(n2p2_training* training, double* status);
+n2p2_status n2p2_training_get_num_weights(n2p2_training* training, int64_t* count);
+/* All elements' connections, weight-file order (NeuralNetwork::getConnections). */
+n2p2_status n2p2_training_get_weights(n2p2_training* training, double* weights);
+n2p2_status n2p2_training_set_weights(n2p2_training* training, const double* weights);
 
 /* ---- autotuning (no counterpart in the reference) -------------------------
  * The symmetry-function passes run their first tier of atoms with one of

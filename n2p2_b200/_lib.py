@@ -25,6 +25,9 @@ EVAL_STORE_DGDR = 2
 EVAL_NO_GRAPH = 4
 EVAL_SF_ONLY = 8
 
+TRAINING_ENERGY = 0
+TRAINING_FORCE = 1
+
 # Every function the header declares, with (restype, argtypes).
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -90,6 +93,22 @@ SIGNATURES = {
     "n2p2_trainer_get_parameters": (_i, [_vp, _P(_d)]),
     "n2p2_trainer_set_parameters": (_i, [_vp, _P(_d)]),
     "n2p2_trainer_step": (_i, [_vp, _vp, _P(_d), _P(_d), ctypes.c_int32, _P(_d), _P(_d)]),
+    "n2p2_training_create": (_i, [_vp, _P(_vp)]),
+    "n2p2_training_destroy": (_i, [_vp]),
+    "n2p2_training_set_references": (_i, [_vp, _P(_d), _P(_d)]),
+    "n2p2_training_set_force_weight": (_i, [_vp, _d]),
+    "n2p2_training_set_kalman_standard": (_i, [_vp, _d, _d, _d, _d, _d, _d, _d]),
+    "n2p2_training_set_kalman_fading_memory": (_i, [_vp, _d, _d, _d, _d, _d, _d]),
+    "n2p2_training_set_gradient_fixed": (_i, [_vp, _d]),
+    "n2p2_training_set_gradient_adam": (_i, [_vp, _d, _d, _d, _d]),
+    "n2p2_training_update": (_i, [_vp, ctypes.c_int32, ctypes.c_int32, _P(ctypes.c_int32), _P(ctypes.c_int32),
+                                  _P(ctypes.c_int32), _P(_d)]),
+    "n2p2_training_observe": (_i, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P(_d),
+                                   _P(_d)]),
+    "n2p2_training_get_kalman_status": (_i, [_vp, _P(_d)]),
+    "n2p2_training_get_num_weights": (_i, [_vp, _P(_i64)]),
+    "n2p2_training_get_weights": (_i, [_vp, _P(_d)]),
+    "n2p2_training_set_weights": (_i, [_vp, _P(_d)]),
     "n2p2_lammps_create": (_i, [_P(_vp), _i]),
     "n2p2_lammps_destroy": (_i, [_vp]),
     "n2p2_lammps_initialize": (_i, [_vp, _cp, _cp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

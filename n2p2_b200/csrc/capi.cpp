@@ -41,6 +41,13 @@ struct n2p2_trainer
     std::unique_ptr<Trainer> trainer;
 };
 
+struct n2p2_training
+{
+    n2p2_mode* mode = nullptr;
+    n2p2_batch* set = nullptr;
+    std::unique_ptr<Training> training;
+};
+
 struct n2p2_lammps
 {
     n2p2_mode mode;                  // the model, its device copy and the stream
@@ -780,6 +787,157 @@ n2p2_status n2p2_trainer_step(n2p2_trainer* trainer, n2p2_batch* batch, const do
         if (!trainer->mode->uploaded) throw std::runtime_error("ERROR: the mode was changed after the trainer was created.\n");
         trainer->trainer->step(*batch->batch, energies, forces, update != 0, loss, gradient);
         if (update) trainer->trainer->syncHostModel(trainer->mode->stream);
+    });
+}
+
+n2p2_status n2p2_training_create(n2p2_batch* set, n2p2_training** training)
+{
+    N2P2_REQUIRE(set);
+    N2P2_REQUIRE(training);
+    return guard([&] {
+        setDevice(set->mode);
+        ensureUploaded(set->mode);
+        auto t = std::make_unique<n2p2_training>();
+        t->mode = set->mode;
+        t->set = set;
+        t->training = std::make_unique<Training>(set->mode->model, set->mode->dmodel, *set->batch, set->mode->sms);
+        *training = t.release();
+    });
+}
+
+n2p2_status n2p2_training_destroy(n2p2_training* training)
+{
+    if (!training) return N2P2_OK;
+    return guard([&] {
+        setDevice(training->mode);
+        delete training;
+    });
+}
+
+n2p2_status n2p2_training_set_references(n2p2_training* training, const double* energies, const double* forces)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(energies);
+    N2P2_REQUIRE(forces);
+    return guard([&] {
+        setDevice(training->mode);
+        training->training->setReferences(energies, forces);
+    });
+}
+
+n2p2_status n2p2_training_set_force_weight(n2p2_training* training, double weight)
+{
+    N2P2_REQUIRE(training);
+    return guard([&] {
+        if (!(weight >= 0.0)) throw std::invalid_argument("ERROR: the force weight must be non-negative.\n");
+        training->training->setForceWeight(weight);
+    });
+}
+
+n2p2_status n2p2_training_set_kalman_standard(n2p2_training* training, double epsilon, double q0, double qtau,
+                                              double qmin, double eta0, double etatau, double etamax)
+{
+    N2P2_REQUIRE(training);
+    return guard([&] {
+        if (!(epsilon > 0.0) || !(eta0 > 0.0)) throw std::invalid_argument("ERROR: invalid Kalman filter parameters.\n");
+        setDevice(training->mode);
+        training->training->setKalmanStandard(epsilon, q0, qtau, qmin, eta0, etatau, etamax);
+    });
+}
+
+n2p2_status n2p2_training_set_kalman_fading_memory(n2p2_training* training, double epsilon, double q0, double qtau,
+                                                   double qmin, double lambda, double nu)
+{
+    N2P2_REQUIRE(training);
+    return guard([&] {
+        if (!(epsilon > 0.0) || !(lambda > 0.0)) throw std::invalid_argument("ERROR: invalid Kalman filter parameters.\n");
+        setDevice(training->mode);
+        training->training->setKalmanFadingMemory(epsilon, q0, qtau, qmin, lambda, nu);
+    });
+}
+
+n2p2_status n2p2_training_set_gradient_fixed(n2p2_training* training, double eta)
+{
+    N2P2_REQUIRE(training);
+    return guard([&] {
+        if (!(eta > 0.0)) throw std::invalid_argument("ERROR: the step size must be positive.\n");
+        training->training->setGradientFixed(eta);
+    });
+}
+
+n2p2_status n2p2_training_set_gradient_adam(n2p2_training* training, double eta, double beta1, double beta2,
+                                            double epsilon)
+{
+    N2P2_REQUIRE(training);
+    return guard([&] {
+        if (!(eta > 0.0) || !(beta1 >= 0.0 && beta1 < 1.0) || !(beta2 >= 0.0 && beta2 < 1.0) || !(epsilon > 0.0))
+            throw std::invalid_argument("ERROR: invalid Adam parameters.\n");
+        setDevice(training->mode);
+        training->training->setGradientAdam(eta, beta1, beta2, epsilon);
+    });
+}
+
+n2p2_status n2p2_training_update(n2p2_training* training, int32_t property, int32_t count, const int32_t* structure,
+                                 const int32_t* atom, const int32_t* component, double* errors)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(count >= 0);
+    N2P2_REQUIRE(count == 0 || structure);
+    N2P2_REQUIRE(property != N2P2_TRAINING_FORCE || count == 0 || (atom && component));
+    return guard([&] {
+        setDevice(training->mode);
+        if (!training->mode->uploaded)
+            throw std::runtime_error("ERROR: the mode was changed after the training was created.\n");
+        training->training->update(property, count, structure, atom, component, errors);
+    });
+}
+
+n2p2_status n2p2_training_observe(n2p2_training* training, int32_t property, int32_t structure, int32_t atom,
+                                  int32_t component, double* error, double* jacobian)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(error);
+    N2P2_REQUIRE(jacobian);
+    return guard([&] {
+        setDevice(training->mode);
+        training->training->observe(property, structure, atom, component, error, jacobian);
+    });
+}
+
+n2p2_status n2p2_training_get_kalman_status(n2p2_training* training, double* status)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(status);
+    return guard([&] {
+        setDevice(training->mode);
+        training->training->kalmanStatus(status);
+    });
+}
+
+n2p2_status n2p2_training_get_num_weights(n2p2_training* training, int64_t* count)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(count);
+    return guard([&] { *count = training->training->numWeights(); });
+}
+
+n2p2_status n2p2_training_get_weights(n2p2_training* training, double* weights)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(weights);
+    return guard([&] {
+        setDevice(training->mode);
+        training->training->getWeights(weights);
+    });
+}
+
+n2p2_status n2p2_training_set_weights(n2p2_training* training, const double* weights)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(weights);
+    return guard([&] {
+        setDevice(training->mode);
+        training->training->setWeights(weights);
     });
 }
 

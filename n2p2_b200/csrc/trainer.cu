@@ -134,23 +134,33 @@ __global__ void __launch_bounds__(256) kLossSum(const double* __restrict__ lossE
 // g_is = -(u_i . dG_is/dr_i + sum_{e = (i -> j)} u_j . dG_is/dr_j): the
 // transpose of the stored-dG/dr force contraction.  Lanes own the rows of an
 // entry (distinct SFs), entries are visited in list order.
-__global__ void __launch_bounds__(kTrainWarps * 32) kSFAdjoint(DevModel model, BatchView b,
-                                                               const double* __restrict__ u, double* __restrict__ g)
+// Atoms [a0, a1) only.  With img, the part of g_imgAtom that comes from the
+// atom's own periodic images (entries with j == i) is also written to
+// img[0..numSF): Mode::calculateForces skips those entries
+// (neighborsUnique.begin() + 1, Mode.cpp:1957) while Training::collectDGdxia
+// (Training.cpp:3604-3615) keeps them.
+__global__ void __launch_bounds__(kTrainWarps * 32) kSFAdjoint(DevModel model, BatchView b, int a0, int a1,
+                                                               const double* __restrict__ u, double* __restrict__ g,
+                                                               int imgAtom = -1, double* __restrict__ img = nullptr)
 {
     __shared__ double acc[kTrainWarps][kTrainMaxInput];
+    __shared__ double accImg[kTrainWarps][kTrainMaxInput];
     const int lane = threadIdx.x & 31;
     double* a = acc[threadIdx.x >> 5];
+    double* ai = accImg[threadIdx.x >> 5];
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
+    for (int i = a0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < a1; i += warpsPerGrid)
     {
         const int ec = b.elem[i];
         DevElement const& E = model.el[ec];
         const double ux = u[3 * (size_t)i + 0], uy = u[3 * (size_t)i + 1], uz = u[3 * (size_t)i + 2];
         __syncwarp();
+        const bool track = img && i == imgAtom;
         for (int s = lane; s < E.numSF; s += 32)
         {
             const double* p = b.dGdrSelf + ((size_t)i * b.gStride + s) * 3;
             a[s] = -(p[0] * ux + p[1] * uy + p[2] * uz);
+            ai[s] = 0.0;
         }
         __syncwarp();
         for (int64_t e = b.nbrOffset[i]; e < b.nbrOffset[i + 1]; ++e)
@@ -162,11 +172,17 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kSFAdjoint(DevModel model, B
             for (int r = lane; r < E.rows[en]; r += 32)
             {
                 const double* p = b.dGdr + ((size_t)r * b.nbrCapacity + e) * 3;
-                a[table[r]] -= p[0] * vx + p[1] * vy + p[2] * vz;
+                const double d = p[0] * vx + p[1] * vy + p[2] * vz;
+                a[table[r]] -= d;
+                if (track && j == i) ai[table[r]] -= d;
             }
             __syncwarp();
         }
-        for (int s = lane; s < E.numSF; s += 32) g[(size_t)i * b.gStride + s] = a[s];
+        for (int s = lane; s < E.numSF; s += 32)
+        {
+            g[(size_t)i * b.gStride + s] = a[s];
+            if (track) img[s] = ai[s];
+        }
     }
 }
 
@@ -184,12 +200,18 @@ struct ParamSmem
     double xb[kTrainMaxWidth], xdb[kTrainMaxWidth];
 };
 
-// Per-atom parameter gradient of a_i E_i + (dE_i/dG_i . g_i), summed into the
-// warp's slice gradPart[warp][P] (parameter layout of the device weights).
-__global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, BatchView b,
-                                                               const double* __restrict__ aStruct,
+// Per-atom parameter gradient of L_i = a_i E_i + (dE_i/dG_i . g_i) over atoms
+// [a0, a1), summed into the warp's slice gradPart[warp][P] (parameter layout
+// of the device weights).  a_i = aStruct[structure of i], or aConst without
+// aStruct; no g means g = 0.  With predPart, the warp's sum of L_i goes to
+// predPart[warp] (the value whose gradient this is).
+__global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, BatchView b, int a0, int a1,
+                                                               const double* __restrict__ aStruct, double aConst,
                                                                const double* __restrict__ g, int P,
-                                                               double* __restrict__ gradPart)
+                                                               double* __restrict__ gradPart,
+                                                               double* __restrict__ predPart,
+                                                               int imgAtom = -1,
+                                                               const double* __restrict__ img = nullptr)
 {
     __shared__ ParamSmem smem[kTrainWarps];
     ParamSmem& S = smem[threadIdx.x >> 5];
@@ -198,17 +220,18 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, B
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
     double* slice = gradPart + (size_t)warp * P;
     for (int p = lane; p < P; p += 32) slice[p] = 0.0;
+    double pred = 0.0;
     __syncwarp();
-    for (int i = warp; i < b.N; i += warpsPerGrid)
+    for (int i = a0 + warp; i < a1; i += warpsPerGrid)
     {
         const int ec = b.elem[i];
         DevElement const& E = model.el[ec];
         const int L = E.numLayers;
-        const double a = aStruct[b.atomStruct[i]];
+        const double a = aStruct ? aStruct[b.atomStruct[i]] : aConst;
         for (int j = lane; j < E.neurons[0]; j += 32)
         {
             S.x0[j] = b.G[(size_t)i * b.gStride + j];
-            S.xd0[j] = g[(size_t)i * b.gStride + j];
+            S.xd0[j] = g ? g[(size_t)i * b.gStride + j] : 0.0;
         }
         __syncwarp();
         for (int l = 1; l < L; ++l)
@@ -235,11 +258,34 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, B
             }
             __syncwarp();
         }
+        // the prediction leaves out the tangent along the atom's self-image part
+        // of g (see kSFAdjoint); the gradient keeps it
+        if (img && i == imgAtom)
+        {
+            for (int l = 1; l < L; ++l)
+            {
+                const int nin = E.neurons[l - 1], nout = E.neurons[l];
+                const double* W = model.weights + E.wOffset[l];
+                double t = 0.0;
+                if (lane < nout)
+                {
+                    const double* row = W + (size_t)lane * nin;
+                    for (int j = 0; j < nin; ++j) t += row[j] * (l == 1 ? img[j] : S.zb[j]);
+                    t *= S.f1[l][lane];
+                }
+                __syncwarp();
+                if (lane < nout) S.zb[lane] = t;
+                __syncwarp();
+            }
+            if (lane == 0) pred -= S.zb[0];
+            __syncwarp();
+        }
         // reverse: seed d(a E + Edot)/dE = a, d/dEdot = 1 on the output neuron
         if (lane == 0)
         {
             S.xb[0] = a;
             S.xdb[0] = 1.0;
+            pred += a * S.x[L - 1][0] + S.xd[L - 1][0];
         }
         __syncwarp();
         for (int l = L - 1; l >= 1; --l)
@@ -276,16 +322,18 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, B
             }
         }
     }
+    if (predPart && lane == 0) predPart[warp] = pred;
 }
 
-// grad[p] = sum over warps w (in order) of gradPart[w][p].
-__global__ void kReduceGrad(const double* __restrict__ gradPart, int warps, int P, double* __restrict__ grad)
+// grad[p] = scale * sum over warps w (in order) of gradPart[w][p].
+__global__ void kReduceGrad(const double* __restrict__ gradPart, int warps, int P, double* __restrict__ grad,
+                            double scale = 1.0)
 {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x)
     {
         double s = 0.0;
         for (int w = 0; w < warps; ++w) s += gradPart[(size_t)w * P + p];
-        grad[p] = s;
+        grad[p] = scale == 1.0 ? s : s * scale;
     }
 }
 
@@ -430,8 +478,8 @@ void Trainer::step(Batch& batch, const double* energiesPhys, const double* force
     kForceResidual<<<(N + tb - 1) / tb, tb, 0, st>>>(b, fRef_, wF_, u_, lossF_);
     kLossSum<<<1, 256, 0, st>>>(lossE_, S, lossF_, N, loss_);
     const int blocks = warps_ / kTrainWarps;
-    kSFAdjoint<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, u_, g_);
-    kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, aStruct_, g_, P_, gradPart_);
+    kSFAdjoint<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, 0, N, u_, g_);
+    kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, 0, N, aStruct_, 0.0, g_, P_, gradPart_, nullptr);
     kReduceGrad<<<(P_ + tb - 1) / tb, tb, 0, st>>>(gradPart_, warps_, P_, grad_);
     cudaCheck(cudaGetLastError(), "trainer launch");
     if (update)
@@ -491,6 +539,497 @@ void Trainer::syncHostModel(cudaStream_t st)
         model_.setConnections((int)e, c);
         pos += need;
     }
+}
+
+namespace {
+
+__global__ void kSetEntry(double* p, int64_t k, double v) { p[k] = v; }
+
+// The observation's prediction (sum of the warps' values, fixed order) and
+// error: err = ref - prediction, xi = scale * err (Training.cpp:2879-2898,
+// the force weight at :2910-2923).
+__global__ void kObsError(const double* __restrict__ predPart, int warps, const double* __restrict__ ref,
+                          int64_t refIndex, double scale, double* __restrict__ xi, double* __restrict__ err)
+{
+    const int lane = threadIdx.x;
+    double p = 0.0;
+    for (int w = lane; w < warps; w += 32) p += predPart[w];
+    p = warpSum(p);
+    if (lane == 0)
+    {
+        const double e = ref[refIndex] - p;
+        *err = e;
+        *xi = scale == 1.0 ? e : e * scale;
+    }
+}
+
+// X = P H, one warp per row (P is kept symmetric, rows are read coalesced).
+__global__ void __launch_bounds__(256) kKalmanX(const double* __restrict__ Pm, const double* __restrict__ H, int n,
+                                                double* __restrict__ X)
+{
+    const int lane = threadIdx.x & 31;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warpsPerGrid)
+    {
+        const double* row = Pm + (size_t)i * n;
+        double acc = 0.0;
+        for (int j = lane; j < n; j += 32) acc += row[j] * H[j];
+        acc = warpSum(acc);
+        if (lane == 0) X[i] = acc;
+    }
+}
+
+// A = H^T X + diag (one observation), K = X A^-1, w += K xi (the transposed
+// weight copy follows).  One block, fixed reduction order.
+__global__ void __launch_bounds__(1024) kKalmanGain(const double* __restrict__ H, const double* __restrict__ X, int n,
+                                                    double diag, const double* __restrict__ xi,
+                                                    double* __restrict__ K, double* __restrict__ w,
+                                                    double* __restrict__ wT, const int* __restrict__ tidx)
+{
+    __shared__ double part[1024];
+    double a = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a += H[i] * X[i];
+    part[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1)
+    {
+        if (threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double inv = 1.0 / (part[0] + diag);
+    const double e = *xi;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        const double k = X[i] * inv;
+        K[i] = k;
+        const double wi = w[i] + k * e;
+        w[i] = wi;
+        wT[tidx[i]] = wi;
+    }
+}
+
+// P = (P - K X^T) * scale + q I, every element with the formula of its lower
+// twin (row max(i, j), column min(i, j)), so P stays exactly symmetric.
+__global__ void __launch_bounds__(256) kKalmanP(double* __restrict__ Pm, const double* __restrict__ K,
+                                                const double* __restrict__ X, int n, double scale, double q)
+{
+    const int i = blockIdx.y;
+    const double Ki = K[i], Xi = X[i];
+    double* row = Pm + (size_t)i * n;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        double v = row[j] - (j <= i ? Ki * X[j] : K[j] * Xi);
+        if (scale != 1.0) v *= scale;
+        if (j == i) v += q;
+        row[j] = v;
+    }
+}
+
+__global__ void kKalmanInit(double* __restrict__ Pm, int n, double d)
+{
+    const size_t total = (size_t)n * n;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x)
+        Pm[k] = (k / n == k % n) ? d : 0.0;
+}
+
+// GradientDescent::update, DT_FIXED: state -= eta * error * -gradient.
+__global__ void kGradFixed(int n, const double* __restrict__ H, const double* __restrict__ xi, double eta,
+                           double* __restrict__ w, double* __restrict__ wT, const int* __restrict__ tidx)
+{
+    const double e = *xi;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const double wi = w[i] - eta * e * -H[i];
+        w[i] = wi;
+        wT[tidx[i]] = wi;
+    }
+}
+
+// GradientDescent::update, DT_ADAM, with g = error * -gradient.
+__global__ void kGradAdam(int n, const double* __restrict__ H, const double* __restrict__ xi, double beta1,
+                          double beta2, double eta, double eps, double* __restrict__ m, double* __restrict__ v,
+                          double* __restrict__ w, double* __restrict__ wT, const int* __restrict__ tidx)
+{
+    const double e = *xi;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const double gi = e * -H[i];
+        const double mi = beta1 * m[i] + (1.0 - beta1) * gi;
+        const double vi = beta2 * v[i] + (1.0 - beta2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const double wi = w[i] - eta * mi / (sqrt(vi) + eps);
+        w[i] = wi;
+        wT[tidx[i]] = wi;
+    }
+}
+
+// Partial sums for KalmanFilter::status: per block sum |P_ii|, sum |P_ij|, sum |K_i|.
+__global__ void __launch_bounds__(256) kKalmanStat(const double* __restrict__ Pm, const double* __restrict__ K, int n,
+                                                   double* __restrict__ out)
+{
+    __shared__ double part[3][256];
+    double d = 0.0, a = 0.0, k = 0.0;
+    const size_t total = (size_t)n * n;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
+    {
+        const double v = fabs(Pm[e]);
+        a += v;
+        if (e / n == e % n) d += v;
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) k += fabs(K[i]);
+    part[0][threadIdx.x] = d;
+    part[1][threadIdx.x] = a;
+    part[2][threadIdx.x] = k;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1)
+    {
+        if (threadIdx.x < s)
+            for (int c = 0; c < 3; ++c) part[c][threadIdx.x] += part[c][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; ++c) out[3 * blockIdx.x + c] = part[c][0];
+}
+
+constexpr int kStatBlocks = 256;
+
+std::vector<int> fileOrderToDevice(DevModel const& v)
+{
+    std::vector<int> map;
+    for (int e = 0; e < v.numElements; ++e)
+    {
+        DevElement const& E = v.el[e];
+        for (int l = 1; l < E.numLayers; ++l)
+        {
+            const int nin = E.neurons[l - 1], nout = E.neurons[l];
+            for (int j = 0; j < nin; ++j)
+                for (int k = 0; k < nout; ++k) map.push_back(E.wOffset[l] + k * nin + j);
+            for (int k = 0; k < nout; ++k) map.push_back(E.bOffset[l] + k);
+        }
+    }
+    return map;
+}
+
+} // namespace
+
+Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
+    : model_(model), dmodel_(dmodel), set_(set), sms_(sms)
+{
+    if (&set.deviceModel() != &dmodel_) throw std::invalid_argument("ERROR: batch belongs to another mode.\n");
+    if (set.external()) throw std::invalid_argument("ERROR: training needs structures, not external lists.\n");
+    DevModel const& v = dmodel_.view;
+    if (v.numCompactGroups > 0)
+        throw std::invalid_argument("ERROR: training needs stored dG/dr, which compact functions do not provide.\n");
+    // the network limits of the gradient kernels
+    Trainer probe(model_, dmodel_, 1);
+    (void)probe;
+    P_ = (int)dmodel_.numWeights;
+    fileToDevice_ = fileOrderToDevice(v);
+    if ((int)fileToDevice_.size() != P_) throw std::runtime_error("ERROR: weight layout mismatch.\n");
+    N_ = set.numAtoms();
+    S_ = set.numStructures();
+    if (N_ == 0) throw std::runtime_error("ERROR: no structures set.\n");
+    // G and dG/dr of the whole set, once (they do not depend on the weights)
+    set.evaluate(EVAL_FORCES | EVAL_STORE_DGDR | EVAL_NO_GRAPH, PREC_FP64, 0);
+    BatchView const& b = set.view();
+    cudaStream_t st = set.stream();
+    atomBegin_.resize((size_t)S_ + 1);
+    cudaCheck(cudaMemcpyAsync(atomBegin_.data(), b.structAtomBegin, sizeof(int) * (S_ + 1), cudaMemcpyDeviceToHost, st),
+              "D2H");
+    cudaCheck(cudaStreamSynchronize(st), "sync");
+    int maxAtoms = 0;
+    for (int k = 0; k < S_; ++k) maxAtoms = std::max(maxAtoms, atomBegin_[k + 1] - atomBegin_[k]);
+    maxWarps_ = std::min(maxAtoms, sms_ * 8);
+    maxWarps_ = (maxWarps_ + kTrainWarps - 1) / kTrainWarps * kTrainWarps;
+    eRef_ = tAlloc<double>(S_);
+    fRef_ = tAlloc<double>(3 * (size_t)N_);
+    u_ = tAlloc<double>(3 * (size_t)N_);
+    g_ = tAlloc<double>((size_t)N_ * b.gStride);
+    gradPart_ = tAlloc<double>((size_t)maxWarps_ * P_);
+    predPart_ = tAlloc<double>(maxWarps_);
+    H_ = tAlloc<double>(P_);
+    xi_ = tAlloc<double>(1);
+    X_ = tAlloc<double>(P_);
+    K_ = tAlloc<double>(P_);
+    stat_ = tAlloc<double>(3 * kStatBlocks);
+    img_ = tAlloc<double>(b.gStride);
+    cudaCheck(cudaMemsetAsync(u_, 0, sizeof(double) * 3 * (size_t)N_, st), "memset");
+    cudaCheck(cudaMemsetAsync(K_, 0, sizeof(double) * P_, st), "memset");
+    cudaCheck(cudaMemsetAsync(eRef_, 0, sizeof(double) * S_, st), "memset");
+    cudaCheck(cudaMemsetAsync(fRef_, 0, sizeof(double) * 3 * (size_t)N_, st), "memset");
+    cudaCheck(cudaStreamSynchronize(st), "sync");
+}
+
+Training::~Training()
+{
+    for (void* p : {(void*)eRef_, (void*)fRef_, (void*)u_, (void*)g_, (void*)gradPart_, (void*)predPart_, (void*)H_,
+                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)X_, (void*)K_, (void*)m_, (void*)v_, (void*)stat_, (void*)img_})
+        cudaFree(p);
+}
+
+void Training::setReferences(const double* energiesPhys, const double* forcesPhys)
+{
+    std::vector<double> e(S_), f(3 * (size_t)N_);
+    set_.energiesToInternal(energiesPhys, e.data());
+    const double cf = set_.forceToInternal();
+    for (size_t q = 0; q < f.size(); ++q) f[q] = forcesPhys[q] * cf;
+    cudaStream_t st = set_.stream();
+    cudaCheck(cudaMemcpyAsync(eRef_, e.data(), sizeof(double) * S_, cudaMemcpyHostToDevice, st), "H2D");
+    cudaCheck(cudaMemcpyAsync(fRef_, f.data(), sizeof(double) * f.size(), cudaMemcpyHostToDevice, st), "H2D");
+    cudaCheck(cudaStreamSynchronize(st), "sync");
+}
+
+void Training::setKalmanStandard(double epsilon, double q0, double qtau, double qmin, double eta0, double etatau,
+                                 double etamax)
+{
+    // KalmanFilter::KalmanFilter (P = I) and setParametersStandard (P /= epsilon), KalmanFilter.cpp:62-117, 199-218
+    if (!Pm_) Pm_ = tAlloc<double>((size_t)P_ * P_);
+    kKalmanInit<<<sms_ * 8, 256, 0, set_.stream()>>>(Pm_, P_, 1.0 / epsilon);
+    cudaCheck(cudaGetLastError(), "kalman init");
+    type_ = KF_STANDARD;
+    epsilon_ = epsilon;
+    q0_ = q0;
+    qtau_ = qtau;
+    qmin_ = qmin;
+    eta0_ = eta0;
+    etatau_ = etatau;
+    etamax_ = etamax;
+    q_ = q0;
+    eta_ = eta0;
+    numUpdates_ = 0;
+}
+
+void Training::setKalmanFadingMemory(double epsilon, double q0, double qtau, double qmin, double lambda, double nu)
+{
+    // KalmanFilter::setParametersFadingMemory, KalmanFilter.cpp:220-238
+    if (!Pm_) Pm_ = tAlloc<double>((size_t)P_ * P_);
+    kKalmanInit<<<sms_ * 8, 256, 0, set_.stream()>>>(Pm_, P_, 1.0 / epsilon);
+    cudaCheck(cudaGetLastError(), "kalman init");
+    type_ = KF_FADING_MEMORY;
+    epsilon_ = epsilon;
+    q0_ = q0;
+    qtau_ = qtau;
+    qmin_ = qmin;
+    lambda_ = lambda;
+    nu_ = nu;
+    q_ = q0;
+    gamma_ = 1.0;
+    numUpdates_ = 0;
+}
+
+void Training::setGradientFixed(double eta)
+{
+    type_ = GD_FIXED;
+    gdEta_ = eta;
+    numUpdates_ = 0;
+}
+
+void Training::setGradientAdam(double eta, double beta1, double beta2, double epsilon)
+{
+    // GradientDescent::setParametersAdam: moments 0, beta1t = beta1, beta2t = beta2
+    if (!m_) m_ = tAlloc<double>(P_);
+    if (!v_) v_ = tAlloc<double>(P_);
+    cudaCheck(cudaMemsetAsync(m_, 0, sizeof(double) * P_, set_.stream()), "memset");
+    cudaCheck(cudaMemsetAsync(v_, 0, sizeof(double) * P_, set_.stream()), "memset");
+    type_ = GD_ADAM;
+    gdEta_ = eta;
+    beta1_ = beta1;
+    beta2_ = beta2;
+    gdEps_ = epsilon;
+    beta1t_ = beta1;
+    beta2t_ = beta2;
+    numUpdates_ = 0;
+}
+
+// Error and Jacobian of one observation at the current weights
+// (Training.cpp:2551-2681 for the 2G networks): the energy of structure s
+// (sum of dE_i/dc over its atoms) or force component c of its atom a (the
+// second-order gradient with the force adjoint e_{a,c}); force errors and
+// Jacobians carry the force weight.
+void Training::observation(int property, int s, int a, int c, int t)
+{
+    cudaStream_t st = set_.stream();
+    BatchView const& b = set_.view();
+    DevModel const& m = dmodel_.view;
+    const int a0 = atomBegin_[s], a1 = atomBegin_[s + 1];
+    const int warps = std::min(maxWarps_, (a1 - a0 + kTrainWarps - 1) / kTrainWarps * kTrainWarps);
+    const int blocks = warps / kTrainWarps;
+    const int tb = 256;
+    if (property == ENERGY)
+    {
+        kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 1.0, nullptr, P_, gradPart_, predPart_);
+        kReduceGrad<<<(P_ + tb - 1) / tb, tb, 0, st>>>(gradPart_, warps, P_, H_, 1.0);
+        kObsError<<<1, 32, 0, st>>>(predPart_, warps, eRef_, s, 1.0, xi_, err_ + t);
+    }
+    else
+    {
+        const int64_t k = 3 * (int64_t)(a0 + a) + c;
+        kSetEntry<<<1, 1, 0, st>>>(u_, k, 1.0);
+        kSFAdjoint<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, u_, g_, a0 + a, img_);
+        kSetEntry<<<1, 1, 0, st>>>(u_, k, 0.0);
+        kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 0.0, g_, P_, gradPart_, predPart_,
+                                                        a0 + a, img_);
+        kReduceGrad<<<(P_ + tb - 1) / tb, tb, 0, st>>>(gradPart_, warps, P_, H_, forceWeight_);
+        kObsError<<<1, 32, 0, st>>>(predPart_, warps, fRef_, k, forceWeight_, xi_, err_ + t);
+    }
+    cudaCheck(cudaGetLastError(), "observation launch");
+}
+
+// The updater's step with the observation in H_ / xi_.
+void Training::step(int t)
+{
+    (void)t;
+    cudaStream_t st = set_.stream();
+    double* w = dmodel_.weightsDevice();
+    double* wT = dmodel_.weightsTDevice();
+    const int* tidx = dmodel_.transIndexDevice();
+    const int tb = 256;
+    if (type_ == KF_STANDARD || type_ == KF_FADING_MEMORY)
+    {
+        // KalmanFilter::update (KalmanFilter.cpp:126-197), one observation
+        double diag, scale = 1.0;
+        if (type_ == KF_STANDARD)
+        {
+            if (eta_ < etamax_) eta_ *= std::exp(etatau_);
+            diag = 1.0 / eta_;
+        }
+        else
+        {
+            diag = lambda_;
+            scale = 1.0 / lambda_;
+        }
+        kKalmanX<<<(P_ + 7) / 8, 256, 0, st>>>(Pm_, H_, P_, X_);
+        kKalmanGain<<<1, 1024, 0, st>>>(H_, X_, P_, diag, xi_, K_, w, wT, tidx);
+        dim3 grid((P_ + 255) / 256, P_);
+        kKalmanP<<<grid, 256, 0, st>>>(Pm_, K_, X_, P_, scale, q_);
+        if (q_ > qmin_) q_ *= std::exp(-qtau_);
+        if (type_ == KF_FADING_MEMORY)
+        {
+            lambda_ = nu_ * lambda_ + 1.0 - nu_;
+            gamma_ = 1.0 / (1.0 + lambda_ / gamma_);
+        }
+    }
+    else if (type_ == GD_FIXED)
+    {
+        kGradFixed<<<(P_ + tb - 1) / tb, tb, 0, st>>>(P_, H_, xi_, gdEta_, w, wT, tidx);
+    }
+    else
+    {
+        const double eta = gdEta_ * std::sqrt(1.0 - beta2t_) / (1.0 - beta1t_);
+        kGradAdam<<<(P_ + tb - 1) / tb, tb, 0, st>>>(P_, H_, xi_, beta1_, beta2_, eta, gdEps_, m_, v_, w, wT, tidx);
+        beta1t_ *= beta1_;
+        beta2t_ *= beta2_;
+    }
+    cudaCheck(cudaGetLastError(), "updater launch");
+    ++numUpdates_;
+}
+
+void Training::update(int property, int count, const int* structure, const int* atom, const int* component,
+                      double* errors)
+{
+    if (type_ < 0) throw std::runtime_error("ERROR: no updater set.\n");
+    if (property != ENERGY && property != FORCE) throw std::invalid_argument("ERROR: unknown property.\n");
+    for (int t = 0; t < count; ++t)
+    {
+        const int s = structure[t];
+        if (s < 0 || s >= S_) throw std::out_of_range("ERROR: structure index out of range.\n");
+        if (property == FORCE)
+        {
+            if (atom[t] < 0 || atom[t] >= atomBegin_[s + 1] - atomBegin_[s])
+                throw std::out_of_range("ERROR: atom index out of range.\n");
+            if (component[t] < 0 || component[t] > 2) throw std::out_of_range("ERROR: force component out of range.\n");
+        }
+    }
+    cudaStream_t st = set_.stream();
+    if (count > errCap_)
+    {
+        cudaFree(err_);
+        errCap_ = count;
+        err_ = tAlloc<double>(count);
+    }
+    for (int t = 0; t < count; ++t)
+    {
+        observation(property, structure[t], property == FORCE ? atom[t] : 0, property == FORCE ? component[t] : 0, t);
+        step(t);
+    }
+    if (errors)
+        cudaCheck(cudaMemcpyAsync(errors, err_, sizeof(double) * count, cudaMemcpyDeviceToHost, st), "D2H");
+    cudaCheck(cudaStreamSynchronize(st), "sync");
+}
+
+void Training::observe(int property, int structure, int atom, int component, double* error,
+                       double* jacobianFileOrder)
+{
+    if (property != ENERGY && property != FORCE) throw std::invalid_argument("ERROR: unknown property.\n");
+    if (structure < 0 || structure >= S_) throw std::out_of_range("ERROR: structure index out of range.\n");
+    if (property == FORCE && (atom < 0 || atom >= atomBegin_[structure + 1] - atomBegin_[structure] ||
+                              component < 0 || component > 2))
+        throw std::out_of_range("ERROR: atom or component out of range.\n");
+    if (errCap_ < 1)
+    {
+        errCap_ = 1;
+        err_ = tAlloc<double>(1);
+    }
+    cudaStream_t st = set_.stream();
+    observation(property, structure, atom, component, 0);
+    std::vector<double> h(P_);
+    cudaCheck(cudaMemcpyAsync(h.data(), H_, sizeof(double) * P_, cudaMemcpyDeviceToHost, st), "D2H");
+    cudaCheck(cudaMemcpyAsync(error, err_, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+    cudaCheck(cudaStreamSynchronize(st), "sync");
+    for (int q = 0; q < P_; ++q) jacobianFileOrder[q] = h[fileToDevice_[q]];
+}
+
+void Training::kalmanStatus(double* out)
+{
+    out[0] = (double)numUpdates_;
+    out[1] = out[2] = out[3] = 0.0;
+    if (Pm_ && (type_ == KF_STANDARD || type_ == KF_FADING_MEMORY))
+    {
+        cudaStream_t st = set_.stream();
+        kKalmanStat<<<kStatBlocks, 256, 0, st>>>(Pm_, K_, P_, stat_);
+        std::vector<double> part(3 * kStatBlocks);
+        cudaCheck(cudaMemcpyAsync(part.data(), stat_, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st),
+                  "D2H");
+        cudaCheck(cudaStreamSynchronize(st), "sync");
+        double d = 0.0, a = 0.0, k = 0.0;
+        for (int bIdx = 0; bIdx < kStatBlocks; ++bIdx)
+        {
+            d += part[3 * bIdx];
+            a += part[3 * bIdx + 1];
+            k += part[3 * bIdx + 2];
+        }
+        const double n = (double)P_;
+        out[1] = d / n;
+        out[2] = (a - d) / (n * (n - 1.0));
+        out[3] = k / n;
+    }
+    out[4] = q_;
+    out[5] = type_ == KF_FADING_MEMORY ? lambda_ : eta_;
+    out[6] = gamma_;
+}
+
+void Training::getWeights(double* fileOrder)
+{
+    std::vector<double> w(P_);
+    cudaStream_t st = set_.stream();
+    cudaCheck(cudaMemcpyAsync(w.data(), dmodel_.weightsDevice(), sizeof(double) * P_, cudaMemcpyDeviceToHost, st),
+              "D2H");
+    cudaCheck(cudaStreamSynchronize(st), "sync");
+    for (int q = 0; q < P_; ++q) fileOrder[q] = w[fileToDevice_[q]];
+}
+
+void Training::setWeights(const double* fileOrder)
+{
+    std::vector<double> w(P_), wt(P_);
+    for (int q = 0; q < P_; ++q) w[fileToDevice_[q]] = fileOrder[q];
+    for (int q = 0; q < P_; ++q) wt[dmodel_.transIndexHost[q]] = w[q];
+    cudaStream_t st = set_.stream();
+    cudaCheck(cudaMemcpyAsync(dmodel_.weightsDevice(), w.data(), sizeof(double) * P_, cudaMemcpyHostToDevice, st),
+              "H2D");
+    cudaCheck(cudaMemcpyAsync(dmodel_.weightsTDevice(), wt.data(), sizeof(double) * P_, cudaMemcpyHostToDevice, st),
+              "H2D");
+    cudaCheck(cudaStreamSynchronize(st), "sync");
 }
 
 } // namespace n2p2b200

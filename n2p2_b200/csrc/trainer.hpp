@@ -66,4 +66,95 @@ private:
     double* lossF_ = nullptr;
 };
 
+// Weight updates of the reference's training program, one observation per
+// update (Training::update, libnnptrain/Training.cpp:2256-3169, with the
+// combined update strategy and one update candidate per update): the error of
+// a structure's energy or of one force component at the current weights, its
+// Jacobian with respect to all weights, and the Kalman filter
+// (KalmanFilter::update, KalmanFilter.cpp:126-197) or gradient descent
+// (GradientDescent::update, GradientDescent.cpp:81-118) step -- all on the
+// device, without host round trips between updates.
+//
+// The symmetry functions and their derivatives do not depend on the weights:
+// they are computed once for the whole training set and stay resident; an
+// update runs the networks and the Jacobian over one structure's atoms only.
+// The filter's covariance P (weights x weights, FP64) is kept symmetric by
+// construction: every element is updated with the formula of its lower-
+// triangle twin, the only half the reference reads
+// (P.selfadjointView<Lower>()).
+class Training
+{
+public:
+    enum Property { ENERGY = 0, FORCE = 1 };
+    enum UpdaterType { KF_STANDARD = 0, KF_FADING_MEMORY = 1, GD_FIXED = 2, GD_ADAM = 3 };
+
+    Training(Model& model, DeviceModel& dmodel, Batch& set, int sms);
+    ~Training();
+    Training(Training const&) = delete;
+    Training& operator=(Training const&) = delete;
+
+    int numWeights() const { return P_; }
+    // Reference energies per structure and forces [N][3] (physical units, with offsets).
+    void setReferences(const double* energiesPhys, const double* forcesPhys);
+    void setForceWeight(double w) { forceWeight_ = w; }
+    void setKalmanStandard(double epsilon, double q0, double qtau, double qmin, double eta0, double etatau,
+                           double etamax);
+    void setKalmanFadingMemory(double epsilon, double q0, double qtau, double qmin, double lambda, double nu);
+    void setGradientFixed(double eta);
+    void setGradientAdam(double eta, double beta1, double beta2, double epsilon);
+    // `count` updates in order: energy of structure[k], or force component
+    // component[k] of atom atom[k] (index inside the structure) of
+    // structure[k].  errors[k] (optional) receives ref - prediction before the
+    // update, internal units.
+    void update(int property, int count, const int* structure, const int* atom, const int* component,
+                double* errors);
+    // Error (ref - prediction, internal units) and Jacobian (weight-file order,
+    // force weight applied for forces) of one observation, no update.
+    void observe(int property, int structure, int atom, int component, double* error, double* jacobianFileOrder);
+    // KalmanFilter::status: numUpdates, mean |P_ii|, mean |P_ij| (i != j),
+    // mean |K|, q, eta (standard) or lambda (fading memory), gamma.
+    void kalmanStatus(double* out);
+    void getWeights(double* fileOrder);
+    void setWeights(const double* fileOrder);
+    int updaterType() const { return type_; }
+
+private:
+    void observation(int property, int s, int a, int c, int t);
+    void step(int t);
+
+    Model& model_;
+    DeviceModel& dmodel_;
+    Batch& set_;
+    int sms_;
+    int P_ = 0, N_ = 0, S_ = 0;
+    std::vector<int> fileToDevice_;
+    std::vector<int> atomBegin_;
+    double forceWeight_ = 1.0;
+    int type_ = -1;
+    // Kalman filter state (host scalars as in KalmanFilter)
+    double epsilon_ = 0.0, q_ = 0.0, q0_ = 0.0, qtau_ = 0.0, qmin_ = 0.0, eta_ = 0.0, eta0_ = 0.0, etatau_ = 0.0,
+           etamax_ = 0.0, lambda_ = 0.0, nu_ = 0.0, gamma_ = 0.0;
+    long numUpdates_ = 0;
+    // gradient descent
+    double gdEta_ = 0.0, beta1_ = 0.0, beta2_ = 0.0, gdEps_ = 0.0, beta1t_ = 0.0, beta2t_ = 0.0;
+    int maxWarps_ = 0;
+    double* eRef_ = nullptr;     // [S] internal units
+    double* fRef_ = nullptr;     // [3N]
+    double* u_ = nullptr;        // [3N] force adjoint (one unit entry during a force update)
+    double* g_ = nullptr;        // [N][gStride]
+    double* gradPart_ = nullptr; // [maxWarps][P]
+    double* predPart_ = nullptr; // [maxWarps]
+    double* H_ = nullptr;        // [P] Jacobian of the observation
+    double* xi_ = nullptr;       // observation error (scaled by the force weight)
+    double* err_ = nullptr;      // [capacity] raw errors of the last update call
+    int errCap_ = 0;
+    double* Pm_ = nullptr;       // [P][P] covariance
+    double* X_ = nullptr;        // [P]
+    double* K_ = nullptr;        // [P]
+    double* m_ = nullptr;        // Adam moments
+    double* v_ = nullptr;
+    double* stat_ = nullptr;     // status partial sums
+    double* img_ = nullptr;      // [gStride] self-image part of the observed atom's adjoint
+};
+
 } // namespace n2p2b200

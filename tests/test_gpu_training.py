@@ -1,0 +1,147 @@
+"""Training updates on the GPU (n2p2_b200.training) against the training
+oracle (oracle/training_ref.py, itself pinned to the reference library by
+finite differences in tests/test_cpu_training.py).
+
+Observation errors and Jacobians to 1e-10 relative; updater sequences
+(Kalman filter standard and fading memory, gradient descent fixed and Adam)
+to 1e-9 relative in the weights after every run.  The set mixes boxes larger
+than the cutoff diameter with one smaller (periodic self-images: the force
+prediction leaves them out as Mode::calculateForces does, the Jacobian keeps
+them as Training::collectDGdxia does)."""
+import numpy as np
+import pytest
+
+from n2p2_b200 import Mode, water
+from n2p2_b200.training import ENERGY, FORCE, Training
+from oracle import ref as oref
+from tests import helpers as H
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oref.available(), reason="reference library not built")]
+
+
+def _set():
+    ss = [water.water_box(8, seed=4, sigma=0.1)] + water.water_batch(3, seed=21, n_min=32, n_max=48)
+    E, F = [], []
+    for s in ss:
+        a = H.reference_snapshot(H.WATER40, s)
+        E.append(a["energy"])
+        F.append(a["forces"])
+    return ss, np.array(E), np.concatenate(F)
+
+
+@pytest.fixture(scope="module")
+def data():
+    ss, E, F = _set()
+    from oracle import training_ref as T
+    nets = T.Networks(H.WATER40)
+    w0 = nets.weights + np.random.default_rng(5).normal(0.0, 0.02, nets.numWeights)   # away from the labels
+    return ss, E, F, w0
+
+
+def _pair(data, updater, force_weight=3.0):
+    from oracle import training_ref as T
+    ss, E, F, w0 = data
+    m = Mode(0)
+    m.setupFromDirectory(H.WATER40)
+    tr = Training(m, ss, E, F)
+    tr.setWeights(w0)
+    tr.setForceWeight(force_weight)
+    n = tr.numWeights
+    kind, args = updater
+    if kind == "kf":
+        tr.setupUpdaterKalman(0, **args)
+        up = T.KalmanFilter(n, 0, args["epsilon"], args["q0"], args["qtau"], args["qmin"], args["eta"], args["etatau"],
+                            args["etamax"])
+    elif kind == "kf_fading":
+        tr.setupUpdaterKalman(1, epsilon=args["epsilon"], q0=args["q0"], qtau=args["qtau"], qmin=args["qmin"],
+                              lambda_=args["lambda_"], nu=args["nu"])
+        up = T.KalmanFilter(n, 1, args["epsilon"], args["q0"], args["qtau"], args["qmin"], lam=args["lambda_"],
+                            nu=args["nu"])
+    elif kind == "gd":
+        tr.setupUpdaterGradient(0, eta=args["eta"])
+        up = T.GradientDescent(n, 0, args["eta"])
+    else:
+        tr.setupUpdaterGradient(1, adam_eta=args["eta"])
+        up = T.GradientDescent(n, 1, args["eta"])
+    ref = T.Training(H.WATER40, ss, E, F, up, force_weight=force_weight)
+    ref.nets.weights = w0.copy()
+    return m, tr, ref
+
+
+def test_observations_match_oracle(data):
+    m, tr, ref = _pair(data, ("gd", {"eta": 1e-3}))
+    try:
+        for prop, s, a, c in ((ENERGY, 1, 0, 0), (FORCE, 2, 7, 1), (FORCE, 0, 5, 2), (FORCE, 0, 0, 0)):
+            e, J = tr.observe(prop, s, a, c)
+            er, Jr = ref.observation(prop, s, a, c)
+            if prop == FORCE:
+                Jr = Jr * tr.forceWeight
+            scale = abs(data[1][s]) if prop == ENERGY else np.abs(data[2]).max()
+            assert abs(e - er) <= 1e-10 * scale, (prop, s, a, c, e, er)
+            assert H.max_rel(J, Jr) <= 1e-10, (prop, s, a, c)
+    finally:
+        tr.close()
+        m.close()
+
+
+SCHEDULE = [(ENERGY, [1, 3, 0]), (FORCE, [(2, 7, 1), (0, 5, 2), (3, 11, 0)]), (ENERGY, [2, 0]),
+            (FORCE, [(1, 4, 2), (0, 0, 0)])]
+
+UPDATERS = [
+    ("kf", {"epsilon": 1e-2, "q0": 0.01, "qtau": 2.302, "qmin": 1e-6, "eta": 0.01, "etatau": 2.302, "etamax": 1.0}),
+    ("kf_fading", {"epsilon": 1e-2, "q0": 0.01, "qtau": 2.302, "qmin": 1e-6, "lambda_": 0.96, "nu": 0.99741}),
+    ("gd", {"eta": 1e-4}),
+    ("adam", {"eta": 1e-3}),
+]
+
+
+@pytest.mark.parametrize("updater", UPDATERS, ids=[u[0] for u in UPDATERS])
+def test_update_sequence_matches_oracle(data, updater):
+    m, tr, ref = _pair(data, updater)
+    try:
+        for prop, cands in SCHEDULE:
+            if prop == ENERGY:
+                errs = tr.update(ENERGY, cands)
+                errs_ref = [ref.update(0, s) for s in cands]
+            else:
+                s, a, c = (np.array(x) for x in zip(*cands))
+                errs = tr.update(FORCE, s, a, c)
+                errs_ref = [ref.update(1, *x) for x in cands]
+            assert np.allclose(errs, errs_ref, rtol=1e-9, atol=1e-12), (prop, errs, errs_ref)
+            assert H.max_rel(tr.weights(), ref.nets.weights) <= 1e-9
+        if updater[0].startswith("kf"):
+            st = tr.kalmanStatus()
+            assert st["numUpdates"] == 10
+            assert abs(st["Pdiag"] - np.mean(np.abs(np.diag(ref.updater.P)))) <= 1e-9 * st["Pdiag"]
+            assert abs(st["q"] - ref.updater.q) <= 1e-15
+    finally:
+        tr.close()
+        m.close()
+
+
+def test_epochs_reduce_errors(data):
+    ss, E, F, w0 = data
+    m = Mode(0)
+    m.setupFromDirectory(H.WATER40)
+    tr = Training(m, ss, E, F)
+    try:
+        tr.setWeights(w0)
+        tr.setupUpdaterKalman(0)
+        tr.setForceWeight(10.0)
+        before = tr.errors()
+        rng = np.random.default_rng(1)
+        for _ in range(3):
+            tr.runEpoch(energyFraction=1.0, forceFraction=0.05, rng=rng)
+        after = tr.errors()
+        assert after["energy_rmse_per_atom"] < 0.5 * before["energy_rmse_per_atom"]
+        assert after["force_rmse"] < before["force_rmse"]
+        # the mode's other batches evaluate the trained weights
+        b = m.batch(ss[:1])
+        b.setPositions(ss[0].positions)
+        b.evaluate(forces=False)
+        e_trained = b.energies()[0]
+        b.close()
+        assert abs(e_trained - E[0]) / ss[0].numAtoms <= before["energy_rmse_per_atom"]
+    finally:
+        tr.close()
+        m.close()
