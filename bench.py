@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--no-lammps", action="store_true")
     ap.add_argument("--no-scaling", action="store_true")
     ap.add_argument("--no-compact", action="store_true")
+    ap.add_argument("--no-training", action="store_true")
     ap.add_argument("--student-boxes", type=int, default=2048)
     return ap.parse_args()
 
@@ -301,6 +302,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_compact:
         compact = bench_compact(args.steps, args.warmup, local, cpu=not args.no_cpu)
 
+    # training updates (Kalman filter over the water40 networks)
+    training = None
+    if rank == 0 and world == 1 and not args.no_training:
+        training = bench_training(args.steps, args.warmup, local, cpu=not args.no_cpu)
+
     # nnp-scaling (input.data read + symmetry-function statistics) on the batched workload
     scal = None
     if rank == 0 and world == 1 and not args.no_scaling:
@@ -376,7 +382,7 @@ def run_ours(args):
                 "e2e": {"value": world * natoms / (e2e_ms / 1000.0), "unit": "atoms/s", "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": nbytes_pos, "d2h_bytes_per_step": nbytes_pos + 8 * len(structs)},
                 "gpu_launches": launches, "autotune": _shape_names(tune), "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
-                "mixed": mixed, "student": stud, "large_system": large, "lammps_interface": lammps, "nnp_scaling": scal, "compact_functions": compact, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
+                "mixed": mixed, "student": stud, "large_system": large, "lammps_interface": lammps, "nnp_scaling": scal, "compact_functions": compact, "training": training, "stages_ms": {n: round(t, 4) for n, t in stages}, "work": work,
                 "fp32_fma_peak_tflops": fp32_peak}
         print(json.dumps(line), flush=True)
     mode.close()
@@ -573,6 +579,88 @@ def bench_compact(steps, warmup, device, cpu=True):
     natoms, o = _compact_run(d, structs, steps, warmup, device, cpu, cpu_sample=512)
     out["weighted"] = {"workload": "QM9 settings (reference training example; weighted types 23 + 24 + 25, five "
                                    "elements), 4096 molecules (%d atoms)" % natoms, **o}
+    return out
+
+
+def bench_training(steps, warmup, device, cpu=True):
+    """Training updates (Training::update with KalmanFilter::update, standard
+    filter, force weight 10): the water40 networks (3402 weights, covariance
+    3402 x 3402 FP64 = 92.6 MB), 256 water boxes of 32-128 molecules labelled
+    by the model's own weights, training from weights perturbed by N(0, 0.02).
+    Energy and force updates are timed separately (CUDA events on the set's
+    stream), 256 updates per timed step.  Each filter update streams the
+    covariance three times (X = P H, then P read and written): 24 n^2 bytes,
+    the HBM roofline of an update.  Beside it the numpy restatement of the
+    same updates on a bounded sample (the reference's training program needs
+    MPI and GSL, which this image lacks)."""
+    import time
+    import torch
+    from n2p2_b200 import Mode, water
+    from n2p2_b200.training import ENERGY, FORCE, Training
+    wdir = os.path.join(ROOT, "tests", "golden", "models", "water40")
+    m = Mode(device)
+    m.setupFromDirectory(wdir)
+    ss = water.water_batch(256, seed=31, n_min=32, n_max=128)
+    b = m.batch(ss)
+    b.setPositions(np.concatenate([x.positions for x in ss]))
+    b.evaluate(forces=True)
+    E, F = b.energies(), b.forces()
+    b.close()
+    tr = Training(m, ss, E, F)
+    w0 = tr.weights() + np.random.default_rng(5).normal(0.0, 0.02, tr.numWeights)
+    tr.setWeights(w0)
+    tr.setupUpdaterKalman(0)
+    tr.setForceWeight(10.0)
+    n = tr.numWeights
+    ec, (fs, fa, fc) = tr.updateCandidates()
+    rng = np.random.default_rng(2)
+    per = 256
+    eo = rng.permutation(ec.size)
+    fo = rng.permutation(fs.size)[:per * (steps + warmup)]
+    stream = torch.cuda.ExternalStream(tr.batch.stream(), device=torch.device("cuda", device))
+    out = {"workload": "water40 networks (%d weights, covariance %.1f MB FP64), 256 water boxes of 32-128 molecules "
+                       "(%d atoms), standard Kalman filter, force weight 10"
+                       % (n, 8.0 * n * n / 1e6, sum(x.numAtoms for x in ss)),
+           "unit": "updates/s"}
+    for name, prop in (("energy", ENERGY), ("force", FORCE)):
+        def run(k):
+            idx = np.arange(k * per, (k + 1) * per)
+            if prop == ENERGY:
+                tr.update(ENERGY, ec[eo[idx % ec.size]])
+            else:
+                tr.update(FORCE, fs[fo[idx]], fa[fo[idx]], fc[fo[idx]])
+        for k in range(warmup):
+            run(k)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(warmup, warmup + steps):
+            run(k)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / (steps * per)
+        out[name] = {"value": 1e3 / ms, "ms_per_update": ms,
+                     "kalman_hbm_GBps_lower_bound": 24.0 * n * n / (ms * 1e-3) / 1e9}
+    out["errors_after"] = tr.errors()
+    out["kalman_status"] = tr.kalmanStatus()
+    tr.close()
+    m.close()
+    if cpu:
+        try:
+            from oracle import training_ref as T
+            sample = ss[:2]
+            up = T.KalmanFilter(n, 0, 1e-2, 0.01, 2.302, 1e-6, 0.01, 2.302, 1.0)
+            ref = T.Training(wdir, sample, E[:2], F[:sum(x.numAtoms for x in sample)], up, force_weight=10.0)
+            ref.nets.weights = w0.copy()
+            t0 = time.perf_counter()
+            for k in range(3):
+                ref.update(0, k % 2)
+            sec = (time.perf_counter() - t0) / 3
+            out["cpu_reference"] = {"value": 1.0 / sec, "unit": "updates/s", "cores": 1, "kind": "port",
+                                    "sample": "3 energy updates (numpy restatement: network Jacobian over a "
+                                              "box's atoms + Kalman update of the full covariance)"}
+        except Exception as exc:
+            out["cpu_reference"] = {"value": None, "sample": "failed: %s" % exc}
     return out
 
 
