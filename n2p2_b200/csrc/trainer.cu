@@ -563,20 +563,63 @@ __global__ void kObsError(const double* __restrict__ predPart, int warps, const 
     }
 }
 
-// X = P H, one warp per row (P is kept symmetric, rows are read coalesced).
-__global__ void __launch_bounds__(256) kKalmanX(const double* __restrict__ Pm, const double* __restrict__ H, int n,
-                                                double* __restrict__ X)
+// out[p] = scale * sum over slices w of part[w][p] in a fixed order: thread
+// row r sums w = r, r + 8, ... in turn, the 8 partial sums are then added in
+// row order.  32 parameters x 8 slice rows per block.
+__global__ void __launch_bounds__(256) kReduceSlices(const double* __restrict__ part, int slices, int P,
+                                                     double* __restrict__ out, double scale)
 {
-    const int lane = threadIdx.x & 31;
-    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warpsPerGrid)
+    __shared__ double acc[8][32];
+    const int lx = threadIdx.x & 31, r = threadIdx.x >> 5;
+    const int p = blockIdx.x * 32 + lx;
+    double s = 0.0;
+    if (p < P)
+        for (int w = r; w < slices; w += 8) s += part[(size_t)w * P + p];
+    acc[r][lx] = s;
+    __syncthreads();
+    if (r == 0 && p < P)
     {
-        const double* row = Pm + (size_t)i * n;
-        double acc = 0.0;
-        for (int j = lane; j < n; j += 32) acc += row[j] * H[j];
-        acc = warpSum(acc);
-        if (lane == 0) X[i] = acc;
+        double t = acc[0][lx];
+        for (int k = 1; k < 8; ++k) t += acc[k][lx];
+        out[p] = scale == 1.0 ? t : t * scale;
     }
+}
+
+// The previous update's pending P = (P - K X^T) * scale + q I (when
+// `pending`), fused with this update's X = P H: one pass that reads and writes
+// P once.  One block per row, fixed-order block reduction; every element is
+// updated with the formula of its lower twin (row max(i, j), column
+// min(i, j)), so P stays exactly symmetric and rows are read coalesced.
+__global__ void __launch_bounds__(128) kKalmanPX(double* __restrict__ Pm, const double* __restrict__ Kp,
+                                                 const double* __restrict__ Xp, int n, int pending, double scale,
+                                                 double q, const double* __restrict__ H, double* __restrict__ X)
+{
+    __shared__ double part[128];
+    const int i = blockIdx.x;
+    double* row = Pm + (size_t)i * n;
+    double acc = 0.0;
+    if (pending)
+    {
+        const double Ki = Kp[i], Xi = Xp[i];
+        for (int j = threadIdx.x; j < n; j += blockDim.x)
+        {
+            double v = row[j] - (j <= i ? Ki * Xp[j] : Kp[j] * Xi);
+            if (scale != 1.0) v *= scale;
+            if (j == i) v += q;
+            row[j] = v;
+            acc += v * H[j];
+        }
+    }
+    else
+        for (int j = threadIdx.x; j < n; j += blockDim.x) acc += row[j] * H[j];
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1)
+    {
+        if (threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) X[i] = part[0];
 }
 
 // A = H^T X + diag (one observation), K = X A^-1, w += K xi (the transposed
@@ -750,12 +793,15 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
     predPart_ = tAlloc<double>(maxWarps_);
     H_ = tAlloc<double>(P_);
     xi_ = tAlloc<double>(1);
-    X_ = tAlloc<double>(P_);
-    K_ = tAlloc<double>(P_);
+    for (int k = 0; k < 2; ++k)
+    {
+        Xb_[k] = tAlloc<double>(P_);
+        Kb_[k] = tAlloc<double>(P_);
+    }
     stat_ = tAlloc<double>(3 * kStatBlocks);
     img_ = tAlloc<double>(b.gStride);
     cudaCheck(cudaMemsetAsync(u_, 0, sizeof(double) * 3 * (size_t)N_, st), "memset");
-    cudaCheck(cudaMemsetAsync(K_, 0, sizeof(double) * P_, st), "memset");
+    for (int k = 0; k < 2; ++k) cudaCheck(cudaMemsetAsync(Kb_[k], 0, sizeof(double) * P_, st), "memset");
     cudaCheck(cudaMemsetAsync(eRef_, 0, sizeof(double) * S_, st), "memset");
     cudaCheck(cudaMemsetAsync(fRef_, 0, sizeof(double) * 3 * (size_t)N_, st), "memset");
     cudaCheck(cudaStreamSynchronize(st), "sync");
@@ -764,7 +810,7 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
 Training::~Training()
 {
     for (void* p : {(void*)eRef_, (void*)fRef_, (void*)u_, (void*)g_, (void*)gradPart_, (void*)predPart_, (void*)H_,
-                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)X_, (void*)K_, (void*)m_, (void*)v_, (void*)stat_, (void*)img_})
+                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)Xb_[0], (void*)Xb_[1], (void*)Kb_[0], (void*)Kb_[1], (void*)m_, (void*)v_, (void*)stat_, (void*)img_})
         cudaFree(p);
 }
 
@@ -787,6 +833,8 @@ void Training::setKalmanStandard(double epsilon, double q0, double qtau, double 
     if (!Pm_) Pm_ = tAlloc<double>((size_t)P_ * P_);
     kKalmanInit<<<sms_ * 8, 256, 0, set_.stream()>>>(Pm_, P_, 1.0 / epsilon);
     cudaCheck(cudaGetLastError(), "kalman init");
+    pending_ = false;
+    cudaCheck(cudaMemsetAsync(Kb_[cur_], 0, sizeof(double) * P_, set_.stream()), "memset");
     type_ = KF_STANDARD;
     epsilon_ = epsilon;
     q0_ = q0;
@@ -806,6 +854,8 @@ void Training::setKalmanFadingMemory(double epsilon, double q0, double qtau, dou
     if (!Pm_) Pm_ = tAlloc<double>((size_t)P_ * P_);
     kKalmanInit<<<sms_ * 8, 256, 0, set_.stream()>>>(Pm_, P_, 1.0 / epsilon);
     cudaCheck(cudaGetLastError(), "kalman init");
+    pending_ = false;
+    cudaCheck(cudaMemsetAsync(Kb_[cur_], 0, sizeof(double) * P_, set_.stream()), "memset");
     type_ = KF_FADING_MEMORY;
     epsilon_ = epsilon;
     q0_ = q0;
@@ -855,11 +905,10 @@ void Training::observation(int property, int s, int a, int c, int t)
     const int a0 = atomBegin_[s], a1 = atomBegin_[s + 1];
     const int warps = std::min(maxWarps_, (a1 - a0 + kTrainWarps - 1) / kTrainWarps * kTrainWarps);
     const int blocks = warps / kTrainWarps;
-    const int tb = 256;
     if (property == ENERGY)
     {
         kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 1.0, nullptr, P_, gradPart_, predPart_);
-        kReduceGrad<<<(P_ + tb - 1) / tb, tb, 0, st>>>(gradPart_, warps, P_, H_, 1.0);
+        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, 1.0);
         kObsError<<<1, 32, 0, st>>>(predPart_, warps, eRef_, s, 1.0, xi_, err_ + t);
     }
     else
@@ -870,7 +919,7 @@ void Training::observation(int property, int s, int a, int c, int t)
         kSetEntry<<<1, 1, 0, st>>>(u_, k, 0.0);
         kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 0.0, g_, P_, gradPart_, predPart_,
                                                         a0 + a, img_);
-        kReduceGrad<<<(P_ + tb - 1) / tb, tb, 0, st>>>(gradPart_, warps, P_, H_, forceWeight_);
+        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, forceWeight_);
         kObsError<<<1, 32, 0, st>>>(predPart_, warps, fRef_, k, forceWeight_, xi_, err_ + t);
     }
     cudaCheck(cudaGetLastError(), "observation launch");
@@ -899,10 +948,15 @@ void Training::step(int t)
             diag = lambda_;
             scale = 1.0 / lambda_;
         }
-        kKalmanX<<<(P_ + 7) / 8, 256, 0, st>>>(Pm_, H_, P_, X_);
-        kKalmanGain<<<1, 1024, 0, st>>>(H_, X_, P_, diag, xi_, K_, w, wT, tidx);
-        dim3 grid((P_ + 255) / 256, P_);
-        kKalmanP<<<grid, 256, 0, st>>>(Pm_, K_, X_, P_, scale, q_);
+        // this update's X with the previous update's P update applied on the way
+        const int cur = cur_ ^ 1;
+        kKalmanPX<<<P_, 128, 0, st>>>(Pm_, Kb_[cur_], Xb_[cur_], P_, pending_ ? 1 : 0, pendingScale_, pendingQ_, H_,
+                                      Xb_[cur]);
+        kKalmanGain<<<1, 1024, 0, st>>>(H_, Xb_[cur], P_, diag, xi_, Kb_[cur], w, wT, tidx);
+        cur_ = cur;
+        pending_ = true;   // P - K X^T, * scale, + q I: applied by the next pass over P
+        pendingScale_ = scale;
+        pendingQ_ = q_;
         if (q_ > qmin_) q_ *= std::exp(-qtau_);
         if (type_ == KF_FADING_MEMORY)
         {
@@ -980,14 +1034,24 @@ void Training::observe(int property, int structure, int atom, int component, dou
     for (int q = 0; q < P_; ++q) jacobianFileOrder[q] = h[fileToDevice_[q]];
 }
 
+void Training::flushKalman()
+{
+    if (!pending_) return;
+    dim3 grid((P_ + 255) / 256, P_);
+    kKalmanP<<<grid, 256, 0, set_.stream()>>>(Pm_, Kb_[cur_], Xb_[cur_], P_, pendingScale_, pendingQ_);
+    cudaCheck(cudaGetLastError(), "kalman flush");
+    pending_ = false;
+}
+
 void Training::kalmanStatus(double* out)
 {
+    flushKalman();
     out[0] = (double)numUpdates_;
     out[1] = out[2] = out[3] = 0.0;
     if (Pm_ && (type_ == KF_STANDARD || type_ == KF_FADING_MEMORY))
     {
         cudaStream_t st = set_.stream();
-        kKalmanStat<<<kStatBlocks, 256, 0, st>>>(Pm_, K_, P_, stat_);
+        kKalmanStat<<<kStatBlocks, 256, 0, st>>>(Pm_, Kb_[cur_], P_, stat_);
         std::vector<double> part(3 * kStatBlocks);
         cudaCheck(cudaMemcpyAsync(part.data(), stat_, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st),
                   "D2H");

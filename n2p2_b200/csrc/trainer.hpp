@@ -120,6 +120,7 @@ public:
 
 private:
     void observation(int property, int s, int a, int c, int t);
+    void flushKalman();
     void step(int t);
 
     Model& model_;
@@ -149,8 +150,11 @@ private:
     double* err_ = nullptr;      // [capacity] raw errors of the last update call
     int errCap_ = 0;
     double* Pm_ = nullptr;       // [P][P] covariance
-    double* X_ = nullptr;        // [P]
-    double* K_ = nullptr;        // [P]
+    double* Xb_[2] = {nullptr, nullptr};   // [P] X of the last two updates (alternating)
+    double* Kb_[2] = {nullptr, nullptr};   // [P] K of the last two updates
+    int cur_ = 0;                // buffer of the latest update
+    bool pending_ = false;       // the latest update's P - K X^T (* scale, + q I) not applied yet
+    double pendingScale_ = 1.0, pendingQ_ = 0.0;
     double* m_ = nullptr;        // Adam moments
     double* v_ = nullptr;
     double* stat_ = nullptr;     // status partial sums
