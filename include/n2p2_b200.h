@@ -377,6 +377,10 @@ n2p2_status n2p2_training_destroy(n2p2_training* training);
 n2p2_status n2p2_training_set_references(n2p2_training* training, const double* energies, const double* forces);
 /* force_weight (Training.cpp:2910-2923): scales force errors and Jacobians. */
 n2p2_status n2p2_training_set_force_weight(n2p2_training* training, double weight);
+/* task_batch_size_energy / task_batch_size_force (Training.cpp:2277-2279 with jacobian_mode 0 or 1 on one
+ * process): that many consecutive candidates form one observation (errors and Jacobians summed at the same
+ * weights) and one updater step. */
+n2p2_status n2p2_training_set_task_batch_size(n2p2_training* training, int32_t energy, int32_t force);
 /* KalmanFilter::setParametersStandard / setParametersFadingMemory (P = I / epsilon). */
 n2p2_status n2p2_training_set_kalman_standard(n2p2_training* training, double epsilon, double q0, double qtau,
                                               double qmin, double eta0, double etatau, double etamax);
@@ -386,7 +390,8 @@ n2p2_status n2p2_training_set_kalman_fading_memory(n2p2_training* training, doub
 n2p2_status n2p2_training_set_gradient_fixed(n2p2_training* training, double eta);
 n2p2_status n2p2_training_set_gradient_adam(n2p2_training* training, double eta, double beta1, double beta2,
                                             double epsilon);
-/* `count` updates in order.  property N2P2_TRAINING_ENERGY: the energy of
+/* `count` candidates in order, one update per task batch of them (count a
+ * multiple of the task batch size).  property N2P2_TRAINING_ENERGY: the energy of
  * structure[k]; N2P2_TRAINING_FORCE: component component[k] (0..2) of atom
  * atom[k] (index inside the structure) of structure[k]; atom and component
  * may be NULL for energy updates.  errors[k] (optional): reference minus

@@ -834,6 +834,15 @@ n2p2_status n2p2_training_set_force_weight(n2p2_training* training, double weigh
     });
 }
 
+n2p2_status n2p2_training_set_task_batch_size(n2p2_training* training, int32_t energy, int32_t force)
+{
+    N2P2_REQUIRE(training);
+    return guard([&] {
+        if (energy < 1 || force < 1) throw std::invalid_argument("ERROR: task batch sizes must be positive.\n");
+        training->training->setTaskBatchSize(energy, force);
+    });
+}
+
 n2p2_status n2p2_training_set_kalman_standard(n2p2_training* training, double epsilon, double q0, double qtau,
                                               double qmin, double eta0, double etatau, double etamax)
 {

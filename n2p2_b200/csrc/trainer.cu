@@ -548,8 +548,11 @@ __global__ void kSetEntry(double* p, int64_t k, double v) { p[k] = v; }
 // The observation's prediction (sum of the warps' values, fixed order) and
 // error: err = ref - prediction, xi = scale * err (Training.cpp:2879-2898,
 // the force weight at :2910-2923).
+// xi[1] keeps the unscaled sum over a task batch's candidates (accumulate),
+// xi[0] that sum times the scale.
 __global__ void kObsError(const double* __restrict__ predPart, int warps, const double* __restrict__ ref,
-                          int64_t refIndex, double scale, double* __restrict__ xi, double* __restrict__ err)
+                          int64_t refIndex, double scale, double* __restrict__ xi, double* __restrict__ err,
+                          int accumulate)
 {
     const int lane = threadIdx.x;
     double p = 0.0;
@@ -559,15 +562,19 @@ __global__ void kObsError(const double* __restrict__ predPart, int warps, const 
     {
         const double e = ref[refIndex] - p;
         *err = e;
-        *xi = scale == 1.0 ? e : e * scale;
+        const double sum = accumulate ? xi[1] + e : e;
+        xi[1] = sum;
+        xi[0] = scale == 1.0 ? sum : sum * scale;
     }
 }
 
 // out[p] = scale * sum over slices w of part[w][p] in a fixed order: thread
 // row r sums w = r, r + 8, ... in turn, the 8 partial sums are then added in
 // row order.  32 parameters x 8 slice rows per block.
+// With `accumulate` the sum is added to out's previous value before scaling
+// (task batches: the candidates' Jacobians are summed, then scaled once).
 __global__ void __launch_bounds__(256) kReduceSlices(const double* __restrict__ part, int slices, int P,
-                                                     double* __restrict__ out, double scale)
+                                                     double* __restrict__ out, double scale, int accumulate)
 {
     __shared__ double acc[8][32];
     const int lx = threadIdx.x & 31, r = threadIdx.x >> 5;
@@ -581,6 +588,7 @@ __global__ void __launch_bounds__(256) kReduceSlices(const double* __restrict__ 
     {
         double t = acc[0][lx];
         for (int k = 1; k < 8; ++k) t += acc[k][lx];
+        if (accumulate) t = out[p] + t;
         out[p] = scale == 1.0 ? t : t * scale;
     }
 }
@@ -792,7 +800,7 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
     gradPart_ = tAlloc<double>((size_t)maxWarps_ * P_);
     predPart_ = tAlloc<double>(maxWarps_);
     H_ = tAlloc<double>(P_);
-    xi_ = tAlloc<double>(1);
+    xi_ = tAlloc<double>(2);
     for (int k = 0; k < 2; ++k)
     {
         Xb_[k] = tAlloc<double>(P_);
@@ -897,8 +905,9 @@ void Training::setGradientAdam(double eta, double beta1, double beta2, double ep
 // (sum of dE_i/dc over its atoms) or force component c of its atom a (the
 // second-order gradient with the force adjoint e_{a,c}); force errors and
 // Jacobians carry the force weight.
-void Training::observation(int property, int s, int a, int c, int t)
+void Training::observation(int property, int s, int a, int c, int t, bool accumulate, bool last)
 {
+    const int acc = accumulate ? 1 : 0;
     cudaStream_t st = set_.stream();
     BatchView const& b = set_.view();
     DevModel const& m = dmodel_.view;
@@ -908,8 +917,8 @@ void Training::observation(int property, int s, int a, int c, int t)
     if (property == ENERGY)
     {
         kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 1.0, nullptr, P_, gradPart_, predPart_);
-        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, 1.0);
-        kObsError<<<1, 32, 0, st>>>(predPart_, warps, eRef_, s, 1.0, xi_, err_ + t);
+        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, 1.0, acc);
+        kObsError<<<1, 32, 0, st>>>(predPart_, warps, eRef_, s, 1.0, xi_, err_ + t, acc);
     }
     else
     {
@@ -919,8 +928,8 @@ void Training::observation(int property, int s, int a, int c, int t)
         kSetEntry<<<1, 1, 0, st>>>(u_, k, 0.0);
         kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 0.0, g_, P_, gradPart_, predPart_,
                                                         a0 + a, img_);
-        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, forceWeight_);
-        kObsError<<<1, 32, 0, st>>>(predPart_, warps, fRef_, k, forceWeight_, xi_, err_ + t);
+        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, last ? forceWeight_ : 1.0, acc);
+        kObsError<<<1, 32, 0, st>>>(predPart_, warps, fRef_, k, forceWeight_, xi_, err_ + t, acc);
     }
     cudaCheck(cudaGetLastError(), "observation launch");
 }
@@ -1002,10 +1011,17 @@ void Training::update(int property, int count, const int* structure, const int* 
         errCap_ = count;
         err_ = tAlloc<double>(count);
     }
+    // a task batch of candidates forms one observation: errors and Jacobians
+    // summed at the same weights, then one updater step (Training.cpp:2879-2923)
+    const int batch = property == ENERGY ? taskBatchEnergy_ : taskBatchForce_;
+    if (count % batch != 0)
+        throw std::invalid_argument("ERROR: the number of candidates is not a multiple of the task batch size.\n");
     for (int t = 0; t < count; ++t)
     {
-        observation(property, structure[t], property == FORCE ? atom[t] : 0, property == FORCE ? component[t] : 0, t);
-        step(t);
+        const int q = t % batch;
+        observation(property, structure[t], property == FORCE ? atom[t] : 0, property == FORCE ? component[t] : 0, t,
+                    q > 0, q == batch - 1);
+        if (q == batch - 1) step(t);
     }
     if (errors)
         cudaCheck(cudaMemcpyAsync(errors, err_, sizeof(double) * count, cudaMemcpyDeviceToHost, st), "D2H");
@@ -1026,7 +1042,7 @@ void Training::observe(int property, int structure, int atom, int component, dou
         err_ = tAlloc<double>(1);
     }
     cudaStream_t st = set_.stream();
-    observation(property, structure, atom, component, 0);
+    observation(property, structure, atom, component, 0, false, true);
     std::vector<double> h(P_);
     cudaCheck(cudaMemcpyAsync(h.data(), H_, sizeof(double) * P_, cudaMemcpyDeviceToHost, st), "D2H");
     cudaCheck(cudaMemcpyAsync(error, err_, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");

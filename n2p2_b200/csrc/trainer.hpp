@@ -97,12 +97,19 @@ public:
     // Reference energies per structure and forces [N][3] (physical units, with offsets).
     void setReferences(const double* energiesPhys, const double* forcesPhys);
     void setForceWeight(double w) { forceWeight_ = w; }
+    // task_batch_size_energy / _force: candidates summed into one observation per update.
+    void setTaskBatchSize(int energy, int force)
+    {
+        taskBatchEnergy_ = energy;
+        taskBatchForce_ = force;
+    }
     void setKalmanStandard(double epsilon, double q0, double qtau, double qmin, double eta0, double etatau,
                            double etamax);
     void setKalmanFadingMemory(double epsilon, double q0, double qtau, double qmin, double lambda, double nu);
     void setGradientFixed(double eta);
     void setGradientAdam(double eta, double beta1, double beta2, double epsilon);
-    // `count` updates in order: energy of structure[k], or force component
+    // `count` candidates in order, task-batch-size consecutive candidates per
+    // update: energy of structure[k], or force component
     // component[k] of atom atom[k] (index inside the structure) of
     // structure[k].  errors[k] (optional) receives ref - prediction before the
     // update, internal units.
@@ -119,7 +126,7 @@ public:
     int updaterType() const { return type_; }
 
 private:
-    void observation(int property, int s, int a, int c, int t);
+    void observation(int property, int s, int a, int c, int t, bool accumulate, bool last);
     void flushKalman();
     void step(int t);
 
@@ -131,6 +138,7 @@ private:
     std::vector<int> fileToDevice_;
     std::vector<int> atomBegin_;
     double forceWeight_ = 1.0;
+    int taskBatchEnergy_ = 1, taskBatchForce_ = 1;
     int type_ = -1;
     // Kalman filter state (host scalars as in KalmanFilter)
     double epsilon_ = 0.0, q_ = 0.0, q0_ = 0.0, qtau_ = 0.0, qmin_ = 0.0, eta_ = 0.0, eta0_ = 0.0, etatau_ = 0.0,

@@ -52,6 +52,7 @@ class Training:
         self.numWeights = n.value
         self.atomsPerStructure = np.array([s.numAtoms for s in self.structures], dtype=np.int64)
         self.forceWeight = 1.0
+        self.taskBatch = {ENERGY: 1, FORCE: 1}
         self.epoch = 0
 
     def close(self):
@@ -92,10 +93,17 @@ class Training:
         self.forceWeight = float(w)
         _lib.check(self._lib.n2p2_training_set_force_weight(self._h, self.forceWeight))
 
+    def setTaskBatchSize(self, energy=1, force=1):
+        """task_batch_size_energy / task_batch_size_force: candidates summed
+        into one observation per update."""
+        _lib.check(self._lib.n2p2_training_set_task_batch_size(self._h, int(energy), int(force)))
+        self.taskBatch = {ENERGY: int(energy), FORCE: int(force)}
+
     # -- updates -----------------------------------------------------------
     def update(self, prop, structure, atom=None, component=None):
-        """Updates in order; returns the errors (reference - prediction,
-        internal units) seen before each update."""
+        """Candidates in order (one update per task batch of them); returns
+        the errors (reference - prediction, internal units) of every
+        candidate, seen before its update."""
         s = np.ascontiguousarray(structure, dtype=np.int32).ravel()
         n = s.size
         errors = np.zeros(n)
@@ -134,8 +142,9 @@ class Training:
         Returns the errors per property (internal units)."""
         rng = np.random.default_rng() if rng is None else rng
         ec, (fs, fa, fc) = self.updateCandidates()
-        ne = int(energyFraction * ec.size)
-        nf = int(forceFraction * fs.size)
+        be, bf = self.taskBatch[ENERGY], self.taskBatch[FORCE]
+        ne = int(energyFraction * ec.size / be)   # updates per property
+        nf = int(forceFraction * fs.size / bf)
         eo = rng.permutation(ec.size)
         fo = rng.permutation(fs.size)
         schedule = np.concatenate([np.full(nf, FORCE), np.full(ne, ENERGY)])
@@ -149,7 +158,7 @@ class Training:
             r = k
             while r < schedule.size and schedule[r] == p:
                 r += 1
-            cnt = r - k
+            cnt = (r - k) * (be if p == ENERGY else bf)   # candidates of this run
             if p == ENERGY:
                 idx = eo[(pos[p] + np.arange(cnt)) % ec.size]
                 errs[p].append(self.update(ENERGY, ec[idx]))

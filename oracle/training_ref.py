@@ -297,10 +297,21 @@ class Training:
         return self.fref[s][atom, comp] - pred, H
 
     def update(self, prop, s, atom=0, comp=0):
-        err, H = self.observation(prop, s, atom, comp)
-        xi = err
+        return self.update_batch(prop, [(s, atom, comp)])[0]
+
+    def update_batch(self, prop, candidates):
+        """One update from a task batch of candidates: errors and Jacobians
+        summed at the same weights, then the force weight
+        (Training.cpp:2879-2923, jacobian_mode 0/1 on one process)."""
+        errs, Hs = 0.0, None
+        out = []
+        for s, atom, comp in candidates:
+            err, H = self.observation(prop, s, atom, comp)
+            out.append(err)
+            errs = errs + err
+            Hs = H if Hs is None else Hs + H
         if prop == 1:
-            xi = err * self.force_weight
-            H = H * self.force_weight
-        self.updater.update(self.nets.weights, H, xi)
-        return err
+            errs = errs * self.force_weight
+            Hs = Hs * self.force_weight
+        self.updater.update(self.nets.weights, Hs, errs)
+        return out

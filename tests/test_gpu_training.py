@@ -145,3 +145,26 @@ def test_epochs_reduce_errors(data):
     finally:
         tr.close()
         m.close()
+
+
+def test_task_batches_match_oracle(data):
+    """task_batch_size > 1: candidates summed into one observation per update."""
+    up = ("kf", UPDATERS[0][1])
+    m, tr, ref = _pair(data, up)
+    try:
+        tr.setTaskBatchSize(energy=3, force=2)
+        e = tr.update(ENERGY, [1, 3, 0, 2, 0, 1])
+        e_ref = ref.update_batch(0, [(1, 0, 0), (3, 0, 0), (0, 0, 0)]) + ref.update_batch(0, [(2, 0, 0), (0, 0, 0),
+                                                                                           (1, 0, 0)])
+        assert np.allclose(e, e_ref, rtol=1e-9, atol=1e-12)
+        cands = [(2, 7, 1), (0, 5, 2), (3, 11, 0), (1, 4, 2)]
+        s, a, c = (np.array(x) for x in zip(*cands))
+        f = tr.update(FORCE, s, a, c)
+        f_ref = ref.update_batch(1, cands[:2]) + ref.update_batch(1, cands[2:])
+        assert np.allclose(f, f_ref, rtol=1e-9, atol=1e-12)
+        assert H.max_rel(tr.weights(), ref.nets.weights) <= 1e-9
+        assert tr.kalmanStatus()["numUpdates"] == 4
+    finally:
+        tr.close()
+        m.close()
+
