@@ -377,6 +377,12 @@ n2p2_status n2p2_training_destroy(n2p2_training* training);
 n2p2_status n2p2_training_set_references(n2p2_training* training, const double* energies, const double* forces);
 /* force_weight (Training.cpp:2910-2923): scales force errors and Jacobians. */
 n2p2_status n2p2_training_set_force_weight(n2p2_training* training, double weight);
+/* update_strategy (0 combined: one updater over all weights; 1 element: one updater per element over its
+ * network's weights, the error shared by the element's fraction of the structure's atoms or of the observed
+ * atom's neighbours, Training.cpp:2900-2922).  Set it before the updater; it resets the updater. */
+#define N2P2_TRAINING_COMBINED 0
+#define N2P2_TRAINING_ELEMENT 1
+n2p2_status n2p2_training_set_update_strategy(n2p2_training* training, int32_t strategy);
 /* task_batch_size_energy / task_batch_size_force (Training.cpp:2277-2279 with jacobian_mode 0 or 1 on one
  * process): that many consecutive candidates form one observation (errors and Jacobians summed at the same
  * weights) and one updater step. */

@@ -834,6 +834,12 @@ n2p2_status n2p2_training_set_force_weight(n2p2_training* training, double weigh
     });
 }
 
+n2p2_status n2p2_training_set_update_strategy(n2p2_training* training, int32_t strategy)
+{
+    N2P2_REQUIRE(training);
+    return guard([&] { training->training->setUpdateStrategy(strategy); });
+}
+
 n2p2_status n2p2_training_set_task_batch_size(n2p2_training* training, int32_t energy, int32_t force)
 {
     N2P2_REQUIRE(training);

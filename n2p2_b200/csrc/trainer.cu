@@ -630,12 +630,23 @@ __global__ void __launch_bounds__(128) kKalmanPX(double* __restrict__ Pm, const 
     if (threadIdx.x == 0) X[i] = part[0];
 }
 
+// The updater's error: xi as it is (div == 0), or the per-element share
+// (xi * mul) / div * post (Training.cpp:2900-2922 with update_strategy 1:
+// mul / div the element's atoms / all atoms, or the atom's neighbours of the
+// element / all its neighbours; post the force weight).
+__device__ __forceinline__ double updaterError(const double* xi, double mul, double div, double post)
+{
+    const double e = *xi;
+    return div == 0.0 ? e : e * mul / div * post;
+}
+
 // A = H^T X + diag (one observation), K = X A^-1, w += K xi (the transposed
 // weight copy follows).  One block, fixed reduction order.
 __global__ void __launch_bounds__(1024) kKalmanGain(const double* __restrict__ H, const double* __restrict__ X, int n,
-                                                    double diag, const double* __restrict__ xi,
-                                                    double* __restrict__ K, double* __restrict__ w,
-                                                    double* __restrict__ wT, const int* __restrict__ tidx)
+                                                    double diag, const double* __restrict__ xi, double mul,
+                                                    double div, double post, double* __restrict__ K,
+                                                    double* __restrict__ w, double* __restrict__ wT,
+                                                    const int* __restrict__ tidx)
 {
     __shared__ double part[1024];
     double a = 0.0;
@@ -648,7 +659,7 @@ __global__ void __launch_bounds__(1024) kKalmanGain(const double* __restrict__ H
         __syncthreads();
     }
     const double inv = 1.0 / (part[0] + diag);
-    const double e = *xi;
+    const double e = updaterError(xi, mul, div, post);
     for (int i = threadIdx.x; i < n; i += blockDim.x)
     {
         const double k = X[i] * inv;
@@ -684,10 +695,11 @@ __global__ void kKalmanInit(double* __restrict__ Pm, int n, double d)
 }
 
 // GradientDescent::update, DT_FIXED: state -= eta * error * -gradient.
-__global__ void kGradFixed(int n, const double* __restrict__ H, const double* __restrict__ xi, double eta,
-                           double* __restrict__ w, double* __restrict__ wT, const int* __restrict__ tidx)
+__global__ void kGradFixed(int n, const double* __restrict__ H, const double* __restrict__ xi, double mul,
+                           double div, double post, double eta, double* __restrict__ w, double* __restrict__ wT,
+                           const int* __restrict__ tidx)
 {
-    const double e = *xi;
+    const double e = updaterError(xi, mul, div, post);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
         const double wi = w[i] - eta * e * -H[i];
@@ -697,11 +709,12 @@ __global__ void kGradFixed(int n, const double* __restrict__ H, const double* __
 }
 
 // GradientDescent::update, DT_ADAM, with g = error * -gradient.
-__global__ void kGradAdam(int n, const double* __restrict__ H, const double* __restrict__ xi, double beta1,
-                          double beta2, double eta, double eps, double* __restrict__ m, double* __restrict__ v,
-                          double* __restrict__ w, double* __restrict__ wT, const int* __restrict__ tidx)
+__global__ void kGradAdam(int n, const double* __restrict__ H, const double* __restrict__ xi, double mul, double div,
+                          double post, double beta1, double beta2, double eta, double eps, double* __restrict__ m,
+                          double* __restrict__ v, double* __restrict__ w, double* __restrict__ wT,
+                          const int* __restrict__ tidx)
 {
-    const double e = *xi;
+    const double e = updaterError(xi, mul, div, post);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
         const double gi = e * -H[i];
@@ -791,6 +804,47 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
     cudaCheck(cudaStreamSynchronize(st), "sync");
     int maxAtoms = 0;
     for (int k = 0; k < S_; ++k) maxAtoms = std::max(maxAtoms, atomBegin_[k + 1] - atomBegin_[k]);
+    // per element: its contiguous block of device weights, atoms per structure, neighbours per atom
+    const int ne = v.numElements;
+    size_t fpos = 0;
+    for (int e = 0; e < ne; ++e)
+    {
+        DevElement const& E = v.el[e];
+        int cnt = 0;
+        for (int l = 1; l < E.numLayers; ++l) cnt += E.neurons[l] * E.neurons[l - 1] + E.neurons[l];
+        int lo = P_, hi = 0;
+        for (int q = 0; q < cnt; ++q)
+        {
+            lo = std::min(lo, fileToDevice_[fpos + q]);
+            hi = std::max(hi, fileToDevice_[fpos + q] + 1);
+        }
+        if (hi - lo != cnt) throw std::runtime_error("ERROR: element weights are not contiguous.\n");
+        elemRange_.push_back({lo, cnt});
+        fpos += cnt;
+    }
+    {
+        std::vector<int> elem(N_);
+        std::vector<int64_t> off((size_t)N_ + 1);
+        cudaCheck(cudaMemcpyAsync(elem.data(), b.elem, sizeof(int) * N_, cudaMemcpyDeviceToHost, st), "D2H");
+        cudaCheck(cudaMemcpyAsync(off.data(), b.nbrOffset, sizeof(int64_t) * (N_ + 1), cudaMemcpyDeviceToHost, st),
+                  "D2H");
+        cudaCheck(cudaStreamSynchronize(st), "sync");
+        std::vector<int> nj((size_t)off[N_]);
+        if (!nj.empty())
+            cudaCheck(cudaMemcpyAsync(nj.data(), b.nbrJ, sizeof(int) * nj.size(), cudaMemcpyDeviceToHost, st), "D2H");
+        cudaCheck(cudaStreamSynchronize(st), "sync");
+        atomsPerElement_.assign((size_t)S_ * ne, 0);
+        for (int k = 0; k < S_; ++k)
+            for (int i = atomBegin_[k]; i < atomBegin_[k + 1]; ++i) ++atomsPerElement_[(size_t)k * ne + elem[i]];
+        nbrPerElement_.assign((size_t)N_ * ne, 0);
+        nbrCount_.assign(N_, 0);
+        for (int i = 0; i < N_; ++i)
+        {
+            nbrCount_[i] = (int)(off[i + 1] - off[i]);
+            for (int64_t q = off[i]; q < off[i + 1]; ++q) ++nbrPerElement_[(size_t)i * ne + elem[nj[q]]];
+        }
+    }
+    blocks_.push_back({0, P_, 0});
     maxWarps_ = std::min(maxAtoms, sms_ * 8);
     maxWarps_ = (maxWarps_ + kTrainWarps - 1) / kTrainWarps * kTrainWarps;
     eRef_ = tAlloc<double>(S_);
@@ -838,11 +892,7 @@ void Training::setKalmanStandard(double epsilon, double q0, double qtau, double 
                                  double etamax)
 {
     // KalmanFilter::KalmanFilter (P = I) and setParametersStandard (P /= epsilon), KalmanFilter.cpp:62-117, 199-218
-    if (!Pm_) Pm_ = tAlloc<double>((size_t)P_ * P_);
-    kKalmanInit<<<sms_ * 8, 256, 0, set_.stream()>>>(Pm_, P_, 1.0 / epsilon);
-    cudaCheck(cudaGetLastError(), "kalman init");
-    pending_ = false;
-    cudaCheck(cudaMemsetAsync(Kb_[cur_], 0, sizeof(double) * P_, set_.stream()), "memset");
+    initKalman(epsilon);
     type_ = KF_STANDARD;
     epsilon_ = epsilon;
     q0_ = q0;
@@ -859,11 +909,7 @@ void Training::setKalmanStandard(double epsilon, double q0, double qtau, double 
 void Training::setKalmanFadingMemory(double epsilon, double q0, double qtau, double qmin, double lambda, double nu)
 {
     // KalmanFilter::setParametersFadingMemory, KalmanFilter.cpp:220-238
-    if (!Pm_) Pm_ = tAlloc<double>((size_t)P_ * P_);
-    kKalmanInit<<<sms_ * 8, 256, 0, set_.stream()>>>(Pm_, P_, 1.0 / epsilon);
-    cudaCheck(cudaGetLastError(), "kalman init");
-    pending_ = false;
-    cudaCheck(cudaMemsetAsync(Kb_[cur_], 0, sizeof(double) * P_, set_.stream()), "memset");
+    initKalman(epsilon);
     type_ = KF_FADING_MEMORY;
     epsilon_ = epsilon;
     q0_ = q0;
@@ -934,18 +980,43 @@ void Training::observation(int property, int s, int a, int c, int t, bool accumu
     cudaCheck(cudaGetLastError(), "observation launch");
 }
 
-// The updater's step with the observation in H_ / xi_.
-void Training::step(int t)
+// The updaters' step with the observation in H_ / xi_: one updater over all
+// weights (combined strategy) or one per element over its block of weights
+// (element strategy), each with its share of the error.
+void Training::step(int property, int s, int a)
 {
-    (void)t;
     cudaStream_t st = set_.stream();
     double* w = dmodel_.weightsDevice();
     double* wT = dmodel_.weightsTDevice();
     const int* tidx = dmodel_.transIndexDevice();
     const int tb = 256;
+    const int ne = (int)blocks_.size();
+    const bool element = strategy_ == US_ELEMENT;
+    auto share = [&](int e, double& mul, double& div) {
+        if (!element)
+        {
+            mul = 1.0;
+            div = 0.0;
+        }
+        else if (property == ENERGY)
+        {
+            mul = (double)atomsPerElement_[(size_t)s * ne + e];
+            div = (double)(atomBegin_[s + 1] - atomBegin_[s]);
+        }
+        else
+        {
+            const size_t k = (size_t)(atomBegin_[s] + a);
+            mul = (double)nbrPerElement_[k * ne + e];
+            div = (double)nbrCount_[k];
+        }
+    };
+    // the combined path reads the scaled error; the element path scales the raw one itself
+    const double* xiPtr = element ? xi_ + 1 : xi_;
+    const double post = element && property == FORCE ? forceWeight_ : 1.0;
     if (type_ == KF_STANDARD || type_ == KF_FADING_MEMORY)
     {
-        // KalmanFilter::update (KalmanFilter.cpp:126-197), one observation
+        // KalmanFilter::update (KalmanFilter.cpp:126-197), one observation per updater; the
+        // updaters advance in lockstep, so their eta, q, lambda and gamma are shared scalars
         double diag, scale = 1.0;
         if (type_ == KF_STANDARD)
         {
@@ -959,9 +1030,17 @@ void Training::step(int t)
         }
         // this update's X with the previous update's P update applied on the way
         const int cur = cur_ ^ 1;
-        kKalmanPX<<<P_, 128, 0, st>>>(Pm_, Kb_[cur_], Xb_[cur_], P_, pending_ ? 1 : 0, pendingScale_, pendingQ_, H_,
-                                      Xb_[cur]);
-        kKalmanGain<<<1, 1024, 0, st>>>(H_, Xb_[cur], P_, diag, xi_, Kb_[cur], w, wT, tidx);
+        for (int e = 0; e < ne; ++e)
+        {
+            Block const& B = blocks_[e];
+            double mul, div;
+            share(e, mul, div);
+            kKalmanPX<<<B.count, 128, 0, st>>>(Pm_ + B.pOffset, Kb_[cur_] + B.begin, Xb_[cur_] + B.begin, B.count,
+                                               pending_ ? 1 : 0, pendingScale_, pendingQ_, H_ + B.begin,
+                                               Xb_[cur] + B.begin);
+            kKalmanGain<<<1, 1024, 0, st>>>(H_ + B.begin, Xb_[cur] + B.begin, B.count, diag, xiPtr, mul, div, post,
+                                            Kb_[cur] + B.begin, w + B.begin, wT, tidx + B.begin);
+        }
         cur_ = cur;
         pending_ = true;   // P - K X^T, * scale, + q I: applied by the next pass over P
         pendingScale_ = scale;
@@ -975,17 +1054,60 @@ void Training::step(int t)
     }
     else if (type_ == GD_FIXED)
     {
-        kGradFixed<<<(P_ + tb - 1) / tb, tb, 0, st>>>(P_, H_, xi_, gdEta_, w, wT, tidx);
+        for (int e = 0; e < ne; ++e)
+        {
+            Block const& B = blocks_[e];
+            double mul, div;
+            share(e, mul, div);
+            kGradFixed<<<(B.count + tb - 1) / tb, tb, 0, st>>>(B.count, H_ + B.begin, xiPtr, mul, div, post, gdEta_,
+                                                               w + B.begin, wT, tidx + B.begin);
+        }
     }
     else
     {
         const double eta = gdEta_ * std::sqrt(1.0 - beta2t_) / (1.0 - beta1t_);
-        kGradAdam<<<(P_ + tb - 1) / tb, tb, 0, st>>>(P_, H_, xi_, beta1_, beta2_, eta, gdEps_, m_, v_, w, wT, tidx);
+        for (int e = 0; e < ne; ++e)
+        {
+            Block const& B = blocks_[e];
+            double mul, div;
+            share(e, mul, div);
+            kGradAdam<<<(B.count + tb - 1) / tb, tb, 0, st>>>(B.count, H_ + B.begin, xiPtr, mul, div, post, beta1_,
+                                                              beta2_, eta, gdEps_, m_ + B.begin, v_ + B.begin,
+                                                              w + B.begin, wT, tidx + B.begin);
+        }
         beta1t_ *= beta1_;
         beta2t_ *= beta2_;
     }
     cudaCheck(cudaGetLastError(), "updater launch");
     ++numUpdates_;
+}
+
+void Training::setUpdateStrategy(int strategy)
+{
+    if (strategy != US_COMBINED && strategy != US_ELEMENT) throw std::invalid_argument("ERROR: unknown update strategy.\n");
+    strategy_ = strategy;
+    blocks_.clear();
+    if (strategy == US_COMBINED) blocks_.push_back({0, P_, 0});
+    else
+    {
+        size_t off = 0;
+        for (auto const& r : elemRange_)
+        {
+            blocks_.push_back({r.first, r.second, off});
+            off += (size_t)r.second * r.second;
+        }
+    }
+    type_ = -1;   // the updater is set up again for the new blocks
+}
+
+void Training::initKalman(double epsilon)
+{
+    if (!Pm_) Pm_ = tAlloc<double>((size_t)P_ * P_);
+    for (Block const& B : blocks_)
+        kKalmanInit<<<sms_ * 8, 256, 0, set_.stream()>>>(Pm_ + B.pOffset, B.count, 1.0 / epsilon);
+    cudaCheck(cudaGetLastError(), "kalman init");
+    pending_ = false;
+    cudaCheck(cudaMemsetAsync(Kb_[cur_], 0, sizeof(double) * P_, set_.stream()), "memset");
 }
 
 void Training::update(int property, int count, const int* structure, const int* atom, const int* component,
@@ -1014,6 +1136,8 @@ void Training::update(int property, int count, const int* structure, const int* 
     // a task batch of candidates forms one observation: errors and Jacobians
     // summed at the same weights, then one updater step (Training.cpp:2879-2923)
     const int batch = property == ENERGY ? taskBatchEnergy_ : taskBatchForce_;
+    if (strategy_ == US_ELEMENT && batch != 1)
+        throw std::invalid_argument("ERROR: the element update strategy needs task batches of one candidate.\n");
     if (count % batch != 0)
         throw std::invalid_argument("ERROR: the number of candidates is not a multiple of the task batch size.\n");
     for (int t = 0; t < count; ++t)
@@ -1021,7 +1145,7 @@ void Training::update(int property, int count, const int* structure, const int* 
         const int q = t % batch;
         observation(property, structure[t], property == FORCE ? atom[t] : 0, property == FORCE ? component[t] : 0, t,
                     q > 0, q == batch - 1);
-        if (q == batch - 1) step(t);
+        if (q == batch - 1) step(property, structure[t], property == FORCE ? atom[t] : 0);
     }
     if (errors)
         cudaCheck(cudaMemcpyAsync(errors, err_, sizeof(double) * count, cudaMemcpyDeviceToHost, st), "D2H");
@@ -1053,8 +1177,12 @@ void Training::observe(int property, int structure, int atom, int component, dou
 void Training::flushKalman()
 {
     if (!pending_) return;
-    dim3 grid((P_ + 255) / 256, P_);
-    kKalmanP<<<grid, 256, 0, set_.stream()>>>(Pm_, Kb_[cur_], Xb_[cur_], P_, pendingScale_, pendingQ_);
+    for (Block const& B : blocks_)
+    {
+        dim3 grid((B.count + 255) / 256, B.count);
+        kKalmanP<<<grid, 256, 0, set_.stream()>>>(Pm_ + B.pOffset, Kb_[cur_] + B.begin, Xb_[cur_] + B.begin, B.count,
+                                                  pendingScale_, pendingQ_);
+    }
     cudaCheck(cudaGetLastError(), "kalman flush");
     pending_ = false;
 }
@@ -1066,22 +1194,27 @@ void Training::kalmanStatus(double* out)
     out[1] = out[2] = out[3] = 0.0;
     if (Pm_ && (type_ == KF_STANDARD || type_ == KF_FADING_MEMORY))
     {
+        // over all updaters' covariance blocks (one block for the combined strategy)
         cudaStream_t st = set_.stream();
-        kKalmanStat<<<kStatBlocks, 256, 0, st>>>(Pm_, Kb_[cur_], P_, stat_);
+        double d = 0.0, a = 0.0, k = 0.0, offCount = 0.0;
         std::vector<double> part(3 * kStatBlocks);
-        cudaCheck(cudaMemcpyAsync(part.data(), stat_, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st),
-                  "D2H");
-        cudaCheck(cudaStreamSynchronize(st), "sync");
-        double d = 0.0, a = 0.0, k = 0.0;
-        for (int bIdx = 0; bIdx < kStatBlocks; ++bIdx)
+        for (Block const& B : blocks_)
         {
-            d += part[3 * bIdx];
-            a += part[3 * bIdx + 1];
-            k += part[3 * bIdx + 2];
+            kKalmanStat<<<kStatBlocks, 256, 0, st>>>(Pm_ + B.pOffset, Kb_[cur_] + B.begin, B.count, stat_);
+            cudaCheck(cudaMemcpyAsync(part.data(), stat_, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, st),
+                      "D2H");
+            cudaCheck(cudaStreamSynchronize(st), "sync");
+            for (int bIdx = 0; bIdx < kStatBlocks; ++bIdx)
+            {
+                d += part[3 * bIdx];
+                a += part[3 * bIdx + 1];
+                k += part[3 * bIdx + 2];
+            }
+            offCount += (double)B.count * (B.count - 1.0);
         }
         const double n = (double)P_;
         out[1] = d / n;
-        out[2] = (a - d) / (n * (n - 1.0));
+        out[2] = (a - d) / offCount;
         out[3] = k / n;
     }
     out[4] = q_;

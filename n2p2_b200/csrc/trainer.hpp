@@ -87,6 +87,7 @@ class Training
 public:
     enum Property { ENERGY = 0, FORCE = 1 };
     enum UpdaterType { KF_STANDARD = 0, KF_FADING_MEMORY = 1, GD_FIXED = 2, GD_ADAM = 3 };
+    enum UpdateStrategy { US_COMBINED = 0, US_ELEMENT = 1 };
 
     Training(Model& model, DeviceModel& dmodel, Batch& set, int sms);
     ~Training();
@@ -98,6 +99,11 @@ public:
     void setReferences(const double* energiesPhys, const double* forcesPhys);
     void setForceWeight(double w) { forceWeight_ = w; }
     // task_batch_size_energy / _force: candidates summed into one observation per update.
+    // update_strategy (Training.cpp, US_COMBINED / US_ELEMENT): one updater over
+    // all weights, or one per element over its networks' weights with the
+    // error shared by the element's fraction of the atoms (energies) or of the
+    // observed atom's neighbours (forces).  Set it before the updater.
+    void setUpdateStrategy(int strategy);
     void setTaskBatchSize(int energy, int force)
     {
         taskBatchEnergy_ = energy;
@@ -128,7 +134,19 @@ public:
 private:
     void observation(int property, int s, int a, int c, int t, bool accumulate, bool last);
     void flushKalman();
-    void step(int t);
+    void initKalman(double epsilon);
+    void step(int property, int s, int a);
+    struct Block
+    {
+        int begin, count;     // device weights [begin, begin + count)
+        size_t pOffset;       // its covariance (count x count) inside Pm_
+    };
+    int strategy_ = US_COMBINED;
+    std::vector<Block> blocks_;
+    std::vector<std::pair<int, int>> elemRange_;
+    std::vector<int> atomsPerElement_;   // [S][elements]
+    std::vector<int> nbrPerElement_;     // [N][elements]
+    std::vector<int> nbrCount_;          // [N]
 
     Model& model_;
     DeviceModel& dmodel_;

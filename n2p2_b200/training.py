@@ -93,6 +93,11 @@ class Training:
         self.forceWeight = float(w)
         _lib.check(self._lib.n2p2_training_set_force_weight(self._h, self.forceWeight))
 
+    def setUpdateStrategy(self, strategy=0):
+        """update_strategy 0 (combined) or 1 (one updater per element); call
+        before setting up the updater."""
+        _lib.check(self._lib.n2p2_training_set_update_strategy(self._h, int(strategy)))
+
     def setTaskBatchSize(self, energy=1, force=1):
         """task_batch_size_energy / task_batch_size_force: candidates summed
         into one observation per update."""

@@ -299,6 +299,30 @@ class Training:
     def update(self, prop, s, atom=0, comp=0):
         return self.update_batch(prop, [(s, atom, comp)])[0]
 
+    def update_element(self, prop, s, atom=0, comp=0):
+        """update_strategy 1: one updater per element (self.updater a list),
+        each on its element's weights with the error times the element's
+        fraction of the atoms (energy) or of the atom's neighbours (force),
+        then the force weight (Training.cpp:2900-2922)."""
+        err, H = self.observation(prop, s, atom, comp)
+        d = self.data[s]
+        ne = len(self.nets.symbols)
+        if prop == 0:
+            frac = [(np.sum(d.elem == e), d.n) for e in range(ne)]
+        else:
+            js = d.nbr_index[d.nbr_offset[atom]:d.nbr_offset[atom + 1]]
+            frac = [(np.sum(d.elem[js] == e), js.size) for e in range(ne)]
+        for e in range(ne):
+            o0, o1 = self.nets.offsets[e], self.nets.offsets[e + 1]
+            xi = err * float(frac[e][0]) / float(frac[e][1])
+            He = H[o0:o1]
+            if prop == 1:
+                xi = xi * self.force_weight
+                He = He * self.force_weight
+            w = self.nets.weights[o0:o1]      # a view: the updater changes the weights in place
+            self.updater[e].update(w, He, xi)
+        return err
+
     def update_batch(self, prop, candidates):
         """One update from a task batch of candidates: errors and Jacobians
         summed at the same weights, then the force weight

@@ -168,3 +168,42 @@ def test_task_batches_match_oracle(data):
         tr.close()
         m.close()
 
+
+@pytest.mark.parametrize("kind", ["kf", "adam"])
+def test_element_strategy_matches_oracle(data, kind):
+    """update_strategy 1: one updater per element with its share of the error."""
+    from oracle import training_ref as T
+    ss, E, F, w0 = data
+    m = Mode(0)
+    m.setupFromDirectory(H.WATER40)
+    tr = Training(m, ss, E, F)
+    try:
+        tr.setWeights(w0)
+        tr.setForceWeight(3.0)
+        tr.setUpdateStrategy(1)
+        ref = T.Training(H.WATER40, ss, E, F, None, force_weight=3.0)
+        ref.nets.weights = w0.copy()
+        offs = ref.nets.offsets
+        sizes = [offs[e + 1] - offs[e] for e in range(len(offs) - 1)]
+        if kind == "kf":
+            a = UPDATERS[0][1]
+            tr.setupUpdaterKalman(0, **a)
+            ref.updater = [T.KalmanFilter(n, 0, a["epsilon"], a["q0"], a["qtau"], a["qmin"], a["eta"], a["etatau"],
+                                          a["etamax"]) for n in sizes]
+        else:
+            tr.setupUpdaterGradient(1, adam_eta=1e-3)
+            ref.updater = [T.GradientDescent(n, 1, 1e-3) for n in sizes]
+        for prop, cands in SCHEDULE:
+            if prop == ENERGY:
+                errs = tr.update(ENERGY, cands)
+                errs_ref = [ref.update_element(0, s) for s in cands]
+            else:
+                s, a_, c = (np.array(x) for x in zip(*cands))
+                errs = tr.update(FORCE, s, a_, c)
+                errs_ref = [ref.update_element(1, *x) for x in cands]
+            assert np.allclose(errs, errs_ref, rtol=1e-9, atol=1e-12)
+            assert H.max_rel(tr.weights(), ref.nets.weights) <= 1e-9
+    finally:
+        tr.close()
+        m.close()
+
