@@ -410,6 +410,18 @@ n2p2_status n2p2_training_update(n2p2_training* training, int32_t property, int3
  * Training::update hands to its updater. */
 n2p2_status n2p2_training_observe(n2p2_training* training, int32_t property, int32_t structure, int32_t atom,
                                   int32_t component, double* error, double* jacobian);
+/* selection_mode 2 (threshold, Training.cpp:2288-2527): num_updates updates; each tries the candidates
+ * of the list in order (wrapping), at most `trials`, until one's |error| exceeds threshold x rmse (rmse:
+ * the training RMSE in internal units -- energy per atom times the structure's atoms, or force component);
+ * the update uses the candidate the trials stopped at (the reference's behaviour also when none exceeds).
+ * *consumed receives the number of candidates taken from the list, errors[u] the used one's error. */
+n2p2_status n2p2_training_update_threshold(n2p2_training* training, int32_t property, int32_t num_updates,
+                                           int32_t num_candidates, const int32_t* structure, const int32_t* atom,
+                                           const int32_t* component, double threshold, int32_t trials, double rmse,
+                                           int32_t* consumed, double* errors);
+/* Training errors at the current weights, internal units (Training::calculateError): RMSE of the energy
+ * per atom and of the force components over the set; errors[2]. */
+n2p2_status n2p2_training_get_errors(n2p2_training* training, double* errors);
 /* KalmanFilter::status: {numUpdates, mean |P_ii|, mean |P_ij| (i != j),
  * mean |K|, q, eta (standard) or lambda (fading memory), gamma}. */
 n2p2_status n2p2_training_get_kalman_status(n2p2_training* training, double* status);

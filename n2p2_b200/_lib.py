@@ -107,6 +107,10 @@ SIGNATURES = {
                                   _P(ctypes.c_int32), _P(_d)]),
     "n2p2_training_observe": (_i, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P(_d),
                                    _P(_d)]),
+    "n2p2_training_update_threshold": (_i, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                            _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_int32), _d,
+                                            ctypes.c_int32, _d, _P(ctypes.c_int32), _P(_d)]),
+    "n2p2_training_get_errors": (_i, [_vp, _P(_d)]),
     "n2p2_training_get_kalman_status": (_i, [_vp, _P(_d)]),
     "n2p2_training_get_num_weights": (_i, [_vp, _P(_i64)]),
     "n2p2_training_get_weights": (_i, [_vp, _P(_d)]),

@@ -919,6 +919,34 @@ n2p2_status n2p2_training_observe(n2p2_training* training, int32_t property, int
     });
 }
 
+n2p2_status n2p2_training_update_threshold(n2p2_training* training, int32_t property, int32_t num_updates,
+                                           int32_t num_candidates, const int32_t* structure, const int32_t* atom,
+                                           const int32_t* component, double threshold, int32_t trials, double rmse,
+                                           int32_t* consumed, double* errors)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(structure);
+    N2P2_REQUIRE(num_updates >= 0);
+    N2P2_REQUIRE(property != N2P2_TRAINING_FORCE || (atom && component));
+    return guard([&] {
+        setDevice(training->mode);
+        if (!(rmse > 0.0)) throw std::invalid_argument("ERROR: the training RMSE must be positive.\n");
+        const int n = training->training->updateThreshold(property, num_updates, num_candidates, structure, atom,
+                                                          component, threshold, trials, rmse, errors);
+        if (consumed) *consumed = n;
+    });
+}
+
+n2p2_status n2p2_training_get_errors(n2p2_training* training, double* errors)
+{
+    N2P2_REQUIRE(training);
+    N2P2_REQUIRE(errors);
+    return guard([&] {
+        setDevice(training->mode);
+        training->training->trainingErrors(errors, errors + 1);
+    });
+}
+
 n2p2_status n2p2_training_get_kalman_status(n2p2_training* training, double* status)
 {
     N2P2_REQUIRE(training);

@@ -883,6 +883,8 @@ void Training::setReferences(const double* energiesPhys, const double* forcesPhy
     const double cf = set_.forceToInternal();
     for (size_t q = 0; q < f.size(); ++q) f[q] = forcesPhys[q] * cf;
     cudaStream_t st = set_.stream();
+    eRefHost_ = e;
+    fRefHost_ = f;
     cudaCheck(cudaMemcpyAsync(eRef_, e.data(), sizeof(double) * S_, cudaMemcpyHostToDevice, st), "H2D");
     cudaCheck(cudaMemcpyAsync(fRef_, f.data(), sizeof(double) * f.size(), cudaMemcpyHostToDevice, st), "H2D");
     cudaCheck(cudaStreamSynchronize(st), "sync");
@@ -1150,6 +1152,92 @@ void Training::update(int property, int count, const int* structure, const int* 
     if (errors)
         cudaCheck(cudaMemcpyAsync(errors, err_, sizeof(double) * count, cudaMemcpyDeviceToHost, st), "D2H");
     cudaCheck(cudaStreamSynchronize(st), "sync");
+}
+
+int Training::updateThreshold(int property, int numUpdates, int numCandidates, const int* structure, const int* atom,
+                              const int* component, double threshold, int trials, double rmse, double* errors)
+{
+    if (type_ < 0) throw std::runtime_error("ERROR: no updater set.\n");
+    if (property != ENERGY && property != FORCE) throw std::invalid_argument("ERROR: unknown property.\n");
+    if ((property == ENERGY ? taskBatchEnergy_ : taskBatchForce_) != 1)
+        throw std::invalid_argument("ERROR: threshold selection needs task batches of one candidate.\n");
+    if (numCandidates < 1 || trials < 1) throw std::invalid_argument("ERROR: no candidates or trials.\n");
+    for (int t = 0; t < numCandidates; ++t)
+    {
+        const int s = structure[t];
+        if (s < 0 || s >= S_) throw std::out_of_range("ERROR: structure index out of range.\n");
+        if (property == FORCE && (atom[t] < 0 || atom[t] >= atomBegin_[s + 1] - atomBegin_[s] || component[t] < 0 ||
+                                  component[t] > 2))
+            throw std::out_of_range("ERROR: atom or component out of range.\n");
+    }
+    if (errCap_ < 1)
+    {
+        errCap_ = 1;
+        err_ = tAlloc<double>(1);
+    }
+    cudaStream_t st = set_.stream();
+    int pos = 0;
+    auto obs = [&](int k) {
+        observation(property, structure[k], property == FORCE ? atom[k] : 0, property == FORCE ? component[k] : 0, 0,
+                    false, true);
+        double e = 0.0;
+        cudaCheck(cudaMemcpyAsync(&e, err_, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
+        cudaCheck(cudaStreamSynchronize(st), "sync");
+        return e;
+    };
+    for (int u = 0; u < numUpdates; ++u)
+    {
+        // When no trial exceeds the threshold the reference records the best
+        // candidate but updates with the one it tried last (the candidate
+        // pointer c is not reset to indexBest, Training.cpp:2492-2505, and
+        // c->s is the structure used at :2527); so does this loop.
+        int chosen = -1;
+        double chosenErr = 0.0;
+        for (int il = 0; il < trials; ++il)
+        {
+            const int k = pos % numCandidates;
+            const double e = obs(k);
+            const int s = structure[k];
+            const double frac =
+                property == ENERGY ? std::fabs(e) / ((atomBegin_[s + 1] - atomBegin_[s]) * rmse) : std::fabs(e) / rmse;
+            ++pos;
+            chosen = k;
+            chosenErr = e;
+            if (frac > threshold) break;
+        }
+        step(property, structure[chosen], property == FORCE ? atom[chosen] : 0);
+        if (errors) errors[u] = chosenErr;
+    }
+    cudaCheck(cudaStreamSynchronize(st), "sync");
+    return pos;
+}
+
+void Training::trainingErrors(double* rmseEnergyPerAtom, double* rmseForce)
+{
+    if (eRefHost_.empty()) throw std::runtime_error("ERROR: no references set.\n");
+    flushKalman();
+    set_.evaluate(EVAL_FORCES | EVAL_STORE_DGDR | EVAL_NO_GRAPH, PREC_FP64, 0);
+    BatchView const& b = set_.view();
+    cudaStream_t st = set_.stream();
+    std::vector<double> E(S_), F(3 * (size_t)N_);
+    cudaCheck(cudaMemcpyAsync(E.data(), b.Estruct, sizeof(double) * S_, cudaMemcpyDeviceToHost, st), "D2H");
+    cudaCheck(cudaMemcpyAsync(F.data(), b.F, sizeof(double) * F.size(), cudaMemcpyDeviceToHost, st), "D2H");
+    cudaCheck(cudaStreamSynchronize(st), "sync");
+    // Structure::updateError / Atom::updateError summed, Training::collectError
+    double se = 0.0, sf = 0.0;
+    for (int k = 0; k < S_; ++k)
+    {
+        const double n = (double)(atomBegin_[k + 1] - atomBegin_[k]);
+        const double d = eRefHost_[k] - E[k];
+        se += d * d / (n * n);
+    }
+    for (size_t q = 0; q < F.size(); ++q)
+    {
+        const double d = fRefHost_[q] - F[q];
+        sf += d * d;
+    }
+    *rmseEnergyPerAtom = std::sqrt(se / S_);
+    *rmseForce = std::sqrt(sf / (double)F.size());
 }
 
 void Training::observe(int property, int structure, int atom, int component, double* error,

@@ -124,6 +124,17 @@ public:
     // Error (ref - prediction, internal units) and Jacobian (weight-file order,
     // force weight applied for forces) of one observation, no update.
     void observe(int property, int structure, int atom, int component, double* error, double* jacobianFileOrder);
+    // selection_mode 2 (threshold, Training.cpp:2288-2447): `numUpdates`
+    // updates; each tries candidates from the list in order (wrapping) until
+    // one's error exceeds `threshold` times the training RMSE (`rmse`: energy
+    // per atom, or force component; internal units), at most `trials`; the
+    // update uses the candidate the trials stopped at.  Returns the
+    // candidates consumed; errors[u] is the used candidate's error.
+    int updateThreshold(int property, int numUpdates, int numCandidates, const int* structure, const int* atom,
+                        const int* component, double threshold, int trials, double rmse, double* errors);
+    // Training errors at the current weights, internal units (Training::calculateError):
+    // RMSE of the energy per atom and of the force components over the set.
+    void trainingErrors(double* rmseEnergyPerAtom, double* rmseForce);
     // KalmanFilter::status: numUpdates, mean |P_ii|, mean |P_ij| (i != j),
     // mean |K|, q, eta (standard) or lambda (fading memory), gamma.
     void kalmanStatus(double* out);
@@ -157,6 +168,7 @@ private:
     std::vector<int> atomBegin_;
     double forceWeight_ = 1.0;
     int taskBatchEnergy_ = 1, taskBatchForce_ = 1;
+    std::vector<double> eRefHost_, fRefHost_;   // references, internal units
     int type_ = -1;
     // Kalman filter state (host scalars as in KalmanFilter)
     double epsilon_ = 0.0, q_ = 0.0, q0_ = 0.0, qtau_ = 0.0, qmin_ = 0.0, eta_ = 0.0, eta0_ = 0.0, etatau_ = 0.0,

@@ -131,6 +131,35 @@ class Training:
                                                    _dp(err), _dp(jac)))
         return float(err[0]), jac
 
+    def updateThreshold(self, prop, numUpdates, structure, atom=None, component=None, threshold=1.0, trials=3,
+                        rmse=None):
+        """selection_mode 2: `numUpdates` updates over the candidate list
+        (see n2p2_training_update_threshold); rmse defaults to the current
+        training RMSE (internal units).  Returns (candidates consumed, errors
+        of the used candidates)."""
+        s = np.ascontiguousarray(structure, dtype=np.int32).ravel()
+        if rmse is None:
+            rmse = self.trainingErrors()[0 if prop == ENERGY else 1]
+        errors = np.zeros(numUpdates)
+        used = ctypes.c_int32()
+        if prop == FORCE:
+            a = np.ascontiguousarray(atom, dtype=np.int32).ravel()
+            c = np.ascontiguousarray(component, dtype=np.int32).ravel()
+            _lib.check(self._lib.n2p2_training_update_threshold(self._h, FORCE, numUpdates, s.size, _ip(s), _ip(a),
+                                                                _ip(c), threshold, trials, rmse, ctypes.byref(used),
+                                                                _dp(errors)))
+        else:
+            _lib.check(self._lib.n2p2_training_update_threshold(self._h, ENERGY, numUpdates, s.size, _ip(s), None,
+                                                                None, threshold, trials, rmse, ctypes.byref(used),
+                                                                _dp(errors)))
+        return used.value, errors
+
+    def trainingErrors(self):
+        """(RMSE energy per atom, RMSE force components), internal units."""
+        out = np.zeros(2)
+        _lib.check(self._lib.n2p2_training_get_errors(self._h, _dp(out)))
+        return float(out[0]), float(out[1])
+
     def updateCandidates(self):
         """Energy candidates (structures) and force candidates (structure,
         atom, component), Training::setupUpdateCandidates for 2G."""
@@ -140,12 +169,15 @@ class Training:
         c = np.tile(np.arange(3, dtype=np.int32), int(self.atomsPerStructure.sum()))
         return e, (s, a, c)
 
-    def runEpoch(self, energyFraction=1.0, forceFraction=0.0, rng=None):
+    def runEpoch(self, energyFraction=1.0, forceFraction=0.0, rng=None, selectionMode=0, threshold=1.0, trials=3):
         """One epoch of Training::loop: candidates shuffled per property, the
         energy and force updates (fraction x candidates each) in a shuffled
-        schedule, each update taking the next candidate of its property.
+        schedule, each update taking the next candidate of its property
+        (selectionMode 0) or trying candidates against threshold x the
+        training RMSE at the epoch's start (selectionMode 2, up to `trials`).
         Returns the errors per property (internal units)."""
         rng = np.random.default_rng() if rng is None else rng
+        rmse = self.trainingErrors() if selectionMode == 2 else None
         ec, (fs, fa, fc) = self.updateCandidates()
         be, bf = self.taskBatch[ENERGY], self.taskBatch[FORCE]
         ne = int(energyFraction * ec.size / be)   # updates per property
@@ -164,6 +196,19 @@ class Training:
             while r < schedule.size and schedule[r] == p:
                 r += 1
             cnt = (r - k) * (be if p == ENERGY else bf)   # candidates of this run
+            if selectionMode == 2:
+                if p == ENERGY:
+                    order = eo[(pos[p] + np.arange(ec.size)) % ec.size]
+                    used, e = self.updateThreshold(ENERGY, r - k, ec[order], threshold=threshold, trials=trials,
+                                                   rmse=rmse[0])
+                else:
+                    order = fo[(pos[p] + np.arange(fs.size)) % fs.size]
+                    used, e = self.updateThreshold(FORCE, r - k, fs[order], fa[order], fc[order],
+                                                   threshold=threshold, trials=trials, rmse=rmse[1])
+                errs[p].append(e)
+                pos[p] += used
+                k = r
+                continue
             if p == ENERGY:
                 idx = eo[(pos[p] + np.arange(cnt)) % ec.size]
                 errs[p].append(self.update(ENERGY, ec[idx]))

@@ -130,8 +130,8 @@ def test_epochs_reduce_errors(data):
         tr.setForceWeight(10.0)
         before = tr.errors()
         rng = np.random.default_rng(1)
-        for _ in range(3):
-            tr.runEpoch(energyFraction=1.0, forceFraction=0.05, rng=rng)
+        for ep in range(3):
+            tr.runEpoch(energyFraction=1.0, forceFraction=0.05, rng=rng, selectionMode=2 if ep == 2 else 0)
         after = tr.errors()
         assert after["energy_rmse_per_atom"] < 0.5 * before["energy_rmse_per_atom"]
         assert after["force_rmse"] < before["force_rmse"]
@@ -203,6 +203,45 @@ def test_element_strategy_matches_oracle(data, kind):
                 errs_ref = [ref.update_element(1, *x) for x in cands]
             assert np.allclose(errs, errs_ref, rtol=1e-9, atol=1e-12)
             assert H.max_rel(tr.weights(), ref.nets.weights) <= 1e-9
+    finally:
+        tr.close()
+        m.close()
+
+
+def test_threshold_selection_matches_oracle(data):
+    """selection_mode 2: trials until an error exceeds threshold x RMSE; the
+    update uses the candidate the trials stopped at."""
+    m, tr, ref = _pair(data, ("kf", UPDATERS[0][1]))
+    try:
+        ss = data[0]
+        rmse_e, rmse_f = tr.trainingErrors()
+        # the oracle's training RMSE at the same weights
+        de = [ref.observation(0, k)[0] / ss[k].numAtoms for k in range(len(ss))]
+        assert abs(rmse_e - np.sqrt(np.mean(np.square(de)))) <= 1e-9 * rmse_e
+
+        def oracle_threshold(prop, cands, n_updates, thr, trials, rmse):
+            pos, errs = 0, []
+            for _ in range(n_updates):
+                for _il in range(trials):
+                    k = cands[pos % len(cands)]
+                    e = ref.observation(prop, *k)[0]
+                    scale = ss[k[0]].numAtoms * rmse if prop == 0 else rmse
+                    pos += 1
+                    if abs(e) / scale > thr:
+                        break
+                errs.append(ref.update(prop, *k))
+            return pos, errs
+
+        ecands = [(s, 0, 0) for s in (2, 0, 3, 1, 2, 3)]
+        used, errs = tr.updateThreshold(ENERGY, 3, [c[0] for c in ecands], threshold=1.0, trials=2, rmse=rmse_e)
+        used_ref, errs_ref = oracle_threshold(0, ecands, 3, 1.0, 2, rmse_e)
+        assert used == used_ref and np.allclose(errs, errs_ref, rtol=1e-9, atol=1e-12)
+        fcands = [(2, 7, 1), (0, 5, 2), (3, 11, 0), (1, 4, 2), (0, 0, 0), (2, 3, 1)]
+        s, a, c = (np.array(x) for x in zip(*fcands))
+        used, errs = tr.updateThreshold(FORCE, 3, s, a, c, threshold=1.0, trials=3, rmse=rmse_f)
+        used_ref, errs_ref = oracle_threshold(1, fcands, 3, 1.0, 3, rmse_f)
+        assert used == used_ref and np.allclose(errs, errs_ref, rtol=1e-9, atol=1e-12)
+        assert H.max_rel(tr.weights(), ref.nets.weights) <= 1e-9
     finally:
         tr.close()
         m.close()
