@@ -589,8 +589,9 @@ def bench_training(steps, warmup, device, cpu=True):
     by the model's own weights, training from weights perturbed by N(0, 0.02).
     Energy and force updates are timed separately (CUDA events on the set's
     stream), 256 updates per timed step.  Each filter update reads and writes
-    the covariance once (the previous update's rank-one change fused with
-    this update's X = P H): 16 n^2 bytes, the HBM roofline of an update.  Beside it the numpy restatement of the
+    the covariance's lower half once (the previous update's rank-one change
+    fused with this update's X = P H): 8 n^2 bytes, the HBM roofline of the
+    filter's share of an update.  Beside it the numpy restatement of the
     same updates on a bounded sample (the reference's training program needs
     MPI and GSL, which this image lacks)."""
     import time
@@ -640,7 +641,7 @@ def bench_training(steps, warmup, device, cpu=True):
         e1.synchronize()
         ms = e0.elapsed_time(e1) / (steps * per)
         out[name] = {"value": 1e3 / ms, "ms_per_update": ms,
-                     "kalman_hbm_GBps_lower_bound": 16.0 * n * n / (ms * 1e-3) / 1e9}
+                     "kalman_hbm_GBps_lower_bound": 8.0 * n * n / (ms * 1e-3) / 1e9}
     out["errors_after"] = tr.errors()
     out["kalman_status"] = tr.kalmanStatus()
     tr.close()

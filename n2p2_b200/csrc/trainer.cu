@@ -593,41 +593,79 @@ __global__ void __launch_bounds__(256) kReduceSlices(const double* __restrict__ 
     }
 }
 
-// The previous update's pending P = (P - K X^T) * scale + q I (when
-// `pending`), fused with this update's X = P H: one pass that reads and writes
-// P once.  One block per row, fixed-order block reduction; every element is
-// updated with the formula of its lower twin (row max(i, j), column
-// min(i, j)), so P stays exactly symmetric and rows are read coalesced.
-__global__ void __launch_bounds__(128) kKalmanPX(double* __restrict__ Pm, const double* __restrict__ Kp,
-                                                 const double* __restrict__ Xp, int n, int pending, double scale,
-                                                 double q, const double* __restrict__ H, double* __restrict__ X)
+constexpr int kTile = 64;   // lower-triangle tiles of the covariance
+
+// Lower-triangle pass over P (the reference reads only that half,
+// P.selfadjointView<Lower>()): one CTA per 64 x 64 tile (I >= J) applies the
+// previous update's pending change (P_ic - K_i X_c) * scale (+ q on the
+// diagonal) to its elements i >= c, and writes two fixed-order partial sums
+// for this update's X = P H: rowPart[tile][r] = sum_c P_ic H_c over its
+// columns, colPart[tile][c] = sum_(i > c) P_ic H_i over its rows (the upper
+// half's contribution, by symmetry).  kKalmanXSum adds them up per row.
+__global__ void __launch_bounds__(256) kKalmanTiles(double* __restrict__ Pm, const double* __restrict__ Kp,
+                                                    const double* __restrict__ Xp, int n, int pending, double scale,
+                                                    double q, const double* __restrict__ H,
+                                                    double* __restrict__ rowPart, double* __restrict__ colPart)
 {
-    __shared__ double part[128];
-    const int i = blockIdx.x;
-    double* row = Pm + (size_t)i * n;
-    double acc = 0.0;
-    if (pending)
+    __shared__ double rowS[kTile][kTile + 1];
+    __shared__ double colS[4][kTile];
+    const int t = blockIdx.x;
+    // tile index t = I (I + 1) / 2 + J, J <= I
+    int I = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    while (I * (I + 1) / 2 > t) --I;
+    const int J = t - I * (I + 1) / 2;
+    const int tx = threadIdx.x & (kTile - 1), ty = threadIdx.x >> 6;
+    const int c = J * kTile + tx;
+    const bool cIn = c < n;
+    const double Hc = cIn ? H[c] : 0.0;
+    const double Xc = cIn && pending ? Xp[c] : 0.0;
+    double colAcc = 0.0;
+    for (int r = ty; r < kTile; r += 4)
     {
-        const double Ki = Kp[i], Xi = Xp[i];
-        for (int j = threadIdx.x; j < n; j += blockDim.x)
+        const int i = I * kTile + r;
+        double contrib = 0.0;
+        if (cIn && i < n && c <= i)
         {
-            double v = row[j] - (j <= i ? Ki * Xp[j] : Kp[j] * Xi);
-            if (scale != 1.0) v *= scale;
-            if (j == i) v += q;
-            row[j] = v;
-            acc += v * H[j];
+            double* pe = Pm + (size_t)i * n + c;
+            double v = *pe;
+            if (pending)
+            {
+                v = v - Kp[i] * Xc;
+                if (scale != 1.0) v *= scale;
+                if (c == i) v += q;
+                *pe = v;
+            }
+            contrib = v * Hc;
+            if (c < i) colAcc += v * H[i];
         }
+        rowS[r][tx] = contrib;
     }
-    else
-        for (int j = threadIdx.x; j < n; j += blockDim.x) acc += row[j] * H[j];
-    part[threadIdx.x] = acc;
+    colS[ty][tx] = colAcc;
     __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1)
+    if (threadIdx.x < kTile)
     {
-        if (threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
-        __syncthreads();
+        const int r = threadIdx.x;
+        double a = 0.0;
+        for (int k = 0; k < kTile; ++k) a += rowS[r][k];
+        rowPart[(size_t)t * kTile + r] = a;
+        colPart[(size_t)t * kTile + r] = ((colS[0][r] + colS[1][r]) + colS[2][r]) + colS[3][r];
     }
-    if (threadIdx.x == 0) X[i] = part[0];
+}
+
+// X_i = sum over the tiles of row block I of rowPart + sum over the tiles of
+// column block I (rows I..T-1) of colPart, in that fixed order.
+__global__ void kKalmanXSum(const double* __restrict__ rowPart, const double* __restrict__ colPart, int n, int T,
+                            double* __restrict__ X)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int I = i / kTile, r = i % kTile;
+        double a = 0.0;
+        for (int J = 0; J <= I; ++J) a += rowPart[((size_t)I * (I + 1) / 2 + J) * kTile + r];
+        for (int I2 = I; I2 < T; ++I2) a += colPart[((size_t)I2 * (I2 + 1) / 2 + I) * kTile + r];
+        X[i] = a;
+    }
 }
 
 // The updater's error: xi as it is (div == 0), or the per-element share
@@ -678,13 +716,14 @@ __global__ void __launch_bounds__(256) kKalmanP(double* __restrict__ Pm, const d
     const int i = blockIdx.y;
     const double Ki = K[i], Xi = X[i];
     double* row = Pm + (size_t)i * n;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= i && j < n; j += gridDim.x * blockDim.x)
     {
-        double v = row[j] - (j <= i ? Ki * X[j] : K[j] * Xi);
+        double v = row[j] - Ki * X[j];
         if (scale != 1.0) v *= scale;
         if (j == i) v += q;
         row[j] = v;
     }
+    (void)Xi;
 }
 
 __global__ void kKalmanInit(double* __restrict__ Pm, int n, double d)
@@ -737,9 +776,11 @@ __global__ void __launch_bounds__(256) kKalmanStat(const double* __restrict__ Pm
     const size_t total = (size_t)n * n;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x)
     {
+        const size_t i = e / n, j = e % n;
+        if (j > i) continue;   // the lower half is the stored one; the upper mirrors it
         const double v = fabs(Pm[e]);
-        a += v;
-        if (e / n == e % n) d += v;
+        a += i == j ? v : 2.0 * v;
+        if (i == j) d += v;
     }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) k += fabs(K[i]);
     part[0][threadIdx.x] = d;
@@ -861,6 +902,11 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
         Kb_[k] = tAlloc<double>(P_);
     }
     stat_ = tAlloc<double>(3 * kStatBlocks);
+    {
+        const int T = (P_ + kTile - 1) / kTile;
+        rowPart_ = tAlloc<double>((size_t)T * (T + 1) / 2 * kTile);
+        colPart_ = tAlloc<double>((size_t)T * (T + 1) / 2 * kTile);
+    }
     img_ = tAlloc<double>(b.gStride);
     cudaCheck(cudaMemsetAsync(u_, 0, sizeof(double) * 3 * (size_t)N_, st), "memset");
     for (int k = 0; k < 2; ++k) cudaCheck(cudaMemsetAsync(Kb_[k], 0, sizeof(double) * P_, st), "memset");
@@ -872,7 +918,7 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
 Training::~Training()
 {
     for (void* p : {(void*)eRef_, (void*)fRef_, (void*)u_, (void*)g_, (void*)gradPart_, (void*)predPart_, (void*)H_,
-                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)Xb_[0], (void*)Xb_[1], (void*)Kb_[0], (void*)Kb_[1], (void*)m_, (void*)v_, (void*)stat_, (void*)img_})
+                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)Xb_[0], (void*)Xb_[1], (void*)Kb_[0], (void*)Kb_[1], (void*)m_, (void*)v_, (void*)stat_, (void*)img_, (void*)rowPart_, (void*)colPart_})
         cudaFree(p);
 }
 
@@ -1037,9 +1083,12 @@ void Training::step(int property, int s, int a)
             Block const& B = blocks_[e];
             double mul, div;
             share(e, mul, div);
-            kKalmanPX<<<B.count, 128, 0, st>>>(Pm_ + B.pOffset, Kb_[cur_] + B.begin, Xb_[cur_] + B.begin, B.count,
-                                               pending_ ? 1 : 0, pendingScale_, pendingQ_, H_ + B.begin,
-                                               Xb_[cur] + B.begin);
+            const int T = (B.count + kTile - 1) / kTile;
+            const int tiles = T * (T + 1) / 2;
+            kKalmanTiles<<<tiles, 256, 0, st>>>(Pm_ + B.pOffset, Kb_[cur_] + B.begin, Xb_[cur_] + B.begin, B.count,
+                                                pending_ ? 1 : 0, pendingScale_, pendingQ_, H_ + B.begin, rowPart_,
+                                                colPart_);
+            kKalmanXSum<<<(B.count + 255) / 256, 256, 0, st>>>(rowPart_, colPart_, B.count, T, Xb_[cur] + B.begin);
             kKalmanGain<<<1, 1024, 0, st>>>(H_ + B.begin, Xb_[cur] + B.begin, B.count, diag, xiPtr, mul, div, post,
                                             Kb_[cur] + B.begin, w + B.begin, wT, tidx + B.begin);
         }

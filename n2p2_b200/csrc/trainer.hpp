@@ -78,9 +78,8 @@ private:
 // The symmetry functions and their derivatives do not depend on the weights:
 // they are computed once for the whole training set and stay resident; an
 // update runs the networks and the Jacobian over one structure's atoms only.
-// The filter's covariance P (weights x weights, FP64) is kept symmetric by
-// construction: every element is updated with the formula of its lower-
-// triangle twin, the only half the reference reads
+// The filter's covariance P (weights x weights, FP64) is stored and updated
+// in its lower half only, the half the reference reads
 // (P.selfadjointView<Lower>()).
 class Training
 {
@@ -197,6 +196,8 @@ private:
     double* v_ = nullptr;
     double* stat_ = nullptr;     // status partial sums
     double* img_ = nullptr;      // [gStride] self-image part of the observed atom's adjoint
+    double* rowPart_ = nullptr;  // [tiles][64] row partial sums of X = P H
+    double* colPart_ = nullptr;  // [tiles][64] column partial sums (the upper half's share)
 };
 
 } // namespace n2p2b200
