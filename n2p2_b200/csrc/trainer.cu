@@ -653,18 +653,23 @@ __global__ void __launch_bounds__(256) kKalmanTiles(double* __restrict__ Pm, con
     }
 }
 
-// X_i = sum over the tiles of row block I of rowPart + sum over the tiles of
-// column block I (rows I..T-1) of colPart, in that fixed order.
-__global__ void kKalmanXSum(const double* __restrict__ rowPart, const double* __restrict__ colPart, int n, int T,
-                            double* __restrict__ X)
+// X_i = the row partials of the tiles of row block I plus the column
+// partials of the tiles of column block I (rows I..T-1): one warp per row,
+// lanes over the partials, fixed shuffle-tree order.
+__global__ void __launch_bounds__(256) kKalmanXSum(const double* __restrict__ rowPart,
+                                                   const double* __restrict__ colPart, int n, int T,
+                                                   double* __restrict__ X)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31;
+    const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warpsPerGrid)
     {
         const int I = i / kTile, r = i % kTile;
         double a = 0.0;
-        for (int J = 0; J <= I; ++J) a += rowPart[((size_t)I * (I + 1) / 2 + J) * kTile + r];
-        for (int I2 = I; I2 < T; ++I2) a += colPart[((size_t)I2 * (I2 + 1) / 2 + I) * kTile + r];
-        X[i] = a;
+        for (int J = lane; J <= I; J += 32) a += rowPart[((size_t)I * (I + 1) / 2 + J) * kTile + r];
+        for (int I2 = I + lane; I2 < T; I2 += 32) a += colPart[((size_t)I2 * (I2 + 1) / 2 + I) * kTile + r];
+        a = warpSum(a);
+        if (lane == 0) X[i] = a;
     }
 }
 
@@ -1088,7 +1093,7 @@ void Training::step(int property, int s, int a)
             kKalmanTiles<<<tiles, 256, 0, st>>>(Pm_ + B.pOffset, Kb_[cur_] + B.begin, Xb_[cur_] + B.begin, B.count,
                                                 pending_ ? 1 : 0, pendingScale_, pendingQ_, H_ + B.begin, rowPart_,
                                                 colPart_);
-            kKalmanXSum<<<(B.count + 255) / 256, 256, 0, st>>>(rowPart_, colPart_, B.count, T, Xb_[cur] + B.begin);
+            kKalmanXSum<<<(B.count + 7) / 8, 256, 0, st>>>(rowPart_, colPart_, B.count, T, Xb_[cur] + B.begin);
             kKalmanGain<<<1, 1024, 0, st>>>(H_ + B.begin, Xb_[cur] + B.begin, B.count, diag, xiPtr, mul, div, post,
                                             Kb_[cur] + B.begin, w + B.begin, wT, tidx + B.begin);
         }
