@@ -139,9 +139,11 @@ __global__ void __launch_bounds__(256) kLossSum(const double* __restrict__ lossE
 // img[0..numSF): Mode::calculateForces skips those entries
 // (neighborsUnique.begin() + 1, Mode.cpp:1957) while Training::collectDGdxia
 // (Training.cpp:3604-3615) keeps them.
+// With `list`, atoms list[0..a1) instead of [a0, a1).
 __global__ void __launch_bounds__(kTrainWarps * 32) kSFAdjoint(DevModel model, BatchView b, int a0, int a1,
                                                                const double* __restrict__ u, double* __restrict__ g,
-                                                               int imgAtom = -1, double* __restrict__ img = nullptr)
+                                                               int imgAtom = -1, double* __restrict__ img = nullptr,
+                                                               const int* __restrict__ list = nullptr)
 {
     __shared__ double acc[kTrainWarps][kTrainMaxInput];
     __shared__ double accImg[kTrainWarps][kTrainMaxInput];
@@ -149,8 +151,9 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kSFAdjoint(DevModel model, B
     double* a = acc[threadIdx.x >> 5];
     double* ai = accImg[threadIdx.x >> 5];
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
-    for (int i = a0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < a1; i += warpsPerGrid)
+    for (int k = a0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < a1; k += warpsPerGrid)
     {
+        const int i = list ? list[k] : k;
         const int ec = b.elem[i];
         DevElement const& E = model.el[ec];
         const double ux = u[3 * (size_t)i + 0], uy = u[3 * (size_t)i + 1], uz = u[3 * (size_t)i + 2];
@@ -211,7 +214,8 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, B
                                                                double* __restrict__ gradPart,
                                                                double* __restrict__ predPart,
                                                                int imgAtom = -1,
-                                                               const double* __restrict__ img = nullptr)
+                                                               const double* __restrict__ img = nullptr,
+                                                               const int* __restrict__ list = nullptr)
 {
     __shared__ ParamSmem smem[kTrainWarps];
     ParamSmem& S = smem[threadIdx.x >> 5];
@@ -222,8 +226,9 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, B
     for (int p = lane; p < P; p += 32) slice[p] = 0.0;
     double pred = 0.0;
     __syncwarp();
-    for (int i = a0 + warp; i < a1; i += warpsPerGrid)
+    for (int k = a0 + warp; k < a1; k += warpsPerGrid)
     {
+        const int i = list ? list[k] : k;
         const int ec = b.elem[i];
         DevElement const& E = model.el[ec];
         const int L = E.numLayers;
@@ -889,6 +894,24 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
             nbrCount_[i] = (int)(off[i + 1] - off[i]);
             for (int64_t q = off[i]; q < off[i + 1]; ++q) ++nbrPerElement_[(size_t)i * ne + elem[nj[q]]];
         }
+        // per atom: itself and its distinct neighbours, ascending (the neighbour relation is
+        // symmetric, so these are the atoms whose functions depend on its position)
+        std::vector<int> nearList;
+        nearOffset_.assign((size_t)N_ + 1, 0);
+        std::vector<int> tmp;
+        for (int i = 0; i < N_; ++i)
+        {
+            tmp.assign(nj.begin() + off[i], nj.begin() + off[i + 1]);
+            tmp.push_back(i);
+            std::sort(tmp.begin(), tmp.end());
+            tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+            nearList.insert(nearList.end(), tmp.begin(), tmp.end());
+            nearOffset_[i + 1] = (int64_t)nearList.size();
+        }
+        near_ = tAlloc<int>(nearList.size());
+        cudaCheck(cudaMemcpyAsync(near_, nearList.data(), sizeof(int) * nearList.size(), cudaMemcpyHostToDevice, st),
+                  "H2D");
+        cudaCheck(cudaStreamSynchronize(st), "sync");
     }
     blocks_.push_back({0, P_, 0});
     maxWarps_ = std::min(maxAtoms, sms_ * 8);
@@ -923,7 +946,7 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
 Training::~Training()
 {
     for (void* p : {(void*)eRef_, (void*)fRef_, (void*)u_, (void*)g_, (void*)gradPart_, (void*)predPart_, (void*)H_,
-                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)Xb_[0], (void*)Xb_[1], (void*)Kb_[0], (void*)Kb_[1], (void*)m_, (void*)v_, (void*)stat_, (void*)img_, (void*)rowPart_, (void*)colPart_})
+                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)Xb_[0], (void*)Xb_[1], (void*)Kb_[0], (void*)Kb_[1], (void*)m_, (void*)v_, (void*)stat_, (void*)img_, (void*)rowPart_, (void*)colPart_, (void*)near_})
         cudaFree(p);
 }
 
@@ -1021,14 +1044,18 @@ void Training::observation(int property, int s, int a, int c, int t, bool accumu
     }
     else
     {
+        // only the atom and its neighbours carry a nonzero adjoint: the passes run over that list
         const int64_t k = 3 * (int64_t)(a0 + a) + c;
+        const int l0 = (int)nearOffset_[a0 + a], l1 = (int)nearOffset_[a0 + a + 1];
+        const int fw = std::min(maxWarps_, (l1 - l0 + kTrainWarps - 1) / kTrainWarps * kTrainWarps);
+        const int fb = fw / kTrainWarps;
         kSetEntry<<<1, 1, 0, st>>>(u_, k, 1.0);
-        kSFAdjoint<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, u_, g_, a0 + a, img_);
+        kSFAdjoint<<<fb, kTrainWarps * 32, 0, st>>>(m, b, l0, l1, u_, g_, a0 + a, img_, near_);
         kSetEntry<<<1, 1, 0, st>>>(u_, k, 0.0);
-        kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 0.0, g_, P_, gradPart_, predPart_,
-                                                        a0 + a, img_);
-        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, last ? forceWeight_ : 1.0, acc);
-        kObsError<<<1, 32, 0, st>>>(predPart_, warps, fRef_, k, forceWeight_, xi_, err_ + t, acc);
+        kParamGrad<<<fb, kTrainWarps * 32, 0, st>>>(m, b, l0, l1, nullptr, 0.0, g_, P_, gradPart_, predPart_, a0 + a,
+                                                    img_, near_);
+        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, fw, P_, H_, last ? forceWeight_ : 1.0, acc);
+        kObsError<<<1, 32, 0, st>>>(predPart_, fw, fRef_, k, forceWeight_, xi_, err_ + t, acc);
     }
     cudaCheck(cudaGetLastError(), "observation launch");
 }

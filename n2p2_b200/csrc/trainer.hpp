@@ -157,6 +157,8 @@ private:
     std::vector<int> atomsPerElement_;   // [S][elements]
     std::vector<int> nbrPerElement_;     // [N][elements]
     std::vector<int> nbrCount_;          // [N]
+    std::vector<int64_t> nearOffset_;    // [N+1] into near_
+    int* near_ = nullptr;                // per atom: itself and its distinct neighbours, ascending
 
     Model& model_;
     DeviceModel& dmodel_;
