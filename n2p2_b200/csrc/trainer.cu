@@ -207,7 +207,9 @@ struct ParamSmem
 // [a0, a1), summed into the warp's slice gradPart[warp][P] (parameter layout
 // of the device weights).  a_i = aStruct[structure of i], or aConst without
 // aStruct; no g means g = 0.  With predPart, the warp's sum of L_i goes to
-// predPart[warp] (the value whose gradient this is).
+// predPart[warp] (the value whose gradient this is).  TANGENT false: g must be
+// null (no tangent is carried; the zero-tangent terms are skipped).
+template <bool TANGENT>
 __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, BatchView b, int a0, int a1,
                                                                const double* __restrict__ aStruct, double aConst,
                                                                const double* __restrict__ g, int P,
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, B
                 for (int j = 0; j < nin; ++j)
                 {
                     z += row[j] * S.in(l, j);
-                    zd += row[j] * S.ind(l, j);
+                    if (TANGENT) zd += row[j] * S.ind(l, j);
                 }
                 double f, f1, f2;
                 activate2(E.activation[l], z, f, f1, f2);
@@ -305,7 +307,10 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, B
                 S.zb[lane] = zb;
                 S.zdb[lane] = zdb;
                 double* gw = slice + E.wOffset[l] + (size_t)lane * nin;
-                for (int j = 0; j < nin; ++j) gw[j] += zb * S.in(l, j) + zdb * S.ind(l, j);
+                if (TANGENT)
+                    for (int j = 0; j < nin; ++j) gw[j] += zb * S.in(l, j) + zdb * S.ind(l, j);
+                else
+                    for (int j = 0; j < nin; ++j) gw[j] += zb * S.in(l, j);
                 slice[E.bOffset[l] + lane] += zb;
             }
             __syncwarp();
@@ -318,7 +323,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kParamGrad(DevModel model, B
                     {
                         const double w = W[(size_t)k * nin + lane];
                         xb += w * S.zb[k];
-                        xdb += w * S.zdb[k];
+                        if (TANGENT) xdb += w * S.zdb[k];
                     }
                     S.xb[lane] = xb;
                     S.xdb[lane] = xdb;
@@ -484,7 +489,7 @@ void Trainer::step(Batch& batch, const double* energiesPhys, const double* force
     kLossSum<<<1, 256, 0, st>>>(lossE_, S, lossF_, N, loss_);
     const int blocks = warps_ / kTrainWarps;
     kSFAdjoint<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, 0, N, u_, g_);
-    kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, 0, N, aStruct_, 0.0, g_, P_, gradPart_, nullptr);
+    kParamGrad<true><<<blocks, kTrainWarps * 32, 0, st>>>(m, b, 0, N, aStruct_, 0.0, g_, P_, gradPart_, nullptr);
     kReduceGrad<<<(P_ + tb - 1) / tb, tb, 0, st>>>(gradPart_, warps_, P_, grad_);
     cudaCheck(cudaGetLastError(), "trainer launch");
     if (update)
@@ -1038,7 +1043,8 @@ void Training::observation(int property, int s, int a, int c, int t, bool accumu
     const int blocks = warps / kTrainWarps;
     if (property == ENERGY)
     {
-        kParamGrad<<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 1.0, nullptr, P_, gradPart_, predPart_);
+        kParamGrad<false><<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 1.0, nullptr, P_, gradPart_,
+                                                               predPart_);
         kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, 1.0, acc);
         kObsError<<<1, 32, 0, st>>>(predPart_, warps, eRef_, s, 1.0, xi_, err_ + t, acc);
     }
@@ -1052,7 +1058,7 @@ void Training::observation(int property, int s, int a, int c, int t, bool accumu
         kSetEntry<<<1, 1, 0, st>>>(u_, k, 1.0);
         kSFAdjoint<<<fb, kTrainWarps * 32, 0, st>>>(m, b, l0, l1, u_, g_, a0 + a, img_, near_);
         kSetEntry<<<1, 1, 0, st>>>(u_, k, 0.0);
-        kParamGrad<<<fb, kTrainWarps * 32, 0, st>>>(m, b, l0, l1, nullptr, 0.0, g_, P_, gradPart_, predPart_, a0 + a,
+        kParamGrad<true><<<fb, kTrainWarps * 32, 0, st>>>(m, b, l0, l1, nullptr, 0.0, g_, P_, gradPart_, predPart_, a0 + a,
                                                     img_, near_);
         kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, fw, P_, H_, last ? forceWeight_ : 1.0, acc);
         kObsError<<<1, 32, 0, st>>>(predPart_, fw, fRef_, k, forceWeight_, xi_, err_ + t, acc);
