@@ -169,12 +169,25 @@ class Training:
         c = np.tile(np.arange(3, dtype=np.int32), int(self.atomsPerStructure.sum()))
         return e, (s, a, c)
 
+    def sortedCandidates(self):
+        """selection_mode 1 (Training::sortUpdateCandidates,
+        Training.cpp:2008-2061): candidate orders by descending error at the
+        current weights -- |E_ref - E| / N per structure, |F_ref - F| per force
+        component (unit factors do not change the order)."""
+        b = self.batch
+        b.evaluate(forces=True, storeDGdr=True, graph=False)
+        E, F = b.energies(), b.forces()
+        ee = np.abs((self.energiesRef - E) / self.atomsPerStructure)
+        ef = np.abs(self.forcesRef - F).ravel()   # (atom, component) in candidate order
+        return np.argsort(-ee, kind="stable"), np.argsort(-ef, kind="stable")
+
     def runEpoch(self, energyFraction=1.0, forceFraction=0.0, rng=None, selectionMode=0, threshold=1.0, trials=3):
         """One epoch of Training::loop: candidates shuffled per property, the
         energy and force updates (fraction x candidates each) in a shuffled
         schedule, each update taking the next candidate of its property
-        (selectionMode 0) or trying candidates against threshold x the
-        training RMSE at the epoch's start (selectionMode 2, up to `trials`).
+        (selectionMode 0 random order, 1 sorted by descending error) or trying
+        candidates against threshold x the training RMSE at the epoch's start
+        (selectionMode 2, up to `trials`).
         Returns the errors per property (internal units)."""
         rng = np.random.default_rng() if rng is None else rng
         rmse = self.trainingErrors() if selectionMode == 2 else None
@@ -182,8 +195,11 @@ class Training:
         be, bf = self.taskBatch[ENERGY], self.taskBatch[FORCE]
         ne = int(energyFraction * ec.size / be)   # updates per property
         nf = int(forceFraction * fs.size / bf)
-        eo = rng.permutation(ec.size)
-        fo = rng.permutation(fs.size)
+        if selectionMode == 1:
+            eo, fo = self.sortedCandidates()
+        else:
+            eo = rng.permutation(ec.size)
+            fo = rng.permutation(fs.size)
         schedule = np.concatenate([np.full(nf, FORCE), np.full(ne, ENERGY)])
         if ne and nf:
             rng.shuffle(schedule)

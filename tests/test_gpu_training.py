@@ -246,3 +246,22 @@ def test_threshold_selection_matches_oracle(data):
         tr.close()
         m.close()
 
+
+def test_sort_selection_order(data):
+    """selection_mode 1: candidates by descending error at the current weights."""
+    m, tr, ref = _pair(data, ("kf", UPDATERS[0][1]))
+    try:
+        ss = data[0]
+        eo, fo = tr.sortedCandidates()
+        ee = [abs(ref.observation(0, k)[0]) / ss[k].numAtoms for k in range(len(ss))]
+        assert list(eo) == list(np.argsort(-np.array(ee), kind="stable"))
+        _, (fs, fa, fc) = tr.updateCandidates()
+        top = [abs(ref.observation(1, fs[q], fa[q], fc[q])[0]) for q in fo[:5]]
+        rest = [abs(ref.observation(1, fs[q], fa[q], fc[q])[0]) for q in fo[-5:]]
+        assert all(x >= y for x, y in zip(top, top[1:])) and min(top) >= max(rest)
+        tr.runEpoch(energyFraction=1.0, forceFraction=0.02, selectionMode=1)
+        assert tr.kalmanStatus()["numUpdates"] > len(ss)
+    finally:
+        tr.close()
+        m.close()
+
