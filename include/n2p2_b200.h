@@ -383,6 +383,10 @@ n2p2_status n2p2_training_set_force_weight(n2p2_training* training, double weigh
 #define N2P2_TRAINING_COMBINED 0
 #define N2P2_TRAINING_ELEMENT 1
 n2p2_status n2p2_training_set_update_strategy(n2p2_training* training, int32_t strategy);
+/* jacobian_mode (0, 1: a task batch's candidates summed into one observation; 2: every candidate its own
+ * observation, one Kalman update with an m x m gain, KalmanFilter.cpp:130-162 with sizeObservation m;
+ * combined strategy, Kalman filter, at most 16 candidates per update). */
+n2p2_status n2p2_training_set_jacobian_mode(n2p2_training* training, int32_t mode);
 /* task_batch_size_energy / task_batch_size_force (Training.cpp:2277-2279 with jacobian_mode 0 or 1 on one
  * process): that many consecutive candidates form one observation (errors and Jacobians summed at the same
  * weights) and one updater step. */

@@ -98,6 +98,7 @@ SIGNATURES = {
     "n2p2_training_set_references": (_i, [_vp, _P(_d), _P(_d)]),
     "n2p2_training_set_force_weight": (_i, [_vp, _d]),
     "n2p2_training_set_update_strategy": (_i, [_vp, ctypes.c_int32]),
+    "n2p2_training_set_jacobian_mode": (_i, [_vp, ctypes.c_int32]),
     "n2p2_training_set_task_batch_size": (_i, [_vp, ctypes.c_int32, ctypes.c_int32]),
     "n2p2_training_set_kalman_standard": (_i, [_vp, _d, _d, _d, _d, _d, _d, _d]),
     "n2p2_training_set_kalman_fading_memory": (_i, [_vp, _d, _d, _d, _d, _d, _d]),

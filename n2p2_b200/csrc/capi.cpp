@@ -840,6 +840,15 @@ n2p2_status n2p2_training_set_update_strategy(n2p2_training* training, int32_t s
     return guard([&] { training->training->setUpdateStrategy(strategy); });
 }
 
+n2p2_status n2p2_training_set_jacobian_mode(n2p2_training* training, int32_t mode)
+{
+    N2P2_REQUIRE(training);
+    return guard([&] {
+        if (mode < 0 || mode > 2) throw std::invalid_argument("ERROR: unknown Jacobian mode.\n");
+        training->training->setFullJacobian(mode == 2);
+    });
+}
+
 n2p2_status n2p2_training_set_task_batch_size(n2p2_training* training, int32_t energy, int32_t force)
 {
     N2P2_REQUIRE(training);

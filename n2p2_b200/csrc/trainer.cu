@@ -615,7 +615,8 @@ constexpr int kTile = 64;   // lower-triangle tiles of the covariance
 __global__ void __launch_bounds__(256) kKalmanTiles(double* __restrict__ Pm, const double* __restrict__ Kp,
                                                     const double* __restrict__ Xp, int n, int pending, double scale,
                                                     double q, const double* __restrict__ H,
-                                                    double* __restrict__ rowPart, double* __restrict__ colPart)
+                                                    double* __restrict__ rowPart, double* __restrict__ colPart,
+                                                    int rank = 1, int ld = 0)
 {
     __shared__ double rowS[kTile][kTile + 1];
     __shared__ double colS[4][kTile];
@@ -642,6 +643,7 @@ __global__ void __launch_bounds__(256) kKalmanTiles(double* __restrict__ Pm, con
             if (pending)
             {
                 v = v - Kp[i] * Xc;
+                for (int o = 1; o < rank; ++o) v = v - Kp[i + (size_t)o * ld] * Xp[c + (size_t)o * ld];
                 if (scale != 1.0) v *= scale;
                 if (c == i) v += q;
                 *pe = v;
@@ -723,10 +725,81 @@ __global__ void __launch_bounds__(1024) kKalmanGain(const double* __restrict__ H
     }
 }
 
+constexpr int kMaxObs = 16;   // observations per update with the full Jacobian
+
+// Several observations (jacobian_mode 2): A = H^T X + diag I (m x m), its
+// inverse by Gauss-Jordan elimination with partial pivoting, K = X A^-1,
+// w += K xi (xi[2 o] the scaled error of observation o).  One block.
+__global__ void __launch_bounds__(1024) kKalmanGainFull(const double* __restrict__ H, const double* __restrict__ X,
+                                                        int n, int ld, int m, double diag,
+                                                        const double* __restrict__ xi, double* __restrict__ K,
+                                                        double* __restrict__ w, double* __restrict__ wT,
+                                                        const int* __restrict__ tidx)
+{
+    __shared__ double part[1024];
+    __shared__ double A[kMaxObs][2 * kMaxObs];
+    for (int a = 0; a < m; ++a)
+        for (int c = 0; c < m; ++c)
+        {
+            double s = 0.0;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) s += H[i + (size_t)a * ld] * X[i + (size_t)c * ld];
+            part[threadIdx.x] = s;
+            __syncthreads();
+            for (int st = blockDim.x / 2; st > 0; st >>= 1)
+            {
+                if (threadIdx.x < st) part[threadIdx.x] += part[threadIdx.x + st];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0)
+            {
+                A[a][c] = part[0] + (a == c ? diag : 0.0);
+                A[a][m + c] = a == c ? 1.0 : 0.0;
+            }
+            __syncthreads();
+        }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < m; ++c)
+        {
+            int piv = c;
+            for (int r = c + 1; r < m; ++r)
+                if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+            if (piv != c)
+                for (int k = 0; k < 2 * m; ++k)
+                {
+                    const double t = A[c][k];
+                    A[c][k] = A[piv][k];
+                    A[piv][k] = t;
+                }
+            const double d = 1.0 / A[c][c];
+            for (int k = 0; k < 2 * m; ++k) A[c][k] *= d;
+            for (int r = 0; r < m; ++r)
+                if (r != c)
+                {
+                    const double f = A[r][c];
+                    for (int k = 0; k < 2 * m; ++k) A[r][k] -= f * A[c][k];
+                }
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        double wi = w[i];
+        for (int c = 0; c < m; ++c)
+        {
+            double k = 0.0;
+            for (int a = 0; a < m; ++a) k += X[i + (size_t)a * ld] * A[a][m + c];
+            K[i + (size_t)c * ld] = k;
+            wi += k * xi[2 * c];
+        }
+        w[i] = wi;
+        wT[tidx[i]] = wi;
+    }
+}
+
 // P = (P - K X^T) * scale + q I, every element with the formula of its lower
 // twin (row max(i, j), column min(i, j)), so P stays exactly symmetric.
 __global__ void __launch_bounds__(256) kKalmanP(double* __restrict__ Pm, const double* __restrict__ K,
-                                                const double* __restrict__ X, int n, double scale, double q)
+                                                const double* __restrict__ X, int n, double scale, double q,
+                                                int rank = 1, int ld = 0)
 {
     const int i = blockIdx.y;
     const double Ki = K[i], Xi = X[i];
@@ -734,6 +807,7 @@ __global__ void __launch_bounds__(256) kKalmanP(double* __restrict__ Pm, const d
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j <= i && j < n; j += gridDim.x * blockDim.x)
     {
         double v = row[j] - Ki * X[j];
+        for (int o = 1; o < rank; ++o) v = v - K[i + (size_t)o * ld] * X[j + (size_t)o * ld];
         if (scale != 1.0) v *= scale;
         if (j == i) v += q;
         row[j] = v;
@@ -927,12 +1001,12 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
     g_ = tAlloc<double>((size_t)N_ * b.gStride);
     gradPart_ = tAlloc<double>((size_t)maxWarps_ * P_);
     predPart_ = tAlloc<double>(maxWarps_);
-    H_ = tAlloc<double>(P_);
-    xi_ = tAlloc<double>(2);
+    H_ = tAlloc<double>((size_t)P_ * kMaxObs);
+    xi_ = tAlloc<double>(2 * kMaxObs);
     for (int k = 0; k < 2; ++k)
     {
-        Xb_[k] = tAlloc<double>(P_);
-        Kb_[k] = tAlloc<double>(P_);
+        Xb_[k] = tAlloc<double>((size_t)P_ * kMaxObs);
+        Kb_[k] = tAlloc<double>((size_t)P_ * kMaxObs);
     }
     stat_ = tAlloc<double>(3 * kStatBlocks);
     {
@@ -942,7 +1016,7 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
     }
     img_ = tAlloc<double>(b.gStride);
     cudaCheck(cudaMemsetAsync(u_, 0, sizeof(double) * 3 * (size_t)N_, st), "memset");
-    for (int k = 0; k < 2; ++k) cudaCheck(cudaMemsetAsync(Kb_[k], 0, sizeof(double) * P_, st), "memset");
+    for (int k = 0; k < 2; ++k) cudaCheck(cudaMemsetAsync(Kb_[k], 0, sizeof(double) * P_ * kMaxObs, st), "memset");
     cudaCheck(cudaMemsetAsync(eRef_, 0, sizeof(double) * S_, st), "memset");
     cudaCheck(cudaMemsetAsync(fRef_, 0, sizeof(double) * 3 * (size_t)N_, st), "memset");
     cudaCheck(cudaStreamSynchronize(st), "sync");
@@ -1032,9 +1106,11 @@ void Training::setGradientAdam(double eta, double beta1, double beta2, double ep
 // (sum of dE_i/dc over its atoms) or force component c of its atom a (the
 // second-order gradient with the force adjoint e_{a,c}); force errors and
 // Jacobians carry the force weight.
-void Training::observation(int property, int s, int a, int c, int t, bool accumulate, bool last)
+void Training::observation(int property, int s, int a, int c, int t, bool accumulate, bool last, int column)
 {
     const int acc = accumulate ? 1 : 0;
+    double* H = H_ + (size_t)column * P_;   // the full Jacobian keeps one column per observation
+    double* xi = xi_ + 2 * column;
     cudaStream_t st = set_.stream();
     BatchView const& b = set_.view();
     DevModel const& m = dmodel_.view;
@@ -1045,8 +1121,8 @@ void Training::observation(int property, int s, int a, int c, int t, bool accumu
     {
         kParamGrad<false><<<blocks, kTrainWarps * 32, 0, st>>>(m, b, a0, a1, nullptr, 1.0, nullptr, P_, gradPart_,
                                                                predPart_);
-        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H_, 1.0, acc);
-        kObsError<<<1, 32, 0, st>>>(predPart_, warps, eRef_, s, 1.0, xi_, err_ + t, acc);
+        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, warps, P_, H, 1.0, acc);
+        kObsError<<<1, 32, 0, st>>>(predPart_, warps, eRef_, s, 1.0, xi, err_ + t, acc);
     }
     else
     {
@@ -1060,8 +1136,8 @@ void Training::observation(int property, int s, int a, int c, int t, bool accumu
         kSetEntry<<<1, 1, 0, st>>>(u_, k, 0.0);
         kParamGrad<true><<<fb, kTrainWarps * 32, 0, st>>>(m, b, l0, l1, nullptr, 0.0, g_, P_, gradPart_, predPart_, a0 + a,
                                                     img_, near_);
-        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, fw, P_, H_, last ? forceWeight_ : 1.0, acc);
-        kObsError<<<1, 32, 0, st>>>(predPart_, fw, fRef_, k, forceWeight_, xi_, err_ + t, acc);
+        kReduceSlices<<<(P_ + 31) / 32, 256, 0, st>>>(gradPart_, fw, P_, H, last ? forceWeight_ : 1.0, acc);
+        kObsError<<<1, 32, 0, st>>>(predPart_, fw, fRef_, k, forceWeight_, xi, err_ + t, acc);
     }
     cudaCheck(cudaGetLastError(), "observation launch");
 }
@@ -1069,7 +1145,7 @@ void Training::observation(int property, int s, int a, int c, int t, bool accumu
 // The updaters' step with the observation in H_ / xi_: one updater over all
 // weights (combined strategy) or one per element over its block of weights
 // (element strategy), each with its share of the error.
-void Training::step(int property, int s, int a)
+void Training::step(int property, int s, int a, int m)
 {
     cudaStream_t st = set_.stream();
     double* w = dmodel_.weightsDevice();
@@ -1116,6 +1192,21 @@ void Training::step(int property, int s, int a)
         }
         // this update's X with the previous update's P update applied on the way
         const int cur = cur_ ^ 1;
+        if (m > 1)
+        {
+            // jacobian_mode 2 (combined strategy): X column by column, the pending change applied
+            // by the first pass, then the m x m gain
+            const int n = P_, T = (n + kTile - 1) / kTile;
+            for (int o = 0; o < m; ++o)
+            {
+                kKalmanTiles<<<T * (T + 1) / 2, 256, 0, st>>>(Pm_, Kb_[cur_], Xb_[cur_], n, (o == 0 && pending_) ? 1 : 0,
+                                                               pendingScale_, pendingQ_, H_ + (size_t)o * n, rowPart_,
+                                                               colPart_, pendingRank_, n);
+                kKalmanXSum<<<(n + 7) / 8, 256, 0, st>>>(rowPart_, colPart_, n, T, Xb_[cur] + (size_t)o * n);
+            }
+            kKalmanGainFull<<<1, 1024, 0, st>>>(H_, Xb_[cur], n, n, m, diag, xi_, Kb_[cur], w, wT, tidx);
+        }
+        else
         for (int e = 0; e < ne; ++e)
         {
             Block const& B = blocks_[e];
@@ -1125,13 +1216,14 @@ void Training::step(int property, int s, int a)
             const int tiles = T * (T + 1) / 2;
             kKalmanTiles<<<tiles, 256, 0, st>>>(Pm_ + B.pOffset, Kb_[cur_] + B.begin, Xb_[cur_] + B.begin, B.count,
                                                 pending_ ? 1 : 0, pendingScale_, pendingQ_, H_ + B.begin, rowPart_,
-                                                colPart_);
+                                                colPart_, pendingRank_, P_);
             kKalmanXSum<<<(B.count + 7) / 8, 256, 0, st>>>(rowPart_, colPart_, B.count, T, Xb_[cur] + B.begin);
             kKalmanGain<<<1, 1024, 0, st>>>(H_ + B.begin, Xb_[cur] + B.begin, B.count, diag, xiPtr, mul, div, post,
                                             Kb_[cur] + B.begin, w + B.begin, wT, tidx + B.begin);
         }
         cur_ = cur;
         pending_ = true;   // P - K X^T, * scale, + q I: applied by the next pass over P
+        pendingRank_ = m;
         pendingScale_ = scale;
         pendingQ_ = q_;
         if (q_ > qmin_) q_ *= std::exp(-qtau_);
@@ -1141,6 +1233,8 @@ void Training::step(int property, int s, int a)
             gamma_ = 1.0 / (1.0 + lambda_ / gamma_);
         }
     }
+    else if (m > 1)
+        throw std::invalid_argument("ERROR: the full Jacobian needs the Kalman filter.\n");
     else if (type_ == GD_FIXED)
     {
         for (int e = 0; e < ne; ++e)
@@ -1196,7 +1290,8 @@ void Training::initKalman(double epsilon)
         kKalmanInit<<<sms_ * 8, 256, 0, set_.stream()>>>(Pm_ + B.pOffset, B.count, 1.0 / epsilon);
     cudaCheck(cudaGetLastError(), "kalman init");
     pending_ = false;
-    cudaCheck(cudaMemsetAsync(Kb_[cur_], 0, sizeof(double) * P_, set_.stream()), "memset");
+    pendingRank_ = 1;
+    cudaCheck(cudaMemsetAsync(Kb_[cur_], 0, sizeof(double) * P_ * kMaxObs, set_.stream()), "memset");
 }
 
 void Training::update(int property, int count, const int* structure, const int* atom, const int* component,
@@ -1227,14 +1322,22 @@ void Training::update(int property, int count, const int* structure, const int* 
     const int batch = property == ENERGY ? taskBatchEnergy_ : taskBatchForce_;
     if (strategy_ == US_ELEMENT && batch != 1)
         throw std::invalid_argument("ERROR: the element update strategy needs task batches of one candidate.\n");
+    if (fullJacobian_ && batch > kMaxObs)
+        throw std::invalid_argument("ERROR: the full Jacobian takes at most 16 candidates per update.\n");
+    if (fullJacobian_ && batch > 1 && type_ != KF_STANDARD && type_ != KF_FADING_MEMORY)
+        throw std::invalid_argument("ERROR: the full Jacobian needs the Kalman filter.\n");
     if (count % batch != 0)
         throw std::invalid_argument("ERROR: the number of candidates is not a multiple of the task batch size.\n");
     for (int t = 0; t < count; ++t)
     {
         const int q = t % batch;
-        observation(property, structure[t], property == FORCE ? atom[t] : 0, property == FORCE ? component[t] : 0, t,
-                    q > 0, q == batch - 1);
-        if (q == batch - 1) step(property, structure[t], property == FORCE ? atom[t] : 0);
+        if (fullJacobian_)   // one observation per candidate
+            observation(property, structure[t], property == FORCE ? atom[t] : 0, property == FORCE ? component[t] : 0,
+                        t, false, true, q);
+        else
+            observation(property, structure[t], property == FORCE ? atom[t] : 0, property == FORCE ? component[t] : 0,
+                        t, q > 0, q == batch - 1);
+        if (q == batch - 1) step(property, structure[t], property == FORCE ? atom[t] : 0, fullJacobian_ ? batch : 1);
     }
     if (errors)
         cudaCheck(cudaMemcpyAsync(errors, err_, sizeof(double) * count, cudaMemcpyDeviceToHost, st), "D2H");
@@ -1266,7 +1369,7 @@ int Training::updateThreshold(int property, int numUpdates, int numCandidates, c
     int pos = 0;
     auto obs = [&](int k) {
         observation(property, structure[k], property == FORCE ? atom[k] : 0, property == FORCE ? component[k] : 0, 0,
-                    false, true);
+                    false, true, 0);
         double e = 0.0;
         cudaCheck(cudaMemcpyAsync(&e, err_, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
         cudaCheck(cudaStreamSynchronize(st), "sync");
@@ -1292,7 +1395,7 @@ int Training::updateThreshold(int property, int numUpdates, int numCandidates, c
             chosenErr = e;
             if (frac > threshold) break;
         }
-        step(property, structure[chosen], property == FORCE ? atom[chosen] : 0);
+        step(property, structure[chosen], property == FORCE ? atom[chosen] : 0, 1);
         if (errors) errors[u] = chosenErr;
     }
     cudaCheck(cudaStreamSynchronize(st), "sync");
@@ -1341,7 +1444,7 @@ void Training::observe(int property, int structure, int atom, int component, dou
         err_ = tAlloc<double>(1);
     }
     cudaStream_t st = set_.stream();
-    observation(property, structure, atom, component, 0, false, true);
+    observation(property, structure, atom, component, 0, false, true, 0);
     std::vector<double> h(P_);
     cudaCheck(cudaMemcpyAsync(h.data(), H_, sizeof(double) * P_, cudaMemcpyDeviceToHost, st), "D2H");
     cudaCheck(cudaMemcpyAsync(error, err_, sizeof(double), cudaMemcpyDeviceToHost, st), "D2H");
@@ -1356,7 +1459,7 @@ void Training::flushKalman()
     {
         dim3 grid((B.count + 255) / 256, B.count);
         kKalmanP<<<grid, 256, 0, set_.stream()>>>(Pm_ + B.pOffset, Kb_[cur_] + B.begin, Xb_[cur_] + B.begin, B.count,
-                                                  pendingScale_, pendingQ_);
+                                                  pendingScale_, pendingQ_, pendingRank_, P_);
     }
     cudaCheck(cudaGetLastError(), "kalman flush");
     pending_ = false;

@@ -103,6 +103,9 @@ public:
     // error shared by the element's fraction of the atoms (energies) or of the
     // observed atom's neighbours (forces).  Set it before the updater.
     void setUpdateStrategy(int strategy);
+    // jacobian_mode 2: every candidate of a task batch is its own observation
+    // (the Kalman filter with the combined strategy; at most 16 per update).
+    void setFullJacobian(bool full) { fullJacobian_ = full; }
     void setTaskBatchSize(int energy, int force)
     {
         taskBatchEnergy_ = energy;
@@ -142,10 +145,10 @@ public:
     int updaterType() const { return type_; }
 
 private:
-    void observation(int property, int s, int a, int c, int t, bool accumulate, bool last);
+    void observation(int property, int s, int a, int c, int t, bool accumulate, bool last, int column = 0);
     void flushKalman();
     void initKalman(double epsilon);
-    void step(int property, int s, int a);
+    void step(int property, int s, int a, int m);
     struct Block
     {
         int begin, count;     // device weights [begin, begin + count)
@@ -169,6 +172,8 @@ private:
     std::vector<int> atomBegin_;
     double forceWeight_ = 1.0;
     int taskBatchEnergy_ = 1, taskBatchForce_ = 1;
+    bool fullJacobian_ = false;
+    int pendingRank_ = 1;
     std::vector<double> eRefHost_, fRefHost_;   // references, internal units
     int type_ = -1;
     // Kalman filter state (host scalars as in KalmanFilter)

@@ -98,6 +98,12 @@ class Training:
         before setting up the updater."""
         _lib.check(self._lib.n2p2_training_set_update_strategy(self._h, int(strategy)))
 
+    def setJacobianMode(self, mode=1):
+        """jacobian_mode 0/1 (a task batch summed into one observation) or 2
+        (every candidate its own observation; Kalman filter, combined
+        strategy, at most 16)."""
+        _lib.check(self._lib.n2p2_training_set_jacobian_mode(self._h, int(mode)))
+
     def setTaskBatchSize(self, energy=1, force=1):
         """task_batch_size_energy / task_batch_size_force: candidates summed
         into one observation per update."""

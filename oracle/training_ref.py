@@ -200,7 +200,7 @@ class KalmanFilter:
         self.numUpdates = 0
 
     def update(self, w, H, xi):
-        H = H.reshape(-1, 1)
+        H = H if H.ndim == 2 else H.reshape(-1, 1)
         xi = np.atleast_1d(xi)
         Pl = np.tril(self.P)
         Psym = Pl + np.tril(self.P, -1).T
@@ -322,6 +322,18 @@ class Training:
             w = self.nets.weights[o0:o1]      # a view: the updater changes the weights in place
             self.updater[e].update(w, He, xi)
         return err
+
+    def update_full(self, prop, candidates):
+        """jacobian_mode 2: every candidate its own observation (columns of
+        H, entries of xi), one updater step."""
+        errs, cols = [], []
+        for s, atom, comp in candidates:
+            err, H = self.observation(prop, s, atom, comp)
+            errs.append(err)
+            cols.append(H * (self.force_weight if prop == 1 else 1.0))
+        xi = np.array(errs) * (self.force_weight if prop == 1 else 1.0)
+        self.updater.update(self.nets.weights, np.stack(cols, axis=1), xi)
+        return errs
 
     def update_batch(self, prop, candidates):
         """One update from a task batch of candidates: errors and Jacobians

@@ -265,3 +265,30 @@ def test_sort_selection_order(data):
         tr.close()
         m.close()
 
+
+@pytest.mark.parametrize("updater", UPDATERS[:2], ids=[u[0] for u in UPDATERS[:2]])
+def test_full_jacobian_matches_oracle(data, updater):
+    """jacobian_mode 2: a task batch's candidates as separate observations of
+    one Kalman update (m x m gain)."""
+    m, tr, ref = _pair(data, updater)
+    try:
+        tr.setJacobianMode(2)
+        tr.setTaskBatchSize(energy=3, force=2)
+        e = tr.update(ENERGY, [1, 3, 0, 2, 0, 1])
+        e_ref = ref.update_full(0, [(1, 0, 0), (3, 0, 0), (0, 0, 0)]) + ref.update_full(0, [(2, 0, 0), (0, 0, 0),
+                                                                                         (1, 0, 0)])
+        # the m x m inverse (Gauss-Jordan here, LU in numpy) rounds differently: errors are held
+        # relative to the largest one of the sequence
+        assert np.allclose(e, e_ref, rtol=1e-9, atol=1e-9 * np.abs(e_ref).max())
+        cands = [(2, 7, 1), (0, 5, 2), (3, 11, 0), (1, 4, 2)]
+        s, a, c = (np.array(x) for x in zip(*cands))
+        f = tr.update(FORCE, s, a, c)
+        f_ref = ref.update_full(1, cands[:2]) + ref.update_full(1, cands[2:])
+        assert np.allclose(f, f_ref, rtol=1e-9, atol=1e-9 * np.abs(f_ref).max())
+        assert H.max_rel(tr.weights(), ref.nets.weights) <= 1e-9
+        st = tr.kalmanStatus()
+        assert abs(st["Pdiag"] - np.mean(np.abs(np.diag(ref.updater.P)))) <= 1e-9 * st["Pdiag"]
+    finally:
+        tr.close()
+        m.close()
+
