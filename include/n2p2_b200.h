@@ -156,11 +156,63 @@ n2p2_status n2p2_batch_set_positions(n2p2_batch* batch, const double* positions,
 
 /* Mode::evaluateNNP (Mode.cpp:2029-2077) on every structure: neighbour list,
  * symmetry functions, networks, energies and (flag) forces.  Asynchronous
- * except for the first call after n2p2_batch_set_structures. */
+ * except for the first call after n2p2_batch_set_structures.  Later calls
+ * replay the work with the neighbour buffers sized by the first; if new
+ * positions make the lists longer than those buffers, the next call that
+ * reads results (any n2p2_batch_get_*, n2p2_batch_synchronize,
+ * n2p2_batch_evaluate_host) grows them and evaluates again before it returns,
+ * so no result ever comes from a truncated list (the reference's list never
+ * truncates, Structure.cpp:287-398). */
 n2p2_status n2p2_batch_evaluate(n2p2_batch* batch, int flags);
+
+/* ---- the stages of Mode::evaluateNNP as separate calls ----
+ *
+ * Same kernels as n2p2_batch_evaluate, launched one stage at a time on the
+ * batch's stream, so the sequence neighbour list -> symmetry functions
+ * (derivatives) -> atomic networks (derivatives) -> energy -> forces gives
+ * the same bits as one evaluation.  The symmetry-function call keeps the
+ * reference's caching flags (Structure::hasSymmetryFunctions /
+ * hasSymmetryFunctionDerivatives, Mode.cpp:1634-1635): it returns at once
+ * when the requested results exist.  New structures or positions clear every
+ * flag; n2p2_batch_evaluate sets them.  A stage whose inputs were not
+ * calculated fails with N2P2_ERR_RUNTIME. */
+#define N2P2_DERIVATIVES_NONE 0     /* values only                                      */
+#define N2P2_DERIVATIVES 1          /* derivatives, contracted with dE/dG by calculate_forces */
+#define N2P2_DERIVATIVES_STORED 2   /* derivatives stored as Atom::dGdr / Atom::Neighbor::dGdr
+                                       (n2p2_batch_get_dGdr; FP64, Gaussian functions only) */
+
+/* Structure::calculateNeighborList(maxCutoffRadius, false)
+ * (Structure.cpp:287-398) on every structure (with external lists: their
+ * entries).  Synchronises (the entry count sizes the buffers). */
+n2p2_status n2p2_batch_calculate_neighbor_list(n2p2_batch* batch);
+
+/* Mode::calculateSymmetryFunctions (Mode.cpp:1549-1628) and
+ * Mode::calculateSymmetryFunctionGroups (Mode.cpp:1630-1709): Atom::G of
+ * every atom, the extrapolation check when statistics are set up, and
+ * derivatives as `derivatives` says.  Both names compute the same values
+ * (the reference's two loops differ only in how they visit the functions). */
+n2p2_status n2p2_batch_calculate_symmetry_functions(n2p2_batch* batch, int derivatives);
+n2p2_status n2p2_batch_calculate_symmetry_function_groups(n2p2_batch* batch, int derivatives);
+
+/* Mode::calculateAtomicNeuralNetworks (Mode.cpp:1711-1732, 2G): Atom::energy
+ * and, with derivatives != 0, Atom::dEdG. */
+n2p2_status n2p2_batch_calculate_atomic_neural_networks(n2p2_batch* batch, int derivatives);
+
+/* Mode::calculateEnergy (Mode.cpp:1876-1901): Structure::energy, read with
+ * n2p2_batch_get_energies. */
+n2p2_status n2p2_batch_calculate_energy(n2p2_batch* batch);
+
+/* Mode::calculateForces (Mode.cpp:1922-1984): Atom::f, read with
+ * n2p2_batch_get_forces; needs symmetry-function derivatives and dE/dG. */
+n2p2_status n2p2_batch_calculate_forces(n2p2_batch* batch);
 
 /* Wait for the batch's stream; reports device-side input errors. */
 n2p2_status n2p2_batch_synchronize(n2p2_batch* batch);
+
+/* Neighbour entries the batch's buffers hold now, and how many evaluations
+ * were repeated because new positions outgrew them (no counterpart in the
+ * reference, whose lists are std::vectors). */
+n2p2_status n2p2_batch_get_neighbor_capacity(n2p2_batch* batch, int64_t* capacity, int64_t* recoveries);
 
 /* Structure::energy per structure after Prediction::predict's conversion
  * (physical units, atomic energy offsets added). */
@@ -217,15 +269,17 @@ n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches);
 /* ---- allocation-free neighbour list (no counterpart in the reference) ---- */
 
 /* Neighbour list of ONE structure, written into device buffers the caller
- * owns, for callers that cannot call cudaMalloc where they need the list: an
- * MD step being recorded into a CUDA graph, a code whose device memory
- * belongs to its own pool allocator, or a loop that must not pay cudaMalloc's
- * device-wide synchronisation.  Nothing is allocated: the scratch (cell
+ * owns, for callers that cannot call cudaMalloc where they need the list: a
+ * code whose device memory belongs to its own pool allocator, or a step loop
+ * that must not pay cudaMalloc's device-wide synchronisation.  Nothing is allocated: the scratch (cell
  * lists, counts, scan partials) is one fixed array in the library's device
  * memory (about 0.7 MB, held by every GPU that loads the library until the
  * process exits), shared by all calls.  Calls that overlap on the GPU race
  * on it; the first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and should come before any stream capture.
+ * (cudaGetSymbolAddress) and should come before any stream capture.  That
+ * address is kept per device for the life of the process: after a
+ * cudaDeviceReset in the host process it is stale, and the entry point must
+ * not be called again in that process.
  *
  * positions: device [numAtoms][3], internal units, inside the cell (e.g.
  * n2p2_batch_get_internal_positions); box: host [3][3] in the same units, or

@@ -25,6 +25,10 @@ EVAL_STORE_DGDR = 2
 EVAL_NO_GRAPH = 4
 EVAL_SF_ONLY = 8
 
+DERIVATIVES_NONE = 0
+DERIVATIVES = 1
+DERIVATIVES_STORED = 2
+
 TRAINING_ENERGY = 0
 TRAINING_FORCE = 1
 
@@ -63,6 +67,13 @@ SIGNATURES = {
     "n2p2_batch_set_positions": (_i, [_vp, _vp, _i]),
     "n2p2_batch_evaluate": (_i, [_vp, _i]),
     "n2p2_batch_synchronize": (_i, [_vp]),
+    "n2p2_batch_get_neighbor_capacity": (_i, [_vp, _P(_i64), _P(_i64)]),
+    "n2p2_batch_calculate_neighbor_list": (_i, [_vp]),
+    "n2p2_batch_calculate_symmetry_functions": (_i, [_vp, _i]),
+    "n2p2_batch_calculate_symmetry_function_groups": (_i, [_vp, _i]),
+    "n2p2_batch_calculate_atomic_neural_networks": (_i, [_vp, _i]),
+    "n2p2_batch_calculate_energy": (_i, [_vp]),
+    "n2p2_batch_calculate_forces": (_i, [_vp]),
     "n2p2_batch_get_energies": (_i, [_vp, _P(_d)]),
     "n2p2_batch_get_forces": (_i, [_vp, _P(_d)]),
     "n2p2_batch_evaluate_host": (_i, [_vp, _vp, _vp, _vp, _i]),

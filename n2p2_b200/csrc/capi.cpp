@@ -430,6 +430,69 @@ n2p2_status n2p2_batch_synchronize(n2p2_batch* batch)
     });
 }
 
+n2p2_status n2p2_batch_calculate_neighbor_list(n2p2_batch* batch)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->calculateNeighborList();
+    });
+}
+
+n2p2_status n2p2_batch_calculate_symmetry_function_groups(n2p2_batch* batch, int derivatives)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->calculateSymmetryFunctions(derivatives, batch->mode->precision,
+                                                 batch->mode->checkExtrapolation ? 1 : 0);
+        afterEvaluate(batch);
+    });
+}
+
+n2p2_status n2p2_batch_calculate_symmetry_functions(n2p2_batch* batch, int derivatives)
+{
+    return n2p2_batch_calculate_symmetry_function_groups(batch, derivatives);
+}
+
+n2p2_status n2p2_batch_calculate_atomic_neural_networks(n2p2_batch* batch, int derivatives)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->calculateAtomicNeuralNetworks(derivatives, batch->mode->precision);
+    });
+}
+
+n2p2_status n2p2_batch_calculate_energy(n2p2_batch* batch)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->calculateEnergy();
+    });
+}
+
+n2p2_status n2p2_batch_calculate_forces(n2p2_batch* batch)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->calculateForces();
+    });
+}
+
+n2p2_status n2p2_batch_get_neighbor_capacity(n2p2_batch* batch, int64_t* capacity, int64_t* recoveries)
+{
+    N2P2_REQUIRE(batch);
+    return guard([&] {
+        setDevice(batch->mode);
+        batch->batch->verify();
+        if (capacity) *capacity = batch->batch->neighborCapacity();
+        if (recoveries) *recoveries = batch->batch->overflowRecoveries();
+    });
+}
+
 n2p2_status n2p2_batch_get_energies(n2p2_batch* batch, double* energies)
 {
     N2P2_REQUIRE(batch);

@@ -701,6 +701,8 @@ void Batch::setStructures(std::vector<StructureInput> const& s, const int* eleme
     cudaCheck(cudaStreamSynchronize(stream_), "setStructures");
     allocateNeighbors(std::max<int64_t>(capacity, 1));
     capacityVerified_ = false;
+    pendingVerify_ = false;
+    stage_ = StageState{};
     tuned_[0] = tuned_[1] = false;   // new workload: shapes come from the cache or are measured again
 }
 
@@ -787,6 +789,8 @@ void Batch::beginExternal(int numCenters, const int* elements, int numTargets, c
               "upload centre indices");
     cudaCheck(cudaMemsetAsync(Ftarget_, 0, sizeof(double) * 3 * T, stream_), "memset");
     capacityVerified_ = false;
+    pendingVerify_ = false;
+    stage_ = StageState{};
     tuned_[0] = tuned_[1] = false;
 }
 
@@ -879,6 +883,7 @@ void Batch::setExternalLists(ExternalLists const& l)
 
 void Batch::targetForces(double* out)
 {
+    verify();
     if (!external_) throw std::runtime_error("ERROR: target forces need external neighbour lists.\n");
     cudaCheck(cudaMemcpyAsync(out, Ftarget_, sizeof(double) * 3 * (size_t)numTargets_, cudaMemcpyDeviceToHost, stream_),
               "F D2H");
@@ -976,6 +981,8 @@ void Batch::allocateDGdr()
 void Batch::setPositionsHost(const double* r)
 {
     if (external_) throw std::runtime_error("ERROR: external neighbour lists carry no positions.\n");
+    verify();   // results of the previous positions stay complete until they are replaced
+    stage_ = StageState{};
     cudaCheck(cudaMemcpyAsync(rin_, r, sizeof(double) * 3 * (size_t)N_, cudaMemcpyHostToDevice, stream_),
               "positions H2D");
 }
@@ -983,17 +990,21 @@ void Batch::setPositionsHost(const double* r)
 void Batch::setPositionsDevice(const double* r)
 {
     if (external_) throw std::runtime_error("ERROR: external neighbour lists carry no positions.\n");
+    verify();
+    stage_ = StageState{};
     cudaCheck(cudaMemcpyAsync(rin_, r, sizeof(double) * 3 * (size_t)N_, cudaMemcpyDeviceToDevice, stream_),
               "positions D2D");
 }
 
 // The kernel sequence of one evaluation (Mode::evaluateNNP, Mode.cpp:2029-2077).
-void Batch::record(int flags, int precision, int checkExtrapolation, std::vector<Mark>* marks)
+void Batch::record(int flags, int precision, int checkExtrapolation, std::vector<Mark>* marks, int stages)
 {
     DevModel const& m = dmodel_.view;
     const bool sfOnly = (flags & EVAL_SF_ONLY) != 0;
     const bool forces = (flags & EVAL_FORCES) != 0 && !sfOnly;
     const bool stored = (flags & EVAL_STORE_DGDR) != 0;
+    const bool whole = stages == STAGE_ALL;   // an evaluation (not one of the separate stage calls)
+    if (sfOnly) stages &= STAGE_NEIGHBORS | STAGE_SF;
     int launches = 0;
     auto mark = [&](char const* name) {
         if (!marks) return;
@@ -1003,83 +1014,91 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         marks->push_back(mk);
     };
     mark("start");
-    cudaCheck(cudaMemsetAsync(v_.status, 0, sizeof(DevStatus), stream_), "status reset");
-    if (external_)
+    if (stages & STAGE_NEIGHBORS)
     {
-        if (extRaw_)
+        cudaCheck(cudaMemsetAsync(v_.status, 0, sizeof(DevStatus), stream_), "status reset");
+        if (external_)
         {
-            launchExternalEntries(raw_, v_, v_.scanTmp, sms_, stream_);
-            launches += 5;
+            if (extRaw_)
+            {
+                launchExternalEntries(raw_, v_, v_.scanTmp, sms_, stream_);
+                launches += 5;
+            }
+            else   // the entry count the neighbour build would report (read by the cutoff stage)
+                cudaCheck(cudaMemcpyAsync(&v_.status->totalNeighbors, entriesDev_, sizeof(int64_t),
+                                          cudaMemcpyDeviceToDevice, stream_),
+                          "entry count");
+            launchExternalTranspose(v_, numTargets_, centerIndex_, tCount_, tFill_, tOffset_, tEntryTmp_, tEntry_,
+                                    targetCenter_, tScanTmp_, sms_, stream_);
+            launches += 7;
+            mark("neighbor_list");
         }
-        else   // the entry count the neighbour build would report (read by the cutoff stage)
-            cudaCheck(cudaMemcpyAsync(&v_.status->totalNeighbors, entriesDev_, sizeof(int64_t),
-                                      cudaMemcpyDeviceToDevice, stream_),
-                      "entry count");
-        launchExternalTranspose(v_, numTargets_, centerIndex_, tCount_, tFill_, tOffset_, tEntryTmp_, tEntry_,
-                                targetCenter_, tScanTmp_, sms_, stream_);
-        launches += 7;
-        mark("neighbor_list");
-    }
-    else
-    {
-        launchPreparePositions(v_, rin_, remap_, model_.normalize ? 1 : 0, model_.convLength, stream_);
-        launches += 1;
-        mark("prepare_positions");
-        launchNeighborBuild(v_, model_.maxCutoffRadius * model_.maxCutoffRadius, stream_);
-        launches += 3 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1;
-        mark("neighbor_list");
-    }
-    launchCutoffValues(m, v_, sms_, stream_);
-    launches += 1;
-    mark("cutoff_values");
-    // the G pass records its candidate acceptance for the force pass
-    v_.candMask = nullptr;
-    v_.maskCapacity = 0;
-    if (forces && !stored)
-    {
-        launchMaskOffsets(m, v_, sms_, stream_);
-        launches += 4;
-        mark("candidate_masks");
-        v_.candMask = maskBuf_;
-        v_.maskCapacity = maskBuf_ ? maskCap_ : 0;
-    }
-    if (stored)
-    {
-        launchSFDerivatives(m, v_, sms_, stream_);
-        launches += 2;
-        mark("sf_derivatives");
-    }
-    else
-    {
-        launchSFValues(m, v_, precision, sms_, stream_, sfShape_[0][precision]);
-        launches += 2;
-        if (m.numCompactGroups > 0)
+        else
         {
-            launchCompactValues(m, v_, sms_, stream_);
+            launchPreparePositions(v_, rin_, remap_, model_.normalize ? 1 : 0, model_.convLength, stream_);
             launches += 1;
+            mark("prepare_positions");
+            launchNeighborBuild(v_, model_.maxCutoffRadius * model_.maxCutoffRadius, stream_);
+            launches += 3 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1;
+            mark("neighbor_list");
         }
-        mark("sf_values");
-    }
-    if (checkExtrapolation)
-    {
-        launchExtrapolationCheck(m, v_, sms_, stream_);
+        launchCutoffValues(m, v_, sms_, stream_);
         launches += 1;
-        mark("extrapolation_check");
+        mark("cutoff_values");
     }
-    if (sfOnly)   // Mode::calculateSymmetryFunctionGroups alone (nnp-scaling)
+    if (stages & STAGE_SF)
     {
-        cudaCheck(cudaGetLastError(), "kernel launch");
-        launches_ = launches;
-        return;
+        if (!whole)   // a separate symmetry-function call counts its own warnings
+            cudaCheck(cudaMemsetAsync(&v_.status->extrapolationWarnings, 0, sizeof(int), stream_), "status reset");
+        // the G pass records its candidate acceptance for the force pass
+        v_.candMask = nullptr;
+        v_.maskCapacity = 0;
+        if (forces && !stored)
+        {
+            launchMaskOffsets(m, v_, sms_, stream_);
+            launches += 4;
+            mark("candidate_masks");
+            v_.candMask = maskBuf_;
+            v_.maskCapacity = maskBuf_ ? maskCap_ : 0;
+        }
+        if (stored)
+        {
+            launchSFDerivatives(m, v_, sms_, stream_);
+            launches += 2;
+            mark("sf_derivatives");
+        }
+        else
+        {
+            launchSFValues(m, v_, precision, sms_, stream_, sfShape_[0][precision]);
+            launches += 2;
+            if (m.numCompactGroups > 0)
+            {
+                launchCompactValues(m, v_, sms_, stream_);
+                launches += 1;
+            }
+            mark("sf_values");
+        }
+        if (checkExtrapolation)
+        {
+            launchExtrapolationCheck(m, v_, sms_, stream_);
+            launches += 1;
+            mark("extrapolation_check");
+        }
     }
-    if (precision == PREC_MIXED && dmodel_.tcNetwork) launchNetworkTC(m, v_, forces ? 1 : 0, sms_, stream_);
-    else launchNetworkFP64(m, v_, forces ? 1 : 0, sms_, stream_);
-    launches += 1;
-    mark("network");
-    launchEnergySum(v_, stream_);
-    launches += 1;
-    mark("energy_sum");
-    if (forces)
+    if (stages & STAGE_NETWORKS)
+    {
+        if (precision == PREC_MIXED && dmodel_.tcNetwork) launchNetworkTC(m, v_, forces ? 1 : 0, sms_, stream_);
+        else launchNetworkFP64(m, v_, forces ? 1 : 0, sms_, stream_);
+        launches += 1;
+        mark("network");
+    }
+    if (stages & STAGE_ENERGY)
+    {
+        launchEnergySum(v_, stream_);
+        launches += 1;
+        mark("energy_sum");
+    }
+    if (forces && (stages & STAGE_FORCES))
     {
         if (stored)
         {
@@ -1104,7 +1123,7 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         mark("gather_forces");
     }
     cudaCheck(cudaGetLastError(), "kernel launch");
-    launches_ = launches;
+    if (whole) launches_ = launches;
 }
 
 std::vector<std::pair<std::string, double>> Batch::profileStages(int flags, int precision, int checkExtrapolation)
@@ -1112,6 +1131,7 @@ std::vector<std::pair<std::string, double>> Batch::profileStages(int flags, int 
     if (!capacityVerified_) evaluate(flags, precision, checkExtrapolation);
     std::vector<Mark> marks;
     record(flags, precision, checkExtrapolation, &marks);
+    pendingVerify_ = true;
     synchronize();
     std::vector<std::pair<std::string, double>> out;
     for (size_t k = 1; k < marks.size(); ++k)
@@ -1126,6 +1146,7 @@ std::vector<std::pair<std::string, double>> Batch::profileStages(int flags, int 
 
 void Batch::countWork(int64_t* counts)
 {
+    verify();
     if (external_) throw std::runtime_error("ERROR: work counters need structures, not external neighbour lists.\n");
     if (dmodel_.view.numCompactGroups > 0)
         throw std::runtime_error("ERROR: work counters cover the Gaussian symmetry functions only.\n");
@@ -1245,6 +1266,7 @@ Batch::TuneResult Batch::autotune(int precision, int checkExtrapolation, bool us
     {
         // fill every pass input (neighbour data, dE/dG) once, then time the passes alone
         record(EVAL_FORCES, precision, checkExtrapolation);
+        pendingVerify_ = true;
         DevModel const& m = dmodel_.view;
         cudaEvent_t e0, e1;
         cudaCheck(cudaEventCreate(&e0), "event");
@@ -1314,6 +1336,81 @@ Batch::TuneResult Batch::autotune(int precision, int checkExtrapolation, bool us
     return r;
 }
 
+void Batch::requireStructures()
+{
+    if (N_ == 0) throw std::runtime_error("ERROR: no structures set.\n");
+}
+
+void Batch::calculateNeighborList()
+{
+    requireStructures();
+    verify();
+    stage_ = StageState{};
+    for (int attempt = 0;; ++attempt)
+    {
+        record(0, PREC_FP64, 0, nullptr, STAGE_NEIGHBORS);
+        const DevStatus st = readStatus();
+        if (st.totalNeighbors <= capacity_) break;
+        if (attempt == 2) throw std::runtime_error("ERROR: neighbour capacity could not be established.\n");
+        allocateNeighbors((int64_t)(st.totalNeighbors * 1.05) + 1024);
+    }
+    stage_.neighbors = true;
+}
+
+void Batch::calculateSymmetryFunctions(int derivatives, int precision, int checkExtrapolation)
+{
+    requireStructures();
+    if (derivatives < 0 || derivatives > 2) throw std::invalid_argument("ERROR: derivatives must be 0, 1 or 2.\n");
+    if (!stage_.neighbors) throw std::runtime_error("ERROR: neighbour list not calculated.\n");
+    // Mode.cpp:1634-1635: skip the whole structure if the results exist
+    if (stage_.sfDerivatives && (derivatives < 2 || stage_.sfStored)) return;
+    if (stage_.sf && derivatives == 0) return;
+    int flags = derivatives ? EVAL_FORCES : 0;
+    if (derivatives == 2)
+    {
+        if (external_) throw std::runtime_error("ERROR: stored dG/dr is not available with external neighbour lists.\n");
+        if (dmodel_.view.numCompactGroups > 0)
+            throw std::runtime_error("ERROR: stored dG/dr is not available for compact symmetry functions.\n");
+        if (precision != PREC_FP64) throw std::runtime_error("ERROR: stored dG/dr is FP64 only.\n");
+        allocateDGdr();
+        flags |= EVAL_STORE_DGDR;
+    }
+    record(flags, precision, checkExtrapolation, nullptr, STAGE_SF);
+    stage_.sf = true;
+    stage_.sfDerivatives = derivatives > 0;
+    stage_.sfStored = derivatives == 2;
+    stage_.sfPrecision = precision;
+    stage_.networks = stage_.dEdG = stage_.energy = stage_.forces = false;
+}
+
+void Batch::calculateAtomicNeuralNetworks(int derivatives, int precision)
+{
+    requireStructures();
+    if (!dmodel_.networksSet) throw std::runtime_error("ERROR: weights of element " + dmodel_.missingWeights + " not set.\n");
+    if (!stage_.sf) throw std::runtime_error("ERROR: symmetry functions not calculated.\n");
+    record(derivatives ? EVAL_FORCES : 0, precision, 0, nullptr, STAGE_NETWORKS);
+    stage_.networks = true;
+    stage_.dEdG = derivatives != 0;
+    stage_.energy = stage_.forces = false;
+}
+
+void Batch::calculateEnergy()
+{
+    requireStructures();
+    if (!stage_.networks) throw std::runtime_error("ERROR: atomic neural networks not calculated.\n");
+    record(0, PREC_FP64, 0, nullptr, STAGE_ENERGY);
+    stage_.energy = true;
+}
+
+void Batch::calculateForces()
+{
+    requireStructures();
+    if (!stage_.sfDerivatives) throw std::runtime_error("ERROR: symmetry function derivatives not calculated.\n");
+    if (!stage_.dEdG) throw std::runtime_error("ERROR: dE/dG not calculated (atomic networks without derivatives).\n");
+    record(EVAL_FORCES | (stage_.sfStored ? EVAL_STORE_DGDR : 0), stage_.sfPrecision, 0, nullptr, STAGE_FORCES);
+    stage_.forces = true;
+}
+
 void Batch::evaluate(int flags, int precision, int checkExtrapolation)
 {
     if (N_ == 0) throw std::runtime_error("ERROR: no structures set.\n");
@@ -1327,17 +1424,31 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
         if (precision != PREC_FP64) throw std::runtime_error("ERROR: stored dG/dr is FP64 only.\n");
         allocateDGdr();
     }
+    {
+        const bool sfOnly = (flags & EVAL_SF_ONLY) != 0, f = (flags & EVAL_FORCES) && !sfOnly;
+        stage_ = StageState{};
+        stage_.neighbors = stage_.sf = true;
+        stage_.sfDerivatives = f;
+        stage_.sfStored = f && (flags & EVAL_STORE_DGDR);
+        stage_.sfPrecision = precision;
+        stage_.networks = stage_.energy = !sfOnly;
+        stage_.dEdG = stage_.forces = f;
+    }
+    lastFlags_ = flags;
+    lastPrecision_ = precision;
+    lastCheck_ = checkExtrapolation;
+    pendingVerify_ = false;
     if (!capacityVerified_)
     {
         for (int attempt = 0; attempt < 3; ++attempt)
         {
             record(flags, precision, checkExtrapolation);
-            DevStatus st = status();
+            DevStatus st = readStatus();
             if (st.totalNeighbors <= capacity_) break;
             allocateNeighbors((int64_t)(st.totalNeighbors * 1.05) + 1024);
             if (flags & EVAL_STORE_DGDR) allocateDGdr();
         }
-        DevStatus st = status();
+        DevStatus st = readStatus();
         if (st.totalNeighbors > capacity_) throw std::runtime_error("ERROR: neighbour capacity could not be established.\n");
         if ((flags & EVAL_FORCES) && st.maskWords > maskCap_)
         {
@@ -1353,6 +1464,8 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
     if (flags & EVAL_NO_GRAPH)
     {
         record(flags, precision, checkExtrapolation);
+        pendingVerify_ = true;
+        verify();
         return;
     }
     const int key = (flags & (EVAL_FORCES | EVAL_STORE_DGDR | EVAL_SF_ONLY)) | (precision << 4) |
@@ -1378,11 +1491,32 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
         graphKey_ = key;
     }
     cudaCheck(cudaGraphLaunch(graphExec_, stream_), "graph launch");
+    pendingVerify_ = true;
+}
+
+void Batch::verify()
+{
+    if (!pendingVerify_) return;
+    pendingVerify_ = false;
+    const DevStatus st = readStatus();
+    if (st.totalNeighbors <= capacity_) return;
+    // The lists outgrew the buffers sized at the first evaluation: size them
+    // again and repeat the evaluation directly (the graph is recaptured at
+    // the next call).
+    ++overflowRecoveries_;
+    capacityVerified_ = false;
+    evaluate(lastFlags_, lastPrecision_, lastCheck_);
 }
 
 void Batch::synchronize() { cudaCheck(cudaStreamSynchronize(stream_), "synchronize"); }
 
 DevStatus Batch::status()
+{
+    verify();
+    return readStatus();
+}
+
+DevStatus Batch::readStatus()
 {
     DevStatus st{};
     cudaCheck(cudaMemcpyAsync(&st, v_.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream_), "status D2H");
@@ -1396,6 +1530,7 @@ DevStatus Batch::status()
 
 int64_t Batch::numNeighborEntries()
 {
+    verify();
     int64_t total = 0;
     cudaCheck(cudaMemcpyAsync(&total, v_.nbrOffset + N_, sizeof(int64_t), cudaMemcpyDeviceToHost, stream_), "D2H");
     synchronize();
@@ -1404,6 +1539,7 @@ int64_t Batch::numNeighborEntries()
 
 void Batch::energies(double* out)
 {
+    verify();
     std::vector<double> e(S_);
     cudaCheck(cudaMemcpyAsync(e.data(), v_.Estruct, sizeof(double) * S_, cudaMemcpyDeviceToHost, stream_), "E D2H");
     synchronize();
@@ -1440,6 +1576,7 @@ double Batch::forceToInternal() const
 
 void Batch::forces(double* out)
 {
+    verify();
     cudaCheck(cudaMemcpyAsync(out, v_.F, sizeof(double) * 3 * (size_t)N_, cudaMemcpyDeviceToHost, stream_), "F D2H");
     synchronize();
     if (model_.normalize)
@@ -1452,6 +1589,7 @@ void Batch::forces(double* out)
 
 void Batch::copyNeighbors(int64_t* offsets, int* index, int* image, double* d, double* dr)
 {
+    verify();
     std::vector<int64_t> off(N_ + 1);
     cudaCheck(cudaMemcpy(off.data(), v_.nbrOffset, sizeof(int64_t) * (N_ + 1), cudaMemcpyDeviceToHost), "D2H");
     const int64_t M = off[N_];
@@ -1488,6 +1626,7 @@ void packPerAtom(std::vector<double> const& src, int stride, std::vector<int> co
 
 void Batch::copyG(double* out)
 {
+    verify();
     std::vector<double> g((size_t)N_ * v_.gStride);
     cudaCheck(cudaMemcpy(g.data(), v_.G, sizeof(double) * g.size(), cudaMemcpyDeviceToHost), "D2H");
     packPerAtom(g, v_.gStride, elemHost_, model_, out);
@@ -1495,6 +1634,7 @@ void Batch::copyG(double* out)
 
 void Batch::copyDEdG(double* out)
 {
+    verify();
     std::vector<double> g((size_t)N_ * v_.gStride);
     cudaCheck(cudaMemcpy(g.data(), v_.dEdG, sizeof(double) * g.size(), cudaMemcpyDeviceToHost), "D2H");
     packPerAtom(g, v_.gStride, elemHost_, model_, out);
@@ -1502,11 +1642,13 @@ void Batch::copyDEdG(double* out)
 
 void Batch::copyAtomicEnergies(double* out)
 {
+    verify();
     cudaCheck(cudaMemcpy(out, v_.Eatom, sizeof(double) * N_, cudaMemcpyDeviceToHost), "D2H");
 }
 
 void Batch::sfStatistics(int64_t* counts, double* stats)
 {
+    verify();
     const int ne = (int)model_.numElements();
     const int maxSF = std::max(dmodel_.maxSF, 1);
     int largest = 0;
@@ -1530,11 +1672,13 @@ void Batch::sfStatistics(int64_t* counts, double* stats)
 
 void Batch::copyAtomWarnings(int* out)
 {
+    verify();
     cudaCheck(cudaMemcpy(out, v_.atomWarnings, sizeof(int) * N_, cudaMemcpyDeviceToHost), "D2H");
 }
 
 void Batch::copyPositions(double* out)
 {
+    verify();
     std::vector<double> x(N_), y(N_), z(N_);
     cudaCheck(cudaMemcpy(x.data(), v_.px, sizeof(double) * N_, cudaMemcpyDeviceToHost), "D2H");
     cudaCheck(cudaMemcpy(y.data(), v_.py, sizeof(double) * N_, cudaMemcpyDeviceToHost), "D2H");
@@ -1549,6 +1693,7 @@ void Batch::copyPositions(double* out)
 
 void Batch::copyDGdr(double* self, double* nbr)
 {
+    verify();
     if (!dgdrAllocated_) throw std::runtime_error("ERROR: dG/dr was not stored (evaluate with the store flag).\n");
     std::vector<int64_t> off(N_ + 1);
     cudaCheck(cudaMemcpy(off.data(), v_.nbrOffset, sizeof(int64_t) * (N_ + 1), cudaMemcpyDeviceToHost), "D2H");

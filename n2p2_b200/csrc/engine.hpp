@@ -142,7 +142,52 @@ public:
     void setPositionsDevice(const double* r);
     // Mode::evaluateNNP; asynchronous unless the neighbour capacity must be
     // (re)established, which happens on the first call and after overflow.
+    // A graph replay runs with the buffers sized at the first call: when new
+    // positions make the lists longer, the kernels skip the atoms whose
+    // entries do not fit, so every reader of the results calls verify()
+    // first, which detects that, grows the buffers and evaluates again.
     void evaluate(int flags, int precision, int checkExtrapolation);
+    // Synchronises; after a truncated evaluation, grows the neighbour
+    // buffers and repeats the evaluation directly (the reference's list never
+    // truncates, Structure.cpp:287-398).  Idempotent until the next evaluate.
+    void verify();
+    // Evaluations repeated by verify() since the batch was created.
+    int64_t overflowRecoveries() const { return overflowRecoveries_; }
+    int64_t neighborCapacity() const { return capacity_; }
+    // The stages of Mode::evaluateNNP as separate calls (Mode.h:298-378),
+    // launched directly on the batch's stream (no CUDA graph) with the same
+    // kernels, so a sequence of them gives the bits evaluate() gives.
+    //   calculateNeighborList          Structure::calculateNeighborList(rc, false)
+    //                                  (Structure.cpp:287-398); synchronises to
+    //                                  size the buffers
+    //   calculateSymmetryFunctions     Mode::calculateSymmetryFunction[Groups]
+    //                                  (Mode.cpp:1549-1709); derivatives 0 = values,
+    //                                  1 = values with derivatives (contracted by
+    //                                  calculateForces, nothing stored), 2 = dG/dr
+    //                                  stored (Atom::dGdr, Atom::Neighbor::dGdr; FP64)
+    //   calculateAtomicNeuralNetworks  Mode.cpp:1711-1732 (2G): E_i, and dE/dG with
+    //                                  derivatives
+    //   calculateEnergy                Mode.cpp:1876-1901
+    //   calculateForces                Mode.cpp:1922-1984 (needs derivatives of both)
+    // The symmetry-function call keeps the reference's caching flags
+    // (Structure::hasSymmetryFunctions / hasSymmetryFunctionDerivatives,
+    // Mode.cpp:1634-1635): it returns at once when its results exist.  New
+    // structures or positions clear every flag; evaluate() sets them.  A stage
+    // whose inputs are missing throws std::runtime_error (the reference would
+    // read empty vectors).
+    void calculateNeighborList();
+    void calculateSymmetryFunctions(int derivatives, int precision, int checkExtrapolation);
+    void calculateAtomicNeuralNetworks(int derivatives, int precision);
+    void calculateEnergy();
+    void calculateForces();
+    struct StageState
+    {
+        bool neighbors = false, sf = false, sfDerivatives = false, sfStored = false, networks = false,
+             dEdG = false, energy = false, forces = false;
+        int sfPrecision = 0;
+    };
+    StageState const& stageState() const { return stage_; }
+
     // Host-side results (synchronise first).
     void energies(double* out);       // physical units, with atomic energy offsets
     // Inverse of the conversions of energies() / forces(): physical energies
@@ -152,7 +197,7 @@ public:
     double forceToInternal() const;
     void forces(double* out);         // physical units, [N][3]
     void synchronize();
-    DevStatus status();
+    DevStatus status();   // verify(), then the device status word
 
     int numAtoms() const { return N_; }
     int numStructures() const { return S_; }
@@ -210,7 +255,18 @@ private:
         std::string name;
         cudaEvent_t event;
     };
-    void record(int flags, int precision, int checkExtrapolation, std::vector<Mark>* marks = nullptr);
+    enum Stage
+    {
+        STAGE_NEIGHBORS = 1,   // positions, neighbour lists, cutoff values
+        STAGE_SF = 2,          // symmetry functions (+ candidate masks, extrapolation check)
+        STAGE_NETWORKS = 4,    // atomic networks (+ dE/dG with EVAL_FORCES)
+        STAGE_ENERGY = 8,      // structure energies
+        STAGE_FORCES = 16,     // force pass + gather (with EVAL_FORCES)
+        STAGE_ALL = 31
+    };
+    void record(int flags, int precision, int checkExtrapolation, std::vector<Mark>* marks = nullptr,
+                int stages = STAGE_ALL);
+    DevStatus readStatus();   // the device status word as it is (synchronises)
     void releaseGraph();
     void releaseAll();
 
@@ -237,6 +293,11 @@ private:
     int* structBeginDev_ = nullptr;
     int64_t capacity_ = 0;
     bool capacityVerified_ = false;
+    bool pendingVerify_ = false;      // an evaluation ran that verify() has not checked
+    StageState stage_;                // results the separate stage calls (or evaluate) produced
+    void requireStructures();
+    int lastFlags_ = 0, lastPrecision_ = 0, lastCheck_ = 0;
+    int64_t overflowRecoveries_ = 0;
     bool dgdrAllocated_ = false;
     cudaGraphExec_t graphExec_ = nullptr;
     int graphKey_ = -1;

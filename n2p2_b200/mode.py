@@ -220,6 +220,31 @@ class Batch:
             (0 if graph else _lib.EVAL_NO_GRAPH) | (_lib.EVAL_SF_ONLY if symmetryFunctionsOnly else 0)
         _lib.check(self._lib.n2p2_batch_evaluate(self._h, flags))
 
+    # -- the stages of Mode::evaluateNNP as separate calls (Mode.h:298-378) --
+    def calculateNeighborList(self):
+        """Structure::calculateNeighborList(maxCutoffRadius, false) on every structure."""
+        _lib.check(self._lib.n2p2_batch_calculate_neighbor_list(self._h))
+
+    def calculateSymmetryFunctionGroups(self, derivatives):
+        """Mode::calculateSymmetryFunctionGroups: derivatives False/True, or
+        "stored" for Atom::dGdr / Atom::Neighbor::dGdr (FP64)."""
+        d = _lib.DERIVATIVES_STORED if derivatives == "stored" else (1 if derivatives else 0)
+        _lib.check(self._lib.n2p2_batch_calculate_symmetry_function_groups(self._h, d))
+
+    def calculateSymmetryFunctions(self, derivatives):
+        """Mode::calculateSymmetryFunctions (the same values as the groups form)."""
+        d = _lib.DERIVATIVES_STORED if derivatives == "stored" else (1 if derivatives else 0)
+        _lib.check(self._lib.n2p2_batch_calculate_symmetry_functions(self._h, d))
+
+    def calculateAtomicNeuralNetworks(self, derivatives):
+        _lib.check(self._lib.n2p2_batch_calculate_atomic_neural_networks(self._h, int(bool(derivatives))))
+
+    def calculateEnergy(self):
+        _lib.check(self._lib.n2p2_batch_calculate_energy(self._h))
+
+    def calculateForces(self):
+        _lib.check(self._lib.n2p2_batch_calculate_forces(self._h))
+
     def symmetryFunctionStatistics(self):
         """Per element: dict(count, min, max, sum, sum2) of the unscaled G of
         the last evaluation (n2p2_batch_get_symmetry_function_statistics)."""
@@ -256,6 +281,13 @@ class Batch:
         out = np.zeros((self.numAtoms, 3))
         _lib.check(self._lib.n2p2_batch_get_forces(self._h, _dp(out)))
         return out
+
+    def neighborCapacity(self):
+        """(entries the neighbour buffers hold, evaluations repeated because
+        new positions outgrew them)."""
+        c, r = ctypes.c_int64(), ctypes.c_int64()
+        _lib.check(self._lib.n2p2_batch_get_neighbor_capacity(self._h, ctypes.byref(c), ctypes.byref(r)))
+        return c.value, r.value
 
     def numNeighborEntries(self):
         n = ctypes.c_int64()
