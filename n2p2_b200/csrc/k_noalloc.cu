@@ -2,10 +2,9 @@
 // any device allocation.
 //
 // Why: some callers cannot call cudaMalloc at the point where they need a
-// neighbour list -- an MD engine that records its time step into a CUDA
-// graph (allocation is not allowed while a stream is being captured), a host
-// code whose device memory is owned by its own pool allocator, or a step loop
-// that must not pay cudaMalloc's implicit device synchronisation.  They pass
+// neighbour list -- a host code whose device memory is owned by its own pool
+// allocator, or a step loop that must not pay cudaMalloc's implicit device
+// synchronisation.  They pass
 // the positions and the output arrays; the scratch memory the build needs
 // (cell lists, per-atom counts, scan partials, a status word) lives in one
 // file-scope __device__ array of fixed size that every GPU loading the
@@ -225,7 +224,8 @@ std::mutex g_naMutex;
 DeviceScratch g_naScratch[64];
 
 // Device address of the scratch array on the current device (looked up once
-// per device; the first call must not happen during stream capture).
+// per device and kept for the process's life, so it is stale after a
+// cudaDeviceReset; the first call must not happen during stream capture).
 unsigned char* scratchForCurrentDevice()
 {
     int dev = 0;

@@ -1,14 +1,17 @@
 """The allocation-free neighbour-list entry point against the batched one.
 
 n2p2_neighbor_list_noalloc serves callers that cannot allocate device memory
-where they need a neighbour list (a step being captured into a CUDA graph,
-memory owned by the caller's pool allocator, loops that must not pay
-cudaMalloc's synchronisation): the caller passes device buffers and the
-library's fixed scratch array does the rest.  Its entries must equal those
-of n2p2_batch_get_neighbors for the same structure -- index, image code,
-distance and distance vector bit for bit (tolerance 0, as for every
-neighbour-list comparison in this suite) -- on two calls in a row, since the
-calls share the scratch array.  This file is collected last on purpose.
+where they need a neighbour list (memory owned by the caller's pool
+allocator, loops that must not pay cudaMalloc's synchronisation): the caller
+passes device buffers and the library's fixed scratch array does the rest.
+Its entries must equal those of n2p2_batch_get_neighbors for the same
+structure -- index, image code, distance and distance vector bit for bit
+(tolerance 0, as for every neighbour-list comparison in this suite) -- on two
+calls in a row, since the calls share the scratch array, for a periodic box
+and for a cluster without one.  Inputs beyond the documented limits fail with
+N2P2_ERR_RUNTIME (the kernels write nothing out of bounds on the way), and a
+valid call right after a rejected one is still exact.  This file is
+collected last on purpose.
 """
 import ctypes
 
@@ -32,11 +35,12 @@ def _noalloc(torch, pos_internal, box_internal, cutoff, capacity):
     img = torch.zeros(capacity, dtype=torch.int32, device=dev)
     d = torch.zeros(capacity, dtype=torch.float64, device=dev)
     dr = torch.zeros(capacity * 3, dtype=torch.float64, device=dev)
-    box = np.ascontiguousarray(box_internal, dtype=np.float64)
+    box = None if box_internal is None else np.ascontiguousarray(box_internal, dtype=np.float64)
     total = ctypes.c_int64()
     stream = torch.cuda.current_stream(dev).cuda_stream
     _lib.check(lib.n2p2_neighbor_list_noalloc(
-        ctypes.c_void_p(pos.data_ptr()), n, box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cutoff, capacity,
+        ctypes.c_void_p(pos.data_ptr()), n, None if box is None else box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+        cutoff, capacity,
         ctypes.c_void_p(off.data_ptr()), ctypes.c_void_p(idx.data_ptr()), ctypes.c_void_p(img.data_ptr()),
         ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(dr.data_ptr()), ctypes.byref(total), ctypes.c_void_p(stream)))
     m = total.value
@@ -60,3 +64,46 @@ def test_noalloc_neighbor_list_matches_batched_path_twice():
         assert np.array_equal(got["image"], ref["image"])
         assert np.array_equal(got["d"].view(np.int64), ref["d"].view(np.int64))
         assert np.array_equal(got["dr"].view(np.int64), ref["dr"].view(np.int64))
+
+
+def _assert_same(got, ref):
+    assert np.array_equal(got["offset"], ref["offset"])
+    assert np.array_equal(got["index"], ref["index"])
+    assert np.array_equal(got["image"], ref["image"])
+    assert np.array_equal(got["d"].view(np.int64), ref["d"].view(np.int64))
+    assert np.array_equal(got["dr"].view(np.int64), ref["dr"].view(np.int64))
+
+
+def test_noalloc_cluster_and_rejections():
+    """A cluster (no box: one cell, no images) bit-identical to the batched
+    path; then each documented rejection, each followed by a valid call."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    from n2p2_b200 import Structure
+    m = H.gpu_mode(H.WATER40)
+    cutoff = m.getMaxCutoffRadius()
+    box_s = water.water_box(48, seed=3)
+    cluster = Structure(box_s.positions, box_s.elements, None)
+    b = H.gpu_batch(m, [cluster])
+    ref = b.neighbors()
+    pos = b.internalPositions()
+    _assert_same(_noalloc(torch, pos, None, cutoff, capacity=len(ref["d"]) + 64), ref)
+
+    # more atoms than the scratch holds: rejected on the host before any launch
+    big = np.zeros((8193, 3))
+    with pytest.raises(_lib.N2P2Error, match="8192"):
+        _noalloc(torch, big, None, cutoff, capacity=16)
+    # output capacity one entry short: the call reports the count it needed
+    with pytest.raises(_lib.N2P2Error, match="capacity too small"):
+        _noalloc(torch, pos, None, cutoff, capacity=len(ref["d"]) - 1)
+    _assert_same(_noalloc(torch, pos, None, cutoff, capacity=len(ref["d"])), ref)
+    # a dense cluster: 300 atoms in a ball of radius 3, every pair within the
+    # cutoff, 299 neighbours per atom > 256
+    rng = np.random.default_rng(0)
+    v = rng.normal(size=(300, 3))
+    dense = 3.0 * v / np.linalg.norm(v, axis=1)[:, None] * rng.random((300, 1)) ** (1.0 / 3.0)
+    with pytest.raises(_lib.N2P2Error, match="256"):
+        _noalloc(torch, dense, None, cutoff, capacity=300 * 300)
+    # and the shared scratch still gives exact lists afterwards
+    _assert_same(_noalloc(torch, pos, None, cutoff, capacity=len(ref["d"]) + 64), ref)
