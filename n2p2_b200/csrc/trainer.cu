@@ -734,10 +734,11 @@ __global__ void __launch_bounds__(1024) kKalmanGainFull(const double* __restrict
                                                         int n, int ld, int m, double diag,
                                                         const double* __restrict__ xi, double* __restrict__ K,
                                                         double* __restrict__ w, double* __restrict__ wT,
-                                                        const int* __restrict__ tidx)
+                                                        const int* __restrict__ tidx, int* __restrict__ singular)
 {
     __shared__ double part[1024];
     __shared__ double A[kMaxObs][2 * kMaxObs];
+    __shared__ int bad;
     for (int a = 0; a < m; ++a)
         for (int c = 0; c < m; ++c)
         {
@@ -758,7 +759,15 @@ __global__ void __launch_bounds__(1024) kKalmanGainFull(const double* __restrict
             __syncthreads();
         }
     if (threadIdx.x == 0)
-        for (int c = 0; c < m; ++c)
+    {
+        // A = H^T P H + diag I is symmetric positive definite while P is; a
+        // pivot that is not finite, or negligible against the largest
+        // diagonal entry (linearly dependent observations with a degenerate
+        // P), makes the inverse meaningless: the update is skipped and counted
+        double scaleA = 0.0;
+        for (int c = 0; c < m; ++c) scaleA = fmax(scaleA, fabs(A[c][c]));
+        bad = !(scaleA > 0.0) || !isfinite(scaleA);
+        for (int c = 0; c < m && !bad; ++c)
         {
             int piv = c;
             for (int r = c + 1; r < m; ++r)
@@ -770,6 +779,11 @@ __global__ void __launch_bounds__(1024) kKalmanGainFull(const double* __restrict
                     A[c][k] = A[piv][k];
                     A[piv][k] = t;
                 }
+            if (!isfinite(A[c][c]) || !(fabs(A[c][c]) > 1e-14 * scaleA))
+            {
+                bad = 1;
+                break;
+            }
             const double d = 1.0 / A[c][c];
             for (int k = 0; k < 2 * m; ++k) A[c][k] *= d;
             for (int r = 0; r < m; ++r)
@@ -779,6 +793,8 @@ __global__ void __launch_bounds__(1024) kKalmanGainFull(const double* __restrict
                     for (int k = 0; k < 2 * m; ++k) A[r][k] -= f * A[c][k];
                 }
         }
+        if (bad) atomicAdd(singular, 1);
+    }
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x)
     {
@@ -786,12 +802,16 @@ __global__ void __launch_bounds__(1024) kKalmanGainFull(const double* __restrict
         for (int c = 0; c < m; ++c)
         {
             double k = 0.0;
-            for (int a = 0; a < m; ++a) k += X[i + (size_t)a * ld] * A[a][m + c];
-            K[i + (size_t)c * ld] = k;
+            if (!bad)
+                for (int a = 0; a < m; ++a) k += X[i + (size_t)a * ld] * A[a][m + c];
+            K[i + (size_t)c * ld] = k;   // a skipped update leaves P's change at zero
             wi += k * xi[2 * c];
         }
-        w[i] = wi;
-        wT[tidx[i]] = wi;
+        if (!bad)
+        {
+            w[i] = wi;
+            wT[tidx[i]] = wi;
+        }
     }
 }
 
@@ -1009,6 +1029,8 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
         Kb_[k] = tAlloc<double>((size_t)P_ * kMaxObs);
     }
     stat_ = tAlloc<double>(3 * kStatBlocks);
+    singular_ = tAlloc<int>(1);
+    cudaCheck(cudaMemsetAsync(singular_, 0, sizeof(int), st), "memset");
     {
         const int T = (P_ + kTile - 1) / kTile;
         rowPart_ = tAlloc<double>((size_t)T * (T + 1) / 2 * kTile);
@@ -1025,7 +1047,8 @@ Training::Training(Model& model, DeviceModel& dmodel, Batch& set, int sms)
 Training::~Training()
 {
     for (void* p : {(void*)eRef_, (void*)fRef_, (void*)u_, (void*)g_, (void*)gradPart_, (void*)predPart_, (void*)H_,
-                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)Xb_[0], (void*)Xb_[1], (void*)Kb_[0], (void*)Kb_[1], (void*)m_, (void*)v_, (void*)stat_, (void*)img_, (void*)rowPart_, (void*)colPart_, (void*)near_})
+                    (void*)xi_, (void*)err_, (void*)Pm_, (void*)Xb_[0], (void*)Xb_[1], (void*)Kb_[0], (void*)Kb_[1], (void*)m_, (void*)v_, (void*)stat_, (void*)singular_, (void*)img_, (void*)rowPart_, (void*)colPart_,
+                    (void*)near_})
         cudaFree(p);
 }
 
@@ -1204,7 +1227,7 @@ void Training::step(int property, int s, int a, int m)
                                                                colPart_, pendingRank_, n);
                 kKalmanXSum<<<(n + 7) / 8, 256, 0, st>>>(rowPart_, colPart_, n, T, Xb_[cur] + (size_t)o * n);
             }
-            kKalmanGainFull<<<1, 1024, 0, st>>>(H_, Xb_[cur], n, n, m, diag, xi_, Kb_[cur], w, wT, tidx);
+            kKalmanGainFull<<<1, 1024, 0, st>>>(H_, Xb_[cur], n, n, m, diag, xi_, Kb_[cur], w, wT, tidx, singular_);
         }
         else
         for (int e = 0; e < ne; ++e)
@@ -1341,7 +1364,18 @@ void Training::update(int property, int count, const int* structure, const int* 
     }
     if (errors)
         cudaCheck(cudaMemcpyAsync(errors, err_, sizeof(double) * count, cudaMemcpyDeviceToHost, st), "D2H");
+    int skipped = 0;
+    if (fullJacobian_ && batch > 1)
+    {
+        cudaCheck(cudaMemcpyAsync(&skipped, singular_, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+        cudaCheck(cudaMemsetAsync(singular_, 0, sizeof(int), st), "memset");
+    }
     cudaCheck(cudaStreamSynchronize(st), "sync");
+    if (skipped > 0)
+        throw std::runtime_error("ERROR: " + std::to_string(skipped) +
+                                 " update(s) skipped: the m x m matrix of the full Jacobian was singular "
+                                 "(linearly dependent observations in one task batch); their weights are "
+                                 "unchanged.\n");
 }
 
 int Training::updateThreshold(int property, int numUpdates, int numCandidates, const int* structure, const int* atom,

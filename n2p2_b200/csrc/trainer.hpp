@@ -202,6 +202,7 @@ private:
     double* m_ = nullptr;        // Adam moments
     double* v_ = nullptr;
     double* stat_ = nullptr;     // status partial sums
+    int* singular_ = nullptr;    // full-Jacobian updates skipped for a singular m x m matrix
     double* img_ = nullptr;      // [gStride] self-image part of the observed atom's adjoint
     double* rowPart_ = nullptr;  // [tiles][64] row partial sums of X = P H
     double* colPart_ = nullptr;  // [tiles][64] column partial sums (the upper half's share)

@@ -292,3 +292,54 @@ def test_full_jacobian_matches_oracle(data, updater):
         tr.close()
         m.close()
 
+
+
+def test_full_jacobian_alternating_ranks_and_limits(data):
+    """A rank-m update followed by rank-one updates and a status read (the
+    pending rank-m change of P is applied by the next rank-one pass and by
+    the flush), the largest task batch (m = 16, with repeated candidates:
+    H^T P H is then rank-deficient, A = H^T P H + I/eta stays positive
+    definite), and the rejection of m = 17 -- all against the oracle to the
+    bounds of test_full_jacobian_matches_oracle."""
+    m, tr, ref = _pair(data, UPDATERS[0])
+    try:
+        tr.setJacobianMode(2)
+        tr.setTaskBatchSize(energy=2, force=2)
+        e = list(tr.update(ENERGY, [1, 3]))
+        e_ref = list(ref.update_full(0, [(1, 0, 0), (3, 0, 0)]))
+        # back to one observation per update: reads P with the rank-2 change pending
+        tr.setJacobianMode(1)
+        tr.setTaskBatchSize(energy=1, force=1)
+        e += list(tr.update(ENERGY, [0]))
+        e_ref += [ref.update(0, 0)]
+        f = list(tr.update(FORCE, [2], [7], [1]))
+        f_ref = [ref.update(1, 2, 7, 1)]
+        tr.setJacobianMode(2)
+        tr.setTaskBatchSize(energy=3, force=2)
+        f += list(tr.update(FORCE, [0, 3], [5, 11], [2, 0]))
+        f_ref += list(ref.update_full(1, [(0, 5, 2), (3, 11, 0)]))
+        st = tr.kalmanStatus()   # flushes the pending rank-2 change
+        assert abs(st["Pdiag"] - np.mean(np.abs(np.diag(ref.updater.P)))) <= 1e-9 * st["Pdiag"]
+        tr.setJacobianMode(1)
+        tr.setTaskBatchSize(energy=1, force=1)
+        e += list(tr.update(ENERGY, [2]))
+        e_ref += [ref.update(0, 2)]
+        # the largest task batch: 16 candidates (structures repeated)
+        tr.setJacobianMode(2)
+        tr.setTaskBatchSize(energy=16, force=1)
+        seq = [k % 4 for k in range(16)]
+        e += list(tr.update(ENERGY, seq))
+        e_ref += list(ref.update_full(0, [(k, 0, 0) for k in seq]))
+        e, e_ref, f, f_ref = (np.array(x) for x in (e, e_ref, f, f_ref))
+        assert np.allclose(e, e_ref, rtol=1e-9, atol=1e-9 * np.abs(e_ref).max())
+        assert np.allclose(f, f_ref, rtol=1e-9, atol=1e-9 * np.abs(f_ref).max())
+        assert H.max_rel(tr.weights(), ref.nets.weights) <= 1e-9
+        # 17 candidates per update are more than the full Jacobian takes
+        w = tr.weights()
+        with pytest.raises(Exception, match="16"):
+            tr.setTaskBatchSize(energy=17, force=1)
+            tr.update(ENERGY, [k % 4 for k in range(17)])
+        assert np.array_equal(tr.weights(), w)
+    finally:
+        tr.close()
+        m.close()
