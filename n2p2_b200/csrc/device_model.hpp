@@ -97,6 +97,7 @@ struct DevCutoff
     int    pad_;
     double rc, rcinv, rci, iw, alpha;
     double tanhPre;        // CutoffFunction::TANH_PRE (CutoffFunction.cpp:28)
+    float  rcF, rciF, iwF, pad2_;   // FP32 copies for the mixed form's per-triplet f_c(r_jk)
 };
 
 // Per symmetry function scaling (SymFnc::scale / unscale, SymFnc.cpp:169-223).

@@ -506,6 +506,9 @@ void DeviceModel::upload(Model const& m)
         c.rci = c.rc * c.alpha;
         c.iw = 1.0 / (c.rc - c.rci);
         c.tanhPre = std::pow((E + 1 / E) / (E - 1 / E), 3);
+        c.rcF = (float)c.rc;
+        c.rciF = (float)c.rci;
+        c.iwF = (float)c.iw;
     }
     // transposed copy of every weight matrix (same offsets; biases copied):
     // element (k, j) of W_l [n_l x n_{l-1}] at j n_l + k, for reads that are

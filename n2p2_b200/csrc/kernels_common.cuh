@@ -154,6 +154,62 @@ __device__ __forceinline__ void cutoffFdf(DevCutoff const& c, double r, double& 
     }
 }
 
+// The cutoff function in FP32 (the mixed form's per-triplet f_c(r_jk); the
+// per-pair f_c(r_ij) values come from cutoffFdf in FP64).  The polynomial
+// cores (types 5-8, poly1..poly4) are 1 - S_n(x) for the smoothstep
+// polynomials S_n, which factor as
+//   1 - S_n(x) = u^(n+1) sum_{k=0..n} C(n+k, k) x^k,   u = 1 - x,
+//   d/dx      = -(2n+1)!/(n!)^2 x^n u^n,
+// (poly2: u^3 (1 + 3x + 6x^2) = ((15 - 6x)x - 10)x^3 + 1 and -30 x^2 u^2).
+// With u = (r_c - r) iw computed directly there is no cancellation as
+// r -> r_c, so FP32 keeps the relative accuracy near the cutoff that the
+// expanded form only has in FP64.  Types without such a form (cos, tanh,
+// exp) use cutoffFdf.
+__device__ __forceinline__ void cutoffFdfF32(DevCutoff const& c, float r, float& fc, float& dfc)
+{
+    if (c.type >= 5 && c.type <= 8)
+    {
+        if (r >= c.rcF)
+        {
+            fc = 0.0f;
+            dfc = 0.0f;
+            return;
+        }
+        if (r < c.rciF)
+        {
+            fc = 1.0f;
+            dfc = 0.0f;
+            return;
+        }
+        const float x = (r - c.rciF) * c.iwF, u = (c.rcF - r) * c.iwF;
+        const float xu = x * u, u2 = u * u;
+        float p, d;
+        switch (c.type)
+        {
+        case 5: p = u2 * (1.0f + 2.0f * x); d = -6.0f * xu; break;
+        case 6: p = u2 * u * ((6.0f * x + 3.0f) * x + 1.0f); d = -30.0f * xu * xu; break;
+        case 7: p = u2 * u2 * (((20.0f * x + 10.0f) * x + 4.0f) * x + 1.0f); d = -140.0f * xu * xu * xu; break;
+        default:
+            p = u2 * u2 * u * ((((70.0f * x + 35.0f) * x + 15.0f) * x + 5.0f) * x + 1.0f);
+            d = -630.0f * (xu * xu) * (xu * xu);
+            break;
+        }
+        fc = p;
+        dfc = d * c.iwF;
+        return;
+    }
+    if (c.type == 0)
+    {
+        fc = r < c.rcF ? 1.0f : 0.0f;
+        dfc = 0.0f;
+        return;
+    }
+    double f, df;
+    cutoffFdf(c, (double)r, f, df);
+    fc = (float)f;
+    dfc = (float)df;
+}
+
 // SymFnc::scale (SymFnc.cpp:169-195)
 __device__ __forceinline__ double scaleG(DevScaling const& s, double v)
 {

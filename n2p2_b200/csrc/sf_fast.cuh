@@ -57,8 +57,11 @@ __device__ __forceinline__ double fpow<double>(double b, double e) { return pow(
 template <>
 __device__ __forceinline__ float fpow<float>(float b, float e) { return __powf(b, e); }
 
+// 16-byte aligned: stageGeometry reuses the first arrays as FP64 scratch in
+// the FP32 form, and every warp's block of the dynamic shared memory starts
+// at a multiple of the struct's size.
 template <typename T, int CAP, bool DF, int NB>
-struct Stage
+struct alignas(16) Stage
 {
     T x[CAP], y[CAP], z[CAP], r[CAP], rinv[CAP], fc[CAP];
     T dfcr[DF ? CAP : 1];                  // (df_c/dr)/r, force pass only
@@ -93,12 +96,15 @@ struct ValuesSmem
     int queue[kQueue];
 };
 
+// h: per staged neighbour, the force the centre's energy puts on it, summed
+// over the atom's triplets in the pass's precision (FP32 in the mixed form,
+// whose final per-atom accumulation, kGatherForces, is FP64).
 template <typename T, int CAP, int FAST>
 struct ForcesSmem
 {
     Stage<T, CAP, true, FAST ? 1 : kMaxStagedBases> st;
     Members<T, FAST != 0> mb;
-    double h[3][CAP];
+    T h[3][CAP];
     int queue[kQueue];
 };
 
@@ -479,16 +485,15 @@ __device__ __forceinline__ void tripletGeometry(Stage<T, CAP, DF, NB> const& S, 
     t.dfcjk = T(0);
 }
 
-// r_jk and its cutoff (narrow groups).
+// r_jk and its cutoff (narrow groups): FP64 in the FP64 form; in the FP32
+// form the cancellation-free factored polynomials (cutoffFdfF32).
 template <typename T>
 __device__ __forceinline__ void tripletJK(DevCutoff const& cut, Triplet<T>& t)
 {
     t.rijk = frsqrt<T>(t.rjk2);
     t.rjk = t.rjk2 * t.rijk;
-    double f, df;
-    cutoffFdf(cut, (double)t.rjk, f, df);   // FP64 near r_c in both forms
-    t.fcjk = (T)f;
-    t.dfcjk = (T)df;
+    if constexpr (sizeof(T) == 4) cutoffFdfF32(cut, t.rjk, t.fcjk, t.dfcjk);
+    else cutoffFdf(cut, t.rjk, t.fcjk, t.dfcjk);
 }
 
 template <typename T, int CAP, bool DF, int NB>
@@ -986,7 +991,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
 template <typename T, int CAP, int FAST, int ILP>
 __device__ __forceinline__ void forcesStepN(Stage<T, CAP, true, 1> const& S, Members<T, true> const& mb, DevGroup const& G,
                                             DevCutoff const& cut, bool narrow, const int* queue, int qh, int take,
-                                            int lane, double (&h)[3][CAP], double& sfx, double& sfy, double& sfz)
+                                            int lane, T (&h)[3][CAP], T& sfx, T& sfy, T& sfz)
 {
     Triplet<T> t[ILP];
     int so[ILP], sp[ILP];
@@ -1001,7 +1006,7 @@ __device__ __forceinline__ void forcesStepN(Stage<T, CAP, true, 1> const& S, Mem
     }
     T T1[ILP], T2[ILP], T3[ILP];
     gridForcesN<T, FAST, true, ILP>(bv, G, mb, cost, T1, T2, T3);
-    double o[ILP][3], q[ILP][3];
+    T o[ILP][3], q[ILP][3];
 #pragma unroll
     for (int u = 0; u < ILP; ++u)
     {
@@ -1014,17 +1019,17 @@ __device__ __forceinline__ void forcesStepN(Stage<T, CAP, true, 1> const& S, Mem
         const T P1 = pfc * ((x.rinv - x.cost * x.ri1 * x.ri1) * T1[u] - T2[u]) + pr1 * T3[u];
         const T P2 = pfc * ((x.rinv - x.cost * x.ri2 * x.ri2) * T1[u] - T2[u]) + pr2 * T3[u];
         const T P3 = narrow ? (pfc * (x.rinv * T1[u] + T2[u]) - pr3 * T3[u]) : (pfc * x.rinv * T1[u]);
-        o[u][0] = (double)(P1 * x.x1 + P3 * x.dx3);
-        o[u][1] = (double)(P1 * x.y1 + P3 * x.dy3);
-        o[u][2] = (double)(P1 * x.z1 + P3 * x.dz3);
-        q[u][0] = (double)(P2 * x.x2 - P3 * x.dx3);
-        q[u][1] = (double)(P2 * x.y2 - P3 * x.dy3);
-        q[u][2] = (double)(P2 * x.z2 - P3 * x.dz3);
+        o[u][0] = P1 * x.x1 + P3 * x.dx3;
+        o[u][1] = P1 * x.y1 + P3 * x.dy3;
+        o[u][2] = P1 * x.z1 + P3 * x.dz3;
+        q[u][0] = P2 * x.x2 - P3 * x.dx3;
+        q[u][1] = P2 * x.y2 - P3 * x.dy3;
+        q[u][2] = P2 * x.z2 - P3 * x.dz3;
         if (ok[u])
         {
-            sfx -= (double)(P1 * x.x1 + P2 * x.x2);
-            sfy -= (double)(P1 * x.y1 + P2 * x.y2);
-            sfz -= (double)(P1 * x.z1 + P2 * x.z2);
+            sfx -= P1 * x.x1 + P2 * x.x2;
+            sfy -= P1 * x.y1 + P2 * x.y2;
+            sfz -= P1 * x.z1 + P2 * x.z2;
         }
     }
 #pragma unroll
@@ -1080,11 +1085,21 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
             (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
         int mwi = 0;
         stageGeometry<T, CAP>(S, off, n, model, b, lane);
-        for (int s = lane; s < n; s += 32) SM.h[0][s] = SM.h[1][s] = SM.h[2][s] = 0.0;
+        for (int s = lane; s < n; s += 32) SM.h[0][s] = SM.h[1][s] = SM.h[2][s] = T(0);
+        // self force: the FP64 form sums every term into gs*; the FP32 form
+        // sums a group's terms in FP32 and adds each group's total to sf* in FP64
         double sfx = 0.0, sfy = 0.0, sfz = 0.0;
+        T gsx = T(0), gsy = T(0), gsz = T(0);
         int slot = -1;
         for (int g = 0; g < E.groupCount; ++g)
         {
+            if constexpr (sizeof(T) == 4)
+            {
+                sfx += (double)gsx;
+                sfy += (double)gsy;
+                sfz += (double)gsz;
+                gsx = gsy = gsz = T(0);
+            }
             DevGroup const G = model.groups[E.groupBegin + g];
             const bool fastG = FAST || G.fast;
             if (G.cutoffSlot != slot)
@@ -1122,14 +1137,13 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                         else v = gaussShifted<T>(mb.eta[q], mb.rs[q], r, mb.rs[q], mb.rs[q], 0);
                         P += mb.cw[q] * (dfc - T(2) * mb.eta[q] * (r - mb.rs[q]) * fc) * v * ri;
                     }
-                    const double Pd = (double)P;
-                    const double ddx = (double)S.x[s] * Pd, ddy = (double)S.y[s] * Pd, ddz = (double)S.z[s] * Pd;
+                    const T ddx = S.x[s] * P, ddy = S.y[s] * P, ddz = S.z[s] * P;
                     SM.h[0][s] += ddx;
                     SM.h[1][s] += ddy;
                     SM.h[2][s] += ddz;
-                    sfx -= ddx;
-                    sfy -= ddy;
-                    sfz -= ddz;
+                    gsx -= ddx;
+                    gsy -= ddy;
+                    gsz -= ddz;
                 }
                 __syncwarp();
                 continue;
@@ -1167,7 +1181,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                         {
                             const int take = min(kStep, qn);
                             forcesStepN<T, CAP, FAST, ILP>(S, mb, G, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh,
-                                                          take, lane, SM.h, sfx, sfy, sfz);
+                                                          take, lane, SM.h, gsx, gsy, gsz);
                             qh = (qh + take) & (kQueue - 1);
                             qn -= take;
                             __syncwarp();
@@ -1179,7 +1193,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                     {
                         const int take = min(32, qn);
                         int keyO = 0, keyP = 0;
-                        double ox = 0.0, oy = 0.0, oz = 0.0, px = 0.0, py = 0.0, pz = 0.0;
+                        T ox = T(0), oy = T(0), oz = T(0), px = T(0), py = T(0), pz = T(0);
                         if (lane < take)
                         {
                             const int e = SM.queue[(qh + lane) & (kQueue - 1)];
@@ -1239,15 +1253,15 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                             const T P1 = pfc * ((t.rinv - t.cost * t.ri1 * t.ri1) * T1 - Uij) + pr1 * T3;
                             const T P2 = pfc * ((t.rinv - t.cost * t.ri2 * t.ri2) * T1 - Uik) + pr2 * T3;
                             const T P3 = narrow ? (pfc * (t.rinv * T1 + Ujk) - pr3 * T3) : (pfc * t.rinv * T1);
-                            ox = (double)(P1 * t.x1 + P3 * t.dx3);
-                            oy = (double)(P1 * t.y1 + P3 * t.dy3);
-                            oz = (double)(P1 * t.z1 + P3 * t.dz3);
-                            px = (double)(P2 * t.x2 - P3 * t.dx3);
-                            py = (double)(P2 * t.y2 - P3 * t.dy3);
-                            pz = (double)(P2 * t.z2 - P3 * t.dz3);
-                            sfx -= (double)(P1 * t.x1 + P2 * t.x2);
-                            sfy -= (double)(P1 * t.y1 + P2 * t.y2);
-                            sfz -= (double)(P1 * t.z1 + P2 * t.z2);
+                            ox = P1 * t.x1 + P3 * t.dx3;
+                            oy = P1 * t.y1 + P3 * t.dy3;
+                            oz = P1 * t.z1 + P3 * t.dz3;
+                            px = P2 * t.x2 - P3 * t.dx3;
+                            py = P2 * t.y2 - P3 * t.dy3;
+                            pz = P2 * t.z2 - P3 * t.dz3;
+                            gsx -= P1 * t.x1 + P2 * t.x2;
+                            gsy -= P1 * t.y1 + P2 * t.y2;
+                            gsz -= P1 * t.z1 + P2 * t.z2;
                         }
                         // One conflict-free add per round present in the batch: inside a
                         // round no slot occurs twice.
@@ -1281,9 +1295,21 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
         for (int s = lane; s < n; s += 32)
         {
             const int64_t e = off + S.perm[s];
-            b.hx[e] = SM.h[0][s];
-            b.hy[e] = SM.h[1][s];
-            b.hz[e] = SM.h[2][s];
+            b.hx[e] = (double)SM.h[0][s];
+            b.hy[e] = (double)SM.h[1][s];
+            b.hz[e] = (double)SM.h[2][s];
+        }
+        if constexpr (sizeof(T) == 4)
+        {
+            sfx += (double)gsx;
+            sfy += (double)gsy;
+            sfz += (double)gsz;
+        }
+        else
+        {
+            sfx = gsx;
+            sfy = gsy;
+            sfz = gsz;
         }
         sfx = warpSum(sfx);
         sfy = warpSum(sfy);

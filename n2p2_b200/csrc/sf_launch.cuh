@@ -23,6 +23,7 @@ int gridFor(int N, int warpsPerBlock, int sms, int perSM)
 template <typename T, int CAP, int WARPS, int FAST>
 void valuesTier(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int lower, int flag, int perSM)
 {
+    static_assert(sizeof(ValuesSmem<T, CAP, FAST>) % 16 == 0, "per-warp blocks must stay 16-byte aligned");
     const size_t smem = sizeof(ValuesSmem<T, CAP, FAST>) * WARPS;
     auto k = kSFValuesF<T, CAP, WARPS, FAST>;
     setDynamicSmemOnce(reinterpret_cast<const void*>(k), smem);
@@ -32,6 +33,7 @@ void valuesTier(DevModel const& m, BatchView const& b, int sms, cudaStream_t st,
 template <typename T, int CAP, int WARPS, int FAST>
 void forcesTier(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int lower, int perSM)
 {
+    static_assert(sizeof(ForcesSmem<T, CAP, FAST>) % 16 == 0, "per-warp blocks must stay 16-byte aligned");
     const size_t smem = sizeof(ForcesSmem<T, CAP, FAST>) * WARPS;
     auto k = kSFForcesF<T, CAP, WARPS, FAST>;
     setDynamicSmemOnce(reinterpret_cast<const void*>(k), smem);
