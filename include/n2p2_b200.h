@@ -526,6 +526,16 @@ n2p2_status n2p2_batch_count_work(n2p2_batch* batch, int64_t* counts);
  * compute roofline of the FP64 and FP32 symmetry-function kernels. */
 n2p2_status n2p2_device_fma_peak(int device, double* fp64Tflops, double* fp32Tflops);
 
+/* CutoffFunction::fdf (CutoffFunction.h:210-220; setCutoffRadius and
+ * setCutoffParameter, CutoffFunction.cpp:95-112) of cutoff type 0..8 (hard,
+ * cos, tanhU, tanh, exp, poly1..poly4; the settings file's cutoff_type) at n
+ * radii, evaluated on the device as the symmetry-function kernels evaluate
+ * it: N2P2_PRECISION_FP64 is the every-pair form, N2P2_PRECISION_MIXED the
+ * FP32 form of the mixed kernels' per-triplet f_c(r_jk).  A diagnostic;
+ * 0 <= alpha < 1 as in the reference (N2P2_ERR_INVALID_ARGUMENT otherwise). */
+n2p2_status n2p2_cutoff_function(int device, int type, double rc, double alpha, int precision, const double* r,
+                                  int64_t n, double* f, double* df);
+
 /* Pinned (page-locked) host memory for fast transfers. */
 n2p2_status n2p2_host_alloc(void** ptr, size_t bytes);
 n2p2_status n2p2_host_free(void* ptr);

@@ -92,6 +92,7 @@ SIGNATURES = {
     "n2p2_batch_profile_stages": (_i, [_vp, _i, _i, _cp, _P(_d), _P(_i)]),
     "n2p2_batch_count_work": (_i, [_vp, _P(_i64)]),
     "n2p2_device_fma_peak": (_i, [_i, _P(_d), _P(_d)]),
+    "n2p2_cutoff_function": (_i, [_i, _i, _d, _d, _i, _P(_d), _i64, _P(_d), _P(_d)]),
     "n2p2_mode_set_autotune": (_i, [_vp, ctypes.c_int32]),
     "n2p2_batch_autotune": (_i, [_vp, ctypes.c_int32, _P(ctypes.c_int32), _P(_d), _P(ctypes.c_int32)]),
     "n2p2_batch_set_shapes": (_i, [_vp, ctypes.c_int32, ctypes.c_int32]),

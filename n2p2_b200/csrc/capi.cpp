@@ -722,6 +722,18 @@ n2p2_status n2p2_device_fma_peak(int device, double* fp64Tflops, double* fp32Tfl
     });
 }
 
+n2p2_status n2p2_cutoff_function(int device, int type, double rc, double alpha, int precision, const double* r,
+                                  int64_t n, double* f, double* df)
+{
+    N2P2_REQUIRE(r);
+    N2P2_REQUIRE(f);
+    N2P2_REQUIRE(df);
+    return guard([&] {
+        cudaCheck(cudaSetDevice(device), "cudaSetDevice");
+        cutoffFunctionValues(type, rc, alpha, precision == N2P2_PRECISION_MIXED ? 1 : 0, r, n, f, df);
+    });
+}
+
 n2p2_status n2p2_mode_set_autotune(n2p2_mode* mode, int32_t enabled)
 {
     N2P2_REQUIRE(mode);

@@ -1,6 +1,9 @@
 // Instrumentation kernels (not on the evaluation path): algorithmic work
 // counters of a batch and FP64/FP32 fused-multiply-add throughput probes used
 // as the compute roofline of the symmetry-function kernels.
+#include <cmath>
+#include <stdexcept>
+
 #include "kernels_common.cuh"
 #include "kernels.hpp"
 
@@ -130,6 +133,54 @@ double measureFmaPeak(int fp64, int sms)
     cudaFree(out);
     const double flops = 2.0 * 8.0 * iters * (double)blocks * 256.0;
     return flops / (best * 1e-3) / 1e12;
+}
+
+// CutoffFunction::fdf (CutoffFunction.h:210-220) on the device, as the
+// symmetry-function kernels evaluate it: FP64 (cutoffFdf, every pair's f_c)
+// or the FP32 form of the mixed kernels' per-triplet f_c(r_jk) (cutoffFdfF32).
+__global__ void kCutoffValues(DevCutoff c, int fp32, const double* __restrict__ r, int64_t n, double* __restrict__ f,
+                              double* __restrict__ df)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    {
+        if (fp32)
+        {
+            float a, b;
+            cutoffFdfF32(c, (float)r[k], a, b);
+            f[k] = a;
+            df[k] = b;
+        }
+        else cutoffFdf(c, r[k], f[k], df[k]);
+    }
+}
+
+void cutoffFunctionValues(int type, double rc, double alpha, int fp32, const double* r, int64_t n, double* f,
+                          double* df)
+{
+    if (type < 0 || type > 8) throw std::invalid_argument("ERROR: unknown cutoff type.\n");
+    if (alpha < 0.0 || alpha >= 1.0) throw std::invalid_argument("ERROR: 0 <= alpha < 1.0 is required.\n");
+    if (n <= 0) return;
+    DevCutoff c{};
+    const double E = std::exp(1.0);
+    c.type = type;
+    c.rc = rc;
+    c.rcinv = 1.0 / rc;
+    c.alpha = alpha;
+    c.rci = rc * alpha;
+    c.iw = 1.0 / (c.rc - c.rci);
+    c.tanhPre = std::pow((E + 1 / E) / (E - 1 / E), 3);
+    c.rcF = (float)c.rc;
+    c.rciF = (float)c.rci;
+    c.iwF = (float)c.iw;
+    double* d = nullptr;
+    cudaCheck(cudaMalloc(&d, sizeof(double) * 3 * (size_t)n), "cudaMalloc");
+    cudaCheck(cudaMemcpy(d, r, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice), "H2D");
+    kCutoffValues<<<(int)std::min<int64_t>((n + 255) / 256, 1024), 256>>>(c, fp32, d, n, d + n, d + 2 * n);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(f, d + n, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(df, d + 2 * n, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    cudaCheck(e, "cutoff values");
 }
 
 } // namespace n2p2b200

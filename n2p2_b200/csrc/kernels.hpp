@@ -170,5 +170,9 @@ void neighborListNoAlloc(const double* positions, int64_t numAtoms, const double
 // instrumentation
 void launchCountWork(DevModel const& m, BatchView const& b, unsigned long long* counts, int sms, cudaStream_t st);
 double measureFmaPeak(int fp64, int sms);
+// CutoffFunction::fdf of type 0..8 at n radii on the current device (FP64, or
+// the FP32 per-triplet form of the mixed kernels with fp32 != 0).
+void cutoffFunctionValues(int type, double rc, double alpha, int fp32, const double* r, int64_t n, double* f,
+                          double* df);
 
 } // namespace n2p2b200

@@ -55,6 +55,10 @@ def _lib(fast=False):
         f = getattr(lib, "nnpref_" + n)
         f.restype = i64
         f.argtypes = [vp, ctypes.POINTER(i64), i64]
+    lib.nnpref_jacobian.restype = i64
+    lib.nnpref_jacobian.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, i64, ctypes.c_int, ctypes.POINTER(dbl), i64]
+    lib.nnpref_loss_gradient.restype = i64
+    lib.nnpref_loss_gradient.argtypes = [vp, ctypes.c_char_p, dbl, ctypes.POINTER(dbl), ctypes.POINTER(dbl), i64]
     lib.nnpref_time_sf_batch.restype = dbl
     lib.nnpref_time_sf_batch.argtypes = [ctypes.c_char_p, i64, ctypes.POINTER(ctypes.c_char_p), i64]
     lib.nnpref_time_batch.restype = dbl
@@ -108,6 +112,32 @@ class RefPrediction:
         if n:
             ct = ctypes.c_double if dtype == np.float64 else ctypes.c_int64
             f(self._h, out.ctypes.data_as(ctypes.POINTER(ct)), n)
+        return out
+
+    def jacobian(self, text, prop, atom=0, comp=0):
+        """Jacobian of a training observation (0: energy, 1: force component)
+        from the reference's NeuralNetwork::calculateDEdc / calculateDFdc, all
+        elements' weights in file order (internal units)."""
+        n = self._lib.nnpref_jacobian(self._h, text.encode(), int(prop), int(atom), int(comp), None, 0)
+        if n < 0:
+            raise RuntimeError("reference jacobian failed: " + self._lib.nnpref_last_error().decode())
+        out = np.zeros(n)
+        self._lib.nnpref_jacobian(self._h, text.encode(), int(prop), int(atom), int(comp),
+                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n)
+        return out
+
+    def loss_gradient(self, text, a_energy, u_forces):
+        """sum aE dE/dw + sum_k u_k dF_k/dw through one structure (the
+        reference's calculateDEdc / calculateDFdc), internal units."""
+        u = np.ascontiguousarray(u_forces, dtype=np.float64).ravel()
+        n = self._lib.nnpref_loss_gradient(self._h, text.encode(), float(a_energy),
+                                           u.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), None, 0)
+        if n < 0:
+            raise RuntimeError("reference gradient failed: " + self._lib.nnpref_last_error().decode())
+        out = np.zeros(n)
+        self._lib.nnpref_loss_gradient(self._h, text.encode(), float(a_energy),
+                                       u.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n)
         return out
 
     @property

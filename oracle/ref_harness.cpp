@@ -14,6 +14,7 @@
 #include "Structure.h"
 #include "Atom.h"
 #include "Element.h"
+#include "NeuralNetwork.h"
 #include "utility.h"
 
 #include <atomic>
@@ -85,6 +86,53 @@ public:
     {
         s.calculateNeighborList(maxCutoffRadius, false);
         calculateSymmetryFunctionGroups(s, false);
+    }
+    // Jacobian of one training observation with respect to every network
+    // weight (elements in index order, each in its weight-file order), as
+    // Training::update assembles it for 2G networks (Training.cpp:2582-2690)
+    // from the reference's own NeuralNetwork::calculateDEdc (an energy: the
+    // sum over the structure's atoms) and NeuralNetwork::calculateDFdc (force
+    // component c of atom a: the sum over atoms of calculateDFdc with the
+    // atom's dG/dx_{a,c}).  dG/dx_{a,c} is gathered as
+    // Training::collectDGdxia does (Training.cpp:3590-3631, restated because
+    // the training library is not built: the rows of the atom's neighbour
+    // entries that name atom a, mapped through the element's symmetry
+    // function table, plus the atom's own dG/dr when it is atom a).  Needs a
+    // structure evaluated with forces (dG/dr stored).
+    void jacobian(Structure& s, int property, size_t a, size_t c, vector<double>& out)
+    {
+        vector<size_t> offset(numElements + 1, 0);
+        for (size_t e = 0; e < numElements; ++e)
+            offset[e + 1] = offset[e] + (size_t)elements.at(e).neuralNetworks.at("short").getNumConnections();
+        out.assign(offset[numElements], 0.0);
+        vector<double> d;
+        for (Atom& at : s.atoms)
+        {
+            NeuralNetwork& nn = elements.at(at.element).neuralNetworks.at("short");
+            d.assign((size_t)nn.getNumConnections(), 0.0);
+            for (size_t j = 0; j < at.G.size(); ++j) nn.setInput(j, at.G.at(j));
+            nn.propagate();
+            if (property == 0) nn.calculateDEdc(d.data());
+            else
+            {
+                vector<double> dGdxia(at.numSymmetryFunctions, 0.0);
+                vector<vector<size_t>> const& tableFull = elements.at(at.element).getSymmetryFunctionTable();
+                for (size_t n = 0; n < at.numNeighbors; ++n)
+                {
+                    Atom::Neighbor const& nb = at.neighbors[n];
+                    if (nb.index != a) continue;
+                    vector<size_t> const& table = tableFull.at(nb.element);
+                    for (size_t q = 0; q < nb.dGdr.size(); ++q) dGdxia[table.at(q)] += nb.dGdr[q][c];
+                }
+                if (at.index == a)
+                    for (size_t q = 0; q < at.numSymmetryFunctions; ++q) dGdxia[q] += at.dGdr[q][c];
+                bool any = false;
+                for (double x : dGdxia) any = any || x != 0.0;
+                if (!any) continue;   // an atom without atom a among its neighbours adds exact zeros
+                nn.calculateDFdc(d.data(), dGdxia.data());
+            }
+            for (size_t q = 0; q < d.size(); ++q) out[offset[at.element] + q] += d[q];
+        }
     }
 };
 
@@ -218,6 +266,62 @@ int nnpref_predict(void* p, const char* text, int useForces)
     {
         g_err = e.what();
         return 1;
+    }
+}
+
+// Jacobian of a training observation (property 0: the structure's energy,
+// 1: force component `component` of atom `atom`) at the model's weights, in
+// internal units; returns its length (copies when out != NULL and cap
+// suffices), -1 on failure.
+int64_t nnpref_jacobian(void* p, const char* text, int property, int64_t atom, int component, double* out,
+                        int64_t cap)
+{
+    Handle& h = *static_cast<Handle*>(p);
+    try
+    {
+        Structure s;
+        h.mode.readStructure(s, text);
+        h.mode.evaluateNNP(s, true);
+        vector<double> jac;
+        h.mode.jacobian(s, property, (size_t)atom, (size_t)component, jac);
+        return copyOut(jac, out, cap);
+    }
+    catch (std::exception const& e)
+    {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// Gradient of a loss through one structure, sum_E aE dE/dw + sum_k u[k] dF_k/dw
+// (k = 3 atom + component, F_k the force components), from the same
+// reference Jacobians, the structure evaluated once; internal units.  Returns
+// the weight count (copies when out != NULL and cap suffices), -1 on failure.
+int64_t nnpref_loss_gradient(void* p, const char* text, double aE, const double* u, double* out, int64_t cap)
+{
+    Handle& h = *static_cast<Handle*>(p);
+    try
+    {
+        Structure s;
+        h.mode.readStructure(s, text);
+        h.mode.evaluateNNP(s, true);
+        vector<double> g, jac;
+        h.mode.jacobian(s, 0, 0, 0, g);
+        for (double& x : g) x *= aE;
+        for (size_t a = 0; a < s.atoms.size(); ++a)
+            for (size_t c = 0; c < 3; ++c)
+            {
+                const double w = u[3 * a + c];
+                if (w == 0.0) continue;
+                h.mode.jacobian(s, 1, a, c, jac);
+                for (size_t q = 0; q < g.size(); ++q) g[q] += w * jac[q];
+            }
+        return copyOut(g, out, cap);
+    }
+    catch (std::exception const& e)
+    {
+        g_err = e.what();
+        return -1;
     }
 }
 

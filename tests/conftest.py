@@ -29,9 +29,10 @@ def _oracle_built():
     targets = []
     if not os.path.exists(os.path.join(out, "libnnpport.so")):
         targets.append("port")
-    if not os.path.exists(os.path.join(out, "libnnpref.so")) and os.path.isdir("/root/reference/src/libnnp"):
+    ref = os.environ.get("N2P2_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+    if not os.path.exists(os.path.join(out, "libnnpref.so")) and os.path.isdir(os.path.join(ref, "src", "libnnp")):
         targets.append("ref")
     if targets:
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", *targets], check=False,
-                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "N2P2_REFERENCE=" + ref, *targets],
+                       check=False, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     yield

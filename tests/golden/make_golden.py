@@ -2,7 +2,10 @@
 
 Run in the development container, where the reference tree is mounted:
 
-    python tests/golden/make_golden.py [--reference /root/reference] [--examples-only]
+    python tests/golden/make_golden.py [--reference DIR] [--examples-only]
+
+DIR is the reference checkout ($N2P2_REFERENCE, else a directory named
+"reference" beside this repository).
 
 It writes
   examples/<name>/        the model and structure files of the reference's
@@ -240,7 +243,9 @@ def compact_models(refdir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("N2P2_REFERENCE") or
+                    os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                                 "reference"))
     ap.add_argument("--examples-only", action="store_true", help="copy the reference examples and their goldens only")
     ap.add_argument("--compact-only", action="store_true", help="write the derived compact-function models only")
     args = ap.parse_args()

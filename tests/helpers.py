@@ -25,6 +25,26 @@ def reference_snapshot(model_dir, structure, use_forces=True):
         p.close()
 
 
+def reference_energies_forces(model_dir, structures, threads=None):
+    """Energies and forces (physical units) of the reference library's
+    Prediction on every structure, structures spread over host threads (one
+    reference Mode per thread; the library calls release the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    import threading
+    threads = threads or max(1, min(16, len(os.sched_getaffinity(0))))
+    local = threading.local()
+
+    def one(s):
+        if not hasattr(local, "p"):
+            local.p = oref.RefPrediction(model_dir)
+        local.p.predict(s.to_text())
+        return local.p.energy, local.p._get("forces", np.float64).reshape(-1, 3)
+
+    with ThreadPoolExecutor(threads) as ex:
+        out = list(ex.map(one, structures))
+    return np.array([e for e, _ in out]), [f for _, f in out]
+
+
 def gpu_mode(model_dir, precision="fp64"):
     from n2p2_b200 import Mode
     m = Mode(0)

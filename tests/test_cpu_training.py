@@ -53,6 +53,31 @@ def test_oracle_jacobians_match_reference_finite_differences(tmp_path):
         assert abs(HF[p] - dF) <= 1e-6 * max(1.0, np.abs(HF).max()), p
 
 
+@pytest.mark.parametrize("box", [(8, 4, 0.1), (32, 7, 0.05)], ids=["8mol_self_images", "32mol"])
+def test_oracle_jacobians_match_reference_analytic(box):
+    """The restatement's energy and force Jacobians against the reference's
+    own analytic derivatives (NeuralNetwork::calculateDEdc /
+    calculateDFdc, NeuralNetwork.cpp:444-527, summed over the structure's
+    atoms as Training::update does): 1e-12 of the largest entry.  The
+    8-molecule box is smaller than the cutoff diameter, so atoms see their
+    own periodic images (the Jacobian keeps them, Training.cpp:3604-3615)."""
+    from oracle import training_ref as T
+    n_mol, seed, sigma = box
+    s = water.water_box(n_mol, seed=seed, sigma=sigma)
+    tr = T.Training(H.WATER40, [s], [0.0], np.zeros((s.numAtoms, 3)), updater=None)
+    p = oref.RefPrediction(H.WATER40)
+    try:
+        _, HE = tr.observation(0, 0)
+        JE = p.jacobian(s.to_text(), 0)
+        assert np.abs(HE - JE).max() <= 1e-12 * np.abs(JE).max()
+        for atom, comp in ((0, 0), (5, 1), (s.numAtoms - 1, 2)):
+            _, HF = tr.observation(1, 0, atom, comp)
+            JF = p.jacobian(s.to_text(), 1, atom, comp)
+            assert np.abs(HF - JF).max() <= 1e-12 * np.abs(JF).max(), (atom, comp)
+    finally:
+        p.close()
+
+
 def test_kalman_restatement_is_recursive_least_squares():
     """With q = 0 and eta fixed, one observation per update, the filter is
     recursive least squares: its state is the regularised least-squares

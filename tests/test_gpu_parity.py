@@ -132,6 +132,41 @@ def test_water_batch_uneven_fp64():
         a0 += s.numAtoms
 
 
+def test_water_batch_largest_boxes_fp64():
+    """The top of the batched workload's size range: two 512-molecule boxes
+    (1536 atoms, ~170 k neighbour entries each) beside a 32-molecule box in
+    one batch; neighbour lists bit-exact, energies and forces within 1e-10."""
+    boxes = [water.water_box(512, seed=101), water.water_box(32, seed=103), water.water_box(512, seed=102)]
+    m = H.gpu_mode(H.WATER40)
+    b = H.gpu_batch(m, boxes)
+    E, F = b.energies(), b.forces()
+    a0 = 0
+    for k, s in enumerate(boxes):
+        snap = H.reference_snapshot(H.WATER40, s)
+        _compare_structure(b, a0, a0 + s.numAtoms, snap, k, E, F, tol_f=_water_tol_f(s))
+        a0 += s.numAtoms
+
+
+def test_mixed_precision_error_budget_across_sizes():
+    """The mixed form against the reference on 32 boxes spanning the batched
+    workload's whole size range (32..512 molecules, log-uniform as the
+    workload draws them, the two ends included): every structure within
+    1 meV/atom and every force component within 30 meV/A."""
+    boxes = water.water_batch(30, seed=17, n_min=32, n_max=512)
+    boxes = [water.water_box(32, seed=171)] + boxes + [water.water_box(512, seed=172)]
+    m = H.gpu_mode(H.WATER40, precision="mixed")
+    b = H.gpu_batch(m, boxes)
+    E, F = b.energies(), b.forces()
+    E_ref, F_ref = H.reference_energies_forces(H.WATER40, boxes)
+    a0, de_max, df_max = 0, 0.0, 0.0
+    for k, s in enumerate(boxes):
+        de_max = max(de_max, abs(E[k] - E_ref[k]) / s.numAtoms * H.HA_TO_MEV)
+        df_max = max(df_max, np.abs(F[a0:a0 + s.numAtoms] - F_ref[k]).max() * H.HA_PER_BOHR_TO_MEV_PER_A)
+        a0 += s.numAtoms
+    assert de_max <= 1.0, de_max
+    assert df_max <= 30.0, df_max
+
+
 def test_stored_dgdr_matches_reference():
     """dG/dr stored per neighbour row (Atom::Neighbor::dGdr layout)."""
     s = water.water_box(32, seed=1)

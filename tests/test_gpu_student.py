@@ -93,6 +93,47 @@ def test_gradient_matches_oracle_finite_differences(student_dir):
         assert abs(fd - grad[p]) <= 2e-6 * scale + 1e-6 * abs(fd), (p, fd, grad[p])
 
 
+def test_gradient_matches_reference_analytic(student_dir):
+    """The trainer's loss gradient (forward with tangents, reverse through
+    both, second derivatives of the activations) against the reference's
+    analytic network derivatives: with a_s = dL/dE_s and u_k = dL/dF_k of
+    L = wE/S sum_s ((E_s - E_s^ref)/N_s)^2 + wF/(3N) sum_k (F_k - F_k^ref)^2,
+    dL/dw = sum_s a_s dE_s/dw + sum_k u_k dF_k/dw with dE/dw and dF/dw from
+    NeuralNetwork::calculateDEdc / calculateDFdc (NeuralNetwork.cpp:444-527)
+    as Training::update sums them.  Bound: 1e-10 of the largest component."""
+    from oracle import ref as oref
+    # clusters (no periodic images): the trainer's force is calculateForces' force, which leaves an atom's
+    # own periodic images out, while the training Jacobian keeps them (Training.cpp:3604-3615)
+    from n2p2_b200 import Structure
+    structs = [Structure(b.positions, b.elements, None)
+               for b in (water.water_box(12, seed=51, sigma=0.1), water.water_box(16, seed=52, sigma=0.05))]
+    m = student.load_mode(student_dir)
+    b = m.batch(structs)
+    b.setPositions(np.concatenate([s.positions for s in structs]))
+    b.evaluate(forces=True, graph=False)
+    E, F = b.energies(), b.forces()
+    rng = np.random.default_rng(4)
+    E_ref = E + rng.normal(0, 0.05, len(structs))
+    F_ref = F + rng.normal(0, 0.01, F.shape)
+    from n2p2_b200 import Trainer
+    wE, wF = 1.0, 10.0
+    tr = Trainer(m, energyWeight=wE, forceWeight=wF)
+    _, grad = tr.step(b, E_ref, F_ref, update=False, gradient=True)
+    p = oref.RefPrediction(student_dir)
+    try:
+        S, N = len(structs), b.numAtoms
+        g_ref, a0 = np.zeros_like(grad), 0
+        for k, s in enumerate(structs):
+            n = s.numAtoms
+            a = wE / S * 2.0 * (E[k] - E_ref[k]) / (n * n)
+            u = wF / (3.0 * N) * 2.0 * (F[a0:a0 + n] - F_ref[a0:a0 + n])
+            g_ref += p.loss_gradient(s.to_text(), a, u)
+            a0 += n
+    finally:
+        p.close()
+    assert np.abs(grad - g_ref).max() <= 1e-10 * np.abs(g_ref).max()
+
+
 def test_parameters_round_trip(student_dir):
     from n2p2_b200 import Trainer
     m = student.load_mode(student_dir)

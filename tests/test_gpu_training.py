@@ -8,6 +8,8 @@ to 1e-9 relative in the weights after every run.  The set mixes boxes larger
 than the cutoff diameter with one smaller (periodic self-images: the force
 prediction leaves them out as Mode::calculateForces does, the Jacobian keeps
 them as Training::collectDGdxia does)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -66,6 +68,42 @@ def _pair(data, updater, force_weight=3.0):
     ref = T.Training(H.WATER40, ss, E, F, up, force_weight=force_weight)
     ref.nets.weights = w0.copy()
     return m, tr, ref
+
+
+def test_jacobians_match_reference_analytic(data):
+    """The device's observation Jacobians (kParamGrad and the force
+    adjoint) against the reference's analytic derivatives
+    (NeuralNetwork::calculateDEdc / calculateDFdc, NeuralNetwork.cpp:444-527,
+    summed as Training::update does) at the set's current weights: 1e-10 of
+    the largest entry (force Jacobians carry the force weight)."""
+    m, tr, ref = _pair(data, ("gd", {"eta": 1e-3}))
+    ss = data[0]
+    d = str(__import__("tempfile").mkdtemp())
+    try:
+        import shutil
+        for fn in os.listdir(H.WATER40):
+            shutil.copy(os.path.join(H.WATER40, fn), d)
+        from oracle import training_ref as T
+        nets = T.Networks(H.WATER40)
+        w = tr.weights()
+        for e, sym in enumerate(nets.symbols):
+            water.write_weights(os.path.join(d, "weights.%03d.data" % T.oref_z(sym)),
+                                w[nets.offsets[e]:nets.offsets[e + 1]])
+        p = oref.RefPrediction(d)
+        try:
+            for prop, s, a, c in ((ENERGY, 0, 0, 0), (ENERGY, 2, 0, 0), (FORCE, 0, 5, 2), (FORCE, 0, 0, 0),
+                                  (FORCE, 2, 7, 1), (FORCE, 3, 11, 0)):
+                _, J = tr.observe(prop, s, a, c)
+                Jr = p.jacobian(ss[s].to_text(), 0 if prop == ENERGY else 1, a, c)
+                if prop == FORCE:
+                    Jr = Jr * tr.forceWeight
+                assert np.abs(J - Jr).max() <= 1e-10 * np.abs(Jr).max(), (prop, s, a, c)
+        finally:
+            p.close()
+    finally:
+        __import__("shutil").rmtree(d, ignore_errors=True)
+        tr.close()
+        m.close()
 
 
 def test_observations_match_oracle(data):
