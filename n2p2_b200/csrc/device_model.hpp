@@ -56,7 +56,10 @@ struct DevGroup
     int    gridNZ;         // zeta slots in use (<= 4)
     int    etaBase[2], etaPow[2];   // eta slot -> staged base and integer power
     int    zetaM1[4];      // zeta - 1 per zeta slot
+    int    etaBits;        // binary digits of the largest etaPow (squares the eta slots share)
+    int    zetaBits;       // binary digits of the largest zetaM1 in use (squares the zeta slots share)
     double lambdaVal[2];
+    float  baseEtaF[4], lambdaValF[2];   // FP32 copies (the mixed form's per-triplet arithmetic)
     signed char comboMember[16];    // (etaSlot * 2 + lambdaSlot) * 4 + zetaSlot -> member, -1 if absent
 };
 
@@ -84,6 +87,17 @@ struct DevCompactGroup
     int    pad_;
     double rmin, rmax;     // group radial window (SymGrpComp*::addMember: rmin stays 0, rmax the
                            // largest upper boundary)
+};
+
+// The groups of a model as a kernel argument (constant bank: warp-uniform
+// loads, no per-thread copy) for the model-specialised symmetry-function
+// kernels; models with more groups run the generic kernels.
+constexpr int kParamGroups = 40;
+struct DevGroupTable
+{
+    int count;
+    int pad_;
+    DevGroup g[kParamGroups];
 };
 
 constexpr int kMaxBases = 4;        // exponential bases per group
@@ -134,6 +148,7 @@ struct DevModel
     int sortByDistance;   // an angular group has a cutoff below the largest: stage blocks sorted by r
     int allFast;          // 0, or the zeta slots (2, 4) when every group is planned (rs = 0 bases) and every
                           // angular group is on the member grid
+    int powBits;          // binary digits of the largest integer power (eta or zeta) of any member grid
     double maxCutoff, maxCutoff2;
     DevElement el[kDevMaxElements];
     DevCutoff cutoff[4];

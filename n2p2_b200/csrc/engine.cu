@@ -386,6 +386,18 @@ void DeviceModel::upload(Model const& m)
                         dg.etaPow[k] = 1;
                     }
                     dg.gridNZ = (int)zetas.size();
+                    auto digits = [](int v) {
+                        int d = 0;
+                        while (v > 0)
+                        {
+                            ++d;
+                            v >>= 1;
+                        }
+                        return d;
+                    };
+                    dg.etaBits = digits(std::max(dg.etaPow[0], dg.etaPow[1]));
+                    dg.zetaBits = 0;
+                    for (int k = 0; k < dg.gridNZ; ++k) dg.zetaBits = std::max(dg.zetaBits, digits(dg.zetaM1[k]));
                 }
                 if (ok) dg.grid = 1;
                 else for (int c = 0; c < 16; ++c) dg.comboMember[c] = -1;
@@ -421,6 +433,7 @@ void DeviceModel::upload(Model const& m)
                 members.push_back(dm);
             }
             if (!dg.fast || (dg.type != 2 && (!dg.grid || dg.numBases > 1))) v.allFast = 0;   // one staged base
+            if (dg.grid) v.powBits = std::max(v.powBits, std::max(dg.etaBits, dg.zetaBits));
             if (dg.type != 2 && dg.rc < m.maxCutoffRadius) v.sortByDistance = 1;
             else if (dg.type != 2 && dg.gridNZ > 2 && v.allFast) v.allFast = 4;
             groups.push_back(dg);
@@ -535,6 +548,11 @@ void DeviceModel::upload(Model const& m)
         cudaCheck(cudaMalloc(dst, bytes ? bytes : 16), "cudaMalloc(model)");
         if (bytes) cudaCheck(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice), "cudaMemcpy(model)");
     };
+    for (auto& g : groups)
+    {
+        for (int b = 0; b < 4; ++b) g.baseEtaF[b] = (float)g.baseEta[b];
+        for (int k = 0; k < 2; ++k) g.lambdaValF[k] = (float)g.lambdaVal[k];
+    }
     up((void**)&groups_, groups.data(), groups.size() * sizeof(DevGroup));
     up((void**)&members_, members.data(), members.size() * sizeof(DevMember));
     up((void**)&scaling_, scaling.data(), scaling.size() * sizeof(DevScaling));
@@ -552,6 +570,13 @@ void DeviceModel::upload(Model const& m)
     v.compactGroups = compactGroups_;
     v.compactMembers = compactMembers_;
     v.groups = groups_;
+    groupTable = DevGroupTable{};
+    if (groups.size() <= (size_t)kParamGroups)
+    {
+        groupTable.count = (int)groups.size();
+        std::copy(groups.begin(), groups.end(), groupTable.g);
+    }
+    else v.allFast = 0;   // the specialised kernels read the groups from their argument
     v.members = members_;
     v.scaling = scaling_;
     v.rowTable = rowTable_;
@@ -1072,7 +1097,7 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         }
         else
         {
-            launchSFValues(m, v_, precision, sms_, stream_, sfShape_[0][precision]);
+            launchSFValues(m, dmodel_.groupTable, v_, precision, sms_, stream_, sfShape_[0][precision]);
             launches += 2;
             if (m.numCompactGroups > 0)
             {
@@ -1111,7 +1136,7 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         }
         else
         {
-            launchSFForces(m, v_, precision, sms_, stream_, sfShape_[1][precision]);
+            launchSFForces(m, dmodel_.groupTable, v_, precision, sms_, stream_, sfShape_[1][precision]);
             launches += 2;
             if (m.numCompactGroups > 0)
             {
@@ -1278,8 +1303,8 @@ Batch::TuneResult Batch::autotune(int precision, int checkExtrapolation, bool us
             for (int v = 0; v < kSFShapeCount; ++v)
             {
                 auto launch = [&] {
-                    if (pass == 0) launchSFValues(m, v_, precision, sms_, stream_, v);
-                    else launchSFForces(m, v_, precision, sms_, stream_, v);
+                    if (pass == 0) launchSFValues(m, dmodel_.groupTable, v_, precision, sms_, stream_, v);
+                    else launchSFForces(m, dmodel_.groupTable, v_, precision, sms_, stream_, v);
                 };
                 launch();
                 double best = 1e300;

@@ -57,6 +57,7 @@ public:
     ~DeviceModel();
     void upload(Model const& m);
     DevModel view;
+    DevGroupTable groupTable{};          // the groups again, passed by value to the specialised kernels
     int maxSF = 0;
     size_t numWeights = 0;               // entries of the flat weight array
     uint64_t fingerprint = 0;            // hash of the evaluation plan (groups, members, cutoffs)

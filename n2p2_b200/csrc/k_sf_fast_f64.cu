@@ -61,26 +61,30 @@ void launchMaskOffsets(DevModel const& m, BatchView const& b, int sms, cudaStrea
     launchExclusiveScan(b.N, b.maskWords, b.maskOffset, b.scanTmp, &b.status->maskWords, st);
 }
 
-void launchSFValuesF64(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int variant)
+void launchSFValuesF64(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int sms, cudaStream_t st,
+                       int variant)
 {
-    valuesT<double>(m, b, sms, st, variant);
+    valuesT<double>(m, gt, b, sms, st, variant);
 }
 
-void launchSFForcesF64(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int variant)
+void launchSFForcesF64(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int sms, cudaStream_t st,
+                       int variant)
 {
-    forcesT<double>(m, b, sms, st, variant);
+    forcesT<double>(m, gt, b, sms, st, variant);
 }
 
-void launchSFValues(DevModel const& m, BatchView const& b, int precision, int sms, cudaStream_t st, int variant)
+void launchSFValues(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int precision, int sms,
+                    cudaStream_t st, int variant)
 {
-    if (precision == 0) launchSFValuesF64(m, b, sms, st, variant);
-    else launchSFValuesF32(m, b, sms, st, variant);
+    if (precision == 0) launchSFValuesF64(m, gt, b, sms, st, variant);
+    else launchSFValuesF32(m, gt, b, sms, st, variant);
 }
 
-void launchSFForces(DevModel const& m, BatchView const& b, int precision, int sms, cudaStream_t st, int variant)
+void launchSFForces(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int precision, int sms,
+                    cudaStream_t st, int variant)
 {
-    if (precision == 0) launchSFForcesF64(m, b, sms, st, variant);
-    else launchSFForcesF32(m, b, sms, st, variant);
+    if (precision == 0) launchSFForcesF64(m, gt, b, sms, st, variant);
+    else launchSFForcesF32(m, gt, b, sms, st, variant);
 }
 
 } // namespace n2p2b200

@@ -102,12 +102,18 @@ void launchCutoffValues(DevModel const& m, BatchView const& b, int sms, cudaStre
 // tier's (stage capacity, warps per block) in the model-specialised kernels:
 // (128, 4), (160, 4), (192, 2).
 constexpr int kSFShapeCount = 3;
-void launchSFValues(DevModel const& m, BatchView const& b, int precision, int sms, cudaStream_t st, int variant);
-void launchSFForces(DevModel const& m, BatchView const& b, int precision, int sms, cudaStream_t st, int variant);
-void launchSFValuesF64(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int variant);
-void launchSFForcesF64(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int variant);
-void launchSFValuesF32(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int variant);
-void launchSFForcesF32(DevModel const& m, BatchView const& b, int sms, cudaStream_t st, int variant);
+void launchSFValues(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int precision, int sms,
+                    cudaStream_t st, int variant);
+void launchSFForces(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int precision, int sms,
+                    cudaStream_t st, int variant);
+void launchSFValuesF64(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int sms, cudaStream_t st,
+                       int variant);
+void launchSFForcesF64(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int sms, cudaStream_t st,
+                       int variant);
+void launchSFValuesF32(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int sms, cudaStream_t st,
+                       int variant);
+void launchSFForcesF32(DevModel const& m, DevGroupTable const& gt, BatchView const& b, int sms, cudaStream_t st,
+                       int variant);
 void launchSFDerivatives(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 void launchContractStored(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 

@@ -210,6 +210,32 @@ __device__ __forceinline__ void cutoffFdfF32(DevCutoff const& c, float r, float&
     dfc = (float)df;
 }
 
+// The poly2 cutoff (type 6) without the type dispatch, for kernels
+// instantiated per cutoff type: FP64 with the arithmetic of cutoffFdf, FP32
+// with that of cutoffFdfF32; the values below r_ci (1, 0) and from r_c on
+// (0, 0) are chosen by selects instead of branches.
+__device__ __forceinline__ void cutoffPoly2(DevCutoff const& c, double r, double& fc, double& dfc)
+{
+    const double x = (r - c.rci) * c.iw;
+    const double x2 = x * x;
+    const double fx = ((15.0 - 6.0 * x) * x - 10.0) * x * x2 + 1.0;
+    const double dfx = x2 * ((60.0 - 30.0 * x) * x - 30.0);
+    const bool in = r < c.rc, inner = r < c.rci;
+    fc = in ? (inner ? 1.0 : fx) : 0.0;
+    dfc = (in && !inner) ? dfx * c.iw : 0.0;
+}
+
+__device__ __forceinline__ void cutoffPoly2(DevCutoff const& c, float r, float& fc, float& dfc)
+{
+    const float x = (r - c.rciF) * c.iwF, u = (c.rcF - r) * c.iwF;
+    const float xu = x * u, u2 = u * u;
+    const float p = u2 * u * ((6.0f * x + 3.0f) * x + 1.0f);
+    const float d = -30.0f * xu * xu;
+    const bool in = r < c.rcF, inner = r < c.rciF;
+    fc = in ? (inner ? 1.0f : p) : 0.0f;
+    dfc = (in && !inner) ? d * c.iwF : 0.0f;
+}
+
 // SymFnc::scale (SymFnc.cpp:169-195)
 __device__ __forceinline__ double scaleG(DevScaling const& s, double v)
 {

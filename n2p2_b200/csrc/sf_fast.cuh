@@ -71,6 +71,46 @@ struct alignas(16) Stage
     int nBelow[4][kDevMaxElements];        // per cutoff slot and element: block entries with r < r_c
 };
 
+// Group gi of the model: the specialised kernels (FAST) read it from the
+// group table argument (warp-uniform constant-bank loads), the generic ones
+// copy it from the model's device array.
+template <int FAST>
+__device__ __forceinline__ DevGroup const& groupOf(DevGroupTable const& gt, DevModel const& model, int gi, DevGroup& scratch)
+{
+    if constexpr (FAST != 0) return gt.g[gi];
+    else
+    {
+        scratch = model.groups[gi];
+        return scratch;
+    }
+}
+
+// A group's base widths and lambda values in the pass's precision (the
+// FP32 copies are the FP64 values rounded once on the host).
+template <typename T>
+__device__ __forceinline__ T groupBaseEta(DevGroup const& G, int q)
+{
+    if constexpr (sizeof(T) == 4) return G.baseEtaF[q];
+    else return G.baseEta[q];
+}
+
+template <typename T>
+__device__ __forceinline__ T groupLambda(DevGroup const& G, int ls)
+{
+    if constexpr (sizeof(T) == 4) return G.lambdaValF[ls];
+    else return G.lambdaVal[ls];
+}
+
+// Force-pass coefficients of one member-grid combination (eta, lambda,
+// zeta): with w = dE/dG * factorNorm, c[0] = w zeta lambda, c[1] = w zeta
+// lambda factorDeriv, c[2] = w (all 0 for an absent combination); one
+// 16-byte aligned record read with vector loads.
+template <typename T>
+struct alignas(16) GridCoef
+{
+    T c[4];
+};
+
 // Per-group member parameters (shared by all lanes).
 // COMPACT (model-specialised kernels): only what planned radial groups and
 // member grids read.
@@ -83,7 +123,7 @@ struct Members
     int base[kM], pw[kM];
     T zl[kC], fd[kC], lambda[kC], zeta[kC];
     int zint[kC], flags[kC];  // flags: 1 intPow, 2 calcExp
-    T gcw[16], gzl[16], gfd[16];   // member grid: coefficients per (eta, lambda, zeta) combination, 0 if absent
+    GridCoef<T> gc[16];       // member grid: force-pass coefficients per (eta, lambda, zeta) combination
 };
 
 constexpr int kQueue = 128;  // ring of accepted (owner, partner) pairs waiting for a full warp (< 32 + 64)
@@ -381,7 +421,7 @@ __device__ void stageFactors(Stage<T, CAP, DF, NB>& S, DevGroup const& G, int la
         for (int s = S.blockBegin[e] + lane; s < S.blockBegin[e + 1]; s += 32)
         {
             const T r = S.r[s];
-            for (int q = 0; q < G.numBases && q < NB; ++q) S.E[q][s] = fexp<T>(-(T)G.baseEta[q] * r * r);
+            for (int q = 0; q < G.numBases && q < NB; ++q) S.E[q][s] = fexp<T>(-groupBaseEta<T>(G, q) * r * r);
         }
     }
     __syncwarp();
@@ -409,17 +449,19 @@ __device__ void stageMembers(Members<T, COMPACT>& mb, DevModel const& model, Dev
             mb.flags[q] = (M.useIntPow ? 1 : 0) | (M.calcExp ? 2 : 0);
         }
     }
-    if (G.grid && lane < 16)
+    if (G.grid && dEdG && lane < 16)
     {
         const int q = G.comboMember[lane];
+        GridCoef<T> cf{};
         if (q >= 0)
         {
             DevMember const& M = model.members[G.memberBegin + q];
-            mb.gcw[lane] = dEdG ? (T)(dEdG[M.sf] * M.factorNorm) : T(0);
-            mb.gzl[lane] = (T)M.zetaLambda;
-            mb.gfd[lane] = (T)M.factorDeriv;
+            const double w = dEdG[M.sf] * M.factorNorm;
+            cf.c[0] = (T)(w * M.zetaLambda);
+            cf.c[1] = (T)(w * M.zetaLambda * M.factorDeriv);
+            cf.c[2] = (T)w;
         }
-        else mb.gcw[lane] = mb.gzl[lane] = mb.gfd[lane] = T(0);
+        mb.gc[lane] = cf;
     }
     __syncwarp();
 }
@@ -485,14 +527,30 @@ __device__ __forceinline__ void tripletGeometry(Stage<T, CAP, DF, NB> const& S, 
     t.dfcjk = T(0);
 }
 
+// Cutoff types with a kernel instance of their own (CUT template argument);
+// every other type runs the instance with the run-time dispatch.
+constexpr int kCutAny = 0, kCutPoly2 = 6;
+
+// The poly2 instances of the model-specialised kernels also take the integer
+// powers of their member grids as compile-time bounded: at most 2 binary
+// digits with two zeta slots (zeta <= 4, eta multiples <= 3), 4 with four
+// slots (zeta <= 16, multiples <= 15).  Models beyond that run the kCutAny
+// instances (run-time bounds).
+template <int FAST, int CUT>
+__host__ __device__ constexpr int sfPowBits()
+{
+    return CUT == kCutPoly2 ? (FAST == 2 ? 2 : 4) : 0;
+}
+
 // r_jk and its cutoff (narrow groups): FP64 in the FP64 form; in the FP32
 // form the cancellation-free factored polynomials (cutoffFdfF32).
-template <typename T>
+template <typename T, int CUT = kCutAny>
 __device__ __forceinline__ void tripletJK(DevCutoff const& cut, Triplet<T>& t)
 {
     t.rijk = frsqrt<T>(t.rjk2);
     t.rjk = t.rjk2 * t.rijk;
-    if constexpr (sizeof(T) == 4) cutoffFdfF32(cut, t.rjk, t.fcjk, t.dfcjk);
+    if constexpr (CUT == kCutPoly2) cutoffPoly2(cut, t.rjk, t.fcjk, t.dfcjk);
+    else if constexpr (sizeof(T) == 4) cutoffFdfF32(cut, t.rjk, t.fcjk, t.dfcjk);
     else cutoffFdf(cut, t.rjk, t.fcjk, t.dfcjk);
 }
 
@@ -511,7 +569,7 @@ __device__ __forceinline__ void loadTriplet(Stage<T, CAP, DF, NB> const& S, DevC
 // chains could interleave; the kernels run ILP = 1: two triplets per lane
 // measured 1.5x slower on B200 (the extra live registers cut residency
 // from 16 to 12 warps per SM and spilled in the force pass).
-template <typename T, int CAP, bool DF, int NB, int ILP>
+template <int CUT, typename T, int CAP, bool DF, int NB, int ILP>
 __device__ __forceinline__ void loadTriplets(Stage<T, CAP, DF, NB> const& S, DevCutoff const& cut, bool narrow,
                                              const int* queue, int qh, int take, int lane, Triplet<T> (&t)[ILP],
                                              int (&so)[ILP], int (&sp)[ILP], bool (&ok)[ILP])
@@ -529,7 +587,7 @@ __device__ __forceinline__ void loadTriplets(Stage<T, CAP, DF, NB> const& S, Dev
     if (narrow)
     {
 #pragma unroll
-        for (int u = 0; u < ILP; ++u) tripletJK<T>(cut, t[u]);
+        for (int u = 0; u < ILP; ++u) tripletJK<T, CUT>(cut, t[u]);
     }
 }
 
@@ -543,7 +601,7 @@ __device__ __forceinline__ void tripletBases(Stage<T, CAP, DF, NB> const& S, Dev
     for (int q = 0; q < kMaxStagedBases; ++q)
     {
         if (q < NB)
-            bv[q] = (q < G.numBases) ? S.E[q][so] * S.E[q][sp] * (narrow ? fexp<T>(-(T)G.baseEta[q] * rjk2) : T(1))
+            bv[q] = (q < G.numBases) ? S.E[q][so] * S.E[q][sp] * (narrow ? fexp<T>(-groupBaseEta<T>(G, q) * rjk2) : T(1))
                                      : T(0);
         else
             bv[q] = T(0);
@@ -582,182 +640,146 @@ __device__ __forceinline__ T powUniform(T x, int e)
     }
 }
 
-// Member grid, G pass: acc[(eta * 2 + lambda) * 4 + zeta] += E_eta * pl^zeta * pfc
+// The squares x^(2^k), k < bits, that pow_int forms (p[0] = x,
+// p[k] = p[k-1]^2; utility.cpp:292-316), shared by the exponents of one
+// base.  BITS > 0: a compile-time bound on the binary digits of every
+// exponent (exactly BITS - 1 squarings); BITS = 0: the warp-uniform run-time
+// `bits` (<= 5; FP32 then forms every square, FP64 selects).
+template <typename T, int BITS>
+__device__ __forceinline__ void powSquares(T x, int bits, T (&p)[5])
+{
+    p[0] = x;
+#pragma unroll
+    for (int k = 1; k < 5; ++k)
+    {
+        if constexpr (BITS > 0)
+        {
+            if (k < BITS) p[k] = p[k - 1] * p[k - 1];
+        }
+        else if constexpr (sizeof(T) == 4) p[k] = p[k - 1] * p[k - 1];
+        else p[k] = (k < bits) ? p[k - 1] * p[k - 1] : T(1);
+    }
+}
+
+// x^e from its squares in pow_int's multiplication order (1 times the
+// square of each set bit of e, in increasing bit order), e < 2^bits and
+// warp-uniform: the same rounding as powUniform with the squares formed once.
+template <typename T, int BITS>
+__device__ __forceinline__ T powFromSquares(T const (&p)[5], int e, int bits)
+{
+    T r = (e & 1) ? p[0] : T(1);
+#pragma unroll
+    for (int k = 1; k < 5; ++k)
+    {
+        if constexpr (BITS > 0)
+        {
+            if (k < BITS && ((e >> k) & 1)) r *= p[k];
+        }
+        else if constexpr (sizeof(T) == 4) r = ((e >> k) & 1) ? r * p[k] : r;
+        else if (k < bits && ((e >> k) & 1)) r *= p[k];
+    }
+    return r;
+}
+
+// The two eta slots' Gaussians of a triplet, E_slot = base^etaPow (one
+// set of squares when both slots use the same staged base).
+template <typename T, int BITS>
+__device__ __forceinline__ void gridEtas(T const* bv, DevGroup const& G, T (&vS)[2])
+{
+    T p[5];
+    powSquares<T, BITS>(G.etaBase[0] == 0 ? bv[0] : bv[1], G.etaBits, p);
+    vS[0] = powFromSquares<T, BITS>(p, G.etaPow[0], G.etaBits);
+    if (G.etaBase[1] != G.etaBase[0]) powSquares<T, BITS>(G.etaBase[1] == 0 ? bv[0] : bv[1], G.etaBits, p);
+    vS[1] = powFromSquares<T, BITS>(p, G.etaPow[1], G.etaBits);
+}
+
+// Member grid, G pass: acc[(eta * 2 + lambda) * STRIDE + zeta] += E_eta * pl^zeta * pfc
 // (pl = 1 + lambda cos; terms with pl <= 0 vanish, SymGrpExpAngn.cpp:295).
-template <typename T, int NZ, int STRIDE>
+template <typename T, int NZ, int STRIDE, int BITS = 0>
 __device__ __forceinline__ void gridValues(T const* bv, DevGroup const& G, T cost, T pfc, T* acc)
 {
     T vS[2];
-#pragma unroll
-    for (int es = 0; es < 2; ++es) vS[es] = powUniform<T>(G.etaBase[es] == 0 ? bv[0] : bv[1], G.etaPow[es]);
+    gridEtas<T, BITS>(bv, G, vS);
 #pragma unroll
     for (int ls = 0; ls < 2; ++ls)
     {
-        const T pl = T(1) + (T)G.lambdaVal[ls] * cost;
+        const T pl = T(1) + groupLambda<T>(G, ls) * cost;
         const T w = pl > T(0) ? pl * pfc : T(0);
+        T q[5];
+        if constexpr (NZ <= 2) powSquares<T, BITS>(pl, G.zetaBits, q);
 #pragma unroll
         for (int zs = 0; zs < NZ; ++zs)
         {
-            const T pz = powUniform<T>(pl, G.zetaM1[zs]) * w;
+            // four zeta slots: the squares per slot (fewer live registers)
+            const T pz =
+                (NZ <= 2 ? powFromSquares<T, BITS>(q, G.zetaM1[zs], G.zetaBits) : powUniform<T>(pl, G.zetaM1[zs])) * w;
 #pragma unroll
             for (int es = 0; es < 2; ++es) acc[(es * 2 + ls) * STRIDE + zs] += vS[es] * pz;
         }
     }
 }
 
-// Member grid, force pass: the dE/dG-weighted member sums T1, T2 (= Uij =
-// Ujk, rs = 0) and T3 of one triplet.
-template <typename T, int NZ, bool COMPACT>
+// Member grid, force pass: the dE/dG-weighted member sums of one triplet,
+// accumulated onto T1, T2, T3: with a = E_eta pl^(zeta - 1) per combination,
+// T1 = sum c[0] a, T2 = Uij = Uik = Ujk (rs = 0) = pl sum c[1] a and
+// T3 = pl sum c[2] a (terms with pl <= 0 vanish).
+template <typename T, int NZ, bool COMPACT, int BITS = 0>
 __device__ __forceinline__ void gridForces(T const* bv, DevGroup const& G, Members<T, COMPACT> const& mb, T cost, T& T1, T& T2,
                                            T& T3)
 {
     T vS[2];
-#pragma unroll
-    for (int es = 0; es < 2; ++es) vS[es] = powUniform<T>(G.etaBase[es] == 0 ? bv[0] : bv[1], G.etaPow[es]);
+    gridEtas<T, BITS>(bv, G, vS);
 #pragma unroll
     for (int ls = 0; ls < 2; ++ls)
     {
-        const T pl = T(1) + (T)G.lambdaVal[ls] * cost;
+        const T pl = T(1) + groupLambda<T>(G, ls) * cost;
         const bool valid = pl > T(0);
+        T q[5];
+        if constexpr (NZ <= 2) powSquares<T, BITS>(pl, G.zetaBits, q);
+        T S1 = T(0), S2 = T(0), S3 = T(0);
 #pragma unroll
         for (int zs = 0; zs < NZ; ++zs)
         {
-            const T pz1 = valid ? powUniform<T>(pl, G.zetaM1[zs]) : T(0);
+            const T pz1 =
+                valid ? (NZ <= 2 ? powFromSquares<T, BITS>(q, G.zetaM1[zs], G.zetaBits) : powUniform<T>(pl, G.zetaM1[zs]))
+                      : T(0);
 #pragma unroll
             for (int es = 0; es < 2; ++es)
             {
-                const int c = (es * 2 + ls) * 4 + zs;
-                const T a = mb.gcw[c] * vS[es] * pz1;
-                const T azl = a * mb.gzl[c];
-                T1 += azl;
-                T3 += a * pl;
-                T2 += azl * pl * mb.gfd[c];
+                const GridCoef<T> cf = mb.gc[(es * 2 + ls) * 4 + zs];
+                const T a = vS[es] * pz1;
+                S1 += cf.c[0] * a;
+                S2 += cf.c[1] * a;
+                S3 += cf.c[2] * a;
             }
         }
-    }
-}
-
-// powUniform of U bases with one exponent (the same multiplications per
-// base, in the same order).
-template <typename T, int U>
-__device__ __forceinline__ void powUniformN(T (&x)[U], int e, T (&r)[U])
-{
-    if constexpr (sizeof(T) == 8)
-    {
-#pragma unroll
-        for (int u = 0; u < U; ++u) r[u] = T(1);
-#pragma unroll 1
-        while (e)
-        {
-            if (e & 1)
-            {
-#pragma unroll
-                for (int u = 0; u < U; ++u) r[u] *= x[u];
-            }
-            e >>= 1;
-            if (e)
-            {
-#pragma unroll
-                for (int u = 0; u < U; ++u) x[u] *= x[u];
-            }
-        }
-    }
-    else
-    {
-#pragma unroll
-        for (int u = 0; u < U; ++u) r[u] = powUniform<T>(x[u], e);
+        T1 += S1;
+        T2 += S2 * pl;
+        T3 += S3 * pl;
     }
 }
 
 // gridValues of U triplets (pfc = 0 for a triplet that is not to count:
 // it then adds zeros).
-template <typename T, int NZ, int STRIDE, int U>
+template <typename T, int NZ, int STRIDE, int U, int BITS>
 __device__ __forceinline__ void gridValuesN(T const (&bv)[U][kMaxStagedBases], DevGroup const& G, T const (&cost)[U],
                                             T const (&pfc)[U], T* acc)
 {
-    T vS[2][U];
 #pragma unroll
-    for (int es = 0; es < 2; ++es)
-    {
-        T x[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) x[u] = G.etaBase[es] == 0 ? bv[u][0] : bv[u][1];
-        powUniformN<T, U>(x, G.etaPow[es], vS[es]);
-    }
-#pragma unroll
-    for (int ls = 0; ls < 2; ++ls)
-    {
-        T pl[U], w[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-        {
-            pl[u] = T(1) + (T)G.lambdaVal[ls] * cost[u];
-            w[u] = pl[u] > T(0) ? pl[u] * pfc[u] : T(0);
-        }
-#pragma unroll
-        for (int zs = 0; zs < NZ; ++zs)
-        {
-            T x[U], pz[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) x[u] = pl[u];
-            powUniformN<T, U>(x, G.zetaM1[zs], pz);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-            {
-                const T p = pz[u] * w[u];
-#pragma unroll
-                for (int es = 0; es < 2; ++es) acc[(es * 2 + ls) * STRIDE + zs] += vS[es][u] * p;
-            }
-        }
-    }
+    for (int u = 0; u < U; ++u) gridValues<T, NZ, STRIDE, BITS>(bv[u], G, cost[u], pfc[u], acc);
 }
 
 // gridForces of U triplets.
-template <typename T, int NZ, bool COMPACT, int U>
+template <typename T, int NZ, bool COMPACT, int U, int BITS>
 __device__ __forceinline__ void gridForcesN(T const (&bv)[U][kMaxStagedBases], DevGroup const& G,
                                             Members<T, COMPACT> const& mb, T const (&cost)[U], T (&T1)[U], T (&T2)[U],
                                             T (&T3)[U])
 {
-    T vS[2][U];
 #pragma unroll
-    for (int es = 0; es < 2; ++es)
+    for (int u = 0; u < U; ++u)
     {
-        T x[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) x[u] = G.etaBase[es] == 0 ? bv[u][0] : bv[u][1];
-        powUniformN<T, U>(x, G.etaPow[es], vS[es]);
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) T1[u] = T2[u] = T3[u] = T(0);
-#pragma unroll
-    for (int ls = 0; ls < 2; ++ls)
-    {
-        T pl[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) pl[u] = T(1) + (T)G.lambdaVal[ls] * cost[u];
-#pragma unroll
-        for (int zs = 0; zs < NZ; ++zs)
-        {
-            T x[U], pz[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) x[u] = pl[u];
-            powUniformN<T, U>(x, G.zetaM1[zs], pz);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-            {
-                const T pz1 = pl[u] > T(0) ? pz[u] : T(0);
-#pragma unroll
-                for (int es = 0; es < 2; ++es)
-                {
-                    const int c = (es * 2 + ls) * 4 + zs;
-                    const T a = mb.gcw[c] * vS[es][u] * pz1;
-                    const T azl = a * mb.gzl[c];
-                    T1[u] += azl;
-                    T3[u] += a * pl[u];
-                    T2[u] += azl * pl[u] * mb.gfd[c];
-                }
-            }
-        }
+        T1[u] = T2[u] = T3[u] = T(0);
+        gridForces<T, NZ, COMPACT, BITS>(bv[u], G, mb, cost[u], T1[u], T2[u], T3[u]);
     }
 }
 
@@ -766,9 +788,22 @@ __device__ __forceinline__ void gridForcesN(T const (&bv)[U][kMaxStagedBases], D
 // ---------------------------------------------------------------------------
 // G values
 // ---------------------------------------------------------------------------
-template <typename T, int CAP, int WARPS, int FAST>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
-    kSFValuesF(DevModel model, BatchView b, int lower, int flagOverflow)
+// Blocks per SM the register allocation must allow (measured on the water
+// workloads, none of these spills): the specialised G pass with the poly2
+// cutoff fits 5 (FP64, <= 96 registers) or 6 (FP32, <= 80) four-warp
+// blocks, the FP32 force pass with two zeta slots 5; every other four-warp
+// instance 4, the larger stages 1.
+template <typename T, int WARPS, int FAST, int CUT, bool FORCES>
+constexpr int sfMinBlocks()
+{
+    if (WARPS != 4 || FAST == 0 || CUT != 6) return WARPS != 4 ? 1 : 4;
+    if (!FORCES) return sizeof(T) == 8 ? 5 : 6;
+    return (sizeof(T) == 4 && FAST == 2) ? 5 : 4;
+}
+
+template <typename T, int CAP, int WARPS, int FAST, int CUT>
+__global__ void __launch_bounds__(WARPS * 32, (sfMinBlocks<T, WARPS, FAST, CUT, false>()))
+    kSFValuesF(DevModel model, BatchView b, int lower, int flagOverflow, DevGroupTable gt)
 {
     constexpr int ILP = 1;            // triplets per lane and step (see loadTriplets)
     constexpr int kStep = 32 * ILP;   // triplets per warp step
@@ -802,7 +837,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
         int slot = -1;
         for (int g = 0; g < E.groupCount; ++g)
         {
-            DevGroup const G = model.groups[E.groupBegin + g];
+            DevGroup scratch;
+            DevGroup const& G = groupOf<FAST>(gt, model, E.groupBegin + g, scratch);
             const bool fastG = FAST || G.fast;
             if (G.cutoffSlot != slot)
             {
@@ -833,7 +869,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                         T eb[kMaxBases];
 #pragma unroll
                         for (int q = 0; q < kMaxBases; ++q)
-                            eb[q] = (fastG && q < G.numBases) ? fexp<T>(-(T)G.baseEta[q] * r * r) : T(0);
+                            eb[q] = (fastG && q < G.numBases) ? fexp<T>(-groupBaseEta<T>(G, q) * r * r) : T(0);
 #pragma unroll
                         for (int q = 0; q < ACC; ++q)
                         {
@@ -891,7 +927,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                                     Triplet<T> t[ILP];
                                     int so[ILP], sp[ILP];
                                     bool ok[ILP];
-                                    loadTriplets<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh, take, lane,
+                                    loadTriplets<CUT, T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh, take, lane,
                                                          t, so, sp, ok);
                                     T bv[ILP][kMaxStagedBases], cost[ILP], pfc[ILP];
 #pragma unroll
@@ -901,7 +937,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                                         cost[u] = t[u].cost;
                                         pfc[u] = ok[u] ? t[u].fc1 * t[u].fc2 * t[u].fcjk : T(0);
                                     }
-                                    gridValuesN<T, FAST, FAST, ILP>(bv, G, cost, pfc, acc);
+                                    gridValuesN<T, FAST, FAST, ILP, sfPowBits<FAST, CUT>()>(bv, G, cost, pfc, acc);
                                 }
                                 else if (lane < take)
                                 {
@@ -988,7 +1024,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
 // entries l + 32 u.  The self-force sums and the scatter into h keep the
 // one-triplet-per-lane order (entry l before l + 32, and the window's
 // halves scattered one after the other).
-template <typename T, int CAP, int FAST, int ILP>
+template <typename T, int CAP, int FAST, int CUT, int ILP>
 __device__ __forceinline__ void forcesStepN(Stage<T, CAP, true, 1> const& S, Members<T, true> const& mb, DevGroup const& G,
                                             DevCutoff const& cut, bool narrow, const int* queue, int qh, int take,
                                             int lane, T (&h)[3][CAP], T& sfx, T& sfy, T& sfz)
@@ -996,7 +1032,7 @@ __device__ __forceinline__ void forcesStepN(Stage<T, CAP, true, 1> const& S, Mem
     Triplet<T> t[ILP];
     int so[ILP], sp[ILP];
     bool ok[ILP];
-    loadTriplets<T, CAP>(S, cut, narrow, queue, qh, take, lane, t, so, sp, ok);
+    loadTriplets<CUT, T, CAP>(S, cut, narrow, queue, qh, take, lane, t, so, sp, ok);
     T bv[ILP][kMaxStagedBases], cost[ILP];
 #pragma unroll
     for (int u = 0; u < ILP; ++u)
@@ -1005,7 +1041,7 @@ __device__ __forceinline__ void forcesStepN(Stage<T, CAP, true, 1> const& S, Mem
         cost[u] = t[u].cost;
     }
     T T1[ILP], T2[ILP], T3[ILP];
-    gridForcesN<T, FAST, true, ILP>(bv, G, mb, cost, T1, T2, T3);
+    gridForcesN<T, FAST, true, ILP, sfPowBits<FAST, CUT>()>(bv, G, mb, cost, T1, T2, T3);
     T o[ILP][3], q[ILP][3];
 #pragma unroll
     for (int u = 0; u < ILP; ++u)
@@ -1059,9 +1095,9 @@ __device__ __forceinline__ void forcesStepN(Stage<T, CAP, true, 1> const& S, Mem
     }
 }
 
-template <typename T, int CAP, int WARPS, int FAST>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
-    kSFForcesF(DevModel model, BatchView b, int lower)
+template <typename T, int CAP, int WARPS, int FAST, int CUT>
+__global__ void __launch_bounds__(WARPS * 32, (sfMinBlocks<T, WARPS, FAST, CUT, true>()))
+    kSFForcesF(DevModel model, BatchView b, int lower, DevGroupTable gt)
 {
     constexpr int ILP = 1;            // triplets per lane and step (see loadTriplets)
     constexpr int kStep = 32 * ILP;   // triplets per warp step
@@ -1100,7 +1136,8 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                 sfz += (double)gsz;
                 gsx = gsy = gsz = T(0);
             }
-            DevGroup const G = model.groups[E.groupBegin + g];
+            DevGroup scratch;
+            DevGroup const& G = groupOf<FAST>(gt, model, E.groupBegin + g, scratch);
             const bool fastG = FAST || G.fast;
             if (G.cutoffSlot != slot)
             {
@@ -1120,7 +1157,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                     T eb[kMaxBases];
 #pragma unroll
                     for (int q = 0; q < kMaxBases; ++q)
-                        eb[q] = (fastG && q < G.numBases) ? fexp<T>(-(T)G.baseEta[q] * r * r) : T(0);
+                        eb[q] = (fastG && q < G.numBases) ? fexp<T>(-groupBaseEta<T>(G, q) * r * r) : T(0);
                     T P = T(0);
                     for (int q = 0; q < M; ++q)
                     {
@@ -1180,7 +1217,7 @@ __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 1)
                         if (qn >= kStep || (drain && qn > 0))
                         {
                             const int take = min(kStep, qn);
-                            forcesStepN<T, CAP, FAST, ILP>(S, mb, G, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh,
+                            forcesStepN<T, CAP, FAST, CUT, ILP>(S, mb, G, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh,
                                                           take, lane, SM.h, gsx, gsy, gsz);
                             qh = (qh + take) & (kQueue - 1);
                             qn -= take;
