@@ -134,6 +134,11 @@ n2p2_status n2p2_mode_get_symmetry_function(n2p2_mode* mode, int element, int in
  * dG/dr rows stored for a neighbour of element `neighborElement` around a
  * centre of element `element`. */
 n2p2_status n2p2_mode_get_num_derivative_rows(n2p2_mode* mode, int element, int neighborElement, int* rows);
+/* The atomic network of `element` (NeuralNetwork::getNumNeuronsPerLayer and the
+ * layers' activation types, NeuralNetwork.h:32-56 numbering): *numLayers layers
+ * including input and output; neurons[l] and activations[l] for l < capacity. */
+n2p2_status n2p2_mode_get_network_topology(n2p2_mode* mode, int element, int capacity, int* numLayers, int* neurons,
+                                           int* activations);
 
 /* ---- structures on the GPU: nnp::Structure ---------------------------------- */
 
@@ -487,6 +492,21 @@ n2p2_status n2p2_training_get_num_weights(n2p2_training* training, int64_t* coun
 /* All elements' connections, weight-file order (NeuralNetwork::getConnections). */
 n2p2_status n2p2_training_get_weights(n2p2_training* training, double* weights);
 n2p2_status n2p2_training_set_weights(n2p2_training* training, const double* weights);
+
+/* ---- the training program's shuffles ----------------------------------------
+ * The reference's training loop orders its update candidates and its epoch
+ * schedule with std::shuffle driven by std::mt19937_64 generators
+ * (Training::rngNew / rngGlobalNew, Training.h:577-579; shuffleUpdateCandidates
+ * and setEpochSchedule, Training.cpp:2062-2111), seeded from its GSL
+ * generators.  These calls run that standard-library code, so a host driver
+ * of the training loop draws the same permutations as the reference built
+ * with the same C++ library. */
+typedef struct n2p2_shuffle_rng n2p2_shuffle_rng;
+/* std::mt19937_64 seeded with `seed` (std::mt19937_64::seed). */
+n2p2_status n2p2_shuffle_rng_create(uint64_t seed, n2p2_shuffle_rng** rng);
+n2p2_status n2p2_shuffle_rng_destroy(n2p2_shuffle_rng* rng);
+/* std::shuffle(values, values + count, generator). */
+n2p2_status n2p2_shuffle_rng_shuffle(n2p2_shuffle_rng* rng, int64_t* values, int64_t count);
 
 /* ---- autotuning (no counterpart in the reference) -------------------------
  * The symmetry-function passes run their first tier of atoms with one of

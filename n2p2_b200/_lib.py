@@ -44,6 +44,10 @@ SIGNATURES = {
     "n2p2_last_error": (_cp, []),
     "n2p2_version": (_cp, []),
     "n2p2_mode_create": (_i, [_P(_vp), _i]),
+    "n2p2_mode_get_network_topology": (_i, [_vp, _i, _i, _P(_i), _P(_i), _P(_i)]),
+    "n2p2_shuffle_rng_create": (_i, [ctypes.c_uint64, _P(_vp)]),
+    "n2p2_shuffle_rng_destroy": (_i, [_vp]),
+    "n2p2_shuffle_rng_shuffle": (_i, [_vp, _P(_i64), _i64]),
     "n2p2_mode_destroy": (_i, [_vp]),
     "n2p2_mode_initialize": (_i, [_vp]),
     "n2p2_mode_load_settings_file": (_i, [_vp, _cp]),

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -348,6 +349,53 @@ n2p2_status n2p2_mode_get_num_derivative_rows(n2p2_mode* mode, int element, int 
     N2P2_REQUIRE(mode);
     N2P2_REQUIRE(rows);
     return guard([&] { *rows = (int)mode->model.elements.at(element).table.at(neighborElement).size(); });
+}
+
+n2p2_status n2p2_mode_get_network_topology(n2p2_mode* mode, int element, int capacity, int* numLayers, int* neurons,
+                                           int* activations)
+{
+    N2P2_REQUIRE(mode);
+    N2P2_REQUIRE(numLayers);
+    return guard([&] {
+        NetworkTopology const& t = mode->model.elements.at(element).topology;
+        *numLayers = t.numLayers;
+        for (int l = 0; l < t.numLayers && l < capacity; ++l)
+        {
+            if (neurons) neurons[l] = t.neurons.at(l);
+            if (activations) activations[l] = t.activations.at(l);
+        }
+    });
+}
+
+struct n2p2_shuffle_rng
+{
+    std::mt19937_64 generator;
+};
+
+n2p2_status n2p2_shuffle_rng_create(uint64_t seed, n2p2_shuffle_rng** rng)
+{
+    N2P2_REQUIRE(rng);
+    return guard([&] {
+        auto r = std::make_unique<n2p2_shuffle_rng>();
+        r->generator.seed(seed);
+        *rng = r.release();
+    });
+}
+
+n2p2_status n2p2_shuffle_rng_destroy(n2p2_shuffle_rng* rng)
+{
+    delete rng;
+    return N2P2_OK;
+}
+
+n2p2_status n2p2_shuffle_rng_shuffle(n2p2_shuffle_rng* rng, int64_t* values, int64_t count)
+{
+    N2P2_REQUIRE(rng);
+    if (count > 0) N2P2_REQUIRE(values);
+    return guard([&] {
+        if (count < 0) throw std::invalid_argument("ERROR: negative count.\n");
+        std::shuffle(values, values + count, rng->generator);
+    });
 }
 
 n2p2_status n2p2_batch_create(n2p2_mode* mode, n2p2_batch** batch)

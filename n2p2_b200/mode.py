@@ -125,6 +125,16 @@ class Mode:
                                                              ctypes.byref(b), _dp(p)))
         return (t.value, a.value, b.value, *p.tolist())
 
+    def networkTopology(self, e):
+        """(neurons per layer, activation per layer) of element e's network,
+        input and output layers included."""
+        n = ctypes.c_int()
+        _lib.check(self._lib.n2p2_mode_get_network_topology(self._h, int(e), 0, ctypes.byref(n), None, None))
+        neurons = (ctypes.c_int * n.value)()
+        act = (ctypes.c_int * n.value)()
+        _lib.check(self._lib.n2p2_mode_get_network_topology(self._h, int(e), n.value, ctypes.byref(n), neurons, act))
+        return list(neurons), list(act)
+
     def numDerivativeRows(self, e, en):
         n = ctypes.c_int()
         _lib.check(self._lib.n2p2_mode_get_num_derivative_rows(self._h, int(e), int(en), ctypes.byref(n)))

@@ -15,6 +15,7 @@ weights: after training, every batch of the mode evaluates the trained
 networks.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -209,24 +210,42 @@ class Training:
         schedule = np.concatenate([np.full(nf, FORCE), np.full(ne, ENERGY)])
         if ne and nf:
             rng.shuffle(schedule)
+        mode = {ENERGY: selectionMode, FORCE: selectionMode}
+        out = self.runSchedule(schedule, {ENERGY: eo, FORCE: fo}, mode, {ENERGY: threshold, FORCE: threshold},
+                               {ENERGY: trials, FORCE: trials}, rmse)
+        self.epoch += 1
+        return out
+
+    def runSchedule(self, schedule, orders, selectionMode, threshold, trials, rmse=None):
+        """The updates of one epoch in the order of `schedule` (ENERGY / FORCE
+        per update, Training::loop's epochSchedule): each property walks its
+        candidate order from where its last update stopped (wrapping), taking
+        the next task batch (selection modes 0 and 1) or trying candidates
+        against threshold[p] x rmse[p] (mode 2, at most trials[p]; rmse in
+        internal units, the training RMSE at the epoch's start).  Per-property
+        dictionaries; returns the errors of the used candidates per property."""
+        ec, (fs, fa, fc) = self.updateCandidates()
+        eo, fo = orders[ENERGY], orders[FORCE]
+        be, bf = self.taskBatch[ENERGY], self.taskBatch[FORCE]
+        schedule = np.asarray(schedule)
         errs = {ENERGY: [], FORCE: []}
         pos = {ENERGY: 0, FORCE: 0}
         k = 0
         while k < schedule.size:   # runs of one property go to the device in one call
-            p = schedule[k]
+            p = int(schedule[k])
             r = k
             while r < schedule.size and schedule[r] == p:
                 r += 1
             cnt = (r - k) * (be if p == ENERGY else bf)   # candidates of this run
-            if selectionMode == 2:
+            if selectionMode[p] == 2:
                 if p == ENERGY:
                     order = eo[(pos[p] + np.arange(ec.size)) % ec.size]
-                    used, e = self.updateThreshold(ENERGY, r - k, ec[order], threshold=threshold, trials=trials,
+                    used, e = self.updateThreshold(ENERGY, r - k, ec[order], threshold=threshold[p], trials=trials[p],
                                                    rmse=rmse[0])
                 else:
                     order = fo[(pos[p] + np.arange(fs.size)) % fs.size]
                     used, e = self.updateThreshold(FORCE, r - k, fs[order], fa[order], fc[order],
-                                                   threshold=threshold, trials=trials, rmse=rmse[1])
+                                                   threshold=threshold[p], trials=trials[p], rmse=rmse[1])
                 errs[p].append(e)
                 pos[p] += used
                 k = r
@@ -239,7 +258,6 @@ class Training:
                 errs[p].append(self.update(FORCE, fs[idx], fa[idx], fc[idx]))
             pos[p] += cnt
             k = r
-        self.epoch += 1
         return {p: (np.concatenate(v) if v else np.zeros(0)) for p, v in errs.items()}
 
     # -- state ---------------------------------------------------------------
@@ -274,3 +292,306 @@ class Training:
         df = (F - self.forcesRef).ravel()
         return {"energy_rmse_per_atom": float(np.sqrt(np.mean(de * de))),
                 "force_rmse": float(np.sqrt(np.mean(df * df)))}
+
+
+# ---------------------------------------------------------------------------
+# The training program (nnp-train) around the update loop
+# ---------------------------------------------------------------------------
+
+# Settings::keywordMap alternatives the training program reads under their
+# primary names (Settings.cpp:138-141).
+_ALIASES = {"rmse_threshold_energy": "short_energy_error_threshold",
+            "rmse_threshold_force": "short_force_error_threshold",
+            "energy_fraction": "short_energy_fraction",
+            "force_fraction": "short_force_fraction"}
+
+
+def read_settings(path):
+    """Keyword -> list of value strings of an input.nn file (comments after
+    '#' dropped; a keyword without values maps to [""])."""
+    out = {}
+    with open(path) as f:
+        for line in f:
+            line = line.split("#", 1)[0].strip()
+            if not line:
+                continue
+            parts = line.split(None, 1)
+            out.setdefault(parts[0], []).append(parts[1].strip() if len(parts) > 1 else "")
+    return out
+
+
+class ShuffleRng:
+    """std::mt19937_64 with std::shuffle (n2p2_shuffle_rng_*): the generators
+    Training::rngNew and rngGlobalNew (Training.h:577-579)."""
+
+    def __init__(self, seed):
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.n2p2_shuffle_rng_create(ctypes.c_uint64(int(seed)), ctypes.byref(h)))
+        self._h = h
+
+    def shuffle(self, values):
+        v = np.ascontiguousarray(values, dtype=np.int64)
+        if v.size:
+            _lib.check(self._lib.n2p2_shuffle_rng_shuffle(self._h, v.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                                          v.size))
+        return v
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.n2p2_shuffle_rng_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TrainingRun:
+    """The reference's nnp-train program for a 2G model directory (input.nn,
+    scaling.data, input.data) with the updates on the GPU: the set-up
+    sequence of nnp-train.cpp (random number generators, the structure
+    distribution's draws on one process, the training/test split, random
+    initial weights, the update plan and updater parameters), then
+    Training::loop -- per epoch the candidate shuffles, the shuffled epoch
+    schedule, the updates, and the errors of both sets (the learning curve).
+
+    References: Dataset::setupRandomNumberGenerator (Dataset.cpp:110-163),
+    distributeStructures (:724-886), Training::selectSets (Training.cpp:82-228),
+    randomizeNeuralNetworkWeights (:3628-3679) with
+    NeuralNetwork::modifyConnections (NeuralNetwork.cpp:212-315),
+    setupTraining (:737-1207), setupUpdatePlan (:3851-3959), setupSelectionMode
+    (:3681-3787), loop (:2147-2254), shuffleUpdateCandidates / setEpochSchedule
+    (:2062-2111), calculateError with Structure::updateError
+    (Structure.cpp:1387-1415) and writeLearningCurve (:1734-1842).
+
+    Supported: the combined update strategy, the Kalman filter (standard,
+    fading memory) and gradient descent (fixed, Adam), energy and optional
+    force updates, every selection mode with a constant schedule, task
+    batches (threshold selection: one candidate per update), random initial
+    weights with the Glorot-Bengio scaling (the reference's default) or the
+    weights of `use_old_weights_short`.  One process (the reference's
+    single-rank run).
+    """
+
+    def __init__(self, directory, device=0):
+        from .gsl_rng import Mt19937, Taus
+        from .mode import Mode
+        from .structure import read_structures
+        self.directory = directory
+        st = read_settings(os.path.join(directory, "input.nn"))
+        self.settings = st
+        for kw in ("nguyen_widrow_weights_short", "precondition_weights", "normalize_data_set"):
+            if kw in st:
+                raise ValueError(f"keyword {kw} is not supported by this training driver")
+        if int(self._get("update_strategy", "0")) != 0:
+            raise ValueError("only the combined update strategy (update_strategy 0) is supported here")
+        self.mode = Mode(device)
+        m = self.mode
+        m.initialize()
+        m.loadSettingsFile(os.path.join(directory, "input.nn"))
+        m.setupGeneric()
+        m.setupSymmetryFunctionScaling(os.path.join(directory, "scaling.data"))
+        self.normalize = all(k in st for k in ("mean_energy", "conv_energy", "conv_length"))
+        self.convEnergy = float(st["conv_energy"][0]) if self.normalize else 1.0
+        self.convLength = float(st["conv_length"][0]) if self.normalize else 1.0
+        structures = read_structures(os.path.join(directory, "input.data"))
+        # Dataset::setupRandomNumberGenerator on one process
+        self.rng = Mt19937(int(self._get("random_seed")))
+        self.rngGlobal = Taus(self.rng.get())
+        # distributeStructures(randomize = true): one gsl_rng_uniform_int(rng, numProcs) per structure
+        for _ in structures:
+            self.rng.uniform_int(1)
+        # selectSets
+        tf = float(self._get("test_fraction"))
+        test = [self.rng.uniform() < tf for _ in structures]
+        self.train = [s for s, t in zip(structures, test) if not t]
+        self.test = [s for s, t in zip(structures, test) if t]
+        # initializeWeights
+        if "use_old_weights_short" in st:
+            m.setupNeuralNetworkWeights(os.path.join(directory, "weights.%03zu.data"))
+        else:
+            self._randomizeWeights()
+        self.useForces = "use_short_forces" in st
+        self.pk = [ENERGY] + ([FORCE] if self.useForces else [])
+        self.training = Training(m, self.train, [s.energyRef for s in self.train],
+                                 np.concatenate([s.forcesRef for s in self.train]))
+        self.testBatch = m.batch(self.test) if self.test else None
+        if self.testBatch is not None:
+            self.testBatch.setPositions(np.concatenate([s.positions for s in self.test]))
+        self._setupTraining()
+        self.epoch = 0
+        self.learningCurve = []
+
+    def _get(self, key, default=None):
+        for k in (key, _ALIASES.get(key)):
+            if k and k in self.settings:
+                return self.settings[k][0]
+        if default is None:
+            raise KeyError(f"keyword {key} missing from input.nn")
+        return default
+
+    def _has(self, key):
+        return key in self.settings or (_ALIASES.get(key) in self.settings)
+
+    def _randomizeWeights(self):
+        """randomizeNeuralNetworkWeights: uniform connections in [weights_min,
+        weights_max) from the global generator, element by element in
+        connection order; then MS_GLOROTBENGIO (the weights of every tanh layer
+        times sqrt(6 / (n_prev + n))) and MS_ZEROBIAS."""
+        wmin = float(self._get("weights_min"))
+        wmax = float(self._get("weights_max"))
+        m = self.mode
+        for e in range(m.numElements):
+            neurons, activations = m.networkTopology(e)
+            n = sum(neurons[l - 1] * neurons[l] + neurons[l] for l in range(1, len(neurons)))
+            w = np.array([wmin + self.rngGlobal.uniform() * (wmax - wmin) for _ in range(n)])
+            q = 0
+            for l in range(1, len(neurons)):
+                nw = neurons[l - 1] * neurons[l]
+                if activations[l] == _ACTIVATION_TANH:
+                    w[q:q + nw] *= np.sqrt(6.0 / (neurons[l - 1] + neurons[l]))
+                q += nw
+                w[q:q + neurons[l]] = 0.0
+                q += neurons[l]
+            m.setConnections(e, w)
+
+    def _setupTraining(self):
+        st, t = self.settings, self.training
+        if self.useForces:
+            t.setForceWeight(float(self._get("force_weight", "1.0")))
+        jm = int(self._get("jacobian_mode", "1"))
+        t.setJacobianMode(jm)
+        # setupSelectionMode: the global keywords, then per property
+        self.selectionMode = {p: 0 for p in self.pk}
+        self.threshold = {p: 0.0 for p in self.pk}
+        self.trials = {p: 0 for p in self.pk}
+        names = {ENERGY: "energy", FORCE: "force"}
+        for scope in ["all"] + self.pk:
+            sfx = "" if scope == "all" else "_" + names[scope]
+            props = self.pk if scope == "all" else [scope]
+            if self._has("selection_mode" + sfx):
+                args = self._get("selection_mode" + sfx).split()
+                if len(args) != 1:
+                    raise ValueError("selection mode schedules are not supported by this training driver")
+                for p in props:
+                    self.selectionMode[p] = int(args[0])
+            if self._has("rmse_threshold" + sfx):
+                for p in props:
+                    self.threshold[p] = float(self._get("rmse_threshold" + sfx))
+            if self._has("rmse_threshold_trials" + sfx):
+                for p in props:
+                    self.trials[p] = int(self._get("rmse_threshold_trials" + sfx))
+        self.epochs = int(self._get("epochs"))
+        # setupUpdatePlan
+        e, (fs, _, _) = t.updateCandidates()
+        patterns = {ENERGY: e.size, FORCE: fs.size}
+        self.batchSize = {}
+        self.numUpdates = {}
+        for p in self.pk:
+            frac = float(self._get(names[p] + "_fraction"))
+            tb = int(self._get("task_batch_size_" + names[p]))
+            if tb == 0:
+                raise ValueError("task batches of the entire training set are not supported by this driver")
+            self.batchSize[p] = tb
+            self.numUpdates[p] = int(patterns[p] * frac / tb)
+        t.setTaskBatchSize(self.batchSize[ENERGY], self.batchSize.get(FORCE, 1))
+        total = float(sum(self.numUpdates.values()))
+        ut = int(self._get("updater_type"))
+        if ut == 1:
+            kt = int(self._get("kalman_type", "0"))
+            eps = float(self._get("kalman_epsilon"))
+            q0 = float(self._get("kalman_q0"))
+            qtau = float(self._get("kalman_qtau")) / total
+            qmin = float(self._get("kalman_qmin"))
+            if kt == 0:
+                eta0 = float(self._get("kalman_eta"))
+                etatau, etamax = 1.0, eta0
+                if self._has("kalman_etatau") and self._has("kalman_etamax"):
+                    etatau = float(self._get("kalman_etatau")) / total
+                    etamax = float(self._get("kalman_etamax"))
+                t.setupUpdaterKalman(0, eps, q0, qtau, qmin, eta0, etatau, etamax)
+            else:
+                t.setupUpdaterKalman(1, eps, q0, qtau, qmin, lambda_=float(self._get("kalman_lambda_short")),
+                                     nu=float(self._get("kalman_nue_short")))
+        elif ut == 0:
+            gt = int(self._get("gradient_type", "0"))
+            if gt == 0:
+                t.setupUpdaterGradient(0, eta=float(self._get("gradient_eta")))
+            else:
+                t.setupUpdaterGradient(1, adam_eta=float(self._get("gradient_adam_eta")),
+                                       beta1=float(self._get("gradient_adam_beta1")),
+                                       beta2=float(self._get("gradient_adam_beta2")),
+                                       epsilon=float(self._get("gradient_adam_epsilon")))
+        else:
+            raise ValueError("unknown updater type")
+        # the shuffle generators, seeded from the GSL generators (Training.cpp:1041-1042)
+        self.rngGlobalNew = ShuffleRng(self.rngGlobal.get())
+        self.rngNew = ShuffleRng(self.rng.get())
+        # update candidates in setup order (selectSets): energies by structure, forces by (structure, atom, component)
+        self.orders = {ENERGY: np.arange(e.size, dtype=np.int64), FORCE: np.arange(fs.size, dtype=np.int64)}
+
+    def errors(self):
+        """calculateError: {"energy": (train, test), "force": (train, test)}
+        RMSE of the energy per atom and of the force components in physical
+        units (the learning curve's RMSEpa and RMSE columns)."""
+        def rmse(batch, structs, stored):
+            if batch is None:
+                return 0.0, 0.0
+            batch.evaluate(forces=True, storeDGdr=stored, graph=False)
+            E, F = batch.energies(), batch.forces()
+            Er = np.array([s.energyRef for s in structs])
+            n = np.array([s.numAtoms for s in structs], dtype=np.float64)
+            de = Er - E
+            df = (np.concatenate([s.forcesRef for s in structs]) - F).ravel()
+            return float(np.sqrt(np.sum(de * de / (n * n)) / len(structs))), float(np.sqrt(np.sum(df * df) / df.size))
+        etr, ftr = rmse(self.training.batch, self.train, True)   # the trainer's batch keeps its stored dG/dr
+        ete, fte = rmse(self.testBatch, self.test, False)
+        return {"energy": (etr, ete), "force": (ftr, fte)}
+
+    def _record(self):
+        e = self.errors()
+        self.learningCurve.append({"epoch": self.epoch, **e})
+        return e
+
+    def runEpoch(self):
+        """One pass of Training::loop's epoch body."""
+        t = self.training
+        rmse = t.trainingErrors() if any(self.selectionMode[p] == 2 for p in self.pk) else None
+        # the candidate vectors are shuffled (or sorted) in place: each epoch starts from the last one's order
+        orders = self.orders
+        for p in self.pk:
+            if self.selectionMode[p] == 1:
+                orders[p] = t.sortedCandidates()[0 if p == ENERGY else 1]
+            else:
+                orders[p] = self.rngNew.shuffle(orders[p])
+        schedule = np.concatenate([np.full(self.numUpdates[p], p, dtype=np.int64) for p in reversed(self.pk)])
+        if len(self.pk) > 1:
+            schedule = self.rngGlobalNew.shuffle(schedule)
+        t.runSchedule(schedule, orders, self.selectionMode, self.threshold, self.trials, rmse)
+        self.epoch += 1
+        return self._record()
+
+    def run(self):
+        """The full loop: errors of epoch 0, then `epochs` epochs; returns the
+        learning curve (one dict per epoch)."""
+        self.learningCurve = []
+        self._record()
+        for _ in range(self.epochs):
+            self.runEpoch()
+        return self.learningCurve
+
+    def close(self):
+        for o in ("rngNew", "rngGlobalNew", "testBatch", "training"):
+            x = getattr(self, o, None)
+            if x is not None:
+                x.close()
+                setattr(self, o, None)
+        if getattr(self, "mode", None) is not None:
+            self.mode.close()
+            self.mode = None
+
+
+_ACTIVATION_TANH = 2   # NeuralNetwork::AF_TANH

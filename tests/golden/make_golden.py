@@ -16,6 +16,10 @@ It writes
                           plus golden.json with the energy and forces that the
                           reference's own regression test asserts
                           (test/cpp/ExamplePrediction.h, 1000 eps absolute).
+  training/<name>/        the reference's nnp-train example H2O_RPBE-D3
+                          (examples/nnp-train/<name>/) with golden.json: the
+                          epoch-2 learning-curve RMSEs its regression test
+                          asserts (test/cpp/Example_nnp_train.h, 1e-8 absolute).
   cutoff_functions.json   f and df of all cutoff types at r = 2.4, rc = 3,
                           alpha = 0.2 (test/cpp/test_CutoffFunction.cpp:17-52).
   models/water40/         the synthetic water model of the batched benchmark
@@ -34,12 +38,19 @@ It writes
                           targets, and boxes with closer O-O pairs extrapolate
                           to forces of 1e4 Ha/bohr.
   models/water56/         the large-system model (+16 wide G9 on (H,O),
-                          56-64-64-1 softplus), scaling from a 512-molecule box
-                          with 0.15 bohr displacements (seed 3) plus 48 boxes
-                          of the student-training recipe (64..128 molecules,
-                          0.05..0.4 bohr displacements, seed 777): the teacher
-                          labels those configurations, and with the single box
-                          alone they extrapolate to forces of 1e4 Ha/bohr.
+                          56-64-64-1 softplus), written here with scaling from
+                          a 512-molecule box with 0.15 bohr displacements
+                          (seed 3) plus 48 boxes of the student-training recipe
+                          (64..128 molecules, 0.05..0.4 bohr displacements,
+                          seed 777).  The committed scaling.data is then
+                          rewritten on the GPU by
+                            python -m n2p2_b200.student teacher-scaling \
+                                --teacher tests/golden/models/water56
+                          (nnp-scaling statistics of that box plus all 20,000
+                          configurations of the student-training recipe,
+                          seed 11: the teacher labels those configurations and
+                          the held-out boxes come from the same recipe, so its
+                          inputs stay inside its scaling range there).
   water40_box64.json      reference energy and forces of the 64-molecule box.
   models/qm9_weighted/    the reference's QM9 training settings
                           (examples/nnp-train/QM9/input.nn: weighted compact
@@ -241,13 +252,76 @@ def compact_models(refdir):
     write_derived_model(os.path.join(HERE, "models", "scan_narrow"), text, frames, 2025)
 
 
+TRAINING_EXAMPLES = ["H2O_RPBE-D3"]
+
+
+def parse_training_goldens(src, name):
+    """lastEpoch, RMSE values and accuracy of one Example_nnp_train entry."""
+    blk = src.split('Example_nnp_train("%s")' % name)[1].split("examples.push_back")[0]
+    def val(key):
+        return float(re.search(r"e->%s\s*=\s*([-0-9.E+]+);" % key, blk).group(1))
+    return {"last_epoch": int(val("lastEpoch")), "rmse_energy_train": val("rmseEnergyTrain"),
+            "rmse_energy_test": val("rmseEnergyTest"), "rmse_forces_train": val("rmseForcesTrain"),
+            "rmse_forces_test": val("rmseForcesTest"), "accuracy": val("accuracy")}
+
+
+def training_examples(refdir):
+    """examples/nnp-train/<name>/ (input.nn, input.data, scaling.data) with the
+    learning-curve values the reference's regression test asserts
+    (test/cpp/Example_nnp_train.h; BOOST_REQUIRE_SMALL of the difference)."""
+    src = open(os.path.join(refdir, "test/cpp/Example_nnp_train.h")).read()
+    for name in TRAINING_EXAMPLES:
+        d_in = os.path.join(refdir, "examples/nnp-train", name)
+        d_out = os.path.join(HERE, "training", name)
+        os.makedirs(d_out, exist_ok=True)
+        for fn in ("input.nn", "scaling.data", "input.data"):
+            shutil.copy(os.path.join(d_in, fn), os.path.join(d_out, fn))
+        g = parse_training_goldens(src, name)
+        g["source"] = "test/cpp/Example_nnp_train.h (n2p2 reference regression test of nnp-train)"
+        g["columns"] = "learning-curve.out: RMSEpa energy (train, test), RMSE forces (train, test), physical units"
+        exe = os.path.join(ROOT, "oracle", "_ref", "nnp-train")
+        if os.path.exists(exe):
+            g["reference_run"] = run_reference_training(exe, d_out)
+        with open(os.path.join(d_out, "golden.json"), "w") as fh:
+            json.dump(g, fh, indent=1)
+
+
+def read_learning_curve(path):
+    """Epoch rows of learning-curve.out: {epoch: (RMSEpa E train, test, RMSE F train, test)}
+    (physical units; columns 1, 2, 9, 10 as the reference's test reads them)."""
+    out = {}
+    for line in open(path):
+        c = line.split()
+        if c and not c[0].startswith("#"):
+            out[int(c[0])] = [float(c[1]), float(c[2]), float(c[9]), float(c[10])]
+    return out
+
+
+def run_reference_training(exe, example_dir):
+    """The reference's nnp-train (oracle/_ref/nnp-train, built from its own
+    sources by oracle/Makefile) on the example in a scratch directory: its
+    learning curve per epoch and its Kalman status lines (updater.000.out)."""
+    import subprocess
+    with tempfile.TemporaryDirectory() as tmp:
+        for fn in ("input.nn", "scaling.data", "input.data"):
+            shutil.copy(os.path.join(example_dir, fn), tmp)
+        subprocess.run([exe], cwd=tmp, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        curve = read_learning_curve(os.path.join(tmp, "learning-curve.out"))
+        status = [[float(x) for x in l.split()] for l in open(os.path.join(tmp, "updater.000.out"))
+                  if l.split() and not l.startswith("#")]
+    return {"source": "oracle/_ref/nnp-train (the reference's nnp-train from its own sources, one process)",
+            "learning_curve": {str(k): v for k, v in sorted(curve.items())},
+            "kalman_status_columns": "epoch nupdates Pdiag Poffdiag Pasym Kmean q eta",
+            "kalman_status": status}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("N2P2_REFERENCE") or
-                    os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
-                                 "reference"))
+                    os.path.join(os.path.dirname(ROOT), "reference"))
     ap.add_argument("--examples-only", action="store_true", help="copy the reference examples and their goldens only")
     ap.add_argument("--compact-only", action="store_true", help="write the derived compact-function models only")
+    ap.add_argument("--training-only", action="store_true", help="copy the nnp-train examples and their goldens only")
     args = ap.parse_args()
     refdir = args.reference
     if not ref.available():
@@ -255,6 +329,9 @@ def main():
 
     if args.compact_only:
         compact_models(refdir)
+        return
+    if args.training_only:
+        training_examples(refdir)
         return
 
     src = open(os.path.join(refdir, "test/cpp/ExamplePrediction.h")).read()
@@ -272,6 +349,7 @@ def main():
 
     if args.examples_only:
         return
+    training_examples(refdir)
     compact_models(refdir)
 
     csrc = open(os.path.join(refdir, "test/cpp/test_CutoffFunction.cpp")).read()

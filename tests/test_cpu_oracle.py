@@ -75,3 +75,31 @@ def test_port_matches_reference_library(case):
     assert np.array_equal(o["G"].view(np.int64), a["G"].view(np.int64))
     assert o["energy"] == a["energy"]
     assert H.max_rel(o["forces"], a["forces"]) <= 1e-13
+
+
+def test_reference_nnp_train_reproduces_its_regression_values(tmp_path):
+    """The reference's nnp-train built here from its own sources
+    (oracle/_ref/nnp-train: one process, stand-ins for MPI, GSL's generators
+    and Eigen's Kalman-filter operations) reproduces the learning curve its
+    regression test asserts for H2O_RPBE-D3 (test/cpp/Example_nnp_train.h,
+    1e-8 absolute): the oracle of the training driver is pinned."""
+    import json
+    import shutil
+    import subprocess
+    exe = os.path.join(H.ROOT, "oracle", "_ref", "nnp-train")
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/nnp-train not built (needs the reference sources)")
+    d = os.path.join(H.GOLDEN, "training", "H2O_RPBE-D3")
+    for fn in ("input.nn", "scaling.data", "input.data"):
+        shutil.copy(os.path.join(d, fn), tmp_path)
+    subprocess.run([exe], cwd=tmp_path, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    g = json.load(open(os.path.join(d, "golden.json")))
+    rows = {}
+    for line in open(tmp_path / "learning-curve.out"):
+        c = line.split()
+        if c and not c[0].startswith("#"):
+            rows[int(c[0])] = [float(c[1]), float(c[2]), float(c[9]), float(c[10])]
+    last = rows[g["last_epoch"]]
+    want = [g["rmse_energy_train"], g["rmse_energy_test"], g["rmse_forces_train"], g["rmse_forces_test"]]
+    for a, b in zip(last, want):
+        assert abs(a - b) <= g["accuracy"], (last, want)
