@@ -281,12 +281,14 @@ def run_ours(args):
         tune_mixed = batch.autotune(useCache=False)
         ms_mixed = timed(args.steps, args.warmup)
         Em, Fm = batch.energies(), batch.forces()
+        stages_mixed = batch.profileStages(forces=True)
         mode.setPrecision("fp64")
         atoms_per = np.array([s.numAtoms for s in structs])
         de = np.abs(Em - E64) / atoms_per * HA_TO_MEV
         df = np.abs(Fm - F64) * HA_BOHR_TO_MEV_A
         mixed = {"value": world * natoms / (ms_mixed / 1000.0), "unit": "atoms/s", "ms_per_step": ms_mixed,
                  "speedup_vs_fp64": ms / ms_mixed, "autotune": _shape_names(tune_mixed),
+                 "stages_ms": {n: round(t, 4) for n, t in stages_mixed},
                  "err_vs_fp64_gpu": {"energy_meV_per_atom_max": float(de.max()),
                                      "force_meV_per_A_max": float(df.max()),
                                      "force_meV_per_A_rms": float(np.sqrt((df ** 2).mean()))}}
@@ -344,6 +346,16 @@ def run_ours(args):
                     "traffic": SF_DRAM_BYTES_PER_ENTRY * work["entries"],
                     "traffic_source": "ncu DRAM bytes of a 256-box capture, scaled by neighbour entries",
                     "traffic_GBps": SF_DRAM_BYTES_PER_ENTRY * work["entries"] / (sf_ms * 1e-3) / 1e9}
+
+    if mixed is not None and fp32_peak:
+        # the FP32 symmetry-function passes of the mixed form against the measured FP32 FMA throughput
+        ms32 = sum(t for n, t in mixed["stages_ms"].items() if n in ("sf_values", "sf_forces"))
+        if ms32 > 0:
+            a32 = sf_flops / (ms32 * 1e-3) / 1e12
+            mixed["roofline"] = {"bound": "fp32", "kernel": "kSFValues + kSFForces, FP32 instances",
+                                 "achieved": a32, "peak": fp32_peak, "unit": "TFLOP/s", "frac": a32 / fp32_peak,
+                                 "peak_source": "measured FP32 FMA throughput of this GPU (n2p2_device_fma_peak)",
+                                 "algorithmic_flops_per_step": sf_flops}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -781,24 +793,34 @@ def bench_lammps(steps, warmup, device, cpu=True):
     return out
 
 
-def student_vs_oracle(pred, count=4):
+def _oracle_teacher(args):
+    """Teacher energy and forces of one structure by the FP64 CPU oracle (a
+    worker of student_vs_oracle's process pool); args = (model directory,
+    input.data text)."""
+    from oracle.port import PortModel
+    from n2p2_b200.structure import read_structures
+    teacher, text = args
+    s = read_structures(text, is_text=True)[0]
+    r = PortModel(teacher).evaluate(s)
+    return r["energy"], np.asarray(r["forces"])
+
+
+def student_vs_oracle(pred, count=64, teacher=TEACHER):
     """Student (with fallback) against the FP64 CPU oracle of the teacher on
     the first `count` held-out structures (the oracle restates the reference
-    on the host; it is the checker here, not a timed path)."""
-    from oracle.port import PortModel
+    on the host; it is the checker here, not a timed path), evaluated by a
+    pool of host processes."""
+    import multiprocessing as mp
     from n2p2_b200 import student as student_mod
     structs, Es, Fs = pred
-    pm = PortModel(TEACHER)
-    E_o, F_o, Fs_sel = [], [], []
-    a0 = 0
-    for k, s in enumerate(structs[:count]):
-        r = pm.evaluate(s)
-        E_o.append(r["energy"])
-        F_o.append(r["forces"])
-        Fs_sel.append(Fs[a0:a0 + s.numAtoms])
-        a0 += s.numAtoms
-    out = student_mod.errors(Es[:count], np.concatenate(Fs_sel), E_o, np.concatenate(F_o),
-                             [s.numAtoms for s in structs[:count]])
+    count = min(count, len(structs))
+    texts = [s.to_text() for s in structs[:count]]
+    with mp.get_context("spawn").Pool(max(1, min(16, host_threads()))) as pool:
+        res = pool.map(_oracle_teacher, [(teacher, t) for t in texts])
+    E_o = [r[0] for r in res]
+    F_o = [r[1] for r in res]
+    na = [s.numAtoms for s in structs[:count]]
+    out = student_mod.errors(Es[:count], Fs[:sum(na)], E_o, np.concatenate(F_o), na)
     out["structures"] = count
     return out
 

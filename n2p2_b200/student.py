@@ -677,9 +677,34 @@ def train(teacher_dir, out_dir, num_configs=20000, epochs=8, batch_size=64, eta=
     return summary
 
 
+def teacher_scaling(teacher_dir, num_configs=20000, seed=11, device=0, log=print):
+    """Rewrites the teacher's scaling.data with nnp-scaling statistics
+    (n2p2_b200.scaling, the library's GPU statistics) over the configurations
+    of the student-training recipe (`num_configs`, `seed`: the structures the
+    teacher labels) plus the 512-molecule large-system box, so that the
+    teacher's own inputs stay inside its scaling range on that distribution."""
+    from . import scaling
+    from .mode import Mode
+    t0 = time.perf_counter()
+    structs = [water.water_box(512, seed=3, sigma=0.15)] + training_structures(num_configs, seed)
+    m = Mode(device)
+    m.initialize()
+    m.loadSettingsFile(os.path.join(teacher_dir, "input.nn"))
+    m.setupGeneric()
+    m.setupSymmetryFunctionScalingNone()
+    stats = scaling.collect_statistics(m, structs)
+    scaling.write_scaling(os.path.join(teacher_dir, "scaling.data"), stats)
+    m.close()
+    log(f"teacher scaling over {len(structs)} structures ({time.perf_counter() - t0:.1f} s)")
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
+    ts = sub.add_parser("teacher-scaling", help="rewrite the teacher's scaling.data over the training recipe")
+    ts.add_argument("--teacher", required=True)
+    ts.add_argument("--configs", type=int, default=20000)
+    ts.add_argument("--seed", type=int, default=11)
     t = sub.add_parser("train")
     t.add_argument("--teacher", required=True)
     t.add_argument("--out", required=True)
@@ -693,6 +718,8 @@ def main():
                    help="descriptor choice: force-span selection from a candidate grid, the teacher's most "
                         "important functions, or the fixed student_sf_lines set")
     a = ap.parse_args()
+    if a.cmd == "teacher-scaling":
+        teacher_scaling(a.teacher, a.configs, a.seed)
     if a.cmd == "train":
         s = train(a.teacher, a.out, a.configs, a.epochs, a.batch_size, a.eta, a.seed, rc_angular=a.rc_angular,
                   select=None if a.select == "fixed" else a.select)
