@@ -46,10 +46,10 @@ HA_TO_EV = 27.211386245988
 
 # DRAM bytes (read + write) of the two symmetry-function passes per neighbour
 # entry, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
-# of the 256-box case, all three tiers: G pass 572.2 + 41.1 MB, force pass
-# 727.3 + 309.2 MB over 13,792,482 entries; scaled to a batch by its entry
-# count.
-SF_DRAM_BYTES_PER_ENTRY = (572.2 + 41.1 + 727.3 + 309.2) * 1e6 / 13792482
+# of the 256-box case (FP64, acceptance masks present, first tier 128 x 4),
+# all three tiers: G pass 571.3 + 118.0 MB, force pass 817.8 + 301.5 MB over
+# 13,792,482 entries; scaled to a batch by its entry count.
+SF_DRAM_BYTES_PER_ENTRY = (571.3 + 118.0 + 817.8 + 301.5) * 1e6 / 13792482
 
 # Algorithmic FLOPs per unit of the reference's symmetry-function algorithm
 # with derivatives (add/mul/div/sqrt = 1, exp counted separately):
