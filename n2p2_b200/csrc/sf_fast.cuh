@@ -114,16 +114,20 @@ struct alignas(16) GridCoef
 // Per-group member parameters (shared by all lanes).
 // COMPACT (model-specialised kernels): only what planned radial groups and
 // member grids read.
-template <typename T, bool COMPACT>
+// GPASS (model-specialised G pass): only the radial plan (base, pw); the
+// arrays of the force pass and of unplanned members shrink to one entry, so
+// the stage of a warp stays small enough for six blocks of four warps.
+template <typename T, bool COMPACT, bool GPASS = false>
 struct Members
 {
-    static constexpr int kM = kMaxMembers, kC = COMPACT ? 1 : kMaxMembers;
-    T cw[kM];                // force pass: dE/dG * factorNorm
-    T eta[kM], rs[kM];
+    static constexpr bool kLean = COMPACT && GPASS;
+    static constexpr int kM = kMaxMembers, kC = COMPACT ? 1 : kMaxMembers, kF = kLean ? 1 : kMaxMembers;
+    T cw[kF];                // force pass: dE/dG * factorNorm
+    T eta[kF], rs[kF];
     int base[kM], pw[kM];
     T zl[kC], fd[kC], lambda[kC], zeta[kC];
     int zint[kC], flags[kC];  // flags: 1 intPow, 2 calcExp
-    GridCoef<T> gc[16];       // member grid: force-pass coefficients per (eta, lambda, zeta) combination
+    GridCoef<T> gc[kLean ? 1 : 16];   // member grid: force-pass coefficients per (eta, lambda, zeta) combination
 };
 
 constexpr int kQueue = 128;  // ring of accepted (owner, partner) pairs waiting for a full warp (< 32 + 64)
@@ -132,7 +136,7 @@ template <typename T, int CAP, int FAST>
 struct ValuesSmem
 {
     Stage<T, CAP, false, FAST ? 1 : kMaxStagedBases> st;
-    Members<T, FAST != 0> mb;
+    Members<T, FAST != 0, true> mb;
     int queue[kQueue];
 };
 
@@ -427,16 +431,21 @@ __device__ void stageFactors(Stage<T, CAP, DF, NB>& S, DevGroup const& G, int la
     __syncwarp();
 }
 
-template <typename T, bool COMPACT>
-__device__ void stageMembers(Members<T, COMPACT>& mb, DevModel const& model, DevGroup const& G, const double* dEdG, int lane)
+template <typename T, bool COMPACT, bool GPASS>
+__device__ void stageMembers(Members<T, COMPACT, GPASS>& mb, DevModel const& model, DevGroup const& G, const double* dEdG,
+                             int lane)
 {
+    constexpr bool lean = Members<T, COMPACT, GPASS>::kLean;
     __syncwarp();
     for (int q = lane; q < G.memberCount; q += 32)
     {
         DevMember const& M = model.members[G.memberBegin + q];
-        mb.cw[q] = dEdG ? (T)(dEdG[M.sf] * M.factorNorm) : T(0);
-        mb.eta[q] = (T)M.eta;
-        mb.rs[q] = (T)M.rs;
+        if constexpr (!lean)
+        {
+            mb.cw[q] = dEdG ? (T)(dEdG[M.sf] * M.factorNorm) : T(0);
+            mb.eta[q] = (T)M.eta;
+            mb.rs[q] = (T)M.rs;
+        }
         mb.base[q] = M.expBase;
         mb.pw[q] = M.expPow;
         if constexpr (!COMPACT)
@@ -449,19 +458,22 @@ __device__ void stageMembers(Members<T, COMPACT>& mb, DevModel const& model, Dev
             mb.flags[q] = (M.useIntPow ? 1 : 0) | (M.calcExp ? 2 : 0);
         }
     }
-    if (G.grid && dEdG && lane < 16)
+    if constexpr (!lean)
     {
-        const int q = G.comboMember[lane];
-        GridCoef<T> cf{};
-        if (q >= 0)
+        if (G.grid && dEdG && lane < 16)
         {
-            DevMember const& M = model.members[G.memberBegin + q];
-            const double w = dEdG[M.sf] * M.factorNorm;
-            cf.c[0] = (T)(w * M.zetaLambda);
-            cf.c[1] = (T)(w * M.zetaLambda * M.factorDeriv);
-            cf.c[2] = (T)w;
+            const int q = G.comboMember[lane];
+            GridCoef<T> cf{};
+            if (q >= 0)
+            {
+                DevMember const& M = model.members[G.memberBegin + q];
+                const double w = dEdG[M.sf] * M.factorNorm;
+                cf.c[0] = (T)(w * M.zetaLambda);
+                cf.c[1] = (T)(w * M.zetaLambda * M.factorDeriv);
+                cf.c[2] = (T)w;
+            }
+            mb.gc[lane] = cf;
         }
-        mb.gc[lane] = cf;
     }
     __syncwarp();
 }
@@ -481,8 +493,8 @@ __device__ __noinline__ T gaussShifted(T eta, T rs, T r1, T r2, T r3, int narrow
     return fexp<T>(-eta * (u * u + v * v + (narrow ? w * w : T(0))));
 }
 
-template <typename T, bool COMPACT>
-__device__ __forceinline__ T angularPow(T pl, Members<T, COMPACT> const& mb, int q)
+template <typename T, bool COMPACT, bool GPASS>
+__device__ __forceinline__ T angularPow(T pl, Members<T, COMPACT, GPASS> const& mb, int q)
 {
     return (mb.flags[q] & 1) ? powInt<T>(pl, mb.zint[q] - 1) : powReal<T>(pl, mb.zeta[q] - T(1));
 }
@@ -789,15 +801,15 @@ __device__ __forceinline__ void gridForcesN(T const (&bv)[U][kMaxStagedBases], D
 // G values
 // ---------------------------------------------------------------------------
 // Blocks per SM the register allocation must allow (measured on the water
-// workloads, none of these spills): the specialised G pass with the poly2
-// cutoff fits 5 (FP64, <= 96 registers) or 6 (FP32, <= 80) four-warp
-// blocks, the FP32 force pass with two zeta slots 5; every other four-warp
-// instance 4, the larger stages 1.
+// workloads): the specialised G pass with the poly2 cutoff fits 6 four-warp
+// blocks (<= 80 registers; its lean member stage leaves room in shared
+// memory; FP64 with four zeta slots 5), the FP32 force pass with two zeta
+// slots 5; every other four-warp instance 4, the larger stages 1.
 template <typename T, int WARPS, int FAST, int CUT, bool FORCES>
 constexpr int sfMinBlocks()
 {
     if (WARPS != 4 || FAST == 0 || CUT != 6) return WARPS != 4 ? 1 : 4;
-    if (!FORCES) return sizeof(T) == 8 ? 5 : 6;
+    if (!FORCES) return (sizeof(T) == 8 && FAST == 4) ? 5 : 6;
     return (sizeof(T) == 4 && FAST == 2) ? 5 : 4;
 }
 
@@ -845,7 +857,7 @@ __global__ void __launch_bounds__(WARPS * 32, (sfMinBlocks<T, WARPS, FAST, CUT, 
                 stageCutoff<T, CAP>(S, off, n, G.cutoffSlot, b, lane);
                 slot = G.cutoffSlot;
             }
-            stageMembers<T>(mb, model, G, nullptr, lane);
+            stageMembers(mb, model, G, nullptr, lane);
             if (G.type != 2 && fastG) stageFactors<T, CAP>(S, G, lane);
             const T rc = (T)G.rc, rc2 = (T)G.rc2;
             const DevMember* mem = model.members + G.memberBegin;
@@ -1144,7 +1156,7 @@ __global__ void __launch_bounds__(WARPS * 32, (sfMinBlocks<T, WARPS, FAST, CUT, 
                 stageCutoff<T, CAP>(S, off, n, G.cutoffSlot, b, lane);
                 slot = G.cutoffSlot;
             }
-            stageMembers<T>(mb, model, G, dEdG, lane);
+            stageMembers(mb, model, G, dEdG, lane);
             const int M = G.memberCount;
             const T rc = (T)G.rc, rc2 = (T)G.rc2;
             if (G.type == 2)
