@@ -72,6 +72,7 @@ struct DevCompactMember
     int    core;           // CompactCore
     int    asym;           // asymmetric polynomial ((2 - x) x argument)
     int    calcComp;       // narrow angular: recompute the r_jk radial part (else carry the last one)
+    int    rIdx, aIdx;     // angular groups: the member's radial and angular part in the group's grid
     double rl, rc, rCenter, rScale;
     double aLeft, aRight, aCenter, aScale;
 };
@@ -84,9 +85,22 @@ struct DevCompactGroup
                            // 24 angular narrow weighted, 25 angular wide weighted
     int    e1, e2;
     int    memberBegin, memberCount;
+    int    nR, nA;         // angular groups: distinct radial and angular parts of the members
+    int    fnBegin;        // into compactFns: the nR radial parts, then the nA angular parts
     int    pad_;
     double rmin, rmax;     // group radial window (SymGrpComp*::addMember: rmin stays 0, rmax the
                            // largest upper boundary)
+};
+
+// One distinct part of an angular group's members: a radial part (core,
+// asymmetric flag, window (left, right) = (rl, rc)) or an angular part (core,
+// window in radians); center and scale as in CompactFunction::setLeftRight
+// (CompactFunction.cpp:62-76).  Every member's value over a pair is the
+// product of its radial part at r_ij and r_ik and its angular part at theta.
+struct DevCompactFn
+{
+    double left, right, center, scale;
+    int    core, asym;
 };
 
 // The groups of a model as a kernel argument (constant bank: warp-uniform
@@ -163,6 +177,9 @@ struct DevModel
     double atomicNumber[kDevMaxElements];   // neighbour weights of the weighted compact functions
     const DevCompactGroup*  compactGroups;
     const DevCompactMember* compactMembers;
+    const DevCompactFn*     compactFns;
+    int compactRows;      // largest nR of a wide angular group (at most the staged kernels' row chunk)
+    int pad2_;
 };
 
 // Per structure geometry for the neighbour build.

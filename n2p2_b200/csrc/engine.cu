@@ -223,8 +223,10 @@ void DeviceModel::release()
     cudaFree(transIndex_);
     cudaFree(compactGroups_);
     cudaFree(compactMembers_);
+    cudaFree(compactFns_);
     compactGroups_ = nullptr;
     compactMembers_ = nullptr;
+    compactFns_ = nullptr;
     groups_ = nullptr;
     members_ = nullptr;
     scaling_ = nullptr;
@@ -253,6 +255,8 @@ void DeviceModel::upload(Model const& m)
     std::vector<DevMember> members;
     std::vector<DevCompactGroup> compactGroups;
     std::vector<DevCompactMember> compactMembers;
+    std::vector<DevCompactFn> compactFns;
+    int compactRows = 0;
     std::vector<DevScaling> scaling;
     std::vector<int> rowTable;
     std::vector<double> weights;
@@ -478,6 +482,32 @@ void DeviceModel::upload(Model const& m)
                 cg.rmax = std::max(cg.rmax, s.rc);
                 compactMembers.push_back(cm);
             }
+            if (g.type != 20 && g.type != 23)
+            {
+                // the members' distinct radial parts (core, asymmetry, window) and angular parts
+                // (core, window): every member is one cell of this grid
+                std::vector<DevCompactFn> rad, ang;
+                auto find = [](std::vector<DevCompactFn>& list, DevCompactFn const& f) {
+                    for (std::size_t k = 0; k < list.size(); ++k)
+                        if (list[k].core == f.core && list[k].asym == f.asym && list[k].left == f.left &&
+                            list[k].right == f.right)
+                            return (int)k;
+                    list.push_back(f);
+                    return (int)list.size() - 1;
+                };
+                for (int mi = cg.memberBegin; mi < cg.memberBegin + cg.memberCount; ++mi)
+                {
+                    DevCompactMember& cm = compactMembers[mi];
+                    cm.rIdx = find(rad, DevCompactFn{cm.rl, cm.rc, cm.rCenter, cm.rScale, cm.core, cm.asym});
+                    cm.aIdx = find(ang, DevCompactFn{cm.aLeft, cm.aRight, cm.aCenter, cm.aScale, cm.core, 0});
+                }
+                cg.nR = (int)rad.size();
+                cg.nA = (int)ang.size();
+                cg.fnBegin = (int)compactFns.size();
+                compactFns.insert(compactFns.end(), rad.begin(), rad.end());
+                compactFns.insert(compactFns.end(), ang.begin(), ang.end());
+                if (g.type == 22 || g.type == 25) compactRows = std::max(compactRows, cg.nR);
+            }
             compactGroups.push_back(cg);
         }
         // network
@@ -562,6 +592,7 @@ void DeviceModel::upload(Model const& m)
     up((void**)&transIndex_, transIndexHost.data(), transIndexHost.size() * sizeof(int));
     up((void**)&compactGroups_, compactGroups.data(), compactGroups.size() * sizeof(DevCompactGroup));
     up((void**)&compactMembers_, compactMembers.data(), compactMembers.size() * sizeof(DevCompactMember));
+    up((void**)&compactFns_, compactFns.data(), compactFns.size() * sizeof(DevCompactFn));
     v.numCompactGroups = (int)compactGroups.size();
     v.compactTypes = 0;
     for (auto const& cg : compactGroups) v.compactTypes |= 1 << (cg.type - 20);
@@ -569,6 +600,8 @@ void DeviceModel::upload(Model const& m)
     for (std::size_t e = 0; e < m.elements.size(); ++e) v.atomicNumber[e] = (double)m.elements[e].atomicNumber;
     v.compactGroups = compactGroups_;
     v.compactMembers = compactMembers_;
+    v.compactFns = compactFns_;
+    v.compactRows = compactRows;
     v.groups = groups_;
     groupTable = DevGroupTable{};
     if (groups.size() <= (size_t)kParamGroups)
@@ -592,6 +625,7 @@ void DeviceModel::upload(Model const& m)
     mix(members.data(), members.size() * sizeof(DevMember));
     mix(compactGroups.data(), compactGroups.size() * sizeof(DevCompactGroup));
     mix(compactMembers.data(), compactMembers.size() * sizeof(DevCompactMember));
+    mix(compactFns.data(), compactFns.size() * sizeof(DevCompactFn));
     mix(&v.numElements, sizeof(int));
     mix(&v.allFast, sizeof(int));
     mix(&v.sortByDistance, sizeof(int));
@@ -1099,11 +1133,7 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         {
             launchSFValues(m, dmodel_.groupTable, v_, precision, sms_, stream_, sfShape_[0][precision]);
             launches += 2;
-            if (m.numCompactGroups > 0)
-            {
-                launchCompactValues(m, v_, sms_, stream_);
-                launches += 1;
-            }
+            if (m.numCompactGroups > 0) launches += launchCompactValues(m, v_, sms_, stream_);
             mark("sf_values");
         }
         if (checkExtrapolation)
@@ -1138,11 +1168,7 @@ void Batch::record(int flags, int precision, int checkExtrapolation, std::vector
         {
             launchSFForces(m, dmodel_.groupTable, v_, precision, sms_, stream_, sfShape_[1][precision]);
             launches += 2;
-            if (m.numCompactGroups > 0)
-            {
-                launchCompactForces(m, v_, sms_, stream_);
-                launches += 1;
-            }
+            if (m.numCompactGroups > 0) launches += launchCompactForces(m, v_, sms_, stream_);
             mark("sf_forces");
         }
         if (external_) launchGatherTargets(v_, numTargets_, tOffset_, tEntry_, targetCenter_, Ftarget_, sms_, stream_);

@@ -80,6 +80,7 @@ private:
     int* transIndex_ = nullptr;
     DevCompactGroup* compactGroups_ = nullptr;
     DevCompactMember* compactMembers_ = nullptr;
+    DevCompactFn* compactFns_ = nullptr;
 };
 
 struct StructureInput

@@ -19,8 +19,11 @@
 // the self force; it runs after the Gaussian force pass and adds to that
 // pass's per-entry forces h and self forces.  No atomics; the same result on
 // every run.
+#include <algorithm>
+
 #include "kernels.hpp"
 #include "kernels_common.cuh"
+#include "pair_rounds.cuh"
 
 namespace n2p2b200 {
 
@@ -247,7 +250,7 @@ __device__ __forceinline__ void angularChunk(DevModel const& model, BatchView co
 // One launch per compact type present: every warp walks its atoms' groups of
 // type TYPE only, so each type's kernel holds only its own state.
 template <int TYPE>
-__global__ void __launch_bounds__(128, 2) kCompactValues(DevModel model, BatchView b)
+__global__ void __launch_bounds__(128, 2) kCompactValues(DevModel model, BatchView b, int minNeighbors)
 {
     const int lane = threadIdx.x & 31;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
@@ -259,6 +262,7 @@ __global__ void __launch_bounds__(128, 2) kCompactValues(DevModel model, BatchVi
         const int64_t end = b.nbrOffset[i + 1];
         if (end > b.nbrCapacity) continue;
         const int n = (int)(end - off);
+        if (n <= minNeighbors) continue;   // staged by the wide-angular kernels
         for (int g = 0; g < E.compactCount; ++g)
         {
             DevCompactGroup const G = model.compactGroups[E.compactBegin + g];
@@ -408,7 +412,7 @@ __device__ __forceinline__ void angularForces(DevModel const& model, BatchView c
 // One launch per compact type present, in type order after the Gaussian
 // force pass; each adds its share to the per-entry and self forces.
 template <int TYPE>
-__global__ void __launch_bounds__(128, 2) kCompactForces(DevModel model, BatchView b)
+__global__ void __launch_bounds__(128, 2) kCompactForces(DevModel model, BatchView b, int minNeighbors)
 {
     const int lane = threadIdx.x & 31;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
@@ -420,6 +424,7 @@ __global__ void __launch_bounds__(128, 2) kCompactForces(DevModel model, BatchVi
         const int64_t end = b.nbrOffset[i + 1];
         if (end > b.nbrCapacity) continue;
         const int n = (int)(end - off);
+        if (n <= minNeighbors) continue;   // staged by the wide-angular kernels
         const double* dEdG = b.dEdG + (size_t)i * b.gStride;
         ForceAcc a;
         for (int sj = lane; sj < n; sj += 32)
@@ -459,6 +464,508 @@ __global__ void __launch_bounds__(128, 2) kCompactForces(DevModel model, BatchVi
     }
 }
 
+// ---------------------------------------------------------------------------
+// Wide angular types (22, 25) on staged neighbours, one block per atom.
+//
+// The members of an angular group factor into a grid: a member's term for a
+// pair (j, k) is f_r(r_ij) f_r(r_ik) f_a(theta_ijk), with f_r one of the
+// group's nR distinct radial parts and f_a one of its nA distinct angular
+// parts (DevCompactFn).  A part is 0, with derivative 0, outside its open
+// window, which is what the reference's window skips amount to
+// (SymGrpCompAngw.cpp:230-236, SymGrpCompAngwWeighted.cpp:211-218); the one
+// skip that is not a window test, the first neighbour's radial value being
+// exactly 0, zeroes that neighbour's radial derivative in the force pass.
+//   G pass: S[r][a] = sum over pairs of f_r(r_ij) f_r(r_ik) f_a(theta)
+//           (times Z_j Z_k for type 25); each member reads its cell.
+//   force:  W[r][a] = sum of dE/dG scalingFactor over the cell's members; per
+//           pair U_r = sum_a W[r][a] f_a, V_r = sum_a W[r][a] f_a',
+//           B_j = sum_r f_r'(r_ij) f_r(r_ik) U_r (B_k likewise), and
+//           C = dtheta/dcos sum_r f_r(r_ij) f_r(r_ik) V_r; with d = r_i - r_j
+//           the force on j is h_j = (B_j / r_ij - C cos / r_ij^2) d_j +
+//           C / (r_ij r_ik) d_k (and j <-> k), and the centre's is -sum_j h_j.
+// The atom's neighbours are staged sorted by element (stable), so a group's
+// pairs are the rounds of matchings of one element block (tournament) or of
+// two blocks (diagonals); the radial parts of the group's neighbours are
+// staged per group.  The G pass gives every thread a strided share of the
+// pairs and sums the grid in registers; the force pass gives each warp
+// batches of 32 consecutive pairs and adds a batch round by round to the
+// warp's own force array, so no slot is written twice at once and every sum
+// runs in a fixed order.
+constexpr int kWideRows = 10;   // radial parts per chunk (grid rows in registers)
+constexpr int kWideCols = 6;    // angular parts per chunk
+constexpr int kWideCells = 64;  // kWideRows x kWideCols cells, padded for the warp reduction
+constexpr int kWideCap = 256;   // staged neighbours; atoms with more run the direct kernels
+constexpr int kWideWarps = 4;
+
+static_assert(kWideRows * kWideCols <= kWideCells, "grid chunk exceeds the reduced cells");
+
+// Value and derivative of one part at x (0 outside the open window).
+__device__ __forceinline__ void compactPartFdf(DevCompactFn const& f, double x, double& v, double& dv)
+{
+    v = 0.0;
+    dv = 0.0;
+    if (x > f.left && x < f.right) compactFdf(f.core, f.asym, f.center, f.scale, x, v, dv);
+}
+
+// The block's shared memory: per staged slot the neighbour's d = r_i - r_j,
+// r, 1/r, element and list position; the group chunk's parts and radial
+// values (and derivatives); the force pass's per-warp force arrays.
+struct WideSmem
+{
+    double *x, *y, *z, *r, *rinv;   // [kWideCap]
+    double *rad, *drad;             // [rows][kWideCap]
+    double *h;                      // [warps][3][kWideCap], force pass
+    double *cell;                   // G pass: [warps][kWideCells] partial sums; force pass: W [kWideCells]
+    DevCompactFn* fn;               // [kWideRows + kWideCols]: radial parts, then angular parts
+    int* blockBegin;                // [kDevMaxElements + 1]
+    short* perm;                    // [kWideCap] slot -> position in the atom's list
+    unsigned char* el;              // [kWideCap]
+};
+
+__host__ __device__ inline size_t wideSmemBytes(int rows, int warps, bool forces)
+{
+    size_t d = 5 * kWideCap + (size_t)rows * kWideCap * (forces ? 2 : 1) +
+               (forces ? (size_t)warps * 3 * kWideCap + kWideCells : (size_t)warps * kWideCells);
+    return d * sizeof(double) + (kWideRows + kWideCols) * sizeof(DevCompactFn) + (kDevMaxElements + 1) * sizeof(int) +
+           kWideCap * sizeof(short) + kWideCap;
+}
+
+__device__ __forceinline__ WideSmem wideCarve(char* base, int rows, int warps, bool forces)
+{
+    WideSmem S;
+    double* d = reinterpret_cast<double*>(base);
+    S.x = d;
+    S.y = d + kWideCap;
+    S.z = d + 2 * kWideCap;
+    S.r = d + 3 * kWideCap;
+    S.rinv = d + 4 * kWideCap;
+    d += 5 * kWideCap;
+    S.rad = d;
+    d += rows * kWideCap;
+    S.drad = forces ? d : nullptr;
+    if (forces) d += rows * kWideCap;
+    S.h = forces ? d : nullptr;
+    if (forces) d += warps * 3 * kWideCap;
+    S.cell = d;
+    d += forces ? kWideCells : warps * kWideCells;
+    S.fn = reinterpret_cast<DevCompactFn*>(d);
+    S.blockBegin = reinterpret_cast<int*>(S.fn + kWideRows + kWideCols);
+    S.perm = reinterpret_cast<short*>(S.blockBegin + kDevMaxElements + 1);
+    S.el = reinterpret_cast<unsigned char*>(S.perm + kWideCap);
+    return S;
+}
+
+// Stage the atom's n <= kWideCap neighbours sorted by element (stable).
+__device__ void wideStage(WideSmem const& S, DevModel const& model, BatchView const& b, int64_t off, int n, int tid,
+                          int threads)
+{
+    if (tid < 32)
+    {
+        const int lane = tid;
+        const int ne = model.numElements;
+        int count = 0;   // lane k < ne: entries of element k
+        for (int c = 0; c < n; c += 32)
+        {
+            const int e = c + lane < n ? (int)b.nbrElem[off + c + lane] : -1;
+            for (int k = 0; k < ne; ++k)
+            {
+                const int cnt = __popc(__ballot_sync(kFullMask, e == k));
+                if (lane == k) count += cnt;
+            }
+        }
+        int incl = count;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int t = __shfl_up_sync(kFullMask, incl, o);
+            if (lane >= o) incl += t;
+        }
+        int begin = incl - count;   // lane k <= ne: first slot of element k (lane ne: n)
+        if (lane <= ne) S.blockBegin[lane] = begin;
+        const unsigned below = (1u << lane) - 1u;
+        for (int c = 0; c < n; c += 32)
+        {
+            const int e = c + lane < n ? (int)b.nbrElem[off + c + lane] : -1;
+            for (int k = 0; k < ne; ++k)
+            {
+                const unsigned mask = __ballot_sync(kFullMask, e == k);
+                const int bk = __shfl_sync(kFullMask, begin, k);
+                if (e == k) S.perm[bk + __popc(mask & below)] = (short)(c + lane);
+                if (lane == k) begin += __popc(mask);
+            }
+        }
+    }
+    __syncthreads();
+    for (int s = tid; s < n; s += threads)
+    {
+        const int64_t e = off + S.perm[s];
+        const double d = b.nbrD[e];
+        S.x[s] = b.nbrDx[e];
+        S.y[s] = b.nbrDy[e];
+        S.z[s] = b.nbrDz[e];
+        S.r[s] = d;
+        S.rinv[s] = 1.0 / d;
+        S.el[s] = b.nbrElem[e];
+    }
+    __syncthreads();
+}
+
+// A group's pairs: the neighbours of its element pair (all neighbours for the
+// weighted type) as rounds of matchings; ns slots carry its radial values.
+struct WidePairs
+{
+    Phase ph;
+    int A0, nA, B0, nB, ns;
+};
+
+template <bool WEIGHTED>
+__device__ __forceinline__ WidePairs widePairs(WideSmem const& S, DevCompactGroup const& G, int n)
+{
+    WidePairs P;
+    bool same = true;
+    if (WEIGHTED)
+    {
+        P.A0 = 0;
+        P.nA = n;
+        P.B0 = 0;
+        P.nB = 0;
+    }
+    else
+    {
+        P.A0 = S.blockBegin[G.e1];
+        P.nA = S.blockBegin[G.e1 + 1] - P.A0;
+        P.B0 = S.blockBegin[G.e2];
+        P.nB = S.blockBegin[G.e2 + 1] - P.B0;
+        same = G.e1 == G.e2;
+        if (same) P.nB = 0;
+    }
+    P.ns = P.nA + P.nB;
+    P.ph = Phase{3, 0, 0, 0, 0, 0, 1};
+    roundPhases(P.A0, P.nA, P.B0, P.nB, same, &P.ph);
+    return P;
+}
+
+// Parts of the chunk (rows r0.., columns a0..) and the radial values of the
+// group's slots.
+template <bool FORCES>
+__device__ __forceinline__ void wideStageChunk(WideSmem const& S, DevModel const& model, DevCompactGroup const& G,
+                                               WidePairs const& P, int r0, int nRc, int a0, int nAc, int tid,
+                                               int threads)
+{
+    if (tid < nRc) S.fn[tid] = model.compactFns[G.fnBegin + r0 + tid];
+    else if (tid >= kWideRows && tid < kWideRows + nAc)
+        S.fn[tid] = model.compactFns[G.fnBegin + G.nR + a0 + tid - kWideRows];
+    __syncthreads();
+    for (int k = tid; k < nRc * P.ns; k += threads)
+    {
+        const int rr = k / P.ns;
+        const int j = k - rr * P.ns;
+        const int s = j < P.nA ? P.A0 + j : P.B0 + (j - P.nA);
+        double f, df;
+        compactPartFdf(S.fn[rr], S.r[s], f, df);
+        S.rad[rr * kWideCap + s] = f;
+        if (FORCES) S.drad[rr * kWideCap + s] = df;
+    }
+}
+
+// Sums v[0..63] over the warp by halving exchanges; afterwards lane l holds
+// the sums of cells 2l and 2l + 1 in v[0] and v[1].
+template <int L, int O>
+__device__ __forceinline__ void halveCells(double (&v)[kWideCells], int lane)
+{
+    const bool up = (lane & O) != 0;
+#pragma unroll
+    for (int q = 0; q < L / 2; ++q)
+    {
+        const double send = up ? v[q] : v[q + L / 2];
+        const double keep = up ? v[q + L / 2] : v[q];
+        v[q] = keep + __shfl_xor_sync(kFullMask, send, O);
+    }
+}
+
+__device__ __forceinline__ void warpReduceCells(double (&v)[kWideCells], int lane)
+{
+    halveCells<64, 16>(v, lane);
+    halveCells<32, 8>(v, lane);
+    halveCells<16, 4>(v, lane);
+    halveCells<8, 2>(v, lane);
+    halveCells<4, 1>(v, lane);
+}
+
+template <int TYPE>
+__device__ __forceinline__ bool hasType(DevModel const& model, DevElement const& E)
+{
+    for (int g = 0; g < E.compactCount; ++g)
+        if (model.compactGroups[E.compactBegin + g].type == TYPE) return true;
+    return false;
+}
+
+template <int TYPE>
+__global__ void __launch_bounds__(kWideWarps * 32, 2) kCompactWideValues(DevModel model, BatchView b, int rows)
+{
+    constexpr bool WEIGHTED = TYPE == 25;
+    constexpr int T = kWideWarps * 32;
+    extern __shared__ __align__(16) char smemRaw[];
+    const WideSmem S = wideCarve(smemRaw, rows, kWideWarps, false);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = blockIdx.x; i < b.N; i += gridDim.x)
+    {
+        DevElement const& E = model.el[b.elem[i]];
+        if (!hasType<TYPE>(model, E)) continue;
+        const int64_t off = b.nbrOffset[i];
+        const int64_t end = b.nbrOffset[i + 1];
+        const int n = (int)(end - off);
+        if (end > b.nbrCapacity || n > kWideCap) continue;
+        wideStage(S, model, b, off, n, tid, T);
+        for (int g = 0; g < E.compactCount; ++g)
+        {
+            DevCompactGroup const G = model.compactGroups[E.compactBegin + g];
+            if (G.type != TYPE) continue;
+            const WidePairs P = widePairs<WEIGHTED>(S, G, n);
+            const DevCompactMember* mem = model.compactMembers + G.memberBegin;
+            const int q = T / P.ph.minor, rem = T - q * P.ph.minor;
+            for (int r0 = 0; r0 < G.nR; r0 += kWideRows)
+                for (int a0 = 0; a0 < G.nA; a0 += kWideCols)
+                {
+                    const int nRc = min(kWideRows, G.nR - r0), nAc = min(kWideCols, G.nA - a0);
+                    wideStageChunk<false>(S, model, G, P, r0, nRc, a0, nAc, tid, T);
+                    __syncthreads();
+                    double acc[kWideCells];
+#pragma unroll
+                    for (int c = 0; c < kWideCells; ++c) acc[c] = 0.0;
+                    Cursor cur;
+                    cur.init(P.ph, tid);
+                    for (int p = tid; p < P.ph.count; p += T, cur.advance(P.ph, q, rem))
+                    {
+                        int u, v;
+                        if (!cur.slots(P.ph, u, v)) continue;
+                        const double cost =
+                            (S.x[u] * S.x[v] + S.y[u] * S.y[v] + S.z[u] * S.z[v]) * (S.rinv[u] * S.rinv[v]);
+                        if (!(cost > -1.0 && cost < 1.0)) continue;
+                        const double acost = acos(cost);
+                        const double zw = WEIGHTED ? model.atomicNumber[S.el[u]] * model.atomicNumber[S.el[v]] : 1.0;
+                        double ang[kWideCols];
+#pragma unroll
+                        for (int a = 0; a < kWideCols; ++a)
+                        {
+                            double f = 0.0, df;
+                            if (a < nAc) compactPartFdf(S.fn[kWideRows + a], acost, f, df);
+                            ang[a] = WEIGHTED ? f * zw : f;
+                        }
+#pragma unroll
+                        for (int r = 0; r < kWideRows; ++r)
+                        {
+                            if (r < nRc)
+                            {
+                                const double pr = S.rad[r * kWideCap + u] * S.rad[r * kWideCap + v];
+#pragma unroll
+                                for (int a = 0; a < kWideCols; ++a) acc[r * kWideCols + a] += pr * ang[a];
+                            }
+                        }
+                    }
+                    warpReduceCells(acc, lane);
+                    S.cell[warp * kWideCells + 2 * lane] = acc[0];
+                    S.cell[warp * kWideCells + 2 * lane + 1] = acc[1];
+                    __syncthreads();
+                    for (int mi = tid; mi < G.memberCount; mi += T)
+                    {
+                        DevCompactMember const& M = mem[mi];
+                        const int rr = M.rIdx - r0, aa = M.aIdx - a0;
+                        if (rr < 0 || rr >= nRc || aa < 0 || aa >= nAc) continue;
+                        const int c = rr * kWideCols + aa;
+                        double sum = S.cell[c];
+                        for (int w = 1; w < kWideWarps; ++w) sum += S.cell[w * kWideCells + c];
+                        b.G[(size_t)i * b.gStride + M.sf] = scaleG(model.scaling[E.sfBegin + M.sf], sum);
+                    }
+                    __syncthreads();
+                }
+        }
+    }
+}
+
+template <int TYPE>
+__global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevModel model, BatchView b, int rows)
+{
+    constexpr bool WEIGHTED = TYPE == 25;
+    constexpr int T = kWideWarps * 32;
+    extern __shared__ __align__(16) char smemRaw[];
+    const WideSmem S = wideCarve(smemRaw, rows, kWideWarps, true);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* hw = S.h + warp * 3 * kWideCap;   // this warp's force array
+    for (int k = tid; k < kWideWarps * 3 * kWideCap; k += T) S.h[k] = 0.0;
+    for (int i = blockIdx.x; i < b.N; i += gridDim.x)
+    {
+        DevElement const& E = model.el[b.elem[i]];
+        if (!hasType<TYPE>(model, E)) continue;
+        const int64_t off = b.nbrOffset[i];
+        const int64_t end = b.nbrOffset[i + 1];
+        const int n = (int)(end - off);
+        if (end > b.nbrCapacity || n > kWideCap) continue;
+        const double* dEdG = b.dEdG + (size_t)i * b.gStride;
+        wideStage(S, model, b, off, n, tid, T);
+        for (int g = 0; g < E.compactCount; ++g)
+        {
+            DevCompactGroup const G = model.compactGroups[E.compactBegin + g];
+            if (G.type != TYPE) continue;
+            const WidePairs P = widePairs<WEIGHTED>(S, G, n);
+            if (P.ph.count == 0) continue;
+            const DevCompactMember* mem = model.compactMembers + G.memberBegin;
+            const int q = (32 * kWideWarps) / P.ph.minor, rem = 32 * kWideWarps - q * P.ph.minor;
+            for (int r0 = 0; r0 < G.nR; r0 += kWideRows)
+                for (int a0 = 0; a0 < G.nA; a0 += kWideCols)
+                {
+                    const int nRc = min(kWideRows, G.nR - r0), nAc = min(kWideCols, G.nA - a0);
+                    wideStageChunk<true>(S, model, G, P, r0, nRc, a0, nAc, tid, T);
+                    // cell weights, members summed in their order
+                    if (tid < kWideCells)
+                    {
+                        double w = 0.0;
+                        for (int mi = 0; mi < G.memberCount; ++mi)
+                        {
+                            DevCompactMember const& M = mem[mi];
+                            const int rr = M.rIdx - r0, aa = M.aIdx - a0;
+                            if (rr < 0 || rr >= nRc || aa < 0 || aa >= nAc || rr * kWideCols + aa != tid) continue;
+                            w += dEdG[M.sf] * model.scaling[E.sfBegin + M.sf].scalingFactor;
+                        }
+                        S.cell[tid] = w;
+                    }
+                    __syncthreads();
+                    Cursor cur;
+                    cur.init(P.ph, 32 * warp + lane);
+                    for (int p0 = 32 * warp; p0 < P.ph.count; p0 += 32 * kWideWarps, cur.advance(P.ph, q, rem))
+                    {
+                        int u = 0, v = 0;
+                        bool ok = p0 + lane < P.ph.count && cur.slots(P.ph, u, v);
+                        double cu = 0.0, cv = 0.0, gm = 0.0;
+                        if (ok)
+                        {
+                            const double riu = S.rinv[u], riv = S.rinv[v];
+                            const double cost = (S.x[u] * S.x[v] + S.y[u] * S.y[v] + S.z[u] * S.z[v]) * (riu * riv);
+                            ok = cost > -1.0 && cost < 1.0;
+                            if (ok)
+                            {
+                                const double acost = acos(cost);
+                                const double dacost = -1.0 / sqrt(1.0 - cost * cost);
+                                double ang[kWideCols], dang[kWideCols];
+#pragma unroll
+                                for (int a = 0; a < kWideCols; ++a)
+                                {
+                                    ang[a] = 0.0;
+                                    dang[a] = 0.0;
+                                    if (a < nAc) compactPartFdf(S.fn[kWideRows + a], acost, ang[a], dang[a]);
+                                }
+                                // the reference's first neighbour of the pair is the lower list index
+                                const bool firstU = S.perm[u] < S.perm[v];
+                                double Bu = 0.0, Bv = 0.0, A = 0.0;
+#pragma unroll
+                                for (int r = 0; r < kWideRows; ++r)
+                                {
+                                    if (r < nRc)
+                                    {
+                                        const double ru = S.rad[r * kWideCap + u], rv = S.rad[r * kWideCap + v];
+                                        double dru = S.drad[r * kWideCap + u], drv = S.drad[r * kWideCap + v];
+                                        if (firstU ? ru == 0.0 : rv == 0.0)
+                                        {
+                                            if (firstU) dru = 0.0;
+                                            else drv = 0.0;
+                                        }
+                                        double U = 0.0, V = 0.0;
+#pragma unroll
+                                        for (int a = 0; a < kWideCols; ++a)
+                                        {
+                                            const double w = S.cell[r * kWideCols + a];
+                                            U += w * ang[a];
+                                            V += w * dang[a];
+                                        }
+                                        Bu += dru * rv * U;
+                                        Bv += ru * drv * U;
+                                        A += ru * rv * V;
+                                    }
+                                }
+                                double C = A * dacost;
+                                if (WEIGHTED)
+                                {
+                                    const double zw = model.atomicNumber[S.el[u]] * model.atomicNumber[S.el[v]];
+                                    Bu *= zw;
+                                    Bv *= zw;
+                                    C *= zw;
+                                }
+                                cu = Bu * riu - C * cost * riu * riu;
+                                cv = Bv * riv - C * cost * riv * riv;
+                                gm = C * (riu * riv);
+                            }
+                        }
+                        // add the batch one round at a time: inside a round no slot occurs twice
+                        const int rnd = cur.a;
+                        const int last = min(31, P.ph.count - 1 - p0);
+                        const int rLo = __shfl_sync(kFullMask, rnd, 0);
+                        const int rHi = __shfl_sync(kFullMask, rnd, last);
+                        for (int rr = rLo; rr <= rHi; ++rr)
+                        {
+                            if (ok && rnd == rr)
+                            {
+                                const double xu = S.x[u], yu = S.y[u], zu = S.z[u];
+                                const double xv = S.x[v], yv = S.y[v], zv = S.z[v];
+                                hw[u] += cu * xu + gm * xv;
+                                hw[kWideCap + u] += cu * yu + gm * yv;
+                                hw[2 * kWideCap + u] += cu * zu + gm * zv;
+                                hw[v] += cv * xv + gm * xu;
+                                hw[kWideCap + v] += cv * yv + gm * yu;
+                                hw[2 * kWideCap + v] += cv * zv + gm * zu;
+                            }
+                            __syncwarp();
+                        }
+                    }
+                    __syncthreads();
+                }
+        }
+        // per-entry forces (warp arrays summed in order) and the centre's share
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int s = tid; s < n; s += T)
+        {
+            double f[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+                f[c] = 0.0;
+                for (int w = 0; w < kWideWarps; ++w)
+                {
+                    f[c] += S.h[(w * 3 + c) * kWideCap + s];
+                    S.h[(w * 3 + c) * kWideCap + s] = 0.0;
+                }
+            }
+            if (f[0] != 0.0 || f[1] != 0.0 || f[2] != 0.0)
+            {
+                const int64_t e = off + S.perm[s];
+                b.hx[e] += f[0];
+                b.hy[e] += f[1];
+                b.hz[e] += f[2];
+            }
+            sx -= f[0];
+            sy -= f[1];
+            sz -= f[2];
+        }
+        sx = warpSum(sx);
+        sy = warpSum(sy);
+        sz = warpSum(sz);
+        if (lane == 0)
+        {
+            S.cell[3 * warp + 0] = sx;
+            S.cell[3 * warp + 1] = sy;
+            S.cell[3 * warp + 2] = sz;
+        }
+        __syncthreads();
+        if (tid == 0)
+        {
+            double t[3] = {0.0, 0.0, 0.0};
+            for (int w = 0; w < kWideWarps; ++w)
+                for (int c = 0; c < 3; ++c) t[c] += S.cell[3 * w + c];
+            if (t[0] != 0.0 || t[1] != 0.0 || t[2] != 0.0)
+                for (int c = 0; c < 3; ++c) b.fSelf[3 * (size_t)i + c] += t[c];
+        }
+        __syncthreads();
+    }
+}
+
 } // namespace
 
 namespace {
@@ -471,28 +978,76 @@ int compactBlocks(BatchView const& b, int sms)
     return blocks;
 }
 
-} // namespace
-
-void launchCompactValues(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
+// One block per atom, at most perSM resident blocks per SM.
+int wideBlocks(BatchView const& b, int sms, int perSM)
 {
-    const int blocks = compactBlocks(b, sms);
-    if (m.compactTypes & (1 << 0)) kCompactValues<20><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 1)) kCompactValues<21><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 2)) kCompactValues<22><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 3)) kCompactValues<23><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 4)) kCompactValues<24><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 5)) kCompactValues<25><<<blocks, 128, 0, st>>>(m, b);
+    return std::max(1, std::min(b.N, sms * perSM));
 }
 
-void launchCompactForces(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
+} // namespace
+
+int launchCompactValues(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
 {
     const int blocks = compactBlocks(b, sms);
-    if (m.compactTypes & (1 << 0)) kCompactForces<20><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 1)) kCompactForces<21><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 2)) kCompactForces<22><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 3)) kCompactForces<23><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 4)) kCompactForces<24><<<blocks, 128, 0, st>>>(m, b);
-    if (m.compactTypes & (1 << 5)) kCompactForces<25><<<blocks, 128, 0, st>>>(m, b);
+    const int rows = std::max(1, std::min(m.compactRows, kWideRows));
+    int launches = 0;
+    auto direct = [&](auto kernel, int minNeighbors) {
+        kernel<<<blocks, 128, 0, st>>>(m, b, minNeighbors);
+        ++launches;
+    };
+    auto wide = [&](auto kernel) {
+        const size_t smem = wideSmemBytes(rows, kWideWarps, false);
+        setDynamicSmemOnce(reinterpret_cast<const void*>(kernel), smem);
+        kernel<<<wideBlocks(b, sms, 4), kWideWarps * 32, smem, st>>>(m, b, rows);
+        ++launches;
+    };
+    if (m.compactTypes & (1 << 0)) direct(kCompactValues<20>, -1);
+    if (m.compactTypes & (1 << 1)) direct(kCompactValues<21>, -1);
+    if (m.compactTypes & (1 << 2))
+    {
+        wide(kCompactWideValues<22>);
+        direct(kCompactValues<22>, kWideCap);
+    }
+    if (m.compactTypes & (1 << 3)) direct(kCompactValues<23>, -1);
+    if (m.compactTypes & (1 << 4)) direct(kCompactValues<24>, -1);
+    if (m.compactTypes & (1 << 5))
+    {
+        wide(kCompactWideValues<25>);
+        direct(kCompactValues<25>, kWideCap);
+    }
+    return launches;
+}
+
+int launchCompactForces(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
+{
+    const int blocks = compactBlocks(b, sms);
+    const int rows = std::max(1, std::min(m.compactRows, kWideRows));
+    int launches = 0;
+    auto direct = [&](auto kernel, int minNeighbors) {
+        kernel<<<blocks, 128, 0, st>>>(m, b, minNeighbors);
+        ++launches;
+    };
+    auto wide = [&](auto kernel) {
+        const size_t smem = wideSmemBytes(rows, kWideWarps, true);
+        setDynamicSmemOnce(reinterpret_cast<const void*>(kernel), smem);
+        kernel<<<wideBlocks(b, sms, 3), kWideWarps * 32, smem, st>>>(m, b, rows);
+        ++launches;
+    };
+    if (m.compactTypes & (1 << 0)) direct(kCompactForces<20>, -1);
+    if (m.compactTypes & (1 << 1)) direct(kCompactForces<21>, -1);
+    if (m.compactTypes & (1 << 2))
+    {
+        wide(kCompactWideForces<22>);
+        direct(kCompactForces<22>, kWideCap);
+    }
+    if (m.compactTypes & (1 << 3)) direct(kCompactForces<23>, -1);
+    if (m.compactTypes & (1 << 4)) direct(kCompactForces<24>, -1);
+    if (m.compactTypes & (1 << 5))
+    {
+        wide(kCompactWideForces<25>);
+        direct(kCompactForces<25>, kWideCap);
+    }
+    return launches;
 }
 
 } // namespace n2p2b200

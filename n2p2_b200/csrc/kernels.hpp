@@ -126,11 +126,11 @@ void launchMaskOffsets(DevModel const& m, BatchView const& b, int sms, cudaStrea
 void launchNetworkTC(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st);
 void launchEnergySum(BatchView const& b, cudaStream_t st);
 void launchGatherForces(BatchView const& b, int sms, cudaStream_t st);
-// Compact symmetry functions (types 20, 22; k_compact.cu): G of their
+// Compact symmetry functions (types 20-25; k_compact.cu): G of their
 // members, then (after the Gaussian force pass) their forces added to h and
-// the self forces.
-void launchCompactValues(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
-void launchCompactForces(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
+// the self forces.  Both return the number of kernels launched.
+int launchCompactValues(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
+int launchCompactForces(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 // Per element and function: min, max, sum, sum of squares of the unscaled G
 // (result [numElements][4][maxSF]; partial [numElements][maxChunks][4][maxSF],
 // maxChunks = ceil(largest element count / 1024)).
