@@ -73,6 +73,8 @@ struct DevCompactMember
     int    asym;           // asymmetric polynomial ((2 - x) x argument)
     int    calcComp;       // narrow angular: recompute the r_jk radial part (else carry the last one)
     int    rIdx, aIdx;     // angular groups: the member's radial and angular part in the group's grid
+    int    impure;         // narrow groups: index among the members whose carried j-k radial part may
+                           // come from another radial part (see DevCompactGroup::walkBegin), else -1
     double rl, rc, rCenter, rScale;
     double aLeft, aRight, aCenter, aScale;
 };
@@ -87,10 +89,22 @@ struct DevCompactGroup
     int    memberBegin, memberCount;
     int    nR, nA;         // angular groups: distinct radial and angular parts of the members
     int    fnBegin;        // into compactFns: the nR radial parts, then the nA angular parts
-    int    pad_;
+    int    walkBegin, walkEnd;   // narrow groups: the members replayed per pair for the carried j-k
+                                 // radial part of the impure members (empty when there are none)
+    int    numImpure;
     double rmin, rmax;     // group radial window (SymGrpComp*::addMember: rmin stays 0, rmax the
                            // largest upper boundary)
 };
+
+constexpr int kCorePoly2 = 6;   // core type "p2" (CoreFunction::Type, numbering of coreFdf)
+
+// Limits of the staged compact angular kernels (k_compact.cu): distinct
+// radial / angular parts per grid chunk, and for the narrow types (one chunk)
+// the impure members and the members replayed per pair.
+constexpr int kCompactStageRows = 10;
+constexpr int kCompactStageCols = 6;
+constexpr int kCompactImpure = 6;
+constexpr int kCompactWalk = 16;
 
 // One distinct part of an angular group's members: a radial part (core,
 // asymmetric flag, window (left, right) = (rl, rc)) or an angular part (core,
@@ -178,7 +192,9 @@ struct DevModel
     const DevCompactGroup*  compactGroups;
     const DevCompactMember* compactMembers;
     const DevCompactFn*     compactFns;
-    int compactRows;      // largest nR of a wide angular group (at most the staged kernels' row chunk)
+    int compactRows;      // largest nR of a wide angular group
+    int compactAngCore;   // the core of every angular part of the staged angular groups, or 0 if they differ
+    int compactNarrowStaged;   // every narrow group fits the staged kernels (one grid chunk, a short walk)
     int pad2_;
 };
 

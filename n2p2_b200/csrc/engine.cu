@@ -257,6 +257,8 @@ void DeviceModel::upload(Model const& m)
     std::vector<DevCompactMember> compactMembers;
     std::vector<DevCompactFn> compactFns;
     int compactRows = 0;
+    int compactAngCore = -1;   // -1: no staged angular part seen yet
+    int compactNarrowStaged = 1;
     std::vector<DevScaling> scaling;
     std::vector<int> rowTable;
     std::vector<double> weights;
@@ -506,7 +508,48 @@ void DeviceModel::upload(Model const& m)
                 cg.fnBegin = (int)compactFns.size();
                 compactFns.insert(compactFns.end(), rad.begin(), rad.end());
                 compactFns.insert(compactFns.end(), ang.begin(), ang.end());
-                if (g.type == 22 || g.type == 25) compactRows = std::max(compactRows, cg.nR);
+                cg.walkBegin = cg.walkEnd = cg.numImpure = 0;
+                bool staged = true;
+                if (g.type == 21 || g.type == 24)
+                {
+                    // The reference carries the j-k radial part along a run of members that do not
+                    // recompute it (calculateComp, SymGrpCompAngn.cpp:253-296): a member's value uses
+                    // the radial part of the run's last recomputing member.  A member whose run since
+                    // its last calculateComp member holds only its own radial part gets its own part
+                    // whatever the pair's skips; the others ("impure") are replayed per pair.
+                    int c0 = 0, numImpure = 0, wb = -1, we = 0;
+                    for (int k = 0; k < cg.memberCount; ++k)
+                    {
+                        DevCompactMember& cm = compactMembers[cg.memberBegin + k];
+                        if (cm.calcComp) c0 = k;
+                        bool impure = false;
+                        for (int j = c0; j < k; ++j)
+                            if (compactMembers[cg.memberBegin + j].rIdx != cm.rIdx) impure = true;
+                        cm.impure = impure ? numImpure++ : -1;
+                        if (impure)
+                        {
+                            if (wb < 0) wb = c0;
+                            we = k + 1;
+                        }
+                    }
+                    cg.numImpure = numImpure;
+                    if (numImpure > 0)
+                    {
+                        cg.walkBegin = wb;
+                        cg.walkEnd = we;
+                    }
+                    staged = cg.nR <= kCompactStageRows && cg.nA <= kCompactStageCols &&
+                             numImpure <= kCompactImpure && we - std::max(wb, 0) <= kCompactWalk;
+                    if (!staged) compactNarrowStaged = 0;
+                }
+                else
+                    for (int k = 0; k < cg.memberCount; ++k) compactMembers[cg.memberBegin + k].impure = -1;
+                if (staged)
+                {
+                    compactRows = std::max(compactRows, cg.nR);
+                    for (auto const& f : ang)
+                        compactAngCore = (compactAngCore == -1 || compactAngCore == f.core) ? f.core : 0;
+                }
             }
             compactGroups.push_back(cg);
         }
@@ -602,6 +645,8 @@ void DeviceModel::upload(Model const& m)
     v.compactMembers = compactMembers_;
     v.compactFns = compactFns_;
     v.compactRows = compactRows;
+    v.compactAngCore = std::max(compactAngCore, 0);
+    v.compactNarrowStaged = compactNarrowStaged;
     v.groups = groups_;
     groupTable = DevGroupTable{};
     if (groups.size() <= (size_t)kParamGroups)

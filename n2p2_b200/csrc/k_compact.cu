@@ -486,20 +486,32 @@ __global__ void __launch_bounds__(128, 2) kCompactForces(DevModel model, BatchVi
 // The atom's neighbours are staged sorted by element (stable), so a group's
 // pairs are the rounds of matchings of one element block (tournament) or of
 // two blocks (diagonals); the radial parts of the group's neighbours are
-// staged per group.  The G pass gives every thread a strided share of the
-// pairs and sums the grid in registers; the force pass gives each warp
-// batches of 32 consecutive pairs and adds a batch round by round to the
-// warp's own force array, so no slot is written twice at once and every sum
-// runs in a fixed order.
-constexpr int kWideRows = 10;   // radial parts per chunk (grid rows in registers)
-constexpr int kWideCols = 6;    // angular parts per chunk
-constexpr int kWideCells = 64;  // kWideRows x kWideCols cells, padded for the warp reduction
+// staged per group.  Each warp takes batches of 32 consecutive pairs.  In
+// the G pass a batch is a k = 32 slice of the product S = P^T A, P the
+// pairs' radial products f_r f_r (32 x nR) and A their angular parts
+// (32 x nA), run on the FP64 tensor cores (mma m8n8k4, FP64 accumulation)
+// from a per-warp shared tile; the force pass adds a batch round by round to
+// the warp's own force array, so no slot is written twice at once.  Every
+// sum runs in a fixed order.
+constexpr int kWideRows = kCompactStageRows;   // radial parts per chunk
+constexpr int kWideCols = kCompactStageCols;   // angular parts per chunk
 constexpr int kWideCap = 256;   // staged neighbours; atoms with more run the direct kernels
 constexpr int kWideWarps = 4;
+constexpr int kCellStride = 8;  // G pass cell sums: row r, column a at r * 8 + a
+constexpr int kTileStride = 36; // per-warp tile: 32 pairs per row, padded against bank conflicts
 
-static_assert(kWideRows * kWideCols <= kWideCells, "grid chunk exceeds the reduced cells");
+// G-pass tile rows: the grid's, and for the narrow types one more per impure
+// member (kWideRows + kCompactImpure = 16, the two 8-row halves of the mma).
+template <bool NARROW>
+__host__ __device__ constexpr int tileRows() { return NARROW ? 16 : kWideRows; }
+template <bool NARROW>
+__host__ __device__ constexpr int tileDoubles() { return (tileRows<NARROW>() + kWideCols) * kTileStride; }
+template <bool NARROW>
+__host__ __device__ constexpr int cellCount() { return tileRows<NARROW>() * kCellStride; }
+static_assert(kWideRows + kCompactImpure <= 16, "impure rows beyond the mma halves");
 
-// Value and derivative of one part at x (0 outside the open window).
+// Value and derivative of a radial part at r (0 outside the open window):
+// CompactFunction::fdf with the part's core and asymmetry.
 __device__ __forceinline__ void compactPartFdf(DevCompactFn const& f, double x, double& v, double& dv)
 {
     v = 0.0;
@@ -507,30 +519,65 @@ __device__ __forceinline__ void compactPartFdf(DevCompactFn const& f, double x, 
     if (x > f.left && x < f.right) compactFdf(f.core, f.asym, f.center, f.scale, x, v, dv);
 }
 
+// The same for an angular part (symmetric core), the core fixed at compile
+// time when ACORE != 0 (every angular part of the model has that core).
+template <int ACORE>
+__device__ __forceinline__ void angularPartFdf(DevCompactFn const& f, double x, double& v, double& dv)
+{
+    v = 0.0;
+    dv = 0.0;
+    if (x > f.left && x < f.right)
+    {
+        const double u = (x - f.center) * f.scale;
+        double fx, dfx;
+        coreFdf(ACORE != 0 ? ACORE : f.core, fabs(u), fx, dfx);
+        v = fx;
+        dv = dfx * copysign(f.scale, u);
+    }
+}
+
+// D = A B + D for one 8 x 4 by 4 x 8 FP64 block (mma.sync m8n8k4): lane l
+// holds A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void mmaF64(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 // The block's shared memory: per staged slot the neighbour's d = r_i - r_j,
 // r, 1/r, element and list position; the group chunk's parts and radial
-// values (and derivatives); the force pass's per-warp force arrays.
+// values (and derivatives); the G pass's per-warp tiles and cell sums, the
+// force pass's per-warp force arrays and cell weights.
 struct WideSmem
 {
     double *x, *y, *z, *r, *rinv;   // [kWideCap]
     double *rad, *drad;             // [rows][kWideCap]
-    double *h;                      // [warps][3][kWideCap], force pass
-    double *cell;                   // G pass: [warps][kWideCells] partial sums; force pass: W [kWideCells]
+    double *h;                      // force pass: [warps][3][kWideCap]
+    double *tile;                   // G pass: [warps][tile rows + kWideCols][kTileStride]
+    double *cell;                   // G pass: [warps][tile rows * kCellStride] sums; force pass: W [kWideRows][kWideCols]
+    double *walkW;                  // force pass: [kCompactWalk] weights of the replayed impure members
     DevCompactFn* fn;               // [kWideRows + kWideCols]: radial parts, then angular parts
+    int* walk;                      // [kCompactWalk][4]: replayed members' rIdx, aIdx, calcComp, impure
     int* blockBegin;                // [kDevMaxElements + 1]
     short* perm;                    // [kWideCap] slot -> position in the atom's list
     unsigned char* el;              // [kWideCap]
 };
 
-__host__ __device__ inline size_t wideSmemBytes(int rows, int warps, bool forces)
+__host__ __device__ inline size_t wideDoubles(int rows, int warps, bool forces, bool narrow)
 {
-    size_t d = 5 * kWideCap + (size_t)rows * kWideCap * (forces ? 2 : 1) +
-               (forces ? (size_t)warps * 3 * kWideCap + kWideCells : (size_t)warps * kWideCells);
-    return d * sizeof(double) + (kWideRows + kWideCols) * sizeof(DevCompactFn) + (kDevMaxElements + 1) * sizeof(int) +
-           kWideCap * sizeof(short) + kWideCap;
+    const size_t tile = narrow ? tileDoubles<true>() + cellCount<true>() : tileDoubles<false>() + cellCount<false>();
+    return 5 * kWideCap + (size_t)rows * kWideCap * (forces ? 2 : 1) +
+           (forces ? (size_t)warps * 3 * kWideCap + kWideRows * kWideCols + kCompactWalk : (size_t)warps * tile);
 }
 
-__device__ __forceinline__ WideSmem wideCarve(char* base, int rows, int warps, bool forces)
+__host__ __device__ inline size_t wideSmemBytes(int rows, int warps, bool forces, bool narrow)
+{
+    return wideDoubles(rows, warps, forces, narrow) * sizeof(double) + (kWideRows + kWideCols) * sizeof(DevCompactFn) +
+           (4 * kCompactWalk + kDevMaxElements + 1) * sizeof(int) + kWideCap * sizeof(short) + kWideCap;
+}
+
+__device__ __forceinline__ WideSmem wideCarve(char* base, int rows, int warps, bool forces, bool narrow)
 {
     WideSmem S;
     double* d = reinterpret_cast<double*>(base);
@@ -542,14 +589,28 @@ __device__ __forceinline__ WideSmem wideCarve(char* base, int rows, int warps, b
     d += 5 * kWideCap;
     S.rad = d;
     d += rows * kWideCap;
-    S.drad = forces ? d : nullptr;
-    if (forces) d += rows * kWideCap;
-    S.h = forces ? d : nullptr;
-    if (forces) d += warps * 3 * kWideCap;
-    S.cell = d;
-    d += forces ? kWideCells : warps * kWideCells;
+    S.drad = S.h = S.tile = S.walkW = nullptr;
+    if (forces)
+    {
+        S.drad = d;
+        d += rows * kWideCap;
+        S.h = d;
+        d += warps * 3 * kWideCap;
+        S.cell = d;
+        d += kWideRows * kWideCols;
+        S.walkW = d;
+        d += kCompactWalk;
+    }
+    else
+    {
+        S.tile = d;
+        d += warps * (narrow ? tileDoubles<true>() : tileDoubles<false>());
+        S.cell = d;
+        d += warps * (narrow ? cellCount<true>() : cellCount<false>());
+    }
     S.fn = reinterpret_cast<DevCompactFn*>(d);
-    S.blockBegin = reinterpret_cast<int*>(S.fn + kWideRows + kWideCols);
+    S.walk = reinterpret_cast<int*>(S.fn + kWideRows + kWideCols);
+    S.blockBegin = S.walk + 4 * kCompactWalk;
     S.perm = reinterpret_cast<short*>(S.blockBegin + kDevMaxElements + 1);
     S.el = reinterpret_cast<unsigned char*>(S.perm + kWideCap);
     return S;
@@ -644,16 +705,28 @@ __device__ __forceinline__ WidePairs widePairs(WideSmem const& S, DevCompactGrou
     return P;
 }
 
-// Parts of the chunk (rows r0.., columns a0..) and the radial values of the
-// group's slots.
-template <bool FORCES>
+// Parts of the chunk (rows r0.., columns a0..), the radial values of the
+// group's slots and, for a narrow group, its replayed members.
+template <bool FORCES, bool NARROW>
 __device__ __forceinline__ void wideStageChunk(WideSmem const& S, DevModel const& model, DevCompactGroup const& G,
-                                               WidePairs const& P, int r0, int nRc, int a0, int nAc, int tid,
+                                               WidePairs const& P, const DevCompactMember* mem, const double* dEdG,
+                                               DevElement const& E, int r0, int nRc, int a0, int nAc, int tid,
                                                int threads)
 {
     if (tid < nRc) S.fn[tid] = model.compactFns[G.fnBegin + r0 + tid];
     else if (tid >= kWideRows && tid < kWideRows + nAc)
         S.fn[tid] = model.compactFns[G.fnBegin + G.nR + a0 + tid - kWideRows];
+    if (NARROW && tid >= 32 && tid < 32 + G.walkEnd - G.walkBegin)
+    {
+        const int st = tid - 32;
+        DevCompactMember const& M = mem[G.walkBegin + st];
+        S.walk[4 * st] = M.rIdx;
+        S.walk[4 * st + 1] = M.aIdx;
+        S.walk[4 * st + 2] = M.calcComp;
+        S.walk[4 * st + 3] = M.impure;
+        if (FORCES)
+            S.walkW[st] = M.impure >= 0 ? dEdG[M.sf] * model.scaling[E.sfBegin + M.sf].scalingFactor : 0.0;
+    }
     __syncthreads();
     for (int k = tid; k < nRc * P.ns; k += threads)
     {
@@ -667,28 +740,29 @@ __device__ __forceinline__ void wideStageChunk(WideSmem const& S, DevModel const
     }
 }
 
-// Sums v[0..63] over the warp by halving exchanges; afterwards lane l holds
-// the sums of cells 2l and 2l + 1 in v[0] and v[1].
-template <int L, int O>
-__device__ __forceinline__ void halveCells(double (&v)[kWideCells], int lane)
+// Skip tests of the narrow members for one pair (SymGrpCompAngn.cpp:263-272):
+// bit r (r < 32) when the first neighbour's radial part r is not 0 and the
+// second neighbour's distance and r_jk are inside its window; bit 32 + a when
+// the angle is inside angular part a's window.
+__device__ __forceinline__ unsigned long long walkMasks(WideSmem const& S, int u, int v, double rjk, double acost,
+                                                       int nRc, int nAc)
 {
-    const bool up = (lane & O) != 0;
-#pragma unroll
-    for (int q = 0; q < L / 2; ++q)
+    const bool firstU = S.perm[u] < S.perm[v];
+    const int s1 = firstU ? u : v, s2 = firstU ? v : u;
+    const double rsec = S.r[s2];
+    unsigned mR = 0u, mA = 0u;
+    for (int r = 0; r < nRc; ++r)
     {
-        const double send = up ? v[q] : v[q + L / 2];
-        const double keep = up ? v[q + L / 2] : v[q];
-        v[q] = keep + __shfl_xor_sync(kFullMask, send, O);
+        DevCompactFn const& f = S.fn[r];
+        if (S.rad[r * kWideCap + s1] != 0.0 && rsec > f.left && rsec < f.right && rjk > f.left && rjk < f.right)
+            mR |= 1u << r;
     }
-}
-
-__device__ __forceinline__ void warpReduceCells(double (&v)[kWideCells], int lane)
-{
-    halveCells<64, 16>(v, lane);
-    halveCells<32, 8>(v, lane);
-    halveCells<16, 4>(v, lane);
-    halveCells<8, 2>(v, lane);
-    halveCells<4, 1>(v, lane);
+    for (int a = 0; a < nAc; ++a)
+    {
+        DevCompactFn const& f = S.fn[kWideRows + a];
+        if (acost > f.left && acost < f.right) mA |= 1u << a;
+    }
+    return ((unsigned long long)mA << 32) | mR;
 }
 
 template <int TYPE>
@@ -699,14 +773,20 @@ __device__ __forceinline__ bool hasType(DevModel const& model, DevElement const&
     return false;
 }
 
-template <int TYPE>
-__global__ void __launch_bounds__(kWideWarps * 32, 2) kCompactWideValues(DevModel model, BatchView b, int rows)
+template <int TYPE, int ACORE>
+__global__ void __launch_bounds__(kWideWarps * 32, 4) kCompactWideValues(DevModel model, BatchView b, int rows)
 {
-    constexpr bool WEIGHTED = TYPE == 25;
+    constexpr bool WEIGHTED = TYPE >= 24;
+    constexpr bool NARROW = TYPE == 21 || TYPE == 24;
     constexpr int T = kWideWarps * 32;
+    constexpr int TR = tileRows<NARROW>();
     extern __shared__ __align__(16) char smemRaw[];
-    const WideSmem S = wideCarve(smemRaw, rows, kWideWarps, false);
+    const WideSmem S = wideCarve(smemRaw, rows, kWideWarps, false, NARROW);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* PT = S.tile + warp * tileDoubles<NARROW>();   // this warp's tile: radial products, then angular parts
+    double* AT = PT + TR * kTileStride;
+    double* cw = S.cell + warp * cellCount<NARROW>();
+    const int g4 = lane >> 2, t4 = lane & 3;              // mma fragment row / column of the lane
     for (int i = blockIdx.x; i < b.N; i += gridDim.x)
     {
         DevElement const& E = model.el[b.elem[i]];
@@ -722,58 +802,133 @@ __global__ void __launch_bounds__(kWideWarps * 32, 2) kCompactWideValues(DevMode
             if (G.type != TYPE) continue;
             const WidePairs P = widePairs<WEIGHTED>(S, G, n);
             const DevCompactMember* mem = model.compactMembers + G.memberBegin;
-            const int q = T / P.ph.minor, rem = T - q * P.ph.minor;
+            const int q = (32 * kWideWarps) / P.ph.minor, rem = 32 * kWideWarps - q * P.ph.minor;
+            const int nImp = NARROW ? G.numImpure : 0;
+            const int wl = NARROW ? G.walkEnd - G.walkBegin : 0;
             for (int r0 = 0; r0 < G.nR; r0 += kWideRows)
                 for (int a0 = 0; a0 < G.nA; a0 += kWideCols)
                 {
                     const int nRc = min(kWideRows, G.nR - r0), nAc = min(kWideCols, G.nA - a0);
-                    wideStageChunk<false>(S, model, G, P, r0, nRc, a0, nAc, tid, T);
+                    wideStageChunk<false, NARROW>(S, model, G, P, mem, nullptr, E, r0, nRc, a0, nAc, tid, T);
                     __syncthreads();
-                    double acc[kWideCells];
-#pragma unroll
-                    for (int c = 0; c < kWideCells; ++c) acc[c] = 0.0;
+                    // sums of tile rows 0-7 (c0x) and 8-15 (c1x), columns 2 t4 + {0, 1}
+                    double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
                     Cursor cur;
-                    cur.init(P.ph, tid);
-                    for (int p = tid; p < P.ph.count; p += T, cur.advance(P.ph, q, rem))
+                    cur.init(P.ph, 32 * warp + lane);
+                    for (int p0 = 32 * warp; p0 < P.ph.count; p0 += 32 * kWideWarps, cur.advance(P.ph, q, rem))
                     {
-                        int u, v;
-                        if (!cur.slots(P.ph, u, v)) continue;
-                        const double cost =
-                            (S.x[u] * S.x[v] + S.y[u] * S.y[v] + S.z[u] * S.z[v]) * (S.rinv[u] * S.rinv[v]);
-                        if (!(cost > -1.0 && cost < 1.0)) continue;
-                        const double acost = acos(cost);
-                        const double zw = WEIGHTED ? model.atomicNumber[S.el[u]] * model.atomicNumber[S.el[v]] : 1.0;
-                        double ang[kWideCols];
-#pragma unroll
-                        for (int a = 0; a < kWideCols; ++a)
+                        int u = 0, v = 0;
+                        bool ok = p0 + lane < P.ph.count && cur.slots(P.ph, u, v);
+                        double cost = 0.0, rjk = 0.0;
+                        if (ok)
                         {
-                            double f = 0.0, df;
-                            if (a < nAc) compactPartFdf(S.fn[kWideRows + a], acost, f, df);
-                            ang[a] = WEIGHTED ? f * zw : f;
-                        }
-#pragma unroll
-                        for (int r = 0; r < kWideRows; ++r)
-                        {
-                            if (r < nRc)
+                            if (NARROW)
                             {
-                                const double pr = S.rad[r * kWideCap + u] * S.rad[r * kWideCap + v];
-#pragma unroll
-                                for (int a = 0; a < kWideCols; ++a) acc[r * kWideCols + a] += pr * ang[a];
+                                // the narrow groups' j-k distance window (SymGrpCompAngn.cpp:218-226)
+                                const double ex = S.x[v] - S.x[u], ey = S.y[v] - S.y[u], ez = S.z[v] - S.z[u];
+                                const double r2 = ex * ex + ey * ey + ez * ez;
+                                ok = r2 < G.rmax * G.rmax && r2 > G.rmin * G.rmin;
+                                rjk = sqrt(r2);
+                            }
+                            cost = (S.x[u] * S.x[v] + S.y[u] * S.y[v] + S.z[u] * S.z[v]) * (S.rinv[u] * S.rinv[v]);
+                            ok = ok && cost > -1.0 && cost < 1.0;
+                        }
+                        // this pair's column of the tile (zeros for a bye, a pair out of range or cos = +-1)
+                        for (int k = 0; k < nImp; ++k) PT[(kWideRows + k) * kTileStride + lane] = 0.0;
+                        if (ok)
+                        {
+                            const double acost = acos(cost);
+                            const double zw =
+                                WEIGHTED ? model.atomicNumber[S.el[u]] * model.atomicNumber[S.el[v]] : 1.0;
+                            for (int a = 0; a < nAc; ++a)
+                            {
+                                double f, df;
+                                angularPartFdf<ACORE>(S.fn[kWideRows + a], acost, f, df);
+                                AT[a * kTileStride + lane] = WEIGHTED ? f * zw : f;
+                            }
+                            for (int r = 0; r < nRc; ++r)
+                            {
+                                double pr = S.rad[r * kWideCap + u] * S.rad[r * kWideCap + v];
+                                if (NARROW)
+                                {
+                                    double fq, dfq;
+                                    compactPartFdf(S.fn[r], rjk, fq, dfq);
+                                    pr *= fq;
+                                }
+                                PT[r * kTileStride + lane] = pr;
+                            }
+                            if (NARROW && wl > 0)
+                            {
+                                // replay the carried j-k radial part for the impure members (their own rows)
+                                const unsigned long long mk = walkMasks(S, u, v, rjk, acost, nRc, nAc);
+                                int src = -1;
+                                bool cskip = false;
+                                double qs = 0.0;
+                                for (int st = 0; st < wl; ++st)
+                                {
+                                    const int R = S.walk[4 * st], A = S.walk[4 * st + 1];
+                                    if (!((mk >> R) & 1ull) || !((mk >> (32 + A)) & 1ull))
+                                    {
+                                        cskip = true;
+                                        continue;
+                                    }
+                                    if (S.walk[4 * st + 2] || cskip)
+                                    {
+                                        if (R != src)
+                                        {
+                                            double dq;
+                                            compactPartFdf(S.fn[R], rjk, qs, dq);
+                                            src = R;
+                                        }
+                                        cskip = false;
+                                    }
+                                    const int imp = S.walk[4 * st + 3];
+                                    if (imp >= 0)
+                                        PT[(kWideRows + imp) * kTileStride + lane] =
+                                            S.rad[R * kWideCap + u] * S.rad[R * kWideCap + v] * qs;
+                                }
                             }
                         }
+                        else
+                        {
+                            for (int a = 0; a < nAc; ++a) AT[a * kTileStride + lane] = 0.0;
+                            for (int r = 0; r < nRc; ++r) PT[r * kTileStride + lane] = 0.0;
+                        }
+                        __syncwarp();
+                        // S += P^T A over the batch's 32 pairs, 4 per step; rows and columns beyond
+                        // the chunk read zeros and their sums are never used
+                        const bool row0 = g4 < nRc;
+                        const bool row1 = g4 + 8 < nRc || (NARROW && g4 >= 2 && g4 - 2 < nImp);
+                        const bool col = g4 < nAc;
+#pragma unroll
+                        for (int ks = 0; ks < 8; ++ks)
+                        {
+                            const int k = 4 * ks + t4;
+                            const double a0f = row0 ? PT[g4 * kTileStride + k] : 0.0;
+                            const double a1f = row1 ? PT[(g4 + 8) * kTileStride + k] : 0.0;
+                            const double bf = col ? AT[g4 * kTileStride + k] : 0.0;
+                            mmaF64(c00, c01, a0f, bf);
+                            mmaF64(c10, c11, a1f, bf);
+                        }
+                        __syncwarp();
                     }
-                    warpReduceCells(acc, lane);
-                    S.cell[warp * kWideCells + 2 * lane] = acc[0];
-                    S.cell[warp * kWideCells + 2 * lane + 1] = acc[1];
+                    cw[g4 * kCellStride + 2 * t4] = c00;
+                    cw[g4 * kCellStride + 2 * t4 + 1] = c01;
+                    if (g4 + 8 < TR)
+                    {
+                        cw[(g4 + 8) * kCellStride + 2 * t4] = c10;
+                        cw[(g4 + 8) * kCellStride + 2 * t4 + 1] = c11;
+                    }
                     __syncthreads();
                     for (int mi = tid; mi < G.memberCount; mi += T)
                     {
                         DevCompactMember const& M = mem[mi];
                         const int rr = M.rIdx - r0, aa = M.aIdx - a0;
                         if (rr < 0 || rr >= nRc || aa < 0 || aa >= nAc) continue;
-                        const int c = rr * kWideCols + aa;
+                        // impure members (narrow groups) have rows of their own after the grid's
+                        const int c = ((NARROW && M.impure >= 0) ? kWideRows + M.impure : rr) * kCellStride + aa;
                         double sum = S.cell[c];
-                        for (int w = 1; w < kWideWarps; ++w) sum += S.cell[w * kWideCells + c];
+                        for (int w = 1; w < kWideWarps; ++w) sum += S.cell[w * cellCount<NARROW>() + c];
                         b.G[(size_t)i * b.gStride + M.sf] = scaleG(model.scaling[E.sfBegin + M.sf], sum);
                     }
                     __syncthreads();
@@ -782,13 +937,14 @@ __global__ void __launch_bounds__(kWideWarps * 32, 2) kCompactWideValues(DevMode
     }
 }
 
-template <int TYPE>
+template <int TYPE, int ACORE>
 __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevModel model, BatchView b, int rows)
 {
-    constexpr bool WEIGHTED = TYPE == 25;
+    constexpr bool WEIGHTED = TYPE >= 24;
+    constexpr bool NARROW = TYPE == 21 || TYPE == 24;
     constexpr int T = kWideWarps * 32;
     extern __shared__ __align__(16) char smemRaw[];
-    const WideSmem S = wideCarve(smemRaw, rows, kWideWarps, true);
+    const WideSmem S = wideCarve(smemRaw, rows, kWideWarps, true, NARROW);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double* hw = S.h + warp * 3 * kWideCap;   // this warp's force array
     for (int k = tid; k < kWideWarps * 3 * kWideCap; k += T) S.h[k] = 0.0;
@@ -810,13 +966,15 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
             if (P.ph.count == 0) continue;
             const DevCompactMember* mem = model.compactMembers + G.memberBegin;
             const int q = (32 * kWideWarps) / P.ph.minor, rem = 32 * kWideWarps - q * P.ph.minor;
+            const int wl = NARROW ? G.walkEnd - G.walkBegin : 0;
             for (int r0 = 0; r0 < G.nR; r0 += kWideRows)
                 for (int a0 = 0; a0 < G.nA; a0 += kWideCols)
                 {
                     const int nRc = min(kWideRows, G.nR - r0), nAc = min(kWideCols, G.nA - a0);
-                    wideStageChunk<true>(S, model, G, P, r0, nRc, a0, nAc, tid, T);
-                    // cell weights, members summed in their order
-                    if (tid < kWideCells)
+                    wideStageChunk<true, NARROW>(S, model, G, P, mem, dEdG, E, r0, nRc, a0, nAc, tid, T);
+                    // cell weights of the grid's members (the impure ones are replayed per pair), summed
+                    // in member order
+                    if (tid < kWideRows * kWideCols)
                     {
                         double w = 0.0;
                         for (int mi = 0; mi < G.memberCount; ++mi)
@@ -824,6 +982,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                             DevCompactMember const& M = mem[mi];
                             const int rr = M.rIdx - r0, aa = M.aIdx - a0;
                             if (rr < 0 || rr >= nRc || aa < 0 || aa >= nAc || rr * kWideCols + aa != tid) continue;
+                            if (NARROW && M.impure >= 0) continue;
                             w += dEdG[M.sf] * model.scaling[E.sfBegin + M.sf].scalingFactor;
                         }
                         S.cell[tid] = w;
@@ -836,6 +995,14 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                         int u = 0, v = 0;
                         bool ok = p0 + lane < P.ph.count && cur.slots(P.ph, u, v);
                         double cu = 0.0, cv = 0.0, gm = 0.0;
+                        double rjk = 0.0;
+                        if (ok && NARROW)
+                        {
+                            const double ex = S.x[v] - S.x[u], ey = S.y[v] - S.y[u], ez = S.z[v] - S.z[u];
+                            const double r2 = ex * ex + ey * ey + ez * ez;
+                            ok = r2 < G.rmax * G.rmax && r2 > G.rmin * G.rmin;
+                            rjk = sqrt(r2);
+                        }
                         if (ok)
                         {
                             const double riu = S.rinv[u], riv = S.rinv[v];
@@ -851,11 +1018,11 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                 {
                                     ang[a] = 0.0;
                                     dang[a] = 0.0;
-                                    if (a < nAc) compactPartFdf(S.fn[kWideRows + a], acost, ang[a], dang[a]);
+                                    if (a < nAc) angularPartFdf<ACORE>(S.fn[kWideRows + a], acost, ang[a], dang[a]);
                                 }
                                 // the reference's first neighbour of the pair is the lower list index
                                 const bool firstU = S.perm[u] < S.perm[v];
-                                double Bu = 0.0, Bv = 0.0, A = 0.0;
+                                double Bu = 0.0, Bv = 0.0, Bjk = 0.0, A = 0.0;
 #pragma unroll
                                 for (int r = 0; r < kWideRows; ++r)
                                 {
@@ -876,9 +1043,57 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                             U += w * ang[a];
                                             V += w * dang[a];
                                         }
-                                        Bu += dru * rv * U;
-                                        Bv += ru * drv * U;
-                                        A += ru * rv * V;
+                                        if (NARROW)
+                                        {
+                                            double fq, dfq;
+                                            compactPartFdf(S.fn[r], rjk, fq, dfq);
+                                            Bu += dru * rv * fq * U;
+                                            Bv += ru * drv * fq * U;
+                                            Bjk += ru * rv * dfq * U;
+                                            A += ru * rv * fq * V;
+                                        }
+                                        else
+                                        {
+                                            Bu += dru * rv * U;
+                                            Bv += ru * drv * U;
+                                            A += ru * rv * V;
+                                        }
+                                    }
+                                }
+                                if (NARROW && wl > 0)
+                                {
+                                    // the impure members with the carried j-k radial part
+                                    const unsigned long long mk = walkMasks(S, u, v, rjk, acost, nRc, nAc);
+                                    int src = -1;
+                                    bool cskip = false;
+                                    double qs = 0.0, dqs = 0.0;
+                                    for (int st = 0; st < wl; ++st)
+                                    {
+                                        const int R = S.walk[4 * st], Ai = S.walk[4 * st + 1];
+                                        if (!((mk >> R) & 1ull) || !((mk >> (32 + Ai)) & 1ull))
+                                        {
+                                            cskip = true;
+                                            continue;
+                                        }
+                                        if (S.walk[4 * st + 2] || cskip)
+                                        {
+                                            if (R != src)
+                                            {
+                                                compactPartFdf(S.fn[R], rjk, qs, dqs);
+                                                src = R;
+                                            }
+                                            cskip = false;
+                                        }
+                                        if (S.walk[4 * st + 3] < 0) continue;
+                                        const double w = S.walkW[st];
+                                        const double ru = S.rad[R * kWideCap + u], rv = S.rad[R * kWideCap + v];
+                                        const double dru = S.drad[R * kWideCap + u], drv = S.drad[R * kWideCap + v];
+                                        double fa, dfa;
+                                        angularPartFdf<ACORE>(S.fn[kWideRows + Ai], acost, fa, dfa);
+                                        Bu += w * (dru * rv * qs * fa);
+                                        Bv += w * (ru * drv * qs * fa);
+                                        Bjk += w * (ru * rv * dqs * fa);
+                                        A += w * (ru * rv * qs * dfa);
                                     }
                                 }
                                 double C = A * dacost;
@@ -887,11 +1102,14 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                     const double zw = model.atomicNumber[S.el[u]] * model.atomicNumber[S.el[v]];
                                     Bu *= zw;
                                     Bv *= zw;
+                                    Bjk *= zw;
                                     C *= zw;
                                 }
-                                cu = Bu * riu - C * cost * riu * riu;
-                                cv = Bv * riv - C * cost * riv * riv;
-                                gm = C * (riu * riv);
+                                // with the j-k term (narrow): h_u -= B_jk / r_jk (d_v - d_u), h_v += the same
+                                const double gjk = NARROW ? Bjk / rjk : 0.0;
+                                cu = Bu * riu - C * cost * riu * riu + gjk;
+                                cv = Bv * riv - C * cost * riv * riv + gjk;
+                                gm = C * (riu * riv) - gjk;
                             }
                         }
                         // add the batch one round at a time: inside a round no slot occurs twice
@@ -986,67 +1204,81 @@ int wideBlocks(BatchView const& b, int sms, int perSM)
 
 } // namespace
 
+// The staged kernel of an angular type for the atoms with at most kWideCap
+// neighbours, then the direct kernel for the rest (or the direct kernel
+// alone for a narrow type the staged kernels do not fit).
+template <bool FORCES, int TYPE>
+int launchAngular(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
+{
+    constexpr bool NARROW = TYPE == 21 || TYPE == 24;
+    const int blocks = compactBlocks(b, sms);
+    if (NARROW && !m.compactNarrowStaged)
+    {
+        if (FORCES) kCompactForces<TYPE><<<blocks, 128, 0, st>>>(m, b, -1);
+        else kCompactValues<TYPE><<<blocks, 128, 0, st>>>(m, b, -1);
+        return 1;
+    }
+    const int rows = std::max(1, std::min(m.compactRows, kWideRows));
+    const size_t smem = wideSmemBytes(rows, kWideWarps, FORCES, NARROW);
+    auto staged = [&](auto kernel, int perSM) {
+        setDynamicSmemOnce(reinterpret_cast<const void*>(kernel), smem);
+        kernel<<<wideBlocks(b, sms, perSM), kWideWarps * 32, smem, st>>>(m, b, rows);
+    };
+    const bool poly2 = m.compactAngCore == kCorePoly2;
+    if (FORCES)
+    {
+        if (poly2) staged(kCompactWideForces<TYPE, kCorePoly2>, 3);
+        else staged(kCompactWideForces<TYPE, 0>, 3);
+        kCompactForces<TYPE><<<blocks, 128, 0, st>>>(m, b, kWideCap);
+    }
+    else
+    {
+        if (poly2) staged(kCompactWideValues<TYPE, kCorePoly2>, NARROW ? 3 : 4);
+        else staged(kCompactWideValues<TYPE, 0>, NARROW ? 3 : 4);
+        kCompactValues<TYPE><<<blocks, 128, 0, st>>>(m, b, kWideCap);
+    }
+    return 2;
+}
+
 int launchCompactValues(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
 {
     const int blocks = compactBlocks(b, sms);
-    const int rows = std::max(1, std::min(m.compactRows, kWideRows));
     int launches = 0;
-    auto direct = [&](auto kernel, int minNeighbors) {
-        kernel<<<blocks, 128, 0, st>>>(m, b, minNeighbors);
-        ++launches;
-    };
-    auto wide = [&](auto kernel) {
-        const size_t smem = wideSmemBytes(rows, kWideWarps, false);
-        setDynamicSmemOnce(reinterpret_cast<const void*>(kernel), smem);
-        kernel<<<wideBlocks(b, sms, 4), kWideWarps * 32, smem, st>>>(m, b, rows);
-        ++launches;
-    };
-    if (m.compactTypes & (1 << 0)) direct(kCompactValues<20>, -1);
-    if (m.compactTypes & (1 << 1)) direct(kCompactValues<21>, -1);
-    if (m.compactTypes & (1 << 2))
+    if (m.compactTypes & (1 << 0))
     {
-        wide(kCompactWideValues<22>);
-        direct(kCompactValues<22>, kWideCap);
+        kCompactValues<20><<<blocks, 128, 0, st>>>(m, b, -1);
+        ++launches;
     }
-    if (m.compactTypes & (1 << 3)) direct(kCompactValues<23>, -1);
-    if (m.compactTypes & (1 << 4)) direct(kCompactValues<24>, -1);
-    if (m.compactTypes & (1 << 5))
+    if (m.compactTypes & (1 << 1)) launches += launchAngular<false, 21>(m, b, sms, st);
+    if (m.compactTypes & (1 << 2)) launches += launchAngular<false, 22>(m, b, sms, st);
+    if (m.compactTypes & (1 << 3))
     {
-        wide(kCompactWideValues<25>);
-        direct(kCompactValues<25>, kWideCap);
+        kCompactValues<23><<<blocks, 128, 0, st>>>(m, b, -1);
+        ++launches;
     }
+    if (m.compactTypes & (1 << 4)) launches += launchAngular<false, 24>(m, b, sms, st);
+    if (m.compactTypes & (1 << 5)) launches += launchAngular<false, 25>(m, b, sms, st);
     return launches;
 }
 
 int launchCompactForces(DevModel const& m, BatchView const& b, int sms, cudaStream_t st)
 {
     const int blocks = compactBlocks(b, sms);
-    const int rows = std::max(1, std::min(m.compactRows, kWideRows));
     int launches = 0;
-    auto direct = [&](auto kernel, int minNeighbors) {
-        kernel<<<blocks, 128, 0, st>>>(m, b, minNeighbors);
-        ++launches;
-    };
-    auto wide = [&](auto kernel) {
-        const size_t smem = wideSmemBytes(rows, kWideWarps, true);
-        setDynamicSmemOnce(reinterpret_cast<const void*>(kernel), smem);
-        kernel<<<wideBlocks(b, sms, 3), kWideWarps * 32, smem, st>>>(m, b, rows);
-        ++launches;
-    };
-    if (m.compactTypes & (1 << 0)) direct(kCompactForces<20>, -1);
-    if (m.compactTypes & (1 << 1)) direct(kCompactForces<21>, -1);
-    if (m.compactTypes & (1 << 2))
+    if (m.compactTypes & (1 << 0))
     {
-        wide(kCompactWideForces<22>);
-        direct(kCompactForces<22>, kWideCap);
+        kCompactForces<20><<<blocks, 128, 0, st>>>(m, b, -1);
+        ++launches;
     }
-    if (m.compactTypes & (1 << 3)) direct(kCompactForces<23>, -1);
-    if (m.compactTypes & (1 << 4)) direct(kCompactForces<24>, -1);
-    if (m.compactTypes & (1 << 5))
+    if (m.compactTypes & (1 << 1)) launches += launchAngular<true, 21>(m, b, sms, st);
+    if (m.compactTypes & (1 << 2)) launches += launchAngular<true, 22>(m, b, sms, st);
+    if (m.compactTypes & (1 << 3))
     {
-        wide(kCompactWideForces<25>);
-        direct(kCompactForces<25>, kWideCap);
+        kCompactForces<23><<<blocks, 128, 0, st>>>(m, b, -1);
+        ++launches;
     }
+    if (m.compactTypes & (1 << 4)) launches += launchAngular<true, 24>(m, b, sms, st);
+    if (m.compactTypes & (1 << 5)) launches += launchAngular<true, 25>(m, b, sms, st);
     return launches;
 }
 
