@@ -102,7 +102,7 @@ constexpr int kCorePoly2 = 6;   // core type "p2" (CoreFunction::Type, numbering
 // radial / angular parts per grid chunk, and for the narrow types (one chunk)
 // the impure members and the members replayed per pair.
 constexpr int kCompactStageRows = 10;
-constexpr int kCompactStageCols = 6;
+constexpr int kCompactStageCols = 8;
 constexpr int kCompactImpure = 6;
 constexpr int kCompactWalk = 16;
 
@@ -111,7 +111,7 @@ constexpr int kCompactWalk = 16;
 // window in radians); center and scale as in CompactFunction::setLeftRight
 // (CompactFunction.cpp:62-76).  Every member's value over a pair is the
 // product of its radial part at r_ij and r_ik and its angular part at theta.
-struct DevCompactFn
+struct alignas(16) DevCompactFn
 {
     double left, right, center, scale;
     int    core, asym;

@@ -509,6 +509,8 @@ __host__ __device__ constexpr int tileDoubles() { return (tileRows<NARROW>() + k
 template <bool NARROW>
 __host__ __device__ constexpr int cellCount() { return tileRows<NARROW>() * kCellStride; }
 static_assert(kWideRows + kCompactImpure <= 16, "impure rows beyond the mma halves");
+static_assert(kWideCols % 2 == 0, "cell weights are read in pairs");
+static_assert(kWideCols <= kCellStride && kWideCols <= 8, "angular parts beyond the mma's 8 columns");
 
 // Value and derivative of a radial part at r (0 outside the open window):
 // CompactFunction::fdf with the part's core and asymmetry.
@@ -552,7 +554,8 @@ __device__ __forceinline__ void mmaF64(double& d0, double& d1, double a, double 
 struct WideSmem
 {
     double *x, *y, *z, *r, *rinv;   // [kWideCap]
-    double *rad, *drad;             // [rows][kWideCap]
+    double *rad;                    // G pass: [rows][kWideCap] radial values
+    double2 *rd;                    // force pass: [rows][kWideCap] radial values and derivatives
     double *h;                      // force pass: [warps][3][kWideCap]
     double *tile;                   // G pass: [warps][tile rows + kWideCols][kTileStride]
     double *cell;                   // G pass: [warps][tile rows * kCellStride] sums; force pass: W [kWideRows][kWideCols]
@@ -587,13 +590,12 @@ __device__ __forceinline__ WideSmem wideCarve(char* base, int rows, int warps, b
     S.r = d + 3 * kWideCap;
     S.rinv = d + 4 * kWideCap;
     d += 5 * kWideCap;
-    S.rad = d;
-    d += rows * kWideCap;
-    S.drad = S.h = S.tile = S.walkW = nullptr;
+    S.rad = S.h = S.tile = S.walkW = nullptr;
+    S.rd = nullptr;
     if (forces)
     {
-        S.drad = d;
-        d += rows * kWideCap;
+        S.rd = reinterpret_cast<double2*>(d);
+        d += 2 * rows * kWideCap;
         S.h = d;
         d += warps * 3 * kWideCap;
         S.cell = d;
@@ -603,6 +605,8 @@ __device__ __forceinline__ WideSmem wideCarve(char* base, int rows, int warps, b
     }
     else
     {
+        S.rad = d;
+        d += rows * kWideCap;
         S.tile = d;
         d += warps * (narrow ? tileDoubles<true>() : tileDoubles<false>());
         S.cell = d;
@@ -735,8 +739,8 @@ __device__ __forceinline__ void wideStageChunk(WideSmem const& S, DevModel const
         const int s = j < P.nA ? P.A0 + j : P.B0 + (j - P.nA);
         double f, df;
         compactPartFdf(S.fn[rr], S.r[s], f, df);
-        S.rad[rr * kWideCap + s] = f;
-        if (FORCES) S.drad[rr * kWideCap + s] = df;
+        if (FORCES) S.rd[rr * kWideCap + s] = make_double2(f, df);
+        else S.rad[rr * kWideCap + s] = f;
     }
 }
 
@@ -744,6 +748,7 @@ __device__ __forceinline__ void wideStageChunk(WideSmem const& S, DevModel const
 // bit r (r < 32) when the first neighbour's radial part r is not 0 and the
 // second neighbour's distance and r_jk are inside its window; bit 32 + a when
 // the angle is inside angular part a's window.
+template <bool FORCES>
 __device__ __forceinline__ unsigned long long walkMasks(WideSmem const& S, int u, int v, double rjk, double acost,
                                                        int nRc, int nAc)
 {
@@ -754,7 +759,8 @@ __device__ __forceinline__ unsigned long long walkMasks(WideSmem const& S, int u
     for (int r = 0; r < nRc; ++r)
     {
         DevCompactFn const& f = S.fn[r];
-        if (S.rad[r * kWideCap + s1] != 0.0 && rsec > f.left && rsec < f.right && rjk > f.left && rjk < f.right)
+        const double r1 = FORCES ? S.rd[r * kWideCap + s1].x : S.rad[r * kWideCap + s1];
+        if (r1 != 0.0 && rsec > f.left && rsec < f.right && rjk > f.left && rjk < f.right)
             mR |= 1u << r;
     }
     for (int a = 0; a < nAc; ++a)
@@ -860,7 +866,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) kCompactWideValues(DevMode
                             if (NARROW && wl > 0)
                             {
                                 // replay the carried j-k radial part for the impure members (their own rows)
-                                const unsigned long long mk = walkMasks(S, u, v, rjk, acost, nRc, nAc);
+                                const unsigned long long mk = walkMasks<false>(S, u, v, rjk, acost, nRc, nAc);
                                 int src = -1;
                                 bool cskip = false;
                                 double qs = 0.0;
@@ -1028,20 +1034,25 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                 {
                                     if (r < nRc)
                                     {
-                                        const double ru = S.rad[r * kWideCap + u], rv = S.rad[r * kWideCap + v];
-                                        double dru = S.drad[r * kWideCap + u], drv = S.drad[r * kWideCap + v];
+                                        const double2 pu = S.rd[r * kWideCap + u], pv = S.rd[r * kWideCap + v];
+                                        const double ru = pu.x, rv = pv.x;
+                                        double dru = pu.y, drv = pv.y;
                                         if (firstU ? ru == 0.0 : rv == 0.0)
                                         {
                                             if (firstU) dru = 0.0;
                                             else drv = 0.0;
                                         }
                                         double U = 0.0, V = 0.0;
+                                        const double2* W2 = reinterpret_cast<const double2*>(S.cell) + r * (kWideCols / 2);
 #pragma unroll
-                                        for (int a = 0; a < kWideCols; ++a)
+                                        for (int a = 0; a < kWideCols / 2; ++a)
                                         {
-                                            const double w = S.cell[r * kWideCols + a];
-                                            U += w * ang[a];
-                                            V += w * dang[a];
+                                            if (2 * a < nAc)
+                                            {
+                                                const double2 w = W2[a];
+                                                U += w.x * ang[2 * a] + w.y * ang[2 * a + 1];
+                                                V += w.x * dang[2 * a] + w.y * dang[2 * a + 1];
+                                            }
                                         }
                                         if (NARROW)
                                         {
@@ -1063,7 +1074,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                 if (NARROW && wl > 0)
                                 {
                                     // the impure members with the carried j-k radial part
-                                    const unsigned long long mk = walkMasks(S, u, v, rjk, acost, nRc, nAc);
+                                    const unsigned long long mk = walkMasks<true>(S, u, v, rjk, acost, nRc, nAc);
                                     int src = -1;
                                     bool cskip = false;
                                     double qs = 0.0, dqs = 0.0;
@@ -1086,8 +1097,8 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                         }
                                         if (S.walk[4 * st + 3] < 0) continue;
                                         const double w = S.walkW[st];
-                                        const double ru = S.rad[R * kWideCap + u], rv = S.rad[R * kWideCap + v];
-                                        const double dru = S.drad[R * kWideCap + u], drv = S.drad[R * kWideCap + v];
+                                        const double2 pu = S.rd[R * kWideCap + u], pv = S.rd[R * kWideCap + v];
+                                        const double ru = pu.x, rv = pv.x, dru = pu.y, drv = pv.y;
                                         double fa, dfa;
                                         angularPartFdf<ACORE>(S.fn[kWideRows + Ai], acost, fa, dfa);
                                         Bu += w * (dru * rv * qs * fa);
@@ -1221,6 +1232,9 @@ int launchAngular(DevModel const& m, BatchView const& b, int sms, cudaStream_t s
     const int rows = std::max(1, std::min(m.compactRows, kWideRows));
     const size_t smem = wideSmemBytes(rows, kWideWarps, FORCES, NARROW);
     auto staged = [&](auto kernel, int perSM) {
+        // resident blocks: the launch bound, or fewer when the stage is larger (228 KB of shared
+        // memory per SM, 1 KB of it reserved per block)
+        perSM = std::max(1, std::min(perSM, (int)(233472 / (smem + 1024))));
         setDynamicSmemOnce(reinterpret_cast<const void*>(kernel), smem);
         kernel<<<wideBlocks(b, sms, perSM), kWideWarps * 32, smem, st>>>(m, b, rows);
     };

@@ -153,12 +153,13 @@ def unscaled_from_files(model_dir, structure, G):
     return out
 
 
-def reference_noise(model_dir, structure):
-    """Relative force and energy spread between the reference built with FMA
-    contraction (-O3, x86-64-v3) and without (-O2, -ffp-contract=off): the
-    floating-point noise floor of the reference on this input."""
+def reference_noise(model_dir, structure, dedg=False):
+    """Relative energy and force spread (and with dedg=True the dE/dG spread)
+    between the reference built with FMA contraction (-O3, x86-64-v3) and
+    without (-O2, -ffp-contract=off): the floating-point noise floor of the
+    reference on this input."""
     if not oref.available(fast=True):
-        return 0.0, 0.0
+        return (0.0, 0.0, 0.0) if dedg else (0.0, 0.0)
     a = reference_snapshot(model_dir, structure)
     p = oref.RefPrediction(model_dir, fast=True)
     try:
@@ -166,7 +167,8 @@ def reference_noise(model_dir, structure):
         b = p.arrays()
     finally:
         p.close()
-    return abs(a["energy"] - b["energy"]) / abs(a["energy"]), max_rel(b["forces"], a["forces"])
+    spread = (abs(a["energy"] - b["energy"]) / abs(a["energy"]), max_rel(b["forces"], a["forces"]))
+    return spread + (max_rel(b["dEdG"], a["dEdG"]),) if dedg else spread
 
 
 BOHR_TO_A = 0.529177210903

@@ -109,10 +109,11 @@ def test_compact_staged_and_direct_tiers(name):
     with the carried j-k radial part).  About 100 of each frame's atoms
     have more than 256 neighbours and run the direct angular kernels, the
     others the staged block-per-atom kernels.  Neighbour lists bit-exact,
-    energies within 1e-10, forces within max(1e-10, 2 x the reference's
-    FMA/no-FMA spread), G within 1e-12 (scaled for the SCAN example, whose
-    scaling file the reference ships; unscaled for the derived model) and
-    dE/dG within 1e-10 of the reference library."""
+    energies within 1e-10, G within 1e-12 (scaled for the SCAN example, whose
+    scaling file the reference ships; unscaled for the derived model), forces
+    and dE/dG within max(1e-10, 2 x the reference's own FMA/no-FMA spread):
+    compressed, the boxes leave the scaling files' range and the derived
+    model's narrow-sample scaling amplifies FP64 rounding of G into dE/dG."""
     from n2p2_b200 import Structure
     d = os.path.join(H.GOLDEN, *name.split("/"))
     s0 = read_structures(os.path.join(d, "input.data"))[0]
@@ -129,13 +130,13 @@ def test_compact_staged_and_direct_tiers(name):
         snap = H.reference_snapshot(d, s)
         a1 = a0 + s.numAtoms
         g1 = g0 + snap["G"].size
-        tol_f = max(TOL_F, 2.0 * H.reference_noise(d, s)[1])
-        _compare_structure(b, a0, a1, snap, k, E, F, tol_f=tol_f)
+        _, noise_f, noise_d = H.reference_noise(d, s, dedg=True)
+        _compare_structure(b, a0, a1, snap, k, E, F, tol_f=max(TOL_F, 2.0 * noise_f))
         if "examples" in name:
             assert H.max_rel(G[g0:g1], snap["G"]) <= TOL_G, k
         else:
             assert H.max_rel(H.unscaled_from_files(d, s, G[g0:g1]), H.unscaled_from_files(d, s, snap["G"])) <= TOL_G, k
-        assert H.max_rel(dEdG[g0:g1], snap["dEdG"]) <= TOL_E, k
+        assert H.max_rel(dEdG[g0:g1], snap["dEdG"]) <= max(TOL_E, 2.0 * noise_d), k
         a0, g0 = a1, g1
 
 
