@@ -558,6 +558,51 @@ def _compact_run(d, structs, steps, warmup, device, cpu, cpu_sample=None):
     return natoms, out
 
 
+def _compact_wide_work(d, structs, nbr):
+    """Pairs and FP64 operations per E+F evaluation of the wide angular
+    groups (types 22, 25) of the model in `d`, counted for the factored
+    algorithm of the staged kernels: per pair of a group with nR radial and
+    nA angular parts, G pass 8 (geometry) + 8 nA (angular parts) + nR
+    (radial products) + 2 nR nA (grid sums); force pass 11 (geometry,
+    dtheta/dcos) + 12 nA (parts and derivatives) + 4 nR nA (U_r, V_r) +
+    9 nR (radial sums) + 34 (coefficients, both neighbours' forces).  The
+    radial parts of the neighbours (per neighbour, not per pair) and acos
+    are not counted."""
+    import collections
+    groups = collections.defaultdict(lambda: (set(), set()))
+    for line in open(os.path.join(d, "input.nn")):
+        t = line.split()
+        if t[:1] != ["symfunction_short"] or t[2] not in ("22", "25"):
+            continue
+        if t[2] == "22":
+            key = (t[1], "22") + tuple(sorted((t[3], t[4])))
+            rl, rc, al, ar, sub = t[5], t[6], t[7], t[8], t[9]
+        else:
+            key = (t[1], "25")
+            rl, rc, al, ar, sub = t[3], t[4], t[5], t[6], t[7]
+        groups[key][0].add((float(rl), float(rc), sub))
+        groups[key][1].add((float(al), float(ar), sub.rstrip("a")))
+    elem = np.concatenate([np.array(x.elements) for x in structs])
+    off, idx = nbr["offset"], nbr["index"]
+    pairs = flops = 0
+    for i in range(len(elem)):
+        ne = collections.Counter(elem[idx[off[i]:off[i + 1]]])
+        n = off[i + 1] - off[i]
+        for key, (rad, ang) in groups.items():
+            if key[0] != elem[i]:
+                continue
+            if key[1] == "25":
+                p = n * (n - 1) // 2
+            elif key[2] == key[3]:
+                p = ne[key[2]] * (ne[key[2]] - 1) // 2
+            else:
+                p = ne[key[2]] * ne[key[3]]
+            nR, nA = len(rad), len(ang)
+            pairs += p
+            flops += p * ((8 + 8 * nA + nR + 2 * nR * nA) + (11 + 12 * nA + 4 * nR * nA + 9 * nR + 34))
+    return pairs, flops
+
+
 def _perturbed(s0, count, seed, sigma):
     from n2p2_b200 import Structure
     rng = np.random.default_rng(seed)
@@ -577,10 +622,29 @@ def bench_compact(steps, warmup, device, cpu=True):
     from n2p2_b200 import read_structures
     golden = os.path.join(ROOT, "tests", "golden")
     d = os.path.join(golden, "examples", "Anisole_SCAN")
-    natoms, out = _compact_run(d, _perturbed(read_structures(os.path.join(d, "input.data"))[0], 64, 5, 0.02),
-                               steps, warmup, device, cpu)
+    anisole = _perturbed(read_structures(os.path.join(d, "input.data"))[0], 64, 5, 0.02)
+    natoms, out = _compact_run(d, anisole, steps, warmup, device, cpu)
     out = {"workload": "Anisole_SCAN model (reference example; compact types 20 + 22), 64 x 256-atom periodic boxes "
                        "(%d atoms)" % natoms, **out}
+    # roofline of the staged angular passes (the stage times include the radial type-20 launches)
+    from n2p2_b200 import Mode
+    m = Mode(device)
+    m.setupFromDirectory(d)
+    b = m.batch(anisole)
+    b.setPositions(np.concatenate([x.positions for x in anisole]))
+    b.evaluate(forces=False)
+    pairs, flops = _compact_wide_work(d, anisole, b.neighbors())
+    d64, d32 = ctypes_double(), ctypes_double()
+    peak = d64.value / 1e12 if m._lib.n2p2_device_fma_peak(device, d64.ref, d32.ref) == 0 else None
+    b.close()
+    m.close()
+    sec = (out["stages_ms"]["sf_values"] + out["stages_ms"]["sf_forces"]) / 1e3
+    out["roofline"] = {"bound": "fp64", "kernel": "kCompactWideValues + kCompactWideForces (with the type-20 launches)",
+                       "achieved": flops / sec / 1e12, "peak": peak, "unit": "TFLOP/s",
+                       "frac": (flops / sec / 1e12 / peak) if peak else None,
+                       "peak_source": "measured FP64 FMA throughput of this GPU (n2p2_device_fma_peak)",
+                       "pairs_per_step": pairs, "flops_per_step": flops,
+                       "flops_model": "factored staged algorithm per pair (bench.py _compact_wide_work)"}
     d = os.path.join(golden, "models", "scan_narrow")
     natoms, o = _compact_run(d, _perturbed(read_structures(os.path.join(d, "input.data"))[0], 16, 6, 0.02),
                              steps, warmup, device, cpu)

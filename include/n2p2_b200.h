@@ -294,10 +294,20 @@ n2p2_status n2p2_batch_get_launch_count(n2p2_batch* batch, int* launches);
  * numAtoms <= 8192, at most 32768 cells, at most 256 neighbours per atom;
  * larger inputs are rejected with N2P2_ERR_RUNTIME.  The call waits for its
  * stream (`stream` is a cudaStream_t, NULL = default stream) and stores the
- * entry count in *numEntries. */
+ * entry count in *numEntries.
+ *
+ * While `stream` is being captured into a CUDA graph the call only records
+ * its work (no host copy, no wait: neither may be captured) and sets
+ * *numEntries to -1; host-side rejections (atom count, cutoff, cell count)
+ * still happen at capture.  After a replay of the graph,
+ * n2p2_neighbor_list_noalloc_status reads the count and the device-side
+ * checks (atoms outside the cell, more than 256 neighbours, capacity) of the
+ * last run on the device, waiting for `stream`, with the same errors. */
 n2p2_status n2p2_neighbor_list_noalloc(const double* positions, int64_t numAtoms, const double* box, double cutoff,
                                        int64_t capacity, int64_t* offsets, int32_t* index, int32_t* image,
                                        double* d, double* dr, int64_t* numEntries, void* stream);
+n2p2_status n2p2_neighbor_list_noalloc_status(int64_t numAtoms, const int64_t* offsets, int64_t capacity,
+                                              int64_t* numEntries, void* stream);
 
 /* ---- structure files --------------------------------------------------------
  * input.data read in one pass: Structure::readFromLines (Structure.cpp:142-271)

@@ -92,6 +92,7 @@ SIGNATURES = {
     "n2p2_batch_get_extrapolation_warnings": (_i, [_vp, _P(_i64), _P(ctypes.c_int32)]),
     "n2p2_batch_get_launch_count": (_i, [_vp, _P(_i)]),
     "n2p2_neighbor_list_noalloc": (_i, [_vp, _i64, _P(_d), _d, _i64, _vp, _vp, _vp, _vp, _vp, _P(_i64), _vp]),
+    "n2p2_neighbor_list_noalloc_status": (_i, [_i64, _vp, _i64, _P(_i64), _vp]),
     "n2p2_batch_get_stream": (_i, [_vp, _P(_vp)]),
     "n2p2_batch_profile_stages": (_i, [_vp, _i, _i, _cp, _P(_d), _P(_i)]),
     "n2p2_batch_count_work": (_i, [_vp, _P(_i64)]),

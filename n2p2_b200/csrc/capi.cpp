@@ -719,6 +719,15 @@ n2p2_status n2p2_neighbor_list_noalloc(const double* positions, int64_t numAtoms
     });
 }
 
+n2p2_status n2p2_neighbor_list_noalloc_status(int64_t numAtoms, const int64_t* offsets, int64_t capacity,
+                                              int64_t* numEntries, void* stream)
+{
+    N2P2_REQUIRE(offsets);
+    return guard([&] {
+        neighborListNoAllocStatus(numAtoms, offsets, capacity, numEntries, static_cast<cudaStream_t>(stream));
+    });
+}
+
 n2p2_status n2p2_batch_get_stream(n2p2_batch* batch, void** stream)
 {
     N2P2_REQUIRE(batch);

@@ -195,7 +195,7 @@ struct DevModel
     int compactRows;      // largest nR of a wide angular group
     int compactAngCore;   // the core of every angular part of the staged angular groups, or 0 if they differ
     int compactNarrowStaged;   // every narrow group fits the staged kernels (one grid chunk, a short walk)
-    int pad2_;
+    int compactCols;      // largest nA of a staged angular group
 };
 
 // Per structure geometry for the neighbour build.

@@ -259,6 +259,7 @@ void DeviceModel::upload(Model const& m)
     int compactRows = 0;
     int compactAngCore = -1;   // -1: no staged angular part seen yet
     int compactNarrowStaged = 1;
+    int compactCols = 0;
     std::vector<DevScaling> scaling;
     std::vector<int> rowTable;
     std::vector<double> weights;
@@ -547,6 +548,7 @@ void DeviceModel::upload(Model const& m)
                 if (staged)
                 {
                     compactRows = std::max(compactRows, cg.nR);
+                    compactCols = std::max(compactCols, cg.nA);
                     for (auto const& f : ang)
                         compactAngCore = (compactAngCore == -1 || compactAngCore == f.core) ? f.core : 0;
                 }
@@ -647,6 +649,7 @@ void DeviceModel::upload(Model const& m)
     v.compactRows = compactRows;
     v.compactAngCore = std::max(compactAngCore, 0);
     v.compactNarrowStaged = compactNarrowStaged;
+    v.compactCols = compactCols;
     v.groups = groups_;
     groupTable = DevGroupTable{};
     if (groups.size() <= (size_t)kParamGroups)

@@ -509,7 +509,6 @@ __host__ __device__ constexpr int tileDoubles() { return (tileRows<NARROW>() + k
 template <bool NARROW>
 __host__ __device__ constexpr int cellCount() { return tileRows<NARROW>() * kCellStride; }
 static_assert(kWideRows + kCompactImpure <= 16, "impure rows beyond the mma halves");
-static_assert(kWideCols % 2 == 0, "cell weights are read in pairs");
 static_assert(kWideCols <= kCellStride && kWideCols <= 8, "angular parts beyond the mma's 8 columns");
 
 // Value and derivative of a radial part at r (0 outside the open window):
@@ -554,8 +553,7 @@ __device__ __forceinline__ void mmaF64(double& d0, double& d1, double a, double 
 struct WideSmem
 {
     double *x, *y, *z, *r, *rinv;   // [kWideCap]
-    double *rad;                    // G pass: [rows][kWideCap] radial values
-    double2 *rd;                    // force pass: [rows][kWideCap] radial values and derivatives
+    double *rad, *drad;             // [rows][kWideCap] radial values (and derivatives, force pass)
     double *h;                      // force pass: [warps][3][kWideCap]
     double *tile;                   // G pass: [warps][tile rows + kWideCols][kTileStride]
     double *cell;                   // G pass: [warps][tile rows * kCellStride] sums; force pass: W [kWideRows][kWideCols]
@@ -590,12 +588,13 @@ __device__ __forceinline__ WideSmem wideCarve(char* base, int rows, int warps, b
     S.r = d + 3 * kWideCap;
     S.rinv = d + 4 * kWideCap;
     d += 5 * kWideCap;
-    S.rad = S.h = S.tile = S.walkW = nullptr;
-    S.rd = nullptr;
+    S.rad = d;
+    d += rows * kWideCap;
+    S.drad = S.h = S.tile = S.walkW = nullptr;
     if (forces)
     {
-        S.rd = reinterpret_cast<double2*>(d);
-        d += 2 * rows * kWideCap;
+        S.drad = d;
+        d += rows * kWideCap;
         S.h = d;
         d += warps * 3 * kWideCap;
         S.cell = d;
@@ -605,8 +604,6 @@ __device__ __forceinline__ WideSmem wideCarve(char* base, int rows, int warps, b
     }
     else
     {
-        S.rad = d;
-        d += rows * kWideCap;
         S.tile = d;
         d += warps * (narrow ? tileDoubles<true>() : tileDoubles<false>());
         S.cell = d;
@@ -739,8 +736,8 @@ __device__ __forceinline__ void wideStageChunk(WideSmem const& S, DevModel const
         const int s = j < P.nA ? P.A0 + j : P.B0 + (j - P.nA);
         double f, df;
         compactPartFdf(S.fn[rr], S.r[s], f, df);
-        if (FORCES) S.rd[rr * kWideCap + s] = make_double2(f, df);
-        else S.rad[rr * kWideCap + s] = f;
+        S.rad[rr * kWideCap + s] = f;
+        if (FORCES) S.drad[rr * kWideCap + s] = df;
     }
 }
 
@@ -748,7 +745,6 @@ __device__ __forceinline__ void wideStageChunk(WideSmem const& S, DevModel const
 // bit r (r < 32) when the first neighbour's radial part r is not 0 and the
 // second neighbour's distance and r_jk are inside its window; bit 32 + a when
 // the angle is inside angular part a's window.
-template <bool FORCES>
 __device__ __forceinline__ unsigned long long walkMasks(WideSmem const& S, int u, int v, double rjk, double acost,
                                                        int nRc, int nAc)
 {
@@ -759,7 +755,7 @@ __device__ __forceinline__ unsigned long long walkMasks(WideSmem const& S, int u
     for (int r = 0; r < nRc; ++r)
     {
         DevCompactFn const& f = S.fn[r];
-        const double r1 = FORCES ? S.rd[r * kWideCap + s1].x : S.rad[r * kWideCap + s1];
+        const double r1 = S.rad[r * kWideCap + s1];
         if (r1 != 0.0 && rsec > f.left && rsec < f.right && rjk > f.left && rjk < f.right)
             mR |= 1u << r;
     }
@@ -866,7 +862,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) kCompactWideValues(DevMode
                             if (NARROW && wl > 0)
                             {
                                 // replay the carried j-k radial part for the impure members (their own rows)
-                                const unsigned long long mk = walkMasks<false>(S, u, v, rjk, acost, nRc, nAc);
+                                const unsigned long long mk = walkMasks(S, u, v, rjk, acost, nRc, nAc);
                                 int src = -1;
                                 bool cskip = false;
                                 double qs = 0.0;
@@ -943,12 +939,13 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) kCompactWideValues(DevMode
     }
 }
 
-template <int TYPE, int ACORE>
+template <int TYPE, int ACORE, int COLS>
 __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevModel model, BatchView b, int rows)
 {
     constexpr bool WEIGHTED = TYPE >= 24;
     constexpr bool NARROW = TYPE == 21 || TYPE == 24;
     constexpr int T = kWideWarps * 32;
+    static_assert(COLS <= kWideCols, "angular parts per chunk");
     extern __shared__ __align__(16) char smemRaw[];
     const WideSmem S = wideCarve(smemRaw, rows, kWideWarps, true, NARROW);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -974,20 +971,20 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
             const int q = (32 * kWideWarps) / P.ph.minor, rem = 32 * kWideWarps - q * P.ph.minor;
             const int wl = NARROW ? G.walkEnd - G.walkBegin : 0;
             for (int r0 = 0; r0 < G.nR; r0 += kWideRows)
-                for (int a0 = 0; a0 < G.nA; a0 += kWideCols)
+                for (int a0 = 0; a0 < G.nA; a0 += COLS)
                 {
-                    const int nRc = min(kWideRows, G.nR - r0), nAc = min(kWideCols, G.nA - a0);
+                    const int nRc = min(kWideRows, G.nR - r0), nAc = min(COLS, G.nA - a0);
                     wideStageChunk<true, NARROW>(S, model, G, P, mem, dEdG, E, r0, nRc, a0, nAc, tid, T);
                     // cell weights of the grid's members (the impure ones are replayed per pair), summed
                     // in member order
-                    if (tid < kWideRows * kWideCols)
+                    if (tid < kWideRows * COLS)
                     {
                         double w = 0.0;
                         for (int mi = 0; mi < G.memberCount; ++mi)
                         {
                             DevCompactMember const& M = mem[mi];
                             const int rr = M.rIdx - r0, aa = M.aIdx - a0;
-                            if (rr < 0 || rr >= nRc || aa < 0 || aa >= nAc || rr * kWideCols + aa != tid) continue;
+                            if (rr < 0 || rr >= nRc || aa < 0 || aa >= nAc || rr * COLS + aa != tid) continue;
                             if (NARROW && M.impure >= 0) continue;
                             w += dEdG[M.sf] * model.scaling[E.sfBegin + M.sf].scalingFactor;
                         }
@@ -1018,9 +1015,9 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                             {
                                 const double acost = acos(cost);
                                 const double dacost = -1.0 / sqrt(1.0 - cost * cost);
-                                double ang[kWideCols], dang[kWideCols];
+                                double ang[COLS], dang[COLS];
 #pragma unroll
-                                for (int a = 0; a < kWideCols; ++a)
+                                for (int a = 0; a < COLS; ++a)
                                 {
                                     ang[a] = 0.0;
                                     dang[a] = 0.0;
@@ -1034,25 +1031,20 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                 {
                                     if (r < nRc)
                                     {
-                                        const double2 pu = S.rd[r * kWideCap + u], pv = S.rd[r * kWideCap + v];
-                                        const double ru = pu.x, rv = pv.x;
-                                        double dru = pu.y, drv = pv.y;
+                                        const double ru = S.rad[r * kWideCap + u], rv = S.rad[r * kWideCap + v];
+                                        double dru = S.drad[r * kWideCap + u], drv = S.drad[r * kWideCap + v];
                                         if (firstU ? ru == 0.0 : rv == 0.0)
                                         {
                                             if (firstU) dru = 0.0;
                                             else drv = 0.0;
                                         }
                                         double U = 0.0, V = 0.0;
-                                        const double2* W2 = reinterpret_cast<const double2*>(S.cell) + r * (kWideCols / 2);
 #pragma unroll
-                                        for (int a = 0; a < kWideCols / 2; ++a)
+                                        for (int a = 0; a < COLS; ++a)
                                         {
-                                            if (2 * a < nAc)
-                                            {
-                                                const double2 w = W2[a];
-                                                U += w.x * ang[2 * a] + w.y * ang[2 * a + 1];
-                                                V += w.x * dang[2 * a] + w.y * dang[2 * a + 1];
-                                            }
+                                            const double w = S.cell[r * COLS + a];
+                                            U += w * ang[a];
+                                            V += w * dang[a];
                                         }
                                         if (NARROW)
                                         {
@@ -1074,7 +1066,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                 if (NARROW && wl > 0)
                                 {
                                     // the impure members with the carried j-k radial part
-                                    const unsigned long long mk = walkMasks<true>(S, u, v, rjk, acost, nRc, nAc);
+                                    const unsigned long long mk = walkMasks(S, u, v, rjk, acost, nRc, nAc);
                                     int src = -1;
                                     bool cskip = false;
                                     double qs = 0.0, dqs = 0.0;
@@ -1097,8 +1089,8 @@ __global__ void __launch_bounds__(kWideWarps * 32, 3) kCompactWideForces(DevMode
                                         }
                                         if (S.walk[4 * st + 3] < 0) continue;
                                         const double w = S.walkW[st];
-                                        const double2 pu = S.rd[R * kWideCap + u], pv = S.rd[R * kWideCap + v];
-                                        const double ru = pu.x, rv = pv.x, dru = pu.y, drv = pv.y;
+                                        const double ru = S.rad[R * kWideCap + u], rv = S.rad[R * kWideCap + v];
+                                        const double dru = S.drad[R * kWideCap + u], drv = S.drad[R * kWideCap + v];
                                         double fa, dfa;
                                         angularPartFdf<ACORE>(S.fn[kWideRows + Ai], acost, fa, dfa);
                                         Bu += w * (dru * rv * qs * fa);
@@ -1241,8 +1233,14 @@ int launchAngular(DevModel const& m, BatchView const& b, int sms, cudaStream_t s
     const bool poly2 = m.compactAngCore == kCorePoly2;
     if (FORCES)
     {
-        if (poly2) staged(kCompactWideForces<TYPE, kCorePoly2>, 3);
-        else staged(kCompactWideForces<TYPE, 0>, 3);
+        // six angular parts per chunk where the model has no more (the SCAN and QM9 groups)
+        if (m.compactCols <= 6)
+        {
+            if (poly2) staged(kCompactWideForces<TYPE, kCorePoly2, 6>, 3);
+            else staged(kCompactWideForces<TYPE, 0, 6>, 3);
+        }
+        else if (poly2) staged(kCompactWideForces<TYPE, kCorePoly2, kWideCols>, 3);
+        else staged(kCompactWideForces<TYPE, 0, kWideCols>, 3);
         kCompactForces<TYPE><<<blocks, 128, 0, st>>>(m, b, kWideCap);
     }
     else

@@ -293,9 +293,28 @@ void neighborListNoAlloc(const double* positions, int64_t numAtoms, const double
     kNaSearch<1><<<wblocks, 128, 0, st>>>(N, rc2, s, positions, atomCell, cellStart64, cellCount, cellAtoms, count,
                                           offsets, capacity, index, image, d, dr, status);
     cudaCheck(cudaGetLastError(), "kernel launch");
+    // Recorded into the caller's graph: no host copy and no wait (neither may be captured); the
+    // count and the limit checks are read after a replay by neighborListNoAllocStatus.
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    cudaCheck(cudaStreamIsCapturing(st, &capture), "cudaStreamIsCapturing");
+    if (capture != cudaStreamCaptureStatusNone)
+    {
+        if (numEntries) *numEntries = -1;
+        return;
+    }
+    neighborListNoAllocStatus(numAtoms, offsets, capacity, numEntries, st);
+}
+
+void neighborListNoAllocStatus(int64_t numAtoms, const int64_t* offsets, int64_t capacity, int64_t* numEntries,
+                               cudaStream_t st)
+{
+    if (numAtoms <= 0 || numAtoms > kNaMaxAtoms)
+        throw std::runtime_error("ERROR: the allocation-free neighbour list takes 1.." + std::to_string(kNaMaxAtoms) +
+                                 " atoms.\n");
+    const int* status = reinterpret_cast<const int*>(scratchForCurrentDevice() + kOffStatus);
     int hostStatus = 0;
     int64_t total = 0;
-    cudaCheck(cudaMemcpyAsync(&total, offsets + N, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
+    cudaCheck(cudaMemcpyAsync(&total, offsets + numAtoms, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "D2H");
     cudaCheck(cudaMemcpyAsync(&hostStatus, status, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
     cudaCheck(cudaStreamSynchronize(st), "synchronize");
     if (numEntries) *numEntries = total;

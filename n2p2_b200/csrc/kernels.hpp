@@ -169,9 +169,13 @@ void launchExternalTranspose(BatchView const& b, int numTargets, const int* cent
 void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cudaStream_t st);
 
 // neighbour list of one structure into caller buffers, no device allocation
+// (during stream capture the launches only; the status call then reads the
+// count and the limit checks after a replay)
 void neighborListNoAlloc(const double* positions, int64_t numAtoms, const double* box, double cutoff,
                          int64_t capacity, int64_t* offsets, int32_t* index, int32_t* image, double* d, double* dr,
                          int64_t* numEntries, cudaStream_t st);
+void neighborListNoAllocStatus(int64_t numAtoms, const int64_t* offsets, int64_t capacity, int64_t* numEntries,
+                               cudaStream_t st);
 
 // instrumentation
 void launchCountWork(DevModel const& m, BatchView const& b, unsigned long long* counts, int sms, cudaStream_t st);

@@ -107,3 +107,66 @@ def test_noalloc_cluster_and_rejections():
         _noalloc(torch, dense, None, cutoff, capacity=300 * 300)
     # and the shared scratch still gives exact lists afterwards
     _assert_same(_noalloc(torch, pos, None, cutoff, capacity=len(ref["d"]) + 64), ref)
+
+
+def test_noalloc_recorded_in_cuda_graph():
+    """The call recorded into a CUDA graph (torch.cuda.graph) and replayed:
+    no host copy or wait at capture (numEntries -1), then after each replay
+    the status call reports the count and passes the device-side checks, and
+    the entries equal the batched path's bit for bit -- for the captured
+    positions and, after new positions are copied into the captured buffer,
+    for the new structure (same box, same atom count)."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("needs a GPU")
+    lib = _lib.load()
+    m = H.gpu_mode(H.WATER40)
+    cutoff = m.getMaxCutoffRadius()
+    s1, s2 = water.water_box(64, seed=0), water.water_box(64, seed=9)
+    assert np.array_equal(s1.box, s2.box)
+    refs, poss = [], []
+    for s in (s1, s2):
+        b = H.gpu_batch(m, [s])
+        refs.append(b.neighbors())
+        poss.append(b.internalPositions())
+    n = s1.numAtoms
+    capacity = max(len(r["d"]) for r in refs) + 64
+    dev = torch.device("cuda", 0)
+    pos = torch.from_numpy(np.ascontiguousarray(poss[0])).to(dev)
+    off = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    idx = torch.zeros(capacity, dtype=torch.int32, device=dev)
+    img = torch.zeros(capacity, dtype=torch.int32, device=dev)
+    d = torch.zeros(capacity, dtype=torch.float64, device=dev)
+    dr = torch.zeros(capacity * 3, dtype=torch.float64, device=dev)
+    box = np.ascontiguousarray(s1.box, dtype=np.float64)
+    ptr = ctypes.c_void_p
+
+    def call(stream, total):
+        _lib.check(lib.n2p2_neighbor_list_noalloc(
+            ptr(pos.data_ptr()), n, box.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cutoff, capacity,
+            ptr(off.data_ptr()), ptr(idx.data_ptr()), ptr(img.data_ptr()), ptr(d.data_ptr()), ptr(dr.data_ptr()),
+            ctypes.byref(total), ptr(stream)))
+
+    def entries(total):
+        k = total.value
+        return {"offset": off.cpu().numpy(), "index": idx[:k].cpu().numpy(), "image": img[:k].cpu().numpy(),
+                "d": d[:k].cpu().numpy(), "dr": dr[:3 * k].cpu().numpy().reshape(-1, 3)}
+
+    total = ctypes.c_int64()
+    call(torch.cuda.current_stream(dev).cuda_stream, total)   # direct call first (scratch address lookup)
+    _assert_same(entries(total), refs[0])
+    g = torch.cuda.CUDAGraph()
+    captured = ctypes.c_int64(0)
+    with torch.cuda.graph(g):
+        call(torch.cuda.current_stream(dev).cuda_stream, captured)
+    assert captured.value == -1
+    for k in (0, 1):
+        pos.copy_(torch.from_numpy(np.ascontiguousarray(poss[k])).to(dev))
+        off.zero_()
+        g.replay()
+        total = ctypes.c_int64()
+        _lib.check(lib.n2p2_neighbor_list_noalloc_status(n, ptr(off.data_ptr()), capacity, ctypes.byref(total),
+                                                         ptr(torch.cuda.current_stream(dev).cuda_stream)))
+        assert total.value == len(refs[k]["d"])
+        _assert_same(entries(total), refs[k])
+    del g
