@@ -635,7 +635,7 @@ def bench_compact(steps, warmup, device, cpu=True):
     b.evaluate(forces=False)
     pairs, flops = _compact_wide_work(d, anisole, b.neighbors())
     d64, d32 = ctypes_double(), ctypes_double()
-    peak = d64.value / 1e12 if m._lib.n2p2_device_fma_peak(device, d64.ref, d32.ref) == 0 else None
+    peak = d64.value if m._lib.n2p2_device_fma_peak(device, d64.ref, d32.ref) == 0 else None   # TFLOP/s
     b.close()
     m.close()
     sec = (out["stages_ms"]["sf_values"] + out["stages_ms"]["sf_forces"]) / 1e3
