@@ -714,6 +714,10 @@ void Batch::releaseAll()
     maskBuf_ = nullptr;
     maskCap_ = 0;
     freeAll(pool_, ownedDGdr_);
+    freeAll(pool_, ownedScr_);
+    scrEntries_ = 0;
+    nbrStride_ = 0;
+    v_.scrStride = 0;
     freeAll(pool_, ownedNbr_);
     freeAll(pool_, owned_);
     dgdrAllocated_ = false;
@@ -856,6 +860,10 @@ void Batch::beginExternal(int numCenters, const int* elements, int numTargets, c
     // sets new lists every step (an MD code) keeps masks of the last size.
     releaseGraph();
     freeAll(pool_, ownedDGdr_);
+    freeAll(pool_, ownedScr_);
+    scrEntries_ = 0;
+    nbrStride_ = 0;
+    v_.scrStride = 0;
     freeAll(pool_, ownedNbr_);
     freeAll(pool_, owned_);
     dgdrAllocated_ = false;
@@ -1055,11 +1063,7 @@ void Batch::allocateNeighbors(int64_t capacity)
     const int slots = std::max(1, dmodel_.view.numCutoffSlots);
     capacity_ = capacity;
     v_.nbrCapacity = capacity;
-    v_.scrKey = devAlloc<int64_t>(pool_, capacity, ownedNbr_);
-    v_.scrD = devAlloc<double>(pool_, capacity, ownedNbr_);
-    v_.scrDx = devAlloc<double>(pool_, capacity, ownedNbr_);
-    v_.scrDy = devAlloc<double>(pool_, capacity, ownedNbr_);
-    v_.scrDz = devAlloc<double>(pool_, capacity, ownedNbr_);
+    allocateScratch(std::max(capacity, (int64_t)N_ * nbrStride_));
     v_.nbrJ = devAlloc<int>(pool_, capacity, ownedNbr_);
     v_.nbrCode = devAlloc<int>(pool_, capacity, ownedNbr_);
     v_.nbrElem = devAlloc<uint8_t>(pool_, capacity, ownedNbr_);
@@ -1075,6 +1079,38 @@ void Batch::allocateNeighbors(int64_t capacity)
     v_.hz = devAlloc<double>(pool_, capacity, ownedNbr_);
     v_.dGdr = nullptr;
     v_.dGdrSelf = nullptr;
+}
+
+// Unordered entries of the neighbour build: the packed entries (two passes)
+// or N x stride (one pass).
+void Batch::allocateScratch(int64_t entries)
+{
+    releaseGraph();
+    freeAll(pool_, ownedScr_);
+    scrEntries_ = entries;
+    v_.scrKey = devAlloc<int64_t>(pool_, entries, ownedScr_);
+    v_.scrD = devAlloc<double>(pool_, entries, ownedScr_);
+    v_.scrDx = devAlloc<double>(pool_, entries, ownedScr_);
+    v_.scrDy = devAlloc<double>(pool_, entries, ownedScr_);
+    v_.scrDz = devAlloc<double>(pool_, entries, ownedScr_);
+}
+
+// Search stride for a largest neighbour count: 1/8 and 16 entries of room,
+// a multiple of 8.
+static int64_t strideFor(int64_t maxNeighbors)
+{
+    return (maxNeighbors + maxNeighbors / 8 + 16 + 7) / 8 * 8;
+}
+
+// Search mode of the neighbour build: 0 = count pass, scan, fill pass; > 0 =
+// one pass into fixed-stride scratch (a recorded graph holds the mode).
+void Batch::setStride(int64_t stride)
+{
+    if (stride == nbrStride_) return;
+    releaseGraph();
+    nbrStride_ = stride;
+    v_.scrStride = stride;
+    if (stride > 0 && (int64_t)N_ * stride > scrEntries_) allocateScratch((int64_t)N_ * stride);
 }
 
 void Batch::allocateDGdr()
@@ -1542,6 +1578,7 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
     pendingVerify_ = false;
     if (!capacityVerified_)
     {
+        setStride(0);   // the two-pass build finds the largest count
         for (int attempt = 0; attempt < 3; ++attempt)
         {
             record(flags, precision, checkExtrapolation);
@@ -1559,6 +1596,14 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
             freeAll(pool_, ownedMask_);
             maskCap_ = st.maskWords + st.maskWords / 4 + 4096;
             maskBuf_ = devAlloc<uint32_t>(pool_, (size_t)maskCap_, ownedMask_);
+        }
+        // Later evaluations search once into a fixed stride of the largest count plus 1/8 and 16
+        // (the count pass skipped), while N x stride stays within twice the packed entries; an
+        // evaluation in which an atom outgrows the stride also runs the fill pass on the device.
+        if (!external_ && st.maxNeighbors > 0)
+        {
+            const int64_t stride = strideFor(st.maxNeighbors);
+            if ((int64_t)N_ * stride <= 2 * capacity_) setStride(stride);
         }
         capacityVerified_ = true;
         return;
@@ -1601,6 +1646,13 @@ void Batch::verify()
     if (!pendingVerify_) return;
     pendingVerify_ = false;
     const DevStatus st = readStatus();
+    // An atom that outgrew the search stride made the evaluation run its fill pass as well (the
+    // results are complete); later evaluations search into a wider stride, recorded anew.
+    if (nbrStride_ > 0 && st.maxNeighbors > nbrStride_)
+    {
+        const int64_t stride = strideFor(st.maxNeighbors);
+        setStride((int64_t)N_ * stride <= 2 * capacity_ ? stride : 0);
+    }
     if (st.totalNeighbors <= capacity_) return;
     // The lists outgrew the buffers sized at the first evaluation: size them
     // again and repeat the evaluation directly (the graph is recaptured at

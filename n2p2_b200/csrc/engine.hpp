@@ -251,6 +251,8 @@ public:
 private:
     void allocateAtoms();
     void allocateNeighbors(int64_t capacity);
+    void allocateScratch(int64_t entries);
+    void setStride(int64_t stride);
     void allocateDGdr();
     struct Mark
     {
@@ -311,6 +313,9 @@ private:
     DevicePool pool_;
     std::vector<void*> owned_;
     std::vector<void*> ownedNbr_;
+    std::vector<void*> ownedScr_;     // neighbour-build scratch (unordered entries)
+    int64_t scrEntries_ = 0;
+    int64_t nbrStride_ = 0;           // > 0: one-pass neighbour search into fixed-stride scratch
     std::vector<void*> ownedDGdr_;
     std::vector<void*> ownedMask_;
     uint32_t* maskBuf_ = nullptr;

@@ -142,7 +142,13 @@ __global__ void kScatterCells(int N, const int* __restrict__ atomCell, const int
 }
 
 // One warp per centre atom.  PASS 0 counts, PASS 1 writes the unordered
-// candidates into the atom's segment of the scratch arrays.  The stencil cells
+// candidates into the atom's segment of the scratch arrays; PASS 2 does both
+// at once into a fixed-stride segment (i * scrStride, sized from an earlier
+// evaluation's largest count), keeping the count for the scan and the sort,
+// and drops entries beyond the stride.  After a PASS 2 the fill pass runs as
+// well, guarded by the status (guardStride): it returns at once unless some
+// atom outgrew the stride, and then writes the packed segments the sort reads
+// instead, so every list is complete either way.  The stencil cells
 // (with their periodic images) are tabulated in shared memory, kStencilChunk
 // at a time, with an exclusive scan of their atom counts; the warp then walks
 // the concatenated candidates 32 at a time (lane -> cell by binary search), so
@@ -164,8 +170,10 @@ __global__ void __launch_bounds__(kSearchWarps * 32) kNeighborSearch(
     const int* __restrict__ atomCell, const int* __restrict__ cellStart, const int* __restrict__ cellCountArr,
     const double4* __restrict__ cellPos, int* __restrict__ nbrCount, const int64_t* __restrict__ nbrOffset,
     int64_t capacity, int64_t* __restrict__ scrKey, double* __restrict__ scrD, double* __restrict__ scrDx,
-    double* __restrict__ scrDy, double* __restrict__ scrDz, DevStatus* __restrict__ status)
+    double* __restrict__ scrDy, double* __restrict__ scrDz, DevStatus* __restrict__ status, int64_t scrStride,
+    int64_t guardStride)
 {
+    if (PASS == 1 && guardStride > 0 && status->maxNeighbors <= guardStride) return;   // the strided search fit
     __shared__ StencilTable tables[kSearchWarps];
     StencilTable& tab = tables[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -188,6 +196,11 @@ __global__ void __launch_bounds__(kSearchWarps * 32) kNeighborSearch(
             base = nbrOffset[i];
             limit = nbrOffset[i + 1];
             if (limit > capacity) limit = capacity;   // overflow is flagged by the host check
+        }
+        else if (PASS == 2)
+        {
+            base = (int64_t)i * scrStride;
+            limit = base + scrStride;
         }
         for (int c0 = 0; c0 < numStencil; c0 += kStencilChunk)
         {
@@ -261,7 +274,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) kNeighborSearch(
                         hit = (d2 <= rc2);
                     }
                 }
-                if (PASS == 0)
+                if constexpr (PASS == 0)
                 {
                     count += hit ? 1 : 0;
                 }
@@ -285,9 +298,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32) kNeighborSearch(
                 }
             }
         }
-        if (PASS == 0)
+        if (PASS != 1)
         {
-            count = warpSumInt(count);
+            if (PASS == 0) count = warpSumInt(count);   // PASS 2 counts warp-wide already
             if (lane == 0)
             {
                 nbrCount[i] = count;
@@ -306,8 +319,11 @@ __global__ void __launch_bounds__(256) kNeighborSort(
     const double* __restrict__ scrD, const double* __restrict__ scrDx, const double* __restrict__ scrDy,
     const double* __restrict__ scrDz, const int* __restrict__ elem, int* __restrict__ nbrJ,
     int* __restrict__ nbrCode, uint8_t* __restrict__ nbrElem, double* __restrict__ nbrD,
-    double* __restrict__ nbrDx, double* __restrict__ nbrDy, double* __restrict__ nbrDz)
+    double* __restrict__ nbrDx, double* __restrict__ nbrDy, double* __restrict__ nbrDz, int64_t scrStride,
+    const DevStatus* __restrict__ status)
 {
+    // the strided segments, unless an atom outgrew the stride and the fill pass wrote packed ones
+    const bool strided = scrStride > 0 && status->maxNeighbors <= scrStride;
     constexpr int kSmemKeys = 512;
     __shared__ int64_t skeys[8][kSmemKeys];
     const int lane = threadIdx.x & 31;
@@ -319,13 +335,14 @@ __global__ void __launch_bounds__(256) kNeighborSort(
         const int64_t end = nbrOffset[i + 1];
         if (end > capacity) continue;
         const int n = (int)(end - off);
+        const int64_t src = strided ? (int64_t)i * scrStride : off;   // the atom's scratch segment
         DevStructInfo const& s = info[atomStruct[i]];
         const int K = (2 * s.pbc[0] + 1) * (2 * s.pbc[1] + 1) * (2 * s.pbc[2] + 1);
         const bool inSmem = n <= kSmemKeys;
         if (inSmem)
-            for (int e = lane; e < n; e += 32) skeys[w][e] = scrKey[off + e];
+            for (int e = lane; e < n; e += 32) skeys[w][e] = scrKey[src + e];
         __syncwarp();
-        const int64_t* keys = inSmem ? skeys[w] : scrKey + off;
+        const int64_t* keys = inSmem ? skeys[w] : scrKey + src;
         for (int e = lane; e < n; e += 32)
         {
             const int64_t k = keys[e];
@@ -336,10 +353,10 @@ __global__ void __launch_bounds__(256) kNeighborSort(
             nbrJ[dst] = j;
             nbrCode[dst] = (int)(k % K);
             nbrElem[dst] = (uint8_t)elem[j];
-            nbrD[dst] = scrD[off + e];
-            nbrDx[dst] = scrDx[off + e];
-            nbrDy[dst] = scrDy[off + e];
-            nbrDz[dst] = scrDz[off + e];
+            nbrD[dst] = scrD[src + e];
+            nbrDx[dst] = scrDx[src + e];
+            nbrDy[dst] = scrDy[src + e];
+            nbrDz[dst] = scrDz[src + e];
         }
         __syncwarp();
     }
@@ -538,19 +555,35 @@ void launchNeighborBuild(BatchView const& b, double rc2, cudaStream_t st)
     kScatterCells<<<blocks, 256, 0, st>>>(N, b.atomCell, b.atomSlot, b.cellStart, b.px, b.py, b.pz, b.cellAtoms,
                                           b.cellPos);
     const int warpBlocks = (N + kSearchWarps - 1) / kSearchWarps > 0 ? (N + kSearchWarps - 1) / kSearchWarps : 1;
-    kNeighborSearch<0><<<warpBlocks, kSearchWarps * 32, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz,
-                                                   b.atomCell, b.cellStart, b.cellCount, b.cellPos, b.nbrCount,
-                                                   nullptr, 0,
-                                                   nullptr, nullptr, nullptr, nullptr, nullptr, b.status);
-    launchExclusiveScan(N, b.nbrCount, b.nbrOffset, b.scanTmp, &b.status->totalNeighbors, st);
-    kNeighborSearch<1><<<warpBlocks, kSearchWarps * 32, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz,
-                                                   b.atomCell, b.cellStart, b.cellCount, b.cellPos, nullptr,
-                                                   b.nbrOffset,
-                                                   b.nbrCapacity, b.scrKey, b.scrD, b.scrDx, b.scrDy, b.scrDz,
-                                                   b.status);
+    if (b.scrStride > 0)
+    {
+        kNeighborSearch<2><<<warpBlocks, kSearchWarps * 32, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz,
+                                                       b.atomCell, b.cellStart, b.cellCount, b.cellPos, b.nbrCount,
+                                                       nullptr, 0, b.scrKey, b.scrD, b.scrDx, b.scrDy, b.scrDz,
+                                                       b.status, b.scrStride, 0);
+        launchExclusiveScan(N, b.nbrCount, b.nbrOffset, b.scanTmp, &b.status->totalNeighbors, st);
+        kNeighborSearch<1><<<warpBlocks, kSearchWarps * 32, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz,
+                                                       b.atomCell, b.cellStart, b.cellCount, b.cellPos, nullptr,
+                                                       b.nbrOffset,
+                                                       b.nbrCapacity, b.scrKey, b.scrD, b.scrDx, b.scrDy, b.scrDz,
+                                                       b.status, 0, b.scrStride);
+    }
+    else
+    {
+        kNeighborSearch<0><<<warpBlocks, kSearchWarps * 32, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz,
+                                                       b.atomCell, b.cellStart, b.cellCount, b.cellPos, b.nbrCount,
+                                                       nullptr, 0,
+                                                       nullptr, nullptr, nullptr, nullptr, nullptr, b.status, 0, 0);
+        launchExclusiveScan(N, b.nbrCount, b.nbrOffset, b.scanTmp, &b.status->totalNeighbors, st);
+        kNeighborSearch<1><<<warpBlocks, kSearchWarps * 32, 0, st>>>(N, rc2, b.atomStruct, b.info, b.px, b.py, b.pz,
+                                                       b.atomCell, b.cellStart, b.cellCount, b.cellPos, nullptr,
+                                                       b.nbrOffset,
+                                                       b.nbrCapacity, b.scrKey, b.scrD, b.scrDx, b.scrDy, b.scrDz,
+                                                       b.status, 0, 0);
+    }
     kNeighborSort<<<warpBlocks, 256, 0, st>>>(N, b.atomStruct, b.info, b.nbrOffset, b.nbrCapacity, b.scrKey, b.scrD,
                                               b.scrDx, b.scrDy, b.scrDz, b.elem, b.nbrJ, b.nbrCode, b.nbrElem,
-                                              b.nbrD, b.nbrDx, b.nbrDy, b.nbrDz);
+                                              b.nbrD, b.nbrDx, b.nbrDy, b.nbrDz, b.scrStride, b.status);
     kNeighborReverse<<<warpBlocks, 256, 0, st>>>(N, b.atomStruct, b.info, b.nbrOffset, b.nbrCapacity, b.nbrJ,
                                                  b.nbrCode, b.rev, b.status);
 }

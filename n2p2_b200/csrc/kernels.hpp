@@ -44,6 +44,8 @@ struct BatchView
     int* nbrCount = nullptr;
     int64_t* nbrOffset = nullptr;      // N+1
     int64_t nbrCapacity = 0;
+    int64_t scrStride = 0;             // > 0: one search pass writes atom i's entries at i * scrStride
+                                       // (no count pass); 0: count, scan, then fill at nbrOffset[i]
     int64_t* scrKey = nullptr;
     double* scrD = nullptr;
     double* scrDx = nullptr;

@@ -101,3 +101,67 @@ def test_denser_positions_through_host_evaluation():
     cap1, rec1 = b.neighborCapacity()
     assert rec1 == 1 and cap1 > cap0
     _check_against_reference(dense, E, F)
+
+
+def _same_lists(a, b):
+    assert np.array_equal(a["offset"], b["offset"])
+    assert np.array_equal(a["index"], b["index"])
+    assert np.array_equal(a["image"], b["image"])
+    assert np.array_equal(a["d"].view(np.int64), b["d"].view(np.int64))
+    assert np.array_equal(a["dr"].view(np.int64), b["dr"].view(np.int64))
+
+
+def test_one_pass_search_and_stride_overflow():
+    """After the first evaluation (count pass, scan, fill pass) a batch
+    searches once into a fixed stride per atom (its largest count plus 1/8
+    and 16).  The one-pass lists equal the two-pass lists bit for bit, on the
+    same positions and on new ones.  New positions that make one atom's list
+    outgrow the stride (forty molecules of one box moved onto a shell of
+    2 bohr around its first oxygen) make the replayed evaluation run the
+    fill pass on the device as well: no repeated evaluation, the same
+    capacity, and lists and energies equal those of a fresh batch of the same
+    frames -- in that evaluation and in the next, recorded with a wider
+    stride."""
+    boxes = [water.water_box(n, seed=60 + k) for k, n in enumerate([64, 96, 128, 160] * 3)]
+    m = H.gpu_mode(H.WATER40)
+    b = m.batch(boxes)
+    b.setPositions(np.concatenate([s.positions for s in boxes]))
+    b.evaluate(forces=True)          # two passes; sizes the buffers and the stride
+    ref = b.neighbors()
+    E0 = b.energies()
+    b.evaluate(forces=True)          # one pass from here on
+    _same_lists(b.neighbors(), ref)
+    assert np.array_equal(b.energies().view(np.int64), E0.view(np.int64))
+    cap0, rec0 = b.neighborCapacity()
+    counts0 = np.diff(ref["offset"])
+
+    rng = np.random.default_rng(3)
+    moved = []
+    for s in boxes:
+        p = s.positions + rng.normal(scale=0.05, size=s.positions.shape)
+        moved.append(Structure(p, s.elements, s.box))
+    b.setPositions(np.concatenate([s.positions for s in moved]))
+    b.evaluate(forces=True)
+    fresh = H.gpu_batch(m, moved)
+    _same_lists(b.neighbors(), fresh.neighbors())
+    assert b.neighborCapacity() == (cap0, rec0)
+
+    last = boxes[-1]
+    p = last.positions.reshape(-1, 3, 3).copy()
+    centre = p[0, 0]
+    dirs = rng.normal(size=(40, 3))
+    dirs /= np.linalg.norm(dirs, axis=1)[:, None]
+    for k in range(40):
+        p[k + 1] += centre + 2.0 * dirs[k] - p[k + 1, 0]
+    dense = boxes[:-1] + [Structure(p.reshape(-1, 3), last.elements, last.box)]
+    fresh = H.gpu_batch(m, dense)
+    nb = fresh.neighbors()
+    stride = ((counts0.max() + counts0.max() // 8 + 16 + 7) // 8) * 8
+    assert np.diff(nb["offset"]).max() > stride, "one atom must outgrow the search stride"
+    assert len(nb["d"]) <= cap0, "the total must still fit the buffers"
+    b.setPositions(np.concatenate([s.positions for s in dense]))
+    for _ in range(2):               # the replay with the old stride, then one recorded with a wider one
+        b.evaluate(forces=True)
+        _same_lists(b.neighbors(), nb)
+        assert np.allclose(b.energies(), fresh.energies(), rtol=1e-12, atol=0.0)
+        assert b.neighborCapacity() == (cap0, rec0)
