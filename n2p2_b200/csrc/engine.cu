@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <mutex>
 #include <set>
 #include <sstream>
@@ -25,20 +26,22 @@ void cudaCheck(cudaError_t e, char const* what)
 
 void setDynamicSmemOnce(const void* kernel, size_t bytes)
 {
+    // per kernel and device the largest size set so far: a model that needs more raises it
     static std::mutex mu;
-    static std::set<std::pair<const void*, int>> done;
+    static std::map<std::pair<const void*, int>, size_t> done;
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(mu);
     auto key = std::make_pair(kernel, dev);
-    if (done.count(key)) return;
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return;
     cudaCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
               "cudaFuncSetAttribute");
     // Warp-per-atom kernels are limited by shared memory per SM: ask for the
     // largest carveout so as many blocks as the registers allow stay resident.
     cudaCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100),
               "cudaFuncSetAttribute");
-    done.insert(key);
+    done[key] = bytes;
 }
 
 // Size classes: 256-byte steps up to 64 KiB, then quarter steps between

@@ -5,6 +5,8 @@
 // 761-896) for the activations of the reference, and dE/dG by reverse-mode
 // accumulation, which equals NeuralNetwork::calculateDEdG
 // (NeuralNetwork.cpp:396-442) including the normalize_nodes divisions.
+#include <algorithm>
+
 #include "kernels_common.cuh"
 
 #include <math_constants.h>
@@ -174,6 +176,189 @@ __global__ void __launch_bounds__(kNNWarps * 32) kNetworkFP64(DevModel model, Ba
         }
     }
 }
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Tiled FP64 networks: one block per tile of kNetTile atoms of one element
+// (element-grouped atom list).  Activations, derivatives and the reverse
+// pass's vectors live in shared memory neuron-major ([neuron][atom], rows of
+// kNetRow doubles); each thread computes a unit of four atoms x one neuron,
+// reading a weight once (through the read-only cache: every block of an
+// element reads the same matrices) for four fused multiply-adds.  Every sum
+// runs over the reduction index in ascending order, as in propagateLayer.
+constexpr int kNetTile = 32;
+constexpr int kNetRow = 36;        // 32 atoms, padded against bank conflicts (rows stay 32-byte aligned)
+constexpr int kNetThreads = 128;
+constexpr int kNetQuads = kNetTile / 4;
+
+__host__ __device__ inline int netSmemDoubles(DevElement const& E)
+{
+    int maxW = 0, sumD = 0;
+    for (int l = 0; l < E.numLayers; ++l) maxW = E.neurons[l] > maxW ? E.neurons[l] : maxW;
+    for (int l = 1; l < E.numLayers; ++l) sumD += E.neurons[l];
+    return (2 * maxW + sumD + 2 * maxW) * kNetRow;   // activations, derivatives per layer, reverse vectors
+}
+
+// out[k][a] = act(sum_j W[k][j] in[j][a] + b[k]) (normalize: x / nin), with f' kept.
+__device__ __forceinline__ void netForwardLayer(int af, int nin, int nout, const double* __restrict__ WT,
+                                                const double* __restrict__ bias, int normalize, const double* in,
+                                                double* out, double* df, int tid)
+{
+    for (int u = tid; u < kNetQuads * nout; u += kNetThreads)
+    {
+        const int k = u % nout, q = u / nout;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        const double* x = in + 4 * q;
+        for (int j = 0; j < nin; ++j)
+        {
+            const double w = __ldg(&WT[(size_t)j * nout + k]);
+            const double2 p = *reinterpret_cast<const double2*>(x + j * kNetRow);
+            const double2 r = *reinterpret_cast<const double2*>(x + j * kNetRow + 2);
+            a0 += w * p.x;
+            a1 += w * p.y;
+            a2 += w * r.x;
+            a3 += w * r.y;
+        }
+        const double bk = __ldg(&bias[k]);
+        double v[4] = {a0 + bk, a1 + bk, a2 + bk, a3 + bk};
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+        {
+            if (normalize) v[c] /= nin;
+            double y, dy;
+            activate(af, v[c], y, dy);
+            out[k * kNetRow + 4 * q + c] = y;
+            df[k * kNetRow + 4 * q + c] = dy;
+        }
+    }
+}
+
+// out[j][a] = scale[j][a] * sum_k W[k][j] g[k][a] (divided by div when > 0;
+// scale = nullptr: 1).
+__device__ __forceinline__ void netBackwardLayer(int nin, int nout, const double* __restrict__ W, const double* g,
+                                                 const double* scale, int div, double* out, int tid)
+{
+    for (int u = tid; u < kNetQuads * nin; u += kNetThreads)
+    {
+        const int j = u % nin, q = u / nin;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        const double* x = g + 4 * q;
+        for (int k = 0; k < nout; ++k)
+        {
+            const double w = __ldg(&W[(size_t)k * nin + j]);
+            const double2 p = *reinterpret_cast<const double2*>(x + k * kNetRow);
+            const double2 r = *reinterpret_cast<const double2*>(x + k * kNetRow + 2);
+            a0 += w * p.x;
+            a1 += w * p.y;
+            a2 += w * r.x;
+            a3 += w * r.y;
+        }
+        double v[4] = {a0, a1, a2, a3};
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+        {
+            if (scale) v[c] *= scale[j * kNetRow + 4 * q + c];
+            if (div > 0) v[c] /= div;
+            out[j * kNetRow + 4 * q + c] = v[c];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kNetThreads) kNetworkTiled(DevModel model, BatchView b, int derivatives)
+{
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    double* sm = reinterpret_cast<double*>(smemRaw);
+    const int tid = threadIdx.x;
+    // tiles of every element, in element order
+    int tilesOf[kDevMaxElements + 1];
+    tilesOf[0] = 0;
+    for (int e = 0; e < model.numElements; ++e)
+        tilesOf[e + 1] = tilesOf[e] + (b.elemBegin[e + 1] - b.elemBegin[e] + kNetTile - 1) / kNetTile;
+    for (int tile = blockIdx.x; tile < tilesOf[model.numElements]; tile += gridDim.x)
+    {
+        int e = 0;
+        while (tile >= tilesOf[e + 1]) ++e;
+        DevElement const& E = model.el[e];
+        const int L = E.numLayers;
+        const int first = b.elemBegin[e] + (tile - tilesOf[e]) * kNetTile;
+        const int count = min(kNetTile, b.elemBegin[e + 1] - first);
+        int maxW = 0;
+        for (int l = 0; l < L; ++l) maxW = max(maxW, E.neurons[l]);
+        double* act[2] = {sm, sm + maxW * kNetRow};
+        double* dfBase = sm + 2 * maxW * kNetRow;
+        double* gv[2];
+        {
+            int sumD = 0;
+            for (int l = 1; l < L; ++l) sumD += E.neurons[l];
+            gv[0] = dfBase + sumD * kNetRow;
+            gv[1] = gv[0] + maxW * kNetRow;
+        }
+        // the tile's G rows, neuron-major (atoms beyond the element's last: zeros)
+        const int nin0 = E.neurons[0];
+        for (int idx = tid; idx < kNetTile * nin0; idx += kNetThreads)
+        {
+            const int a = idx / nin0, j = idx - a * nin0;
+            act[0][j * kNetRow + a] = a < count ? b.G[(size_t)b.elemAtoms[first + a] * b.gStride + j] : 0.0;
+        }
+        __syncthreads();
+        int cur = 0;
+        double* df = dfBase;
+        double* dfOf[kDevMaxLayers];
+        for (int l = 1; l < L; ++l)
+        {
+            dfOf[l] = df;
+            netForwardLayer(E.activation[l], E.neurons[l - 1], E.neurons[l], model.weightsT + E.wOffset[l],
+                            model.weights + E.bOffset[l], model.normalizeNeurons, act[cur], act[cur ^ 1], df, tid);
+            df += E.neurons[l] * kNetRow;
+            __syncthreads();
+            cur ^= 1;
+        }
+        if (tid < count) b.Eatom[b.elemAtoms[first + tid]] = act[cur][tid];
+        if (!derivatives) continue;
+        // reverse pass: g = f'_L (/ n_{L-1}), g_{l-1} = f'_{l-1} (W_l^T g_l) (/ n_{l-2}), dE/dG = W_1^T g_1
+        for (int a = tid; a < kNetTile; a += kNetThreads)
+        {
+            double g0 = dfOf[L - 1][a];
+            if (model.normalizeNeurons) g0 /= E.neurons[L - 2];
+            gv[0][a] = g0;
+        }
+        __syncthreads();
+        int gc = 0;
+        for (int l = L - 1; l >= 2; --l)
+        {
+            netBackwardLayer(E.neurons[l - 1], E.neurons[l], model.weights + E.wOffset[l], gv[gc], dfOf[l - 1],
+                             model.normalizeNeurons ? E.neurons[l - 2] : 0, gv[gc ^ 1], tid);
+            __syncthreads();
+            gc ^= 1;
+        }
+        // dE/dG into the atoms' rows (four atoms per unit; rows of atoms beyond the element are not written)
+        const int nout1 = E.neurons[1];
+        const double* W1 = model.weights + E.wOffset[1];
+        for (int u = tid; u < kNetQuads * nin0; u += kNetThreads)
+        {
+            const int j = u % nin0, q = u / nin0;
+            double v[4] = {0.0, 0.0, 0.0, 0.0};
+            const double* x = gv[gc] + 4 * q;
+            for (int k = 0; k < nout1; ++k)
+            {
+                const double w = __ldg(&W1[(size_t)k * nin0 + j]);
+                const double2 p = *reinterpret_cast<const double2*>(x + k * kNetRow);
+                const double2 r = *reinterpret_cast<const double2*>(x + k * kNetRow + 2);
+                v[0] += w * p.x;
+                v[1] += w * p.y;
+                v[2] += w * r.x;
+                v[3] += w * r.y;
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (4 * q + c < count) b.dEdG[(size_t)b.elemAtoms[first + 4 * q + c] * b.gStride + j] = v[c];
+        }
+        __syncthreads();
+    }
+}
+
+} // namespace
 
 // E_s = sum of atomic energies of structure s (Mode::calculateEnergy,
 // Mode.cpp:1876-1901), one warp per structure, fixed summation order.
@@ -377,6 +562,22 @@ void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cu
 
 void launchNetworkFP64(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st)
 {
+    // tiles of 32 atoms while their shared memory leaves at least two blocks per SM
+    int doubles = 0, tiles = 0;
+    for (int e = 0; e < m.numElements; ++e)
+    {
+        doubles = std::max(doubles, netSmemDoubles(m.el[e]));
+        tiles += (b.elemBegin[e + 1] - b.elemBegin[e] + kNetTile - 1) / kNetTile;
+    }
+    const size_t tileSmem = (size_t)doubles * sizeof(double);
+    if (tileSmem <= 110 * 1024)
+    {
+        if (tiles == 0) return;
+        setDynamicSmemOnce(reinterpret_cast<const void*>(kNetworkTiled), tileSmem);
+        const int perSM = std::max(1, std::min(4, (int)(233472 / (tileSmem + 1024))));
+        kNetworkTiled<<<std::min(tiles, sms * perSM), kNetThreads, tileSmem, st>>>(m, b, derivatives);
+        return;
+    }
     size_t smem = sizeof(NNWarpSmem) * kNNWarps;
     setDynamicSmemOnce(reinterpret_cast<const void*>(kNetworkFP64), smem);
     int blocks = (b.N + kNNWarps - 1) / kNNWarps;

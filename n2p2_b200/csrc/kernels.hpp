@@ -87,7 +87,8 @@ void inverseBoxOf(double const* box, double* invbox);
 // Throws std::runtime_error("CUDA error in ...") on failure.
 void cudaCheck(cudaError_t e, char const* what);
 
-// Raise a kernel's dynamic shared-memory limit once per process.
+// Raise a kernel's dynamic shared-memory limit to `bytes` on the current
+// device (a no-op when an earlier call already set as much).
 void setDynamicSmemOnce(const void* kernel, size_t bytes);
 
 // neighbour list
