@@ -183,14 +183,15 @@ namespace {
 // Tiled FP64 networks: one block per tile of kNetTile atoms of one element
 // (element-grouped atom list).  Activations, derivatives and the reverse
 // pass's vectors live in shared memory neuron-major ([neuron][atom], rows of
-// kNetRow doubles); each thread computes a unit of four atoms x one neuron,
-// reading a weight once (through the read-only cache: every block of an
-// element reads the same matrices) for four fused multiply-adds.  Every sum
+// kNetRow doubles); each thread computes a unit of kNetUnit atoms x one
+// neuron, reading a weight once (through the read-only cache: every block of
+// an element reads the same matrices) for kNetUnit fused multiply-adds.  Every sum
 // runs over the reduction index in ascending order, as in propagateLayer.
 constexpr int kNetTile = 32;
 constexpr int kNetRow = 36;        // 32 atoms, padded against bank conflicts (rows stay 32-byte aligned)
 constexpr int kNetThreads = 128;
-constexpr int kNetQuads = kNetTile / 4;
+constexpr int kNetUnit = 8;                 // atoms per thread unit (independent sums)
+constexpr int kNetUnits = kNetTile / kNetUnit;
 
 __host__ __device__ inline int netSmemDoubles(DevElement const& E)
 {
@@ -200,72 +201,71 @@ __host__ __device__ inline int netSmemDoubles(DevElement const& E)
     return (2 * maxW + sumD + 2 * maxW) * kNetRow;   // activations, derivatives per layer, reverse vectors
 }
 
+// Sum over the reduction index r < n of w(r) x[r][a] for the unit's kNetUnit
+// atoms (x rows kNetRow apart), in ascending r.
+template <typename WF>
+__device__ __forceinline__ void netUnitSums(int n, WF w, const double* x, double (&v)[kNetUnit])
+{
+#pragma unroll
+    for (int c = 0; c < kNetUnit; ++c) v[c] = 0.0;
+#pragma unroll 4
+    for (int r = 0; r < n; ++r)
+    {
+        const double wr = w(r);
+#pragma unroll
+        for (int c = 0; c < kNetUnit; c += 2)
+        {
+            const double2 p = *reinterpret_cast<const double2*>(x + r * kNetRow + c);
+            v[c] += wr * p.x;
+            v[c + 1] += wr * p.y;
+        }
+    }
+}
+
 // out[k][a] = act(sum_j W[k][j] in[j][a] + b[k]) (normalize: x / nin), with f' kept.
 __device__ __forceinline__ void netForwardLayer(int af, int nin, int nout, const double* __restrict__ WT,
                                                 const double* __restrict__ bias, int normalize, const double* in,
                                                 double* out, double* df, int tid)
 {
-    for (int u = tid; u < kNetQuads * nout; u += kNetThreads)
+    for (int u = tid; u < kNetUnits * nout; u += kNetThreads)
     {
         const int k = u % nout, q = u / nout;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-        const double* x = in + 4 * q;
-        for (int j = 0; j < nin; ++j)
-        {
-            const double w = __ldg(&WT[(size_t)j * nout + k]);
-            const double2 p = *reinterpret_cast<const double2*>(x + j * kNetRow);
-            const double2 r = *reinterpret_cast<const double2*>(x + j * kNetRow + 2);
-            a0 += w * p.x;
-            a1 += w * p.y;
-            a2 += w * r.x;
-            a3 += w * r.y;
-        }
+        double v[kNetUnit];
+        netUnitSums(nin, [&](int j) { return __ldg(&WT[(size_t)j * nout + k]); }, in + kNetUnit * q, v);
         const double bk = __ldg(&bias[k]);
-        double v[4] = {a0 + bk, a1 + bk, a2 + bk, a3 + bk};
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+        for (int c = 0; c < kNetUnit; ++c)
         {
-            if (normalize) v[c] /= nin;
+            double x = v[c] + bk;
+            if (normalize) x /= nin;
             double y, dy;
-            activate(af, v[c], y, dy);
-            out[k * kNetRow + 4 * q + c] = y;
-            df[k * kNetRow + 4 * q + c] = dy;
+            activate(af, x, y, dy);
+            out[k * kNetRow + kNetUnit * q + c] = y;
+            df[k * kNetRow + kNetUnit * q + c] = dy;
         }
     }
 }
 
-// out[j][a] = scale[j][a] * sum_k W[k][j] g[k][a] (divided by div when > 0;
-// scale = nullptr: 1).
+// out[j][a] = scale[j][a] * sum_k W[k][j] g[k][a] (divided by div when > 0).
 __device__ __forceinline__ void netBackwardLayer(int nin, int nout, const double* __restrict__ W, const double* g,
                                                  const double* scale, int div, double* out, int tid)
 {
-    for (int u = tid; u < kNetQuads * nin; u += kNetThreads)
+    for (int u = tid; u < kNetUnits * nin; u += kNetThreads)
     {
         const int j = u % nin, q = u / nin;
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-        const double* x = g + 4 * q;
-        for (int k = 0; k < nout; ++k)
-        {
-            const double w = __ldg(&W[(size_t)k * nin + j]);
-            const double2 p = *reinterpret_cast<const double2*>(x + k * kNetRow);
-            const double2 r = *reinterpret_cast<const double2*>(x + k * kNetRow + 2);
-            a0 += w * p.x;
-            a1 += w * p.y;
-            a2 += w * r.x;
-            a3 += w * r.y;
-        }
-        double v[4] = {a0, a1, a2, a3};
+        double v[kNetUnit];
+        netUnitSums(nout, [&](int k) { return __ldg(&W[(size_t)k * nin + j]); }, g + kNetUnit * q, v);
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+        for (int c = 0; c < kNetUnit; ++c)
         {
-            if (scale) v[c] *= scale[j * kNetRow + 4 * q + c];
-            if (div > 0) v[c] /= div;
-            out[j * kNetRow + 4 * q + c] = v[c];
+            double x = v[c] * scale[j * kNetRow + kNetUnit * q + c];
+            if (div > 0) x /= div;
+            out[j * kNetRow + kNetUnit * q + c] = x;
         }
     }
 }
 
-__global__ void __launch_bounds__(kNetThreads) kNetworkTiled(DevModel model, BatchView b, int derivatives)
+__global__ void __launch_bounds__(kNetThreads, 3) kNetworkTiled(DevModel model, BatchView b, int derivatives)
 {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     double* sm = reinterpret_cast<double*>(smemRaw);
@@ -332,27 +332,18 @@ __global__ void __launch_bounds__(kNetThreads) kNetworkTiled(DevModel model, Bat
             __syncthreads();
             gc ^= 1;
         }
-        // dE/dG into the atoms' rows (four atoms per unit; rows of atoms beyond the element are not written)
+        // dE/dG into the atoms' rows (rows of atoms beyond the element are not written)
         const int nout1 = E.neurons[1];
         const double* W1 = model.weights + E.wOffset[1];
-        for (int u = tid; u < kNetQuads * nin0; u += kNetThreads)
+        for (int u = tid; u < kNetUnits * nin0; u += kNetThreads)
         {
             const int j = u % nin0, q = u / nin0;
-            double v[4] = {0.0, 0.0, 0.0, 0.0};
-            const double* x = gv[gc] + 4 * q;
-            for (int k = 0; k < nout1; ++k)
-            {
-                const double w = __ldg(&W1[(size_t)k * nin0 + j]);
-                const double2 p = *reinterpret_cast<const double2*>(x + k * kNetRow);
-                const double2 r = *reinterpret_cast<const double2*>(x + k * kNetRow + 2);
-                v[0] += w * p.x;
-                v[1] += w * p.y;
-                v[2] += w * r.x;
-                v[3] += w * r.y;
-            }
+            double v[kNetUnit];
+            netUnitSums(nout1, [&](int k) { return __ldg(&W1[(size_t)k * nin0 + j]); }, gv[gc] + kNetUnit * q, v);
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
-                if (4 * q + c < count) b.dEdG[(size_t)b.elemAtoms[first + 4 * q + c] * b.gStride + j] = v[c];
+            for (int c = 0; c < kNetUnit; ++c)
+                if (kNetUnit * q + c < count)
+                    b.dEdG[(size_t)b.elemAtoms[first + kNetUnit * q + c] * b.gStride + j] = v[c];
         }
         __syncthreads();
     }
