@@ -180,30 +180,31 @@ __global__ void __launch_bounds__(kNNWarps * 32) kNetworkFP64(DevModel model, Ba
 namespace {
 
 // ---------------------------------------------------------------------------
-// Tiled FP64 networks: one block per tile of kNetTile atoms of one element
+// Tiled FP64 networks: one block per tile of TILE (32, or 16 for wide networks) atoms of one element
 // (element-grouped atom list).  Activations, derivatives and the reverse
 // pass's vectors live in shared memory neuron-major ([neuron][atom], rows of
-// kNetRow doubles); each thread computes a unit of kNetUnit atoms x one
+// netRow doubles); each thread computes a unit of kNetUnit atoms x one
 // neuron, reading a weight once (through the read-only cache: every block of
 // an element reads the same matrices) for kNetUnit fused multiply-adds.  Every sum
 // runs over the reduction index in ascending order, as in propagateLayer.
-constexpr int kNetTile = 32;
-constexpr int kNetRow = 36;        // 32 atoms, padded against bank conflicts (rows stay 32-byte aligned)
 constexpr int kNetThreads = 128;
-constexpr int kNetUnit = 8;                 // atoms per thread unit (independent sums)
-constexpr int kNetUnits = kNetTile / kNetUnit;
+constexpr int kNetUnit = 8;        // atoms per thread unit (independent sums)
 
-__host__ __device__ inline int netSmemDoubles(DevElement const& E)
+// Row of a tile of TILE atoms: padded by four against bank conflicts (rows stay 32-byte aligned).
+template <int TILE>
+__host__ __device__ constexpr int netRow() { return TILE + 4; }
+
+__host__ __device__ inline int netSmemDoubles(DevElement const& E, int row)
 {
     int maxW = 0, sumD = 0;
     for (int l = 0; l < E.numLayers; ++l) maxW = E.neurons[l] > maxW ? E.neurons[l] : maxW;
     for (int l = 1; l < E.numLayers; ++l) sumD += E.neurons[l];
-    return (2 * maxW + sumD + 2 * maxW) * kNetRow;   // activations, derivatives per layer, reverse vectors
+    return (2 * maxW + sumD + 2 * maxW) * row;   // activations, derivatives per layer, reverse vectors
 }
 
 // Sum over the reduction index r < n of w(r) x[r][a] for the unit's kNetUnit
-// atoms (x rows kNetRow apart), in ascending r.
-template <typename WF>
+// atoms (x rows ROW apart), in ascending r.
+template <int ROW, typename WF>
 __device__ __forceinline__ void netUnitSums(int n, WF w, const double* x, double (&v)[kNetUnit])
 {
 #pragma unroll
@@ -215,7 +216,7 @@ __device__ __forceinline__ void netUnitSums(int n, WF w, const double* x, double
 #pragma unroll
         for (int c = 0; c < kNetUnit; c += 2)
         {
-            const double2 p = *reinterpret_cast<const double2*>(x + r * kNetRow + c);
+            const double2 p = *reinterpret_cast<const double2*>(x + r * ROW + c);
             v[c] += wr * p.x;
             v[c + 1] += wr * p.y;
         }
@@ -223,15 +224,16 @@ __device__ __forceinline__ void netUnitSums(int n, WF w, const double* x, double
 }
 
 // out[k][a] = act(sum_j W[k][j] in[j][a] + b[k]) (normalize: x / nin), with f' kept.
+template <int TILE>
 __device__ __forceinline__ void netForwardLayer(int af, int nin, int nout, const double* __restrict__ WT,
                                                 const double* __restrict__ bias, int normalize, const double* in,
                                                 double* out, double* df, int tid)
 {
-    for (int u = tid; u < kNetUnits * nout; u += kNetThreads)
+    for (int u = tid; u < (TILE / kNetUnit) * nout; u += kNetThreads)
     {
         const int k = u % nout, q = u / nout;
         double v[kNetUnit];
-        netUnitSums(nin, [&](int j) { return __ldg(&WT[(size_t)j * nout + k]); }, in + kNetUnit * q, v);
+        netUnitSums<netRow<TILE>()>(nin, [&](int j) { return __ldg(&WT[(size_t)j * nout + k]); }, in + kNetUnit * q, v);
         const double bk = __ldg(&bias[k]);
 #pragma unroll
         for (int c = 0; c < kNetUnit; ++c)
@@ -240,31 +242,33 @@ __device__ __forceinline__ void netForwardLayer(int af, int nin, int nout, const
             if (normalize) x /= nin;
             double y, dy;
             activate(af, x, y, dy);
-            out[k * kNetRow + kNetUnit * q + c] = y;
-            df[k * kNetRow + kNetUnit * q + c] = dy;
+            out[k * netRow<TILE>() + kNetUnit * q + c] = y;
+            df[k * netRow<TILE>() + kNetUnit * q + c] = dy;
         }
     }
 }
 
 // out[j][a] = scale[j][a] * sum_k W[k][j] g[k][a] (divided by div when > 0).
+template <int TILE>
 __device__ __forceinline__ void netBackwardLayer(int nin, int nout, const double* __restrict__ W, const double* g,
                                                  const double* scale, int div, double* out, int tid)
 {
-    for (int u = tid; u < kNetUnits * nin; u += kNetThreads)
+    for (int u = tid; u < (TILE / kNetUnit) * nin; u += kNetThreads)
     {
         const int j = u % nin, q = u / nin;
         double v[kNetUnit];
-        netUnitSums(nout, [&](int k) { return __ldg(&W[(size_t)k * nin + j]); }, g + kNetUnit * q, v);
+        netUnitSums<netRow<TILE>()>(nout, [&](int k) { return __ldg(&W[(size_t)k * nin + j]); }, g + kNetUnit * q, v);
 #pragma unroll
         for (int c = 0; c < kNetUnit; ++c)
         {
-            double x = v[c] * scale[j * kNetRow + kNetUnit * q + c];
+            double x = v[c] * scale[j * netRow<TILE>() + kNetUnit * q + c];
             if (div > 0) x /= div;
-            out[j * kNetRow + kNetUnit * q + c] = x;
+            out[j * netRow<TILE>() + kNetUnit * q + c] = x;
         }
     }
 }
 
+template <int TILE>
 __global__ void __launch_bounds__(kNetThreads, 3) kNetworkTiled(DevModel model, BatchView b, int derivatives)
 {
     extern __shared__ __align__(16) unsigned char smemRaw[];
@@ -274,32 +278,32 @@ __global__ void __launch_bounds__(kNetThreads, 3) kNetworkTiled(DevModel model, 
     int tilesOf[kDevMaxElements + 1];
     tilesOf[0] = 0;
     for (int e = 0; e < model.numElements; ++e)
-        tilesOf[e + 1] = tilesOf[e] + (b.elemBegin[e + 1] - b.elemBegin[e] + kNetTile - 1) / kNetTile;
+        tilesOf[e + 1] = tilesOf[e] + (b.elemBegin[e + 1] - b.elemBegin[e] + TILE - 1) / TILE;
     for (int tile = blockIdx.x; tile < tilesOf[model.numElements]; tile += gridDim.x)
     {
         int e = 0;
         while (tile >= tilesOf[e + 1]) ++e;
         DevElement const& E = model.el[e];
         const int L = E.numLayers;
-        const int first = b.elemBegin[e] + (tile - tilesOf[e]) * kNetTile;
-        const int count = min(kNetTile, b.elemBegin[e + 1] - first);
+        const int first = b.elemBegin[e] + (tile - tilesOf[e]) * TILE;
+        const int count = min(TILE, b.elemBegin[e + 1] - first);
         int maxW = 0;
         for (int l = 0; l < L; ++l) maxW = max(maxW, E.neurons[l]);
-        double* act[2] = {sm, sm + maxW * kNetRow};
-        double* dfBase = sm + 2 * maxW * kNetRow;
+        double* act[2] = {sm, sm + maxW * netRow<TILE>()};
+        double* dfBase = sm + 2 * maxW * netRow<TILE>();
         double* gv[2];
         {
             int sumD = 0;
             for (int l = 1; l < L; ++l) sumD += E.neurons[l];
-            gv[0] = dfBase + sumD * kNetRow;
-            gv[1] = gv[0] + maxW * kNetRow;
+            gv[0] = dfBase + sumD * netRow<TILE>();
+            gv[1] = gv[0] + maxW * netRow<TILE>();
         }
         // the tile's G rows, neuron-major (atoms beyond the element's last: zeros)
         const int nin0 = E.neurons[0];
-        for (int idx = tid; idx < kNetTile * nin0; idx += kNetThreads)
+        for (int idx = tid; idx < TILE * nin0; idx += kNetThreads)
         {
             const int a = idx / nin0, j = idx - a * nin0;
-            act[0][j * kNetRow + a] = a < count ? b.G[(size_t)b.elemAtoms[first + a] * b.gStride + j] : 0.0;
+            act[0][j * netRow<TILE>() + a] = a < count ? b.G[(size_t)b.elemAtoms[first + a] * b.gStride + j] : 0.0;
         }
         __syncthreads();
         int cur = 0;
@@ -308,16 +312,16 @@ __global__ void __launch_bounds__(kNetThreads, 3) kNetworkTiled(DevModel model, 
         for (int l = 1; l < L; ++l)
         {
             dfOf[l] = df;
-            netForwardLayer(E.activation[l], E.neurons[l - 1], E.neurons[l], model.weightsT + E.wOffset[l],
+            netForwardLayer<TILE>(E.activation[l], E.neurons[l - 1], E.neurons[l], model.weightsT + E.wOffset[l],
                             model.weights + E.bOffset[l], model.normalizeNeurons, act[cur], act[cur ^ 1], df, tid);
-            df += E.neurons[l] * kNetRow;
+            df += E.neurons[l] * netRow<TILE>();
             __syncthreads();
             cur ^= 1;
         }
         if (tid < count) b.Eatom[b.elemAtoms[first + tid]] = act[cur][tid];
         if (!derivatives) continue;
         // reverse pass: g = f'_L (/ n_{L-1}), g_{l-1} = f'_{l-1} (W_l^T g_l) (/ n_{l-2}), dE/dG = W_1^T g_1
-        for (int a = tid; a < kNetTile; a += kNetThreads)
+        for (int a = tid; a < TILE; a += kNetThreads)
         {
             double g0 = dfOf[L - 1][a];
             if (model.normalizeNeurons) g0 /= E.neurons[L - 2];
@@ -327,7 +331,7 @@ __global__ void __launch_bounds__(kNetThreads, 3) kNetworkTiled(DevModel model, 
         int gc = 0;
         for (int l = L - 1; l >= 2; --l)
         {
-            netBackwardLayer(E.neurons[l - 1], E.neurons[l], model.weights + E.wOffset[l], gv[gc], dfOf[l - 1],
+            netBackwardLayer<TILE>(E.neurons[l - 1], E.neurons[l], model.weights + E.wOffset[l], gv[gc], dfOf[l - 1],
                              model.normalizeNeurons ? E.neurons[l - 2] : 0, gv[gc ^ 1], tid);
             __syncthreads();
             gc ^= 1;
@@ -335,11 +339,11 @@ __global__ void __launch_bounds__(kNetThreads, 3) kNetworkTiled(DevModel model, 
         // dE/dG into the atoms' rows (rows of atoms beyond the element are not written)
         const int nout1 = E.neurons[1];
         const double* W1 = model.weights + E.wOffset[1];
-        for (int u = tid; u < kNetUnits * nin0; u += kNetThreads)
+        for (int u = tid; u < (TILE / kNetUnit) * nin0; u += kNetThreads)
         {
             const int j = u % nin0, q = u / nin0;
             double v[kNetUnit];
-            netUnitSums(nout1, [&](int k) { return __ldg(&W1[(size_t)k * nin0 + j]); }, gv[gc] + kNetUnit * q, v);
+            netUnitSums<netRow<TILE>()>(nout1, [&](int k) { return __ldg(&W1[(size_t)k * nin0 + j]); }, gv[gc] + kNetUnit * q, v);
 #pragma unroll
             for (int c = 0; c < kNetUnit; ++c)
                 if (kNetUnit * q + c < count)
@@ -553,22 +557,24 @@ void launchExtrapolationCheck(DevModel const& m, BatchView const& b, int sms, cu
 
 void launchNetworkFP64(DevModel const& m, BatchView const& b, int derivatives, int sms, cudaStream_t st)
 {
-    // tiles of 32 atoms while their shared memory leaves at least two blocks per SM
-    int doubles = 0, tiles = 0;
+    // tiles of 32 atoms (16 for wide networks) while their shared memory leaves at least two blocks per SM
+    int d32 = 0, d16 = 0, t32 = 0, t16 = 0;
     for (int e = 0; e < m.numElements; ++e)
     {
-        doubles = std::max(doubles, netSmemDoubles(m.el[e]));
-        tiles += (b.elemBegin[e + 1] - b.elemBegin[e] + kNetTile - 1) / kNetTile;
+        d32 = std::max(d32, netSmemDoubles(m.el[e], netRow<32>()));
+        d16 = std::max(d16, netSmemDoubles(m.el[e], netRow<16>()));
+        t32 += (b.elemBegin[e + 1] - b.elemBegin[e] + 31) / 32;
+        t16 += (b.elemBegin[e + 1] - b.elemBegin[e] + 15) / 16;
     }
-    const size_t tileSmem = (size_t)doubles * sizeof(double);
-    if (tileSmem <= 110 * 1024)
-    {
+    auto tiled = [&](auto kernel, size_t bytes, int tiles) {
         if (tiles == 0) return;
-        setDynamicSmemOnce(reinterpret_cast<const void*>(kNetworkTiled), tileSmem);
-        const int perSM = std::max(1, std::min(4, (int)(233472 / (tileSmem + 1024))));
-        kNetworkTiled<<<std::min(tiles, sms * perSM), kNetThreads, tileSmem, st>>>(m, b, derivatives);
-        return;
-    }
+        setDynamicSmemOnce(reinterpret_cast<const void*>(kernel), bytes);
+        const int perSM = std::max(1, std::min(4, (int)(233472 / (bytes + 1024))));
+        kernel<<<std::min(tiles, sms * perSM), kNetThreads, bytes, st>>>(m, b, derivatives);
+    };
+    constexpr size_t kTileBudget = 110 * 1024;
+    if ((size_t)d32 * sizeof(double) <= kTileBudget) return tiled(kNetworkTiled<32>, (size_t)d32 * sizeof(double), t32);
+    if ((size_t)d16 * sizeof(double) <= kTileBudget) return tiled(kNetworkTiled<16>, (size_t)d16 * sizeof(double), t16);
     size_t smem = sizeof(NNWarpSmem) * kNNWarps;
     setDynamicSmemOnce(reinterpret_cast<const void*>(kNetworkFP64), smem);
     int blocks = (b.N + kNNWarps - 1) / kNNWarps;

@@ -82,10 +82,10 @@ CUTOFFS = [(0, 0.0), (1, 0.2), (2, 0.0), (3, 0.0), (4, 0.2), (5, 0.2), (6, 0.2),
 ACTIVATIONS = ["t t l", "s s l", "r r l", "g g l", "c c l", "S S l", "e e l", "h h l", "l l l", "p t s"]
 
 
-def _variant(tmp_path, name, cutoff=None, activations=None, structures=None):
-    """The water model with another cutoff or activation line; a changed
-    cutoff gets scaling statistics of its own (nnp-scaling on the device over
-    `structures`)."""
+def _variant(tmp_path, name, cutoff=None, activations=None, structures=None, normalize=False):
+    """The water model with another cutoff or activation line (or with
+    normalize_nodes); a changed cutoff gets scaling statistics of its own
+    (nnp-scaling on the device over `structures`)."""
     d = str(tmp_path / name)
     shutil.copytree(H.WATER40, d)
     p = os.path.join(d, "input.nn")
@@ -97,6 +97,8 @@ def _variant(tmp_path, name, cutoff=None, activations=None, structures=None):
         if w and w[0] == "global_activation_short" and activations is not None:
             ln = "global_activation_short %s\n" % activations
         lines.append(ln)
+    if normalize:
+        lines.append("normalize_nodes\n")
     open(p, "w").write("".join(lines))
     if cutoff is not None:
         from n2p2_b200 import Mode
@@ -146,3 +148,17 @@ def test_activation_models(tmp_path, act):
     ss = _structures()
     d = _variant(tmp_path, "act_" + act.replace(" ", "_"), activations=act)
     _check(d, ss, "fp64")
+
+
+def test_normalize_nodes_model(tmp_path):
+    """normalize_nodes: every neuron's weighted input sum divided by the
+    number of neurons feeding it (NeuralNetwork::propagateLayer,
+    NeuralNetwork.cpp:761-790), and the same divisions in dE/dG
+    (calculateDEdG, NeuralNetwork.cpp:396-442).  The water model with the
+    keyword, FP64 (the tiled network kernel) against the reference library;
+    the mixed form runs its networks in FP64 for such models (the
+    tensor-core kernel does not take them)."""
+    ss = _structures()
+    d = _variant(tmp_path, "normalize", normalize=True)
+    _check(d, ss, "fp64")
+    _check(d, ss, "mixed")
