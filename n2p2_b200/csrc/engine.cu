@@ -719,7 +719,7 @@ void Batch::releaseAll()
     freeAll(pool_, ownedDGdr_);
     freeAll(pool_, ownedScr_);
     scrEntries_ = 0;
-    nbrStride_ = 0;
+    nbrStride_ = strideWanted_ = 0;
     v_.scrStride = 0;
     freeAll(pool_, ownedNbr_);
     freeAll(pool_, owned_);
@@ -865,7 +865,7 @@ void Batch::beginExternal(int numCenters, const int* elements, int numTargets, c
     freeAll(pool_, ownedDGdr_);
     freeAll(pool_, ownedScr_);
     scrEntries_ = 0;
-    nbrStride_ = 0;
+    nbrStride_ = strideWanted_ = 0;
     v_.scrStride = 0;
     freeAll(pool_, ownedNbr_);
     freeAll(pool_, owned_);
@@ -1603,14 +1603,17 @@ void Batch::evaluate(int flags, int precision, int checkExtrapolation)
         // Later evaluations search once into a fixed stride of the largest count plus 1/8 and 16
         // (the count pass skipped), while N x stride stays within twice the packed entries; an
         // evaluation in which an atom outgrows the stride also runs the fill pass on the device.
+        // (the scratch is allocated at the next evaluation: a batch evaluated once never needs it).
+        strideWanted_ = 0;
         if (!external_ && st.maxNeighbors > 0)
         {
             const int64_t stride = strideFor(st.maxNeighbors);
-            if ((int64_t)N_ * stride <= 2 * capacity_) setStride(stride);
+            if ((int64_t)N_ * stride <= 2 * capacity_) strideWanted_ = stride;
         }
         capacityVerified_ = true;
         return;
     }
+    setStride(strideWanted_);
     if (flags & EVAL_NO_GRAPH)
     {
         record(flags, precision, checkExtrapolation);
@@ -1654,7 +1657,7 @@ void Batch::verify()
     if (nbrStride_ > 0 && st.maxNeighbors > nbrStride_)
     {
         const int64_t stride = strideFor(st.maxNeighbors);
-        setStride((int64_t)N_ * stride <= 2 * capacity_ ? stride : 0);
+        strideWanted_ = (int64_t)N_ * stride <= 2 * capacity_ ? stride : 0;
     }
     if (st.totalNeighbors <= capacity_) return;
     // The lists outgrew the buffers sized at the first evaluation: size them

@@ -316,6 +316,7 @@ private:
     std::vector<void*> ownedScr_;     // neighbour-build scratch (unordered entries)
     int64_t scrEntries_ = 0;
     int64_t nbrStride_ = 0;           // > 0: one-pass neighbour search into fixed-stride scratch
+    int64_t strideWanted_ = 0;        // the stride the next evaluation sets (0: two passes)
     std::vector<void*> ownedDGdr_;
     std::vector<void*> ownedMask_;
     uint32_t* maskBuf_ = nullptr;
