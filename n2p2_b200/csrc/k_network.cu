@@ -298,6 +298,7 @@ __global__ void __launch_bounds__(kNetThreads, 3) kNetworkTiled(DevModel model, 
             gv[0] = dfBase + sumD * netRow<TILE>();
             gv[1] = gv[0] + maxW * netRow<TILE>();
         }
+        __syncthreads();   // the previous tile's reads of the buffers are done (its output may sit in act[0])
         // the tile's G rows, neuron-major (atoms beyond the element's last: zeros)
         const int nin0 = E.neurons[0];
         for (int idx = tid; idx < TILE * nin0; idx += kNetThreads)
