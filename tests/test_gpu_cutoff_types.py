@@ -162,3 +162,49 @@ def test_normalize_nodes_model(tmp_path):
     d = _variant(tmp_path, "normalize", normalize=True)
     _check(d, ss, "fp64")
     _check(d, ss, "mixed")
+
+
+def test_one_hidden_layer_energies_only(tmp_path):
+    """A network with one hidden layer (40-25-1: an even number of weight
+    layers, so the tiled network kernel's output lands in the buffer the next
+    tile loads) on 48 boxes of 128 molecules: more tiles than resident blocks,
+    so blocks evaluate several tiles in turn.  Seeded weights; energies of an
+    energy-only evaluation and energies and forces of a full one against the
+    reference library."""
+    d = str(tmp_path / "hidden1")
+    shutil.copytree(H.WATER40, d)
+    p = os.path.join(d, "input.nn")
+    lines = []
+    for ln in open(p):
+        w = ln.split()
+        if w and w[0] == "global_hidden_layers_short":
+            ln = "global_hidden_layers_short 1\n"
+        elif w and w[0] == "global_nodes_short":
+            ln = "global_nodes_short 25\n"
+        elif w and w[0] == "global_activation_short":
+            ln = "global_activation_short p l\n"
+        lines.append(ln)
+    open(p, "w").write("".join(lines))
+    rng = np.random.default_rng(17)
+    for z in (1, 8):
+        w = rng.normal(scale=0.3, size=40 * 25 + 25 + 25 + 1)
+        with open(os.path.join(d, "weights.%03d.data" % z), "w") as f:
+            f.write("# seeded weights of a 40-25-1 network\n")
+            f.write("".join("%24.16E\n" % x for x in w))
+    ss = [water.water_box(128, seed=200 + k) for k in range(48)]
+    m = H.gpu_mode(d)
+    b = m.batch(ss)
+    b.setPositions(np.concatenate([s.positions for s in ss]))
+    b.evaluate(forces=False)
+    E0 = b.energies()
+    b.evaluate(forces=True)
+    E, F = b.energies(), b.forces()
+    E_ref, F_ref = H.reference_energies_forces(d, ss)
+    a0 = 0
+    for k, s in enumerate(ss):
+        e_ref, f_ref = E_ref[k], F_ref[k]
+        assert abs(E0[k] - e_ref) <= 1e-10 * abs(e_ref), k
+        assert abs(E[k] - e_ref) <= 1e-10 * abs(e_ref), k
+        assert H.max_rel(F[a0:a0 + s.numAtoms], f_ref) <= 1e-10, k
+        a0 += s.numAtoms
+    m.close()
