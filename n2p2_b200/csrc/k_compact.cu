@@ -10,15 +10,20 @@
 // (the product of both for an angle); the narrow types also need the j-k
 // distance inside the radial window and multiply by its radial function.
 //
-// One warp per atom, neighbour data read from the entry arrays.  The G pass
-// sums every member over the neighbours (radial) or the unordered pairs
-// (j < k, angular) lane by lane and combines the lanes by a fixed shuffle
-// tree.  The force pass gives every lane its own neighbours: for entry j it
-// adds the force E_i puts on j over all partners k (each pair is evaluated
-// from both ends, with j in the role of the first neighbour) and its half of
-// the self force; it runs after the Gaussian force pass and adds to that
-// pass's per-entry forces h and self forces.  No atomics; the same result on
-// every run.
+// Two kernel families, one launch per type present, after the Gaussian
+// passes (adding to their G, per-entry forces h and self forces):
+//  * staged angular kernels (kCompactWide*, below): one block per atom with
+//    at most kWideCap neighbours, the members factored into a grid of
+//    distinct radial x angular parts;
+//  * direct kernels (kCompactValues / kCompactForces): the radial types and
+//    the atoms with more neighbours.  One warp per atom over the entry
+//    arrays; the G pass sums every member over the neighbours (radial) or
+//    the unordered pairs (j < k, angular) lane by lane and combines the
+//    lanes by a fixed shuffle tree; the force pass gives every lane its own
+//    entries j and adds the force E_i puts on j over all partners k (each
+//    pair evaluated from both ends, with j in the role of the first
+//    neighbour) and its half of the self force.
+// No atomics; the same result on every run.
 #include <algorithm>
 
 #include "kernels.hpp"
