@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
+#include <thread>
+#include <vector>
 
 namespace n2p2b200 {
 
@@ -212,26 +214,43 @@ void LammpsInterface::transferNeighborList(int inum, const int* ilist, const int
         if (listed[center_[c]]) total += numneigh[center_[c]];
     auto* off = static_cast<int64_t*>(candOffBuf_.ensure(sizeof(int64_t) * ((size_t)n + 1)));
     auto* cand = static_cast<int*>(candBuf_.ensure(sizeof(int) * (size_t)std::max<int64_t>(total, 1)));
-    int maxIndex = 0;
-    int64_t at = 0;
     off[0] = 0;
-    for (int c = 0; c < n; ++c)
-    {
-        const int i = center_[c];
-        maxIndex = std::max(maxIndex, i);
-        if (listed[i])
+    for (int c = 0; c < n; ++c) off[c + 1] = off[c] + (listed[center_[c]] ? numneigh[center_[c]] : 0);
+    // the gather itself by host threads over ranges of centres (each writes its own segments)
+    auto gather = [&](int c0, int c1) {
+        int mx = 0;
+        for (int c = c0; c < c1; ++c)
         {
+            const int i = center_[c];
+            mx = std::max(mx, i);
+            if (!listed[i]) continue;
             const int* nb = firstneigh[i];
+            int* out = cand + off[c];
             for (int q = 0; q < numneigh[i]; ++q)
             {
                 const int j = nb[q] & kNeighMask;
-                cand[at++] = j;
-                maxIndex = std::max(maxIndex, j);
+                out[q] = j;
+                mx = std::max(mx, j);
             }
         }
-        off[c + 1] = at;
+        return mx;
+    };
+    int maxIndex = 0;
+    const int threads = total >= (1 << 20) ? (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency())) : 1;
+    if (threads <= 1) maxIndex = gather(0, n);
+    else
+    {
+        std::vector<int> mx((size_t)threads, 0);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; ++t)
+        {
+            const int c0 = (int)((int64_t)n * t / threads), c1 = (int)((int64_t)n * (t + 1) / threads);
+            pool.emplace_back([&, t, c0, c1] { mx[(size_t)t] = gather(c0, c1); });
+        }
+        for (auto& th : pool) th.join();
+        for (int v : mx) maxIndex = std::max(maxIndex, v);
     }
-    numCand_ = at;
+    numCand_ = off[n];
     numAll_ = maxIndex + 1;
     auto* xs = static_cast<double*>(xBuf_.ensure(sizeof(double) * 3 * (size_t)numAll_));
     auto* ts = static_cast<int*>(typeBuf_.ensure(sizeof(int) * (size_t)numAll_));
