@@ -16,20 +16,41 @@ __global__ void kMaskWords(DevModel model, BatchView b)
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
     {
         const int64_t off = b.nbrOffset[i], end = b.nbrOffset[i + 1];
-        int cnt[4][kDevMaxElements];
-        for (int c = 0; c < 4; ++c)
-            for (int e = 0; e < kDevMaxElements; ++e) cnt[c][e] = 0;
+        // per cutoff slot the neighbour counts of elements 0-3 and 4-7 in 16-bit fields: exact up to
+        // 65535 entries per atom, far beyond the 1024 of the last stage tier (larger atoms are flagged
+        // by the symmetry-function passes and write no masks)
+        uint64_t lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
         if (end <= b.nbrCapacity)
             for (int64_t q = off + lane; q < end; q += 32)
             {
                 const int e = b.nbrElem[q];
                 const double d = b.nbrD[q];
+                const uint64_t one = 1ull << (16 * (e & 3));
+#pragma unroll
                 for (int c = 0; c < 4; ++c)
                     if (c < model.numCutoffSlots && (!model.sortByDistance || d < model.cutoff[c].rc))
-                        for (int f = 0; f < kDevMaxElements; ++f) cnt[c][f] += (e == f) ? 1 : 0;
+                    {
+                        if (e < 4) lo[c] += one;
+                        else hi[c] += one;
+                    }
             }
-        for (int c = 0; c < model.numCutoffSlots; ++c)
-            for (int f = 0; f < model.numElements; ++f) cnt[c][f] = warpSumInt(cnt[c][f]);
+        int cnt[4][kDevMaxElements];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+        {
+            uint64_t l = lo[c], h = hi[c];
+            for (int o = 16; o > 0; o >>= 1)
+            {
+                l += __shfl_xor_sync(kFullMask, l, o);
+                h += __shfl_xor_sync(kFullMask, h, o);
+            }
+#pragma unroll
+            for (int f = 0; f < 4; ++f)
+            {
+                cnt[c][f] = (int)((l >> (16 * f)) & 0xffff);
+                cnt[c][f + 4] = (int)((h >> (16 * f)) & 0xffff);
+            }
+        }
         DevElement const& E = model.el[b.elem[i]];
         int words = 0;
         for (int g = 0; g < E.groupCount; ++g)
