@@ -313,6 +313,27 @@ __global__ void __launch_bounds__(kSearchWarps * 32) kNeighborSearch(
 // Orders every atom's segment by key = (j - atomBegin) * K + imageCode, i.e.
 // j ascending, then images in the reference loop order.  Rank sort: keys are
 // unique within a segment, so an entry's rank is the number of smaller keys.
+// Ranks of the lane's keys e = lane + 32 r (r < R) among the segment's n
+// unique keys: one pass over the keys for all R of them.
+template <int R>
+__device__ __forceinline__ void rankKeys32(const int* keys, int n, int lane, int (&kk)[8], int (&rank)[8])
+{
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+    {
+        const int e = lane + 32 * r;
+        kk[r] = e < n ? keys[e] : 0x7fffffff;
+        rank[r] = 0;
+    }
+#pragma unroll 4
+    for (int q = 0; q < n; ++q)
+    {
+        const int kq = keys[q];
+#pragma unroll
+        for (int r = 0; r < R; ++r) rank[r] += kq < kk[r] ? 1 : 0;
+    }
+}
+
 __global__ void __launch_bounds__(256) kNeighborSort(
     int N, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
     const int64_t* __restrict__ nbrOffset, int64_t capacity, const int64_t* __restrict__ scrKey,
@@ -338,6 +359,43 @@ __global__ void __launch_bounds__(256) kNeighborSort(
         const int64_t src = strided ? (int64_t)i * scrStride : off;   // the atom's scratch segment
         DevStructInfo const& s = info[atomStruct[i]];
         const int K = (2 * s.pbc[0] + 1) * (2 * s.pbc[1] + 1) * (2 * s.pbc[2] + 1);
+        if (n <= 256 && (int64_t)s.numAtoms * K < 0x7fffffff)
+        {
+            // keys as 32-bit integers, every lane's (up to eight) ranked in one pass
+            int* k32 = reinterpret_cast<int*>(skeys[w]);
+            for (int e = lane; e < n; e += 32) k32[e] = (int)scrKey[src + e];
+            __syncwarp();
+            int kk[8], rank[8];
+            switch ((n + 31) >> 5)
+            {
+            case 0: break;
+            case 1: rankKeys32<1>(k32, n, lane, kk, rank); break;
+            case 2: rankKeys32<2>(k32, n, lane, kk, rank); break;
+            case 3: rankKeys32<3>(k32, n, lane, kk, rank); break;
+            case 4: rankKeys32<4>(k32, n, lane, kk, rank); break;
+            case 5: rankKeys32<5>(k32, n, lane, kk, rank); break;
+            case 6: rankKeys32<6>(k32, n, lane, kk, rank); break;
+            case 7: rankKeys32<7>(k32, n, lane, kk, rank); break;
+            default: rankKeys32<8>(k32, n, lane, kk, rank); break;
+            }
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+            {
+                const int e = lane + 32 * r;
+                if (e >= n) break;
+                const int64_t dst = off + rank[r];
+                const int j = kk[r] / K + s.atomBegin;
+                nbrJ[dst] = j;
+                nbrCode[dst] = kk[r] % K;
+                nbrElem[dst] = (uint8_t)elem[j];
+                nbrD[dst] = scrD[src + e];
+                nbrDx[dst] = scrDx[src + e];
+                nbrDy[dst] = scrDy[src + e];
+                nbrDz[dst] = scrDz[src + e];
+            }
+            __syncwarp();
+            continue;
+        }
         const bool inSmem = n <= kSmemKeys;
         if (inSmem)
             for (int e = lane; e < n; e += 32) skeys[w][e] = scrKey[src + e];
