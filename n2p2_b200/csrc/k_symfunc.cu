@@ -111,202 +111,215 @@ __global__ void __launch_bounds__(WARPS * 32) kSFDerivatives(DevModel model, Bat
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < b.N; i += warpsPerGrid)
+    // the warp's atoms i = warp + k warpsPerGrid, tested 32 at a time for the tier
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    for (int k0 = 0; warp + k0 * warpsPerGrid < b.N; k0 += 32)
     {
-        const int64_t off = b.nbrOffset[i];
-        const int64_t end = b.nbrOffset[i + 1];
-        if (end > b.nbrCapacity) continue;
-        const int n = (int)(end - off);
-        if (!takesAtom<CAP, LOWER>(n)) continue;
-        NbrStage<double, CAP>& nb = stage[w];
-        const int ec = b.elem[i];
-        DevElement const& E = model.el[ec];
-        for (int r = 0; r < model.maxRows; ++r)
-            for (int j = lane; j < n; j += 32)
-            {
-                double* p = b.dGdr + ((size_t)r * b.nbrCapacity + off + j) * 3;
-                p[0] = 0.0;
-                p[1] = 0.0;
-                p[2] = 0.0;
-            }
-        int stagedSlot = -1;
-        for (int g = 0; g < E.groupCount; ++g)
+        const int mine = warp + (k0 + lane) * warpsPerGrid;
+        bool inTier = false;
+        if (mine < b.N && b.nbrOffset[mine + 1] <= b.nbrCapacity)
+            inTier = takesAtom<CAP, LOWER>((int)(b.nbrOffset[mine + 1] - b.nbrOffset[mine]));
+        unsigned todo = __ballot_sync(kFullMask, inTier);
+        while (todo)
         {
-            DevGroup const G = model.groups[E.groupBegin + g];
-            if (G.cutoffSlot != stagedSlot)
-            {
-                stageNeighbors<double, CAP>(nb, off, n, b, G.cutoffSlot, lane);
-                stagedSlot = G.cutoffSlot;
-            }
-            const T rc = G.rc, rc2 = G.rc2;
-            for (int m0 = 0; m0 < G.memberCount; m0 += kC)
-            {
-                const int mc = min(kC, G.memberCount - m0);
-                const DevMember* mem = model.members + G.memberBegin + m0;
-                T acc[kC], selfx[kC], selfy[kC], selfz[kC];
-#pragma unroll
-                for (int q = 0; q < kC; ++q) acc[q] = selfx[q] = selfy[q] = selfz[q] = 0.0;
-                if (G.type == 2)
+            const int i = warp + (k0 + __ffs(todo) - 1) * warpsPerGrid;
+            todo &= todo - 1;
+            const int64_t off = b.nbrOffset[i];
+            const int64_t end = b.nbrOffset[i + 1];
+            if (end > b.nbrCapacity) continue;
+            const int n = (int)(end - off);
+            if (!takesAtom<CAP, LOWER>(n)) continue;
+            NbrStage<double, CAP>& nb = stage[w];
+            const int ec = b.elem[i];
+            DevElement const& E = model.el[ec];
+            for (int r = 0; r < model.maxRows; ++r)
+                for (int j = lane; j < n; j += 32)
                 {
-                    for (int j = lane; j < n; j += 32)
-                    {
-                        if (nb.e[j] != G.e1 || !(nb.d[j] < rc)) continue;
-                        const T r = nb.d[j], fc = nb.fc[j], dfc = nb.dfc[j];
-                        const T x = nb.x[j], y = nb.y[j], z = nb.z[j];
-#pragma unroll
-                        for (int q = 0; q < kC; ++q)
-                        {
-                            if (q < mc)
-                            {
-                                DevMember const& M = mem[q];
-                                const T pexp = exp(-M.eta * (r - M.rs) * (r - M.rs));
-                                acc[q] += pexp * fc;
-                                const T p1 = M.factorNorm * (dfc - 2.0 * M.eta * (r - M.rs) * fc) * pexp / r;
-                                selfx[q] += p1 * x;
-                                selfy[q] += p1 * y;
-                                selfz[q] += p1 * z;
-                                double* p = b.dGdr + ((size_t)M.rowE1 * b.nbrCapacity + off + j) * 3;
-                                p[0] -= p1 * x;
-                                p[1] -= p1 * y;
-                                p[2] -= p1 * z;
-                            }
-                        }
-                    }
+                    double* p = b.dGdr + ((size_t)r * b.nbrCapacity + off + j) * 3;
+                    p[0] = 0.0;
+                    p[1] = 0.0;
+                    p[2] = 0.0;
                 }
-                else
+            int stagedSlot = -1;
+            for (int g = 0; g < E.groupCount; ++g)
+            {
+                DevGroup const G = model.groups[E.groupBegin + g];
+                if (G.cutoffSlot != stagedSlot)
                 {
-                    const bool narrow = (G.type == 3);
-                    for (int j = lane; j < n; j += 32)
+                    stageNeighbors<double, CAP>(nb, off, n, b, G.cutoffSlot, lane);
+                    stagedSlot = G.cutoffSlot;
+                }
+                const T rc = G.rc, rc2 = G.rc2;
+                for (int m0 = 0; m0 < G.memberCount; m0 += kC)
+                {
+                    const int mc = min(kC, G.memberCount - m0);
+                    const DevMember* mem = model.members + G.memberBegin + m0;
+                    T acc[kC], selfx[kC], selfy[kC], selfz[kC];
+    #pragma unroll
+                    for (int q = 0; q < kC; ++q) acc[q] = selfx[q] = selfy[q] = selfz[q] = 0.0;
+                    if (G.type == 2)
                     {
-                        const int ej = nb.e[j];
-                        const T rij = nb.d[j];
-                        if (!((ej == G.e1 || ej == G.e2) && rij < rc)) continue;
-                        const int needK = (ej == G.e1) ? G.e2 : G.e1;
-                        const T x1 = nb.x[j], y1 = nb.y[j], z1 = nb.z[j], fcij = nb.fc[j], dfcij = nb.dfc[j];
-                        const T r2ij = rij * rij;
-                        const int Hg = halfRange(j, n);
-                        T rowx[kC], rowy[kC], rowz[kC];
-#pragma unroll
-                        for (int q = 0; q < kC; ++q) rowx[q] = rowy[q] = rowz[q] = 0.0;
-                        for (int t = 1; t <= n - 1; ++t)
+                        for (int j = lane; j < n; j += 32)
                         {
-                            int k = j + t;
-                            if (k >= n) k -= n;
-                            if (nb.e[k] != needK || !(nb.d[k] < rc)) continue;
-                            const T x2 = nb.x[k], y2 = nb.y[k], z2 = nb.z[k];
-                            const T dx3 = x2 - x1, dy3 = y2 - y1, dz3 = z2 - z1;
-                            const T rjk2 = dx3 * dx3 + dy3 * dy3 + dz3 * dz3;
-                            if (narrow && !(rjk2 < rc2)) continue;
-                            const T rik = nb.d[k], fcik = nb.fc[k];
-                            T pfc, pr1, pr3 = 0.0, rjk = 0.0, r2sum;
-                            if (narrow)
-                            {
-                                rjk = sqrt(rjk2);
-                                double fcjk, dfcjk;
-                                cutoffFdf(model.cutoff[G.cutoffSlot], rjk, fcjk, dfcjk);
-                                pfc = fcij * fcik * fcjk;
-                                pr1 = fcik * fcjk * dfcij / rij;
-                                pr3 = fcij * fcik * dfcjk / rjk;
-                                r2sum = r2ij + rik * rik + rjk * rjk;
-                            }
-                            else
-                            {
-                                pfc = fcij * fcik;
-                                pr1 = fcik * dfcij / rij;
-                                r2sum = r2ij + rik * rik;
-                            }
-                            const T rinv = 1.0 / rij / rik;
-                            const T cost = (x1 * x2 + y1 * y2 + z1 * z2) * rinv;
-                            const bool countG = (t <= Hg);
-                            T vexp = 0.0, rijs = 0.0, rjks = 0.0;
-#pragma unroll
+                            if (nb.e[j] != G.e1 || !(nb.d[j] < rc)) continue;
+                            const T r = nb.d[j], fc = nb.fc[j], dfc = nb.dfc[j];
+                            const T x = nb.x[j], y = nb.y[j], z = nb.z[j];
+    #pragma unroll
                             for (int q = 0; q < kC; ++q)
                             {
                                 if (q < mc)
                                 {
                                     DevMember const& M = mem[q];
-                                    if (M.calcExp || q == 0)
-                                    {
-                                        if (M.rs > 0.0)
-                                        {
-                                            rijs = rij - M.rs;
-                                            const T riks = rik - M.rs;
-                                            rjks = rjk - M.rs;
-                                            vexp = exp(-M.eta * (narrow ? (rijs * rijs + riks * riks + rjks * rjks)
-                                                                        : (rijs * rijs + riks * riks)));
-                                        }
-                                        else vexp = exp(-M.eta * r2sum);
-                                    }
-                                    const T plambda = 1.0 + M.lambda * cost;
-                                    T fg = vexp;
-                                    if (plambda <= 0.0) fg = 0.0;
-                                    else
-                                    {
-                                        if (M.useIntPow) fg *= powInt<T>(plambda, M.zetaInt - 1);
-                                        else fg *= pow(plambda, M.zeta - 1.0);
-                                    }
-                                    if (countG) acc[q] += fg * plambda * pfc;
-                                    fg *= M.factorNorm;
-                                    const T pfczl = pfc * M.zetaLambda;
-                                    const T p2etapl = plambda * M.factorDeriv;
-                                    T p1, p3;
-                                    if (M.rs > 0.0)
-                                    {
-                                        p1 = fg * (pfczl * (rinv - cost / r2ij - p2etapl * rijs / rij) + pr1 * plambda);
-                                        p3 = narrow ? fg * (pfczl * (rinv + p2etapl * rjks / rjk) - pr3 * plambda)
-                                                    : fg * pfczl * rinv;
-                                    }
-                                    else
-                                    {
-                                        p1 = fg * (pfczl * (rinv - cost / r2ij - p2etapl) + pr1 * plambda);
-                                        p3 = narrow ? fg * (pfczl * (rinv + p2etapl) - pr3 * plambda)
-                                                    : fg * pfczl * rinv;
-                                    }
-                                    selfx[q] += p1 * x1;
-                                    selfy[q] += p1 * y1;
-                                    selfz[q] += p1 * z1;
-                                    rowx[q] -= p1 * x1 + p3 * dx3;
-                                    rowy[q] -= p1 * y1 + p3 * dy3;
-                                    rowz[q] -= p1 * z1 + p3 * dz3;
+                                    const T pexp = exp(-M.eta * (r - M.rs) * (r - M.rs));
+                                    acc[q] += pexp * fc;
+                                    const T p1 = M.factorNorm * (dfc - 2.0 * M.eta * (r - M.rs) * fc) * pexp / r;
+                                    selfx[q] += p1 * x;
+                                    selfy[q] += p1 * y;
+                                    selfz[q] += p1 * z;
+                                    double* p = b.dGdr + ((size_t)M.rowE1 * b.nbrCapacity + off + j) * 3;
+                                    p[0] -= p1 * x;
+                                    p[1] -= p1 * y;
+                                    p[2] -= p1 * z;
                                 }
                             }
                         }
-#pragma unroll
-                        for (int q = 0; q < kC; ++q)
+                    }
+                    else
+                    {
+                        const bool narrow = (G.type == 3);
+                        for (int j = lane; j < n; j += 32)
                         {
-                            if (q < mc)
+                            const int ej = nb.e[j];
+                            const T rij = nb.d[j];
+                            if (!((ej == G.e1 || ej == G.e2) && rij < rc)) continue;
+                            const int needK = (ej == G.e1) ? G.e2 : G.e1;
+                            const T x1 = nb.x[j], y1 = nb.y[j], z1 = nb.z[j], fcij = nb.fc[j], dfcij = nb.dfc[j];
+                            const T r2ij = rij * rij;
+                            const int Hg = halfRange(j, n);
+                            T rowx[kC], rowy[kC], rowz[kC];
+    #pragma unroll
+                            for (int q = 0; q < kC; ++q) rowx[q] = rowy[q] = rowz[q] = 0.0;
+                            for (int t = 1; t <= n - 1; ++t)
                             {
-                                const int row = (ej == G.e1) ? mem[q].rowE1 : mem[q].rowE2;
-                                double* p = b.dGdr + ((size_t)row * b.nbrCapacity + off + j) * 3;
-                                p[0] += rowx[q];
-                                p[1] += rowy[q];
-                                p[2] += rowz[q];
+                                int k = j + t;
+                                if (k >= n) k -= n;
+                                if (nb.e[k] != needK || !(nb.d[k] < rc)) continue;
+                                const T x2 = nb.x[k], y2 = nb.y[k], z2 = nb.z[k];
+                                const T dx3 = x2 - x1, dy3 = y2 - y1, dz3 = z2 - z1;
+                                const T rjk2 = dx3 * dx3 + dy3 * dy3 + dz3 * dz3;
+                                if (narrow && !(rjk2 < rc2)) continue;
+                                const T rik = nb.d[k], fcik = nb.fc[k];
+                                T pfc, pr1, pr3 = 0.0, rjk = 0.0, r2sum;
+                                if (narrow)
+                                {
+                                    rjk = sqrt(rjk2);
+                                    double fcjk, dfcjk;
+                                    cutoffFdf(model.cutoff[G.cutoffSlot], rjk, fcjk, dfcjk);
+                                    pfc = fcij * fcik * fcjk;
+                                    pr1 = fcik * fcjk * dfcij / rij;
+                                    pr3 = fcij * fcik * dfcjk / rjk;
+                                    r2sum = r2ij + rik * rik + rjk * rjk;
+                                }
+                                else
+                                {
+                                    pfc = fcij * fcik;
+                                    pr1 = fcik * dfcij / rij;
+                                    r2sum = r2ij + rik * rik;
+                                }
+                                const T rinv = 1.0 / rij / rik;
+                                const T cost = (x1 * x2 + y1 * y2 + z1 * z2) * rinv;
+                                const bool countG = (t <= Hg);
+                                T vexp = 0.0, rijs = 0.0, rjks = 0.0;
+    #pragma unroll
+                                for (int q = 0; q < kC; ++q)
+                                {
+                                    if (q < mc)
+                                    {
+                                        DevMember const& M = mem[q];
+                                        if (M.calcExp || q == 0)
+                                        {
+                                            if (M.rs > 0.0)
+                                            {
+                                                rijs = rij - M.rs;
+                                                const T riks = rik - M.rs;
+                                                rjks = rjk - M.rs;
+                                                vexp = exp(-M.eta * (narrow ? (rijs * rijs + riks * riks + rjks * rjks)
+                                                                            : (rijs * rijs + riks * riks)));
+                                            }
+                                            else vexp = exp(-M.eta * r2sum);
+                                        }
+                                        const T plambda = 1.0 + M.lambda * cost;
+                                        T fg = vexp;
+                                        if (plambda <= 0.0) fg = 0.0;
+                                        else
+                                        {
+                                            if (M.useIntPow) fg *= powInt<T>(plambda, M.zetaInt - 1);
+                                            else fg *= pow(plambda, M.zeta - 1.0);
+                                        }
+                                        if (countG) acc[q] += fg * plambda * pfc;
+                                        fg *= M.factorNorm;
+                                        const T pfczl = pfc * M.zetaLambda;
+                                        const T p2etapl = plambda * M.factorDeriv;
+                                        T p1, p3;
+                                        if (M.rs > 0.0)
+                                        {
+                                            p1 = fg * (pfczl * (rinv - cost / r2ij - p2etapl * rijs / rij) + pr1 * plambda);
+                                            p3 = narrow ? fg * (pfczl * (rinv + p2etapl * rjks / rjk) - pr3 * plambda)
+                                                        : fg * pfczl * rinv;
+                                        }
+                                        else
+                                        {
+                                            p1 = fg * (pfczl * (rinv - cost / r2ij - p2etapl) + pr1 * plambda);
+                                            p3 = narrow ? fg * (pfczl * (rinv + p2etapl) - pr3 * plambda)
+                                                        : fg * pfczl * rinv;
+                                        }
+                                        selfx[q] += p1 * x1;
+                                        selfy[q] += p1 * y1;
+                                        selfz[q] += p1 * z1;
+                                        rowx[q] -= p1 * x1 + p3 * dx3;
+                                        rowy[q] -= p1 * y1 + p3 * dy3;
+                                        rowz[q] -= p1 * z1 + p3 * dz3;
+                                    }
+                                }
+                            }
+    #pragma unroll
+                            for (int q = 0; q < kC; ++q)
+                            {
+                                if (q < mc)
+                                {
+                                    const int row = (ej == G.e1) ? mem[q].rowE1 : mem[q].rowE2;
+                                    double* p = b.dGdr + ((size_t)row * b.nbrCapacity + off + j) * 3;
+                                    p[0] += rowx[q];
+                                    p[1] += rowy[q];
+                                    p[2] += rowz[q];
+                                }
                             }
                         }
                     }
-                }
-#pragma unroll
-                for (int q = 0; q < kC; ++q)
-                {
-                    if (q < mc)
+    #pragma unroll
+                    for (int q = 0; q < kC; ++q)
                     {
-                        double s = warpSum(acc[q]);
-                        const double sx = warpSum(selfx[q]), sy = warpSum(selfy[q]), sz = warpSum(selfz[q]);
-                        if (lane == q)
+                        if (q < mc)
                         {
-                            DevMember const& M = mem[q];
-                            if (G.type != 2) s *= M.gNorm;
-                            b.G[(size_t)i * b.gStride + M.sf] = scaleG(model.scaling[E.sfBegin + M.sf], s);
-                            double* p = b.dGdrSelf + ((size_t)i * b.gStride + M.sf) * 3;
-                            p[0] = sx;
-                            p[1] = sy;
-                            p[2] = sz;
+                            double s = warpSum(acc[q]);
+                            const double sx = warpSum(selfx[q]), sy = warpSum(selfy[q]), sz = warpSum(selfz[q]);
+                            if (lane == q)
+                            {
+                                DevMember const& M = mem[q];
+                                if (G.type != 2) s *= M.gNorm;
+                                b.G[(size_t)i * b.gStride + M.sf] = scaleG(model.scaling[E.sfBegin + M.sf], s);
+                                double* p = b.dGdrSelf + ((size_t)i * b.gStride + M.sf) * 3;
+                                p[0] = sx;
+                                p[1] = sy;
+                                p[2] = sz;
+                            }
                         }
                     }
                 }
             }
         }
     }
+
 }
 
 // Per-entry contraction of stored dG/dr with dE/dG:

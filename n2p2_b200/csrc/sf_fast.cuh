@@ -763,192 +763,192 @@ __global__ void __launch_bounds__(WARPS * 32, (sfMinBlocks<T, WARPS, FAST, CUT, 
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     for (int k0 = 0; warp + k0 * warpsPerGrid < b.N; k0 += 32)
     {
-        unsigned todo =
-            __ballot_sync(kFullMask, atomInTier(b, warp + (k0 + (threadIdx.x & 31)) * warpsPerGrid, lower, CAP, flagOverflow != 0));
+        const int mine = warp + (k0 + (threadIdx.x & 31)) * warpsPerGrid;
+        unsigned todo = __ballot_sync(kFullMask, atomInTier(b, mine, lower, CAP, flagOverflow != 0));
         while (todo)
         {
             const int i = warp + (k0 + __ffs(todo) - 1) * warpsPerGrid;
             todo &= todo - 1;
-                const int64_t off = b.nbrOffset[i];
-                const int64_t end = b.nbrOffset[i + 1];
-                if (end > b.nbrCapacity) continue;
-                const int n = (int)(end - off);
-                if (flagOverflow && n > CAP)
+            const int64_t off = b.nbrOffset[i];
+            const int64_t end = b.nbrOffset[i + 1];
+            if (end > b.nbrCapacity) continue;
+            const int n = (int)(end - off);
+            if (flagOverflow && n > CAP)
+            {
+                if (lane == 0) atomicAdd(&b.status->badInput, 1);
+                continue;
+            }
+            if (!(n <= CAP && n > lower)) continue;
+            const int ec = b.elem[i];
+            DevElement const& E = model.el[ec];
+            uint32_t* maskOut =
+                (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
+            int mwi = 0;
+            stageGeometry<T, CAP>(S, off, n, model, b, lane);
+            int slot = -1;
+            for (int g = 0; g < E.groupCount; ++g)
+            {
+                DevGroup scratch;
+                DevGroup const& G = groupOf<FAST>(gt, model, E.groupBegin + g, scratch);
+                const bool fastG = FAST || G.fast;
+                if (G.cutoffSlot != slot)
                 {
-                    if (lane == 0) atomicAdd(&b.status->badInput, 1);
-                    continue;
+                    stageCutoff<T, CAP>(S, off, n, G.cutoffSlot, b, lane);
+                    slot = G.cutoffSlot;
                 }
-                if (!(n <= CAP && n > lower)) continue;
-                const int ec = b.elem[i];
-                DevElement const& E = model.el[ec];
-                uint32_t* maskOut =
-                    (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
-                int mwi = 0;
-                stageGeometry<T, CAP>(S, off, n, model, b, lane);
-                int slot = -1;
-                for (int g = 0; g < E.groupCount; ++g)
+                stageMembers(mb, model, G, nullptr, lane);
+                if (G.type != 2 && fastG) stageFactors<T, CAP>(S, G, lane);
+                const T rc = (T)G.rc, rc2 = (T)G.rc2;
+                const DevMember* mem = model.members + G.memberBegin;
+                const bool narrow = (G.type == 3);
+                const bool grid = (G.type != 2) && (FAST || G.grid);
+                const int mwiGroup = mwi;
+                for (int m0 = 0; m0 < G.memberCount; m0 += (grid ? G.memberCount : ACC))
                 {
-                    DevGroup scratch;
-                    DevGroup const& G = groupOf<FAST>(gt, model, E.groupBegin + g, scratch);
-                    const bool fastG = FAST || G.fast;
-                    if (G.cutoffSlot != slot)
+                    mwi = mwiGroup;   // every member chunk enumerates the same candidates; the first records them
+                    const int mc = min(ACC, G.memberCount - m0);
+                    T acc[ACC];
+    #pragma unroll
+                    for (int q = 0; q < ACC; ++q) acc[q] = T(0);
+                    if (G.type == 2)
                     {
-                        stageCutoff<T, CAP>(S, off, n, G.cutoffSlot, b, lane);
-                        slot = G.cutoffSlot;
-                    }
-                    stageMembers(mb, model, G, nullptr, lane);
-                    if (G.type != 2 && fastG) stageFactors<T, CAP>(S, G, lane);
-                    const T rc = (T)G.rc, rc2 = (T)G.rc2;
-                    const DevMember* mem = model.members + G.memberBegin;
-                    const bool narrow = (G.type == 3);
-                    const bool grid = (G.type != 2) && (FAST || G.grid);
-                    const int mwiGroup = mwi;
-                    for (int m0 = 0; m0 < G.memberCount; m0 += (grid ? G.memberCount : ACC))
-                    {
-                        mwi = mwiGroup;   // every member chunk enumerates the same candidates; the first records them
-                        const int mc = min(ACC, G.memberCount - m0);
-                        T acc[ACC];
-        #pragma unroll
-                        for (int q = 0; q < ACC; ++q) acc[q] = T(0);
-                        if (G.type == 2)
+                        for (int s = S.blockBegin[G.e1] + lane; s < S.blockBegin[G.e1 + 1]; s += 32)
                         {
-                            for (int s = S.blockBegin[G.e1] + lane; s < S.blockBegin[G.e1 + 1]; s += 32)
+                            const T r = S.r[s];
+                            if (!(r < rc)) continue;
+                            const T fc = S.fc[s];
+                            T eb[kMaxBases];
+    #pragma unroll
+                            for (int q = 0; q < kMaxBases; ++q)
+                                eb[q] = (fastG && q < G.numBases) ? fexp<T>(-groupBaseEta<T>(G, q) * r * r) : T(0);
+    #pragma unroll
+                            for (int q = 0; q < ACC; ++q)
                             {
-                                const T r = S.r[s];
-                                if (!(r < rc)) continue;
-                                const T fc = S.fc[s];
-                                T eb[kMaxBases];
-        #pragma unroll
-                                for (int q = 0; q < kMaxBases; ++q)
-                                    eb[q] = (fastG && q < G.numBases) ? fexp<T>(-groupBaseEta<T>(G, q) * r * r) : T(0);
-        #pragma unroll
-                                for (int q = 0; q < ACC; ++q)
+                                if (q < mc)
                                 {
-                                    if (q < mc)
+                                    const int qq = m0 + q;
+                                    T v;
+                                    if (fastG)
                                     {
-                                        const int qq = m0 + q;
-                                        T v;
-                                        if (fastG)
-                                        {
-                                            const int bq = mb.base[qq];
-                                            T e0 = eb[0];
-        #pragma unroll
-                                            for (int t = 1; t < kMaxBases; ++t)
-                                                if (bq == t) e0 = eb[t];
-                                            v = powUniform<T>(e0, mb.pw[qq]);
-                                        }
-                                        else v = gaussShifted<T>(mb.eta[qq], mb.rs[qq], r, mb.rs[qq], mb.rs[qq], 0);
-                                        acc[q] += v * fc;
+                                        const int bq = mb.base[qq];
+                                        T e0 = eb[0];
+    #pragma unroll
+                                        for (int t = 1; t < kMaxBases; ++t)
+                                            if (bq == t) e0 = eb[t];
+                                        v = powUniform<T>(e0, mb.pw[qq]);
                                     }
+                                    else v = gaussShifted<T>(mb.eta[qq], mb.rs[qq], r, mb.rs[qq], mb.rs[qq], 0);
+                                    acc[q] += v * fc;
                                 }
                             }
                         }
-                        else
+                    }
+                    else
+                    {
+                        const bool same = (G.e1 == G.e2);
+                        const int A0 = S.blockBegin[G.e1], nA = S.nBelow[G.cutoffSlot][G.e1];
+                        const int B0 = S.blockBegin[G.e2], nB = S.nBelow[G.cutoffSlot][G.e2];
+                        Phase ph[2];
+                        const int nph = roundPhases(A0, nA, B0, nB, same, ph);
+                        int qn = 0, qh = 0;
+                        for (int k = 0; k <= nph; ++k)
                         {
-                            const bool same = (G.e1 == G.e2);
-                            const int A0 = S.blockBegin[G.e1], nA = S.nBelow[G.cutoffSlot][G.e1];
-                            const int B0 = S.blockBegin[G.e2], nB = S.nBelow[G.cutoffSlot][G.e2];
-                            Phase ph[2];
-                            const int nph = roundPhases(A0, nA, B0, nB, same, ph);
-                            int qn = 0, qh = 0;
-                            for (int k = 0; k <= nph; ++k)
+                            const bool drain = (k == nph);
+                            Cursor cur;
+                            int cnt = 0;
+                            if (!drain)
                             {
-                                const bool drain = (k == nph);
-                                Cursor cur;
-                                int cnt = 0;
-                                if (!drain)
+                                cur.init(ph[k], lane);
+                                cnt = ph[k].count;
+                            }
+                            int p0 = 0;
+                            while (true)
+                            {
+                                if (qn < kStep && p0 < cnt)   // queue stays below kStep + 64 entries
                                 {
-                                    cur.init(ph[k], lane);
-                                    cnt = ph[k].count;
+                                    enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane,
+                                                              m0 == 0 ? maskOut : nullptr, nullptr, mwi);
+                                    p0 += 64;
                                 }
-                                int p0 = 0;
-                                while (true)
+                                if (qn >= kStep || (drain && qn > 0))
                                 {
-                                    if (qn < kStep && p0 < cnt)   // queue stays below kStep + 64 entries
+                                    const int take = min(kStep, qn);
+                                    if constexpr (FAST > 0)
                                     {
-                                        enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane,
-                                                                  m0 == 0 ? maskOut : nullptr, nullptr, mwi);
-                                        p0 += 64;
-                                    }
-                                    if (qn >= kStep || (drain && qn > 0))
-                                    {
-                                        const int take = min(kStep, qn);
-                                        if constexpr (FAST > 0)
+                                        Triplet<T> t[ILP];
+                                        int so[ILP], sp[ILP];
+                                        bool ok[ILP];
+                                        loadTriplets<CUT, T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh, take, lane,
+                                                             t, so, sp, ok);
+                                        T bv[ILP][kMaxStagedBases], cost[ILP], pfc[ILP];
+    #pragma unroll
+                                        for (int u = 0; u < ILP; ++u)
                                         {
-                                            Triplet<T> t[ILP];
-                                            int so[ILP], sp[ILP];
-                                            bool ok[ILP];
-                                            loadTriplets<CUT, T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh, take, lane,
-                                                                 t, so, sp, ok);
-                                            T bv[ILP][kMaxStagedBases], cost[ILP], pfc[ILP];
-        #pragma unroll
-                                            for (int u = 0; u < ILP; ++u)
-                                            {
-                                                tripletBases<T, CAP>(S, G, narrow, so[u], sp[u], t[u].rjk2, bv[u]);
-                                                cost[u] = t[u].cost;
-                                                pfc[u] = ok[u] ? t[u].fc1 * t[u].fc2 * t[u].fcjk : T(0);
-                                            }
-                                            gridValuesN<T, FAST, FAST, ILP, sfPowBits<FAST, CUT>()>(bv, G, cost, pfc, acc);
+                                            tripletBases<T, CAP>(S, G, narrow, so[u], sp[u], t[u].rjk2, bv[u]);
+                                            cost[u] = t[u].cost;
+                                            pfc[u] = ok[u] ? t[u].fc1 * t[u].fc2 * t[u].fcjk : T(0);
                                         }
-                                        else if (lane < take)
+                                        gridValuesN<T, FAST, FAST, ILP, sfPowBits<FAST, CUT>()>(bv, G, cost, pfc, acc);
+                                    }
+                                    else if (lane < take)
+                                    {
+                                        const int e = SM.queue[(qh + lane) & (kQueue - 1)];
+                                        const int so = entryOwner(e), sp = entryPartner(e);
+                                        Triplet<T> t;
+                                        loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
+                                        const T pfc = t.fc1 * t.fc2 * t.fcjk;
+                                        T bv[kMaxStagedBases];
+                                        if (fastG) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
+                                        T vexp = T(0);
+                                        if (grid)
                                         {
-                                            const int e = SM.queue[(qh + lane) & (kQueue - 1)];
-                                            const int so = entryOwner(e), sp = entryPartner(e);
-                                            Triplet<T> t;
-                                            loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
-                                            const T pfc = t.fc1 * t.fc2 * t.fcjk;
-                                            T bv[kMaxStagedBases];
-                                            if (fastG) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
-                                            T vexp = T(0);
-                                            if (grid)
+                                            if (G.gridNZ <= 2) gridValues<T, 2, 4>(bv, G, t.cost, pfc, acc);
+                                            else gridValues<T, 4, 4>(bv, G, t.cost, pfc, acc);
+                                        }
+                                        else
+                                        {
+    #pragma unroll
+                                            for (int q = 0; q < ACC; ++q)
                                             {
-                                                if (G.gridNZ <= 2) gridValues<T, 2, 4>(bv, G, t.cost, pfc, acc);
-                                                else gridValues<T, 4, 4>(bv, G, t.cost, pfc, acc);
-                                            }
-                                            else
-                                            {
-        #pragma unroll
-                                                for (int q = 0; q < ACC; ++q)
+                                                if (q < mc)
                                                 {
-                                                    if (q < mc)
-                                                    {
-                                                        const int qq = m0 + q;
-                                                        if ((mb.flags[qq] & 2) || q == 0)
-                                                            vexp = fastG ? powUniform<T>(mb.base[qq] == 0 ? bv[0] : bv[1], mb.pw[qq])
-                                                                         : gaussShifted<T>(mb.eta[qq], mb.rs[qq], t.r1, t.r2,
-                                                                                           t.rjk, narrow ? 1 : 0);
-                                                        const T pl = T(1) + mb.lambda[qq] * t.cost;
-                                                        if (pl > T(0)) acc[q] += vexp * angularPow<T>(pl, mb, qq) * pl * pfc;
-                                                    }
+                                                    const int qq = m0 + q;
+                                                    if ((mb.flags[qq] & 2) || q == 0)
+                                                        vexp = fastG ? powUniform<T>(mb.base[qq] == 0 ? bv[0] : bv[1], mb.pw[qq])
+                                                                     : gaussShifted<T>(mb.eta[qq], mb.rs[qq], t.r1, t.r2,
+                                                                                       t.rjk, narrow ? 1 : 0);
+                                                    const T pl = T(1) + mb.lambda[qq] * t.cost;
+                                                    if (pl > T(0)) acc[q] += vexp * angularPow<T>(pl, mb, qq) * pl * pfc;
                                                 }
                                             }
                                         }
-                                        qh = (qh + take) & (kQueue - 1);
-                                        qn -= take;
-                                        __syncwarp();
                                     }
-                                    else if (p0 >= cnt) break;
+                                    qh = (qh + take) & (kQueue - 1);
+                                    qn -= take;
+                                    __syncwarp();
                                 }
+                                else if (p0 >= cnt) break;
                             }
                         }
-        #pragma unroll
-                        for (int q = 0; q < ACC; ++q)
+                    }
+    #pragma unroll
+                    for (int q = 0; q < ACC; ++q)
+                    {
+                        const int c = FAST ? (q / (FAST ? FAST : 1)) * 4 + q % (FAST ? FAST : 1) : q;
+                        const int qq = grid ? (int)G.comboMember[c] : (q < mc ? m0 + q : -1);
+                        if (qq >= 0)
                         {
-                            const int c = FAST ? (q / (FAST ? FAST : 1)) * 4 + q % (FAST ? FAST : 1) : q;
-                            const int qq = grid ? (int)G.comboMember[c] : (q < mc ? m0 + q : -1);
-                            if (qq >= 0)
+                            double sum = warpSum((double)acc[q]);
+                            if (lane == (q & 31))
                             {
-                                double sum = warpSum((double)acc[q]);
-                                if (lane == (q & 31))
-                                {
-                                    DevMember const& M = mem[qq];
-                                    if (G.type != 2) sum *= M.gNorm;
-                                    b.G[(size_t)i * b.gStride + M.sf] = scaleG(model.scaling[E.sfBegin + M.sf], sum);
-                                }
+                                DevMember const& M = mem[qq];
+                                if (G.type != 2) sum *= M.gNorm;
+                                b.G[(size_t)i * b.gStride + M.sf] = scaleG(model.scaling[E.sfBegin + M.sf], sum);
                             }
                         }
                     }
                 }
+            }
         }
     }
 
@@ -1065,261 +1065,261 @@ __global__ void __launch_bounds__(WARPS * 32, (sfMinBlocks<T, WARPS, FAST, CUT, 
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     for (int k0 = 0; warp + k0 * warpsPerGrid < b.N; k0 += 32)
     {
-        unsigned todo =
-            __ballot_sync(kFullMask, atomInTier(b, warp + (k0 + (threadIdx.x & 31)) * warpsPerGrid, lower, CAP, false));
+        const int mine = warp + (k0 + (threadIdx.x & 31)) * warpsPerGrid;
+        unsigned todo = __ballot_sync(kFullMask, atomInTier(b, mine, lower, CAP, false));
         while (todo)
         {
             const int i = warp + (k0 + __ffs(todo) - 1) * warpsPerGrid;
             todo &= todo - 1;
-                const int64_t off = b.nbrOffset[i];
-                const int64_t end = b.nbrOffset[i + 1];
-                if (end > b.nbrCapacity) continue;
-                const int n = (int)(end - off);
-                if (!(n <= CAP && n > lower)) continue;
-                const int ec = b.elem[i];
-                DevElement const& E = model.el[ec];
-                const double* dEdG = b.dEdG + (size_t)i * b.gStride;
-                const uint32_t* maskIn =
-                    (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
-                int mwi = 0;
-                stageGeometry<T, CAP>(S, off, n, model, b, lane);
-                for (int s = lane; s < n; s += 32) SM.h[0][s] = SM.h[1][s] = SM.h[2][s] = T(0);
-                // self force: the FP64 form sums every term into gs*; the FP32 form
-                // sums a group's terms in FP32 and adds each group's total to sf* in FP64
-                double sfx = 0.0, sfy = 0.0, sfz = 0.0;
-                T gsx = T(0), gsy = T(0), gsz = T(0);
-                int slot = -1;
-                for (int g = 0; g < E.groupCount; ++g)
-                {
-                    if constexpr (sizeof(T) == 4)
-                    {
-                        sfx += (double)gsx;
-                        sfy += (double)gsy;
-                        sfz += (double)gsz;
-                        gsx = gsy = gsz = T(0);
-                    }
-                    DevGroup scratch;
-                    DevGroup const& G = groupOf<FAST>(gt, model, E.groupBegin + g, scratch);
-                    const bool fastG = FAST || G.fast;
-                    if (G.cutoffSlot != slot)
-                    {
-                        stageCutoff<T, CAP>(S, off, n, G.cutoffSlot, b, lane);
-                        slot = G.cutoffSlot;
-                    }
-                    stageMembers(mb, model, G, dEdG, lane);
-                    const int M = G.memberCount;
-                    const T rc = (T)G.rc, rc2 = (T)G.rc2;
-                    if (G.type == 2)
-                    {
-                        for (int s = S.blockBegin[G.e1] + lane; s < S.blockBegin[G.e1 + 1]; s += 32)
-                        {
-                            const T r = S.r[s];
-                            if (!(r < rc)) continue;
-                            const T fc = S.fc[s], dfc = S.dfcr[s] * r, ri = S.rinv[s];
-                            T eb[kMaxBases];
-        #pragma unroll
-                            for (int q = 0; q < kMaxBases; ++q)
-                                eb[q] = (fastG && q < G.numBases) ? fexp<T>(-groupBaseEta<T>(G, q) * r * r) : T(0);
-                            T P = T(0);
-                            for (int q = 0; q < M; ++q)
-                            {
-                                T v;
-                                if (fastG)
-                                {
-                                    const int bq = mb.base[q];
-                                    T e0 = eb[0];
-        #pragma unroll
-                                    for (int t = 1; t < kMaxBases; ++t)
-                                        if (bq == t) e0 = eb[t];
-                                    v = powUniform<T>(e0, mb.pw[q]);
-                                }
-                                else v = gaussShifted<T>(mb.eta[q], mb.rs[q], r, mb.rs[q], mb.rs[q], 0);
-                                P += mb.cw[q] * (dfc - T(2) * mb.eta[q] * (r - mb.rs[q]) * fc) * v * ri;
-                            }
-                            const T ddx = S.x[s] * P, ddy = S.y[s] * P, ddz = S.z[s] * P;
-                            SM.h[0][s] += ddx;
-                            SM.h[1][s] += ddy;
-                            SM.h[2][s] += ddz;
-                            gsx -= ddx;
-                            gsy -= ddy;
-                            gsz -= ddz;
-                        }
-                        __syncwarp();
-                        continue;
-                    }
-                    if (fastG) stageFactors<T, CAP>(S, G, lane);
-                    const bool narrow = (G.type == 3);
-                    const bool same = (G.e1 == G.e2);
-                    const int A0 = S.blockBegin[G.e1], nA = S.nBelow[G.cutoffSlot][G.e1];
-                    const int B0 = S.blockBegin[G.e2], nB = S.nBelow[G.cutoffSlot][G.e2];
-                    Phase ph[2];
-                    const int nph = roundPhases(A0, nA, B0, nB, same, ph);
-                    int qn = 0, qh = 0;
-                    for (int k = 0; k <= nph; ++k)
-                    {
-                        const bool drain = (k == nph);
-                        Cursor cur;
-                        int cnt = 0;
-                        if (!drain)
-                        {
-                            cur.init(ph[k], lane);
-                            cnt = ph[k].count;
-                        }
-                        int p0 = 0;
-                        while (true)
-                        {
-                            if (qn < kStep && p0 < cnt)   // queue stays below kStep + 64 entries
-                            {
-                                enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane,
-                                                          nullptr, maskIn, mwi);
-                                p0 += 64;
-                            }
-                            if constexpr (FAST > 0)
-                            {
-                                if (qn >= kStep || (drain && qn > 0))
-                                {
-                                    const int take = min(kStep, qn);
-                                    forcesStepN<T, CAP, FAST, CUT, ILP>(S, mb, G, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh,
-                                                                  take, lane, SM.h, gsx, gsy, gsz);
-                                    qh = (qh + take) & (kQueue - 1);
-                                    qn -= take;
-                                    __syncwarp();
-                                }
-                                else if (p0 >= cnt) break;
-                                continue;
-                            }
-                            if (qn >= 32 || (drain && qn > 0))
-                            {
-                                const int take = min(32, qn);
-                                int keyO = 0, keyP = 0;
-                                T ox = T(0), oy = T(0), oz = T(0), px = T(0), py = T(0), pz = T(0);
-                                if (lane < take)
-                                {
-                                    const int e = SM.queue[(qh + lane) & (kQueue - 1)];
-                                    const int so = entryOwner(e), sp = entryPartner(e);
-                                    keyO = so;
-                                    keyP = sp;
-                                    Triplet<T> t;
-                                    loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
-                                    const T dfcr2 = S.dfcr[sp];
-                                    const T pfc = t.fc1 * t.fc2 * t.fcjk;
-                                    const T pr1 = t.fc2 * t.fcjk * t.dfcr1;
-                                    const T pr2 = t.fc1 * t.fcjk * dfcr2;
-                                    const T pr3 = narrow ? t.fc1 * t.fc2 * t.dfcjk * t.rijk : T(0);
-                                    T bv[kMaxStagedBases];
-                                    if (fastG) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
-                                    T T1 = T(0), T3 = T(0), Uij = T(0), Uik = T(0), Ujk = T(0), vexp = T(0);
-                                    if (G.grid)
-                                    {
-                                        T T2 = T(0);
-                                        if (G.gridNZ <= 2) gridForces<T, 2>(bv, G, mb, t.cost, T1, T2, T3);
-                                        else gridForces<T, 4>(bv, G, mb, t.cost, T1, T2, T3);
-                                        Uij = T2;
-                                        Uik = T2;
-                                        Ujk = T2;
-                                    }
-                                    else
-                                    {
-                                    for (int q = 0; q < M; ++q)
-                                    {
-                                        if ((mb.flags[q] & 2) || q == 0)
-                                            vexp = fastG ? powUniform<T>(mb.base[q] == 0 ? bv[0] : bv[1], mb.pw[q])
-                                                          : gaussShifted<T>(mb.eta[q], mb.rs[q], t.r1, t.r2, t.rjk,
-                                                                            narrow ? 1 : 0);
-                                        const T pl = T(1) + mb.lambda[q] * t.cost;
-                                        if (!(pl > T(0))) continue;
-                                        const T a = mb.cw[q] * vexp * angularPow<T>(pl, mb, q);
-                                        const T azl = a * mb.zl[q];
-                                        const T azq = azl * pl * mb.fd[q];
-                                        T1 += azl;
-                                        T3 += a * pl;
-                                        if (mb.rs[q] > T(0))
-                                        {
-                                            Uij += azq * (t.r1 - mb.rs[q]) * t.ri1;
-                                            Uik += azq * (t.r2 - mb.rs[q]) * t.ri2;
-                                            if (narrow) Ujk += azq * (t.rjk - mb.rs[q]) * t.rijk;
-                                        }
-                                        else
-                                        {
-                                            Uij += azq;
-                                            Uik += azq;
-                                            Ujk += azq;
-                                        }
-                                    }
-                                    }
-                                    // both ends of the unordered pair (j, k): P1 for j, P2 (= P1 with j, k
-                                    // exchanged) for k; P3 is symmetric and enters with opposite signs.
-                                    const T P1 = pfc * ((t.rinv - t.cost * t.ri1 * t.ri1) * T1 - Uij) + pr1 * T3;
-                                    const T P2 = pfc * ((t.rinv - t.cost * t.ri2 * t.ri2) * T1 - Uik) + pr2 * T3;
-                                    const T P3 = narrow ? (pfc * (t.rinv * T1 + Ujk) - pr3 * T3) : (pfc * t.rinv * T1);
-                                    ox = P1 * t.x1 + P3 * t.dx3;
-                                    oy = P1 * t.y1 + P3 * t.dy3;
-                                    oz = P1 * t.z1 + P3 * t.dz3;
-                                    px = P2 * t.x2 - P3 * t.dx3;
-                                    py = P2 * t.y2 - P3 * t.dy3;
-                                    pz = P2 * t.z2 - P3 * t.dz3;
-                                    gsx -= P1 * t.x1 + P2 * t.x2;
-                                    gsy -= P1 * t.y1 + P2 * t.y2;
-                                    gsz -= P1 * t.z1 + P2 * t.z2;
-                                }
-                                // One conflict-free add per round present in the batch: inside a
-                                // round no slot occurs twice.
-                                const int rnd = lane < take ? entryRound(SM.queue[(qh + lane) & (kQueue - 1)]) : -1;
-                                const int prevRnd = __shfl_up_sync(kFullMask, rnd, 1);
-                                const unsigned heads = __ballot_sync(kFullMask, lane < take && (lane == 0 || prevRnd != rnd));
-                                const int mySub = __popc(heads & ((2u << lane) - 1u)) - 1;
-                                const int nSub = __popc(heads);
-                                for (int r = 0; r < nSub; ++r)
-                                {
-                                    if (lane < take && mySub == r)
-                                    {
-                                        SM.h[0][keyO] += ox;
-                                        SM.h[1][keyO] += oy;
-                                        SM.h[2][keyO] += oz;
-                                        SM.h[0][keyP] += px;
-                                        SM.h[1][keyP] += py;
-                                        SM.h[2][keyP] += pz;
-                                    }
-                                    __syncwarp();
-                                }
-                                qh = (qh + take) & (kQueue - 1);
-                                qn -= take;
-                                __syncwarp();
-                            }
-                            else if (p0 >= cnt) break;
-                        }
-                    }
-                }
-                __syncwarp();
-                for (int s = lane; s < n; s += 32)
-                {
-                    const int64_t e = off + S.perm[s];
-                    b.hx[e] = (double)SM.h[0][s];
-                    b.hy[e] = (double)SM.h[1][s];
-                    b.hz[e] = (double)SM.h[2][s];
-                }
+            const int64_t off = b.nbrOffset[i];
+            const int64_t end = b.nbrOffset[i + 1];
+            if (end > b.nbrCapacity) continue;
+            const int n = (int)(end - off);
+            if (!(n <= CAP && n > lower)) continue;
+            const int ec = b.elem[i];
+            DevElement const& E = model.el[ec];
+            const double* dEdG = b.dEdG + (size_t)i * b.gStride;
+            const uint32_t* maskIn =
+                (b.candMask && b.maskOffset[i + 1] <= b.maskCapacity) ? b.candMask + b.maskOffset[i] : nullptr;
+            int mwi = 0;
+            stageGeometry<T, CAP>(S, off, n, model, b, lane);
+            for (int s = lane; s < n; s += 32) SM.h[0][s] = SM.h[1][s] = SM.h[2][s] = T(0);
+            // self force: the FP64 form sums every term into gs*; the FP32 form
+            // sums a group's terms in FP32 and adds each group's total to sf* in FP64
+            double sfx = 0.0, sfy = 0.0, sfz = 0.0;
+            T gsx = T(0), gsy = T(0), gsz = T(0);
+            int slot = -1;
+            for (int g = 0; g < E.groupCount; ++g)
+            {
                 if constexpr (sizeof(T) == 4)
                 {
                     sfx += (double)gsx;
                     sfy += (double)gsy;
                     sfz += (double)gsz;
+                    gsx = gsy = gsz = T(0);
                 }
-                else
+                DevGroup scratch;
+                DevGroup const& G = groupOf<FAST>(gt, model, E.groupBegin + g, scratch);
+                const bool fastG = FAST || G.fast;
+                if (G.cutoffSlot != slot)
                 {
-                    sfx = gsx;
-                    sfy = gsy;
-                    sfz = gsz;
+                    stageCutoff<T, CAP>(S, off, n, G.cutoffSlot, b, lane);
+                    slot = G.cutoffSlot;
                 }
-                sfx = warpSum(sfx);
-                sfy = warpSum(sfy);
-                sfz = warpSum(sfz);
-                if (lane == 0)
+                stageMembers(mb, model, G, dEdG, lane);
+                const int M = G.memberCount;
+                const T rc = (T)G.rc, rc2 = (T)G.rc2;
+                if (G.type == 2)
                 {
-                    b.fSelf[3 * (size_t)i + 0] = sfx;
-                    b.fSelf[3 * (size_t)i + 1] = sfy;
-                    b.fSelf[3 * (size_t)i + 2] = sfz;
+                    for (int s = S.blockBegin[G.e1] + lane; s < S.blockBegin[G.e1 + 1]; s += 32)
+                    {
+                        const T r = S.r[s];
+                        if (!(r < rc)) continue;
+                        const T fc = S.fc[s], dfc = S.dfcr[s] * r, ri = S.rinv[s];
+                        T eb[kMaxBases];
+    #pragma unroll
+                        for (int q = 0; q < kMaxBases; ++q)
+                            eb[q] = (fastG && q < G.numBases) ? fexp<T>(-groupBaseEta<T>(G, q) * r * r) : T(0);
+                        T P = T(0);
+                        for (int q = 0; q < M; ++q)
+                        {
+                            T v;
+                            if (fastG)
+                            {
+                                const int bq = mb.base[q];
+                                T e0 = eb[0];
+    #pragma unroll
+                                for (int t = 1; t < kMaxBases; ++t)
+                                    if (bq == t) e0 = eb[t];
+                                v = powUniform<T>(e0, mb.pw[q]);
+                            }
+                            else v = gaussShifted<T>(mb.eta[q], mb.rs[q], r, mb.rs[q], mb.rs[q], 0);
+                            P += mb.cw[q] * (dfc - T(2) * mb.eta[q] * (r - mb.rs[q]) * fc) * v * ri;
+                        }
+                        const T ddx = S.x[s] * P, ddy = S.y[s] * P, ddz = S.z[s] * P;
+                        SM.h[0][s] += ddx;
+                        SM.h[1][s] += ddy;
+                        SM.h[2][s] += ddz;
+                        gsx -= ddx;
+                        gsy -= ddy;
+                        gsz -= ddz;
+                    }
+                    __syncwarp();
+                    continue;
                 }
-                __syncwarp();
+                if (fastG) stageFactors<T, CAP>(S, G, lane);
+                const bool narrow = (G.type == 3);
+                const bool same = (G.e1 == G.e2);
+                const int A0 = S.blockBegin[G.e1], nA = S.nBelow[G.cutoffSlot][G.e1];
+                const int B0 = S.blockBegin[G.e2], nB = S.nBelow[G.cutoffSlot][G.e2];
+                Phase ph[2];
+                const int nph = roundPhases(A0, nA, B0, nB, same, ph);
+                int qn = 0, qh = 0;
+                for (int k = 0; k <= nph; ++k)
+                {
+                    const bool drain = (k == nph);
+                    Cursor cur;
+                    int cnt = 0;
+                    if (!drain)
+                    {
+                        cur.init(ph[k], lane);
+                        cnt = ph[k].count;
+                    }
+                    int p0 = 0;
+                    while (true)
+                    {
+                        if (qn < kStep && p0 < cnt)   // queue stays below kStep + 64 entries
+                        {
+                            enqueueCandidates<T, CAP>(S, ph[k], cur, p0, rc, rc2, narrow, SM.queue, qh, qn, lane,
+                                                      nullptr, maskIn, mwi);
+                            p0 += 64;
+                        }
+                        if constexpr (FAST > 0)
+                        {
+                            if (qn >= kStep || (drain && qn > 0))
+                            {
+                                const int take = min(kStep, qn);
+                                forcesStepN<T, CAP, FAST, CUT, ILP>(S, mb, G, model.cutoff[G.cutoffSlot], narrow, SM.queue, qh,
+                                                              take, lane, SM.h, gsx, gsy, gsz);
+                                qh = (qh + take) & (kQueue - 1);
+                                qn -= take;
+                                __syncwarp();
+                            }
+                            else if (p0 >= cnt) break;
+                            continue;
+                        }
+                        if (qn >= 32 || (drain && qn > 0))
+                        {
+                            const int take = min(32, qn);
+                            int keyO = 0, keyP = 0;
+                            T ox = T(0), oy = T(0), oz = T(0), px = T(0), py = T(0), pz = T(0);
+                            if (lane < take)
+                            {
+                                const int e = SM.queue[(qh + lane) & (kQueue - 1)];
+                                const int so = entryOwner(e), sp = entryPartner(e);
+                                keyO = so;
+                                keyP = sp;
+                                Triplet<T> t;
+                                loadTriplet<T, CAP>(S, model.cutoff[G.cutoffSlot], narrow, so, sp, t);
+                                const T dfcr2 = S.dfcr[sp];
+                                const T pfc = t.fc1 * t.fc2 * t.fcjk;
+                                const T pr1 = t.fc2 * t.fcjk * t.dfcr1;
+                                const T pr2 = t.fc1 * t.fcjk * dfcr2;
+                                const T pr3 = narrow ? t.fc1 * t.fc2 * t.dfcjk * t.rijk : T(0);
+                                T bv[kMaxStagedBases];
+                                if (fastG) tripletBases<T, CAP>(S, G, narrow, so, sp, t.rjk2, bv);
+                                T T1 = T(0), T3 = T(0), Uij = T(0), Uik = T(0), Ujk = T(0), vexp = T(0);
+                                if (G.grid)
+                                {
+                                    T T2 = T(0);
+                                    if (G.gridNZ <= 2) gridForces<T, 2>(bv, G, mb, t.cost, T1, T2, T3);
+                                    else gridForces<T, 4>(bv, G, mb, t.cost, T1, T2, T3);
+                                    Uij = T2;
+                                    Uik = T2;
+                                    Ujk = T2;
+                                }
+                                else
+                                {
+                                for (int q = 0; q < M; ++q)
+                                {
+                                    if ((mb.flags[q] & 2) || q == 0)
+                                        vexp = fastG ? powUniform<T>(mb.base[q] == 0 ? bv[0] : bv[1], mb.pw[q])
+                                                      : gaussShifted<T>(mb.eta[q], mb.rs[q], t.r1, t.r2, t.rjk,
+                                                                        narrow ? 1 : 0);
+                                    const T pl = T(1) + mb.lambda[q] * t.cost;
+                                    if (!(pl > T(0))) continue;
+                                    const T a = mb.cw[q] * vexp * angularPow<T>(pl, mb, q);
+                                    const T azl = a * mb.zl[q];
+                                    const T azq = azl * pl * mb.fd[q];
+                                    T1 += azl;
+                                    T3 += a * pl;
+                                    if (mb.rs[q] > T(0))
+                                    {
+                                        Uij += azq * (t.r1 - mb.rs[q]) * t.ri1;
+                                        Uik += azq * (t.r2 - mb.rs[q]) * t.ri2;
+                                        if (narrow) Ujk += azq * (t.rjk - mb.rs[q]) * t.rijk;
+                                    }
+                                    else
+                                    {
+                                        Uij += azq;
+                                        Uik += azq;
+                                        Ujk += azq;
+                                    }
+                                }
+                                }
+                                // both ends of the unordered pair (j, k): P1 for j, P2 (= P1 with j, k
+                                // exchanged) for k; P3 is symmetric and enters with opposite signs.
+                                const T P1 = pfc * ((t.rinv - t.cost * t.ri1 * t.ri1) * T1 - Uij) + pr1 * T3;
+                                const T P2 = pfc * ((t.rinv - t.cost * t.ri2 * t.ri2) * T1 - Uik) + pr2 * T3;
+                                const T P3 = narrow ? (pfc * (t.rinv * T1 + Ujk) - pr3 * T3) : (pfc * t.rinv * T1);
+                                ox = P1 * t.x1 + P3 * t.dx3;
+                                oy = P1 * t.y1 + P3 * t.dy3;
+                                oz = P1 * t.z1 + P3 * t.dz3;
+                                px = P2 * t.x2 - P3 * t.dx3;
+                                py = P2 * t.y2 - P3 * t.dy3;
+                                pz = P2 * t.z2 - P3 * t.dz3;
+                                gsx -= P1 * t.x1 + P2 * t.x2;
+                                gsy -= P1 * t.y1 + P2 * t.y2;
+                                gsz -= P1 * t.z1 + P2 * t.z2;
+                            }
+                            // One conflict-free add per round present in the batch: inside a
+                            // round no slot occurs twice.
+                            const int rnd = lane < take ? entryRound(SM.queue[(qh + lane) & (kQueue - 1)]) : -1;
+                            const int prevRnd = __shfl_up_sync(kFullMask, rnd, 1);
+                            const unsigned heads = __ballot_sync(kFullMask, lane < take && (lane == 0 || prevRnd != rnd));
+                            const int mySub = __popc(heads & ((2u << lane) - 1u)) - 1;
+                            const int nSub = __popc(heads);
+                            for (int r = 0; r < nSub; ++r)
+                            {
+                                if (lane < take && mySub == r)
+                                {
+                                    SM.h[0][keyO] += ox;
+                                    SM.h[1][keyO] += oy;
+                                    SM.h[2][keyO] += oz;
+                                    SM.h[0][keyP] += px;
+                                    SM.h[1][keyP] += py;
+                                    SM.h[2][keyP] += pz;
+                                }
+                                __syncwarp();
+                            }
+                            qh = (qh + take) & (kQueue - 1);
+                            qn -= take;
+                            __syncwarp();
+                        }
+                        else if (p0 >= cnt) break;
+                    }
+                }
+            }
+            __syncwarp();
+            for (int s = lane; s < n; s += 32)
+            {
+                const int64_t e = off + S.perm[s];
+                b.hx[e] = (double)SM.h[0][s];
+                b.hy[e] = (double)SM.h[1][s];
+                b.hz[e] = (double)SM.h[2][s];
+            }
+            if constexpr (sizeof(T) == 4)
+            {
+                sfx += (double)gsx;
+                sfy += (double)gsy;
+                sfz += (double)gsz;
+            }
+            else
+            {
+                sfx = gsx;
+                sfy = gsy;
+                sfz = gsz;
+            }
+            sfx = warpSum(sfx);
+            sfy = warpSum(sfy);
+            sfz = warpSum(sfz);
+            if (lane == 0)
+            {
+                b.fSelf[3 * (size_t)i + 0] = sfx;
+                b.fSelf[3 * (size_t)i + 1] = sfy;
+                b.fSelf[3 * (size_t)i + 2] = sfz;
+            }
+            __syncwarp();
         }
     }
 
