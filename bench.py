@@ -465,9 +465,9 @@ def bench_large(steps, warmup, device):
     res["mixed"]["err_vs_fp64_gpu"] = {"energy_meV_per_atom": float(de), "force_meV_per_A_max": float(df.max()),
                                        "force_meV_per_A_rms": float(np.sqrt((df ** 2).mean()))}
     out.update(res)
-    out["network"] = ("FP64 form: CUDA-core kernel (warp per atom); mixed form: tcgen05 tensor-core products with "
-                      "split-bfloat16 operands and FP32 accumulators (tensor-pipe utilisation is an ncu counter, "
-                      "not measured here)")
+    out["network"] = ("FP64 form: CUDA-core kernel over 16-atom tiles (the 56-64-64-1 stage does not fit 32-atom "
+                      "tiles); mixed form: tcgen05 tensor-core products with split-bfloat16 operands and FP32 "
+                      "accumulators (tensor-pipe activity is an ncu counter: profiles/ncu_network_tc_water110k_mixed.md)")
     mode.close()
     return out
 
