@@ -185,8 +185,8 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded water boxes)",
-            "config": {"workload": "2048 water boxes, 32-512 molecules log-uniform (%d atoms), water40 model, FP64"
-                       % total_atoms, "boxes": args.boxes, "atoms": total_atoms,
+            "config": {"workload": "%d water boxes, 32-512 molecules log-uniform (%d atoms), water40 model, FP64"
+                       % (args.boxes, total_atoms), "boxes": args.boxes, "atoms": total_atoms,
                        "timed_sample": "%d of the %d structures (%d atoms) per step" % (len(sample), len(structs), natoms),
                        "full_workload_ms_estimate": 1000.0 * total_atoms / v},
             "cpu_baseline": {"value": v, "unit": "atoms/s", "cores": threads, "kind": "reference",
@@ -387,9 +387,9 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded water boxes)",
-                "config": {"workload": "2048 water boxes, 32-512 molecules log-uniform (%d atoms per GPU), "
+                "config": {"workload": "%d water boxes, 32-512 molecules log-uniform (%d atoms per GPU), "
                                        "water40 model (40 SFs/element, 40-25-25-1 softplus), plain FP64, "
-                                       "one CUDA-graph launch per step" % natoms,
+                                       "one CUDA-graph launch per step" % (args.boxes, natoms),
                            "boxes": args.boxes, "atoms_per_gpu": natoms,
                            "neighbor_entries_per_gpu": work["entries"],
                            "l2": "inputs larger than L2 (neighbour data %.1f GB per step)" % (
