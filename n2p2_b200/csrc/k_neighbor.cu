@@ -334,7 +334,9 @@ __device__ __forceinline__ void rankKeys32(const int* keys, int n, int lane, int
     }
 }
 
-__global__ void __launch_bounds__(256) kNeighborSort(
+// Four blocks per SM (at most 64 registers): the sort waits on global loads,
+// and 32 resident warps hide more of that wait than the 24 that 80 registers allow.
+__global__ void __launch_bounds__(256, 4) kNeighborSort(
     int N, const int* __restrict__ atomStruct, const DevStructInfo* __restrict__ info,
     const int64_t* __restrict__ nbrOffset, int64_t capacity, const int64_t* __restrict__ scrKey,
     const double* __restrict__ scrD, const double* __restrict__ scrDx, const double* __restrict__ scrDy,
